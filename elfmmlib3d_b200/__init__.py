@@ -1,0 +1,260 @@
+"""B200-native elastostatic triangle-layer-potential FMM.
+
+Python host layer over the C ABI of ``libelfmm3d_b200.so`` (declared in
+``include/elfmm3d_b200.h``).  The functions mirror the reference's Fortran
+routines (same names, argument meaning, array layouts and ``ier`` codes):
+
+    elfmm3dtria(iprec, rlam, rmu, triangle, trinorm, source, ...)
+        -> src/elfmm3dtria.f:71
+    elfmm3dtriatarg(iprec, rlam, rmu, triangle, trinorm, source, ..., target=...)
+        -> src/elfmm3dtria.f:162
+    el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, ...)
+        -> src/elfmm3dtria.f:1483
+
+Arrays are numpy, shaped in C order as the transpose of the Fortran shapes:
+``triangle`` (n,3,3) [triangle][vertex][xyz], ``sigma`` (n,3), ``ptfrc`` (n,3),
+``strain`` (n,3,3).  Outputs carry no 1/(4 pi) factor, like the reference.
+
+There is no CPU fallback: if the CUDA library is missing or no GPU is
+visible, every compute call raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "Plan", "load",
+           "library_path", "device_count", "ElfmmError"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libelfmm3d_b200.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+_llp = ctypes.POINTER(ctypes.c_longlong)
+_fp = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+# symbols the library must export (checked by the CPU test suite)
+EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_device_count",
+           "efmm_plan_create", "efmm_plan_destroy", "efmm_plan_set_geometry",
+           "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings",
+           "efmm_plan_info", "efmm_plan_tree_export"]
+
+
+class ElfmmError(RuntimeError):
+    def __init__(self, ier, where=""):
+        super().__init__(f"elfmm3d_b200 error ier={ier} {where}")
+        self.ier = ier
+
+
+def library_path():
+    return _LIB_PATH
+
+
+def load():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(_LIB_PATH):
+        raise ElfmmError(-1, f"CUDA library not built: {_LIB_PATH} (run python -m elfmmlib3d_b200.build)")
+    L = ctypes.CDLL(_LIB_PATH)
+    L.efmm_device_count.restype = ctypes.c_int
+    L.efmm_plan_create.restype = _vp
+    L.efmm_plan_create.argtypes = [ctypes.c_int]
+    L.efmm_plan_destroy.argtypes = [_vp]
+    L.efmm_plan_set_geometry.restype = ctypes.c_int
+    L.efmm_plan_set_geometry.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.c_int, _vp,
+                                         ctypes.c_int, ctypes.c_int, ctypes.c_int]
+    for f in (L.efmm_plan_evaluate, L.efmm_plan_evaluate_direct):
+        f.restype = ctypes.c_int
+        f.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.efmm_plan_timings.argtypes = [_vp, _fp]
+    L.efmm_plan_info.argtypes = [_vp, _llp]
+    L.efmm_plan_tree_export.restype = ctypes.c_int
+    L.efmm_plan_tree_export.argtypes = [_vp, _ip, _ip, _ip, _ip, _dp, _ip, _ip, _llp]
+    _lib = L
+    return L
+
+
+def device_count():
+    return load().efmm_device_count()
+
+
+def _need_gpu():
+    if device_count() < 1:
+        raise ElfmmError(1024, "no CUDA device visible")
+
+
+def _c(a, shape):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(shape))
+
+
+def _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl):
+    tri = _c(triangle, (-1, 3, 3))
+    n = tri.shape[0]
+    nrm = _c(trinorm, (n, 3))
+    src = _c(source, (n, 3))
+    ssl = _c(sigma_sl, (n, 3)) if sigma_sl is not None else np.zeros((n, 3))
+    sdl = _c(sigma_dl, (n, 3)) if sigma_dl is not None else np.zeros((n, 3))
+    return tri, nrm, src, ssl, sdl, n
+
+
+def _byref_i(v):
+    return ctypes.byref(ctypes.c_int(int(v)))
+
+
+def _byref_d(v):
+    return ctypes.byref(ctypes.c_double(float(v)))
+
+
+def elfmm3dtriatarg(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                    target=None, ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1):
+    """Displacement/strain of piecewise-constant single (traction ``sigma_sl``)
+    and double (displacement jump ``sigma_dl``) layers on flat triangles, at the
+    n source points and at optional targets (src/elfmm3dtria.f:162).
+
+    Returns (ier, ptfrc (n,3), strain (n,3,3), ptfrctarg (m,3), straintarg (m,3,3)).
+    """
+    L = load()
+    _need_gpu()
+    tri, nrm, src, ssl, sdl, n = _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    pt = np.zeros((n, 3))
+    st = np.zeros((n, 3, 3))
+    ptt = np.zeros((max(m, 1), 3))
+    stt = np.zeros((max(m, 1), 3, 3))
+    ier = ctypes.c_int(0)
+    L.elfmm3dtriatarg_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu),
+                       tri.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp), _byref_i(n),
+                       src.ctypes.data_as(_dp), _byref_i(sigma_sl is not None), ssl.ctypes.data_as(_dp),
+                       _byref_i(sigma_dl is not None), sdl.ctypes.data_as(_dp), _byref_i(ifptfrc),
+                       pt.ctypes.data_as(_dp), _byref_i(ifstrain), st.ctypes.data_as(_dp), _byref_i(m),
+                       tg.ctypes.data_as(_dp), _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp),
+                       _byref_i(ifstraintarg), stt.ctypes.data_as(_dp))
+    return ier.value, pt, st, ptt[:m], stt[:m]
+
+
+def elfmm3dtria(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                ifptfrc=1, ifstrain=1):
+    """On-surface evaluation only (src/elfmm3dtria.f:71). Returns (ier, ptfrc, strain)."""
+    ier, pt, st, _, _ = elfmm3dtriatarg(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl,
+                                        sigma_dl, None, ifptfrc, ifstrain, 0, 0)
+    return ier, pt, st
+
+
+def el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                       target=None, ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1):
+    """O(N^2) direct evaluation on the GPU (src/elfmm3dtria.f:1483).
+    Returns (ptfrc, strain, ptfrctarg, straintarg)."""
+    L = load()
+    _need_gpu()
+    tri, nrm, src, ssl, sdl, n = _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    pt = np.zeros((n, 3))
+    st = np.zeros((n, 3, 3))
+    ptt = np.zeros((max(m, 1), 3))
+    stt = np.zeros((max(m, 1), 3, 3))
+    L.el3dtriadirecttarg_(_byref_d(rlam), _byref_d(rmu), tri.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp),
+                          _byref_i(n), src.ctypes.data_as(_dp), _byref_i(sigma_sl is not None),
+                          ssl.ctypes.data_as(_dp), _byref_i(sigma_dl is not None), sdl.ctypes.data_as(_dp),
+                          _byref_i(ifptfrc), pt.ctypes.data_as(_dp), _byref_i(ifstrain),
+                          st.ctypes.data_as(_dp), _byref_i(m), tg.ctypes.data_as(_dp),
+                          _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp), _byref_i(ifstraintarg),
+                          stt.ctypes.data_as(_dp))
+    return pt, st, ptt[:m], stt[:m]
+
+
+class Plan:
+    """Device-resident plan (native API).  Arguments are CUDA tensors (torch)
+    or raw device addresses (int); float64, contiguous, user order."""
+
+    def __init__(self, device=0):
+        L = load()
+        _need_gpu()
+        self._L = L
+        self._h = L.efmm_plan_create(int(device))
+        if not self._h:
+            raise ElfmmError(1024, f"cannot create plan on device {device}")
+
+    @staticmethod
+    def _ptr(t):
+        if t is None:
+            return None
+        if isinstance(t, int):
+            return t
+        return t.data_ptr()
+
+    def set_geometry(self, tri, nrm, src, tgt=None, iprec=2, iter=False, mindlin=False):
+        n = int(src.shape[0]) if hasattr(src, "shape") else None
+        nt = int(tgt.shape[0]) if tgt is not None else 0
+        ier = self._L.efmm_plan_set_geometry(self._h, n, self._ptr(tri), self._ptr(nrm), self._ptr(src), nt,
+                                             self._ptr(tgt), int(iprec), int(iter), int(mindlin))
+        if ier:
+            raise ElfmmError(ier, "set_geometry")
+        self.n, self.nt = n, nt
+
+    def evaluate(self, rlam, rmu, ssl=None, sdl=None, u=None, e=None, ut=None, et=None, direct=False):
+        f = self._L.efmm_plan_evaluate_direct if direct else self._L.efmm_plan_evaluate
+        ier = f(self._h, float(rlam), float(rmu), self._ptr(ssl), self._ptr(sdl), self._ptr(u),
+                self._ptr(e), self._ptr(ut), self._ptr(et))
+        if ier:
+            raise ElfmmError(ier, "evaluate")
+
+    def timings(self):
+        a = (ctypes.c_float * 8)()
+        self._L.efmm_plan_timings(self._h, a)
+        return dict(zip(["total", "prep", "p2m", "m2m", "m2l", "l2l", "l2t", "near"], list(a)))
+
+    def info(self):
+        a = (ctypes.c_longlong * 8)()
+        self._L.efmm_plan_info(self._h, a)
+        return dict(zip(["nboxes", "nlev", "p", "nbox", "near_pairs", "m2l_pairs", "launches", "far"],
+                        list(a)))
+
+    def tree(self):
+        """Tree in the reference's layout (1-based ids): dict with boxes (nb,20),
+        iz, iztarg, laddr (nlev+1,2), center, size, lists {1..5: [array per box]}."""
+        info = self.info()
+        nb, nlev = info["nboxes"], info["nlev"]
+        lc = (ctypes.c_longlong * 5)()
+        z = ctypes.POINTER(ctypes.c_int)()
+        self._L.efmm_plan_tree_export(self._h, z, z, z, z, ctypes.POINTER(ctypes.c_double)(), z, z, lc)
+        tot = int(sum(lc))
+        boxes = np.zeros((nb, 20), dtype=np.int32)
+        iz = np.zeros(max(self.n, 1), dtype=np.int32)
+        izt = np.zeros(max(self.nt, 1), dtype=np.int32)
+        laddr = np.zeros((nlev + 1, 2), dtype=np.int32)
+        cs = np.zeros(4)
+        lstart = np.zeros((5, nb + 1), dtype=np.int32)
+        litems = np.zeros(max(tot, 1), dtype=np.int32)
+        ier = self._L.efmm_plan_tree_export(self._h, boxes.ctypes.data_as(_ip), iz.ctypes.data_as(_ip),
+                                            izt.ctypes.data_as(_ip), laddr.ctypes.data_as(_ip),
+                                            cs.ctypes.data_as(_dp), lstart.ctypes.data_as(_ip),
+                                            litems.ctypes.data_as(_ip), lc)
+        if ier:
+            raise ElfmmError(ier, "tree_export")
+        lists = {}
+        off = 0
+        for t in range(5):
+            items = litems[off:off + lc[t]]
+            off += lc[t]
+            st = lstart[t]
+            lists[t + 1] = [items[st[b]:st[b + 1]].copy() for b in range(nb)]
+        return dict(boxes=boxes, iz=iz[:self.n], iztarg=izt[:self.nt], laddr=laddr, center=cs[:3],
+                    size=cs[3], lists=lists)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.efmm_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,457 @@
+// fmm.cu -- Laplace far field for the four canonical-decomposition passes.
+//
+// The elastostatic far field is the reference's canonical decomposition
+// (src/elfmm3dtria.f:437-615, recombination src/el3routs.f:1392/:1452): three
+// Laplace passes with constant densities per Cartesian component j plus one
+// with linear densities.  All four passes share one tree and are carried as
+// four columns of every expansion, so each translation operator is applied to
+// a [D x 4*pairs] panel at once.
+//
+//   P2M  leaf boxes: 12-node degree-6 quadrature of the (linear) charge and
+//        dipole densities on every triangle (src/lfmm3dtrilhess.f:671-748).
+//   M2M / M2L / L2L: dense real operator per relative offset (level
+//        independent in box units), applied by one grouped gather-GEMM-scatter
+//        kernel; M2L order truncated per offset (src/l3dterms.f:144).
+//   L2T  leaf boxes: potential, gradient and Hessian of the local expansion
+//        with the Lame recombination fused in, writing displacement and strain.
+#include "common.cuh"
+#include "fmm.h"
+
+namespace efmm {
+
+// -------------------------------------------------------------- operators
+// Build one real operator matrix per CTA.  kind 0: M2L (offset vector in box
+// units), kind 1: M2M (child centre - parent centre, parent units), kind 2:
+// L2L (child centre - parent centre, parent units).
+__global__ void k_build_ops(int nop, const OpDesc* __restrict__ ops, double* __restrict__ mats) {
+  extern __shared__ cplx tab[];
+  const OpDesc o = ops[blockIdx.x];
+  int p = o.p;
+  if (o.kind == 0) {
+    if (threadIdx.x == 0) irregular_harmonics(2 * p, o.d[0], o.d[1], o.d[2], tab);
+  } else {
+    if (threadIdx.x == 0) regular_harmonics(p, o.d[0], o.d[1], o.d[2], tab);
+  }
+  __syncthreads();
+  int nc = ncoef(p), dim = 2 * nc;
+  double* M = mats + o.off;
+  long long tot = (long long)nc * nc;
+  for (long long q = threadIdx.x; q < tot; q += blockDim.x) {
+    int r = (int)(q / nc), c = (int)(q % nc);
+    // (n,m) of row r, (k,l) of column c
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= r) n++;
+    int m = r - n * (n + 1) / 2;
+    int k = 0;
+    while ((k + 1) * (k + 2) / 2 <= c) k++;
+    int l = c - k * (k + 1) / 2;
+    cplx A, B;
+    if (o.kind == 0) {
+      A = m2l_coef(tab, n, m, k, l);
+      B = m2l_coef(tab, n, m, k, -l);
+    } else if (o.kind == 1) {  // M2M: rows (n,m) parent, cols (k,l) child
+      double sc = ldexp(1.0, -k);
+      A = shift_coef(tab, n, m, k, l, sc);
+      B = shift_coef(tab, n, m, k, -l, sc);
+    } else {  // L2L: rows (n,m) child, cols (k,l) parent: 2^-n conj(Y_{k-n}^{l-m})
+      double sc = ldexp(1.0, -n);
+      A = shift_coef(tab, k, l, n, m, sc);
+      B = shift_coef(tab, k, -l, n, m, sc);
+    }
+    double rr, ri, ir, ii;
+    real_block(A, B, l, &rr, &ri, &ir, &ii);
+    size_t r2 = 2 * (size_t)r, c2 = 2 * (size_t)c;
+    M[r2 * dim + c2] = rr;
+    M[r2 * dim + c2 + 1] = ri;
+    M[(r2 + 1) * dim + c2] = ir;
+    M[(r2 + 1) * dim + c2 + 1] = ii;
+  }
+}
+
+// -------------------------------------------------------------------- P2M
+constexpr int P2M_THREADS = 256;
+constexpr int P2M_NODES = 8;  // quadrature nodes per batch (one per warp)
+
+__global__ void __launch_bounds__(P2M_THREADS)
+k_p2m(const P2MArgs a) {
+  extern __shared__ double sm[];
+  int box = a.leaves[blockIdx.x];
+  int p = a.p, nc = ncoef(p), D = 2 * nc;
+  cplx* Ys = reinterpret_cast<cplx*>(sm);                       // [P2M_NODES][nc]
+  double* qd = sm + 2 * (size_t)P2M_NODES * nc;                 // [P2M_NODES][16]
+  int lev = a.level[box];
+  double s = a.size / (double)(1ull << lev);
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  int t0 = a.sstart[box], tn = a.scount[box];
+  int nnode = 12 * tn;
+  const int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
+  double acc[CMAX][4][2];
+#pragma unroll
+  for (int i = 0; i < CMAX; i++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[i][q][0] = acc[i][q][1] = 0.0;
+  Quad12 Q;
+  quad12(Q);
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double c1 = a.c1, inv2mu = a.inv2mu, c2 = a.c2;
+  for (int b0 = 0; b0 < nnode; b0 += P2M_NODES) {
+    __syncthreads();
+    int node = b0 + warp;
+    if (node < nnode) {
+      int it = t0 + node / 12, iq = node % 12;
+      const double* T = a.tri + 9 * (size_t)it;
+      double y[3];
+      for (int d = 0; d < 3; d++)
+        y[d] = Q.b[iq][0] * T[d] + Q.b[iq][1] * T[3 + d] + Q.b[iq][2] * T[6 + d];
+      double e1[3] = {T[3] - T[0], T[4] - T[1], T[5] - T[2]};
+      double e2[3] = {T[6] - T[0], T[7] - T[1], T[8] - T[2]};
+      double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                      e1[0] * e2[1] - e1[1] * e2[0]};
+      double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      double w = Q.w[iq] * area;
+      double z[3] = {(y[0] - c[0]) / s, (y[1] - c[1]) / s, (y[2] - c[2]) / s};
+      // column chains of the regular harmonics, one order m per lane
+      cplx* Y = Ys + (size_t)warp * nc;
+      for (int m = lane; m <= p; m += 32) {
+        cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+        for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+        double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+        Y[cidx(m, m)] = dm;
+        cplx ym2 = {0, 0}, ym1 = dm;
+        for (int n = m + 1; n <= p; n++) {
+          double aa = (2.0 * n - 1.0) * z[2];
+          double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+          cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+          Y[cidx(n, m)] = yn;
+          ym2 = ym1;
+          ym1 = yn;
+        }
+      }
+      if (lane == 0) {
+        const double* ss = a.ssl + 3 * (size_t)it;
+        const double* sd = a.sdl + 3 * (size_t)it;
+        const double* nn = a.nrm + 3 * (size_t)it;
+        double* o = qd + 16 * warp;
+        double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+        if (a.dosl) { sl[0] = ss[0]; sl[1] = ss[1]; sl[2] = ss[2]; }
+        if (a.dodl) { dl[0] = sd[0]; dl[1] = sd[1]; dl[2] = sd[2]; }
+        // passes 0..2: charge s_j/(2mu), dipole (n s_j + s n_j)/2
+        for (int j = 0; j < 3; j++) {
+          o[j] = w * sl[j] * inv2mu;
+          for (int d = 0; d < 3; d++) o[4 + 3 * j + d] = w * 0.5 * (nn[d] * dl[j] + dl[d] * nn[j]);
+        }
+        // pass 3: charge (s_sl.y) c1/(2mu) + (s_dl.n) c2, dipole c1 [n (s_dl.y) + s_dl (n.y)]/2
+        double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
+        double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+        double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
+        double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+        o[3] = w * (sly * c1 * inv2mu + dln * c2);
+        for (int d = 0; d < 3; d++) o[13 + d] = w * 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
+      }
+    }
+    __syncthreads();
+    int nb = min(P2M_NODES, nnode - b0);
+    double is = 1.0 / s;
+#pragma unroll
+    for (int i = 0; i < CMAX; i++) {
+      int cc = threadIdx.x + i * P2M_THREADS;
+      if (cc >= nc) break;
+      int n = 0;
+      while ((n + 1) * (n + 2) / 2 <= cc) n++;
+      int m = cc - n * (n + 1) / 2;
+      for (int k = 0; k < nb; k++) {
+        const cplx* Y = Ys + (size_t)k * nc;
+        const double* o = qd + 16 * k;
+        cplx y = Y[cc];
+        cplx ya = {0, 0}, yb = {0, 0}, yc = {0, 0};
+        if (n > 0) {
+          ya = hget(Y, n - 1, m);
+          yb = hget(Y, n - 1, m + 1);
+          yc = hget(Y, n - 1, m - 1);
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+          const double* dv = (q < 3) ? o + 4 + 3 * q : o + 13;
+          // conj(d.grad Y) = conj(dz ya + (dx - i dy)/2 yb - (dx + i dy)/2 yc)
+          double gre = dv[2] * ya.re + 0.5 * (dv[0] * yb.re + dv[1] * yb.im) -
+                       0.5 * (dv[0] * yc.re - dv[1] * yc.im);
+          double gim = dv[2] * ya.im + 0.5 * (dv[0] * yb.im - dv[1] * yb.re) -
+                       0.5 * (dv[0] * yc.im + dv[1] * yc.re);
+          double qq = o[q];
+          acc[i][q][0] += qq * y.re + is * gre;
+          acc[i][q][1] -= qq * y.im + is * gim;
+        }
+      }
+    }
+  }
+  double* M = a.mpole + (size_t)box * 4 * D;
+#pragma unroll
+  for (int i = 0; i < CMAX; i++) {
+    int cc = threadIdx.x + i * P2M_THREADS;
+    if (cc >= nc) break;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      M[(size_t)q * D + 2 * cc] = acc[i][q][0];
+      M[(size_t)q * D + 2 * cc + 1] = acc[i][q][1];
+    }
+  }
+}
+
+// --------------------------------------------------- grouped translations
+// For every task: dst[:, 4 passes] += alpha * Op(group) * src[:, 4 passes]
+// over one 64-row tile and up to 16 (src, dst) pairs (= 64 columns).
+constexpr int TR_TILE_R = 64, TR_TILE_C = 64, TR_TILE_K = 16;
+
+__global__ void __launch_bounds__(256)
+k_translate(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
+            const double* __restrict__ mats, const long long* __restrict__ mat_off,
+            const int* __restrict__ mat_dim, int D, const double* __restrict__ src,
+            double* __restrict__ dst) {
+  __shared__ double As[TR_TILE_K][TR_TILE_R + 1];
+  __shared__ double Bs[TR_TILE_K][TR_TILE_C + 1];
+  const TransTask t = tasks[blockIdx.x];
+  const double* A = mats + mat_off[t.group];
+  int dim = mat_dim[t.group];
+  int r0 = t.row0;
+  int np = t.npair;
+  int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  double acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; i++)
+#pragma unroll
+    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+  for (int k0 = 0; k0 < dim; k0 += TR_TILE_K) {
+    // A tile: rows r0..r0+63, cols k0..k0+15
+    for (int q = threadIdx.x; q < TR_TILE_R * TR_TILE_K; q += 256) {
+      int rr = q / TR_TILE_K, kk = q % TR_TILE_K;
+      int r = r0 + rr, k = k0 + kk;
+      As[kk][rr] = (r < dim && k < dim) ? A[(size_t)r * dim + k] : 0.0;
+    }
+    // B tile: column j = (pair j/4, pass j%4)
+    for (int q = threadIdx.x; q < TR_TILE_C * TR_TILE_K; q += 256) {
+      int jj = q / TR_TILE_K, kk = q % TR_TILE_K;
+      int pj = jj >> 2, ps = jj & 3;
+      int k = k0 + kk;
+      double v = 0.0;
+      if (pj < np && k < dim) {
+        const TransPair& pr = pairs[t.pair0 + pj];
+        v = src[((size_t)pr.src * 4 + ps) * D + k];
+      }
+      Bs[kk][jj] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int kk = 0; kk < TR_TILE_K; kk++) {
+      double a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 4; j++) {
+    int jj = tx * 4 + j;
+    int pj = jj >> 2, ps = jj & 3;
+    if (pj >= np) continue;
+    const TransPair& pr = pairs[t.pair0 + pj];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      int r = r0 + ty * 4 + i;
+      if (r < dim) atomicAdd(&dst[((size_t)pr.dst * 4 + ps) * D + r], pr.alpha * acc[i][j]);
+    }
+  }
+}
+
+// ------------------------------------------------- L2T + recombination
+constexpr int L2T_WARPS = 8;
+
+__global__ void __launch_bounds__(L2T_WARPS * 32)
+k_l2t(const L2TArgs a) {
+  // blockDim.x = 32 * (number of warps); each warp owns one Y table in smem
+  extern __shared__ double sm[];
+  int box = a.leaves[blockIdx.x];
+  int p = a.p, nc = ncoef(p), D = 2 * nc;
+  double* Ls = sm;                                              // [4][D]
+  cplx* Yall = reinterpret_cast<cplx*>(sm + 4 * (size_t)D);     // [warps][nc]
+  const double* L = a.local + (size_t)box * 4 * D;
+  for (int q = threadIdx.x; q < 4 * D; q += blockDim.x) Ls[q] = L[q];
+  int lev = a.level[box];
+  double s = a.size / (double)(1ull << lev);
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  __syncthreads();
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  cplx* Y = Yall + (size_t)warp * nc;
+  int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
+  int s0 = a.sstart[box], t0 = a.tstart[box];
+  double is = 1.0 / s, is2 = is * is;
+  int nw = blockDim.x >> 5;
+  for (int e = warp; e < sn + tn; e += nw) {
+    bool is_src = e < sn;
+    int pidx = is_src ? s0 + e : t0 + (e - sn);
+    const double* X = is_src ? a.src_pts + 3 * (size_t)pidx : a.tgt_pts + 3 * (size_t)pidx;
+    double x[3] = {X[0], X[1], X[2]};
+    double z[3] = {(x[0] - c[0]) * is, (x[1] - c[1]) * is, (x[2] - c[2]) * is};
+    __syncwarp();
+    double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+    for (int m = lane; m <= p; m += 32) {
+      cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+      for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+      Y[cidx(m, m)] = dm;
+      cplx ym2 = {0, 0}, ym1 = dm;
+      for (int n = m + 1; n <= p; n++) {
+        double aa = (2.0 * n - 1.0) * z[2];
+        double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+        cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        Y[cidx(n, m)] = yn;
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+    __syncwarp();
+    // per pass: phi, dz, dzz (real); dp, dpz, dpp (complex) -> 9 doubles x 4
+    double S[4][9];
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int v = 0; v < 9; v++) S[q][v] = 0.0;
+    // iterate over (n, m) with m in [-n, n]: total (p+1)^2 terms
+    int tot = (p + 1) * (p + 1);
+    for (int idx = lane; idx < tot; idx += 32) {
+      int n = (int)sqrt((double)idx);
+      while (n * n > idx) n--;
+      while ((n + 1) * (n + 1) <= idx) n++;
+      int m = idx - n * n - n;
+      cplx yc = cconj(hget(Y, n, m));
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const double* Lq = Ls + (size_t)q * D;
+        auto Lg = [&](int nn, int mm) -> cplx {
+          if (nn > p || mm > nn || -mm > nn) return cplx{0.0, 0.0};
+          if (mm >= 0) return cplx{Lq[2 * cidx(nn, mm)], Lq[2 * cidx(nn, mm) + 1]};
+          double re = Lq[2 * cidx(nn, -mm)], im = Lq[2 * cidx(nn, -mm) + 1];
+          return ((-mm) & 1) ? cplx{-re, im} : cplx{re, -im};
+        };
+        cplx c0 = Lg(n, m);
+        S[q][0] += c0.re * yc.re - c0.im * yc.im;
+        if (n + 1 <= p) {
+          cplx c1 = Lg(n + 1, m);
+          S[q][1] += c1.re * yc.re - c1.im * yc.im;
+          cplx c2 = Lg(n + 1, m + 1);  // D+ : -L_{n+1}^{m+1}
+          S[q][3] -= c2.re * yc.re - c2.im * yc.im;
+          S[q][4] -= c2.re * yc.im + c2.im * yc.re;
+        }
+        if (n + 2 <= p) {
+          cplx c3 = Lg(n + 2, m);
+          S[q][2] += c3.re * yc.re - c3.im * yc.im;
+          cplx c4 = Lg(n + 2, m + 1);  // D+Dz : -L_{n+2}^{m+1}
+          S[q][5] -= c4.re * yc.re - c4.im * yc.im;
+          S[q][6] -= c4.re * yc.im + c4.im * yc.re;
+          cplx c5 = Lg(n + 2, m + 2);  // D+D+ : L_{n+2}^{m+2}
+          S[q][7] += c5.re * yc.re - c5.im * yc.im;
+          S[q][8] += c5.re * yc.im + c5.im * yc.re;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++)
+#pragma unroll
+      for (int v = 0; v < 9; v++) S[q][v] = warp_sum(S[q][v]);
+    if (lane == 0) {
+      double pot[4], g[4][3], H[4][3][3];
+      for (int q = 0; q < 4; q++) {
+        pot[q] = S[q][0];
+        g[q][0] = S[q][3] * is;
+        g[q][1] = S[q][4] * is;
+        g[q][2] = S[q][1] * is;
+        double hzz = S[q][2];
+        double hxx = 0.5 * (S[q][7] - hzz), hyy = 0.5 * (-S[q][7] - hzz), hxy = 0.5 * S[q][8];
+        double hxz = S[q][5], hyz = S[q][6];
+        H[q][0][0] = hxx * is2; H[q][1][1] = hyy * is2; H[q][2][2] = hzz * is2;
+        H[q][0][1] = H[q][1][0] = hxy * is2;
+        H[q][0][2] = H[q][2][0] = hxz * is2;
+        H[q][1][2] = H[q][2][1] = hyz * is2;
+      }
+      double c1 = a.c1;
+      // u_a = (2-c1) phi_a - c1 x_j d_a phi_j + d_a Phi4
+      double u[3];
+      for (int i = 0; i < 3; i++) {
+        u[i] = (2.0 - c1) * pot[i] + g[3][i];
+        for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+      }
+      double* U = is_src ? a.u_src : a.u_tgt;
+      double* E = is_src ? a.e_src : a.e_tgt;
+      U[3 * (size_t)pidx] += u[0];
+      U[3 * (size_t)pidx + 1] += u[1];
+      U[3 * (size_t)pidx + 2] += u[2];
+      bool dostrain = is_src ? a.dostrain_src : a.dostrain_tgt;
+      if (dostrain) {
+        // G_ab = d_b u_a = (2-c1) d_b phi_a - c1 d_a phi_b - c1 x_j d_ab phi_j + d_ab Phi4
+        double G[3][3];
+        for (int aa = 0; aa < 3; aa++)
+          for (int bb = 0; bb < 3; bb++) {
+            double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
+            for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+            G[aa][bb] = v;
+          }
+        double* ee = E + 6 * (size_t)pidx;
+        ee[0] += G[0][0];
+        ee[1] += G[1][1];
+        ee[2] += G[2][2];
+        ee[3] += 0.5 * (G[0][1] + G[1][0]);
+        ee[4] += 0.5 * (G[0][2] + G[2][0]);
+        ee[5] += 0.5 * (G[1][2] + G[2][1]);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp) {
+  if (nop <= 0) return;
+  size_t smem = sizeof(cplx) * (size_t)ncoef(2 * maxp);
+  if (smem > 48 * 1024)
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_build_ops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_build_ops<<<nop, 256, smem, st>>>(nop, ops, mats);
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a) {
+  if (nleaf <= 0) return;
+  size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 16 * P2M_NODES);
+  if (smem > 48 * 1024)
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_p2m<<<nleaf, P2M_THREADS, smem, st>>>(a);
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
+                      const double* mats, const long long* mat_off, const int* mat_dim, int D,
+                      const double* src, double* dst) {
+  if (ntask <= 0) return;
+  k_translate<<<ntask, 256, 0, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, src, dst);
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a) {
+  if (nleaf <= 0) return;
+  int nw = L2T_WARPS;
+  auto need = [&](int w) {
+    return sizeof(double) * 4 * 2 * (size_t)ncoef(a.p) + sizeof(cplx) * w * (size_t)ncoef(a.p);
+  };
+  while (nw > 1 && need(nw) > 220 * 1024) nw /= 2;
+  size_t smem = need(nw);
+  if (smem > 48 * 1024)
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_l2t<<<nleaf, nw * 32, smem, st>>>(a);
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace efmm

@@ -1,0 +1,211 @@
+// nearfield.cu -- analytic near-field kernels (FP64).
+//
+// The near field of the reference (src/elfmm3dtria.f:968 _evalloc and the
+// ITER variant src/elfmm3dtria_iter_1.f:1240-1419) sums, for each evaluation
+// point, the exact single/double layer potential of every triangle in the
+// source boxes paired with the point's leaf box.  Here one CTA owns one leaf
+// box: the paired triangles stream through shared memory in tiles, each warp
+// takes one evaluation point against a tile (lanes split the triangles), and
+// the per-point partial sums are reduced with warp shuffles into shared-memory
+// accumulators that are written once at the end.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace efmm {
+
+// Build the per-triangle frame records in tree order and rotate the densities
+// into each triangle frame.
+__global__ void k_tri_prep(int n, const double* __restrict__ tri, const int* __restrict__ perm,
+                           const double* __restrict__ ssl, const double* __restrict__ sdl,
+                           int dosl, int dodl, TriRec* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int j = perm ? perm[i] : i;
+  double t[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) t[c] = tri[9 * (size_t)j + c];
+  TriRec r;
+  tri_frame(t, r.f);
+  double a[3] = {0, 0, 0}, b[3] = {0, 0, 0};
+  if (dosl) { a[0] = ssl[3 * (size_t)j]; a[1] = ssl[3 * (size_t)j + 1]; a[2] = ssl[3 * (size_t)j + 2]; }
+  if (dodl) { b[0] = sdl[3 * (size_t)j]; b[1] = sdl[3 * (size_t)j + 1]; b[2] = sdl[3 * (size_t)j + 2]; }
+  const double* ax[3] = {r.f.e1, r.f.e2, r.f.e3};
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    r.ssl[c] = ax[c][0] * a[0] + ax[c][1] * a[1] + ax[c][2] * a[2];
+    r.sdl[c] = ax[c][0] * b[0] + ax[c][1] * b[1] + ax[c][2] * b[2];
+  }
+  r.pad[0] = r.pad[1] = 0.0;
+  out[i] = r;
+}
+
+constexpr int NF_TILE = 64;    // triangles staged per tile
+constexpr int NF_WARPS = 4;    // warps per CTA
+constexpr int NF_MAXEP = 512;  // max evaluation points per leaf held in shared memory
+
+__device__ __forceinline__ void stage_tile(TriRec* sm, const TriRec* __restrict__ g, int cnt) {
+  const double2* src = reinterpret_cast<const double2*>(g);
+  double2* dst = reinterpret_cast<double2*>(sm);
+  int nv = cnt * (int)(sizeof(TriRec) / sizeof(double2));
+  for (int q = threadIdx.x; q < nv; q += blockDim.x) dst[q] = src[q];
+}
+
+// One CTA per leaf box.  Evaluation points of the leaf: its sources (sorted
+// centroids, self-aware) then its targets.  nb_start/nb_items: CSR of the
+// source boxes paired with the leaf; box_src_start/count give their triangle
+// ranges.  Outputs are ADDED to u (3/pt) and e (6/pt, xx yy zz xy xz yz).
+__global__ void __launch_bounds__(NF_WARPS * 32)
+k_near_leaf(int nleaf, const int* __restrict__ leaves, const int* __restrict__ nb_start,
+            const int* __restrict__ nb_items, const int* __restrict__ box_src_start,
+            const int* __restrict__ box_src_count, const int* __restrict__ box_tgt_start,
+            const int* __restrict__ box_tgt_count, const TriRec* __restrict__ trir,
+            const double* __restrict__ src_pts, const double* __restrict__ tgt_pts, int dosl,
+            int dodl, int dostrain_src, int dostrain_tgt, int do_src, int do_tgt, double rlam,
+            double rmu, double* __restrict__ u_src, double* __restrict__ e_src,
+            double* __restrict__ u_tgt, double* __restrict__ e_tgt) {
+  __shared__ TriRec tile[NF_TILE];
+  __shared__ double acc[NF_MAXEP][9];
+  int leaf = leaves[blockIdx.x];
+  int s0 = box_src_start[leaf], sn = do_src ? box_src_count[leaf] : 0;
+  int t0 = box_tgt_start[leaf], tn = do_tgt ? box_tgt_count[leaf] : 0;
+  int nep = sn + tn;
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  // process evaluation points in chunks of NF_MAXEP
+  for (int ep0 = 0; ep0 < nep; ep0 += NF_MAXEP) {
+    int nepc = min(NF_MAXEP, nep - ep0);
+    for (int q = threadIdx.x; q < nepc * 9; q += blockDim.x) (&acc[0][0])[q] = 0.0;
+    __syncthreads();
+    for (int b = nb_start[blockIdx.x]; b < nb_start[blockIdx.x + 1]; b++) {
+      int sb = nb_items[b];
+      int tr0 = box_src_start[sb], trn = box_src_count[sb];
+      for (int k0 = 0; k0 < trn; k0 += NF_TILE) {
+        int cnt = min(NF_TILE, trn - k0);
+        __syncthreads();
+        stage_tile(tile, trir + tr0 + k0, cnt);
+        __syncthreads();
+        for (int e = warp; e < nepc; e += NF_WARPS) {
+          int ep = ep0 + e;
+          bool is_src = ep < sn;
+          int pidx = is_src ? s0 + ep : t0 + (ep - sn);
+          const double* P = is_src ? src_pts + 3 * (size_t)pidx : tgt_pts + 3 * (size_t)pidx;
+          double X[3] = {P[0], P[1], P[2]};
+          bool dostrain = is_src ? dostrain_src : dostrain_tgt;
+          double u[3] = {0, 0, 0}, ee[6] = {0, 0, 0, 0, 0, 0};
+          for (int k = lane; k < cnt; k += 32) {
+            int tidx = tr0 + k0 + k;
+            bool self = is_src && (tidx == pidx);
+            const TriRec& r = tile[k];
+            pair_eval(r.f, r.ssl, r.sdl, dosl, dodl, dostrain, X, self, rlam, rmu, u, ee);
+          }
+#pragma unroll
+          for (int c = 0; c < 3; c++) u[c] = warp_sum(u[c]);
+          if (dostrain) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) ee[c] = warp_sum(ee[c]);
+          }
+          if (lane == 0) {
+            acc[e][0] += u[0]; acc[e][1] += u[1]; acc[e][2] += u[2];
+            if (dostrain)
+              for (int c = 0; c < 6; c++) acc[e][3 + c] += ee[c];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < nepc; e += blockDim.x) {
+      int ep = ep0 + e;
+      bool is_src = ep < sn;
+      int pidx = is_src ? s0 + ep : t0 + (ep - sn);
+      double* U = is_src ? u_src : u_tgt;
+      double* E = is_src ? e_src : e_tgt;
+      U[3 * (size_t)pidx] += acc[e][0];
+      U[3 * (size_t)pidx + 1] += acc[e][1];
+      U[3 * (size_t)pidx + 2] += acc[e][2];
+      bool dostrain = is_src ? dostrain_src : dostrain_tgt;
+      if (dostrain)
+        for (int c = 0; c < 6; c++) E[6 * (size_t)pidx + c] += acc[e][3 + c];
+    }
+    __syncthreads();
+  }
+}
+
+// All-pairs direct sum (el3dtriadirecttarg, src/elfmm3dtria.f:1483): one warp
+// per evaluation point, all triangles streamed through shared memory.
+// Points [0, nsrc) are the centroids (self pair when the indices match),
+// [nsrc, nsrc+ntgt) the targets.  Outputs are overwritten.
+__global__ void __launch_bounds__(NF_WARPS * 32)
+k_direct_all(int ntri, const TriRec* __restrict__ trir, int nsrc, const double* __restrict__ src_pts,
+             int ntgt, const double* __restrict__ tgt_pts, int dosl, int dodl, int dostrain_src,
+             int dostrain_tgt, double rlam, double rmu, double* __restrict__ u_src,
+             double* __restrict__ e_src, double* __restrict__ u_tgt, double* __restrict__ e_tgt) {
+  __shared__ TriRec tile[NF_TILE];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int ep = blockIdx.x * NF_WARPS + warp;
+  int nep = nsrc + ntgt;
+  bool active = ep < nep;
+  bool is_src = ep < nsrc;
+  int pidx = is_src ? ep : ep - nsrc;
+  double X[3] = {0, 0, 0};
+  if (active) {
+    const double* P = is_src ? src_pts + 3 * (size_t)pidx : tgt_pts + 3 * (size_t)pidx;
+    X[0] = P[0]; X[1] = P[1]; X[2] = P[2];
+  }
+  bool dostrain = is_src ? dostrain_src : dostrain_tgt;
+  double u[3] = {0, 0, 0}, ee[6] = {0, 0, 0, 0, 0, 0};
+  for (int k0 = 0; k0 < ntri; k0 += NF_TILE) {
+    int cnt = min(NF_TILE, ntri - k0);
+    __syncthreads();
+    stage_tile(tile, trir + k0, cnt);
+    __syncthreads();
+    if (active) {
+      for (int k = lane; k < cnt; k += 32) {
+        bool self = is_src && (k0 + k == pidx);
+        const TriRec& r = tile[k];
+        pair_eval(r.f, r.ssl, r.sdl, dosl, dodl, dostrain, X, self, rlam, rmu, u, ee);
+      }
+    }
+  }
+  if (!active) return;
+#pragma unroll
+  for (int c = 0; c < 3; c++) u[c] = warp_sum(u[c]);
+#pragma unroll
+  for (int c = 0; c < 6; c++) ee[c] = warp_sum(ee[c]);
+  if (lane == 0) {
+    double* U = is_src ? u_src : u_tgt;
+    double* E = is_src ? e_src : e_tgt;
+    U[3 * (size_t)pidx] = u[0];
+    U[3 * (size_t)pidx + 1] = u[1];
+    U[3 * (size_t)pidx + 2] = u[2];
+    if (dostrain)
+      for (int c = 0; c < 6; c++) E[6 * (size_t)pidx + c] = ee[c];
+  }
+}
+
+// ---------------------------------------------------------------- launchers
+void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
+                     const double* sdl, int dosl, int dodl, TriRec* out) {
+  if (n <= 0) return;
+  k_tri_prep<<<(n + 127) / 128, 128, 0, st>>>(n, tri, perm, ssl, sdl, dosl, dodl, out);
+}
+
+void launch_near_leaf(cudaStream_t st, const NearArgs& a) {
+  if (a.nleaf <= 0) return;
+  k_near_leaf<<<a.nleaf, NF_WARPS * 32, 0, st>>>(
+      a.nleaf, a.leaves, a.nb_start, a.nb_items, a.box_src_start, a.box_src_count,
+      a.box_tgt_start, a.box_tgt_count, a.trir, a.src_pts, a.tgt_pts, a.dosl, a.dodl,
+      a.dostrain_src, a.dostrain_tgt, a.do_src, a.do_tgt, a.rlam, a.rmu, a.u_src, a.e_src,
+      a.u_tgt, a.e_tgt);
+}
+
+void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
+                       int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
+                       int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,
+                       double* u_tgt, double* e_tgt) {
+  int nep = nsrc + ntgt;
+  if (nep <= 0) return;
+  k_direct_all<<<(nep + NF_WARPS - 1) / NF_WARPS, NF_WARPS * 32, 0, st>>>(
+      ntri, trir, nsrc, src_pts, ntgt, tgt_pts, dosl, dodl, dostrain_src, dostrain_tgt, rlam, rmu,
+      u_src, e_src, u_tgt, e_tgt);
+}
+
+}  // namespace efmm

@@ -1,0 +1,514 @@
+// plan.cu -- host orchestration: geometry -> tree -> work lists -> kernels.
+#include <algorithm>
+#include <map>
+#include <mutex>
+#include <vector>
+#include <cstring>
+#include "plan.h"
+
+namespace efmm {
+
+double iprec_eps(int iprec) {
+  switch (iprec) {
+    case -2: return 0.5;
+    case -1: return 0.5e-1;
+    case 0: return 0.5e-2;
+    case 1: return 0.5e-3;
+    case 2: return 0.5e-6;
+    case 3: return 0.5e-9;
+    case 4: return 0.5e-12;
+    case 5: return 0.5e-15;
+    default: return 0.0;
+  }
+}
+
+int iprec_nbox(int iprec, int nsrc, int ntarg, bool iter) {
+  int base;
+  switch (iprec) {
+    case -2: base = 8; break;
+    case -1: base = 15; break;
+    case 0: base = 30; break;
+    case 1: base = 60; break;
+    case 2: base = 120; break;
+    case 3: base = 240; break;
+    case 4: base = 480; break;
+    case 5: base = 700; break;
+    default: return nsrc + ntarg;
+  }
+  return iter ? 2 * base : base / 3;
+}
+
+// ------------------------------------------------------------ small kernels
+__global__ void k_gather(int n, int w, const int* __restrict__ perm, const double* __restrict__ in,
+                         double* __restrict__ out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int j = perm[i];
+  for (int c = 0; c < w; c++) out[(size_t)w * i + c] = in[(size_t)w * j + c];
+}
+// tree order -> user order; strain 6 (xx yy zz xy xz yz) -> 3x3
+__global__ void k_scatter_out(int n, const int* __restrict__ perm, const double* __restrict__ u,
+                              const double* __restrict__ e, double* __restrict__ uo,
+                              double* __restrict__ eo) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int j = perm[i];
+  if (uo)
+    for (int c = 0; c < 3; c++) uo[3 * (size_t)j + c] = u[3 * (size_t)i + c];
+  if (eo) {
+    const double* s = e + 6 * (size_t)i;
+    double* o = eo + 9 * (size_t)j;
+    o[0] = s[0]; o[4] = s[1]; o[8] = s[2];
+    o[1] = o[3] = s[3];
+    o[2] = o[6] = s[4];
+    o[5] = o[7] = s[5];
+  }
+}
+__global__ void k_sym6to9(int n, const double* __restrict__ e, double* __restrict__ eo) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* s = e + 6 * (size_t)i;
+  double* o = eo + 9 * (size_t)i;
+  o[0] = s[0]; o[4] = s[1]; o[8] = s[2];
+  o[1] = o[3] = s[3];
+  o[2] = o[6] = s[4];
+  o[5] = o[7] = s[5];
+}
+
+// --------------------------------------------------------------- op pools
+static std::mutex g_ops_mu;
+static std::map<std::pair<int, std::pair<int, long long>>, OpPool*> g_ops;  // (device, (p, eps bits))
+
+void Plan::ensure_ops() {
+  long long ebits;
+  std::memcpy(&ebits, &eps_, 8);
+  auto key = std::make_pair(dev_, std::make_pair(p_, ebits));
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  auto it = g_ops.find(key);
+  if (it != g_ops.end()) {
+    ops_ = it->second;
+    return;
+  }
+  OpPool* P = new OpPool();
+  P->p = p_;
+  P->eps = eps_;
+  std::vector<OpDesc> descs;
+  long long off = 0;
+  for (int q = 0; q < 343; q++) P->m2l_group[q] = -1;
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = -3; k <= 3; k++) {
+        int mx = std::max(abs(i), std::max(abs(j), abs(k)));
+        if (mx < 2) continue;
+        int po = std::min(p_, m2l_order(eps_, i, j, k));
+        OpDesc d;
+        d.kind = 0;
+        d.p = po;
+        d.d[0] = i; d.d[1] = j; d.d[2] = k;
+        d.off = off;
+        int dim = 2 * ncoef(po);
+        off += (long long)dim * dim;
+        P->m2l_group[(i + 3) * 49 + (j + 3) * 7 + (k + 3)] = (int)descs.size();
+        P->dims.push_back(dim);
+        descs.push_back(d);
+      }
+  for (int kind = 1; kind <= 2; kind++)
+    for (int dg = 0; dg < 8; dg++) {
+      OpDesc d;
+      d.kind = kind;
+      d.p = p_;
+      d.d[0] = ((dg & 1) ? 0.25 : -0.25);
+      d.d[1] = (((dg >> 1) & 1) ? 0.25 : -0.25);
+      d.d[2] = (((dg >> 2) & 1) ? 0.25 : -0.25);
+      d.off = off;
+      int dim = 2 * ncoef(p_);
+      off += (long long)dim * dim;
+      (kind == 1 ? P->m2m_group : P->l2l_group)[dg] = (int)descs.size();
+      P->dims.push_back(dim);
+      descs.push_back(d);
+    }
+  P->mats.resize(off);
+  DevBuf<OpDesc> dd;
+  dd.resize(descs.size());
+  EFMM_CUDA_TRY(cudaMemcpyAsync(dd.get(), descs.data(), descs.size() * sizeof(OpDesc),
+                                cudaMemcpyHostToDevice, st_));
+  launch_build_ops(st_, (int)descs.size(), dd.get(), P->mats.get(), p_);
+  std::vector<long long> offs(descs.size());
+  for (size_t i = 0; i < descs.size(); i++) offs[i] = descs[i].off;
+  P->off.resize(offs.size());
+  P->dim.resize(P->dims.size());
+  EFMM_CUDA_TRY(cudaMemcpyAsync(P->off.get(), offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st_));
+  EFMM_CUDA_TRY(cudaMemcpyAsync(P->dim.get(), P->dims.data(), P->dims.size() * 4, cudaMemcpyHostToDevice, st_));
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  g_ops[key] = P;
+  ops_ = P;
+}
+
+// ------------------------------------------------------------------ plan
+Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
+  for (int i = 0; i < 10; i++) EFMM_CUDA_TRY(cudaEventCreate(&ev_[i]));
+}
+Plan::~Plan() {
+  for (int i = 0; i < 10; i++) cudaEventDestroy(ev_[i]);
+}
+
+template <class T>
+static std::vector<T> d2h(const DevBuf<T>& b, size_t n, cudaStream_t st) {
+  std::vector<T> h(n);
+  if (n) EFMM_CUDA_TRY(cudaMemcpyAsync(h.data(), b.get(), n * sizeof(T), cudaMemcpyDeviceToHost, st));
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+  return h;
+}
+template <class T>
+static void h2d(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
+  b.resize(h.size());
+  if (!h.empty()) EFMM_CUDA_TRY(cudaMemcpyAsync(b.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
+int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const double* d_src, int nt,
+                       const double* d_tgt, int iprec, bool iter, bool mindlin) {
+  if (n < 1 || nt < 0) return IER_BADARG;
+  if (iprec < -2 || iprec > 6) return IER_BADARG;
+  n_ = n;
+  nt_ = nt;
+  iprec_ = iprec;
+  eps_ = iprec_eps(iprec);
+  nbox_ = iprec_nbox(iprec, n, nt, iter);
+  p_ = eps_ > 0 ? order_for_eps(eps_, 1.5) : 0;
+  // Expansion orders above 54 (iprec 5, eps 5e-16) exceed the P2M register
+  // tiling; at that tolerance the near-field-only evaluation (one box) is used.
+  if (p_ > 54) {
+    p_ = 0;
+    nbox_ = n + nt;
+  }
+  tri_u_.resize(9 * (size_t)n);
+  src_u_.resize(3 * (size_t)n);
+  tgt_u_.resize(3 * (size_t)nt);
+  EFMM_CUDA_TRY(cudaMemcpyAsync(tri_u_.get(), d_tri, 72 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+  EFMM_CUDA_TRY(cudaMemcpyAsync(src_u_.get(), d_src, 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+  if (nt) EFMM_CUDA_TRY(cudaMemcpyAsync(tgt_u_.get(), d_tgt, 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
+  int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_);
+  if (ier) return ier;
+  ier = build_lists(st_, tr_);
+  if (ier) return ier;
+  tri_s_.resize(9 * (size_t)n);
+  nrm_s_.resize(3 * (size_t)n);
+  src_s_.resize(3 * (size_t)n);
+  tgt_s_.resize(3 * (size_t)nt);
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 9, tr_.iz.get(), d_tri, tri_s_.get());
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_nrm, nrm_s_.get());
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_src, src_s_.get());
+  if (nt) k_gather<<<(nt + 255) / 256, 256, 0, st_>>>(nt, 3, tr_.izt.get(), d_tgt, tgt_s_.get());
+  build_worklists();
+  if (far_) ensure_ops();
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  return IER_OK;
+}
+
+void Plan::build_worklists() {
+  int nb = tr_.nboxes;
+  auto level = d2h(tr_.level, nb, st_);
+  auto ijk = d2h(tr_.ijk, 3 * (size_t)nb, st_);
+  auto parent = d2h(tr_.parent, nb, st_);
+  auto nkids = d2h(tr_.nkids, nb, st_);
+  auto kids = d2h(tr_.kids, 8 * (size_t)nb, st_);
+  auto scount = d2h(tr_.scount, nb, st_);
+  auto tcount = d2h(tr_.tcount, nb, st_);
+  auto csr = [&](const DevBuf<int>& s, const DevBuf<int>& it, std::vector<int>& hs, std::vector<int>& hi) {
+    hs = d2h(s, nb + 1, st_);
+    hi = d2h(it, hs[nb], st_);
+  };
+  std::vector<int> l1s, l1i, l2s, l2i, l3s, l3i, l4s, l4i;
+  csr(tr_.l1_start, tr_.l1_items, l1s, l1i);
+  csr(tr_.l2_start, tr_.l2_items, l2s, l2i);
+  csr(tr_.l3_start, tr_.l3_items, l3s, l3i);
+  csr(tr_.l4_start, tr_.l4_items, l4s, l4i);
+
+  // near field: per leaf with evaluation points, source boxes from
+  // list1 U self U list3 U list4(ancestors-or-self)  (ITER pairing,
+  // src/elfmm3dtria_iter_1.f:1188-1225, read from the target side)
+  std::vector<int> nleaves, nstart, nitems;
+  nstart.push_back(0);
+  for (int b = 0; b < nb; b++) {
+    if (nkids[b] != 0) continue;
+    if (scount[b] + tcount[b] == 0) continue;
+    size_t before = nitems.size();
+    auto add = [&](int s) {
+      if (scount[s] > 0) nitems.push_back(s);
+    };
+    for (int q = l1s[b]; q < l1s[b + 1]; q++) add(l1i[q]);
+    add(b);
+    for (int q = l3s[b]; q < l3s[b + 1]; q++) add(l3i[q]);
+    for (int a = b; a >= 0; a = parent[a])
+      for (int q = l4s[a]; q < l4s[a + 1]; q++) add(l4i[q]);
+    if (nitems.size() == before) continue;
+    nleaves.push_back(b);
+    nstart.push_back((int)nitems.size());
+  }
+  near_pairs_ = 0;
+  {
+    // count point pairs for the throughput model
+    auto sst = d2h(tr_.sstart, nb, st_);
+    for (size_t i = 0; i < nleaves.size(); i++) {
+      int b = nleaves[i];
+      long long ne = scount[b] + tcount[b];
+      long long ns = 0;
+      for (int q = nstart[i]; q < nstart[i + 1]; q++) ns += scount[nitems[q]];
+      near_pairs_ += ne * ns;
+    }
+    (void)sst;
+  }
+  nnear_ = (int)nleaves.size();
+  h2d(near_leaves_, nleaves, st_);
+  h2d(near_start_, nstart, st_);
+  h2d(near_items_, nitems, st_);
+
+  // far field
+  far_ = (p_ > 0) && (tr_.nlev >= 2);
+  std::vector<int> p2m, l2t;
+  for (int b = 0; b < nb; b++) {
+    if (nkids[b] != 0 || level[b] < 2) continue;
+    if (scount[b] > 0) p2m.push_back(b);
+    if (scount[b] + tcount[b] > 0) l2t.push_back(b);
+  }
+  if (p2m.empty()) far_ = false;
+  np2m_ = (int)p2m.size();
+  nl2t_ = (int)l2t.size();
+  h2d(p2m_leaves_, p2m, st_);
+  h2d(l2t_leaves_, l2t, st_);
+  m2m_lev_.clear();
+  l2l_lev_.clear();
+  if (!far_) return;
+  ensure_ops();
+  const int* m2lg = ops_->m2l_group;
+  const std::vector<int>& dims = ops_->dims;
+  auto tile = [&](std::vector<std::pair<int, TransPair>>& gp, std::vector<TransPair>& pairs,
+                  std::vector<TransTask>& tasks) {
+    std::stable_sort(gp.begin(), gp.end(),
+                     [](const std::pair<int, TransPair>& a, const std::pair<int, TransPair>& b) {
+                       return a.first < b.first;
+                     });
+    size_t i = 0;
+    while (i < gp.size()) {
+      size_t j = i;
+      while (j < gp.size() && gp[j].first == gp[i].first) j++;
+      int g = gp[i].first;
+      for (size_t c = i; c < j; c += 16) {
+        int np = (int)std::min<size_t>(16, j - c);
+        int p0 = (int)pairs.size();
+        for (int q = 0; q < np; q++) pairs.push_back(gp[c + q].second);
+        for (int r0 = 0; r0 < dims[g]; r0 += 64) tasks.push_back({g, r0, p0, np});
+      }
+      i = j;
+    }
+  };
+  std::vector<TransPair> m2m_pairs, l2l_pairs, m2l_pairs;
+  std::vector<TransTask> m2m_tasks, l2l_tasks, m2l_tasks;
+  // M2M bottom-up: children at level lev -> parents at lev-1 (parents >= 2)
+  for (int lev = tr_.nlev; lev >= 3; lev--) {
+    std::vector<std::pair<int, TransPair>> gp;
+    int lo = tr_.laddr[lev].first, cnt = tr_.laddr[lev].second;
+    for (int b = lo; b < lo + cnt; b++) {
+      if (scount[b] == 0) continue;
+      int P = parent[b];
+      int dg = ((ijk[3 * b] - 1) & 1) + 2 * ((ijk[3 * b + 1] - 1) & 1) + 4 * ((ijk[3 * b + 2] - 1) & 1);
+      gp.push_back({ops_->m2m_group[dg], TransPair{b, P, 1.0}});
+    }
+    int t0 = (int)m2m_tasks.size();
+    tile(gp, m2m_pairs, m2m_tasks);
+    m2m_lev_.push_back({t0, (int)m2m_tasks.size() - t0});
+  }
+  // M2L: list 2 of every box at level >= 2
+  {
+    std::vector<std::pair<int, TransPair>> gp;
+    for (int b = 0; b < nb; b++) {
+      if (level[b] < 2 || scount[b] + tcount[b] == 0) continue;
+      double s = tr_.size / (double)(1ull << level[b]);
+      for (int q = l2s[b]; q < l2s[b + 1]; q++) {
+        int sb = l2i[q];
+        if (scount[sb] == 0) continue;
+        int di = ijk[3 * b] - ijk[3 * sb], dj = ijk[3 * b + 1] - ijk[3 * sb + 1],
+            dk = ijk[3 * b + 2] - ijk[3 * sb + 2];
+        int g = m2lg[(di + 3) * 49 + (dj + 3) * 7 + (dk + 3)];
+        gp.push_back({g, TransPair{sb, b, 1.0 / s}});
+      }
+    }
+    m2l_pairs_h_ = gp.size();
+    tile(gp, m2l_pairs, m2l_tasks);
+  }
+  // L2L top-down: parents at level lev (>= 2) -> children
+  for (int lev = 2; lev < tr_.nlev; lev++) {
+    std::vector<std::pair<int, TransPair>> gp;
+    int lo = tr_.laddr[lev].first, cnt = tr_.laddr[lev].second;
+    for (int b = lo; b < lo + cnt; b++) {
+      for (int q = 0; q < nkids[b]; q++) {
+        int k = kids[8 * b + q];
+        if (scount[k] + tcount[k] == 0) continue;
+        int dg = ((ijk[3 * k] - 1) & 1) + 2 * ((ijk[3 * k + 1] - 1) & 1) + 4 * ((ijk[3 * k + 2] - 1) & 1);
+        gp.push_back({ops_->l2l_group[dg], TransPair{b, k, 1.0}});
+      }
+    }
+    int t0 = (int)l2l_tasks.size();
+    tile(gp, l2l_pairs, l2l_tasks);
+    l2l_lev_.push_back({t0, (int)l2l_tasks.size() - t0});
+  }
+  h2d(m2m_pairs_, m2m_pairs, st_);
+  h2d(m2m_tasks_, m2m_tasks, st_);
+  h2d(m2l_pairs_, m2l_pairs, st_);
+  h2d(m2l_tasks_, m2l_tasks, st_);
+  h2d(l2l_pairs_, l2l_pairs, st_);
+  h2d(l2l_tasks_, l2l_tasks, st_);
+  nm2l_tasks_ = (int)m2l_tasks.size();
+  int D = 2 * ncoef(p_);
+  mpole_.resize((size_t)nb * 4 * D);
+  local_.resize((size_t)nb * 4 * D);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+}
+
+int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
+                   double* d_e_src, double* d_u_tgt, double* d_e_tgt) {
+  int n = n_, nt = nt_;
+  int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+  int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
+  int ds_src = d_e_src ? 1 : 0, ds_tgt = d_e_tgt ? 1 : 0;
+  launches_ = 0;
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  ssl_s_.resize(3 * (size_t)n);
+  sdl_s_.resize(3 * (size_t)n);
+  if (dosl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_ssl, ssl_s_.get()); launches_++; }
+  if (dodl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_sdl, sdl_s_.get()); launches_++; }
+  u_s_.resize(3 * (size_t)n);
+  e_s_.resize(6 * (size_t)n);
+  ut_s_.resize(3 * (size_t)std::max(nt, 1));
+  et_s_.resize(6 * (size_t)std::max(nt, 1));
+  u_s_.zero(st_);
+  e_s_.zero(st_);
+  ut_s_.zero(st_);
+  et_s_.zero(st_);
+  double c1 = (rlam + rmu) / (rlam + 2 * rmu), c2 = rmu / (rlam + 2 * rmu);
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  int D = 2 * ncoef(p_);
+  if (far_ && (do_src || do_tgt)) {
+    mpole_.zero(st_);
+    local_.zero(st_);
+    P2MArgs pa;
+    pa.leaves = p2m_leaves_.get();
+    pa.level = tr_.level.get(); pa.ijk = tr_.ijk.get();
+    pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
+    for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
+    pa.size = tr_.size;
+    pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
+    pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
+    pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
+    pa.mpole = mpole_.get();
+    launch_p2m(st_, np2m_, pa);
+    launches_++;
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+    for (auto& r : m2m_lev_) {
+      launch_translate(st_, r.second, m2m_tasks_.get() + r.first, m2m_pairs_.get(), ops_->mats.get(),
+                       ops_->off.get(), ops_->dim.get(), D, mpole_.get(), mpole_.get());
+      if (r.second) launches_++;
+    }
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+    launch_translate(st_, nm2l_tasks_, m2l_tasks_.get(), m2l_pairs_.get(), ops_->mats.get(), ops_->off.get(),
+                     ops_->dim.get(), D, mpole_.get(), local_.get());
+    if (nm2l_tasks_) launches_++;
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+    for (auto& r : l2l_lev_) {
+      launch_translate(st_, r.second, l2l_tasks_.get() + r.first, l2l_pairs_.get(), ops_->mats.get(),
+                       ops_->off.get(), ops_->dim.get(), D, local_.get(), local_.get());
+      if (r.second) launches_++;
+    }
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
+    L2TArgs la;
+    la.leaves = l2t_leaves_.get();
+    la.level = tr_.level.get(); la.ijk = tr_.ijk.get();
+    la.sstart = tr_.sstart.get(); la.scount = tr_.scount.get();
+    la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
+    for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
+    la.size = tr_.size;
+    la.local = local_.get();
+    la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
+    la.p = p_; la.do_src = do_src; la.do_tgt = do_tgt;
+    la.dostrain_src = ds_src; la.dostrain_tgt = ds_tgt;
+    la.c1 = c1;
+    la.u_src = u_s_.get(); la.e_src = e_s_.get(); la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
+    launch_l2t(st_, nl2t_, la);
+    launches_++;
+  } else {
+    for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
+  // near field
+  trir_.resize(n);
+  launch_tri_prep(st_, n, tri_s_.get(), nullptr, ssl_s_.get(), sdl_s_.get(), dosl, dodl, trir_.get());
+  launches_++;
+  NearArgs na;
+  na.nleaf = nnear_;
+  na.leaves = near_leaves_.get(); na.nb_start = near_start_.get(); na.nb_items = near_items_.get();
+  na.box_src_start = tr_.sstart.get(); na.box_src_count = tr_.scount.get();
+  na.box_tgt_start = tr_.tstart.get(); na.box_tgt_count = tr_.tcount.get();
+  na.trir = trir_.get();
+  na.src_pts = src_s_.get(); na.tgt_pts = tgt_s_.get();
+  na.dosl = dosl; na.dodl = dodl; na.dostrain_src = ds_src; na.dostrain_tgt = ds_tgt;
+  na.do_src = do_src; na.do_tgt = do_tgt;
+  na.rlam = rlam; na.rmu = rmu;
+  na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
+  launch_near_leaf(st_, na);
+  launches_++;
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
+  if (do_src) {
+    k_scatter_out<<<(n + 255) / 256, 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src, d_e_src);
+    launches_++;
+  }
+  if (do_tgt) {
+    k_scatter_out<<<(nt + 255) / 256, 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(), d_u_tgt, d_e_tgt);
+    launches_++;
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+  EFMM_CUDA_TRY(cudaGetLastError());
+  EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
+  cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
+  cudaEventElapsedTime(&timings.prep, ev_[0], ev_[1]);
+  cudaEventElapsedTime(&timings.p2m, ev_[1], ev_[2]);
+  cudaEventElapsedTime(&timings.m2m, ev_[2], ev_[3]);
+  cudaEventElapsedTime(&timings.m2l, ev_[3], ev_[4]);
+  cudaEventElapsedTime(&timings.l2l, ev_[4], ev_[5]);
+  cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
+  cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
+  return IER_OK;
+}
+
+int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,
+                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt) {
+  int n = n_, nt = nt_;
+  int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+  trir_.resize(n);
+  launch_tri_prep(st_, n, tri_u_.get(), nullptr, d_ssl, d_sdl, dosl, dodl, trir_.get());
+  u_s_.resize(3 * (size_t)n);
+  e_s_.resize(6 * (size_t)n);
+  ut_s_.resize(3 * (size_t)std::max(nt, 1));
+  et_s_.resize(6 * (size_t)std::max(nt, 1));
+  u_s_.zero(st_);
+  e_s_.zero(st_);
+  ut_s_.zero(st_);
+  et_s_.zero(st_);
+  int do_src = (d_u_src || d_e_src) ? n : 0;
+  int do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? nt : 0;
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  launch_direct_all(st_, n, trir_.get(), do_src, src_u_.get(), do_tgt, tgt_u_.get(), dosl, dodl,
+                    d_e_src ? 1 : 0, d_e_tgt ? 1 : 0, rlam, rmu, u_s_.get(), e_s_.get(), ut_s_.get(),
+                    et_s_.get());
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  if (d_u_src) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_src, u_s_.get(), 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+  if (d_e_src) k_sym6to9<<<(n + 255) / 256, 256, 0, st_>>>(n, e_s_.get(), d_e_src);
+  if (nt && d_u_tgt) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_tgt, ut_s_.get(), 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
+  if (nt && d_e_tgt) k_sym6to9<<<(nt + 255) / 256, 256, 0, st_>>>(nt, et_s_.get(), d_e_tgt);
+  EFMM_CUDA_TRY(cudaGetLastError());
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  cudaEventElapsedTime(&timings.near, ev_[0], ev_[1]);
+  timings.total = timings.near;
+  return IER_OK;
+}
+
+}  // namespace efmm

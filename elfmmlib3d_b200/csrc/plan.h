@@ -1,0 +1,86 @@
+// plan.h -- host orchestration of one elastostatic layer-potential evaluation.
+#pragma once
+#include <vector>
+#include <utility>
+#include "devbuf.h"
+#include "tree.h"
+#include "fmm.h"
+#include "kernels.h"
+
+namespace efmm {
+
+// iprec -> tolerance and leaf capacity (src/elfmm3dtria.f:702-722; the ITER
+// routines double the leaf capacity, src/elhfmm3dtria_iter.f:1481-1491).
+double iprec_eps(int iprec);
+int iprec_nbox(int iprec, int nsrc, int ntarg, bool iter);
+
+struct OpPool {
+  int p = -1;
+  double eps = -1;
+  DevBuf<double> mats;
+  DevBuf<long long> off;
+  DevBuf<int> dim;
+  int m2l_group[343];
+  int m2m_group[8], l2l_group[8];
+  std::vector<int> dims;
+};
+
+struct Timings {  // milliseconds of the last evaluate(), CUDA events
+  float total = 0, p2m = 0, m2m = 0, m2l = 0, l2l = 0, l2t = 0, near = 0, prep = 0;
+};
+
+class Plan {
+ public:
+  Plan(int device, cudaStream_t stream);
+  ~Plan();
+  // geometry in user order, device pointers: tri (n,3,3), nrm (n,3), src (n,3), tgt (nt,3)
+  int set_geometry(int n, const double* d_tri, const double* d_nrm, const double* d_src, int nt,
+                   const double* d_tgt, int iprec, bool iter, bool mindlin);
+  // densities in user order (device); outputs in user order (device):
+  // u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3); null pointers disable them.
+  int evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
+               double* d_e_src, double* d_u_tgt, double* d_e_tgt);
+  // all-pairs direct sum on the same geometry (no tree needed)
+  int evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,
+                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt);
+  cudaStream_t stream() const { return st_; }
+  const Tree& tree() const { return tr_; }
+  Timings timings;
+  int n() const { return n_; }
+  int nt() const { return nt_; }
+  int order() const { return p_; }
+  int nbox() const { return nbox_; }
+  long long near_pairs() const { return near_pairs_; }
+  long long m2l_pairs() const { return (long long)m2l_pairs_h_; }
+  int kernel_launches() const { return launches_; }
+  bool far_enabled() const { return far_; }
+
+ private:
+  void build_worklists();
+  void ensure_ops();
+  int dev_;
+  cudaStream_t st_;
+  int n_ = 0, nt_ = 0, iprec_ = 2, nbox_ = 40, p_ = 0;
+  double eps_ = 0.5e-6;
+  bool far_ = false;
+  Tree tr_;
+  DevBuf<double> tri_s_, nrm_s_, src_s_, tgt_s_;
+  DevBuf<double> tri_u_;  // user-order triangles (for the direct sum)
+  DevBuf<double> src_u_, tgt_u_;
+  DevBuf<int> p2m_leaves_, l2t_leaves_, near_leaves_, near_start_, near_items_;
+  int np2m_ = 0, nl2t_ = 0, nnear_ = 0;
+  long long near_pairs_ = 0;
+  DevBuf<TransPair> m2m_pairs_, m2l_pairs_, l2l_pairs_;
+  DevBuf<TransTask> m2m_tasks_, m2l_tasks_, l2l_tasks_;
+  std::vector<std::pair<int, int>> m2m_lev_, l2l_lev_;  // task ranges per level (execution order)
+  int nm2l_tasks_ = 0;
+  size_t m2l_pairs_h_ = 0;
+  DevBuf<double> mpole_, local_;
+  DevBuf<double> ssl_s_, sdl_s_, u_s_, e_s_, ut_s_, et_s_;
+  DevBuf<TriRec> trir_;
+  OpPool* ops_ = nullptr;
+  cudaEvent_t ev_[10];
+  int launches_ = 0;
+};
+
+}  // namespace efmm

@@ -1,0 +1,110 @@
+/*
+ * elfmm3d_b200.h -- C ABI of the B200 elastostatic triangle-layer FMM.
+ *
+ * Two families of entry points:
+ *
+ * 1. Drop-in replacements for the reference's Fortran subroutines.  Every
+ *    argument is passed by reference, arrays are Fortran column-major
+ *    (triangle(3,3,n), sigma(3,n), ptfrc(3,n), strain(3,3,n)), integers are
+ *    32-bit and no hidden string lengths exist.  The symbols carry the
+ *    gfortran/ifort trailing underscore, so an unmodified Fortran caller links
+ *    against libelfmm3d_b200.so in place of the reference objects.  Host
+ *    arrays in, host arrays out; device memory is managed internally (the
+ *    reference likewise allocates its own scratch).  Outputs carry no 1/(4 pi)
+ *    factor, exactly like the reference.
+ *
+ * 2. A native device API (efmm_*) taking device pointers and returning ier,
+ *    used for resident-data pipelines, benchmarking and tests.
+ *
+ * Error codes (ier): 0 ok, 4 tree construction failed, 8 device allocation
+ * failed, 16 invalid argument; 256 CUDA error, 512 stored-operator handle
+ * mismatch, 1024 no CUDA device.
+ */
+#ifndef ELFMM3D_B200_H
+#define ELFMM3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- reference-compatible entry points ------------------------------- */
+
+/* Replaces elfmm3dtria (src/elfmm3dtria.f:71-74): on-surface evaluation at the
+ * n source points (triangle centroids). */
+void elfmm3dtria_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                  const double *triangle, const double *trinorm, const int *nparts,
+                  const double *source, const int *ifsingle, const double *sigma_sl,
+                  const int *ifdouble, const double *sigma_dl, const int *ifptfrc, double *ptfrc,
+                  const int *ifstrain, double *strain);
+
+/* Replaces elfmm3dtriatarg (src/elfmm3dtria.f:162-167): on-surface and
+ * off-surface targets. */
+void elfmm3dtriatarg_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                      const double *triangle, const double *trinorm, const int *nparts,
+                      const double *source, const int *ifsingle, const double *sigma_sl,
+                      const int *ifdouble, const double *sigma_dl, const int *ifptfrc,
+                      double *ptfrc, const int *ifstrain, double *strain, const int *ntargs,
+                      const double *target, const int *ifptfrctarg, double *ptfrctarg,
+                      const int *ifstraintarg, double *straintarg);
+
+/* Replaces el3dtriadirecttarg (src/elfmm3dtria.f:1483-1487): O(N^2) direct
+ * evaluation with the analytic triangle integrals.  (No ier, as in the
+ * reference; failures are reported on stderr and leave outputs at zero.) */
+void el3dtriadirecttarg_(const double *rlam, const double *rmu, const double *triangle,
+                         const double *trinorm, const int *nsource, const double *source,
+                         const int *ifsingle, const double *sigma_sl, const int *ifdouble,
+                         const double *sigma_dl, const int *ifptfrc, double *ptfrc,
+                         const int *ifstrain, double *strain, const int *ntarget,
+                         const double *target, const int *ifptfrctarg, double *ptfrctarg,
+                         const int *ifstraintarg, double *straintarg);
+
+/* ---- native device API ----------------------------------------------- */
+
+typedef struct efmm_plan efmm_plan;
+
+int efmm_device_count(void);
+
+/* Create a plan on CUDA device `device` (its own stream).  NULL on failure. */
+efmm_plan *efmm_plan_create(int device);
+void efmm_plan_destroy(efmm_plan *plan);
+
+/* Geometry (device pointers, user order): tri (n,3,3), nrm (n,3), src (n,3),
+ * tgt (nt,3).  iter != 0 selects the ITER leaf capacity (2x), mindlin != 0
+ * the half-space root box (centred on z = 0).  Builds the tree, the lists,
+ * the work lists and the translation operators. */
+int efmm_plan_set_geometry(efmm_plan *plan, int n, const double *tri, const double *nrm,
+                           const double *src, int nt, const double *tgt, int iprec, int iter,
+                           int mindlin);
+
+/* Evaluate with device densities ssl/sdl (n,3; NULL disables a layer) into
+ * device outputs u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3)
+ * (NULL disables an output).  Blocks until the results are complete. */
+int efmm_plan_evaluate(efmm_plan *plan, double rlam, double rmu, const double *ssl,
+                       const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                       double *e_tgt);
+
+/* Same outputs from the all-pairs direct sum on the plan's geometry. */
+int efmm_plan_evaluate_direct(efmm_plan *plan, double rlam, double rmu, const double *ssl,
+                              const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                              double *e_tgt);
+
+/* Per-stage device times (ms) of the last evaluate: total, prep, p2m, m2m,
+ * m2l, l2l, l2t, near. */
+void efmm_plan_timings(const efmm_plan *plan, float *ms8);
+
+/* info[0..7] = nboxes, nlev, expansion order p, leaf capacity nbox,
+ * near-field point pairs, M2L box pairs, kernels launched by the last
+ * evaluate, far field enabled. */
+void efmm_plan_info(const efmm_plan *plan, long long *info8);
+
+/* Export the tree in the reference layout (1-based, src/d3tstrcr.f:1292-1310):
+ * boxes (nboxes,20), iz (n), iztarg (nt), laddr (nlev+1,2), center (3), size,
+ * and lists 1..5 as CSR: lstart (5, nboxes+1) and litems (sum of counts).
+ * With litems == NULL only lcount[5] is filled. */
+int efmm_plan_tree_export(const efmm_plan *plan, int *boxes, int *iz, int *iztarg, int *laddr,
+                          double *center_size4, int *lstart, int *litems, long long *lcount5);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
