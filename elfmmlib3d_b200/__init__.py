@@ -27,7 +27,8 @@ __all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "Plan", "load
            "library_path", "device_count", "ElfmmError"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-_LIB_PATH = os.path.join(_HERE, "libelfmm3d_b200.so")
+# ELFMM3D_LIB may point at another build of the same library (e.g. a variant)
+_LIB_PATH = os.environ.get("ELFMM3D_LIB", os.path.join(_HERE, "libelfmm3d_b200.so"))
 _lib = None
 
 _dp = ctypes.POINTER(ctypes.c_double)
@@ -40,7 +41,8 @@ _vp = ctypes.c_void_p
 EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_device_count",
            "efmm_plan_create", "efmm_plan_destroy", "efmm_plan_set_geometry",
            "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings",
-           "efmm_plan_info", "efmm_plan_tree_export"]
+           "efmm_plan_info", "efmm_plan_tree_export", "efmm_kernel_launches", "efmm_plan_record",
+           "efmm_plan_elapsed"]
 
 
 class ElfmmError(RuntimeError):
@@ -73,6 +75,11 @@ def load():
         f.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp]
     L.efmm_plan_timings.argtypes = [_vp, _fp]
     L.efmm_plan_info.argtypes = [_vp, _llp]
+    L.efmm_kernel_launches.restype = ctypes.c_longlong
+    L.efmm_plan_record.restype = ctypes.c_int
+    L.efmm_plan_record.argtypes = [_vp, ctypes.c_int]
+    L.efmm_plan_elapsed.restype = ctypes.c_float
+    L.efmm_plan_elapsed.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.efmm_plan_tree_export.restype = ctypes.c_int
     L.efmm_plan_tree_export.argtypes = [_vp, _ip, _ip, _ip, _ip, _dp, _ip, _ip, _llp]
     _lib = L
@@ -81,6 +88,11 @@ def load():
 
 def device_count():
     return load().efmm_device_count()
+
+
+def kernel_launches():
+    """Kernels of this library launched so far in the process."""
+    return int(load().efmm_kernel_launches())
 
 
 def _need_gpu():
@@ -204,6 +216,15 @@ class Plan:
                 self._ptr(e), self._ptr(ut), self._ptr(et))
         if ier:
             raise ElfmmError(ier, "evaluate")
+
+    def record(self, slot):
+        """Record CUDA event `slot` (0..7) on the plan's stream."""
+        if self._L.efmm_plan_record(self._h, int(slot)):
+            raise ElfmmError(16, "record")
+
+    def elapsed(self, a, b):
+        """Device milliseconds between recorded slots a and b."""
+        return float(self._L.efmm_plan_elapsed(self._h, int(a), int(b)))
 
     def timings(self):
         a = (ctypes.c_float * 8)()

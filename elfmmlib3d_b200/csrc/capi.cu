@@ -13,6 +13,7 @@ struct efmm_plan {
   int device;
   cudaStream_t stream;
   std::unique_ptr<Plan> plan;
+  cudaEvent_t user_ev[8];
 };
 
 static int env_device() {
@@ -34,6 +35,7 @@ extern "C" efmm_plan* efmm_plan_create(int device) {
     p->device = device;
     EFMM_CUDA_TRY(cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking));
     p->plan.reset(new Plan(device, p->stream));
+    for (int i = 0; i < 8; i++) EFMM_CUDA_TRY(cudaEventCreate(&p->user_ev[i]));
     return p;
   } catch (...) {
     return nullptr;
@@ -44,6 +46,7 @@ extern "C" void efmm_plan_destroy(efmm_plan* p) {
   if (!p) return;
   cudaSetDevice(p->device);
   p->plan.reset();
+  for (int i = 0; i < 8; i++) cudaEventDestroy(p->user_ev[i]);
   cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -77,6 +80,22 @@ extern "C" int efmm_plan_evaluate_direct(efmm_plan* p, double rlam, double rmu, 
                                          double* u_tgt, double* e_tgt) {
   if (!p) return IER_BADARG;
   EFMM_GUARD(return p->plan->evaluate_direct(rlam, rmu, ssl, sdl, u_src, e_src, u_tgt, e_tgt);)
+}
+
+extern "C" long long efmm_kernel_launches(void) { return efmm::launches_total(); }
+
+extern "C" int efmm_plan_record(efmm_plan* p, int slot) {
+  if (!p || slot < 0 || slot >= 8) return IER_BADARG;
+  EFMM_GUARD(EFMM_CUDA_TRY(cudaEventRecord(p->user_ev[slot], p->stream)); return IER_OK;)
+}
+
+extern "C" float efmm_plan_elapsed(efmm_plan* p, int a, int b) {
+  if (!p || a < 0 || a >= 8 || b < 0 || b >= 8) return -1.0f;
+  cudaSetDevice(p->device);
+  float ms = -1.0f;
+  if (cudaEventSynchronize(p->user_ev[b]) != cudaSuccess) return -1.0f;
+  if (cudaEventElapsedTime(&ms, p->user_ev[a], p->user_ev[b]) != cudaSuccess) return -1.0f;
+  return ms;
 }
 
 extern "C" void efmm_plan_timings(const efmm_plan* p, float* ms) {

@@ -4,7 +4,6 @@
 #include <cstdint>
 #include <cstdio>
 
-#include "jets.cuh"
 #include "tri_integrals.cuh"
 #include "harmonics.cuh"
 
@@ -62,6 +61,10 @@ struct __align__(16) TriRec {
   double pad[2];
 };
 static_assert(sizeof(TriRec) == 192, "TriRec layout");
+
+// Number of this library's kernels launched so far (all devices, all plans).
+long long launches_total();
+void count_launch(int k = 1);
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll

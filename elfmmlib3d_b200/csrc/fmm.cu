@@ -419,7 +419,7 @@ void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats,
   size_t smem = sizeof(cplx) * (size_t)ncoef(2 * maxp);
   if (smem > 48 * 1024)
     EFMM_CUDA_TRY(cudaFuncSetAttribute(k_build_ops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_build_ops<<<nop, 256, smem, st>>>(nop, ops, mats);
+  k_build_ops<<<nop, 256, smem, st>>>(nop, ops, mats); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
@@ -428,7 +428,7 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a) {
   size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 16 * P2M_NODES);
   if (smem > 48 * 1024)
     EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_p2m<<<nleaf, P2M_THREADS, smem, st>>>(a);
+  k_p2m<<<nleaf, P2M_THREADS, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
@@ -436,7 +436,7 @@ void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const 
                       const double* mats, const long long* mat_off, const int* mat_dim, int D,
                       const double* src, double* dst) {
   if (ntask <= 0) return;
-  k_translate<<<ntask, 256, 0, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, src, dst);
+  k_translate<<<ntask, 256, 0, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, src, dst); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
@@ -450,7 +450,7 @@ void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a) {
   size_t smem = need(nw);
   if (smem > 48 * 1024)
     EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_l2t<<<nleaf, nw * 32, smem, st>>>(a);
+  k_l2t<<<nleaf, nw * 32, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 

@@ -1,9 +1,8 @@
-"""Generate jets_gen.cuh: straight-line code for order-3 jet products and for
-the table/assembly steps of the analytic near field.
+"""Generate assemble_gen.cuh: straight-line code for the local-frame single
+and double layer assembly of the analytic near field from the R/B tables.
 
-Fully unrolled nested template loops made nvcc's front end explode, so the
-index arithmetic is resolved here once and emitted as plain statements.
-Run: python gen_jets.py > jets_gen.cuh
+The index arithmetic of the assembly is resolved here once and emitted as
+plain statements.  Run: python gen_assemble.py > assemble_gen.cuh
 """
 
 
@@ -29,44 +28,6 @@ def fact(n):
     return r
 
 
-def emit_mul(N, name):
-    idx = multi(N)
-    assert [jidx(*t) for t in idx] == list(range(len(idx)))
-    out = [f"EFMM_HD void {name}(const double* __restrict__ x, const double* __restrict__ y, double* __restrict__ z) {{"]
-    for (a, b, c) in idx:
-        terms = []
-        for (a1, b1, c1) in multi(a + b + c):
-            if a1 <= a and b1 <= b and c1 <= c:
-                terms.append(f"x[{jidx(a1, b1, c1)}] * y[{jidx(a - a1, b - b1, c - c1)}]")
-        out.append(f"  z[{jidx(a, b, c)}] = " + " + ".join(terms) + ";")
-    out.append("}")
-    return "\n".join(out)
-
-
-def emit_tables():
-    # in-plane entries: X(a) += sgn * m_d * D^(a - e_d) L ; D^b L = b! * coef_b
-    out = ["// Accumulate one edge's contribution to the in-plane table entries.",
-           "EFMM_HD void tables_edge(const double* __restrict__ L1, const double* __restrict__ Lr,",
-           "                         double mx, double my, double* __restrict__ R, double* __restrict__ B) {"]
-    for (ix, iy, iz) in multi(4):
-        if ix + iy == 0:
-            continue
-        n = ix + iy + iz
-        sgn = 1.0 if n % 2 == 1 else -1.0
-        if ix >= 1:
-            d = (ix - 1, iy, iz)
-            m = "mx"
-        else:
-            d = (ix, iy - 1, iz)
-            m = "my"
-        f = sgn * fact(d[0]) * fact(d[1]) * fact(d[2])
-        out.append(f"  B[{jidx(ix, iy, iz)}] += ({f!r}) * {m} * Lr[{jidx(*d)}];")
-        if n <= 2:
-            out.append(f"  R[{jidx(ix, iy, iz)}] += ({f!r}) * {m} * L1[{jidx(*d)}];")
-    out.append("}")
-    return "\n".join(out)
-
-
 def e(*ax):
     c = [0, 0, 0]
     for a in ax:
@@ -76,8 +37,8 @@ def e(*ax):
 
 def emit_assemble():
     L = []
-    L.append("// Local-frame single/double layer displacement and (unsymmetrised x2)")
-    L.append("// displacement gradient from the tables (see assemble_local in tri_integrals.cuh).")
+    L.append("// Local-frame single/double layer displacement and symmetric")
+    L.append("// strain from the R/B tables; pair_eval (tri_integrals.cuh) rotates and scales.")
     L.append("EFMM_HD void assemble_gen(const double* __restrict__ R, const double* __restrict__ B,")
     L.append("    double rlam, double rmu, double c1, const double* ssl, const double* sdl,")
     L.append("    bool dosl, bool dodl, bool dostrain, double* __restrict__ ul, double* __restrict__ el) {")
@@ -155,11 +116,9 @@ def emit_assemble():
 
 
 if __name__ == "__main__":
-    print("// jets_gen.cuh -- GENERATED by gen_jets.py; do not edit by hand.")
+    print("// assemble_gen.cuh -- GENERATED by gen_assemble.py; do not edit by hand.")
     print("#pragma once")
-    print('#include "jets.cuh"')
+    print("// included from tri_integrals.cuh (needs EFMM_HD)")
     print("namespace efmm {")
-    print(emit_mul(3, "jet3_mul"))
-    print(emit_tables())
     print(emit_assemble())
     print("}  // namespace efmm")

@@ -20,7 +20,8 @@
 // independent in these units (M2L carries an extra 1/s), so each translation
 // is one real matrix per relative offset, applied as a dense contraction.
 #pragma once
-#include "jets.cuh"
+#include <math.h>
+#include "tri_index.cuh"
 
 namespace efmm {
 

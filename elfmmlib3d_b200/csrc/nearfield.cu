@@ -42,6 +42,9 @@ __global__ void k_tri_prep(int n, const double* __restrict__ tri, const int* __r
 constexpr int NF_TILE = 64;    // triangles staged per tile
 constexpr int NF_WARPS = 4;    // warps per CTA
 constexpr int NF_MAXEP = 512;  // max evaluation points per leaf held in shared memory
+#ifndef NF_MINB
+#define NF_MINB 2               // resident CTAs per SM the register budget targets
+#endif
 
 __device__ __forceinline__ void stage_tile(TriRec* sm, const TriRec* __restrict__ g, int cnt) {
   const double2* src = reinterpret_cast<const double2*>(g);
@@ -54,7 +57,7 @@ __device__ __forceinline__ void stage_tile(TriRec* sm, const TriRec* __restrict_
 // centroids, self-aware) then its targets.  nb_start/nb_items: CSR of the
 // source boxes paired with the leaf; box_src_start/count give their triangle
 // ranges.  Outputs are ADDED to u (3/pt) and e (6/pt, xx yy zz xy xz yz).
-__global__ void __launch_bounds__(NF_WARPS * 32)
+__global__ void __launch_bounds__(NF_WARPS * 32, NF_MINB)
 k_near_leaf(int nleaf, const int* __restrict__ leaves, const int* __restrict__ nb_start,
             const int* __restrict__ nb_items, const int* __restrict__ box_src_start,
             const int* __restrict__ box_src_count, const int* __restrict__ box_tgt_start,
@@ -133,7 +136,7 @@ k_near_leaf(int nleaf, const int* __restrict__ leaves, const int* __restrict__ n
 // per evaluation point, all triangles streamed through shared memory.
 // Points [0, nsrc) are the centroids (self pair when the indices match),
 // [nsrc, nsrc+ntgt) the targets.  Outputs are overwritten.
-__global__ void __launch_bounds__(NF_WARPS * 32)
+__global__ void __launch_bounds__(NF_WARPS * 32, NF_MINB)
 k_direct_all(int ntri, const TriRec* __restrict__ trir, int nsrc, const double* __restrict__ src_pts,
              int ntgt, const double* __restrict__ tgt_pts, int dosl, int dodl, int dostrain_src,
              int dostrain_tgt, double rlam, double rmu, double* __restrict__ u_src,
@@ -185,7 +188,7 @@ k_direct_all(int ntri, const TriRec* __restrict__ trir, int nsrc, const double* 
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out) {
   if (n <= 0) return;
-  k_tri_prep<<<(n + 127) / 128, 128, 0, st>>>(n, tri, perm, ssl, sdl, dosl, dodl, out);
+  k_tri_prep<<<(n + 127) / 128, 128, 0, st>>>(n, tri, perm, ssl, sdl, dosl, dodl, out); count_launch();
 }
 
 void launch_near_leaf(cudaStream_t st, const NearArgs& a) {
@@ -194,7 +197,7 @@ void launch_near_leaf(cudaStream_t st, const NearArgs& a) {
       a.nleaf, a.leaves, a.nb_start, a.nb_items, a.box_src_start, a.box_src_count,
       a.box_tgt_start, a.box_tgt_count, a.trir, a.src_pts, a.tgt_pts, a.dosl, a.dodl,
       a.dostrain_src, a.dostrain_tgt, a.do_src, a.do_tgt, a.rlam, a.rmu, a.u_src, a.e_src,
-      a.u_tgt, a.e_tgt);
+      a.u_tgt, a.e_tgt); count_launch();
 }
 
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
@@ -205,7 +208,7 @@ void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, 
   if (nep <= 0) return;
   k_direct_all<<<(nep + NF_WARPS - 1) / NF_WARPS, NF_WARPS * 32, 0, st>>>(
       ntri, trir, nsrc, src_pts, ntgt, tgt_pts, dosl, dodl, dostrain_src, dostrain_tgt, rlam, rmu,
-      u_src, e_src, u_tgt, e_tgt);
+      u_src, e_src, u_tgt, e_tgt); count_launch();
 }
 
 }  // namespace efmm

@@ -4,9 +4,14 @@
 #include <mutex>
 #include <vector>
 #include <cstring>
+#include <atomic>
 #include "plan.h"
 
 namespace efmm {
+
+static std::atomic<long long> g_launches{0};
+long long launches_total() { return g_launches.load(); }
+void count_launch(int k) { g_launches += k; }
 
 double iprec_eps(int iprec) {
   switch (iprec) {
@@ -195,10 +200,10 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   nrm_s_.resize(3 * (size_t)n);
   src_s_.resize(3 * (size_t)n);
   tgt_s_.resize(3 * (size_t)nt);
-  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 9, tr_.iz.get(), d_tri, tri_s_.get());
-  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_nrm, nrm_s_.get());
-  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_src, src_s_.get());
-  if (nt) k_gather<<<(nt + 255) / 256, 256, 0, st_>>>(nt, 3, tr_.izt.get(), d_tgt, tgt_s_.get());
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 9, tr_.iz.get(), d_tri, tri_s_.get()); count_launch();
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_nrm, nrm_s_.get()); count_launch();
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_src, src_s_.get()); count_launch();
+  if (nt) { k_gather<<<(nt + 255) / 256, 256, 0, st_>>>(nt, 3, tr_.izt.get(), d_tgt, tgt_s_.get()); count_launch(); }
   build_worklists();
   if (far_) ensure_ops();
   EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
@@ -371,12 +376,12 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
   int ds_src = d_e_src ? 1 : 0, ds_tgt = d_e_tgt ? 1 : 0;
-  launches_ = 0;
+  long long launch0 = launches_total();
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
   ssl_s_.resize(3 * (size_t)n);
   sdl_s_.resize(3 * (size_t)n);
-  if (dosl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_ssl, ssl_s_.get()); launches_++; }
-  if (dodl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_sdl, sdl_s_.get()); launches_++; }
+  if (dosl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_ssl, ssl_s_.get()); count_launch(); }
+  if (dodl) { k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_sdl, sdl_s_.get()); count_launch(); }
   u_s_.resize(3 * (size_t)n);
   e_s_.resize(6 * (size_t)n);
   ut_s_.resize(3 * (size_t)std::max(nt, 1));
@@ -402,22 +407,18 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
     pa.mpole = mpole_.get();
     launch_p2m(st_, np2m_, pa);
-    launches_++;
     EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
     for (auto& r : m2m_lev_) {
       launch_translate(st_, r.second, m2m_tasks_.get() + r.first, m2m_pairs_.get(), ops_->mats.get(),
                        ops_->off.get(), ops_->dim.get(), D, mpole_.get(), mpole_.get());
-      if (r.second) launches_++;
     }
     EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
     launch_translate(st_, nm2l_tasks_, m2l_tasks_.get(), m2l_pairs_.get(), ops_->mats.get(), ops_->off.get(),
                      ops_->dim.get(), D, mpole_.get(), local_.get());
-    if (nm2l_tasks_) launches_++;
     EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
     for (auto& r : l2l_lev_) {
       launch_translate(st_, r.second, l2l_tasks_.get() + r.first, l2l_pairs_.get(), ops_->mats.get(),
                        ops_->off.get(), ops_->dim.get(), D, local_.get(), local_.get());
-      if (r.second) launches_++;
     }
     EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
     L2TArgs la;
@@ -434,7 +435,6 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     la.c1 = c1;
     la.u_src = u_s_.get(); la.e_src = e_s_.get(); la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
     launch_l2t(st_, nl2t_, la);
-    launches_++;
   } else {
     for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
   }
@@ -442,7 +442,6 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   // near field
   trir_.resize(n);
   launch_tri_prep(st_, n, tri_s_.get(), nullptr, ssl_s_.get(), sdl_s_.get(), dosl, dodl, trir_.get());
-  launches_++;
   NearArgs na;
   na.nleaf = nnear_;
   na.leaves = near_leaves_.get(); na.nb_start = near_start_.get(); na.nb_items = near_items_.get();
@@ -455,15 +454,12 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   na.rlam = rlam; na.rmu = rmu;
   na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
   launch_near_leaf(st_, na);
-  launches_++;
   EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
   if (do_src) {
-    k_scatter_out<<<(n + 255) / 256, 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src, d_e_src);
-    launches_++;
+    k_scatter_out<<<(n + 255) / 256, 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src, d_e_src); count_launch();
   }
   if (do_tgt) {
-    k_scatter_out<<<(nt + 255) / 256, 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(), d_u_tgt, d_e_tgt);
-    launches_++;
+    k_scatter_out<<<(nt + 255) / 256, 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(), d_u_tgt, d_e_tgt); count_launch();
   }
   EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
   EFMM_CUDA_TRY(cudaGetLastError());
@@ -476,6 +472,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   cudaEventElapsedTime(&timings.l2l, ev_[4], ev_[5]);
   cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
   cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
+  launches_ = (int)(launches_total() - launch0);
   return IER_OK;
 }
 
@@ -501,9 +498,9 @@ int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const do
                     et_s_.get());
   EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
   if (d_u_src) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_src, u_s_.get(), 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
-  if (d_e_src) k_sym6to9<<<(n + 255) / 256, 256, 0, st_>>>(n, e_s_.get(), d_e_src);
+  if (d_e_src) { k_sym6to9<<<(n + 255) / 256, 256, 0, st_>>>(n, e_s_.get(), d_e_src); count_launch(); }
   if (nt && d_u_tgt) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_tgt, ut_s_.get(), 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
-  if (nt && d_e_tgt) k_sym6to9<<<(nt + 255) / 256, 256, 0, st_>>>(nt, et_s_.get(), d_e_tgt);
+  if (nt && d_e_tgt) { k_sym6to9<<<(nt + 255) / 256, 256, 0, st_>>>(nt, et_s_.get(), d_e_tgt); count_launch(); }
   EFMM_CUDA_TRY(cudaGetLastError());
   EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
   cudaEventElapsedTime(&timings.near, ev_[0], ev_[1]);

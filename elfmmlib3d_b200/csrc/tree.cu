@@ -313,7 +313,7 @@ static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, D
   v0.resize(np);
   items.resize(np);
   if (np > 0) {
-    k_pair_keys<<<(np + 255) / 256, 256, 0, st>>>(np, pairs.get(), k0.get(), v0.get());
+    k_pair_keys<<<(np + 255) / 256, 256, 0, st>>>(np, pairs.get(), k0.get(), v0.get()); count_launch();
     size_t bytes = 0;
     cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.get(), k1.get(), v0.get(), items.get(), np, 0, 64, st);
     if (bytes > tmp.size()) tmp.resize(bytes);
@@ -322,7 +322,7 @@ static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, D
   DevBuf<int> cnt;
   cnt.resize(nb + 1);
   cnt.zero(st);
-  if (np > 0) k_csr_count<<<(np + 255) / 256, 256, 0, st>>>(np, k1.get(), cnt.get());
+  if (np > 0) { k_csr_count<<<(np + 255) / 256, 256, 0, st>>>(np, k1.get(), cnt.get()); count_launch(); }
   start.resize(nb + 1);
   exclusive_scan(st, cnt.get(), start.get(), nb + 1, tmp);
   EFMM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -356,8 +356,8 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
       init[3 + c] = 0ull;
     }
     EFMM_CUDA_TRY(cudaMemcpyAsync(bb.get(), init, sizeof(init), cudaMemcpyHostToDevice, st));
-    k_bbox<<<148, 256, 0, st>>>(n, d_src, bb.get());
-    if (nt > 0) k_bbox<<<148, 256, 0, st>>>(nt, d_tgt, bb.get());
+    k_bbox<<<148, 256, 0, st>>>(n, d_src, bb.get()); count_launch();
+    if (nt > 0) { k_bbox<<<148, 256, 0, st>>>(nt, d_tgt, bb.get()); count_launch(); }
   }
   std::vector<unsigned long long> hb = to_host((unsigned long long*)bb.get(), 6, st);
   double mn[3], mx[3];
@@ -445,16 +445,16 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     off.resize(nl);
     cs.zero(st);
     ct.zero(st);
-    k_split<<<(nl + 255) / 256, 256, 0, st>>>(lo, hi, nbox, tr.scount.get(), tr.tcount.get(), split.get());
+    k_split<<<(nl + 255) / 256, 256, 0, st>>>(lo, hi, nbox, tr.scount.get(), tr.tcount.get(), split.get()); count_launch();
     double side = size / (double)(1ull << lev);
     k_digits<<<(n + 255) / 256, 256, 0, st>>>(n, d_src, tr.iz.get(), pbs.get(), tr.level.get(), lev, lo,
                                               split.get(), tr.ijk.get(), tr.sstart.get(), tr.c0[0],
-                                              tr.c0[1], tr.c0[2], size, side, ks.get(), cs.get());
+                                              tr.c0[1], tr.c0[2], size, side, ks.get(), cs.get()); count_launch();
     if (nt > 0)
       k_digits<<<(nt + 255) / 256, 256, 0, st>>>(nt, d_tgt, tr.izt.get(), pbt.get(), tr.level.get(), lev,
                                                  lo, split.get(), tr.ijk.get(), tr.tstart.get(), tr.c0[0],
-                                                 tr.c0[1], tr.c0[2], size, side, kt.get(), ct.get());
-    k_nchild<<<(nl + 255) / 256, 256, 0, st>>>(nl, split.get(), cs.get(), ct.get(), nch.get());
+                                                 tr.c0[1], tr.c0[2], size, side, kt.get(), ct.get()); count_launch();
+    k_nchild<<<(nl + 255) / 256, 256, 0, st>>>(nl, split.get(), cs.get(), ct.get(), nch.get()); count_launch();
     exclusive_scan(st, nch.get(), off.get(), nl, tmp);
     int last[2];
     EFMM_CUDA_TRY(cudaMemcpyAsync(&last[0], nch.get() + nl - 1, 4, cudaMemcpyDeviceToHost, st));
@@ -484,11 +484,11 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     k_children<<<(nl + 127) / 128, 128, 0, st>>>(lo, hi, lev, split.get(), cs.get(), ct.get(), off.get(),
                                                  tr.level.get(), tr.ijk.get(), tr.parent.get(), tr.kids.get(),
                                                  tr.nkids.get(), tr.sstart.get(), tr.scount.get(),
-                                                 tr.tstart.get(), tr.tcount.get());
+                                                 tr.tstart.get(), tr.tcount.get()); count_launch();
     int nh = hi + nnew;
-    k_pbox<<<(nnew * 32 + 255) / 256, 256, 0, st>>>(hi, nh, tr.sstart.get(), tr.scount.get(), pbs.get());
+    k_pbox<<<(nnew * 32 + 255) / 256, 256, 0, st>>>(hi, nh, tr.sstart.get(), tr.scount.get(), pbs.get()); count_launch();
     if (nt > 0)
-      k_pbox<<<(nnew * 32 + 255) / 256, 256, 0, st>>>(hi, nh, tr.tstart.get(), tr.tcount.get(), pbt.get());
+      k_pbox<<<(nnew * 32 + 255) / 256, 256, 0, st>>>(hi, nh, tr.tstart.get(), tr.tcount.get(), pbt.get()); count_launch();
     tr.laddr.push_back({hi, nnew});
     lo = hi;
     hi = nh;
@@ -514,7 +514,7 @@ int build_lists(cudaStream_t st, Tree& tr) {
   // lists 5 and 2, level by level (colleagues of the parent must exist)
   for (int lev = 1; lev <= tr.nlev; lev++) {
     int lo = tr.laddr[lev].first, cnt = tr.laddr[lev].second;
-    k_list52<<<(cnt + 127) / 128, 128, 0, st>>>(T, lo, lo + cnt, 0, l2cnt.get(), nullptr, nullptr);
+    k_list52<<<(cnt + 127) / 128, 128, 0, st>>>(T, lo, lo + cnt, 0, l2cnt.get(), nullptr, nullptr); count_launch();
   }
   exclusive_scan(st, l2cnt.get(), l2off.get(), nb, tmp);
   int tot2 = 0;
@@ -529,12 +529,12 @@ int build_lists(cudaStream_t st, Tree& tr) {
   l2items.resize(tot2);
   for (int lev = 1; lev <= tr.nlev; lev++) {
     int lo = tr.laddr[lev].first, cnt = tr.laddr[lev].second;
-    k_list52<<<(cnt + 127) / 128, 128, 0, st>>>(T, lo, lo + cnt, 1, nullptr, l2off.get(), l2items.get());
+    k_list52<<<(cnt + 127) / 128, 128, 0, st>>>(T, lo, lo + cnt, 1, nullptr, l2off.get(), l2items.get()); count_launch();
   }
   {
     DevBuf<int2> pairs;
     pairs.resize(tot2);
-    if (nb) k_l2_pairs<<<(nb + 127) / 128, 128, 0, st>>>(nb, l2off.get(), l2cnt.get(), l2items.get(), pairs.get());
+    if (nb) { k_l2_pairs<<<(nb + 127) / 128, 128, 0, st>>>(nb, l2off.get(), l2cnt.get(), l2items.get(), pairs.get()); count_launch(); }
     pairs_to_csr(st, pairs, tot2, nb, tr.l2_start, tr.l2_items, tmp);
   }
   // lists 1 and 3
@@ -543,7 +543,7 @@ int build_lists(cudaStream_t st, Tree& tr) {
   c3.resize(nb);
   o1.resize(nb + 1);
   o3.resize(nb + 1);
-  k_list13<<<(nb + 127) / 128, 128, 0, st>>>(T, nb, 0, c1.get(), c3.get(), nullptr, nullptr, nullptr, nullptr);
+  k_list13<<<(nb + 127) / 128, 128, 0, st>>>(T, nb, 0, c1.get(), c3.get(), nullptr, nullptr, nullptr, nullptr); count_launch();
   exclusive_scan(st, c1.get(), o1.get(), nb, tmp);
   exclusive_scan(st, c3.get(), o3.get(), nb, tmp);
   int h[4];
@@ -556,10 +556,10 @@ int build_lists(cudaStream_t st, Tree& tr) {
   DevBuf<int2> p1, p3, p4;
   p1.resize(tot1);
   p3.resize(tot3);
-  k_list13<<<(nb + 127) / 128, 128, 0, st>>>(T, nb, 1, nullptr, nullptr, o1.get(), o3.get(), p1.get(), p3.get());
+  k_list13<<<(nb + 127) / 128, 128, 0, st>>>(T, nb, 1, nullptr, nullptr, o1.get(), o3.get(), p1.get(), p3.get()); count_launch();
   pairs_to_csr(st, p1, tot1, nb, tr.l1_start, tr.l1_items, tmp);
   p4.resize(tot3);
-  if (tot3) k_transpose_pairs<<<(tot3 + 255) / 256, 256, 0, st>>>(tot3, p3.get(), p4.get());
+  if (tot3) { k_transpose_pairs<<<(tot3 + 255) / 256, 256, 0, st>>>(tot3, p3.get(), p4.get()); count_launch(); }
   pairs_to_csr(st, p3, tot3, nb, tr.l3_start, tr.l3_items, tmp);
   pairs_to_csr(st, p4, tot3, nb, tr.l4_start, tr.l4_items, tmp);
   EFMM_CUDA_TRY(cudaStreamSynchronize(st));

@@ -14,9 +14,14 @@
 //   * every derivative with an in-plane component a in {x, y} is moved onto
 //     the boundary by the divergence theorem,
 //         int_T d_a g dS = sum_edges m_a int_edge g dl   (m = outward normal),
-//     leaving line integrals L1_e = int_e 1/r dl and Lr_e = int_e r dl whose
-//     remaining target derivatives (up to third order) come from evaluating
-//     their closed forms on Taylor jets (jets.cuh);
+//     leaving line integrals L1_e = int_e 1/r dl and Lr_e = int_e r dl;
+//   * a line integral depends on the target only through the endpoint
+//     distances and c^2 = v^2 + h^2 (v, h: in-plane normal and normal offsets
+//     from the edge line), so its derivatives are endpoint terms (derivatives
+//     along the edge) and derivatives of F(c^2), which need only the three
+//     integrals K_n = int (s^2 + c^2)^(-n/2) ds, n = 1, 3, 5, in closed form;
+//     the rotation from the edge frame to the triangle frame is generated
+//     (gen_edge.py -> edge_gen.cuh);
 //   * pure normal derivatives follow from harmonicity of 1/r and from
 //     d_h int r = h int 1/r, which needs only the triangle potential
 //     Phi = int_T 1/r and the signed solid angle Omega = int_T h/r^3.
@@ -28,7 +33,10 @@
 // targets collinear with an edge (every centroid of a structured planar mesh)
 // are exact.
 #pragma once
-#include "jets.cuh"
+#include <math.h>
+#include "tri_index.cuh"
+#include "assemble_gen.cuh"
+#include "edge_gen.cuh"
 
 namespace efmm {
 
@@ -74,66 +82,81 @@ struct TriTables {
   double B[35];
 };
 
-// Line integrals over one edge A->B of int 1/r dl and int r dl as order-3 jets
-// in the target coordinates (x, y, h).  Returns false if the target lies on
-// the edge itself (singular; the reference returns 0 there, triahquad.f:1509).
-EFMM_HD bool edge_jets(double ax, double ay, double bx, double by, double x0, double y0,
-                       double h, Jet<3>& L1, Jet<3>& Lr, double& dsigned,
-                       double& omega_part) {
-  double ex = bx - ax, ey = by - ay;
-  double len = sqrt(ex * ex + ey * ey);
-  double tx = ex / len, ty = ey / len;
-  double mx = ty, my = -tx;  // outward normal of a CCW polygon
-  double u0 = (x0 - ax) * tx + (y0 - ay) * ty;
-  double v0 = (x0 - ax) * mx + (y0 - ay) * my;
-  dsigned = -v0;
-  Jet<3> u = Jet<3>::affine(u0, tx, ty, 0.0);
-  Jet<3> v = Jet<3>::affine(v0, mx, my, 0.0);
-  Jet<3> H = Jet<3>::affine(h, 0.0, 0.0, 1.0);
-  Jet<3> c2 = v * v + H * H;
-  double sm = -u0, sp = len - u0;  // endpoint coordinates relative to the foot
-  double c20 = v0 * v0 + h * h;
-
-  // signed solid-angle contribution of this edge (h != 0 only)
-  omega_part = 0.0;
-  if (h != 0.0) {
-    double d = dsigned, ah = fabs(h);
-    double th[2];
-    double ss[2] = {sm, sp};
-    for (int q = 0; q < 2; q++) {
-      double s = ss[q];
-      double R = sqrt(s * s + d * d + h * h);
-      double num = s * d * (s * s + d * d);
-      double den = (R + ah) * (d * d * R + ah * s * s);
-      th[q] = (den > 0.0) ? atan(num / den) : 0.0;
-    }
-    omega_part = th[1] - th[0];
-  }
-
-  bool same = (sm >= 0.0 && sp >= 0.0) || (sm <= 0.0 && sp <= 0.0);
-  if (same) {
-    double sg = (sm + sp >= 0.0) ? 1.0 : -1.0;
-    if ((sg > 0 ? sm : -sp) == 0.0 && c20 == 0.0) return false;  // at a vertex
-    // a = |s_-|, b = |s_+| as jets; b - a = sg*len exactly
-    Jet<3> a = sg * (Jet<3>::constant(0.0) - u);
-    Jet<3> b = a + sg * len;
-    Jet<3> a2 = a * a, b2 = b * b;
-    Jet<3> Ra = jsqrt(a2 + c2), Rb = jsqrt(b2 + c2);
-    Jet<3> sab = a + b;
-    // ln((b+Rb)/(a+Ra)) = log1p( sg*len*(1 + (a+b)/(Ra+Rb)) / (a+Ra) )
-    Jet<3> q = (sg * len) * ((sab * jinv(Ra + Rb) + 1.0) * jinv(a + Ra));
-    Jet<3> lr = jlog1p(q);
-    L1 = sg * lr;
-    // b Rb - a Ra = sg*len*(a+b)*(a^2+b^2+c^2)/(b Rb + a Ra)
-    Jet<3> diff = (sg * len) * (sab * (a2 + b2 + c2) * jinv(b * Rb + a * Ra));
-    Lr = 0.5 * (sg * diff + c2 * L1);
+// Edge-frame derivatives of the line integrals over one edge of length len
+// lying on the u axis from u = 0 (vertex A) to u = len (vertex B), for a target
+// at (u0, v0, h): L1[jidx(i,j,k)] = d_u^i d_v^j d_h^k int 1/r dl (|b| <= 2) and
+// Lr[...] = the same of int r dl (1 <= |b| <= 3).  Returns false when the
+// target lies on the closed edge (singular; the reference returns 0 there,
+// src/triahquad.f:1509).
+EFMM_HD bool edge_derivs(double len, double u0, double v0, double h, double* L1, double* Lr) {
+  const double sm = -u0, sp = len - u0;  // endpoint coordinates relative to the foot
+  const double c2 = v0 * v0 + h * h;
+  const double RA = sqrt(u0 * u0 + c2), RB = sqrt(sp * sp + c2);
+  // antiderivatives on [0, inf) shifted to vanish at infinity:
+  //   int (w^2+c^2)^-3/2 = -1/(R (w+R)),
+  //   int (w^2+c^2)^-5/2 = -(3w^2+4c^2) / (3 R^3 (w (2w^2+3c^2) + 2 R^3))
+  auto A3 = [c2](double w, double R) { return -1.0 / (R * (w + R)); };
+  auto A5 = [c2](double w, double R) {
+    return -(3.0 * w * w + 4.0 * c2) / (3.0 * R * R * R * (w * (2.0 * w * w + 3.0 * c2) + 2.0 * R * R * R));
+  };
+  double K1, K3, K5;
+  if ((sm >= 0.0 && sp >= 0.0) || (sm <= 0.0 && sp <= 0.0)) {
+    // both endpoints on one side of the foot: cancellation-free forms
+    const double sg = (sm + sp >= 0.0) ? 1.0 : -1.0;
+    const double a = sg * sm, b = sg * sp;  // |s_-|, |s_+|; b - a = sg*len
+    if (fmin(a, b) == 0.0 && c2 == 0.0) return false;  // at a vertex
+    // ln((b+RB)/(a+RA)) with (b+RB)-(a+RA) = sg*len*(1 + (a+b)/(RA+RB))
+    K1 = sg * log1p(sg * len * (1.0 + (a + b) / (RA + RB)) / (a + RA));
+    K3 = sg * (A3(b, RB) - A3(a, RA));
+    K5 = sg * (A5(b, RB) - A5(a, RA));
   } else {
-    if (c20 == 0.0) return false;  // on the edge
-    Jet<3> a = u;                                                   // a = -s_- = u
-    Jet<3> b = Jet<3>::constant(len) - u;                          // b = s_+
-    Jet<3> Ra = jsqrt(a * a + c2), Rb = jsqrt(b * b + c2);
-    L1 = jlog(b + Rb) + jlog(a + Ra) - jlog(c2);
-    Lr = 0.5 * (b * Rb + a * Ra + c2 * L1);
+    if (c2 == 0.0) return false;  // on the edge
+    const double a = u0, b = sp;   // both > 0, split at the foot
+    K1 = log((b + RB) * (a + RA) / c2);
+    K3 = A3(b, RB) + A3(a, RA) + 2.0 / c2;
+    K5 = A5(b, RB) + A5(a, RA) + 4.0 / (3.0 * c2 * c2);
+  }
+  const double iA = 1.0 / RA, iB = 1.0 / RB;
+  const double iA3 = iA * iA * iA, iB3 = iB * iB * iB;
+  const double ub = u0 - len;  // u-coordinate of the target relative to B
+  // int 1/r dl: F(c^2) part (d/dc^2: -K3/2, 3 K5/4) and endpoint part 1/r
+  {
+    const double F1 = -0.5 * K3, F2 = 0.75 * K5;
+    L1[jidx(0, 0, 0)] = K1;
+    L1[jidx(0, 1, 0)] = 2.0 * v0 * F1;
+    L1[jidx(0, 0, 1)] = 2.0 * h * F1;
+    L1[jidx(0, 2, 0)] = 2.0 * F1 + 4.0 * v0 * v0 * F2;
+    L1[jidx(0, 1, 1)] = 4.0 * v0 * h * F2;
+    L1[jidx(0, 0, 2)] = 2.0 * F1 + 4.0 * h * h * F2;
+    L1[jidx(1, 0, 0)] = iA - iB;
+    L1[jidx(2, 0, 0)] = -u0 * iA3 + ub * iB3;
+    L1[jidx(1, 1, 0)] = -v0 * (iA3 - iB3);
+    L1[jidx(1, 0, 1)] = -h * (iA3 - iB3);
+  }
+  // int r dl: F(c^2) part (K1/2, -K3/4, 3 K5/8) and endpoint part r
+  {
+    const double F1 = 0.5 * K1, F2 = -0.25 * K3, F3 = 0.375 * K5;
+    Lr[jidx(0, 1, 0)] = 2.0 * v0 * F1;
+    Lr[jidx(0, 0, 1)] = 2.0 * h * F1;
+    Lr[jidx(0, 2, 0)] = 2.0 * F1 + 4.0 * v0 * v0 * F2;
+    Lr[jidx(0, 1, 1)] = 4.0 * v0 * h * F2;
+    Lr[jidx(0, 0, 2)] = 2.0 * F1 + 4.0 * h * h * F2;
+    Lr[jidx(0, 3, 0)] = 12.0 * v0 * F2 + 8.0 * v0 * v0 * v0 * F3;
+    Lr[jidx(0, 2, 1)] = 4.0 * h * F2 + 8.0 * v0 * v0 * h * F3;
+    Lr[jidx(0, 1, 2)] = 4.0 * v0 * F2 + 8.0 * v0 * h * h * F3;
+    Lr[jidx(0, 0, 3)] = 12.0 * h * F2 + 8.0 * h * h * h * F3;
+    // RA - RB without cancellation: (RA^2 - RB^2) / (RA + RB)
+    Lr[jidx(1, 0, 0)] = len * (2.0 * u0 - len) / (RA + RB);
+    Lr[jidx(2, 0, 0)] = u0 * iA - ub * iB;
+    Lr[jidx(1, 1, 0)] = v0 * (iA - iB);
+    Lr[jidx(1, 0, 1)] = h * (iA - iB);
+    // second derivatives of r: d_ab r = delta_ab / r - P_a P_b / r^3
+    Lr[jidx(3, 0, 0)] = (iA - u0 * u0 * iA3) - (iB - ub * ub * iB3);
+    Lr[jidx(2, 1, 0)] = -v0 * (u0 * iA3 - ub * iB3);
+    Lr[jidx(2, 0, 1)] = -h * (u0 * iA3 - ub * iB3);
+    Lr[jidx(1, 2, 0)] = (iA - v0 * v0 * iA3) - (iB - v0 * v0 * iB3);
+    Lr[jidx(1, 1, 1)] = -v0 * h * (iA3 - iB3);
+    Lr[jidx(1, 0, 2)] = (iA - h * h * iA3) - (iB - h * h * iB3);
   }
   return true;
 }
@@ -150,18 +173,30 @@ EFMM_HD void tri_tables(const TriFrame& f, double x0, double y0, double h, bool 
 #pragma unroll 1
   for (int e = 0; e < 3; e++) {
     int e2 = (e == 2) ? 0 : e + 1;
-    double ax = vx[e], ay = vy[e], bx = vx[e2], by = vy[e2];
-    Jet<3> L1, Lr;
-    double ds, om;
-    if (!edge_jets(ax, ay, bx, by, x0, y0, h, L1, Lr, ds, om)) continue;
-    double ex = bx - ax, ey = by - ay;
-    double len = sqrt(ex * ex + ey * ey);
-    double m[2] = {ey / len, -ex / len};
-    phi += ds * L1.c[0];
-    omega += om;
-    sh += m[0] * L1.deriv(1, 0, 1) + m[1] * L1.deriv(0, 1, 1);
-    // in-plane entries: X(a) = sum_e m_d (-1)^(|a|-1) D^(a - e_d) L_e
-    tables_edge(L1.c, Lr.c, m[0], m[1], T.R, T.B);
+    const double ax = vx[e], ay = vy[e];
+    const double ex = vx[e2] - ax, ey = vy[e2] - ay;
+    const double len = sqrt(ex * ex + ey * ey);
+    const double tx = ex / len, ty = ey / len;  // unit tangent; outward normal (ty, -tx)
+    const double u0 = (x0 - ax) * tx + (y0 - ay) * ty;
+    const double v0 = (x0 - ax) * ty - (y0 - ay) * tx;
+    double L1[10], Lr[20];
+    if (!edge_derivs(len, u0, v0, h, L1, Lr)) continue;
+    // signed solid-angle contribution of this edge (h != 0 only)
+    if (h != 0.0) {
+      const double d = -v0, ah = fabs(h);
+      const double ss[2] = {-u0, len - u0};
+      double th[2];
+      for (int q = 0; q < 2; q++) {
+        const double s = ss[q];
+        const double R = sqrt(s * s + d * d + h * h);
+        const double num = s * d * (s * s + d * d);
+        const double den = (R + ah) * (d * d * R + ah * s * s);
+        th[q] = (den > 0.0) ? atan(num / den) : 0.0;
+      }
+      omega += th[1] - th[0];
+    }
+    phi += -v0 * L1[0];
+    edge_tables_gen(tx, ty, L1, Lr, T.R, T.B, sh);
   }
   if (h == 0.0) omega = 0.0;
   else omega = (h > 0.0) ? omega : -omega;

@@ -26,27 +26,25 @@ def _icosahedron():
 
 
 def icosphere(level, radius=1.0):
-    """Vertices (nv,3) and faces (nf,3) of the refined icosahedron."""
+    """Vertices (nv,3) and faces (nf,3) of the refined icosahedron (midpoints
+    pushed to the sphere; vectorised, shared edges deduplicated)."""
     v, f = _icosahedron()
-    verts = [tuple(x) for x in v]
     for _ in range(level):
-        cache = {}
-        nf = []
-
-        def mid(a, b):
-            key = (min(a, b), max(a, b))
-            if key not in cache:
-                p = (np.array(verts[a]) + np.array(verts[b])) / 2.0
-                p /= np.linalg.norm(p)
-                cache[key] = len(verts)
-                verts.append(tuple(p))
-            return cache[key]
-
-        for (a, b, c) in f:
-            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
-            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
-        f = np.array(nf, int)
-    return np.array(verts) * radius, f
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0].astype(np.int64) * (len(v) + 1) + e[:, 1]
+        uk, inv = np.unique(key, return_inverse=True)
+        a = uk // (len(v) + 1)
+        b = uk % (len(v) + 1)
+        mid = (v[a] + v[b]) / 2.0
+        mid /= np.linalg.norm(mid, axis=1)[:, None]
+        nf = len(f)
+        m = inv.reshape(3, nf).T + len(v)
+        ab, bc, ca = m[:, 0], m[:, 1], m[:, 2]
+        f = np.concatenate([np.stack([f[:, 0], ab, ca], 1), np.stack([f[:, 1], bc, ab], 1),
+                            np.stack([f[:, 2], ca, bc], 1), np.stack([ab, bc, ca], 1)])
+        v = np.vstack([v, mid])
+    return v * radius, f
 
 
 def triangles_from_mesh(verts, faces):

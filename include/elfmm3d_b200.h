@@ -88,6 +88,14 @@ int efmm_plan_evaluate_direct(efmm_plan *plan, double rlam, double rmu, const do
                               const double *sdl, double *u_src, double *e_src, double *u_tgt,
                               double *e_tgt);
 
+/* Number of this library's kernels launched so far in the process. */
+long long efmm_kernel_launches(void);
+
+/* CUDA events on the plan's stream: record slot (0..7); elapsed time in ms
+ * between two recorded slots (waits for the second). */
+int efmm_plan_record(efmm_plan *plan, int slot);
+float efmm_plan_elapsed(efmm_plan *plan, int a, int b);
+
 /* Per-stage device times (ms) of the last evaluate: total, prep, p2m, m2m,
  * m2l, l2l, l2t, near. */
 void efmm_plan_timings(const efmm_plan *plan, float *ms8);

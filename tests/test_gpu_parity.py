@@ -1,0 +1,151 @@
+"""GPU parity tests: the CUDA path against the oracle (golden fixtures and live
+oracle runs) and against exact identities.  All calls go through the C ABI."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel
+from elfmmlib3d_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+# reference tolerances per iprec (elfmm3dtria.f:102-124); strain loses ~1 digit
+TOL = {0: 0.5e-2, 1: 0.5e-3, 2: 0.5e-6, 3: 0.5e-9}
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def dev(a):
+    torch = _torch()
+    return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+
+
+@pytest.mark.parametrize("name", ["golden_sphere320.npz", "golden_fault100.npz"])
+def test_direct_matches_oracle_golden(gpu, name):
+    g = golden(name)
+    pt, st, ptt, stt = gpu.el3dtriadirecttarg(float(g["rlam"]), float(g["rmu"]), g["tri"], g["nrm"], g["cen"],
+                                              g["ssl"], g["sdl"], g["tgt"])
+    assert rel(pt, g["pt"]) < 1e-12 and rel(st, g["st"]) < 1e-12
+    assert rel(ptt, g["ptt"]) < 1e-12 and rel(stt, g["stt"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["golden_sphere320.npz", "golden_fault100.npz"])
+def test_fmm_matches_oracle_golden(gpu, name):
+    g = golden(name)
+    ier, pt, st, ptt, stt = gpu.elfmm3dtriatarg(2, float(g["rlam"]), float(g["rmu"]), g["tri"], g["nrm"],
+                                                g["cen"], g["ssl"], g["sdl"], g["tgt"])
+    assert ier == 0
+    assert rel(pt, g["pt"]) < TOL[2] and rel(ptt, g["ptt"]) < TOL[2]
+    assert rel(st, g["st"]) < 10 * TOL[2] and rel(stt, g["stt"]) < 10 * TOL[2]
+
+
+def test_direct_matches_live_oracle_single_layer_only(gpu, oracle):
+    tri, nrm, cen = G.sphere_triangles(1)
+    rng = np.random.default_rng(4)
+    ssl = rng.normal(size=cen.shape)
+    tg = G.box_targets(10, 2)
+    pt, st, ptt, stt = gpu.el3dtriadirecttarg(1.0, 1.0, tri, nrm, cen, ssl, None, tg)
+    o = oracle.direct(1.0, 1.0, tri, cen, ssl, None, tg)
+    assert rel(pt, o[0]) < 1e-12 and rel(st, o[1]) < 1e-12 and rel(ptt, o[2]) < 1e-12 and rel(stt, o[3]) < 1e-12
+
+
+@pytest.mark.parametrize("iprec", [0, 1, 2, 3])
+def test_fmm_within_iprec_tolerance(gpu, iprec):
+    tri, nrm, cen = G.sphere_triangles(3)
+    tg = G.box_targets(200, 9)
+    rng = np.random.default_rng(iprec)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    d = gpu.el3dtriadirecttarg(3.2, 2.3, tri, nrm, cen, ssl, sdl, tg)
+    ier, pt, st, ptt, stt = gpu.elfmm3dtriatarg(iprec, 3.2, 2.3, tri, nrm, cen, ssl, sdl, tg)
+    assert ier == 0
+    assert rel(pt, d[0]) < TOL[iprec] and rel(ptt, d[2]) < TOL[iprec]
+    assert rel(st, d[1]) < 10 * TOL[iprec] and rel(stt, d[3]) < 10 * TOL[iprec]
+
+
+def _tree_vs_oracle(gpu, oracle, src, tgt, iprec, iter_, mindlin):
+    P = gpu.Plan(0)
+    n = len(src)
+    P.set_geometry(dev(np.zeros((n, 3, 3))), dev(np.zeros((n, 3))), dev(src), dev(tgt) if len(tgt) else None,
+                   iprec=iprec, iter=iter_, mindlin=mindlin)
+    T = P.tree()
+    OT = oracle.Tree(src, tgt, P.info()["nbox"], mindlin)
+    assert T["boxes"].shape[0] == OT.nboxes
+    assert np.array_equal(T["boxes"][:, :17], OT.boxes[:, :17])
+    assert np.array_equal(T["iz"], OT.iz) and np.array_equal(T["iztarg"], OT.iztarg)
+    assert np.array_equal(T["laddr"], OT.laddr)
+    assert np.array_equal(T["center"], OT.center) and T["size"] == OT.size
+    for t in range(1, 6):
+        for b in range(OT.nboxes):
+            assert sorted(T["lists"][t][b].tolist()) == sorted(OT.lists[t][b].tolist()), (t, b)
+    for b in range(OT.nboxes):
+        assert T["lists"][5][b].tolist() == OT.lists[5][b].tolist()
+    P.close()
+
+
+@pytest.mark.parametrize("iprec", [1, 2])
+def test_tree_bit_exact_sphere(gpu, oracle, iprec):
+    tri, nrm, cen = G.sphere_triangles(4)
+    _tree_vs_oracle(gpu, oracle, cen, G.box_targets(1000, 7), iprec, False, False)
+
+
+def test_tree_bit_exact_mindlin_fault(gpu, oracle):
+    tri, nrm, cen, _ = G.planar_fault(100, 40)
+    _tree_vs_oracle(gpu, oracle, cen, np.zeros((0, 3)), 2, True, True)
+
+
+def test_tree_bit_exact_duplicate_and_clustered_points(gpu, oracle):
+    rng = np.random.default_rng(5)
+    src = np.vstack([rng.normal(size=(500, 3)) * 0.01, rng.normal(size=(500, 3)), np.zeros((30, 3))])
+    _tree_vs_oracle(gpu, oracle, src, rng.normal(size=(100, 3)), 1, False, False)
+
+
+def test_fmm_linearity(gpu):
+    tri, nrm, cen = G.sphere_triangles(3)
+    rng = np.random.default_rng(8)
+    a, b, c, d = (rng.normal(size=cen.shape) for _ in range(4))
+    r1 = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, a, b)
+    r2 = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, c, d)
+    r3 = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, a + 2 * c, b + 2 * d)
+    assert rel(r3[1], r1[1] + 2 * r2[1]) < 1e-12 and rel(r3[2], r1[2] + 2 * r2[2]) < 1e-12
+
+
+def test_elfmm3dtria_equals_targ_variant(gpu):
+    tri, nrm, cen = G.sphere_triangles(2)
+    rng = np.random.default_rng(9)
+    s1, s2 = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    ier, pt, st = gpu.elfmm3dtria(2, 1.0, 1.0, tri, nrm, cen, s1, s2)
+    ier2, pt2, st2, _, _ = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, s1, s2, G.box_targets(5, 1))
+    assert ier == 0 and ier2 == 0
+    assert rel(pt, pt2) < 1e-13 and rel(st, st2) < 1e-13
+
+
+def test_edge_cases(gpu):
+    tri = np.array([[[0, 0, 0], [1, 0, 0], [0, 1, 0]]], float)
+    nrm = np.array([[0, 0, 1.0]])
+    cen = tri.mean(1)
+    # one triangle, iprec 6 (direct) and iprec 2 give the same self value
+    ier, pt, st, _, _ = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, [[1, 2, 3]], [[0.5, -1, 2]])
+    pt6, st6, _, _ = gpu.el3dtriadirecttarg(1.0, 1.0, tri, nrm, cen, [[1, 2, 3]], [[0.5, -1, 2]])
+    assert ier == 0 and rel(pt, pt6) < 1e-14 and rel(st, st6) < 1e-14
+    # bad arguments -> ier 16
+    ier, *_ = gpu.elfmm3dtriatarg(9, 1.0, 1.0, tri, nrm, cen, [[1, 2, 3]])
+    assert ier == 16
+    # no targets, double layer only, iprec 6
+    ier, pt, st, ptt, stt = gpu.elfmm3dtriatarg(6, 1.0, 1.0, tri, nrm, cen, None, [[0.5, -1, 2]])
+    assert ier == 0 and ptt.shape == (0, 3)
+
+
+def test_rigid_body_identity_large(gpu):
+    """Size-independent property at the C3 sphere scale (81920 triangles, level 6):
+    constant jump b -> u = -4 pi b inside, 0 outside, -2 pi b on the surface."""
+    tri, nrm, cen = G.sphere_triangles(6)
+    b = np.array([0.3, -0.7, 0.5])
+    tg = np.vstack([G.shell_targets(500, 1, 0.1, 0.8), G.shell_targets(500, 2, 1.3, 3.0)])
+    ier, pt, st, ptt, stt = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, None, np.tile(b, (len(cen), 1)), tg)
+    assert ier == 0
+    scale = 4 * np.pi * np.linalg.norm(b)
+    assert np.abs(ptt[:500] + 4 * np.pi * b).max() < 1e-6 * scale
+    assert np.abs(ptt[500:]).max() < 1e-6 * scale
+    assert np.abs(pt + 2 * np.pi * b).max() < 1e-6 * scale
