@@ -139,10 +139,11 @@ def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     return nsample * n / dt, dt, cores, nsample
 
 
-# algorithmic FP64 operations per near-field (point, triangle) pair of the
-# analytic kernel, from the ncu instruction counts of k_near_leaf
-# (dadd + dmul + 2*dfma per pair; profiles/near_leaf_sphere5120.md)
-NEAR_FLOPS_PER_PAIR = float(os.environ.get("ELFMM_NEAR_FLOPS_PER_PAIR", "11700"))
+# FP64 operations per near-field (point, triangle) pair of the analytic
+# kernel: ncu thread-instruction counts of k_near_leaf on the sphere-5120 case,
+# (dadd + dmul + 2 dfma) / pairs = (0.984e9 + 1.749e9 + 2 * 3.029e9) / 3.194e6
+# (profiles/near_leaf_sphere5120.md)
+NEAR_FLOPS_PER_PAIR = 2752.0
 
 
 def run_ours(args, rank, world, local_rank):

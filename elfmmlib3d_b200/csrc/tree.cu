@@ -436,7 +436,11 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
   int lo = 0, hi = 1, nlev = 0;
   tr.laddr.clear();
   tr.laddr.push_back({0, 1});
-  for (int lev = 0; lev < 198; lev++) {
+  // The reference allows 198 levels but its integer box indices overflow past
+  // ~30; only more than nbox coincident points get that deep, so subdivision
+  // stops at MAX_LEVELS (boxes at that level stay leaves).
+  const int MAX_LEVELS = 50;
+  for (int lev = 0; lev < MAX_LEVELS; lev++) {
     int nl = hi - lo;
     split.resize(nl);
     cs.resize(8 * (size_t)nl);
