@@ -42,7 +42,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_create", "efmm_plan_destroy", "efmm_plan_set_geometry",
            "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings",
            "efmm_plan_info", "efmm_plan_tree_export", "efmm_kernel_launches", "efmm_plan_record",
-           "efmm_plan_elapsed"]
+           "efmm_plan_elapsed", "efmm_direct_noalloc"]
 
 
 class ElfmmError(RuntimeError):
@@ -80,6 +80,9 @@ def load():
     L.efmm_plan_record.argtypes = [_vp, ctypes.c_int]
     L.efmm_plan_elapsed.restype = ctypes.c_float
     L.efmm_plan_elapsed.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.efmm_direct_noalloc.restype = ctypes.c_int
+    L.efmm_direct_noalloc.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp,
+                                      ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
     L.efmm_plan_tree_export.restype = ctypes.c_int
     L.efmm_plan_tree_export.argtypes = [_vp, _ip, _ip, _ip, _ip, _dp, _ip, _ip, _llp]
     _lib = L

@@ -96,6 +96,25 @@ long long efmm_kernel_launches(void);
 int efmm_plan_record(efmm_plan *plan, int slot);
 float efmm_plan_elapsed(efmm_plan *plan, int a, int b);
 
+/* Direct sum without device allocation.  No counterpart in the reference: it
+ * is for callers that cannot allocate device memory when they need the
+ * result (a memory pool that already holds the free device memory, or a
+ * latency-bound loop that cannot afford an allocation's synchronisation).
+ * Same result as el3dtriadirecttarg_ for device-resident inputs (user order):
+ * tri (n,3,3), src (n,3), ssl/sdl (n,3; NULL disables a layer), tgt (nt,3);
+ * outputs u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3), NULL
+ * disables one.  Intermediates live in fixed file-scope device arrays
+ * (about 11 MB, present on every GPU that loads the library until exit):
+ * at most 32768 triangles and 65536 evaluation points (n + nt) per call;
+ * larger sizes return 16 with a message on stderr.  Enqueues on `stream`
+ * (a cudaStream_t, NULL = legacy default stream) and returns; the first call
+ * on a device looks up the scratch addresses for that device and should come
+ * before any stream capture.  Calls that overlap on the GPU share the scratch
+ * and race. */
+int efmm_direct_noalloc(double rlam, double rmu, int n, const double *tri, const double *src,
+                        const double *ssl, const double *sdl, int nt, const double *tgt,
+                        double *u_src, double *e_src, double *u_tgt, double *e_tgt, void *stream);
+
 /* Per-stage device times (ms) of the last evaluate: total, prep, p2m, m2m,
  * m2l, l2l, l2t, near. */
 void efmm_plan_timings(const efmm_plan *plan, float *ms8);
