@@ -10,6 +10,8 @@ routines (same names, argument meaning, array layouts and ``ier`` codes):
         -> src/elfmm3dtria.f:162
     el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, ...)
         -> src/elfmm3dtria.f:1483
+    elfmm3dtriatargiter(iprec, rlam, rmu, ..., icomp_type=, wsave=)
+        -> src/elfmm3dtria_iter_1.f:160
 
 Arrays are numpy, shaped in C order as the transpose of the Fortran shapes:
 ``triangle`` (n,3,3) [triangle][vertex][xyz], ``sigma`` (n,3), ``ptfrc`` (n,3),
@@ -23,7 +25,8 @@ import os
 
 import numpy as np
 
-__all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "Plan", "load",
+__all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "elfmm3dtriatargiter",
+           "elfmm3dtriaiter", "iter_release", "iter_stored_bytes", "Plan", "load",
            "library_path", "device_count", "ElfmmError"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -42,7 +45,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_create", "efmm_plan_destroy", "efmm_plan_set_geometry",
            "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings",
            "efmm_plan_info", "efmm_plan_tree_export", "efmm_kernel_launches", "efmm_plan_record",
-           "efmm_plan_elapsed", "efmm_direct_noalloc"]
+           "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
+           "efmm_iter_release", "efmm_iter_stored_bytes"]
 
 
 class ElfmmError(RuntimeError):
@@ -83,6 +87,10 @@ def load():
     L.efmm_direct_noalloc.restype = ctypes.c_int
     L.efmm_direct_noalloc.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp,
                                       ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.efmm_iter_release.restype = ctypes.c_int
+    L.efmm_iter_release.argtypes = [_dp, ctypes.c_int]
+    L.efmm_iter_stored_bytes.restype = ctypes.c_longlong
+    L.efmm_iter_stored_bytes.argtypes = [_dp, ctypes.c_int]
     L.efmm_plan_tree_export.restype = ctypes.c_int
     L.efmm_plan_tree_export.argtypes = [_vp, _ip, _ip, _ip, _ip, _dp, _ip, _ip, _llp]
     _lib = L
@@ -182,6 +190,66 @@ def el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigm
                           _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp), _byref_i(ifstraintarg),
                           stt.ctypes.data_as(_dp))
     return pt, st, ptt[:m], stt[:m]
+
+
+ITER_LUSED = 8  # words of wsave the ITER handle occupies
+
+
+def elfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                        target=None, icomp_type=1, wsave=None, ifptfrc=1, ifstrain=1, ifptfrctarg=1,
+                        ifstraintarg=1):
+    """Iterative-solver variant (src/elfmm3dtria_iter_1.f:160): icomp_type 2
+    evaluates and stores the near-field interactions, 3 reuses them with new
+    densities on the same geometry, 1 evaluates without storage, 4 builds the
+    tree only, 5 stores and evaluates the near field alone.  ``wsave`` is a
+    float64 array (at least ``ITER_LUSED`` words) that receives / supplies the
+    handle of the device-resident store.
+
+    Returns (ier, lused, ptfrc, strain, ptfrctarg, straintarg).
+    """
+    L = load()
+    _need_gpu()
+    tri, nrm, src, ssl, sdl, n = _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    if wsave is None:
+        wsave = np.zeros(ITER_LUSED)
+    if wsave.dtype != np.float64 or not wsave.flags.c_contiguous:
+        raise ValueError("wsave must be a contiguous float64 array")
+    pt = np.zeros((n, 3))
+    st = np.zeros((n, 3, 3))
+    ptt = np.zeros((max(m, 1), 3))
+    stt = np.zeros((max(m, 1), 3, 3))
+    ier = ctypes.c_int(0)
+    lused = ctypes.c_int(0)
+    L.elfmm3dtriatargiter_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu),
+                           tri.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp), _byref_i(n),
+                           src.ctypes.data_as(_dp), _byref_i(sigma_sl is not None), ssl.ctypes.data_as(_dp),
+                           _byref_i(sigma_dl is not None), sdl.ctypes.data_as(_dp), _byref_i(ifptfrc),
+                           pt.ctypes.data_as(_dp), _byref_i(ifstrain), st.ctypes.data_as(_dp), _byref_i(m),
+                           tg.ctypes.data_as(_dp), _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp),
+                           _byref_i(ifstraintarg), stt.ctypes.data_as(_dp), _byref_i(icomp_type),
+                           wsave.ctypes.data_as(_dp), _byref_i(wsave.size), ctypes.byref(lused))
+    return ier.value, lused.value, pt, st, ptt[:m], stt[:m]
+
+
+def elfmm3dtriaiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                    icomp_type=1, wsave=None, ifptfrc=1, ifstrain=1):
+    """On-surface ITER variant (src/elfmm3dtria_iter_1.f:43).
+    Returns (ier, lused, ptfrc, strain)."""
+    ier, lused, pt, st, _, _ = elfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl,
+                                                   sigma_dl, None, icomp_type, wsave, ifptfrc, ifstrain, 0, 0)
+    return ier, lused, pt, st
+
+
+def iter_release(wsave):
+    """Free the device store an ITER handle names; returns ier (512 if none)."""
+    return int(load().efmm_iter_release(wsave.ctypes.data_as(_dp), int(wsave.size)))
+
+
+def iter_stored_bytes(wsave):
+    """Device bytes held by the store an ITER handle names (-1 if none)."""
+    return int(load().efmm_iter_stored_bytes(wsave.ctypes.data_as(_dp), int(wsave.size)))
 
 
 class Plan:

@@ -220,7 +220,8 @@ void down(T* h, const DevBuf<T>& b, size_t n, cudaStream_t st) {
 int host_call(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n,
               const double* src, int ifsingle, const double* ssl, int ifdouble, const double* sdl,
               int ifptfrc, double* ptfrc, int ifstrain, double* strain, int nt, const double* tgt,
-              int ifptfrctarg, double* ptfrctarg, int ifstraintarg, double* straintarg, bool direct) {
+              int ifptfrctarg, double* ptfrctarg, int ifstraintarg, double* straintarg, bool direct,
+              bool iter = false) {
   if (n < 1 || nt < 0) return IER_BADARG;
   std::lock_guard<std::mutex> lk(g_mu);
   efmm_plan* p = shared_plan();
@@ -241,7 +242,7 @@ int host_call(int iprec, double rlam, double rmu, const double* tri, const doubl
     B.ut.resize(3 * (size_t)std::max(nt, 1));
     B.et.resize(9 * (size_t)std::max(nt, 1));
     int ier = p->plan->set_geometry(n, B.tri.get(), B.nrm.get(), B.src.get(), nt, B.tgt.get(),
-                                    iprec, false, false);
+                                    iprec, iter, false);
     if (ier) return ier;
     bool src_out = ifptfrc || ifstrain, tgt_out = nt > 0 && (ifptfrctarg || ifstraintarg);
     double* du = src_out ? B.u.get() : nullptr;
@@ -300,4 +301,213 @@ extern "C" void el3dtriadirecttarg_(const double* rlam, const double* rmu, const
                       *ifdouble, sigma_dl, *ifptfrc, ptfrc, *ifstrain, strain, *ntarget, target,
                       *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, true);
   if (ier) fprintf(stderr, "el3dtriadirecttarg: error %d\n", ier);
+}
+
+// ---------------------------------------------------------------------------
+// ITER entry point (src/elfmm3dtria_iter_1.f:160-165).  The reference keeps
+// the near-field operator in the caller's wsave array.  Here the operator
+// stays in device memory owned by the library, and wsave holds an 8-word
+// handle naming it:
+//   [0] magic  [1] layout version  [2] store id  [3] nparts  [4] ntargs
+//   [5] iprec  [6] geometry checksum  [7] layer/output flags
+// At most ITER_SLOTS stores are live; a store call beyond that evicts the
+// least recently used one, whose handle then fails validation (ier 512).
+// ---------------------------------------------------------------------------
+namespace {
+constexpr double ITER_MAGIC = 1162626637.0;  // "ELFM"
+constexpr double ITER_VERSION = 1.0;
+constexpr int ITER_LUSED = 8;
+constexpr int ITER_SLOTS = 4;
+
+struct IterSlot {
+  efmm_plan* p = nullptr;
+  HostCall bufs;
+  long long id = 0;
+  long long last_use = 0;
+  int n = 0, nt = 0, iprec = 0;
+  double checksum = 0;
+  int flags = 0;
+};
+std::vector<IterSlot*> g_iter;
+long long g_iter_next_id = 1, g_iter_clock = 0;
+
+// 64-bit FNV-1a over the geometry bytes, kept to 53 bits so it is exact in a double
+double geometry_checksum(const double* tri, const double* nrm, const double* src, int n,
+                         const double* tgt, int nt) {
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](const double* a, size_t cnt) {
+    const unsigned char* b = reinterpret_cast<const unsigned char*>(a);
+    for (size_t i = 0; i < cnt * sizeof(double); i++) {
+      h ^= b[i];
+      h *= 1099511628211ull;
+    }
+  };
+  mix(tri, 9 * (size_t)n);
+  mix(nrm, 3 * (size_t)n);
+  mix(src, 3 * (size_t)n);
+  if (nt > 0) mix(tgt, 3 * (size_t)nt);
+  return (double)(h >> 11);
+}
+
+IterSlot* iter_find(const double* wsave, int lwsave) {
+  if (!wsave || lwsave < ITER_LUSED || wsave[0] != ITER_MAGIC || wsave[1] != ITER_VERSION) return nullptr;
+  for (IterSlot* s : g_iter)
+    if ((double)s->id == wsave[2]) return s;
+  return nullptr;
+}
+
+IterSlot* iter_acquire(IterSlot* reuse) {
+  if (reuse) return reuse;
+  if ((int)g_iter.size() < ITER_SLOTS) {
+    IterSlot* s = new IterSlot();
+    s->p = efmm_plan_create(env_device());
+    if (!s->p) {
+      delete s;
+      return nullptr;
+    }
+    g_iter.push_back(s);
+    return s;
+  }
+  IterSlot* lru = g_iter[0];
+  for (IterSlot* s : g_iter)
+    if (s->last_use < lru->last_use) lru = s;
+  return lru;
+}
+
+int iter_flags(int ifsingle, int ifdouble, int ifptfrc, int ifstrain, int nt, int ifptfrctarg,
+               int ifstraintarg) {
+  return (ifsingle ? 1 : 0) | (ifdouble ? 2 : 0) | (ifptfrc ? 4 : 0) | (ifstrain ? 8 : 0) |
+         ((nt > 0 && ifptfrctarg) ? 16 : 0) | ((nt > 0 && ifstraintarg) ? 32 : 0);
+}
+
+int iter_call(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n,
+              const double* src, int ifsingle, const double* ssl, int ifdouble, const double* sdl,
+              int ifptfrc, double* ptfrc, int ifstrain, double* strain, int nt, const double* tgt,
+              int ifptfrctarg, double* ptfrctarg, int ifstraintarg, double* straintarg, int icomp,
+              double* wsave, int lwsave, int* lused) {
+  *lused = ITER_LUSED;
+  if (n < 1 || nt < 0) return IER_BADARG;
+  if (icomp == 0) return IER_OK;  // the reference evaluates nothing for icomp_type 0
+  if (icomp < 1 || icomp > 5) return IER_BADARG;
+  // a work array too short for the handle: plain evaluation, as the reference
+  // does when wsave cannot hold the stored interactions
+  bool storing = (icomp == 2 || icomp == 3 || icomp == 5) && lwsave >= ITER_LUSED && wsave;
+  if (icomp == 1 || ((icomp == 2 || icomp == 3) && !storing))
+    return host_call(iprec, rlam, rmu, tri, nrm, n, src, ifsingle, ssl, ifdouble, sdl, ifptfrc, ptfrc,
+                     ifstrain, strain, nt, tgt, ifptfrctarg, ptfrctarg, ifstraintarg, straintarg, false,
+                     true);
+  if (icomp == 5 && !storing) return IER_BADARG;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int flags = iter_flags(ifsingle, ifdouble, ifptfrc, ifstrain, nt, ifptfrctarg, ifstraintarg);
+  IterSlot* S = iter_find(wsave, lwsave);
+  double cks = geometry_checksum(tri, nrm, src, n, tgt, nt);
+  if (icomp == 3) {
+    if (!S || S->n != n || S->nt != nt || S->iprec != iprec || S->checksum != cks || S->flags != flags ||
+        wsave[3] != n || wsave[4] != nt || wsave[5] != iprec || wsave[6] != cks || wsave[7] != flags)
+      return IER_HANDLE;
+  } else {
+    S = iter_acquire(S);
+    if (!S) return IER_NODEVICE;
+    S->id = 0;  // invalid until this store completes
+  }
+  S->last_use = ++g_iter_clock;
+  efmm_plan* p = S->p;
+  try {
+    cudaSetDevice(p->device);
+    HostCall& B = S->bufs;
+    cudaStream_t st = p->stream;
+    if (icomp != 3) {
+      up(B.tri, tri, 9 * (size_t)n, st);
+      up(B.nrm, nrm, 3 * (size_t)n, st);
+      up(B.src, src, 3 * (size_t)n, st);
+      up(B.tgt, tgt, 3 * (size_t)nt, st);
+      int ier = p->plan->set_geometry(n, B.tri.get(), B.nrm.get(), B.src.get(), nt, B.tgt.get(), iprec,
+                                      true, false);
+      if (ier) return ier;
+      if (icomp == 4) return IER_OK;  // tree only
+    }
+    if (ifsingle) up(B.ssl, ssl, 3 * (size_t)n, st);
+    if (ifdouble) up(B.sdl, sdl, 3 * (size_t)n, st);
+    B.u.resize(3 * (size_t)n);
+    B.e.resize(9 * (size_t)n);
+    B.ut.resize(3 * (size_t)std::max(nt, 1));
+    B.et.resize(9 * (size_t)std::max(nt, 1));
+    bool src_out = ifptfrc || ifstrain, tgt_out = nt > 0 && (ifptfrctarg || ifstraintarg);
+    int ier = p->plan->evaluate(rlam, rmu, ifsingle ? B.ssl.get() : nullptr, ifdouble ? B.sdl.get() : nullptr,
+                                src_out ? B.u.get() : nullptr, ifstrain ? B.e.get() : nullptr,
+                                tgt_out ? B.ut.get() : nullptr, (nt > 0 && ifstraintarg) ? B.et.get() : nullptr,
+                                icomp == 3 ? 2 : 1, icomp != 5);
+    if (ier) return ier;
+    if (ifptfrc) down(ptfrc, B.u, 3 * (size_t)n, st);
+    if (ifstrain) down(strain, B.e, 9 * (size_t)n, st);
+    if (nt > 0 && ifptfrctarg) down(ptfrctarg, B.ut, 3 * (size_t)nt, st);
+    if (nt > 0 && ifstraintarg) down(straintarg, B.et, 9 * (size_t)nt, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (icomp != 3) {
+      S->id = g_iter_next_id++;
+      S->n = n;
+      S->nt = nt;
+      S->iprec = iprec;
+      S->checksum = cks;
+      S->flags = flags;
+      wsave[0] = ITER_MAGIC;
+      wsave[1] = ITER_VERSION;
+      wsave[2] = (double)S->id;
+      wsave[3] = n;
+      wsave[4] = nt;
+      wsave[5] = iprec;
+      wsave[6] = cks;
+      wsave[7] = flags;
+    }
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+}  // namespace
+
+extern "C" void elfmm3dtriatargiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
+                                     const double* triangle, const double* trinorm, const int* nparts,
+                                     const double* source, const int* ifsingle, const double* sigma_sl,
+                                     const int* ifdouble, const double* sigma_dl, const int* ifptfrc,
+                                     double* ptfrc, const int* ifstrain, double* strain,
+                                     const int* ntargs, const double* target, const int* ifptfrctarg,
+                                     double* ptfrctarg, const int* ifstraintarg, double* straintarg,
+                                     const int* icomp_type, double* wsave, const int* lwsave, int* lused) {
+  *ier = iter_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
+                   sigma_dl, *ifptfrc, ptfrc, *ifstrain, strain, *ntargs, target, *ifptfrctarg, ptfrctarg,
+                   *ifstraintarg, straintarg, *icomp_type, wsave, *lwsave, lused);
+}
+
+extern "C" void elfmm3dtriaiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
+                                 const double* triangle, const double* trinorm, const int* nparts,
+                                 const double* source, const int* ifsingle, const double* sigma_sl,
+                                 const int* ifdouble, const double* sigma_dl, const int* ifptfrc,
+                                 double* ptfrc, const int* ifstrain, double* strain, const int* icomp_type,
+                                 double* wsave, const int* lwsave, int* lused) {
+  *ier = iter_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
+                   sigma_dl, *ifptfrc, ptfrc, *ifstrain, strain, 0, nullptr, 0, nullptr, 0, nullptr,
+                   *icomp_type, wsave, *lwsave, lused);
+}
+
+extern "C" int efmm_iter_release(const double* wsave, int lwsave) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  IterSlot* S = iter_find(wsave, lwsave);
+  if (!S) return IER_HANDLE;
+  for (size_t i = 0; i < g_iter.size(); i++)
+    if (g_iter[i] == S) g_iter.erase(g_iter.begin() + i);
+  cudaSetDevice(S->p->device);
+  efmm_plan* p = S->p;
+  delete S;  // frees the host-call buffers on the plan's device
+  efmm_plan_destroy(p);
+  return IER_OK;
+}
+
+extern "C" long long efmm_iter_stored_bytes(const double* wsave, int lwsave) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  IterSlot* S = iter_find(wsave, lwsave);
+  if (!S) return -1;
+  return 8 * S->p->plan->stored_doubles();
 }

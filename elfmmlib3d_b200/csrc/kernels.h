@@ -19,6 +19,10 @@ struct NearArgs {
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out);
 void launch_near_leaf(cudaStream_t st, const NearArgs& a);
+void launch_near_store(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K,
+                       int dodisp, double* store);
+void launch_near_replay(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K,
+                        int dodisp, const double* ssl, const double* sdl, const double* store);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
                        int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,

@@ -184,6 +184,112 @@ k_direct_all(int ntri, const TriRec* __restrict__ trir, int nsrc, const double* 
   }
 }
 
+// ITER mode, first call: compute and store the unit-density response blocks
+// of every near (point, triangle) pair of each leaf.  Layout per leaf:
+// [evaluation point][near triangle][K doubles], at base[leaf]; near triangles
+// are the concatenated source ranges of the leaf's paired boxes.
+__global__ void __launch_bounds__(NF_WARPS * 32, NF_MINB)
+k_near_store(const NearArgs a, const long long* __restrict__ base, const int* __restrict__ ntri,
+             int K, int dodisp, double* __restrict__ store) {
+  __shared__ TriRec tile[NF_TILE];
+  int leaf = a.leaves[blockIdx.x];
+  int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  int t0 = a.box_tgt_start[leaf], tn = a.do_tgt ? a.box_tgt_count[leaf] : 0;
+  int nep = sn + tn;
+  int nt = ntri[blockIdx.x];
+  double* out = store + base[blockIdx.x];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int pos = 0;  // running index of the leaf's near triangles
+  for (int b = a.nb_start[blockIdx.x]; b < a.nb_start[blockIdx.x + 1]; b++) {
+    int sb = a.nb_items[b];
+    int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+    for (int k0 = 0; k0 < trn; k0 += NF_TILE) {
+      int cnt = min(NF_TILE, trn - k0);
+      __syncthreads();
+      stage_tile(tile, a.trir + tr0 + k0, cnt);
+      __syncthreads();
+      for (int e = warp; e < nep; e += NF_WARPS) {
+        bool is_src = e < sn;
+        int pidx = is_src ? s0 + e : t0 + (e - sn);
+        const double* P = is_src ? a.src_pts + 3 * (size_t)pidx : a.tgt_pts + 3 * (size_t)pidx;
+        double X[3] = {P[0], P[1], P[2]};
+        bool dostrain = is_src ? a.dostrain_src : a.dostrain_tgt;
+        for (int k = lane; k < cnt; k += 32) {
+          int tidx = tr0 + k0 + k;
+          bool self = is_src && (tidx == pidx);
+          double blk[54];
+          pair_blocks(tile[k].f, a.dosl, a.dodl, dodisp, dostrain, X, self, a.rlam, a.rmu, blk);
+          double* o = out + ((size_t)e * nt + (pos + k0 + k)) * K;
+          for (int q = 0; q < K; q++) o[q] = blk[q];
+        }
+      }
+    }
+    pos += trn;
+  }
+}
+
+// ITER mode, later calls: replay the stored blocks against new densities
+// (tree order, global frame) and ADD to the outputs.  One CTA per leaf, one
+// warp per evaluation point, lanes over the point's near triangles so each
+// warp reads one contiguous row of blocks.
+__global__ void __launch_bounds__(256)
+k_near_replay(const NearArgs a, const long long* __restrict__ base, const int* __restrict__ ntri,
+              int K, int dodisp, const double* __restrict__ ssl, const double* __restrict__ sdl,
+              const double* __restrict__ store) {
+  int leaf = a.leaves[blockIdx.x];
+  int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  int t0 = a.box_tgt_start[leaf], tn = a.do_tgt ? a.box_tgt_count[leaf] : 0;
+  int nep = sn + tn;
+  int nt = ntri[blockIdx.x];
+  const double* blocks = store + base[blockIdx.x];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  for (int e = warp; e < nep; e += nw) {
+    bool is_src = e < sn;
+    int pidx = is_src ? s0 + e : t0 + (e - sn);
+    bool dostrain = is_src ? a.dostrain_src : a.dostrain_tgt;
+    double u[3] = {0, 0, 0}, ee[6] = {0, 0, 0, 0, 0, 0};
+    const double* row = blocks + (size_t)e * nt * K;
+    int pos = 0;
+    for (int b = a.nb_start[blockIdx.x]; b < a.nb_start[blockIdx.x + 1]; b++) {
+      int sb = a.nb_items[b];
+      int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+      for (int k = lane; k < trn; k += 32) {
+        int t = tr0 + k;
+        const double* B = row + (size_t)(pos + k) * K;
+        int w = 0;
+        for (int layer = 0; layer < 2; layer++) {
+          if ((layer == 0 && !a.dosl) || (layer == 1 && !a.dodl)) continue;
+          const double* sg = (layer == 0 ? ssl : sdl) + 3 * (size_t)t;
+          double sv[3] = {sg[0], sg[1], sg[2]};
+          for (int c = 0; c < 3; c++) {
+            if (dodisp) {
+              u[0] += B[w] * sv[c]; u[1] += B[w + 1] * sv[c]; u[2] += B[w + 2] * sv[c];
+              w += 3;
+            }
+            if (dostrain) {
+              for (int q = 0; q < 6; q++) ee[q] += B[w + q] * sv[c];
+              w += 6;
+            }
+          }
+        }
+      }
+      pos += trn;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) u[c] = warp_sum(u[c]);
+#pragma unroll
+    for (int c = 0; c < 6; c++) ee[c] = warp_sum(ee[c]);
+    if (lane == 0) {
+      double* U = is_src ? a.u_src : a.u_tgt;
+      double* E = is_src ? a.e_src : a.e_tgt;
+      if (dodisp)
+        for (int c = 0; c < 3; c++) U[3 * (size_t)pidx + c] += u[c];
+      if (dostrain)
+        for (int c = 0; c < 6; c++) E[6 * (size_t)pidx + c] += ee[c];
+    }
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out) {
@@ -198,6 +304,18 @@ void launch_near_leaf(cudaStream_t st, const NearArgs& a) {
       a.box_tgt_start, a.box_tgt_count, a.trir, a.src_pts, a.tgt_pts, a.dosl, a.dodl,
       a.dostrain_src, a.dostrain_tgt, a.do_src, a.do_tgt, a.rlam, a.rmu, a.u_src, a.e_src,
       a.u_tgt, a.e_tgt); count_launch();
+}
+
+void launch_near_store(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K,
+                       int dodisp, double* store) {
+  if (a.nleaf <= 0) return;
+  k_near_store<<<a.nleaf, NF_WARPS * 32, 0, st>>>(a, base, ntri, K, dodisp, store); count_launch();
+}
+
+void launch_near_replay(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K,
+                        int dodisp, const double* ssl, const double* sdl, const double* store) {
+  if (a.nleaf <= 0) return;
+  k_near_replay<<<a.nleaf, 256, 0, st>>>(a, base, ntri, K, dodisp, ssl, sdl, store); count_launch();
 }
 
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,

@@ -250,6 +250,18 @@ void Plan::build_worklists() {
     nleaves.push_back(b);
     nstart.push_back((int)nitems.size());
   }
+  near_sc_h_.clear();
+  near_tc_h_.clear();
+  near_ntri_h_.clear();
+  for (size_t i = 0; i < nleaves.size(); i++) {
+    int b = nleaves[i], nt = 0;
+    for (int q = nstart[i]; q < nstart[i + 1]; q++) nt += scount[nitems[q]];
+    near_sc_h_.push_back(scount[b]);
+    near_tc_h_.push_back(tcount[b]);
+    near_ntri_h_.push_back(nt);
+  }
+  h2d(near_ntri_, near_ntri_h_, st_);
+  store_valid_ = false;
   near_pairs_ = 0;
   {
     // count point pairs for the throughput model
@@ -371,11 +383,37 @@ void Plan::build_worklists() {
 }
 
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
-                   double* d_e_src, double* d_u_tgt, double* d_e_tgt) {
+                   double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode, bool do_far) {
   int n = n_, nt = nt_;
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
   int ds_src = d_e_src ? 1 : 0, ds_tgt = d_e_tgt ? 1 : 0;
+  // stored operator layout: layers, evaluation point sets, strain rows
+  const int flags = dosl | (dodl << 1) | (do_src << 2) | (do_tgt << 3) | ((ds_src || ds_tgt) << 4);
+  if (mode == 2 && (!store_valid_ || flags != store_flags_ || rlam != store_lam_ || rmu != store_mu_))
+    return IER_HANDLE;
+  if (mode == 1) {
+    // size and place the blocks: K doubles per (point, triangle) pair
+    const int nl = dosl + dodl, dstr = (ds_src || ds_tgt) ? 1 : 0;
+    const int K = nl * 3 * (3 + 6 * dstr);
+    std::vector<long long> base(near_ntri_h_.size());
+    long long tot = 0;
+    for (size_t i = 0; i < near_ntri_h_.size(); i++) {
+      base[i] = tot;
+      long long nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+      tot += nep * near_ntri_h_[i] * K;
+    }
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    if ((double)tot * 8.0 > 0.9 * (double)freeb + (double)store_.cap * 8.0) return IER_ALLOC;
+    store_.resize((size_t)tot);
+    h2d(near_base_, base, st_);
+    store_K_ = K;
+    store_flags_ = flags;
+    store_lam_ = rlam;
+    store_mu_ = rmu;
+    store_valid_ = false;
+  }
   long long launch0 = launches_total();
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
   ssl_s_.resize(3 * (size_t)n);
@@ -393,7 +431,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   double c1 = (rlam + rmu) / (rlam + 2 * rmu), c2 = rmu / (rlam + 2 * rmu);
   EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
   int D = 2 * ncoef(p_);
-  if (far_ && (do_src || do_tgt)) {
+  if (far_ && do_far && (do_src || do_tgt)) {
     mpole_.zero(st_);
     local_.zero(st_);
     P2MArgs pa;
@@ -441,7 +479,8 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
   // near field
   trir_.resize(n);
-  launch_tri_prep(st_, n, tri_s_.get(), nullptr, ssl_s_.get(), sdl_s_.get(), dosl, dodl, trir_.get());
+  if (mode != 2)  // the stored operator replaces the triangle records
+    launch_tri_prep(st_, n, tri_s_.get(), nullptr, ssl_s_.get(), sdl_s_.get(), dosl, dodl, trir_.get());
   NearArgs na;
   na.nleaf = nnear_;
   na.leaves = near_leaves_.get(); na.nb_start = near_start_.get(); na.nb_items = near_items_.get();
@@ -453,7 +492,22 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   na.do_src = do_src; na.do_tgt = do_tgt;
   na.rlam = rlam; na.rmu = rmu;
   na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
-  launch_near_leaf(st_, na);
+  if (mode == 0) {
+    launch_near_leaf(st_, na);
+  } else {
+    // stored operator rows carry displacement and (if any output wants it) strain
+    NearArgs sa = na;
+    sa.dostrain_src = sa.dostrain_tgt = (store_flags_ >> 4) & 1;
+    if (mode == 1) {
+      launch_near_store(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, 1, store_.get());
+      store_valid_ = true;
+    }
+    NearArgs ra = na;  // outputs as requested by this call
+    ra.dostrain_src = sa.dostrain_src;
+    ra.dostrain_tgt = sa.dostrain_tgt;
+    launch_near_replay(st_, ra, near_base_.get(), near_ntri_.get(), store_K_, 1, ssl_s_.get(), sdl_s_.get(),
+                       store_.get());
+  }
   EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
   if (do_src) {
     k_scatter_out<<<(n + 255) / 256, 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src, d_e_src); count_launch();

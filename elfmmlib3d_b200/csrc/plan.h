@@ -38,8 +38,14 @@ class Plan {
                    const double* d_tgt, int iprec, bool iter, bool mindlin);
   // densities in user order (device); outputs in user order (device):
   // u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3); null pointers disable them.
+  // mode 0: analytic near field; 1: compute and store the near-field
+  // operator (ITER first call), then apply it; 2: apply the stored operator
+  // (ITER later calls; same layers/outputs/Lame constants as the store,
+  // else IER_HANDLE).  do_far = false skips the far field (near part only).
   int evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
-               double* d_e_src, double* d_u_tgt, double* d_e_tgt);
+               double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode = 0, bool do_far = true);
+  long long stored_doubles() const { return store_valid_ ? (long long)store_.size() : 0; }
+  bool store_valid() const { return store_valid_; }
   // all-pairs direct sum on the same geometry (no tree needed)
   int evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,
                       double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt);
@@ -69,6 +75,13 @@ class Plan {
   DevBuf<double> src_u_, tgt_u_;
   DevBuf<int> p2m_leaves_, l2t_leaves_, near_leaves_, near_start_, near_items_;
   int np2m_ = 0, nl2t_ = 0, nnear_ = 0;
+  std::vector<int> near_sc_h_, near_tc_h_, near_ntri_h_;  // per near leaf
+  DevBuf<int> near_ntri_;
+  DevBuf<long long> near_base_;
+  DevBuf<double> store_;
+  bool store_valid_ = false;
+  int store_flags_ = 0, store_K_ = 0;
+  double store_lam_ = 0, store_mu_ = 0;
   long long near_pairs_ = 0;
   DevBuf<TransPair> m2m_pairs_, m2l_pairs_, l2l_pairs_;
   DevBuf<TransTask> m2m_tasks_, m2l_tasks_, l2l_tasks_;

@@ -211,31 +211,16 @@ EFMM_HD void tri_tables(const TriFrame& f, double x0, double y0, double h, bool 
   T.B[jidx(0, 0, 4)] = 3.0 * r002 + h * sh;
 }
 
-// One (triangle, target) interaction in global coordinates.  ssl/sdl are the
-// single/double layer densities already rotated into the triangle frame.
-// The local-frame assembly (assemble_gen, generated) follows the single layer
-// 2mu*u_i = sum_k s_k (2 d_ik R - c1 B_ik) (elfmm3dtria.f:1762-1987) and the
-// traction-kernel contraction with the frame normal for the double layer
-// (elfmm3dtria.f:2465-2911).  Outputs are ADDED to u[3] and e[6]
-// (xx, yy, zz, xy, xz, yz); strain = -(rotated local gradient)/(2 mu).
-EFMM_HD void pair_eval(const TriFrame& f, const double* ssl, const double* sdl, bool dosl,
-                       bool dodl, bool dostrain, const double* X, bool self, double rlam,
-                       double rmu, double* u, double* e) {
-  double d[3] = {X[0] - f.org[0], X[1] - f.org[1], X[2] - f.org[2]};
-  double x0 = f.e1[0] * d[0] + f.e1[1] * d[1] + f.e1[2] * d[2];
-  double y0 = f.e2[0] * d[0] + f.e2[1] * d[1] + f.e2[2] * d[2];
-  double h = f.e3[0] * d[0] + f.e3[1] * d[1] + f.e3[2] * d[2];
-  TriTables T;
-  tri_tables(f, x0, y0, h, self, T);
-  double c1 = (rlam + rmu) / (rlam + 2.0 * rmu);
-  double ul[3], el[6];
-  assemble_gen(T.R, T.B, rlam, rmu, c1, ssl, sdl, dosl, dodl, dostrain, ul, el);
-  double inv2mu = 0.5 / rmu;
+// Rotate local-frame outputs (ul: displacement, el: symmetric strain xx yy zz
+// xy xz yz, both before the 1/(2 mu) and strain-sign factors) to the global
+// frame and ADD them to u[3], e[6].
+EFMM_HD void rotate_add(const TriFrame& f, const double* ul, const double* el, bool dostrain,
+                        double inv2mu, double* u, double* e) {
 #pragma unroll
   for (int i = 0; i < 3; i++)
     u[i] += inv2mu * (f.e1[i] * ul[0] + f.e2[i] * ul[1] + f.e3[i] * ul[2]);
   if (dostrain) {
-    // G = Q el Q^T with Q = [e1 e2 e3]
+    // G = Q el Q^T with Q = [e1 e2 e3]; strain = -G / (2 mu)
     double E[3][3] = {{el[0], el[3], el[4]}, {el[3], el[1], el[5]}, {el[4], el[5], el[2]}};
     double t[3][3];
 #pragma unroll
@@ -251,6 +236,68 @@ EFMM_HD void pair_eval(const TriFrame& f, const double* ssl, const double* sdl, 
       e[q] -= inv2mu * g;
     }
   }
+}
+
+EFMM_HD void pair_local(const TriFrame& f, const double* X, bool self, TriTables& T) {
+  double d[3] = {X[0] - f.org[0], X[1] - f.org[1], X[2] - f.org[2]};
+  double x0 = f.e1[0] * d[0] + f.e1[1] * d[1] + f.e1[2] * d[2];
+  double y0 = f.e2[0] * d[0] + f.e2[1] * d[1] + f.e2[2] * d[2];
+  double h = f.e3[0] * d[0] + f.e3[1] * d[1] + f.e3[2] * d[2];
+  tri_tables(f, x0, y0, h, self, T);
+}
+
+// One (triangle, target) interaction in global coordinates.  ssl/sdl are the
+// single/double layer densities already rotated into the triangle frame.
+// The local-frame assembly (assemble_gen, generated) follows the single layer
+// 2mu*u_i = sum_k s_k (2 d_ik R - c1 B_ik) (elfmm3dtria.f:1762-1987) and the
+// traction-kernel contraction with the frame normal for the double layer
+// (elfmm3dtria.f:2465-2911).  Outputs are ADDED to u[3] and e[6]
+// (xx, yy, zz, xy, xz, yz); strain = -(rotated local gradient)/(2 mu).
+EFMM_HD void pair_eval(const TriFrame& f, const double* ssl, const double* sdl, bool dosl,
+                       bool dodl, bool dostrain, const double* X, bool self, double rlam,
+                       double rmu, double* u, double* e) {
+  TriTables T;
+  pair_local(f, X, self, T);
+  double c1 = (rlam + rmu) / (rlam + 2.0 * rmu);
+  double ul[3], el[6];
+  assemble_gen(T.R, T.B, rlam, rmu, c1, ssl, sdl, dosl, dodl, dostrain, ul, el);
+  rotate_add(f, ul, el, dostrain, 0.5 / rmu, u, e);
+}
+
+// Response of one (triangle, target) pair to unit densities along the global
+// axes, the stored near-field operator of the ITER mode
+// (src/elfmm3dtria_iter_1.f:1559-1760 stores the same three unit responses):
+// for each enabled layer (single, then double) and direction k = x, y, z the
+// displacement (3 doubles, if dodisp) and strain (6, if dostrain) in global
+// coordinates.  Returns the number of doubles written to out.
+EFMM_HD int pair_blocks(const TriFrame& f, bool dosl, bool dodl, bool dodisp, bool dostrain,
+                        const double* X, bool self, double rlam, double rmu, double* out) {
+  TriTables T;
+  pair_local(f, X, self, T);
+  double c1 = (rlam + rmu) / (rlam + 2.0 * rmu);
+  double inv2mu = 0.5 / rmu;
+  const double zero[3] = {0.0, 0.0, 0.0};
+  int w = 0;
+  for (int layer = 0; layer < 2; layer++) {
+    if ((layer == 0 && !dosl) || (layer == 1 && !dodl)) continue;
+    for (int k = 0; k < 3; k++) {
+      const double s[3] = {f.e1[k], f.e2[k], f.e3[k]};  // global e_k in the triangle frame
+      double ul[3], el[6];
+      assemble_gen(T.R, T.B, rlam, rmu, c1, layer == 0 ? s : zero, layer == 1 ? s : zero,
+                   layer == 0, layer == 1, dostrain, ul, el);
+      double u[3] = {0, 0, 0}, e[6] = {0, 0, 0, 0, 0, 0};
+      rotate_add(f, ul, el, dostrain, inv2mu, u, e);
+      if (dodisp) {
+        out[w] = u[0]; out[w + 1] = u[1]; out[w + 2] = u[2];
+        w += 3;
+      }
+      if (dostrain) {
+        for (int q = 0; q < 6; q++) out[w + q] = e[q];
+        w += 6;
+      }
+    }
+  }
+  return w;
 }
 
 }  // namespace efmm

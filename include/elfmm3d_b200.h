@@ -58,6 +58,45 @@ void el3dtriadirecttarg_(const double *rlam, const double *rmu, const double *tr
                          const double *target, const int *ifptfrctarg, double *ptfrctarg,
                          const int *ifstraintarg, double *straintarg);
 
+/* Replaces elfmm3dtriatargiter (src/elfmm3dtria_iter_1.f:160-165): the
+ * iterative-solver variant that keeps the near-field interactions between
+ * calls on the same geometry.  icomp_type as in the reference
+ * (src/elfmm3dtria_iter_1.f:95-107): 1 evaluate without storage, 2 evaluate
+ * and store, 3 evaluate with the stored near field (same geometry, iprec,
+ * layers and outputs as the store; new densities), 4 tree only (sets lused),
+ * 5 store and evaluate the near field alone, 0 nothing.  The stored operator
+ * lives in device memory owned by the library; wsave receives an 8-word
+ * handle naming it, so lused is always 8.  With lwsave < 8, icomp_type 2 and 3
+ * evaluate without storage, as the reference does when wsave is too short.
+ * A handle that no longer matches (other geometry, iprec, layers, outputs or
+ * Lame constants, released or evicted store) gives ier 512.  At most four
+ * stores are live; a fifth evicts the least recently used. */
+void elfmm3dtriatargiter_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                          const double *triangle, const double *trinorm, const int *nparts,
+                          const double *source, const int *ifsingle, const double *sigma_sl,
+                          const int *ifdouble, const double *sigma_dl, const int *ifptfrc,
+                          double *ptfrc, const int *ifstrain, double *strain, const int *ntargs,
+                          const double *target, const int *ifptfrctarg, double *ptfrctarg,
+                          const int *ifstraintarg, double *straintarg, const int *icomp_type,
+                          double *wsave, const int *lwsave, int *lused);
+
+/* Replaces elfmm3dtriaiter (src/elfmm3dtria_iter_1.f:43-47): the ITER variant
+ * without off-surface targets. */
+void elfmm3dtriaiter_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                      const double *triangle, const double *trinorm, const int *nparts,
+                      const double *source, const int *ifsingle, const double *sigma_sl,
+                      const int *ifdouble, const double *sigma_dl, const int *ifptfrc,
+                      double *ptfrc, const int *ifstrain, double *strain, const int *icomp_type,
+                      double *wsave, const int *lwsave, int *lused);
+
+/* Frees the device store named by an ITER handle (no counterpart in the
+ * reference, whose store is the caller's wsave array).  512 if the handle
+ * names no live store. */
+int efmm_iter_release(const double *wsave, int lwsave);
+
+/* Device bytes held by the store an ITER handle names; -1 if none. */
+long long efmm_iter_stored_bytes(const double *wsave, int lwsave);
+
 /* ---- native device API ----------------------------------------------- */
 
 typedef struct efmm_plan efmm_plan;
