@@ -199,72 +199,134 @@ k_p2m(const P2MArgs a) {
 }
 
 // --------------------------------------------------- grouped translations
-// For every task: dst[:, 4 passes] += alpha * Op(group) * src[:, 4 passes]
-// over one 64-row tile and up to 16 (src, dst) pairs (= 64 columns).
-constexpr int TR_TILE_R = 64, TR_TILE_C = 64, TR_TILE_K = 16;
+// A task is one 128 x 128 output tile of the product Op(group) * B, where B's
+// columns are the concatenated columns of the group's (src, dst) pairs: column
+// j of the task is column c = (col0 + j) % C of pair pair0 + (col0 + j) / C.
+// Each box carries C columns (4 Laplace passes x right-hand sides) of length D.
+//   dst[pair.dst][c][rows] += alpha * Op[rows][:] * src[pair.src][c][:]
+// 256 threads, 8 x 8 outputs per thread, K tiles of 16 double-buffered in
+// shared memory (one barrier per tile), results scattered with atomics (the
+// pairs of one group have distinct destinations, different groups overlap).
+constexpr int TR_R = 128, TR_C = 128, TR_K = 16;
 
-__global__ void __launch_bounds__(256)
+template <class T>
+struct Vec2;
+template <>
+struct Vec2<double> { using type = double2; };
+template <>
+struct Vec2<float> { using type = float2; };
+
+template <class T>
+__global__ void __launch_bounds__(256, 1)
 k_translate(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
-            const double* __restrict__ mats, const long long* __restrict__ mat_off,
-            const int* __restrict__ mat_dim, int D, const double* __restrict__ src,
-            double* __restrict__ dst) {
-  __shared__ double As[TR_TILE_K][TR_TILE_R + 1];
-  __shared__ double Bs[TR_TILE_K][TR_TILE_C + 1];
+            const T* __restrict__ mats, const long long* __restrict__ mat_off,
+            const int* __restrict__ mat_dim, int D, int C, const T* __restrict__ src,
+            T* __restrict__ dst) {
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char tr_smem[];
+  T* As = reinterpret_cast<T*>(tr_smem);          // [2][TR_K][TR_R]
+  T* Bs = As + 2 * TR_K * TR_R;                    // [2][TR_K][TR_C]
   const TransTask t = tasks[blockIdx.x];
-  const double* A = mats + mat_off[t.group];
-  int dim = mat_dim[t.group];
-  int r0 = t.row0;
-  int np = t.npair;
-  int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  double acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
-  for (int k0 = 0; k0 < dim; k0 += TR_TILE_K) {
-    // A tile: rows r0..r0+63, cols k0..k0+15
-    for (int q = threadIdx.x; q < TR_TILE_R * TR_TILE_K; q += 256) {
-      int rr = q / TR_TILE_K, kk = q % TR_TILE_K;
-      int r = r0 + rr, k = k0 + kk;
-      As[kk][rr] = (r < dim && k < dim) ? A[(size_t)r * dim + k] : 0.0;
+  const T* A = mats + mat_off[t.group];
+  const int dim = mat_dim[t.group];
+  const int r0 = t.row0;
+  const int tid = threadIdx.x;
+  // loader roles: A row (tid >> 1), k half (tid & 1); B column (tid & 127), k half (tid >> 7)
+  const int arow = tid >> 1, akh = (tid & 1) * 8;
+  const bool arow_ok = r0 + arow < dim;
+  const T* Ap = A + (size_t)(arow_ok ? r0 + arow : 0) * dim;
+  const int bcol = tid & 127, bkh = (tid >> 7) * 8;
+  const T* Bp = nullptr;
+  {
+    int col = t.col0 + bcol;
+    if (col < t.ncols) {
+      const TransPair pr = pairs[t.pair0 + col / C];
+      Bp = src + ((size_t)pr.src * C + (col % C)) * D;
     }
-    // B tile: column j = (pair j/4, pass j%4)
-    for (int q = threadIdx.x; q < TR_TILE_C * TR_TILE_K; q += 256) {
-      int jj = q / TR_TILE_K, kk = q % TR_TILE_K;
-      int pj = jj >> 2, ps = jj & 3;
-      int k = k0 + kk;
-      double v = 0.0;
-      if (pj < np && k < dim) {
-        const TransPair& pr = pairs[t.pair0 + pj];
-        v = src[((size_t)pr.src * 4 + ps) * D + k];
+  }
+  T ra[8], rb[8];
+  auto load = [&](int k0) {
+    int ka = k0 + akh, kb = k0 + bkh;
+    if (arow_ok && ka + 8 <= dim) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(Ap + ka + 2 * i);
+        ra[2 * i] = v.x;
+        ra[2 * i + 1] = v.y;
       }
-      Bs[kk][jj] = v;
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) ra[i] = (arow_ok && ka + i < dim) ? Ap[ka + i] : T(0);
     }
-    __syncthreads();
+    if (Bp && kb + 8 <= dim) {
 #pragma unroll
-    for (int kk = 0; kk < TR_TILE_K; kk++) {
-      double a[4], b[4];
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(Bp + kb + 2 * i);
+        rb[2 * i] = v.x;
+        rb[2 * i + 1] = v.y;
+      }
+    } else {
 #pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] += a[i] * b[j];
+      for (int i = 0; i < 8; i++) rb[i] = (Bp && kb + i < dim) ? Bp[kb + i] : T(0);
     }
+  };
+  auto store = [&](int buf) {
+    T* as = As + buf * TR_K * TR_R;
+    T* bs = Bs + buf * TR_K * TR_C;
+#pragma unroll
+    for (int i = 0; i < 8; i++) as[(akh + i) * TR_R + arow] = ra[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) bs[(bkh + i) * TR_C + bcol] = rb[i];
+  };
+  const int tx = tid & 15, ty = tid >> 4;
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = T(0);
+  const int nk = (dim + TR_K - 1) / TR_K;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; kt++) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) load((kt + 1) * TR_K);
+    const T* as = As + cur * TR_K * TR_R;
+    const T* bs = Bs + cur * TR_K * TR_C;
+#pragma unroll
+    for (int kk = 0; kk < TR_K; kk++) {
+      T a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(as + kk * TR_R + ty * 8 + 2 * i);
+        a[2 * i] = v.x;
+        a[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        V2 v = *reinterpret_cast<const V2*>(bs + kk * TR_C + 32 * j + 2 * tx);
+        b[2 * j] = v.x;
+        b[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] += a[i] * b[j];
+    }
+    if (kt + 1 < nk) store(cur ^ 1);
     __syncthreads();
   }
 #pragma unroll
-  for (int j = 0; j < 4; j++) {
-    int jj = tx * 4 + j;
-    int pj = jj >> 2, ps = jj & 3;
-    if (pj >= np) continue;
-    const TransPair& pr = pairs[t.pair0 + pj];
+  for (int j = 0; j < 8; j++) {
+    int col = t.col0 + 32 * (j >> 1) + 2 * tx + (j & 1);
+    if (col >= t.ncols) continue;
+    const TransPair pr = pairs[t.pair0 + col / C];
+    T* dp = dst + ((size_t)pr.dst * C + (col % C)) * D;
+    T al = (T)pr.alpha;
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
-      int r = r0 + ty * 4 + i;
-      if (r < dim) atomicAdd(&dst[((size_t)pr.dst * 4 + ps) * D + r], pr.alpha * acc[i][j]);
+    for (int i = 0; i < 8; i++) {
+      int r = r0 + ty * 8 + i;
+      if (r < dim) atomicAdd(dp + r, al * acc[i][j]);
     }
   }
 }
@@ -432,13 +494,26 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a) {
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
+template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
-                      const double* mats, const long long* mat_off, const int* mat_dim, int D,
-                      const double* src, double* dst) {
+                      const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,
+                      const T* src, T* dst) {
   if (ntask <= 0) return;
-  k_translate<<<ntask, 256, 0, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, src, dst); count_launch();
+  const int smem = (int)(sizeof(T) * 2 * TR_K * (TR_R + TR_C));
+  static bool attr_set[64] = {};  // per T instantiation and device
+  int dev = 0;
+  EFMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev >= 64 || !attr_set[dev]) {
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_translate<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    if (dev < 64) attr_set[dev] = true;
+  }
+  k_translate<T><<<ntask, 256, smem, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, C, src, dst); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+template void launch_translate<double>(cudaStream_t, int, const TransTask*, const TransPair*, const double*,
+                                       const long long*, const int*, int, int, const double*, double*);
+template void launch_translate<float>(cudaStream_t, int, const TransTask*, const TransPair*, const float*,
+                                      const long long*, const int*, int, int, const float*, float*);
 
 void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a) {
   if (nleaf <= 0) return;

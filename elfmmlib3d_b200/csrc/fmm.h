@@ -17,8 +17,10 @@ struct TransPair {
   int src, dst;
   double alpha;
 };
+// One 128 x 128 output tile: operator group, first row, the group's first
+// pair, the group's column count (pairs x C) and the tile's first column.
 struct TransTask {
-  int group, row0, pair0, npair;
+  int group, row0, pair0, ncols, col0;
 };
 
 struct P2MArgs {
@@ -44,9 +46,10 @@ struct L2TArgs {
 
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);
 void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a);
+template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
-                      const double* mats, const long long* mat_off, const int* mat_dim, int D,
-                      const double* src, double* dst);
+                      const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,
+                      const T* src, T* dst);
 void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a);
 
 }  // namespace efmm

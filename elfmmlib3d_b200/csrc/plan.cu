@@ -293,34 +293,35 @@ void Plan::build_worklists() {
   nl2t_ = (int)l2t.size();
   h2d(p2m_leaves_, p2m, st_);
   h2d(l2t_leaves_, l2t, st_);
-  m2m_lev_.clear();
-  l2l_lev_.clear();
+  m2m_.clear();
+  m2l_.clear();
+  l2l_.clear();
   if (!far_) return;
   ensure_ops();
   const int* m2lg = ops_->m2l_group;
   const std::vector<int>& dims = ops_->dims;
-  auto tile = [&](std::vector<std::pair<int, TransPair>>& gp, std::vector<TransPair>& pairs,
-                  std::vector<TransTask>& tasks) {
+  // group the pairs of one level by operator; one segment per group
+  auto add_level = [&](std::vector<std::pair<int, TransPair>>& gp, std::vector<TransPair>& pairs,
+                       TransSched& S) {
     std::stable_sort(gp.begin(), gp.end(),
                      [](const std::pair<int, TransPair>& a, const std::pair<int, TransPair>& b) {
                        return a.first < b.first;
                      });
+    int s0 = (int)S.segs.size();
     size_t i = 0;
     while (i < gp.size()) {
       size_t j = i;
       while (j < gp.size() && gp[j].first == gp[i].first) j++;
-      int g = gp[i].first;
-      for (size_t c = i; c < j; c += 16) {
-        int np = (int)std::min<size_t>(16, j - c);
-        int p0 = (int)pairs.size();
-        for (int q = 0; q < np; q++) pairs.push_back(gp[c + q].second);
-        for (int r0 = 0; r0 < dims[g]; r0 += 64) tasks.push_back({g, r0, p0, np});
-      }
+      S.segs.push_back({gp[i].first, (int)pairs.size(), (int)(j - i)});
+      for (size_t q = i; q < j; q++) pairs.push_back(gp[q].second);
       i = j;
     }
+    S.lev.push_back({s0, (int)S.segs.size() - s0});
   };
+  m2m_.clear();
+  m2l_.clear();
+  l2l_.clear();
   std::vector<TransPair> m2m_pairs, l2l_pairs, m2l_pairs;
-  std::vector<TransTask> m2m_tasks, l2l_tasks, m2l_tasks;
   // M2M bottom-up: children at level lev -> parents at lev-1 (parents >= 2)
   for (int lev = tr_.nlev; lev >= 3; lev--) {
     std::vector<std::pair<int, TransPair>> gp;
@@ -331,9 +332,7 @@ void Plan::build_worklists() {
       int dg = ((ijk[3 * b] - 1) & 1) + 2 * ((ijk[3 * b + 1] - 1) & 1) + 4 * ((ijk[3 * b + 2] - 1) & 1);
       gp.push_back({ops_->m2m_group[dg], TransPair{b, P, 1.0}});
     }
-    int t0 = (int)m2m_tasks.size();
-    tile(gp, m2m_pairs, m2m_tasks);
-    m2m_lev_.push_back({t0, (int)m2m_tasks.size() - t0});
+    add_level(gp, m2m_pairs, m2m_);
   }
   // M2L: list 2 of every box at level >= 2
   {
@@ -351,7 +350,7 @@ void Plan::build_worklists() {
       }
     }
     m2l_pairs_h_ = gp.size();
-    tile(gp, m2l_pairs, m2l_tasks);
+    add_level(gp, m2l_pairs, m2l_);
   }
   // L2L top-down: parents at level lev (>= 2) -> children
   for (int lev = 2; lev < tr_.nlev; lev++) {
@@ -365,21 +364,44 @@ void Plan::build_worklists() {
         gp.push_back({ops_->l2l_group[dg], TransPair{b, k, 1.0}});
       }
     }
-    int t0 = (int)l2l_tasks.size();
-    tile(gp, l2l_pairs, l2l_tasks);
-    l2l_lev_.push_back({t0, (int)l2l_tasks.size() - t0});
+    add_level(gp, l2l_pairs, l2l_);
   }
-  h2d(m2m_pairs_, m2m_pairs, st_);
-  h2d(m2m_tasks_, m2m_tasks, st_);
-  h2d(m2l_pairs_, m2l_pairs, st_);
-  h2d(m2l_tasks_, m2l_tasks, st_);
-  h2d(l2l_pairs_, l2l_pairs, st_);
-  h2d(l2l_tasks_, l2l_tasks, st_);
-  nm2l_tasks_ = (int)m2l_tasks.size();
+  h2d(m2m_.pairs, m2m_pairs, st_);
+  h2d(m2l_.pairs, m2l_pairs, st_);
+  h2d(l2l_.pairs, l2l_pairs, st_);
   int D = 2 * ncoef(p_);
   mpole_.resize((size_t)nb * 4 * D);
   local_.resize((size_t)nb * 4 * D);
   EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+}
+
+void Plan::cut_tasks(TransSched& S, int C) {
+  if (S.C == C) return;
+  std::vector<TransTask> tasks;
+  S.lev_tasks.clear();
+  const std::vector<int>& dims = ops_->dims;
+  for (auto& r : S.lev) {
+    int t0 = (int)tasks.size();
+    for (int q = r.first; q < r.first + r.second; q++) {
+      const TransSeg& g = S.segs[q];
+      int ncols = g.npair * C, dim = dims[g.group];
+      // row tiles innermost: the tasks of one column tile share their source columns
+      for (int c0 = 0; c0 < ncols; c0 += 128)
+        for (int r0 = 0; r0 < dim; r0 += 128) tasks.push_back({g.group, r0, g.pair0, ncols, c0});
+    }
+    S.lev_tasks.push_back({t0, (int)tasks.size() - t0});
+  }
+  h2d(S.tasks, tasks, st_);
+  S.C = C;
+}
+
+template <class T>
+void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst) {
+  cut_tasks(S, C);
+  int D = 2 * ncoef(p_);
+  for (auto& r : S.lev_tasks)
+    launch_translate<T>(st_, r.second, S.tasks.get() + r.first, S.pairs.get(), mats, ops_->off.get(),
+                        ops_->dim.get(), D, C, src, dst);
 }
 
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
@@ -446,18 +468,11 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     pa.mpole = mpole_.get();
     launch_p2m(st_, np2m_, pa);
     EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
-    for (auto& r : m2m_lev_) {
-      launch_translate(st_, r.second, m2m_tasks_.get() + r.first, m2m_pairs_.get(), ops_->mats.get(),
-                       ops_->off.get(), ops_->dim.get(), D, mpole_.get(), mpole_.get());
-    }
+    run_translations(m2m_, 4, ops_->mats.get(), mpole_.get(), mpole_.get());
     EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
-    launch_translate(st_, nm2l_tasks_, m2l_tasks_.get(), m2l_pairs_.get(), ops_->mats.get(), ops_->off.get(),
-                     ops_->dim.get(), D, mpole_.get(), local_.get());
+    run_translations(m2l_, 4, ops_->mats.get(), mpole_.get(), local_.get());
     EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
-    for (auto& r : l2l_lev_) {
-      launch_translate(st_, r.second, l2l_tasks_.get() + r.first, l2l_pairs_.get(), ops_->mats.get(),
-                       ops_->off.get(), ops_->dim.get(), D, local_.get(), local_.get());
-    }
+    run_translations(l2l_, 4, ops_->mats.get(), local_.get(), local_.get());
     EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
     L2TArgs la;
     la.leaves = l2t_leaves_.get();

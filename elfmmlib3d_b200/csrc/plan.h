@@ -29,6 +29,27 @@ struct Timings {  // milliseconds of the last evaluate(), CUDA events
   float total = 0, p2m = 0, m2m = 0, m2l = 0, l2l = 0, l2t = 0, near = 0, prep = 0;
 };
 
+// Translation schedule of one kind (M2M, M2L or L2L): pairs sorted by
+// operator group, one segment per (level, group); tasks are cut for a given
+// number of columns per box C and cached.
+struct TransSeg {
+  int group, pair0, npair;
+};
+struct TransSched {
+  DevBuf<TransPair> pairs;
+  std::vector<TransSeg> segs;
+  std::vector<std::pair<int, int>> lev;  // segment ranges in execution order
+  int C = -1;
+  DevBuf<TransTask> tasks;
+  std::vector<std::pair<int, int>> lev_tasks;  // task ranges in execution order
+  void clear() {
+    segs.clear();
+    lev.clear();
+    C = -1;
+    lev_tasks.clear();
+  }
+};
+
 class Plan {
  public:
   Plan(int device, cudaStream_t stream);
@@ -83,10 +104,10 @@ class Plan {
   int store_flags_ = 0, store_K_ = 0;
   double store_lam_ = 0, store_mu_ = 0;
   long long near_pairs_ = 0;
-  DevBuf<TransPair> m2m_pairs_, m2l_pairs_, l2l_pairs_;
-  DevBuf<TransTask> m2m_tasks_, m2l_tasks_, l2l_tasks_;
-  std::vector<std::pair<int, int>> m2m_lev_, l2l_lev_;  // task ranges per level (execution order)
-  int nm2l_tasks_ = 0;
+  TransSched m2m_, m2l_, l2l_;
+  void cut_tasks(TransSched& S, int C);
+  template <class T>
+  void run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst);
   size_t m2l_pairs_h_ = 0;
   DevBuf<double> mpole_, local_;
   DevBuf<double> ssl_s_, sdl_s_, u_s_, e_s_, ut_s_, et_s_;
