@@ -187,6 +187,7 @@ def run_ours(args, rank, world, local_rank):
     launches = E.kernel_launches() - l0
     info = P.info()
     tim = P.timings()
+    setup = P.setup_timings()
     t_max = ms
     if world > 1:
         import torch.distributed as dist
@@ -238,7 +239,7 @@ def run_ours(args, rank, world, local_rank):
         "config": {"workload": args.workload, "triangles": n, "targets": m, "iprec": iprec,
                    "evals_per_step": evals, "parallelism": f"replicas{world}",
                    "l2_policy": "inputs + expansions > L2 (126 MB)",
-                   "stage_ms": tim, "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")},
+                   "stage_ms": tim, "setup_ms": setup, "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")},
                    "near_pairs": info["near_pairs"], "m2l_pairs": info["m2l_pairs"]},
         "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "timing": "host wall clock around blocking C-ABI calls"},

@@ -46,7 +46,9 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings",
            "efmm_plan_info", "efmm_plan_tree_export", "efmm_kernel_launches", "efmm_plan_record",
            "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
-           "efmm_iter_release", "efmm_iter_stored_bytes"]
+           "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
+           "efmm_plan_evaluate_batch", "efmm_plan_flops",
+           "efmm_plan_evaluate_direct_subset"]
 
 
 class ElfmmError(RuntimeError):
@@ -77,8 +79,16 @@ def load():
     for f in (L.efmm_plan_evaluate, L.efmm_plan_evaluate_direct):
         f.restype = ctypes.c_int
         f.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.efmm_plan_evaluate_batch.restype = ctypes.c_int
+    L.efmm_plan_evaluate_batch.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp,
+                                           _vp, _vp, _vp, ctypes.c_int]
+    L.efmm_plan_flops.argtypes = [_vp, _dp]
+    L.efmm_plan_evaluate_direct_subset.restype = ctypes.c_int
+    L.efmm_plan_evaluate_direct_subset.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp,
+                                                   _vp, _vp, _vp]
     L.efmm_plan_timings.argtypes = [_vp, _fp]
     L.efmm_plan_info.argtypes = [_vp, _llp]
+    L.efmm_plan_setup_timings.argtypes = [_vp, _fp]
     L.efmm_kernel_launches.restype = ctypes.c_longlong
     L.efmm_plan_record.restype = ctypes.c_int
     L.efmm_plan_record.argtypes = [_vp, ctypes.c_int]
@@ -288,6 +298,17 @@ class Plan:
         if ier:
             raise ElfmmError(ier, "evaluate")
 
+    def evaluate_batch(self, rlam, rmu, nrhs, ssl=None, sdl=None, u=None, e=None, ut=None, et=None,
+                       precision=0):
+        """nrhs right-hand sides in one pass: ssl/sdl (nrhs,n,3); outputs
+        (nrhs,n,3), (nrhs,n,3,3), (nrhs,nt,3), (nrhs,nt,3,3).  precision 0 =
+        FP64, 1 = mixed (FP32 expansions and translations)."""
+        ier = self._L.efmm_plan_evaluate_batch(self._h, float(rlam), float(rmu), int(nrhs), self._ptr(ssl),
+                                               self._ptr(sdl), self._ptr(u), self._ptr(e), self._ptr(ut),
+                                               self._ptr(et), int(precision))
+        if ier:
+            raise ElfmmError(ier, "evaluate_batch")
+
     def record(self, slot):
         """Record CUDA event `slot` (0..7) on the plan's stream."""
         if self._L.efmm_plan_record(self._h, int(slot)):
@@ -301,6 +322,25 @@ class Plan:
         a = (ctypes.c_float * 8)()
         self._L.efmm_plan_timings(self._h, a)
         return dict(zip(["total", "prep", "p2m", "m2m", "m2l", "l2l", "l2t", "near"], list(a)))
+
+    def evaluate_direct_subset(self, rlam, rmu, nsub, ssl=None, sdl=None, u=None, e=None):
+        """Direct sum at the first nsub centroids: u (nsub,3), e (nsub,3,3)."""
+        ier = self._L.efmm_plan_evaluate_direct_subset(self._h, float(rlam), float(rmu), int(nsub),
+                                                       self._ptr(ssl), self._ptr(sdl), self._ptr(u), self._ptr(e))
+        if ier:
+            raise ElfmmError(ier, "evaluate_direct_subset")
+
+    def flops_per_column(self):
+        """Useful flops per expansion column: P2M, M2M, M2L, L2L, L2T."""
+        a = (ctypes.c_double * 5)()
+        self._L.efmm_plan_flops(self._h, a)
+        return dict(zip(["p2m", "m2m", "m2l", "l2l", "l2t"], list(a)))
+
+    def setup_timings(self):
+        """Host milliseconds of the last set_geometry, by phase."""
+        a = (ctypes.c_float * 4)()
+        self._L.efmm_plan_setup_timings(self._h, a)
+        return dict(zip(["tree", "lists", "worklists", "operators"], list(a)))
 
     def info(self):
         a = (ctypes.c_longlong * 8)()

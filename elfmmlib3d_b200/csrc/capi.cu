@@ -75,6 +75,22 @@ extern "C" int efmm_plan_evaluate(efmm_plan* p, double rlam, double rmu, const d
   EFMM_GUARD(return p->plan->evaluate(rlam, rmu, ssl, sdl, u_src, e_src, u_tgt, e_tgt);)
 }
 
+extern "C" int efmm_plan_evaluate_direct_subset(efmm_plan* p, double rlam, double rmu, int nsub,
+                                                const double* ssl, const double* sdl, double* u_src,
+                                                double* e_src) {
+  if (!p || nsub < 1) return IER_BADARG;
+  EFMM_GUARD(return p->plan->evaluate_direct(rlam, rmu, ssl, sdl, u_src, e_src, nullptr, nullptr, nsub);)
+}
+
+extern "C" int efmm_plan_evaluate_batch(efmm_plan* p, double rlam, double rmu, int nrhs, const double* ssl,
+                                        const double* sdl, double* u_src, double* e_src, double* u_tgt,
+                                        double* e_tgt, int precision) {
+  if (!p) return IER_BADARG;
+  EFMM_GUARD(return p->plan->evaluate_batch(rlam, rmu, nrhs, ssl, sdl, u_src, e_src, u_tgt, e_tgt, precision);)
+}
+
+extern "C" void efmm_plan_flops(const efmm_plan* p, double* f5) { p->plan->flops_per_column(f5); }
+
 extern "C" int efmm_plan_evaluate_direct(efmm_plan* p, double rlam, double rmu, const double* ssl,
                                          const double* sdl, double* u_src, double* e_src,
                                          double* u_tgt, double* e_tgt) {
@@ -102,6 +118,11 @@ extern "C" void efmm_plan_timings(const efmm_plan* p, float* ms) {
   const Timings& t = p->plan->timings;
   ms[0] = t.total; ms[1] = t.prep; ms[2] = t.p2m; ms[3] = t.m2m;
   ms[4] = t.m2l; ms[5] = t.l2l; ms[6] = t.l2t; ms[7] = t.near;
+}
+
+extern "C" void efmm_plan_setup_timings(const efmm_plan* p, float* ms) {
+  const Timings& t = p->plan->timings;
+  ms[0] = t.geo_tree; ms[1] = t.geo_lists; ms[2] = t.geo_work; ms[3] = t.geo_ops;
 }
 
 extern "C" void efmm_plan_info(const efmm_plan* p, long long* info) {

@@ -129,13 +129,12 @@ k_p2m(const P2MArgs a) {
         }
       }
       if (lane == 0) {
-        const double* ss = a.ssl + 3 * (size_t)it;
-        const double* sd = a.sdl + 3 * (size_t)it;
+        const long long off = blockIdx.y * a.rstride + it * a.tstride, ds = a.dstride;
         const double* nn = a.nrm + 3 * (size_t)it;
         double* o = qd + 16 * warp;
         double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
-        if (a.dosl) { sl[0] = ss[0]; sl[1] = ss[1]; sl[2] = ss[2]; }
-        if (a.dodl) { dl[0] = sd[0]; dl[1] = sd[1]; dl[2] = sd[2]; }
+        if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
+        if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
         // passes 0..2: charge s_j/(2mu), dipole (n s_j + s n_j)/2
         for (int j = 0; j < 3; j++) {
           o[j] = w * sl[j] * inv2mu;
@@ -185,7 +184,7 @@ k_p2m(const P2MArgs a) {
       }
     }
   }
-  double* M = a.mpole + (size_t)box * 4 * D;
+  double* M = a.mpole + ((size_t)box * a.C + 4 * blockIdx.y) * D;
 #pragma unroll
   for (int i = 0; i < CMAX; i++) {
     int cc = threadIdx.x + i * P2M_THREADS;
@@ -194,6 +193,201 @@ k_p2m(const P2MArgs a) {
     for (int q = 0; q < 4; q++) {
       M[(size_t)q * D + 2 * cc] = acc[i][q][0];
       M[(size_t)q * D + 2 * cc + 1] = acc[i][q][1];
+    }
+  }
+}
+
+template <class T>
+struct Vec2;
+template <>
+struct Vec2<double> { using type = double2; };
+template <>
+struct Vec2<float> { using type = float2; };
+
+// ---------------------------------------------- P2M, many right-hand sides
+// For C = 4R columns the multipole of a leaf is a product
+//   M[row][col] = sum over (node, k) F[row][node, k] * W[node, k][col]
+// with F the conjugated regular harmonics and their gradients at the 12 P2M
+// nodes of each triangle (k = 0 charge, 1..3 dipole x, y, z) and W the per
+// node charge and dipole strengths of column col = (rhs r, pass q).  One CTA
+// per (leaf, 128-row tile, 128-column tile); node chunks of PG_NODES nodes
+// build Y in shared memory, then the F and W tiles, then an 8 x 8-per-thread
+// register-blocked product.  Rows are the interleaved (re, im) coefficients.
+constexpr int PG_NODES = 8, PG_K = 4 * PG_NODES, PG_R = 128, PG_C = 128;
+
+template <class T>
+__global__ void __launch_bounds__(256, 1)
+k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char pg_smem[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc, C = 4 * R;
+  cplx* Ys = reinterpret_cast<cplx*>(pg_smem);                  // [PG_NODES][nc]
+  double* nd = reinterpret_cast<double*>(Ys + PG_NODES * nc);   // [PG_NODES][8]: y, n, w
+  int* nt = reinterpret_cast<int*>(nd + PG_NODES * 8);          // [PG_NODES] triangle
+  T* Fs = reinterpret_cast<T*>(nt + PG_NODES + (PG_NODES & 1)); // [PG_K][PG_R]
+  T* Ws = Fs + PG_K * PG_R;                                      // [PG_K][PG_C]
+  const int box = a.leaves[blockIdx.x];
+  const int row0 = blockIdx.y * PG_R, col0 = blockIdx.z * PG_C;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int nnode = 12 * tn;
+  Quad12 Q;
+  quad12(Q);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // F-tile role: one row, nodes j = (tid >> 7) + 2 i
+  const int frow = tid & 127, fj0 = tid >> 7;
+  const int grow = row0 + frow;
+  const bool frow_ok = grow < D;
+  const int cc = frow_ok ? grow >> 1 : 0, part = grow & 1;
+  int fn = 0;
+  while ((fn + 1) * (fn + 2) / 2 <= cc) fn++;
+  const int fm = cc - fn * (fn + 1) / 2;
+  const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu;
+  const int tx = tid & 15, ty = tid >> 4;
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = T(0);
+  for (int b0 = 0; b0 < nnode; b0 += PG_NODES) {
+    __syncthreads();
+    // Y of node b0 + warp (regular harmonics, one order m per lane)
+    if (warp < PG_NODES) {
+      const int node = b0 + warp;
+      cplx* Y = Ys + (size_t)warp * nc;
+      if (node < nnode) {
+        const int it = t0 + node / 12, iq = node % 12;
+        const double* Tr = a.tri + 9 * (size_t)it;
+        double y[3];
+        for (int d = 0; d < 3; d++)
+          y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
+        const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
+        const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+        for (int m = lane; m <= p; m += 32) {
+          cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+          for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+          Y[cidx(m, m)] = dm;
+          cplx ym2 = {0, 0}, ym1 = dm;
+          for (int n = m + 1; n <= p; n++) {
+            const double aa = (2.0 * n - 1.0) * z[2];
+            const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+            cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+            Y[cidx(n, m)] = yn;
+            ym2 = ym1;
+            ym1 = yn;
+          }
+        }
+        if (lane == 0) {
+          const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+          const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+          const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                                e1[0] * e2[1] - e1[1] * e2[0]};
+          const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+          double* o = nd + 8 * warp;
+          o[0] = y[0]; o[1] = y[1]; o[2] = y[2];
+          const double* nn = a.nrm + 3 * (size_t)it;
+          o[3] = nn[0]; o[4] = nn[1]; o[5] = nn[2];
+          o[6] = Q.w[iq] * area;
+          nt[warp] = it;
+        }
+      } else if (lane == 0) {
+        nd[8 * warp + 6] = 0.0;
+        nt[warp] = -1;
+      }
+    }
+    __syncthreads();
+    // F tile: rows x (node, k)
+    for (int j = fj0; j < PG_NODES; j += 2) {
+      T f[4] = {T(0), T(0), T(0), T(0)};
+      if (frow_ok && nt[j] >= 0) {
+        const double sc = a.wnorm ? a.wnorm[grow] : 1.0;
+        const cplx* Y = Ys + (size_t)j * nc;
+        const cplx y = Y[cc];
+        cplx ya = {0, 0}, yb = {0, 0}, yc = {0, 0};
+        if (fn > 0) {
+          ya = hget(Y, fn - 1, fm);
+          yb = hget(Y, fn - 1, fm + 1);
+          yc = hget(Y, fn - 1, fm - 1);
+        }
+        if (part == 0) {
+          f[0] = (T)(sc * y.re);
+          f[1] = (T)(sc * 0.5 * is * (yb.re - yc.re));
+          f[2] = (T)(sc * 0.5 * is * (yb.im + yc.im));
+          f[3] = (T)(sc * is * ya.re);
+        } else {
+          f[0] = (T)(-sc * y.im);
+          f[1] = (T)(-sc * 0.5 * is * (yb.im - yc.im));
+          f[2] = (T)(sc * 0.5 * is * (yb.re + yc.re));
+          f[3] = (T)(-sc * is * ya.im);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) Fs[(4 * j + k) * PG_R + frow] = f[k];
+    }
+    // W tile: (node, k) x columns; column = (rhs r, pass q)
+    for (int q2 = tid; q2 < PG_NODES * PG_C; q2 += 256) {
+      const int j = q2 / PG_C, col = q2 % PG_C, gcol = col0 + col;
+      T wv[4] = {T(0), T(0), T(0), T(0)};
+      const int it = nt[j];
+      if (it >= 0 && gcol < C) {
+        const int r = gcol >> 2, q = gcol & 3;
+        const double* o = nd + 8 * j;
+        const double y[3] = {o[0], o[1], o[2]}, nn[3] = {o[3], o[4], o[5]}, w = o[6];
+        const long long off = r * a.rstride + it * a.tstride, ds = a.dstride;
+        double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+        if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
+        if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
+        if (q < 3) {
+          // pass q: charge s_q/(2mu), dipole (n s_q + s n_q)/2
+          wv[0] = (T)(w * sl[q] * inv2mu);
+          for (int d = 0; d < 3; d++) wv[1 + d] = (T)(w * 0.5 * (nn[d] * dl[q] + dl[d] * nn[q]));
+        } else {
+          // pass 3: charge (s_sl.y) c1/(2mu) + (s_dl.n) c2, dipole c1 [n (s_dl.y) + s_dl (n.y)]/2
+          const double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
+          const double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+          const double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
+          const double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+          wv[0] = (T)(w * (sly * c1 * inv2mu + dln * c2));
+          for (int d = 0; d < 3; d++) wv[1 + d] = (T)(w * 0.5 * c1 * (nn[d] * dly + dl[d] * ny));
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; k++) Ws[(4 * j + k) * PG_C + col] = wv[k];
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < PG_K; kk++) {
+      T av[8], bv[8];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(Fs + kk * PG_R + ty * 8 + 2 * i);
+        av[2 * i] = v.x;
+        av[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        V2 v = *reinterpret_cast<const V2*>(Ws + kk * PG_C + 32 * j + 2 * tx);
+        bv[2 * j] = v.x;
+        bv[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] += av[i] * bv[j];
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int gcol = col0 + 32 * (j >> 1) + 2 * tx + (j & 1);
+    if (gcol >= C) continue;
+    T* M = mpole + ((size_t)box * C + gcol) * D;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = row0 + ty * 8 + i;
+      if (r < D) M[r] = acc[i][j];
     }
   }
 }
@@ -208,13 +402,6 @@ k_p2m(const P2MArgs a) {
 // shared memory (one barrier per tile), results scattered with atomics (the
 // pairs of one group have distinct destinations, different groups overlap).
 constexpr int TR_R = 128, TR_C = 128, TR_K = 16;
-
-template <class T>
-struct Vec2;
-template <>
-struct Vec2<double> { using type = double2; };
-template <>
-struct Vec2<float> { using type = float2; };
 
 template <class T>
 __global__ void __launch_bounds__(256, 1)
@@ -342,7 +529,7 @@ k_l2t(const L2TArgs a) {
   int p = a.p, nc = ncoef(p), D = 2 * nc;
   double* Ls = sm;                                              // [4][D]
   cplx* Yall = reinterpret_cast<cplx*>(sm + 4 * (size_t)D);     // [warps][nc]
-  const double* L = a.local + (size_t)box * 4 * D;
+  const double* L = a.local + ((size_t)box * a.C + 4 * blockIdx.y) * D;
   for (int q = threadIdx.x; q < 4 * D; q += blockDim.x) Ls[q] = L[q];
   int lev = a.level[box];
   double s = a.size / (double)(1ull << lev);
@@ -448,8 +635,9 @@ k_l2t(const L2TArgs a) {
         u[i] = (2.0 - c1) * pot[i] + g[3][i];
         for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
       }
-      double* U = is_src ? a.u_src : a.u_tgt;
-      double* E = is_src ? a.e_src : a.e_tgt;
+      const size_t np = is_src ? a.nsrc : a.ntgt;
+      double* U = (is_src ? a.u_src : a.u_tgt) + 3 * np * blockIdx.y;
+      double* E = (is_src ? a.e_src : a.e_tgt) + 6 * np * blockIdx.y;
       U[3 * (size_t)pidx] += u[0];
       U[3 * (size_t)pidx + 1] += u[1];
       U[3 * (size_t)pidx + 2] += u[2];
@@ -475,6 +663,197 @@ k_l2t(const L2TArgs a) {
   }
 }
 
+// ----------------------------------------- L2T, many right-hand sides
+// For C = 4R columns the nine derivative sums of a local expansion at a point
+// are linear functionals of the stored real coefficient rows:
+//   S[point, v][col] = sum over rows G_v[row](point) * L_box[row][col]
+// (v: pot, d_z, d_zz, the D+ pair, the D+D_z pair, the D+D+ pair; the same
+// sums as k_l2t, with the m < 0 terms folded onto the stored m >= 0 rows by
+// conjugate symmetry).  One CTA per (leaf, chunk of 8 points, 256 columns):
+// warp w owns point w, lane l the columns of right-hand sides l and l + 32;
+// FP64 throughout (the local expansions may be FP32 in the normalised
+// basis, converted while staged), then the Lame recombination of k_l2t.
+constexpr int LG_PTS = 8, LG_K = 16, LG_C = 256;
+
+struct LgTerm {
+  int a, b, sg, im;  // shift in n, shift in m, sign, imaginary part
+};
+__constant__ LgTerm c_lg_terms[9] = {{0, 0, 1, 0},  {1, 0, 1, 0},  {2, 0, 1, 0},
+                                     {1, 1, -1, 0}, {1, 1, -1, 1}, {2, 1, -1, 0},
+                                     {2, 1, -1, 1}, {2, 2, 1, 0},  {2, 2, 1, 1}};
+
+template <class TB>
+__global__ void __launch_bounds__(256, 1)
+k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __restrict__ chunk_e0, int R,
+           const TB* __restrict__ local, const double* __restrict__ wnorm) {
+  extern __shared__ __align__(16) unsigned char lg_smem[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc, C = 4 * R;
+  cplx* Ys = reinterpret_cast<cplx*>(lg_smem);                     // [LG_PTS][nc]
+  double* Gs = reinterpret_cast<double*>(Ys + LG_PTS * nc);         // [LG_K][LG_PTS][9]
+  double* Bs = Gs + LG_K * LG_PTS * 9;                              // [LG_K][LG_C]
+  const int box = a.leaves[chunk_leaf[blockIdx.x]];
+  const int e0 = chunk_e0[blockIdx.x];
+  const int col0 = blockIdx.y * LG_C;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
+  const int s0 = a.sstart[box], t0 = a.tstart[box];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // this warp's point
+  const int e = e0 + warp;
+  const bool ok = e < sn + tn;
+  const bool is_src = e < sn;
+  const int pidx = ok ? (is_src ? s0 + e : t0 + (e - sn)) : 0;
+  double x[3] = {0, 0, 0};
+  if (ok) {
+    const double* X = is_src ? a.src_pts + 3 * (size_t)pidx : a.tgt_pts + 3 * (size_t)pidx;
+    x[0] = X[0]; x[1] = X[1]; x[2] = X[2];
+  }
+  {
+    cplx* Y = Ys + (size_t)warp * nc;
+    const double z[3] = {(x[0] - c[0]) * is, (x[1] - c[1]) * is, (x[2] - c[2]) * is};
+    const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+    for (int m = lane; m <= p; m += 32) {
+      cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+      for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+      Y[cidx(m, m)] = dm;
+      cplx ym2 = {0, 0}, ym1 = dm;
+      for (int n = m + 1; n <= p; n++) {
+        const double aa = (2.0 * n - 1.0) * z[2];
+        const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+        cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        Y[cidx(n, m)] = yn;
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+  }
+  double acc[9][8];
+#pragma unroll
+  for (int v = 0; v < 9; v++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[v][j] = 0.0;
+  const TB* Lb = local + (size_t)box * C * D;
+  for (int k0 = 0; k0 < D; k0 += LG_K) {
+    __syncthreads();
+    // G tile: (k, point, v)
+    for (int q = tid; q < LG_K * LG_PTS * 9; q += 256) {
+      const int kk = q / (LG_PTS * 9), pt = (q / 9) % LG_PTS, v = q % 9;
+      const int row = k0 + kk;
+      double g = 0.0;
+      if (row < D) {
+        const int cc = row >> 1, part = row & 1;
+        int N = 0;
+        while ((N + 1) * (N + 2) / 2 <= cc) N++;
+        const int M = cc - N * (N + 1) / 2;
+        const LgTerm t = c_lg_terms[v];
+        const int n = N - t.a;
+        if (n >= 0) {
+          const cplx* Y = Ys + (size_t)pt * nc;
+          const double sM = (M & 1) ? -1.0 : 1.0;
+          double yrd = 0, yid = 0, yrm = 0, yim = 0;
+          const int md = M - t.b, mm = -M - t.b;
+          if (md >= -n && md <= n) {
+            cplx y = hget(Y, n, md);
+            yrd = y.re; yid = y.im;
+          }
+          if (M > 0 && mm >= -n && mm <= n) {
+            cplx y = hget(Y, n, mm);
+            yrm = y.re; yim = y.im;
+          }
+          if (!t.im)
+            g = part == 0 ? yrd + sM * yrm : yid - sM * yim;
+          else
+            g = part == 0 ? -yid - sM * yim : yrd - sM * yrm;
+          g *= t.sg;
+        }
+      }
+      Gs[q] = g;
+    }
+    // B tile: rows k0.., columns col0..; FP32 normalised rows are rescaled by w
+    for (int q = tid; q < LG_K * LG_C; q += 256) {
+      const int kk = q % LG_K, col = q / LG_K;
+      const int row = k0 + kk, gcol = col0 + col;
+      double b = 0.0;
+      if (row < D && gcol < C) {
+        b = (double)Lb[(size_t)gcol * D + row];
+        if (wnorm) b *= wnorm[row];
+      }
+      Bs[kk * LG_C + col] = b;
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < LG_K; kk++) {
+      double gv[9], bv[8];
+#pragma unroll
+      for (int v = 0; v < 9; v++) gv[v] = Gs[(kk * LG_PTS + warp) * 9 + v];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const double* br = Bs + kk * LG_C + 128 * h + 4 * lane;
+        const double2 u0 = *reinterpret_cast<const double2*>(br);
+        const double2 u1 = *reinterpret_cast<const double2*>(br + 2);
+        bv[4 * h] = u0.x; bv[4 * h + 1] = u0.y; bv[4 * h + 2] = u1.x; bv[4 * h + 3] = u1.y;
+      }
+#pragma unroll
+      for (int v = 0; v < 9; v++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[v][j] += gv[v] * bv[j];
+    }
+  }
+  if (!ok) return;
+  const double c1 = a.c1;
+  const bool dostrain = is_src ? a.dostrain_src : a.dostrain_tgt;
+  const size_t np = is_src ? a.nsrc : a.ntgt;
+#pragma unroll
+  for (int h = 0; h < 2; h++) {
+    const int r = (col0 >> 2) + 32 * h + lane;
+    if (r >= R) continue;
+    double pot[4], g[4][3], H[4][3][3];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int j = 4 * h + q;
+      pot[q] = acc[0][j];
+      g[q][0] = acc[3][j] * is;
+      g[q][1] = acc[4][j] * is;
+      g[q][2] = acc[1][j] * is;
+      const double hzz = acc[2][j];
+      const double hxx = 0.5 * (acc[7][j] - hzz), hyy = 0.5 * (-acc[7][j] - hzz), hxy = 0.5 * acc[8][j];
+      const double hxz = acc[5][j], hyz = acc[6][j];
+      H[q][0][0] = hxx * is2; H[q][1][1] = hyy * is2; H[q][2][2] = hzz * is2;
+      H[q][0][1] = H[q][1][0] = hxy * is2;
+      H[q][0][2] = H[q][2][0] = hxz * is2;
+      H[q][1][2] = H[q][2][1] = hyz * is2;
+    }
+    double u[3];
+    for (int i = 0; i < 3; i++) {
+      u[i] = (2.0 - c1) * pot[i] + g[3][i];
+      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+    }
+    double* U = (is_src ? a.u_src : a.u_tgt) + 3 * (np * r + pidx);
+    U[0] += u[0];
+    U[1] += u[1];
+    U[2] += u[2];
+    if (dostrain) {
+      double G[3][3];
+      for (int aa = 0; aa < 3; aa++)
+        for (int bb = 0; bb < 3; bb++) {
+          double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
+          for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+          G[aa][bb] = v;
+        }
+      double* E = (is_src ? a.e_src : a.e_tgt) + 6 * (np * r + pidx);
+      E[0] += G[0][0];
+      E[1] += G[1][1];
+      E[2] += G[2][2];
+      E[3] += 0.5 * (G[0][1] + G[1][0]);
+      E[4] += 0.5 * (G[0][2] + G[2][0]);
+      E[5] += 0.5 * (G[1][2] + G[2][1]);
+    }
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp) {
   if (nop <= 0) return;
@@ -485,14 +864,49 @@ void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats,
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
-void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a) {
+void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs) {
   if (nleaf <= 0) return;
   size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 16 * P2M_NODES);
   if (smem > 48 * 1024)
     EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_p2m<<<nleaf, P2M_THREADS, smem, st>>>(a); count_launch();
+  k_p2m<<<dim3(nleaf, nrhs), P2M_THREADS, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+
+template <class TB>
+bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
+                     int R, const TB* local, const double* wnorm) {
+  const int nc = ncoef(a.p);
+  size_t smem = sizeof(cplx) * LG_PTS * nc + sizeof(double) * (LG_K * LG_PTS * 9 + LG_K * LG_C);
+  if (smem > 227 * 1024) return false;
+  if (nchunk <= 0 || R <= 0) return true;
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_gemm<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(nchunk, (4 * R + LG_C - 1) / LG_C);
+  k_l2t_gemm<TB><<<grid, 256, smem, st>>>(a, chunk_leaf, chunk_e0, R, local, wnorm); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+  return true;
+}
+template bool launch_l2t_gemm<double>(cudaStream_t, int, const int*, const int*, const L2TArgs&, int,
+                                      const double*, const double*);
+template bool launch_l2t_gemm<float>(cudaStream_t, int, const int*, const int*, const L2TArgs&, int,
+                                     const float*, const double*);
+
+template <class T>
+bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpole) {
+  const int nc = ncoef(a.p), D = 2 * nc, C = 4 * R;
+  size_t smem = sizeof(cplx) * PG_NODES * nc + sizeof(double) * PG_NODES * 8 + sizeof(int) * (PG_NODES + 2) +
+                sizeof(T) * PG_K * (PG_R + PG_C);
+  smem = (smem + 15) / 16 * 16;
+  if (smem > 227 * 1024) return false;  // high orders: the caller uses k_p2m
+  if (nleaf <= 0 || R <= 0) return true;
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_gemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  dim3 grid(nleaf, (D + PG_R - 1) / PG_R, (C + PG_C - 1) / PG_C);
+  k_p2m_gemm<T><<<grid, 256, smem, st>>>(a, R, mpole); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+  return true;
+}
+template bool launch_p2m_gemm<double>(cudaStream_t, int, const P2MArgs&, int, double*);
+template bool launch_p2m_gemm<float>(cudaStream_t, int, const P2MArgs&, int, float*);
 
 template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
@@ -515,7 +929,7 @@ template void launch_translate<double>(cudaStream_t, int, const TransTask*, cons
 template void launch_translate<float>(cudaStream_t, int, const TransTask*, const TransPair*, const float*,
                                       const long long*, const int*, int, int, const float*, float*);
 
-void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a) {
+void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs) {
   if (nleaf <= 0) return;
   int nw = L2T_WARPS;
   auto need = [&](int w) {
@@ -525,7 +939,7 @@ void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a) {
   size_t smem = need(nw);
   if (smem > 48 * 1024)
     EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_l2t<<<nleaf, nw * 32, smem, st>>>(a); count_launch();
+  k_l2t<<<dim3(nleaf, nrhs), nw * 32, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 

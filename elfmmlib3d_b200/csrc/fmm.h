@@ -31,6 +31,12 @@ struct P2MArgs {
   int dosl, dodl, p;
   double c1, c2, inv2mu;
   double* mpole;
+  // right-hand side r = blockIdx.y: density component d of triangle t at
+  // ssl/sdl[r * rstride + t * tstride + d * dstride]; expansion columns
+  // 4r..4r+3 of C per box
+  int C = 4;
+  long long rstride = 0, tstride = 3, dstride = 1;
+  const double* wnorm = nullptr;  // product form: rows scaled by wnorm[row] if set
 };
 
 struct L2TArgs {
@@ -42,14 +48,29 @@ struct L2TArgs {
   int p, do_src, do_tgt, dostrain_src, dostrain_tgt;
   double c1;
   double *u_src, *e_src, *u_tgt, *e_tgt;
+  // right-hand side blockIdx.y: expansion columns 4r..4r+3 of C per box,
+  // outputs at r * (3 or 6) * (number of sources or targets)
+  int C = 4;
+  long long nsrc = 0, ntgt = 0;
 };
 
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);
-void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a);
+void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs = 1);
+// P2M of R right-hand sides as a product (columns 4R per box); writes mpole
+// (T = double, or float for the mixed-precision form).  Returns false (and
+// launches nothing) when the order is too high for its shared-memory tiles.
+template <class T>
+bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpole);
+// L2T of R right-hand sides as a product over (chunks of 8 points of a leaf,
+// 256 columns); local (boxes, 4R, D) in TB (float: normalised basis, rows
+// rescaled by wnorm).  Returns false when the order is too high.
+template <class TB>
+bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
+                     int R, const TB* local, const double* wnorm);
 template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                       const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,
                       const T* src, T* dst);
-void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a);
+void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs = 1);
 
 }  // namespace efmm

@@ -290,6 +290,125 @@ k_near_replay(const NearArgs a, const long long* __restrict__ base, const int* _
   }
 }
 
+// Many right-hand sides at once (densities tree order, right-hand side
+// innermost: sigma[(tri * 3 + component) * R + r]).  The pair response to unit densities
+// (pair_blocks, as stored by the ITER mode) does not depend on the densities,
+// so it is computed once per (point, triangle) pair and contracted with all
+// R right-hand sides: per tile of NB_PTS points x NB_TRI triangles, phase 1
+// writes the pair blocks to shared memory (one pair per thread), phase 2 is a
+// small dense product  out[point][9][R] += block[point][tri][9 x 6] *
+// sigma[tri][6][R]  with the outputs held in registers (9 x RB per thread;
+// R <= 16 RB).  One CTA per (near leaf, chunk of NB_PTS evaluation points).
+constexpr int NB_PTS = 8, NB_TRI = 16, NB_THREADS = NB_PTS * NB_TRI;
+
+template <int RB>
+__global__ void __launch_bounds__(NB_THREADS)
+k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __restrict__ chunk_e0,
+             int R, int K, int dostrain, const double* __restrict__ ssl, const double* __restrict__ sdl,
+             int ntri_all, int nsrc, int ntgt) {
+  constexpr int RW = 16 * RB;  // right-hand sides held per tile
+  __shared__ TriRec tile[NB_TRI];
+  extern __shared__ __align__(16) double nb_sm[];
+  double* Bk = nb_sm;                            // [NB_PTS][NB_TRI][K]
+  double* Sg = Bk + NB_PTS * NB_TRI * K;         // [NB_TRI][6][RW]
+  const int li = chunk_leaf[blockIdx.x], e0 = chunk_e0[blockIdx.x];
+  const int leaf = a.leaves[li];
+  const int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int t0 = a.box_tgt_start[leaf], tn = a.do_tgt ? a.box_tgt_count[leaf] : 0;
+  const int nep = sn + tn;
+  const int tid = threadIdx.x;
+  const int pp = tid / NB_TRI, tt = tid % NB_TRI;  // phase 1: (point, triangle)
+  const int rr = tid % 16, pq = tid / 16;          // phase 2: (point, rhs lane)
+  // phase-1 point
+  const int e1 = e0 + pp;
+  const bool ok1 = e1 < nep;
+  const bool src1 = e1 < sn;
+  const int pid1 = ok1 ? (src1 ? s0 + e1 : t0 + (e1 - sn)) : 0;
+  double X[3] = {0, 0, 0};
+  if (ok1) {
+    const double* P = src1 ? a.src_pts + 3 * (size_t)pid1 : a.tgt_pts + 3 * (size_t)pid1;
+    X[0] = P[0]; X[1] = P[1]; X[2] = P[2];
+  }
+  double acc[9][RB];
+#pragma unroll
+  for (int c = 0; c < 9; c++)
+#pragma unroll
+    for (int k = 0; k < RB; k++) acc[c][k] = 0.0;
+  const int nl = a.dosl + a.dodl;
+  for (int b = a.nb_start[li]; b < a.nb_start[li + 1]; b++) {
+    const int sb = a.nb_items[b];
+    const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+    for (int k0 = 0; k0 < trn; k0 += NB_TRI) {
+      const int cnt = min(NB_TRI, trn - k0);
+      __syncthreads();
+      stage_tile(tile, a.trir + tr0 + k0, cnt);
+      for (int q = tid; q < NB_TRI * 6 * RW; q += NB_THREADS) {
+        int t = q / (6 * RW), j = (q / RW) % 6, r = q % RW;
+        int layer = j / 3, d = j % 3;
+        double v = 0.0;
+        if (t < cnt && r < R && (layer == 0 ? a.dosl : a.dodl)) {
+          const double* sg = layer == 0 ? ssl : sdl;
+          v = sg[((size_t)(tr0 + k0 + t) * 3 + d) * R + r];
+        }
+        Sg[q] = v;
+      }
+      __syncthreads();
+      {
+        double* o = Bk + (pp * NB_TRI + tt) * K;
+        if (ok1 && tt < cnt) {
+          const int tidx = tr0 + k0 + tt;
+          pair_blocks(tile[tt].f, a.dosl, a.dodl, true, dostrain, X, src1 && tidx == pid1, a.rlam, a.rmu, o);
+        } else {
+          for (int q = 0; q < K; q++) o[q] = 0.0;
+        }
+      }
+      __syncthreads();
+      for (int t = 0; t < cnt; t++) {
+        const double* Bt = Bk + (pq * NB_TRI + t) * K;
+        int w = 0;
+        for (int j = 0; j < 6; j++) {
+          if ((j < 3 && !a.dosl) || (j >= 3 && !a.dodl)) continue;
+          double sv[RB];
+#pragma unroll
+          for (int k = 0; k < RB; k++) sv[k] = Sg[(t * 6 + j) * RW + rr + 16 * k];
+#pragma unroll
+          for (int c = 0; c < 3; c++)
+#pragma unroll
+            for (int k = 0; k < RB; k++) acc[c][k] += Bt[w + c] * sv[k];
+          w += 3;
+          if (dostrain) {
+#pragma unroll
+            for (int c = 0; c < 6; c++)
+#pragma unroll
+              for (int k = 0; k < RB; k++) acc[3 + c][k] += Bt[w + c] * sv[k];
+            w += 6;
+          }
+        }
+      }
+    }
+  }
+  (void)nl;
+  const int e2 = e0 + pq;
+  if (e2 >= nep) return;
+  const bool src2 = e2 < sn;
+  const int pid2 = src2 ? s0 + e2 : t0 + (e2 - sn);
+  const size_t np = src2 ? (size_t)nsrc : (size_t)ntgt;
+  const bool ds2 = src2 ? a.dostrain_src : a.dostrain_tgt;
+#pragma unroll
+  for (int k = 0; k < RB; k++) {
+    const int r = rr + 16 * k;
+    if (r >= R) continue;
+    double* U = (src2 ? a.u_src : a.u_tgt) + 3 * (np * r + pid2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) U[c] += acc[c][k];
+    if (ds2) {
+      double* E = (src2 ? a.e_src : a.e_tgt) + 6 * (np * r + pid2);
+#pragma unroll
+      for (int c = 0; c < 6; c++) E[c] += acc[3 + c][k];
+    }
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out) {
@@ -316,6 +435,30 @@ void launch_near_replay(cudaStream_t st, const NearArgs& a, const long long* bas
                         int dodisp, const double* ssl, const double* sdl, const double* store) {
   if (a.nleaf <= 0) return;
   k_near_replay<<<a.nleaf, 256, 0, st>>>(a, base, ntri, K, dodisp, ssl, sdl, store); count_launch();
+}
+
+void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int* chunk_leaf,
+                       const int* chunk_e0, int R, int dostrain, const double* ssl, const double* sdl,
+                       int ntri_all, int nsrc, int ntgt) {
+  if (nchunk <= 0 || R <= 0) return;
+  if (R > 64) throw CudaError{(int)cudaErrorInvalidValue};
+  const int nl = a.dosl + a.dodl;
+  const int K = nl * 3 * (3 + 6 * dostrain);
+  const int RB = (R + 15) / 16;
+  const int smem = (int)(sizeof(double) * (NB_PTS * NB_TRI * K + NB_TRI * 6 * 16 * RB));
+  auto go = [&](auto kern) {
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    kern<<<nchunk, NB_THREADS, smem, st>>>(a, chunk_leaf, chunk_e0, R, K, dostrain, ssl, sdl, ntri_all, nsrc,
+                                           ntgt);
+    count_launch();
+  };
+  switch (RB) {
+    case 1: go(k_near_batch<1>); break;
+    case 2: go(k_near_batch<2>); break;
+    case 3: go(k_near_batch<3>); break;
+    default: go(k_near_batch<4>); break;
+  }
+  EFMM_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,

@@ -5,6 +5,8 @@
 #include <vector>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <cmath>
 #include "plan.h"
 
 namespace efmm {
@@ -49,7 +51,18 @@ __global__ void k_gather(int n, int w, const int* __restrict__ perm, const doubl
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int j = perm[i];
-  for (int c = 0; c < w; c++) out[(size_t)w * i + c] = in[(size_t)w * j + c];
+  size_t r = (size_t)blockIdx.y * w * n;  // right-hand side blockIdx.y
+  for (int c = 0; c < w; c++) out[r + (size_t)w * i + c] = in[r + (size_t)w * j + c];
+}
+// user (R, n, 3) -> tree order, right-hand side innermost: out[(i*3+d)*R + r]
+__global__ void k_gather_rhs(int n, int R, const int* __restrict__ perm, const double* __restrict__ in,
+                             double* __restrict__ out) {
+  long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= (long long)n * R) return;
+  int i = (int)(idx / R), r = (int)(idx % R);
+  int j = perm[i];
+  const double* src = in + 3 * ((size_t)r * n + j);
+  for (int d = 0; d < 3; d++) out[((size_t)i * 3 + d) * R + r] = src[d];
 }
 // tree order -> user order; strain 6 (xx yy zz xy xz yz) -> 3x3
 __global__ void k_scatter_out(int n, const int* __restrict__ perm, const double* __restrict__ u,
@@ -58,11 +71,12 @@ __global__ void k_scatter_out(int n, const int* __restrict__ perm, const double*
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int j = perm[i];
+  size_t r = (size_t)blockIdx.y * n;  // right-hand side blockIdx.y
   if (uo)
-    for (int c = 0; c < 3; c++) uo[3 * (size_t)j + c] = u[3 * (size_t)i + c];
+    for (int c = 0; c < 3; c++) uo[3 * (r + j) + c] = u[3 * (r + i) + c];
   if (eo) {
-    const double* s = e + 6 * (size_t)i;
-    double* o = eo + 9 * (size_t)j;
+    const double* s = e + 6 * (r + i);
+    double* o = eo + 9 * (r + j);
     o[0] = s[0]; o[4] = s[1]; o[8] = s[2];
     o[1] = o[3] = s[3];
     o[2] = o[6] = s[4];
@@ -78,6 +92,32 @@ __global__ void k_sym6to9(int n, const double* __restrict__ e, double* __restric
   o[1] = o[3] = s[3];
   o[2] = o[6] = s[4];
   o[5] = o[7] = s[5];
+}
+
+__global__ void k_d2f(size_t n, const double* __restrict__ in, float* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (float)in[i];
+}
+// normalised single-precision local expansions -> FP64 factorial basis
+__global__ void k_f2d_local(size_t n, int D, const double* __restrict__ w, const float* __restrict__ in,
+                            double* __restrict__ out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i] * w[i % D];
+}
+// operator g in the normalised basis: rows scaled by (M2M) w or (M2L, L2L) 1/w,
+// columns by (M2M, M2L) 1/w or (L2L) w
+__global__ void k_ops_normalised(const int* __restrict__ kinds, const long long* __restrict__ off,
+                                 const int* __restrict__ dims, const double* __restrict__ w,
+                                 const double* __restrict__ mats, float* __restrict__ out) {
+  const int g = blockIdx.x, kind = kinds[g], dim = dims[g];
+  const double* A = mats + off[g];
+  float* B = out + off[g];
+  for (long long q = threadIdx.x; q < (long long)dim * dim; q += blockDim.x) {
+    int i = (int)(q / dim), j = (int)(q % dim);
+    double si = kind == 1 ? w[i] : 1.0 / w[i];
+    double sj = kind == 2 ? w[j] : 1.0 / w[j];
+    B[q] = (float)(A[q] * si * sj);
+  }
 }
 
 // --------------------------------------------------------------- op pools
@@ -140,6 +180,16 @@ void Plan::ensure_ops() {
   launch_build_ops(st_, (int)descs.size(), dd.get(), P->mats.get(), p_);
   std::vector<long long> offs(descs.size());
   for (size_t i = 0; i < descs.size(); i++) offs[i] = descs[i].off;
+  std::vector<int> kinds(descs.size());
+  for (size_t i = 0; i < descs.size(); i++) kinds[i] = descs[i].kind;
+  P->kinds.resize(kinds.size());
+  EFMM_CUDA_TRY(cudaMemcpyAsync(P->kinds.get(), kinds.data(), kinds.size() * 4, cudaMemcpyHostToDevice, st_));
+  std::vector<double> wn(2 * (size_t)ncoef(p_));
+  for (int n = 0; n <= p_; n++)
+    for (int m = 0; m <= n; m++)
+      wn[2 * cidx(n, m)] = wn[2 * cidx(n, m) + 1] = std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  P->wnorm.resize(wn.size());
+  EFMM_CUDA_TRY(cudaMemcpyAsync(P->wnorm.get(), wn.data(), wn.size() * 8, cudaMemcpyHostToDevice, st_));
   P->off.resize(offs.size());
   P->dim.resize(P->dims.size());
   EFMM_CUDA_TRY(cudaMemcpyAsync(P->off.get(), offs.data(), offs.size() * 8, cudaMemcpyHostToDevice, st_));
@@ -192,10 +242,20 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   EFMM_CUDA_TRY(cudaMemcpyAsync(tri_u_.get(), d_tri, 72 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
   EFMM_CUDA_TRY(cudaMemcpyAsync(src_u_.get(), d_src, 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
   if (nt) EFMM_CUDA_TRY(cudaMemcpyAsync(tgt_u_.get(), d_tgt, 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
+  auto now = [&]() {
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+    return std::chrono::steady_clock::now();
+  };
+  auto ms = [](std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
+    return (float)std::chrono::duration<double, std::milli>(b - a).count();
+  };
+  auto t0 = now();
   int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_);
   if (ier) return ier;
+  auto t1 = now();
   ier = build_lists(st_, tr_);
   if (ier) return ier;
+  auto t2 = now();
   tri_s_.resize(9 * (size_t)n);
   nrm_s_.resize(3 * (size_t)n);
   src_s_.resize(3 * (size_t)n);
@@ -205,8 +265,13 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_src, src_s_.get()); count_launch();
   if (nt) { k_gather<<<(nt + 255) / 256, 256, 0, st_>>>(nt, 3, tr_.izt.get(), d_tgt, tgt_s_.get()); count_launch(); }
   build_worklists();
+  auto t3 = now();
   if (far_) ensure_ops();
-  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  auto t4 = now();
+  timings.geo_tree = ms(t0, t1);
+  timings.geo_lists = ms(t1, t2);
+  timings.geo_work = ms(t2, t3);
+  timings.geo_ops = ms(t3, t4);
   return IER_OK;
 }
 
@@ -262,6 +327,7 @@ void Plan::build_worklists() {
   }
   h2d(near_ntri_, near_ntri_h_, st_);
   store_valid_ = false;
+  chunk_key_ = -1;
   near_pairs_ = 0;
   {
     // count point pairs for the throughput model
@@ -291,6 +357,13 @@ void Plan::build_worklists() {
   if (p2m.empty()) far_ = false;
   np2m_ = (int)p2m.size();
   nl2t_ = (int)l2t.size();
+  l2t_sc_h_.clear();
+  l2t_tc_h_.clear();
+  for (int b : l2t) {
+    l2t_sc_h_.push_back(scount[b]);
+    l2t_tc_h_.push_back(tcount[b]);
+  }
+  lchunk_key_ = -1;
   h2d(p2m_leaves_, p2m, st_);
   h2d(l2t_leaves_, l2t, st_);
   m2m_.clear();
@@ -303,19 +376,19 @@ void Plan::build_worklists() {
   // group the pairs of one level by operator; one segment per group
   auto add_level = [&](std::vector<std::pair<int, TransPair>>& gp, std::vector<TransPair>& pairs,
                        TransSched& S) {
-    std::stable_sort(gp.begin(), gp.end(),
-                     [](const std::pair<int, TransPair>& a, const std::pair<int, TransPair>& b) {
-                       return a.first < b.first;
-                     });
+    // stable counting sort by operator group
+    int ng = 0;
+    for (auto& e : gp) ng = std::max(ng, e.first + 1);
+    std::vector<int> cnt(ng + 1, 0);
+    for (auto& e : gp) cnt[e.first + 1]++;
+    for (int g = 0; g < ng; g++) cnt[g + 1] += cnt[g];
+    size_t base = pairs.size();
+    pairs.resize(base + gp.size());
+    std::vector<int> pos(cnt.begin(), cnt.end() - 1);
+    for (auto& e : gp) pairs[base + pos[e.first]++] = e.second;
     int s0 = (int)S.segs.size();
-    size_t i = 0;
-    while (i < gp.size()) {
-      size_t j = i;
-      while (j < gp.size() && gp[j].first == gp[i].first) j++;
-      S.segs.push_back({gp[i].first, (int)pairs.size(), (int)(j - i)});
-      for (size_t q = i; q < j; q++) pairs.push_back(gp[q].second);
-      i = j;
-    }
+    for (int g = 0; g < ng; g++)
+      if (cnt[g + 1] > cnt[g]) S.segs.push_back({g, (int)(base + cnt[g]), cnt[g + 1] - cnt[g]});
     S.lev.push_back({s0, (int)S.segs.size() - s0});
   };
   m2m_.clear();
@@ -454,6 +527,8 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
   int D = 2 * ncoef(p_);
   if (far_ && do_far && (do_src || do_tgt)) {
+    mpole_.resize((size_t)tr_.nboxes * 4 * D);
+    local_.resize((size_t)tr_.nboxes * 4 * D);
     mpole_.zero(st_);
     local_.zero(st_);
     P2MArgs pa;
@@ -545,9 +620,240 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   return IER_OK;
 }
 
+void Plan::flops_per_column(double* f) const {
+  for (int i = 0; i < 5; i++) f[i] = 0;
+  if (!far_ || !ops_) return;
+  const double D = 2.0 * ncoef(p_);
+  const long long nodes = 12LL * n_;
+  f[0] = 2.0 * D * 4.0 * (double)nodes;  // rows x (charge + 3 dipole) per node
+  const TransSched* S[3] = {&m2m_, &m2l_, &l2l_};
+  for (int k = 0; k < 3; k++)
+    for (const TransSeg& g : S[k]->segs) {
+      double dim = ops_->dims[g.group];
+      f[1 + k] += 2.0 * dim * dim * g.npair;
+    }
+  f[4] = 2.0 * D * 9.0 * (double)(n_ + nt_);  // 9 derivative sums per point
+}
+
+int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                         double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision) {
+  if (R < 1 || precision < 0 || precision > 1) return IER_BADARG;
+  const int n = n_, nt = nt_;
+  const int D = 2 * ncoef(p_);
+  const size_t nb = tr_.nboxes;
+  // right-hand sides per pass: at most 64 (near-field kernel), and the
+  // expansions (2 x boxes x 4 rc x D doubles) within half the free memory
+  int Rc = std::min(R, 64);
+  if (far_) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    double have = 0.5 * (double)freeb + 8.0 * (double)(mpole_.cap + local_.cap);
+    while (Rc > 1 && 16.0 * nb * 4 * Rc * D > have) Rc /= 2;
+  }
+  float tot = 0, near = 0, far = 0;
+  for (int r0 = 0; r0 < R; r0 += Rc) {
+    const int rc = std::min(Rc, R - r0);
+    int ier = batch_pass(rlam, rmu, rc, d_ssl ? d_ssl + 3 * (size_t)n * r0 : nullptr,
+                         d_sdl ? d_sdl + 3 * (size_t)n * r0 : nullptr,
+                         d_u_src ? d_u_src + 3 * (size_t)n * r0 : nullptr,
+                         d_e_src ? d_e_src + 9 * (size_t)n * r0 : nullptr,
+                         d_u_tgt ? d_u_tgt + 3 * (size_t)nt * r0 : nullptr,
+                         d_e_tgt ? d_e_tgt + 9 * (size_t)nt * r0 : nullptr, precision == 1);
+    if (ier) return ier;
+    tot += timings.total;
+    near += timings.near;
+    far += timings.p2m + timings.m2m + timings.m2l + timings.l2l + timings.l2t;
+  }
+  timings.total = tot;
+  return IER_OK;
+}
+
+int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                     double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed) {
+  const int n = n_, nt = nt_;
+  const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+  const int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
+  const int ds_src = d_e_src ? 1 : 0, ds_tgt = d_e_tgt ? 1 : 0;
+  const int D = 2 * ncoef(p_);
+  const size_t nb = tr_.nboxes;
+  long long launch0 = launches_total();
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  ssl_s_.resize(3 * (size_t)n * R);
+  sdl_s_.resize(3 * (size_t)n * R);
+  const int gb = (int)(((long long)n * R + 255) / 256);
+  if (dosl) { k_gather_rhs<<<gb, 256, 0, st_>>>(n, R, tr_.iz.get(), d_ssl, ssl_s_.get()); count_launch(); }
+  if (dodl) { k_gather_rhs<<<gb, 256, 0, st_>>>(n, R, tr_.iz.get(), d_sdl, sdl_s_.get()); count_launch(); }
+  u_s_.resize(3 * (size_t)n * R);
+  e_s_.resize(6 * (size_t)n * R);
+  ut_s_.resize(3 * (size_t)std::max(nt, 1) * R);
+  et_s_.resize(6 * (size_t)std::max(nt, 1) * R);
+  u_s_.zero(st_);
+  e_s_.zero(st_);
+  ut_s_.zero(st_);
+  et_s_.zero(st_);
+  const double c1 = (rlam + rmu) / (rlam + 2 * rmu), c2 = rmu / (rlam + 2 * rmu);
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  const int C = 4 * R;
+  if (far_ && (do_src || do_tgt)) {
+    if (mixed) {
+      std::lock_guard<std::mutex> lk(g_ops_mu);
+      if (ops_->mats_f.size() != ops_->mats.size()) {
+        ops_->mats_f.resize(ops_->mats.size());
+        k_ops_normalised<<<(int)ops_->dims.size(), 256, 0, st_>>>(ops_->kinds.get(), ops_->off.get(),
+                                                                  ops_->dim.get(), ops_->wnorm.get(),
+                                                                  ops_->mats.get(), ops_->mats_f.get());
+        count_launch();
+        EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+      }
+      mpole_f_.resize(nb * C * D);
+      local_f_.resize(nb * C * D);
+      mpole_f_.zero(st_);
+      local_f_.zero(st_);
+    } else {
+      mpole_.resize(nb * C * D);
+      local_.resize(nb * C * D);
+      mpole_.zero(st_);
+      local_.zero(st_);
+    }
+    P2MArgs pa;
+    pa.leaves = p2m_leaves_.get();
+    pa.level = tr_.level.get(); pa.ijk = tr_.ijk.get();
+    pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
+    for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
+    pa.size = tr_.size;
+    pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
+    pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
+    pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
+    pa.mpole = mpole_.get();
+    pa.C = C; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
+    if (mixed) {
+      pa.wnorm = ops_->wnorm.get();  // multipoles in the normalised basis
+      if (!launch_p2m_gemm<float>(st_, np2m_, pa, R, mpole_f_.get())) return IER_BADARG;
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      run_translations(m2m_, C, ops_->mats_f.get(), mpole_f_.get(), mpole_f_.get());
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      run_translations(m2l_, C, ops_->mats_f.get(), mpole_f_.get(), local_f_.get());
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      run_translations(l2l_, C, ops_->mats_f.get(), local_f_.get(), local_f_.get());
+    } else {
+      // product form once the columns fill its tiles
+      if (C < 32 || !launch_p2m_gemm<double>(st_, np2m_, pa, R, mpole_.get())) launch_p2m(st_, np2m_, pa, R);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      run_translations(m2m_, C, ops_->mats.get(), mpole_.get(), mpole_.get());
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      run_translations(m2l_, C, ops_->mats.get(), mpole_.get(), local_.get());
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      run_translations(l2l_, C, ops_->mats.get(), local_.get(), local_.get());
+    }
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
+    L2TArgs la;
+    la.leaves = l2t_leaves_.get();
+    la.level = tr_.level.get(); la.ijk = tr_.ijk.get();
+    la.sstart = tr_.sstart.get(); la.scount = tr_.scount.get();
+    la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
+    for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
+    la.size = tr_.size;
+    la.local = local_.get();
+    la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
+    la.p = p_; la.do_src = do_src; la.do_tgt = do_tgt;
+    la.dostrain_src = ds_src; la.dostrain_tgt = ds_tgt;
+    la.c1 = c1;
+    la.u_src = u_s_.get(); la.e_src = e_s_.get(); la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
+    la.C = C; la.nsrc = n; la.ntgt = nt;
+    // product form (chunks of 8 points of a leaf) once the columns fill its tiles
+    bool done = false;
+    if (C >= 32) {
+      const int key = do_src | (do_tgt << 1);
+      if (lchunk_key_ != key) {
+        std::vector<int> cl, ce;
+        for (size_t i = 0; i < l2t_sc_h_.size(); i++) {
+          int nep = (do_src ? l2t_sc_h_[i] : 0) + (do_tgt ? l2t_tc_h_[i] : 0);
+          for (int e0 = 0; e0 < nep; e0 += 8) {
+            cl.push_back((int)i);
+            ce.push_back(e0);
+          }
+        }
+        h2d(lchunk_leaf_, cl, st_);
+        h2d(lchunk_e0_, ce, st_);
+        nlchunk_ = (int)cl.size();
+        lchunk_key_ = key;
+      }
+      done = mixed ? launch_l2t_gemm<float>(st_, nlchunk_, lchunk_leaf_.get(), lchunk_e0_.get(), la, R,
+                                            local_f_.get(), ops_->wnorm.get())
+                   : launch_l2t_gemm<double>(st_, nlchunk_, lchunk_leaf_.get(), lchunk_e0_.get(), la, R,
+                                             local_.get(), nullptr);
+    }
+    if (!done) {
+      if (mixed) {
+        local_.resize(nb * C * D);
+        k_f2d_local<<<1184, 256, 0, st_>>>(local_f_.size(), D, ops_->wnorm.get(), local_f_.get(), local_.get());
+        count_launch();
+      }
+      launch_l2t(st_, nl2t_, la, R);
+    }
+  } else {
+    for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
+  // near field: frames only (densities enter the batched contraction)
+  trir_.resize(n);
+  launch_tri_prep(st_, n, tri_s_.get(), nullptr, nullptr, nullptr, 0, 0, trir_.get());
+  const int key = do_src | (do_tgt << 1);
+  if (chunk_key_ != key) {
+    std::vector<int> cl, ce;
+    for (size_t i = 0; i < near_sc_h_.size(); i++) {
+      int nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+      for (int e0 = 0; e0 < nep; e0 += 8) {
+        cl.push_back((int)i);
+        ce.push_back(e0);
+      }
+    }
+    h2d(chunk_leaf_, cl, st_);
+    h2d(chunk_e0_, ce, st_);
+    nchunk_ = (int)cl.size();
+    chunk_key_ = key;
+  }
+  NearArgs na;
+  na.nleaf = nnear_;
+  na.leaves = near_leaves_.get(); na.nb_start = near_start_.get(); na.nb_items = near_items_.get();
+  na.box_src_start = tr_.sstart.get(); na.box_src_count = tr_.scount.get();
+  na.box_tgt_start = tr_.tstart.get(); na.box_tgt_count = tr_.tcount.get();
+  na.trir = trir_.get();
+  na.src_pts = src_s_.get(); na.tgt_pts = tgt_s_.get();
+  na.dosl = dosl; na.dodl = dodl; na.dostrain_src = ds_src; na.dostrain_tgt = ds_tgt;
+  na.do_src = do_src; na.do_tgt = do_tgt;
+  na.rlam = rlam; na.rmu = rmu;
+  na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
+  if (dosl || dodl)
+    launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, (ds_src || ds_tgt) ? 1 : 0,
+                      ssl_s_.get(), sdl_s_.get(), n, n, nt);
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
+  if (do_src) {
+    k_scatter_out<<<dim3((n + 255) / 256, R), 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src,
+                                                              d_e_src); count_launch();
+  }
+  if (do_tgt) {
+    k_scatter_out<<<dim3((nt + 255) / 256, R), 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(),
+                                                               d_u_tgt, d_e_tgt); count_launch();
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+  EFMM_CUDA_TRY(cudaGetLastError());
+  EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
+  cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
+  cudaEventElapsedTime(&timings.prep, ev_[0], ev_[1]);
+  cudaEventElapsedTime(&timings.p2m, ev_[1], ev_[2]);
+  cudaEventElapsedTime(&timings.m2m, ev_[2], ev_[3]);
+  cudaEventElapsedTime(&timings.m2l, ev_[3], ev_[4]);
+  cudaEventElapsedTime(&timings.l2l, ev_[4], ev_[5]);
+  cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
+  cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
+  launches_ = (int)(launches_total() - launch0);
+  return IER_OK;
+}
+
 int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,
-                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt) {
-  int n = n_, nt = nt_;
+                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int nsub) {
+  int n = n_, nt = nsub > 0 ? 0 : nt_;
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   trir_.resize(n);
   launch_tri_prep(st_, n, tri_u_.get(), nullptr, d_ssl, d_sdl, dosl, dodl, trir_.get());
@@ -559,15 +865,16 @@ int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const do
   e_s_.zero(st_);
   ut_s_.zero(st_);
   et_s_.zero(st_);
-  int do_src = (d_u_src || d_e_src) ? n : 0;
+  int do_src = (d_u_src || d_e_src) ? (nsub > 0 ? std::min(nsub, n) : n) : 0;
   int do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? nt : 0;
+  const int ns = nsub > 0 ? std::min(nsub, n) : n;
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
   launch_direct_all(st_, n, trir_.get(), do_src, src_u_.get(), do_tgt, tgt_u_.get(), dosl, dodl,
                     d_e_src ? 1 : 0, d_e_tgt ? 1 : 0, rlam, rmu, u_s_.get(), e_s_.get(), ut_s_.get(),
                     et_s_.get());
   EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
-  if (d_u_src) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_src, u_s_.get(), 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
-  if (d_e_src) { k_sym6to9<<<(n + 255) / 256, 256, 0, st_>>>(n, e_s_.get(), d_e_src); count_launch(); }
+  if (d_u_src) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_src, u_s_.get(), 24 * (size_t)ns, cudaMemcpyDeviceToDevice, st_));
+  if (d_e_src) { k_sym6to9<<<(ns + 255) / 256, 256, 0, st_>>>(ns, e_s_.get(), d_e_src); count_launch(); }
   if (nt && d_u_tgt) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_tgt, ut_s_.get(), 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
   if (nt && d_e_tgt) { k_sym6to9<<<(nt + 255) / 256, 256, 0, st_>>>(nt, et_s_.get(), d_e_tgt); count_launch(); }
   EFMM_CUDA_TRY(cudaGetLastError());

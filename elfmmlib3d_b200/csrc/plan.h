@@ -18,6 +18,13 @@ struct OpPool {
   int p = -1;
   double eps = -1;
   DevBuf<double> mats;
+  // Mixed-precision form: operators in the normalised basis (multipole
+  // coefficients x w, local coefficients / w, w(n,m) = sqrt((n+m)!(n-m)!)),
+  // where regular and irregular harmonics are O(1) and FP32 neither
+  // overflows nor underflows; made on first use.
+  DevBuf<float> mats_f;
+  DevBuf<double> wnorm;   // w per real row (2 ncoef(p))
+  DevBuf<int> kinds;      // operator kind per group (0 M2L, 1 M2M, 2 L2L)
   DevBuf<long long> off;
   DevBuf<int> dim;
   int m2l_group[343];
@@ -27,6 +34,8 @@ struct OpPool {
 
 struct Timings {  // milliseconds of the last evaluate(), CUDA events
   float total = 0, p2m = 0, m2m = 0, m2l = 0, l2l = 0, l2t = 0, near = 0, prep = 0;
+  // last set_geometry(), host wall clock: tree, lists, work lists (+ gathers), operators
+  float geo_tree = 0, geo_lists = 0, geo_work = 0, geo_ops = 0;
 };
 
 // Translation schedule of one kind (M2M, M2L or L2L): pairs sorted by
@@ -67,9 +76,21 @@ class Plan {
                double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode = 0, bool do_far = true);
   long long stored_doubles() const { return store_valid_ ? (long long)store_.size() : 0; }
   bool store_valid() const { return store_valid_; }
+  // R right-hand sides at once: densities (R, n, 3) user order, outputs
+  // (R, n, 3) / (R, n, 3, 3) / (R, nt, 3) / (R, nt, 3, 3) user order.  The
+  // tree, lists and operators are shared; the near-field pair responses are
+  // computed once and contracted with all right-hand sides.
+  // precision 0: FP64 throughout; 1: mixed (P2M products and translations
+  // in FP32 with FP32 expansions, everything else FP64).
+  int evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                     double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt,
+                     int precision = 0);
+  // useful flops per expansion column of one pass: P2M, M2M, M2L, L2L, L2T
+  void flops_per_column(double* f5) const;
   // all-pairs direct sum on the same geometry (no tree needed)
+  // nsub > 0: only the first nsub source points (centroids), no targets
   int evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,
-                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt);
+                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int nsub = 0);
   cudaStream_t stream() const { return st_; }
   const Tree& tree() const { return tr_; }
   Timings timings;
@@ -84,6 +105,14 @@ class Plan {
 
  private:
   void build_worklists();
+  int batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                 double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed);
+  DevBuf<float> mpole_f_, local_f_;
+  DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA
+  int nchunk_ = 0, chunk_key_ = -1;
+  std::vector<int> l2t_sc_h_, l2t_tc_h_;  // per L2T leaf
+  DevBuf<int> lchunk_leaf_, lchunk_e0_;   // (L2T leaf index, first point) per product-form L2T CTA
+  int nlchunk_ = 0, lchunk_key_ = -1;
   void ensure_ops();
   int dev_;
   cudaStream_t st_;

@@ -122,6 +122,30 @@ int efmm_plan_evaluate(efmm_plan *plan, double rlam, double rmu, const double *s
                        const double *sdl, double *u_src, double *e_src, double *u_tgt,
                        double *e_tgt);
 
+/* nrhs right-hand sides in one pass (no counterpart in the reference, which
+ * takes one density pair per call): ssl/sdl (nrhs,n,3), outputs
+ * u_src (nrhs,n,3), e_src (nrhs,n,3,3), u_tgt (nrhs,nt,3), e_tgt (nrhs,nt,3,3),
+ * device pointers, NULL disables as in efmm_plan_evaluate.  The near-field
+ * pair responses are computed once for all right-hand sides and the
+ * P2M and translations run as products over boxes x passes x right-hand
+ * sides.  precision 0: FP64 throughout, the same results as nrhs calls of
+ * efmm_plan_evaluate; precision 1: mixed, P2M products, expansions and
+ * translations in FP32, near field and local evaluation in FP64. */
+int efmm_plan_evaluate_batch(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
+                             const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                             double *e_tgt, int precision);
+
+/* Useful flops per expansion column (one Laplace pass of one right-hand
+ * side) of the current geometry: P2M, M2M, M2L, L2L, L2T. */
+void efmm_plan_flops(const efmm_plan *plan, double *f5);
+
+/* Direct sum at the first nsub source points only (centroids 0..nsub-1,
+ * self-aware), outputs u_src (nsub,3), e_src (nsub,3,3): the FP64 check of a
+ * large evaluation on a subset. */
+int efmm_plan_evaluate_direct_subset(efmm_plan *plan, double rlam, double rmu, int nsub,
+                                     const double *ssl, const double *sdl, double *u_src,
+                                     double *e_src);
+
 /* Same outputs from the all-pairs direct sum on the plan's geometry. */
 int efmm_plan_evaluate_direct(efmm_plan *plan, double rlam, double rmu, const double *ssl,
                               const double *sdl, double *u_src, double *e_src, double *u_tgt,
@@ -157,6 +181,10 @@ int efmm_direct_noalloc(double rlam, double rmu, int n, const double *tri, const
 /* Per-stage device times (ms) of the last evaluate: total, prep, p2m, m2m,
  * m2l, l2l, l2t, near. */
 void efmm_plan_timings(const efmm_plan *plan, float *ms8);
+
+/* Host wall-clock ms of the last set_geometry: tree, lists, work lists
+ * (with the tree-order gathers), translation operators. */
+void efmm_plan_setup_timings(const efmm_plan *plan, float *ms4);
 
 /* info[0..7] = nboxes, nlev, expansion order p, leaf capacity nbox,
  * near-field point pairs, M2L box pairs, kernels launched by the last

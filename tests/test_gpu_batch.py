@@ -1,0 +1,119 @@
+"""Many right-hand sides in one pass (efmm_plan_evaluate_batch) against the
+same number of single evaluations on the same plan, and against the direct
+sum at the iprec tolerance."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from elfmmlib3d_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+# the batched pass reorders the same FP64 sums (pair blocks x densities,
+# wider translation tiles)
+SAME = 1e-12
+
+
+def _t():
+    import torch
+    return torch
+
+
+def _plan(gpu, level=3, ntarg=120, iprec=2, seed=0):
+    torch = _t()
+    tri, nrm, cen = G.sphere_triangles(level)
+    tg = G.box_targets(ntarg, 21 + seed)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    P = gpu.Plan(0)
+    P.set_geometry(d(tri), d(nrm), d(cen), d(tg), iprec=iprec)
+    return P, tri, nrm, cen, tg, d
+
+
+def _single(P, d, ssl, sdl, n, m, strain=True):
+    torch = _t()
+    R = ssl.shape[0] if ssl is not None else sdl.shape[0]
+    out = [np.zeros((R, n, 3)), np.zeros((R, n, 3, 3)), np.zeros((R, m, 3)), np.zeros((R, m, 3, 3))]
+    for r in range(R):
+        u = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+        e = torch.zeros((n, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+        ut = torch.zeros((m, 3), dtype=torch.float64, device="cuda")
+        et = torch.zeros((m, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+        P.evaluate(1.3, 0.7, d(ssl[r]) if ssl is not None else None, d(sdl[r]) if sdl is not None else None,
+                   u, e, ut, et)
+        out[0][r], out[2][r] = u.cpu().numpy(), ut.cpu().numpy()
+        if strain:
+            out[1][r], out[3][r] = e.cpu().numpy(), et.cpu().numpy()
+    return out
+
+
+def _batch(P, d, R, ssl, sdl, n, m, strain=True):
+    torch = _t()
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device="cuda")
+    e = torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    ut = torch.zeros((R, m, 3), dtype=torch.float64, device="cuda")
+    et = torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    P.evaluate_batch(1.3, 0.7, R, d(ssl) if ssl is not None else None, d(sdl) if sdl is not None else None,
+                     u, e, ut, et)
+    return [u.cpu().numpy(), e.cpu().numpy() if strain else None, ut.cpu().numpy(),
+            et.cpu().numpy() if strain else None]
+
+
+@pytest.mark.parametrize("R", [1, 5, 37, 70])
+def test_batch_equals_single_evaluations(gpu, R):
+    P, tri, nrm, cen, tg, d = _plan(gpu, seed=R)
+    n, m = len(cen), len(tg)
+    rng = np.random.default_rng(R)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, sdl, n, m)
+    b = _single(P, d, ssl, sdl, n, m)
+    for x, y in zip(a, b):
+        assert rel(x, y) < SAME
+    P.close()
+
+
+def test_batch_single_layer_without_strain(gpu):
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=2, ntarg=50, iprec=1, seed=3)
+    n, m = len(cen), len(tg)
+    R = 20
+    ssl = np.random.default_rng(9).normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, None, n, m, strain=False)
+    b = _single(P, d, ssl, None, n, m, strain=False)
+    assert rel(a[0], b[0]) < SAME and rel(a[2], b[2]) < SAME
+    P.close()
+
+
+def test_batch_within_tolerance_of_direct(gpu):
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=3, ntarg=100, iprec=2, seed=5)
+    n, m = len(cen), len(tg)
+    R = 3
+    rng = np.random.default_rng(11)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, sdl, n, m)
+    for r in range(R):
+        dd = gpu.el3dtriadirecttarg(1.3, 0.7, tri, nrm, cen, ssl[r], sdl[r], tg)
+        assert rel(a[0][r], dd[0]) < 1e-6 and rel(a[2][r], dd[2]) < 1e-6
+        assert rel(a[1][r], dd[1]) < 1e-5 and rel(a[3][r], dd[3]) < 1e-5
+    P.close()
+
+
+def test_batch_mixed_precision_error(gpu):
+    # mixed form: FP32 expansions and translations; its error against the
+    # FP64 form stays within the iprec-2 tolerance (relative l2)
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=4, ntarg=300, iprec=2, seed=7)
+    n, m = len(cen), len(tg)
+    R = 8
+    rng = np.random.default_rng(13)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, sdl, n, m)
+    torch = _t()
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device="cuda")
+    e = torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda")
+    ut = torch.zeros((R, m, 3), dtype=torch.float64, device="cuda")
+    et = torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda")
+    P.evaluate_batch(1.3, 0.7, R, d(ssl), d(sdl), u, e, ut, et, precision=1)
+    b = [u.cpu().numpy(), e.cpu().numpy(), ut.cpu().numpy(), et.cpu().numpy()]
+    assert rel(b[0], a[0]) < 0.5e-6 and rel(b[2], a[2]) < 0.5e-6
+    assert rel(b[1], a[1]) < 0.5e-5 and rel(b[3], a[3]) < 0.5e-5
+    # and the FP32 parts do change the result (the mixed path ran)
+    assert rel(b[0], a[0]) > 1e-13
+    P.close()
