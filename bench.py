@@ -1,21 +1,36 @@
 """Benchmark: triangle-evaluations per second of the elastostatic layer-potential
 FMM on one or more B200s.
 
-A step is one complete elfmm3dtriatarg evaluation (tree + lists + four-pass
-Laplace far field + analytic near field) of the workload below, with inputs
-resident in device memory; `e2e` runs the same evaluation through the
-reference-compatible C ABI (elfmm3dtriatarg_) from pinned host buffers, host
-copies included.  One triangle-evaluation = one (evaluation point, source
-triangle) interaction; the evaluation points are the centroids plus the
-off-surface targets (elhfmm3dtria_self_iter_dr.f:270 counts the same product).
+One triangle-evaluation = one (evaluation point, source triangle, right-hand
+side) interaction (elhfmm3dtria_self_iter_dr.f:270 counts points x triangles;
+times the number of right-hand sides for the batched forms).
 
 Workloads (seeded synthetic inputs, no datasets):
-  sphere-1.3M : unit icosphere refined 8x (1,310,720 flat triangles) plus
-                1,000,000 targets uniform in the shell 1.05 < |x| < 3,
-                single + double layer densities i.i.d. N(0,1), lambda = mu = 1,
-                iprec 2 (tolerance 0.5e-6), plain FP64.   [default]
-  sphere-5120 : icosphere level 4 (5,120 triangles) plus 1,000 targets uniform
-                in [-2,2]^3 with |x| > 1.1 (the CPU-runnable configuration).
+  fault-100k-r64 : [default] planar fault 40 x 20 dipping 45 degrees, top edge
+                   at depth 1, 250 x 200 cells x 2 = 100,000 right triangles,
+                   64 displacement-jump right-hand sides i.i.d. N(0,1) (double
+                   layer), lambda = mu = 1, displacement + strain at the
+                   centroids, free space, iprec 3.  The 64-RHS fault shape of
+                   the half-space configuration, evaluated with the free-space
+                   Green's function (the half-space image path is not built).
+                   A step = set_geometry + one batched evaluation of all 64
+                   right-hand sides in the mixed-precision form (P2M products,
+                   expansions and translations FP32 in the normalised basis;
+                   near field and local evaluation FP64).  The plain FP64 form
+                   (64 single evaluations, each with its own set_geometry) and
+                   the batched FP64 form are timed beside it, and the relative
+                   l2 error of every form against the FP64 direct sum on 2,000
+                   centroids is measured in the same run.
+  sphere-1.3M    : unit icosphere refined 8x (1,310,720 flat triangles) plus
+                   1,000,000 targets uniform in the shell 1.05 < |x| < 3,
+                   single + double layer N(0,1), iprec 2, one right-hand side,
+                   plain FP64 (step = set_geometry + evaluate).
+  sphere-5120    : icosphere level 4 (5,120 triangles) plus 1,000 targets
+                   uniform in [-2,2]^3 with |x| > 1.1, iprec 2, plain FP64.
+
+Inputs are resident in device memory for `value`; `e2e` runs the same step
+through the C ABI from pinned host buffers (efmm_batch_host for the batched
+workload, elfmm3dtriatarg_ for the single ones), host copies included.
 
 --impl reference times the CPU stand-in for the reference (the oracle's direct
 restatement of el3dtriadirecttarg; the Fortran reference cannot be compiled on
@@ -37,14 +52,27 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
-    "sphere-1.3M": dict(level=8, ntarg=1_000_000, targets="shell", iprec=2),
-    "sphere-5120": dict(level=4, ntarg=1_000, targets="box", iprec=2),
+    "fault-100k-r64": dict(kind="batch", nl=250, nw=200, nrhs=64, iprec=3),
+    "sphere-1.3M": dict(kind="single", level=8, ntarg=1_000_000, targets="shell", iprec=2),
+    "sphere-5120": dict(kind="single", level=4, ntarg=1_000, targets="box", iprec=2),
 }
+
+
+def make_fault(name, seed=1):
+    from elfmmlib3d_b200 import geometry as G
+    w = WORKLOADS[name]
+    tri, nrm, cen, _ = G.planar_fault(w["nl"], w["nw"])
+    R = w["nrhs"]
+    sdl = np.stack([np.random.default_rng(seed * 1000 + r).normal(size=cen.shape) for r in range(R)])
+    return tri, nrm, cen, sdl, w["iprec"]
 
 
 def make_inputs(name, seed=1):
     from elfmmlib3d_b200 import geometry as G
     w = WORKLOADS[name]
+    if w["kind"] == "batch":
+        tri, nrm, cen, sdl, iprec = make_fault(name, seed)
+        return tri, nrm, cen, np.zeros((0, 3)), None, sdl[0], iprec
     tri, nrm, cen = G.sphere_triangles(w["level"])
     if w["targets"] == "shell":
         tgt = G.shell_targets(w["ntarg"], seed + 1)
@@ -106,11 +134,13 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def fp64_gemm_peak(torch, dev):
-    """Measured FP64 throughput (cuBLAS DGEMM 8192^3, best of 5, CUDA events)."""
+def gemm_peak(torch, dev, dtype):
+    """Measured GEMM throughput (cuBLAS 8192^3, best of 5, CUDA events), in
+    TFLOP/s; FP32 with TF32 disabled (plain FP32 pipe)."""
+    torch.backends.cuda.matmul.allow_tf32 = False
     n = 8192
-    a = torch.randn(n, n, dtype=torch.float64, device=dev)
-    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    a = torch.randn(n, n, dtype=dtype, device=dev)
+    b = torch.randn(n, n, dtype=dtype, device=dev)
     torch.matmul(a, b)
     torch.cuda.synchronize()
     best = 1e30
@@ -133,6 +163,8 @@ def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     n = len(cen)
     half = nsample // 2
     t0 = time.perf_counter()
+    if len(tgt) == 0:
+        half = nsample
     O.direct(1.0, 1.0, tri, cen, ssl, sdl, tgt, rows=(0, half), trows=(0, nsample - half))
     dt = time.perf_counter() - t0
     cores = os.cpu_count()
@@ -218,7 +250,7 @@ def run_ours(args, rank, world, local_rank):
 
     if rank != 0:
         return None
-    peak = fp64_gemm_peak(torch, dev)
+    peak = gemm_peak(torch, dev, torch.float64)
     near_avg = float(np.mean(near_ms))
     flops = NEAR_FLOPS_PER_PAIR * info["near_pairs"]
     achieved = flops / (near_avg * 1e-3) / 1e12
@@ -251,11 +283,164 @@ def run_ours(args, rank, world, local_rank):
     return out
 
 
+def run_batch(args, rank, world, local_rank):
+    """The batched workload: mixed-precision batched form timed as `value`,
+    plain FP64 and batched FP64 forms beside it, errors vs the direct sum."""
+    import torch
+    import elfmmlib3d_b200 as E
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    tri, nrm, cen, sdl, iprec = make_fault(args.workload, seed=1 + rank)
+    R, n = sdl.shape[0], len(cen)
+    evals = n * n * R
+
+    def d(a):
+        return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    dtri, dnrm, dcen, dsdl = map(d, (tri, nrm, cen, sdl))
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device=dev)
+    e = torch.zeros((R, n, 3, 3), dtype=torch.float64, device=dev)
+    P = E.Plan(local_rank)
+
+    def step(precision=1):
+        P.set_geometry(dtri, dnrm, dcen, None, iprec=iprec)
+        P.evaluate_batch(1.0, 1.0, R, None, dsdl, u, e, precision=precision)
+
+    for _ in range(args.warmup):
+        step()
+    l0 = E.kernel_launches()
+    stage = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        P.record(0)
+        for _ in range(args.steps):
+            step()
+            stage.append(P.timings())
+        P.record(1)
+        ms = P.elapsed(0, 1)
+    torch.cuda.synchronize()
+    launches = E.kernel_launches() - l0
+    t_max = ms
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        dist.barrier()
+    value = world * evals * args.steps / (t_max * 1e-3)
+    info = P.info()
+    fl = P.flops_per_column()
+    setup = P.setup_timings()
+    tim = {k: float(np.mean([s_[k] for s_ in stage])) for k in stage[0]}
+    u_mixed, e_mixed = u.clone(), e.clone()
+
+    # end to end from pinned host buffers through the C ABI (efmm_batch_host)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    htri, hnrm, hcen, hsdl = map(pin, (tri, nrm, cen, sdl))
+    hout = (pin(np.zeros((R, n, 3))), pin(np.zeros((R, n, 3, 3))), pin(np.zeros((R, 1, 3))),
+            pin(np.zeros((R, 1, 3, 3))))
+    ier, *_ = E.batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, out=hout)
+    assert ier == 0, ier
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ier, *_ = E.batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, out=hout)
+        assert ier == 0, ier
+    e2e_s = time.perf_counter() - t0
+    e2e_t = e2e_s
+    if world > 1:
+        import torch.distributed as dist
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_t = float(tt.item())
+    e2e_value = world * evals * args.steps / e2e_t
+    h2d = 8 * (9 * n + 3 * n + 3 * n + 3 * n * R)
+    d2h = 8 * (3 * n * R + 9 * n * R)
+
+    # the other forms, same inputs: plain FP64 = one full evaluation per
+    # right-hand side (set_geometry + evaluate each); batched FP64
+    u1 = torch.zeros((R, n, 3), dtype=torch.float64, device=dev)
+    e1 = torch.zeros((R, n, 3, 3), dtype=torch.float64, device=dev)
+    P.set_geometry(dtri, dnrm, dcen, None, iprec=iprec)
+    P.evaluate(1.0, 1.0, None, dsdl[0], u1[0], e1[0])
+    P.record(0)
+    for r in range(R):
+        P.set_geometry(dtri, dnrm, dcen, None, iprec=iprec)
+        P.evaluate(1.0, 1.0, None, dsdl[r], u1[r], e1[r])
+    P.record(1)
+    plain_ms = P.elapsed(0, 1)
+    step(0)
+    P.record(0)
+    step(0)
+    P.record(1)
+    b64_ms = P.elapsed(0, 1)
+    u64, e64 = u.clone(), e.clone()
+    ns = min(2000, n)
+    ud = torch.zeros((ns, 3), dtype=torch.float64, device=dev)
+    ed = torch.zeros((ns, 3, 3), dtype=torch.float64, device=dev)
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    errs = {"plain_fp64": [0.0, 0.0], "batched_fp64": [0.0, 0.0], "mixed_batched": [0.0, 0.0]}
+    for r in (0, R - 1):
+        P.evaluate_direct_subset(1.0, 1.0, ns, None, dsdl[r], ud, ed)
+        for key, (uu, ee) in (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)),
+                              ("mixed_batched", (u_mixed, e_mixed))):
+            errs[key][0] = max(errs[key][0], rel(uu[r, :ns], ud))
+            errs[key][1] = max(errs[key][1], rel(ee[r, :ns], ed))
+    if rank != 0:
+        return None
+    # roofline: the translation kernel (k_translate<float>: M2M + M2L + L2L)
+    C = 4 * R
+    tr_flops = (fl["m2m"] + fl["m2l"] + fl["l2l"]) * C
+    tr_ms = tim["m2m"] + tim["m2l"] + tim["l2l"]
+    achieved = tr_flops / (tr_ms * 1e-3) / 1e12
+    peak32 = gemm_peak(torch, dev, torch.float32)
+    roof = {"kernel": "k_translate<float> (M2M+M2L+L2L)", "bound": "fp32", "achieved": achieved, "peak": peak32,
+            "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
+            "peak_source": "measured cuBLAS SGEMM 8192^3 (FP32 pipe, TF32 off) in this run; "
+                           "MEASURED_PEAKS.json has no FP32 entry",
+            "algorithmic": f"dense per-offset operators: {tr_flops:.4g} flop per step over "
+                           f"{info['m2l_pairs']} M2L pairs x {C} columns"}
+    stage_tf = {k: fl[k] * C / (tim[k] * 1e-3) / 1e12 for k in ("p2m", "m2m", "m2l", "l2l", "l2t") if tim[k] > 0}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
+        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
+               "sample": f"oracle direct sum, {npts} centroids x {n} triangles x 1 right-hand side "
+                         f"({dt:.1f} s)"}
+    plain_value = evals / (plain_ms * 1e-3)
+    b64_value = evals / (b64_ms * 1e-3)
+    return {
+        "metric": "triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)",
+        "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "triangles": n, "rhs": R, "targets": 0, "iprec": iprec,
+                   "green": "free space", "evals_per_step": evals, "parallelism": f"replicas{world}",
+                   "l2_policy": "expansions (2 x 3.5 GB FP32) and pair data > L2 (126 MB)",
+                   "forms": {"mixed_batched": value / world, "batched_fp64": b64_value,
+                             "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
+                             "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms},
+                   "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
+                   "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
+                   "stage_ms": tim, "stage_tflops": stage_tf, "setup_ms": setup,
+                   "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")},
+                   "near_pairs": info["near_pairs"], "m2l_pairs": info["m2l_pairs"]},
+        "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h, "timing": "host wall clock around blocking efmm_batch_host calls"},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+
+
 def run_reference(args, rank):
     if rank != 0:
         return None
     tri, nrm, cen, tgt, ssl, sdl, iprec = make_inputs(args.workload)
     n = len(cen)
+    batch = WORKLOADS[args.workload]["kind"] == "batch"
     for _ in range(args.warmup):
         cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
     t0 = time.perf_counter()
@@ -263,13 +448,16 @@ def run_reference(args, rank):
         ev, dt, cores, npts = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
     tot = time.perf_counter() - t0
     value = args.steps * args.ref_sample * n / tot
+    metric = ("triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)" if batch
+              else "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)")
     return {
         "impl": "reference",
-        "metric": "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)",
+        "metric": metric,
         "value": value, "unit": "triangle-evals/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "triangles": n, "targets": len(tgt), "iprec": iprec},
+        "config": {"workload": args.workload, "triangles": n, "targets": len(tgt), "iprec": iprec,
+                   **({"rhs": WORKLOADS[args.workload]["nrhs"], "green": "free space"} if batch else {})},
         "cpu_baseline": {"value": value, "unit": "triangle-evals/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"oracle direct sum (el3dtriadirecttarg restated), {args.ref_sample} "
                                    f"evaluation points x {n} triangles per step"},
@@ -283,7 +471,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="sphere-1.3M", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="fault-100k-r64", choices=list(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--ref-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -300,7 +488,10 @@ def main():
             import torch.distributed as dist
             torch.cuda.set_device(local_rank)
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-        out = run_ours(args, rank, world, local_rank)
+        if WORKLOADS[args.workload]["kind"] == "batch":
+            out = run_batch(args, rank, world, local_rank)
+        else:
+            out = run_ours(args, rank, world, local_rank)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()

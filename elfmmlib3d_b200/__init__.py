@@ -25,7 +25,7 @@ import os
 
 import numpy as np
 
-__all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "elfmm3dtriatargiter",
+__all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "elfmm3dtriatargiter", "batch_host",
            "elfmm3dtriaiter", "iter_release", "iter_stored_bytes", "Plan", "load",
            "library_path", "device_count", "ElfmmError"]
 
@@ -48,7 +48,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
-           "efmm_plan_evaluate_direct_subset"]
+           "efmm_plan_evaluate_direct_subset", "efmm_batch_host"]
 
 
 class ElfmmError(RuntimeError):
@@ -97,6 +97,9 @@ def load():
     L.efmm_direct_noalloc.restype = ctypes.c_int
     L.efmm_direct_noalloc.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp,
                                       ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.efmm_batch_host.restype = ctypes.c_int
+    L.efmm_batch_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
+                                  ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
     L.efmm_iter_release.restype = ctypes.c_int
     L.efmm_iter_release.argtypes = [_dp, ctypes.c_int]
     L.efmm_iter_stored_bytes.restype = ctypes.c_longlong
@@ -200,6 +203,32 @@ def el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigm
                           _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp), _byref_i(ifstraintarg),
                           stt.ctypes.data_as(_dp))
     return pt, st, ptt[:m], stt[:m]
+
+
+def batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, target=None,
+               precision=0, out=None):
+    """nrhs right-hand sides in one pass from host arrays: sigma_sl/sigma_dl
+    (nrhs,n,3).  Returns (ier, ptfrc (nrhs,n,3), strain (nrhs,n,3,3),
+    ptfrctarg (nrhs,m,3), straintarg (nrhs,m,3,3)).  precision 0 = FP64,
+    1 = mixed.  ``out`` may pass preallocated (e.g. pinned) output arrays."""
+    L = load()
+    _need_gpu()
+    tri = _c(triangle, (-1, 3, 3))
+    n = tri.shape[0]
+    nrm, src = _c(trinorm, (n, 3)), _c(source, (n, 3))
+    ssl = _c(sigma_sl, (-1, n, 3)) if sigma_sl is not None else None
+    sdl = _c(sigma_dl, (-1, n, 3)) if sigma_dl is not None else None
+    R = (ssl if ssl is not None else sdl).shape[0]
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    if out is None:
+        out = (np.zeros((R, n, 3)), np.zeros((R, n, 3, 3)), np.zeros((R, max(m, 1), 3)),
+               np.zeros((R, max(m, 1), 3, 3)))
+    pt, st, ptt, stt = out
+    p = lambda a: a.ctypes.data_as(_dp) if a is not None else None
+    ier = L.efmm_batch_host(int(iprec), float(rlam), float(rmu), n, p(tri), p(nrm), p(src), m, p(tg), R, p(ssl),
+                            p(sdl), p(pt), p(st), p(ptt) if m else None, p(stt) if m else None, int(precision))
+    return ier, pt, st, ptt[:, :m], stt[:, :m]
 
 
 ITER_LUSED = 8  # words of wsave the ITER handle occupies

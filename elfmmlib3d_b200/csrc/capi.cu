@@ -324,6 +324,52 @@ extern "C" void el3dtriadirecttarg_(const double* rlam, const double* rmu, const
   if (ier) fprintf(stderr, "el3dtriadirecttarg: error %d\n", ier);
 }
 
+// Many right-hand sides from host arrays (no counterpart in the reference):
+// the reference-style call of the batched forms, host copies included.
+extern "C" int efmm_batch_host(int iprec, double rlam, double rmu, int n, const double* tri, const double* nrm,
+                               const double* src, int nt, const double* tgt, int nrhs, const double* ssl,
+                               const double* sdl, double* u_src, double* e_src, double* u_tgt, double* e_tgt,
+                               int precision) {
+  if (n < 1 || nt < 0 || nrhs < 1) return IER_BADARG;
+  std::lock_guard<std::mutex> lk(g_mu);
+  efmm_plan* p = shared_plan();
+  if (!p) return IER_NODEVICE;
+  try {
+    cudaSetDevice(p->device);
+    if (!g_bufs) g_bufs = new HostCall();
+    HostCall& B = *g_bufs;
+    cudaStream_t st = p->stream;
+    const size_t R = nrhs;
+    up(B.tri, tri, 9 * (size_t)n, st);
+    up(B.nrm, nrm, 3 * (size_t)n, st);
+    up(B.src, src, 3 * (size_t)n, st);
+    up(B.tgt, tgt, 3 * (size_t)nt, st);
+    if (ssl) up(B.ssl, ssl, 3 * (size_t)n * R, st);
+    if (sdl) up(B.sdl, sdl, 3 * (size_t)n * R, st);
+    B.u.resize(3 * (size_t)n * R);
+    B.e.resize(9 * (size_t)n * R);
+    B.ut.resize(3 * (size_t)std::max(nt, 1) * R);
+    B.et.resize(9 * (size_t)std::max(nt, 1) * R);
+    int ier = p->plan->set_geometry(n, B.tri.get(), B.nrm.get(), B.src.get(), nt, B.tgt.get(), iprec, false, false);
+    if (ier) return ier;
+    ier = p->plan->evaluate_batch(rlam, rmu, nrhs, ssl ? B.ssl.get() : nullptr, sdl ? B.sdl.get() : nullptr,
+                                  (u_src || e_src) ? B.u.get() : nullptr, e_src ? B.e.get() : nullptr,
+                                  (nt > 0 && (u_tgt || e_tgt)) ? B.ut.get() : nullptr,
+                                  (nt > 0 && e_tgt) ? B.et.get() : nullptr, precision);
+    if (ier) return ier;
+    if (u_src) down(u_src, B.u, 3 * (size_t)n * R, st);
+    if (e_src) down(e_src, B.e, 9 * (size_t)n * R, st);
+    if (nt > 0 && u_tgt) down(u_tgt, B.ut, 3 * (size_t)nt * R, st);
+    if (nt > 0 && e_tgt) down(e_tgt, B.et, 9 * (size_t)nt * R, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // ITER entry point (src/elfmm3dtria_iter_1.f:160-165).  The reference keeps
 // the near-field operator in the caller's wsave array.  Here the operator

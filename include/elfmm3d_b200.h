@@ -89,6 +89,16 @@ void elfmm3dtriaiter_(int *ier, const int *iprec, const double *rlam, const doub
                       double *ptfrc, const int *ifstrain, double *strain, const int *icomp_type,
                       double *wsave, const int *lwsave, int *lused);
 
+/* nrhs right-hand sides from host arrays (no counterpart in the reference):
+ * geometry as in elfmm3dtriatarg_, sigma_sl/sigma_dl (3,n,nrhs) column-major
+ * (NULL disables a layer), outputs ptfrc (3,n,nrhs), strain (3,3,n,nrhs),
+ * ptfrctarg (3,nt,nrhs), straintarg (3,3,nt,nrhs) (NULL disables one).
+ * precision as in efmm_plan_evaluate_batch.  Blocking; returns ier. */
+int efmm_batch_host(int iprec, double rlam, double rmu, int n, const double *triangle,
+                    const double *trinorm, const double *source, int nt, const double *target,
+                    int nrhs, const double *sigma_sl, const double *sigma_dl, double *ptfrc,
+                    double *strain, double *ptfrctarg, double *straintarg, int precision);
+
 /* Frees the device store named by an ITER handle (no counterpart in the
  * reference, whose store is the caller's wsave array).  512 if the handle
  * names no live store. */
