@@ -21,6 +21,8 @@ Workloads (seeded synthetic inputs, no datasets):
                    the batched FP64 form are timed beside it, and the relative
                    l2 error of every form against the FP64 direct sum on 2,000
                    centroids is measured in the same run.
+  fault-10k-r32  : the same fault at 100 x 50 cells (10,000 triangles), 32
+                   right-hand sides: the small case for profiler captures.
   sphere-1.3M    : unit icosphere refined 8x (1,310,720 flat triangles) plus
                    1,000,000 targets uniform in the shell 1.05 < |x| < 3,
                    single + double layer N(0,1), iprec 2, one right-hand side,
@@ -53,6 +55,7 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     "fault-100k-r64": dict(kind="batch", nl=250, nw=200, nrhs=64, iprec=3),
+    "fault-10k-r32": dict(kind="batch", nl=100, nw=50, nrhs=32, iprec=3),
     "sphere-1.3M": dict(kind="single", level=8, ntarg=1_000_000, targets="shell", iprec=2),
     "sphere-5120": dict(kind="single", level=4, ntarg=1_000, targets="box", iprec=2),
 }

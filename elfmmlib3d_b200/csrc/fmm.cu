@@ -392,6 +392,233 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
   }
 }
 
+// ------------------------------------------- P2M in two stages (product form)
+// Stage 1 writes, per leaf, the node features A[k][row] (k = 4 node + comp,
+// comp 0 charge, 1..3 dipole x, y, z; rows the interleaved coefficients) and
+// the node weights B[col][k] of every column; stage 2 is the plain batched
+// product  mpole[box][col][row] = sum_k A[k][row] B[col][k]  (k_gemm_tn).
+// The features depend on the geometry only; each is computed once per node
+// instead of once per output tile.
+template <class T>
+__global__ void __launch_bounds__(256)
+k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ foff,
+               T* __restrict__ F) {
+  extern __shared__ __align__(16) unsigned char pf_smem[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc;
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int nnode = 12 * tn;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int node = blockIdx.y * 8 + warp;
+  if (node >= nnode) return;
+  cplx* Y = reinterpret_cast<cplx*>(pf_smem) + (size_t)warp * nc;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  Quad12 Q;
+  quad12(Q);
+  const int it = t0 + node / 12, iq = node % 12;
+  const double* Tr = a.tri + 9 * (size_t)it;
+  double y[3];
+  for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
+  const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
+  const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+  for (int m = lane; m <= p; m += 32) {
+    cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+    for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+    Y[cidx(m, m)] = dm;
+    cplx ym2 = {0, 0}, ym1 = dm;
+    for (int n = m + 1; n <= p; n++) {
+      const double aa = (2.0 * n - 1.0) * z[2];
+      const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+      cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+      Y[cidx(n, m)] = yn;
+      ym2 = ym1;
+      ym1 = yn;
+    }
+  }
+  __syncwarp();
+  T* out = F + foff[blockIdx.x] + (size_t)(4 * node) * D;
+  for (int cc = lane; cc < nc; cc += 32) {
+    int fn = 0;
+    while ((fn + 1) * (fn + 2) / 2 <= cc) fn++;
+    const int fm = cc - fn * (fn + 1) / 2;
+    const cplx yv = Y[cc];
+    cplx ya = {0, 0}, yb = {0, 0}, yc = {0, 0};
+    if (fn > 0) {
+      ya = hget(Y, fn - 1, fm);
+      yb = hget(Y, fn - 1, fm + 1);
+      yc = hget(Y, fn - 1, fm - 1);
+    }
+    const double sr = a.wnorm ? a.wnorm[2 * cc] : 1.0;
+    // real row 2cc, imaginary row 2cc + 1 (as in k_p2m_gemm)
+    out[2 * cc] = (T)(sr * yv.re);
+    out[2 * cc + 1] = (T)(-sr * yv.im);
+    out[D + 2 * cc] = (T)(sr * 0.5 * is * (yb.re - yc.re));
+    out[D + 2 * cc + 1] = (T)(-sr * 0.5 * is * (yb.im - yc.im));
+    out[2 * D + 2 * cc] = (T)(sr * 0.5 * is * (yb.im + yc.im));
+    out[2 * D + 2 * cc + 1] = (T)(sr * 0.5 * is * (yb.re + yc.re));
+    out[3 * D + 2 * cc] = (T)(sr * is * ya.re);
+    out[3 * D + 2 * cc + 1] = (T)(-sr * is * ya.im);
+  }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256)
+k_p2m_weights(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ woff,
+              T* __restrict__ W) {
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int nnode = 12 * tn, K = 4 * nnode, C = 4 * R;
+  Quad12 Q;
+  quad12(Q);
+  const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu;
+  T* out = W + woff[blockIdx.x];
+  for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < (long long)nnode * C;
+       q += (long long)gridDim.y * blockDim.x) {
+    const int col = (int)(q / nnode), node = (int)(q % nnode);
+    const int r = col >> 2, pass = col & 3;
+    const int it = t0 + node / 12, iq = node % 12;
+    const double* Tr = a.tri + 9 * (size_t)it;
+    double y[3];
+    for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
+    const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+    const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+    const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                          e1[0] * e2[1] - e1[1] * e2[0]};
+    const double w = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    const double* nn = a.nrm + 3 * (size_t)it;
+    const long long off = r * a.rstride + it * a.tstride, ds = a.dstride;
+    double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+    if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
+    if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
+    double wv[4];
+    if (pass < 3) {
+      wv[0] = w * sl[pass] * inv2mu;
+      for (int d = 0; d < 3; d++) wv[1 + d] = w * 0.5 * (nn[d] * dl[pass] + dl[d] * nn[pass]);
+    } else {
+      const double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
+      const double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+      const double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
+      const double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+      wv[0] = w * (sly * c1 * inv2mu + dln * c2);
+      for (int d = 0; d < 3; d++) wv[1 + d] = w * 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
+    }
+    T* o = out + (size_t)col * K + 4 * node;
+#pragma unroll
+    for (int k = 0; k < 4; k++) o[k] = (T)wv[k];
+  }
+}
+
+// Batched product  C[col][row] = sum_k A[k][row] * B[col][k]  over 128 x 128
+// output tiles (GemmTask), 8 x 8 outputs per thread, K tiles of 16
+// double-buffered in shared memory; C is stored (each task owns its tile).
+template <class T>
+__global__ void __launch_bounds__(256, 1)
+k_gemm_tn(const GemmTask* __restrict__ tasks, const T* __restrict__ A, const T* __restrict__ B,
+          T* __restrict__ Cm) {
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char gt_smem[];
+  T* As = reinterpret_cast<T*>(gt_smem);  // [2][16][128]
+  T* Bs = As + 2 * 16 * 128;              // [2][16][128]
+  const GemmTask t = tasks[blockIdx.x];
+  const int tid = threadIdx.x;
+  // A loader: k row (tid >> 4), 8 consecutive output rows from (tid & 15) * 8
+  const int ak = tid >> 4, ar = (tid & 15) * 8;
+  const T* Ap = A + t.a_off + t.row0 + ar;
+  const bool arow_all = t.row0 + ar + 8 <= t.M;
+  // B loader: column (tid & 127), k half (tid >> 7)
+  const int bcol = tid & 127, bkh = (tid >> 7) * 8;
+  const bool bcol_ok = t.col0 + bcol < t.N;
+  const T* Bp = B + t.b_off + (size_t)(bcol_ok ? t.col0 + bcol : 0) * t.ldb;
+  T ra[8], rb[8];
+  auto load = [&](int k0) {
+    const int k = k0 + ak;
+    if (k < t.K && arow_all) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(Ap + (size_t)k * t.lda + 2 * i);
+        ra[2 * i] = v.x;
+        ra[2 * i + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+        ra[i] = (k < t.K && t.row0 + ar + i < t.M) ? Ap[(size_t)k * t.lda + i] : T(0);
+    }
+    const int kb = k0 + bkh;
+    if (bcol_ok && kb + 8 <= t.K) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(Bp + kb + 2 * i);
+        rb[2 * i] = v.x;
+        rb[2 * i + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) rb[i] = (bcol_ok && kb + i < t.K) ? Bp[kb + i] : T(0);
+    }
+  };
+  auto store = [&](int buf) {
+    T* as = As + buf * 16 * 128;
+    T* bs = Bs + buf * 16 * 128;
+#pragma unroll
+    for (int i = 0; i < 8; i++) as[ak * 128 + ar + i] = ra[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) bs[(bkh + i) * 128 + bcol] = rb[i];
+  };
+  const int tx = tid & 15, ty = tid >> 4;
+  T acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = T(0);
+  const int nk = (t.K + 15) / 16;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; kt++) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) load((kt + 1) * 16);
+    const T* as = As + cur * 16 * 128;
+    const T* bs = Bs + cur * 16 * 128;
+#pragma unroll
+    for (int kk = 0; kk < 16; kk++) {
+      T av[8], bv[8];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        V2 v = *reinterpret_cast<const V2*>(as + kk * 128 + ty * 8 + 2 * i);
+        av[2 * i] = v.x;
+        av[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        V2 v = *reinterpret_cast<const V2*>(bs + kk * 128 + 32 * j + 2 * tx);
+        bv[2 * j] = v.x;
+        bv[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] += av[i] * bv[j];
+    }
+    if (kt + 1 < nk) store(cur ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int col = t.col0 + 32 * (j >> 1) + 2 * tx + (j & 1);
+    if (col >= t.N) continue;
+    T* cp = Cm + t.c_off + (size_t)col * t.ldc;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = t.row0 + ty * 8 + i;
+      if (r < t.M) cp[r] = acc[i][j];
+    }
+  }
+}
+
 // --------------------------------------------------- grouped translations
 // A task is one 128 x 128 output tile of the product Op(group) * B, where B's
 // columns are the concatenated columns of the group's (src, dst) pairs: column
@@ -404,7 +631,7 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
 constexpr int TR_R = 128, TR_C = 128, TR_K = 16;
 
 template <class T>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 k_translate(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
             const T* __restrict__ mats, const long long* __restrict__ mat_off,
             const int* __restrict__ mat_dim, int D, int C, const T* __restrict__ src,
@@ -872,6 +1099,26 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs) {
   k_p2m<<<dim3(nleaf, nrhs), P2M_THREADS, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+
+template <class T>
+void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
+                         const long long* foff, const long long* woff, int max_nodes, T* F, T* W, int ntask,
+                         const GemmTask* tasks, T* mpole) {
+  if (nwleaf <= 0) return;
+  const int nc = ncoef(a.p);
+  const int smem = (int)(sizeof(cplx) * 8 * nc);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_p2m_features<T><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, F); count_launch();
+  k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, W); count_launch();
+  const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+  k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+template void launch_p2m_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
+                                          const long long*, int, double*, double*, int, const GemmTask*, double*);
+template void launch_p2m_twostage<float>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
+                                         const long long*, int, float*, float*, int, const GemmTask*, float*);
 
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,

@@ -23,6 +23,13 @@ struct TransTask {
   int group, row0, pair0, ncols, col0;
 };
 
+// One 128 x 128 tile of C[col][row] = sum_k A[k][row] B[col][k]
+// (A: K rows of lda, B: N columns of ldb, C: N columns of ldc).
+struct GemmTask {
+  long long a_off, b_off, c_off;
+  int M, N, K, lda, ldb, ldc, row0, col0;
+};
+
 struct P2MArgs {
   const int* leaves;
   const int *level, *ijk, *sstart, *scount;
@@ -64,6 +71,14 @@ bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpo
 // L2T of R right-hand sides as a product over (chunks of 8 points of a leaf,
 // 256 columns); local (boxes, 4R, D) in TB (float: normalised basis, rows
 // rescaled by wnorm).  Returns false when the order is too high.
+// Two-stage P2M of R right-hand sides for one wave of leaves: node features
+// F (per leaf at foff: 4 x 12 x triangles rows of D), node weights W (per
+// leaf at woff: 4R columns of 4 x 12 x triangles), then the batched product
+// into mpole (tasks cut by the caller).
+template <class T>
+void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
+                         const long long* foff, const long long* woff, int max_nodes, T* F, T* W, int ntask,
+                         const GemmTask* tasks, T* mpole);
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
                      int R, const TB* local, const double* wnorm);

@@ -357,6 +357,9 @@ void Plan::build_worklists() {
   if (p2m.empty()) far_ = false;
   np2m_ = (int)p2m.size();
   nl2t_ = (int)l2t.size();
+  p2m_h_ = p2m;
+  p2m_sc_h_.clear();
+  for (int b : p2m) p2m_sc_h_.push_back(scount[b]);
   l2t_sc_h_.clear();
   l2t_tc_h_.clear();
   for (int b : l2t) {
@@ -668,6 +671,52 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
   return IER_OK;
 }
 
+// Two-stage P2M over waves of leaves whose node features and weights fit a
+// scratch budget (at most 8 GB or a quarter of the free memory).
+template <class T>
+void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
+  const int D = 2 * ncoef(p_), C = 4 * R;
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  const size_t budget_bytes =
+      std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double));
+  const size_t budget = budget_bytes / sizeof(T);  // elements
+  size_t i = 0;
+  const size_t nl = p2m_h_.size();
+  while (i < nl) {
+    std::vector<int> wl;
+    std::vector<long long> fo, wo;
+    std::vector<GemmTask> tasks;
+    long long used = 0;
+    int max_nodes = 0;
+    while (i < nl) {
+      const long long K = 48LL * p2m_sc_h_[i];
+      const long long need = K * D + K * C;
+      if (!wl.empty() && used + need > (long long)budget) break;
+      wl.push_back((int)i);
+      fo.push_back(used);
+      wo.push_back(used + K * D);
+      const int box = p2m_h_[i];
+      for (int c0 = 0; c0 < C; c0 += 128)
+        for (int r0 = 0; r0 < D; r0 += 128)
+          tasks.push_back({used, used + K * D, (long long)box * C * D, D, C, (int)K, D, (int)K, D, r0, c0});
+      used += need;
+      max_nodes = std::max(max_nodes, 12 * p2m_sc_h_[i]);
+      i++;
+    }
+    p2m_scratch_.resize(((size_t)used * sizeof(T) + sizeof(double) - 1) / sizeof(double));
+    h2d(wave_leaves_, wl, st_);
+    h2d(wave_foff_, fo, st_);
+    h2d(wave_woff_, wo, st_);
+    h2d(wave_tasks_, tasks, st_);
+    T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
+    launch_p2m_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
+                           max_nodes, scratch, scratch, (int)tasks.size(), wave_tasks_.get(), mpole);
+  }
+}
+template void Plan::p2m_twostage<double>(const P2MArgs&, int, double*);
+template void Plan::p2m_twostage<float>(const P2MArgs&, int, float*);
+
 int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed) {
   const int n = n_, nt = nt_;
@@ -728,7 +777,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.C = C; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
     if (mixed) {
       pa.wnorm = ops_->wnorm.get();  // multipoles in the normalised basis
-      if (!launch_p2m_gemm<float>(st_, np2m_, pa, R, mpole_f_.get())) return IER_BADARG;
+      p2m_twostage<float>(pa, R, mpole_f_.get());
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, C, ops_->mats_f.get(), mpole_f_.get(), mpole_f_.get());
       EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
@@ -737,7 +786,10 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       run_translations(l2l_, C, ops_->mats_f.get(), local_f_.get(), local_f_.get());
     } else {
       // product form once the columns fill its tiles
-      if (C < 32 || !launch_p2m_gemm<double>(st_, np2m_, pa, R, mpole_.get())) launch_p2m(st_, np2m_, pa, R);
+      if (C < 32)
+        launch_p2m(st_, np2m_, pa, R);
+      else
+        p2m_twostage<double>(pa, R, mpole_.get());
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, C, ops_->mats.get(), mpole_.get(), mpole_.get());
       EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));

@@ -111,6 +111,13 @@ class Plan {
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA
   int nchunk_ = 0, chunk_key_ = -1;
   std::vector<int> l2t_sc_h_, l2t_tc_h_;  // per L2T leaf
+  std::vector<int> p2m_h_, p2m_sc_h_;     // P2M leaves and their triangle counts
+  DevBuf<double> p2m_scratch_;            // node features + weights of one wave of leaves
+  DevBuf<int> wave_leaves_;
+  DevBuf<long long> wave_foff_, wave_woff_;
+  DevBuf<GemmTask> wave_tasks_;
+  template <class T>
+  void p2m_twostage(const P2MArgs& pa, int R, T* mpole);
   DevBuf<int> lchunk_leaf_, lchunk_e0_;   // (L2T leaf index, first point) per product-form L2T CTA
   int nlchunk_ = 0, lchunk_key_ = -1;
   void ensure_ops();

@@ -289,7 +289,7 @@ static void exclusive_scan(cudaStream_t st, const int* in, int* out, int n, DevB
 
 // sort pairs (a, b) of box ids by (a, b) and build CSR over nb boxes
 static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, DevBuf<int>& start,
-                         DevBuf<int>& items, DevBuf<char>& tmp);
+                         DevBuf<int>& items, TreeScratch& S);
 
 __global__ void k_pair_keys(int np, const int2* __restrict__ p, unsigned long long* __restrict__ k,
                             int* __restrict__ v) {
@@ -305,9 +305,10 @@ __global__ void k_csr_count(int np, const unsigned long long* __restrict__ k, in
 }
 
 static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, DevBuf<int>& start,
-                         DevBuf<int>& items, DevBuf<char>& tmp) {
-  DevBuf<unsigned long long> k0, k1;
-  DevBuf<int> v0;
+                         DevBuf<int>& items, TreeScratch& S) {
+  DevBuf<unsigned long long>&k0 = S.k0, &k1 = S.k1;
+  DevBuf<int>& v0 = S.v0;
+  DevBuf<char>& tmp = S.tmp;
   k0.resize(np);
   k1.resize(np);
   v0.resize(np);
@@ -319,7 +320,7 @@ static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, D
     if (bytes > tmp.size()) tmp.resize(bytes);
     cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, k0.get(), k1.get(), v0.get(), items.get(), np, 0, 64, st);
   }
-  DevBuf<int> cnt;
+  DevBuf<int>& cnt = S.cnt;
   cnt.resize(nb + 1);
   cnt.zero(st);
   if (np > 0) { k_csr_count<<<(np + 255) / 256, 256, 0, st>>>(np, k1.get(), cnt.get()); count_launch(); }
@@ -343,11 +344,12 @@ __global__ void k_transpose_pairs(int np, const int2* __restrict__ in, int2* __r
 int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double* d_tgt, int nbox,
                int mindlin, Tree& tr) {
   if (n < 1) return IER_BADARG;
-  DevBuf<char> tmp;
+  TreeScratch& S = tr.scr;
+  DevBuf<char>& tmp = S.tmp;
   tr.n = n;
   tr.nt = nt;
   // ---- root
-  DevBuf<double> bb;
+  DevBuf<double>& bb = S.bb;
   bb.resize(6);
   {
     unsigned long long init[6];
@@ -421,8 +423,9 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     if (nt) EFMM_CUDA_TRY(cudaMemcpyAsync(tr.izt.get(), id.data(), 4 * (size_t)nt, cudaMemcpyHostToDevice, st));
     EFMM_CUDA_TRY(cudaStreamSynchronize(st));
   }
-  DevBuf<int> pbs, pbt, izs2, izt2, split, cs, ct, nch, off;
-  DevBuf<unsigned long long> ks, ks2, kt, kt2;
+  DevBuf<int>&pbs = S.pbs, &pbt = S.pbt, &izs2 = S.izs2, &izt2 = S.izt2, &split = S.split, &cs = S.cs,
+              &ct = S.ct, &nch = S.nch, &off = S.off;
+  DevBuf<unsigned long long>&ks = S.ks, &ks2 = S.ks2, &kt = S.kt, &kt2 = S.kt2;
   pbs.resize(n);
   pbs.zero(st);
   pbt.resize(nt);
@@ -505,12 +508,13 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
 }
 
 int build_lists(cudaStream_t st, Tree& tr) {
-  DevBuf<char> tmp;
+  TreeScratch& S = tr.scr;
+  DevBuf<char>& tmp = S.tmp;
   int nb = tr.nboxes;
   tr.coll.resize(27 * (size_t)nb);
   tr.ncoll.resize(nb);
   tr.ncoll.zero(st);
-  DevBuf<int> l2cnt, l2off;
+  DevBuf<int>&l2cnt = S.l2cnt, &l2off = S.l2off;
   l2cnt.resize(nb);
   l2cnt.zero(st);
   l2off.resize(nb + 1);
@@ -529,20 +533,20 @@ int build_lists(cudaStream_t st, Tree& tr) {
     EFMM_CUDA_TRY(cudaStreamSynchronize(st));
     tot2 = a + b;
   }
-  DevBuf<int> l2items;
+  DevBuf<int>& l2items = S.l2items;
   l2items.resize(tot2);
   for (int lev = 1; lev <= tr.nlev; lev++) {
     int lo = tr.laddr[lev].first, cnt = tr.laddr[lev].second;
     k_list52<<<(cnt + 127) / 128, 128, 0, st>>>(T, lo, lo + cnt, 1, nullptr, l2off.get(), l2items.get()); count_launch();
   }
   {
-    DevBuf<int2> pairs;
+    DevBuf<int2>& pairs = S.pairs;
     pairs.resize(tot2);
     if (nb) { k_l2_pairs<<<(nb + 127) / 128, 128, 0, st>>>(nb, l2off.get(), l2cnt.get(), l2items.get(), pairs.get()); count_launch(); }
-    pairs_to_csr(st, pairs, tot2, nb, tr.l2_start, tr.l2_items, tmp);
+    pairs_to_csr(st, pairs, tot2, nb, tr.l2_start, tr.l2_items, S);
   }
   // lists 1 and 3
-  DevBuf<int> c1, c3, o1, o3;
+  DevBuf<int>&c1 = S.c1, &c3 = S.c3, &o1 = S.o1, &o3 = S.o3;
   c1.resize(nb);
   c3.resize(nb);
   o1.resize(nb + 1);
@@ -557,15 +561,15 @@ int build_lists(cudaStream_t st, Tree& tr) {
   EFMM_CUDA_TRY(cudaMemcpyAsync(&h[3], o3.get() + nb - 1, 4, cudaMemcpyDeviceToHost, st));
   EFMM_CUDA_TRY(cudaStreamSynchronize(st));
   int tot1 = h[0] + h[1], tot3 = h[2] + h[3];
-  DevBuf<int2> p1, p3, p4;
+  DevBuf<int2>&p1 = S.p1, &p3 = S.p3, &p4 = S.p4;
   p1.resize(tot1);
   p3.resize(tot3);
   k_list13<<<(nb + 127) / 128, 128, 0, st>>>(T, nb, 1, nullptr, nullptr, o1.get(), o3.get(), p1.get(), p3.get()); count_launch();
-  pairs_to_csr(st, p1, tot1, nb, tr.l1_start, tr.l1_items, tmp);
+  pairs_to_csr(st, p1, tot1, nb, tr.l1_start, tr.l1_items, S);
   p4.resize(tot3);
   if (tot3) { k_transpose_pairs<<<(tot3 + 255) / 256, 256, 0, st>>>(tot3, p3.get(), p4.get()); count_launch(); }
-  pairs_to_csr(st, p3, tot3, nb, tr.l3_start, tr.l3_items, tmp);
-  pairs_to_csr(st, p4, tot3, nb, tr.l4_start, tr.l4_items, tmp);
+  pairs_to_csr(st, p3, tot3, nb, tr.l3_start, tr.l3_items, S);
+  pairs_to_csr(st, p4, tot3, nb, tr.l4_start, tr.l4_items, S);
   EFMM_CUDA_TRY(cudaStreamSynchronize(st));
   return IER_OK;
 }

@@ -15,6 +15,18 @@ struct TreeDev {
   double size;
 };
 
+// Device scratch of the tree and list builds, kept between builds so that a
+// repeated set_geometry allocates nothing (cudaMalloc/cudaFree on every call
+// stalled the host for up to a quarter second).
+struct TreeScratch {
+  DevBuf<char> tmp;
+  DevBuf<double> bb;
+  DevBuf<int> pbs, pbt, izs2, izt2, split, cs, ct, nch, off;
+  DevBuf<unsigned long long> ks, ks2, kt, kt2, k0, k1;
+  DevBuf<int> l2cnt, l2off, l2items, c1, c3, o1, o3, cnt, v0;
+  DevBuf<int2> pairs, p1, p3, p4;
+};
+
 // Box ids are 0-based; ijk are the reference's 1-based grid indices; point
 // ranges are 0-based offsets into the tree-ordered arrays; iz/izt map tree
 // order -> user order (0-based).
@@ -26,6 +38,7 @@ struct Tree {
   std::vector<std::pair<int, int>> laddr;  // (first box, count) per level
   DevBuf<int> coll, ncoll;                 // list 5, 27 slots per box
   DevBuf<int> l1_start, l1_items, l2_start, l2_items, l3_start, l3_items, l4_start, l4_items;
+  TreeScratch scr;
 
   TreeDev dev() const {
     TreeDev t;

@@ -117,3 +117,33 @@ def test_batch_mixed_precision_error(gpu):
     # and the FP32 parts do change the result (the mixed path ran)
     assert rel(b[0], a[0]) > 1e-13
     P.close()
+
+
+def test_batch_host_entry_matches_device_batch(gpu):
+    # efmm_batch_host (host arrays, C ABI) == device-resident batch
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=3, ntarg=60, iprec=2, seed=17)
+    n, m = len(cen), len(tg)
+    R = 9
+    rng = np.random.default_rng(23)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, sdl, n, m)
+    ier, pt, st, ptt, stt = gpu.batch_host(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, tg, precision=0)
+    assert ier == 0
+    for x, y in zip((pt, st, ptt, stt), a):
+        assert rel(x, y) < SAME
+    P.close()
+
+
+def test_direct_subset_matches_full_direct(gpu):
+    torch = _t()
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=3, ntarg=10, iprec=2, seed=19)
+    n = len(cen)
+    rng = np.random.default_rng(29)
+    ssl, sdl = rng.normal(size=(n, 3)), rng.normal(size=(n, 3))
+    full = gpu.el3dtriadirecttarg(1.3, 0.7, tri, nrm, cen, ssl, sdl, tg)
+    ns = 100
+    u = torch.zeros((ns, 3), dtype=torch.float64, device="cuda")
+    e = torch.zeros((ns, 3, 3), dtype=torch.float64, device="cuda")
+    P.evaluate_direct_subset(1.3, 0.7, ns, d(ssl), d(sdl), u, e)
+    assert rel(u.cpu().numpy(), full[0][:ns]) < 1e-14 and rel(e.cpu().numpy(), full[1][:ns]) < 1e-14
+    P.close()
