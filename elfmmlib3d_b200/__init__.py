@@ -48,7 +48,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
-           "efmm_plan_evaluate_direct_subset", "efmm_batch_host"]
+           "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck"]
 
 
 class ElfmmError(RuntimeError):

@@ -85,6 +85,14 @@ __device__ __forceinline__ double warp_sum(double v) {
   } while (0)
 
 namespace efmm {
+// two-element vector type of a scalar (8- or 16-byte loads)
+template <class T>
+struct Vec2;
+template <>
+struct Vec2<double> { using type = double2; };
+template <>
+struct Vec2<float> { using type = float2; };
+
 struct CudaError {
   int code;
 };

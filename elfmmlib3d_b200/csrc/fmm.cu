@@ -38,28 +38,8 @@ __global__ void k_build_ops(int nop, const OpDesc* __restrict__ ops, double* __r
   long long tot = (long long)nc * nc;
   for (long long q = threadIdx.x; q < tot; q += blockDim.x) {
     int r = (int)(q / nc), c = (int)(q % nc);
-    // (n,m) of row r, (k,l) of column c
-    int n = 0;
-    while ((n + 1) * (n + 2) / 2 <= r) n++;
-    int m = r - n * (n + 1) / 2;
-    int k = 0;
-    while ((k + 1) * (k + 2) / 2 <= c) k++;
-    int l = c - k * (k + 1) / 2;
-    cplx A, B;
-    if (o.kind == 0) {
-      A = m2l_coef(tab, n, m, k, l);
-      B = m2l_coef(tab, n, m, k, -l);
-    } else if (o.kind == 1) {  // M2M: rows (n,m) parent, cols (k,l) child
-      double sc = ldexp(1.0, -k);
-      A = shift_coef(tab, n, m, k, l, sc);
-      B = shift_coef(tab, n, m, k, -l, sc);
-    } else {  // L2L: rows (n,m) child, cols (k,l) parent: 2^-n conj(Y_{k-n}^{l-m})
-      double sc = ldexp(1.0, -n);
-      A = shift_coef(tab, k, l, n, m, sc);
-      B = shift_coef(tab, k, -l, n, m, sc);
-    }
     double rr, ri, ir, ii;
-    real_block(A, B, l, &rr, &ri, &ir, &ii);
+    op_entry(o.kind, tab, r, c, &rr, &ri, &ir, &ii);
     size_t r2 = 2 * (size_t)r, c2 = 2 * (size_t)c;
     M[r2 * dim + c2] = rr;
     M[r2 * dim + c2 + 1] = ri;
@@ -196,13 +176,6 @@ k_p2m(const P2MArgs a) {
     }
   }
 }
-
-template <class T>
-struct Vec2;
-template <>
-struct Vec2<double> { using type = double2; };
-template <>
-struct Vec2<float> { using type = float2; };
 
 // ---------------------------------------------- P2M, many right-hand sides
 // For C = 4R columns the multipole of a leaf is a product

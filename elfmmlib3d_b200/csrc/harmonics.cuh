@@ -131,6 +131,34 @@ EFMM_HD cplx shift_coef(const cplx* Y, int nhi, int mhi, int nlo, int mlo, doubl
   return {scale_lo * y.re, -scale_lo * y.im};
 }
 
+// 2 x 2 real block of the operator of `kind` (0 M2L, 1 M2M, 2 L2L) between
+// output coefficient r = cidx(n,m) and input coefficient c = cidx(k,l), from
+// the harmonics table of the offset (irregular up to 2p for M2L, regular up
+// to p for the shifts).
+EFMM_HD void op_entry(int kind, const cplx* tab, int r, int c, double* rr, double* ri, double* ir,
+                      double* ii) {
+  int n = 0;
+  while ((n + 1) * (n + 2) / 2 <= r) n++;
+  int m = r - n * (n + 1) / 2;
+  int k = 0;
+  while ((k + 1) * (k + 2) / 2 <= c) k++;
+  int l = c - k * (k + 1) / 2;
+  cplx A, B;
+  if (kind == 0) {
+    A = m2l_coef(tab, n, m, k, l);
+    B = m2l_coef(tab, n, m, k, -l);
+  } else if (kind == 1) {  // M2M: rows (n,m) parent, cols (k,l) child
+    double sc = ldexp(1.0, -k);
+    A = shift_coef(tab, n, m, k, l, sc);
+    B = shift_coef(tab, n, m, k, -l, sc);
+  } else {  // L2L: rows (n,m) child, cols (k,l) parent: 2^-n conj(Y_{k-n}^{l-m})
+    double sc = ldexp(1.0, -n);
+    A = shift_coef(tab, k, l, n, m, sc);
+    B = shift_coef(tab, k, -l, n, m, sc);
+  }
+  real_block(A, B, l, rr, ri, ir, ii);
+}
+
 // Evaluate potential, gradient and Hessian of a local expansion at scaled
 // point z (box side s).  L: 2*ncoef(p) interleaved.  Outputs are the physical
 // derivatives (divided by s, s^2).  hess order: xx, yy, zz, xy, xz, yz.

@@ -4,6 +4,7 @@
 #include <mutex>
 #include <vector>
 #include <cstring>
+#include <cstdlib>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -172,6 +173,7 @@ void Plan::ensure_ops() {
       P->dims.push_back(dim);
       descs.push_back(d);
     }
+  P->descs = descs;
   P->mats.resize(off);
   DevBuf<OpDesc> dd;
   dd.resize(descs.size());
@@ -201,6 +203,8 @@ void Plan::ensure_ops() {
 
 // ------------------------------------------------------------------ plan
 Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
+  const char* tr = getenv("ELFMM3D_TRANSLATIONS");  // "dense": per-offset dense operators
+  factored_ = !(tr && strcmp(tr, "dense") == 0);
   for (int i = 0; i < 10; i++) EFMM_CUDA_TRY(cudaEventCreate(&ev_[i]));
 }
 Plan::~Plan() {
@@ -471,10 +475,92 @@ void Plan::cut_tasks(TransSched& S, int C) {
   S.C = C;
 }
 
+void Plan::cut_rot_tasks(TransSched& S, int C, int W) {
+  if (S.rC == C && S.rW == W) return;
+  std::vector<TransTask> tasks;
+  S.lev_rtasks.clear();
+  S.lev_rdim.clear();
+  const std::vector<int>& dims = ops_->dims;
+  for (auto& r : S.lev) {
+    // within a level, one launch per operator size (shared memory per size)
+    std::vector<int> segs;
+    for (int q = r.first; q < r.first + r.second; q++) segs.push_back(q);
+    std::stable_sort(segs.begin(), segs.end(),
+                     [&](int a, int b) { return dims[S.segs[a].group] > dims[S.segs[b].group]; });
+    size_t i = 0;
+    while (i < segs.size()) {
+      const int dim = dims[S.segs[segs[i]].group];
+      int t0 = (int)tasks.size();
+      for (; i < segs.size() && dims[S.segs[segs[i]].group] == dim; i++) {
+        const TransSeg& g = S.segs[segs[i]];
+        int ncols = g.npair * C;
+        for (int c0 = 0; c0 < ncols; c0 += W) tasks.push_back({g.group, 0, g.pair0, ncols, c0});
+      }
+      S.lev_rtasks.push_back({t0, (int)tasks.size() - t0});
+      S.lev_rdim.push_back(dim);
+    }
+  }
+  h2d(S.rtasks, tasks, st_);
+  S.rC = C;
+  S.rW = W;
+}
+
+// factored operators of the pool: host construction once per (device, p, eps)
+void Plan::ensure_factored() {
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  OpPool* P = ops_;
+  if (P->rot_ready) return;
+  std::vector<int> kinds, orders;
+  std::vector<double> offs;
+  for (const OpDesc& d : P->descs) {
+    kinds.push_back(d.kind);
+    orders.push_back(d.p);
+    offs.insert(offs.end(), {d.d[0], d.d[1], d.d[2]});
+  }
+  std::vector<RotOp> rops;
+  std::vector<double> pool;
+  build_factored_ops(p_, kinds, orders, offs, rops, pool);
+  std::vector<double> w(2 * (size_t)ncoef(p_));
+  for (int n = 0; n <= p_; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] =
+          std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<float> poolf;
+  normalise_factored_ops(kinds, rops, pool, w, poolf);
+  // device layout: blocks column-major
+  column_major_factored(rops, pool);
+  {
+    std::vector<double> tmp(poolf.begin(), poolf.end());
+    column_major_factored(rops, tmp);
+    for (size_t i = 0; i < tmp.size(); i++) poolf[i] = (float)tmp[i];
+  }
+  h2d(P->rot_ops, rops, st_);
+  h2d(P->rot_d, pool, st_);
+  h2d(P->rot_f, poolf, st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  P->rot_ready = true;
+}
+
 template <class T>
 void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst) {
-  cut_tasks(S, C);
   int D = 2 * ncoef(p_);
+  // factored form when its column tiles fit in shared memory
+  const int W = rot_cols_per_cta(D, (int)sizeof(T));
+  const size_t smem = sizeof(T) * 2 * (size_t)D * W;
+  if (factored_ && smem <= 227 * 1024) {
+    ensure_factored();
+    cut_rot_tasks(S, C, W);
+    const T* pool = nullptr;
+    if (sizeof(T) == 8)
+      pool = reinterpret_cast<const T*>(ops_->rot_d.get());
+    else
+      pool = reinterpret_cast<const T*>(ops_->rot_f.get());
+    for (size_t i = 0; i < S.lev_rtasks.size(); i++)
+      launch_translate_rot<T>(st_, S.lev_rtasks[i].second, S.rtasks.get() + S.lev_rtasks[i].first, S.pairs.get(),
+                              ops_->rot_ops.get(), pool, D, C, S.lev_rdim[i], src, dst);
+    return;
+  }
+  cut_tasks(S, C);
   for (auto& r : S.lev_tasks)
     launch_translate<T>(st_, r.second, S.tasks.get() + r.first, S.pairs.get(), mats, ops_->off.get(),
                         ops_->dim.get(), D, C, src, dst);

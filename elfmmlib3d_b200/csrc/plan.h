@@ -6,6 +6,7 @@
 #include "tree.h"
 #include "fmm.h"
 #include "kernels.h"
+#include "rotations.h"
 
 namespace efmm {
 
@@ -25,6 +26,13 @@ struct OpPool {
   DevBuf<float> mats_f;
   DevBuf<double> wnorm;   // w per real row (2 ncoef(p))
   DevBuf<int> kinds;      // operator kind per group (0 M2L, 1 M2M, 2 L2L)
+  std::vector<OpDesc> descs;
+  // factored form (rotation, shift along z, rotation back) of every group,
+  // FP64 factorial basis and FP32 normalised basis; made on first use
+  bool rot_ready = false;
+  DevBuf<RotOp> rot_ops;
+  DevBuf<double> rot_d;
+  DevBuf<float> rot_f;
   DevBuf<long long> off;
   DevBuf<int> dim;
   int m2l_group[343];
@@ -51,11 +59,19 @@ struct TransSched {
   int C = -1;
   DevBuf<TransTask> tasks;
   std::vector<std::pair<int, int>> lev_tasks;  // task ranges in execution order
+  // column tiles of the factored kernel (cut for C and tile width)
+  int rC = -1, rW = -1;
+  DevBuf<TransTask> rtasks;
+  std::vector<std::pair<int, int>> lev_rtasks;  // task ranges in execution order,
+  std::vector<int> lev_rdim;                     // each with its largest operator size
   void clear() {
     segs.clear();
     lev.clear();
     C = -1;
     lev_tasks.clear();
+    rC = rW = -1;
+    lev_rtasks.clear();
+    lev_rdim.clear();
   }
 };
 
@@ -142,6 +158,9 @@ class Plan {
   long long near_pairs_ = 0;
   TransSched m2m_, m2l_, l2l_;
   void cut_tasks(TransSched& S, int C);
+  void cut_rot_tasks(TransSched& S, int C, int W);
+  void ensure_factored();
+  bool factored_ = true;  // translations in factored form when they fit
   template <class T>
   void run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst);
   size_t m2l_pairs_h_ = 0;

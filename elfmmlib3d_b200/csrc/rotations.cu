@@ -1,0 +1,607 @@
+// rotations.cu -- translations factored as rotation, shift along z, rotation
+// back: host construction of the factored operators and the device kernel.
+//
+// The rotation blocks are obtained by least-squares fits of the harmonic
+// basis of one degree at fixed sample points on the unit sphere: the
+// coefficients of a field in the rotated frame are those that reproduce the
+// field's values at the sample points, mapped back through the rotation.
+// This uses only the evaluation routines of harmonics.cuh (the same
+// conventions as the dense operators, conjugate symmetry of real fields
+// included), and check_factored_ops compares the product with the dense
+// operator of every group.
+#include <algorithm>
+#include <cmath>
+#include <random>
+#include <thread>
+#include "common.cuh"
+#include "harmonics.cuh"
+#include "fmm.h"
+#include "rotations.h"
+
+namespace efmm {
+
+namespace {
+
+// offset (elements) of degree block n in a rotation part: sum_{j<n} (2j+2)^2
+EFMM_HD long long rot_block_off(int n) { return (long long)2 * n * (n + 1) * (2 * n + 1) / 3; }
+EFMM_HD long long rot_size(int p) { return rot_block_off(p + 1); }
+// offset of order block m in a shift part: sum_{m'<m} (2(p-m'+1))^2
+EFMM_HD long long sq_sum(long long x) { return x * (x + 1) * (2 * x + 1) / 6; }
+EFMM_HD long long z_block_off(int p, int m) { return 4 * (sq_sum(p + 1) - sq_sum(p + 1 - m)); }
+EFMM_HD long long z_size(int p) { return z_block_off(p, p + 1); }
+
+// Value of the field of storage slot s (= 2m + part) of degree n at a point,
+// from a harmonics table: multipole basis (irregular T, coefficient of T) or
+// local basis (conjugated regular Y).
+inline double slot_value(int basis, const cplx* tab, int n, int s) {
+  const int m = s >> 1, part = s & 1;
+  const double w = m == 0 ? 1.0 : 2.0;
+  const cplx v = tab[cidx(n, m)];
+  if (basis == 0) return part == 0 ? w * v.re : -w * v.im;
+  return part == 0 ? w * v.re : w * v.im;
+}
+
+struct Fitter {
+  int p = 0, K = 0;
+  std::vector<double> pts;             // K x 3
+  std::vector<std::vector<double>> pinv[2];  // [basis][n]: (2n+1) x K over active slots
+
+  void init(int pmax) {
+    p = pmax;
+    K = 2 * (2 * p + 2) + 16;
+    pts.resize(3 * (size_t)K);
+    const double ga = M_PI * (3.0 - std::sqrt(5.0));
+    for (int k = 0; k < K; k++) {
+      double z = 1.0 - (2.0 * k + 1.0) / K, r = std::sqrt(std::max(0.0, 1.0 - z * z)), ph = ga * k;
+      pts[3 * k] = r * std::cos(ph);
+      pts[3 * k + 1] = r * std::sin(ph);
+      pts[3 * k + 2] = z;
+    }
+    std::vector<cplx> tab(ncoef(p));
+    std::vector<std::vector<cplx>> T(K), Y(K);
+    for (int k = 0; k < K; k++) {
+      T[k].resize(ncoef(p));
+      Y[k].resize(ncoef(p));
+      irregular_harmonics(p, pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], T[k].data());
+      regular_harmonics(p, pts[3 * k], pts[3 * k + 1], pts[3 * k + 2], Y[k].data());
+    }
+    for (int basis = 0; basis < 2; basis++) {
+      pinv[basis].resize(p + 1);
+      for (int n = 0; n <= p; n++) {
+        const int b = 2 * n + 1;  // active slots: 0, then 2..2n+1
+        // B (K x b), column-scaled, thin QR by modified Gram-Schmidt (twice)
+        std::vector<double> Q((size_t)K * b), R((size_t)b * b, 0.0), sc(b);
+        for (int j = 0; j < b; j++) {
+          const int s = j == 0 ? 0 : j + 1;
+          double nrm = 0;
+          for (int k = 0; k < K; k++) {
+            double v = slot_value(basis, basis == 0 ? T[k].data() : Y[k].data(), n, s);
+            Q[(size_t)k * b + j] = v;
+            nrm += v * v;
+          }
+          sc[j] = nrm > 0 ? 1.0 / std::sqrt(nrm) : 1.0;
+          for (int k = 0; k < K; k++) Q[(size_t)k * b + j] *= sc[j];
+        }
+        for (int j = 0; j < b; j++) {
+          for (int pass = 0; pass < 2; pass++)
+            for (int i = 0; i < j; i++) {
+              double d = 0;
+              for (int k = 0; k < K; k++) d += Q[(size_t)k * b + i] * Q[(size_t)k * b + j];
+              for (int k = 0; k < K; k++) Q[(size_t)k * b + j] -= d * Q[(size_t)k * b + i];
+              R[(size_t)i * b + j] += d;
+            }
+          double nrm = 0;
+          for (int k = 0; k < K; k++) nrm += Q[(size_t)k * b + j] * Q[(size_t)k * b + j];
+          nrm = std::sqrt(nrm);
+          R[(size_t)j * b + j] = nrm;
+          for (int k = 0; k < K; k++) Q[(size_t)k * b + j] /= nrm;
+        }
+        // pinv = diag(sc) R^-1 Q^T
+        std::vector<double>& P = pinv[basis][n];
+        P.assign((size_t)b * K, 0.0);
+        for (int k = 0; k < K; k++) {
+          // solve R x = Q^T e_k by back substitution
+          std::vector<double> x(b);
+          for (int i = b - 1; i >= 0; i--) {
+            double v = Q[(size_t)k * b + i];
+            for (int j = i + 1; j < b; j++) v -= R[(size_t)i * b + j] * x[j];
+            x[i] = v / R[(size_t)i * b + i];
+          }
+          for (int i = 0; i < b; i++) P[(size_t)i * K + k] = sc[i] * x[i];
+        }
+      }
+    }
+  }
+
+  // Rotation of basis `basis` for frame change x' = Q3 x, degrees 0..pr,
+  // written as degree blocks into out (rot_size(pr) elements).
+  void rotation(int basis, int pr, const double Q3[9], double* out) const {
+    std::vector<std::vector<cplx>> tab(K);
+    for (int k = 0; k < K; k++) {
+      const double* x = &pts[3 * k];
+      // back-rotated point y = Q3^T x
+      double y[3];
+      for (int i = 0; i < 3; i++) y[i] = Q3[i] * x[0] + Q3[3 + i] * x[1] + Q3[6 + i] * x[2];
+      tab[k].resize(ncoef(pr));
+      if (basis == 0)
+        irregular_harmonics(pr, y[0], y[1], y[2], tab[k].data());
+      else
+        regular_harmonics(pr, y[0], y[1], y[2], tab[k].data());
+    }
+    for (int n = 0; n <= pr; n++) {
+      const int b = 2 * n + 1, bb = 2 * n + 2;
+      double* blk = out + rot_block_off(n);
+      std::fill(blk, blk + (size_t)bb * bb, 0.0);
+      const std::vector<double>& P = pinv[basis][n];
+      std::vector<double> g(K);
+      for (int j = 0; j < b; j++) {  // input slot
+        const int sj = j == 0 ? 0 : j + 1;
+        for (int k = 0; k < K; k++) g[k] = slot_value(basis, tab[k].data(), n, sj);
+        for (int i = 0; i < b; i++) {  // output slot
+          const int si = i == 0 ? 0 : i + 1;
+          double v = 0;
+          const double* Pi = &P[(size_t)i * K];
+          for (int k = 0; k < K; k++) v += Pi[k] * g[k];
+          blk[(size_t)si * bb + sj] = v;
+        }
+      }
+    }
+  }
+};
+
+// frame rotation with Q3 d = |d| e_z (rows u1, u2, d^)
+void frame_for(const double d[3], double Q3[9]) {
+  double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  double u3[3] = {d[0] / r, d[1] / r, d[2] / r};
+  if (std::fabs(u3[0]) < 1e-14 && std::fabs(u3[1]) < 1e-14) {
+    double s = u3[2] > 0 ? 1.0 : -1.0;  // identity, or a half turn about x
+    const double q[9] = {1, 0, 0, 0, s, 0, 0, 0, s};
+    for (int i = 0; i < 9; i++) Q3[i] = q[i];
+    return;
+  }
+  double u1[3] = {-u3[1], u3[0], 0.0};  // e_z x d^
+  double n1 = std::sqrt(u1[0] * u1[0] + u1[1] * u1[1]);
+  u1[0] /= n1;
+  u1[1] /= n1;
+  double u2[3] = {u3[1] * u1[2] - u3[2] * u1[1], u3[2] * u1[0] - u3[0] * u1[2], u3[0] * u1[1] - u3[1] * u1[0]};
+  for (int i = 0; i < 3; i++) {
+    Q3[i] = u1[i];
+    Q3[3 + i] = u2[i];
+    Q3[6 + i] = u3[i];
+  }
+}
+
+// shift along z by rho of `kind` truncated at p, order blocks into out
+void zshift(int kind, int p, double rho, double* out) {
+  std::vector<cplx> tab(ncoef(2 * p + 1));
+  if (kind == 0)
+    irregular_harmonics(2 * p, 0.0, 0.0, rho, tab.data());
+  else
+    regular_harmonics(p, 0.0, 0.0, rho, tab.data());
+  for (int m = 0; m <= p; m++) {
+    const int bz = 2 * (p - m + 1);
+    double* blk = out + z_block_off(p, m);
+    for (int n = m; n <= p; n++)
+      for (int k = m; k <= p; k++) {
+        double rr, ri, ir, ii;
+        op_entry(kind, tab.data(), cidx(n, m), cidx(k, m), &rr, &ri, &ir, &ii);
+        const int a = 2 * (n - m), c = 2 * (k - m);
+        blk[(size_t)a * bz + c] = rr;
+        blk[(size_t)a * bz + c + 1] = ri;
+        blk[(size_t)(a + 1) * bz + c] = ir;
+        blk[(size_t)(a + 1) * bz + c + 1] = ii;
+      }
+  }
+}
+
+template <class F>
+void parallel_for(int n, F f) {
+  int nt = (int)std::max(1u, std::min(64u, std::thread::hardware_concurrency()));
+  nt = std::min(nt, std::max(n, 1));
+  std::vector<std::thread> th;
+  for (int t = 0; t < nt; t++)
+    th.emplace_back([&, t]() {
+      for (int i = t; i < n; i += nt) f(i);
+    });
+  for (auto& x : th) x.join();
+}
+
+}  // namespace
+
+void build_factored_ops(int pmax, const std::vector<int>& kinds, const std::vector<int>& orders,
+                        const std::vector<double>& offsets, std::vector<RotOp>& ops,
+                        std::vector<double>& pool) {
+  Fitter F;
+  F.init(pmax);
+  const int ng = (int)kinds.size();
+  ops.resize(ng);
+  long long off = 0;
+  for (int g = 0; g < ng; g++) {
+    const int p = orders[g];
+    ops[g].p = p;
+    ops[g].fw = off;
+    off += rot_size(p);
+    ops[g].z = off;
+    off += z_size(p);
+    ops[g].bk = off;
+    off += rot_size(p);
+  }
+  pool.assign((size_t)off, 0.0);
+  parallel_for(ng, [&](int g) {
+    const int kind = kinds[g], p = orders[g];
+    const double* d = &offsets[3 * g];
+    double Q3[9], Qt[9];
+    frame_for(d, Q3);
+    for (int i = 0; i < 3; i++)
+      for (int j = 0; j < 3; j++) Qt[3 * i + j] = Q3[3 * j + i];
+    const double rho = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+    // input basis of the forward rotation, output basis of the backward one
+    const int bin = kind == 2 ? 1 : 0, bout = kind == 1 ? 0 : 1;
+    F.rotation(bin, p, Q3, &pool[ops[g].fw]);
+    zshift(kind, p, rho, &pool[ops[g].z]);
+    F.rotation(bout, p, Qt, &pool[ops[g].bk]);
+  });
+}
+
+void normalise_factored_ops(const std::vector<int>& kinds, const std::vector<RotOp>& ops,
+                            const std::vector<double>& pool, const std::vector<double>& w,
+                            std::vector<float>& out) {
+  out.assign(pool.size(), 0.0f);
+  parallel_for((int)ops.size(), [&](int g) {
+    const RotOp& o = ops[g];
+    const int kind = kinds[g], p = o.p;
+    // scale factors: multipole rows x w, local rows / w (columns inverse)
+    auto rs = [&](bool local, int row) { return local ? 1.0 / w[row] : w[row]; };
+    const bool fw_in_local = kind == 2, z_in_local = kind == 2, z_out_local = kind != 1,
+               bk_local = kind != 1;
+    for (int n = 0; n <= p; n++) {
+      const int bb = 2 * n + 2, r0 = n * (n + 1);
+      for (int i = 0; i < bb; i++)
+        for (int j = 0; j < bb; j++) {
+          size_t q = (size_t)i * bb + j;
+          out[o.fw + rot_block_off(n) + q] =
+              (float)(pool[o.fw + rot_block_off(n) + q] * rs(fw_in_local, r0 + i) / rs(fw_in_local, r0 + j));
+          out[o.bk + rot_block_off(n) + q] =
+              (float)(pool[o.bk + rot_block_off(n) + q] * rs(bk_local, r0 + i) / rs(bk_local, r0 + j));
+        }
+    }
+    for (int m = 0; m <= p; m++) {
+      const int bz = 2 * (p - m + 1);
+      for (int a = 0; a < bz; a++)
+        for (int c = 0; c < bz; c++) {
+          const int ra = 2 * cidx(m + a / 2, m) + (a & 1), rc = 2 * cidx(m + c / 2, m) + (c & 1);
+          size_t q = (size_t)z_block_off(p, m) + (size_t)a * bz + c;
+          out[o.z + q] = (float)(pool[o.z + q] * rs(z_out_local, ra) / rs(z_in_local, rc));
+        }
+    }
+  });
+}
+
+void column_major_factored(const std::vector<RotOp>& ops, std::vector<double>& pool) {
+  parallel_for((int)ops.size(), [&](int g) {
+    const RotOp& o = ops[g];
+    const int p = o.p;
+    std::vector<double> tmp;
+    auto tr = [&](long long off, int b) {
+      tmp.assign(pool.begin() + off, pool.begin() + off + (size_t)b * b);
+      for (int i = 0; i < b; i++)
+        for (int j = 0; j < b; j++) pool[off + (size_t)j * b + i] = tmp[(size_t)i * b + j];
+    };
+    for (int n = 0; n <= p; n++) {
+      tr(o.fw + rot_block_off(n), 2 * n + 2);
+      tr(o.bk + rot_block_off(n), 2 * n + 2);
+    }
+    for (int m = 0; m <= p; m++) tr(o.z + z_block_off(p, m), 2 * (p - m + 1));
+  });
+}
+
+double check_factored_ops(const std::vector<int>& kinds, const std::vector<int>& orders,
+                          const std::vector<double>& offsets, const std::vector<RotOp>& ops,
+                          const std::vector<double>& pool, int stride) {
+  double worst = 0;
+  std::mt19937_64 rng(7);
+  std::normal_distribution<double> N01;
+  for (int g = 0; g < (int)kinds.size(); g += std::max(stride, 1)) {
+    const int kind = kinds[g], p = orders[g], nc = ncoef(p), dim = 2 * nc;
+    const double* d = &offsets[3 * g];
+    std::vector<cplx> tab(ncoef(2 * p + 1));
+    if (kind == 0)
+      irregular_harmonics(2 * p, d[0], d[1], d[2], tab.data());
+    else
+      regular_harmonics(p, d[0], d[1], d[2], tab.data());
+    // a random expansion of a real field (Im of m = 0 is zero), O(1) in the
+    // normalised basis (multipole x w, local / w, w = sqrt((n+m)!(n-m)!)),
+    // where the harmonics are O(1) and the error measure is meaningful
+    std::vector<double> v(dim), a(dim, 0.0), f(dim, 0.0), z(dim, 0.0), b(dim, 0.0), wr(dim);
+    for (int n = 0; n <= p; n++)
+      for (int m = 0; m <= n; m++)
+        wr[2 * cidx(n, m)] = wr[2 * cidx(n, m) + 1] =
+            std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+    const bool in_local = kind == 2, out_local = kind != 1;
+    for (int q = 0; q < dim; q++) v[q] = N01(rng) * (in_local ? wr[q] : 1.0 / wr[q]);
+    for (int n = 0; n <= p; n++) v[2 * cidx(n, 0) + 1] = 0.0;
+    for (int r = 0; r < nc; r++)
+      for (int c = 0; c < nc; c++) {
+        double rr, ri, ir, ii;
+        op_entry(kind, tab.data(), r, c, &rr, &ri, &ir, &ii);
+        a[2 * r] += rr * v[2 * c] + ri * v[2 * c + 1];
+        a[2 * r + 1] += ir * v[2 * c] + ii * v[2 * c + 1];
+      }
+    const RotOp& o = ops[g];
+    for (int n = 0; n <= p; n++) {
+      const int bb = 2 * n + 2, r0 = n * (n + 1);
+      const double* B = &pool[o.fw + rot_block_off(n)];
+      for (int i = 0; i < bb; i++)
+        for (int j = 0; j < bb; j++) f[r0 + i] += B[(size_t)i * bb + j] * v[r0 + j];
+    }
+    for (int m = 0; m <= p; m++) {
+      const int bz = 2 * (p - m + 1);
+      const double* Z = &pool[o.z + z_block_off(p, m)];
+      for (int a_ = 0; a_ < bz; a_++)
+        for (int c = 0; c < bz; c++)
+          z[2 * cidx(m + a_ / 2, m) + (a_ & 1)] += Z[(size_t)a_ * bz + c] * f[2 * cidx(m + c / 2, m) + (c & 1)];
+    }
+    for (int n = 0; n <= p; n++) {
+      const int bb = 2 * n + 2, r0 = n * (n + 1);
+      const double* B = &pool[o.bk + rot_block_off(n)];
+      for (int i = 0; i < bb; i++)
+        for (int j = 0; j < bb; j++) b[r0 + i] += B[(size_t)i * bb + j] * z[r0 + j];
+    }
+    double num = 0, den = 0;
+    for (int n = 0; n <= p; n++)
+      for (int m = 0; m <= n; m++)
+        for (int part = 0; part < 2; part++) {
+          if (m == 0 && part == 1) continue;  // not part of a real field
+          const int q = 2 * cidx(n, m) + part;
+          const double sc = out_local ? 1.0 / wr[q] : wr[q];
+          num += (a[q] - b[q]) * (a[q] - b[q]) * sc * sc;
+          den += a[q] * a[q] * sc * sc;
+        }
+    worst = std::max(worst, std::sqrt(num / std::max(den, 1e-300)));
+  }
+  return worst;
+}
+
+// ------------------------------------------------------------------ kernel
+// One CTA per tile of NCT columns of one group.  The columns are staged in
+// shared memory (rows x NCT), rotated (X -> Y), shifted (Y -> X), rotated
+// back (X -> Y) and added to the destinations.  The device pool stores every
+// block column-major, so the 8 coefficients a warp works on read one
+// contiguous operator segment per k; a lane computes the re and im rows of
+// one coefficient for G consecutive columns (G = 4 FP32, 2 FP64).
+template <class T>
+struct Vec4T;
+template <>
+struct Vec4T<float> {
+  static __device__ __forceinline__ void ld(const float* p, float* v) {
+    float4 q = *reinterpret_cast<const float4*>(p);
+    v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+  }
+  static __device__ __forceinline__ void st(float* p, const float* v) {
+    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+};
+template <>
+struct Vec4T<double> {
+  static __device__ __forceinline__ void ld(const double* p, double* v) {
+    double2 q = *reinterpret_cast<const double2*>(p);
+    v[0] = q.x; v[1] = q.y;
+  }
+  static __device__ __forceinline__ void st(double* p, const double* v) {
+    *reinterpret_cast<double2*>(p) = make_double2(v[0], v[1]);
+  }
+};
+
+__device__ __forceinline__ void coef_nm(int cc, int& n, int& m) {
+  n = (int)((sqrt(8.0 * cc + 1.0) - 1.0) * 0.5);
+  while ((n + 1) * (n + 2) / 2 <= cc) n++;
+  while (n * (n + 1) / 2 > cc) n--;
+  m = cc - n * (n + 1) / 2;
+}
+
+template <class T, int NCT>
+__global__ void __launch_bounds__(256)
+k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
+                const RotOp* __restrict__ ops, const T* __restrict__ pool, int D, int C,
+                const T* __restrict__ src, T* __restrict__ dst) {
+  constexpr int G = NCT / 4;  // columns per lane
+  using V = Vec4T<T>;
+  using V2 = typename Vec2<T>::type;
+  extern __shared__ __align__(16) unsigned char rt_smem[];
+  const TransTask t = tasks[blockIdx.x];
+  const RotOp op = ops[t.group];
+  const int p = op.p, dim = (p + 1) * (p + 2), nc = dim / 2;
+  T* X = reinterpret_cast<T*>(rt_smem);
+  T* Y = X + (size_t)dim * NCT;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // stage: thread (row r, column group) loads G columns, one vector store
+  {
+    const T* sp[NCT];
+#pragma unroll
+    for (int j = 0; j < NCT; j++) {
+      const int col = t.col0 + j;
+      sp[j] = nullptr;
+      if (col < t.ncols) {
+        const TransPair pr = pairs[t.pair0 + col / C];
+        sp[j] = src + ((size_t)pr.src * C + col % C) * D;
+      }
+    }
+    for (int q = tid; q < dim * 4; q += 256) {
+      const int r = q % dim, cg = q / dim;
+      T v[G];
+#pragma unroll
+      for (int g = 0; g < G; g++) v[g] = sp[cg * G + g] ? sp[cg * G + g][r] : T(0);
+      V::st(X + (size_t)r * NCT + cg * G, v);
+    }
+  }
+  __syncthreads();
+  const int sub = lane >> 2, cg = lane & 3;  // coefficient within the warp's 8, column group
+  // rotation stage (degree blocks), coefficients in storage order
+  auto rotate = [&](const T* in, T* out, long long base) {
+    for (int c0 = warp * 8; c0 < nc; c0 += 64) {
+      const int cc = c0 + sub;
+      if (cc >= nc) continue;
+      int n, m;
+      coef_nm(cc, n, m);
+      const int r0 = n * (n + 1), bb = 2 * n + 2;
+      const T* o = pool + base + rot_block_off(n) + 2 * m;  // column-major: (row, k) at k*bb + row
+      T a0[G], a1[G];
+#pragma unroll
+      for (int g = 0; g < G; g++) a0[g] = a1[g] = T(0);
+      // bb = 2n + 2 is even: two k per step, operator pairs as vectors,
+      // UNR steps of loads issued before their products
+      constexpr int UNR = 4;
+      int k = 0;
+      for (; k + 2 * UNR <= bb; k += 2 * UNR) {
+        V2 w[2 * UNR];
+#pragma unroll
+        for (int u = 0; u < 2 * UNR; u++) w[u] = *reinterpret_cast<const V2*>(o + (size_t)(k + u) * bb);
+#pragma unroll
+        for (int u = 0; u < 2 * UNR; u++) {
+          T xv[G];
+          V::ld(in + (size_t)(r0 + k + u) * NCT + cg * G, xv);
+#pragma unroll
+          for (int g = 0; g < G; g++) {
+            a0[g] += w[u].x * xv[g];
+            a1[g] += w[u].y * xv[g];
+          }
+        }
+      }
+      for (; k < bb; k++) {
+        const V2 w = *reinterpret_cast<const V2*>(o + (size_t)k * bb);
+        T xv[G];
+        V::ld(in + (size_t)(r0 + k) * NCT + cg * G, xv);
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          a0[g] += w.x * xv[g];
+          a1[g] += w.y * xv[g];
+        }
+      }
+      V::st(out + (size_t)(2 * cc) * NCT + cg * G, a0);
+      V::st(out + (size_t)(2 * cc + 1) * NCT + cg * G, a1);
+    }
+  };
+  rotate(X, Y, op.fw);
+  __syncthreads();
+  // shift along z: coefficients in order-major order (m, then n = m..p)
+  for (int q0 = warp * 8; q0 < nc; q0 += 64) {
+    const int q = q0 + sub;
+    if (q >= nc) continue;
+    int m = 0, start = 0;
+    while (start + (p - m + 1) <= q) {
+      start += p - m + 1;
+      m++;
+    }
+    const int n = m + (q - start);
+    const int bz = 2 * (p - m + 1), a = 2 * (n - m);
+    const T* o = pool + op.z + z_block_off(p, m) + a;  // column-major: (row, col) at col*bz + row
+    T a0[G], a1[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) a0[g] = a1[g] = T(0);
+    int k = m;
+    constexpr int UNZ = 4;
+    for (; k + UNZ <= p + 1; k += UNZ) {
+      V2 wr[UNZ], wi[UNZ];
+#pragma unroll
+      for (int u = 0; u < UNZ; u++) {
+        const int c = 2 * (k + u - m);
+        wr[u] = *reinterpret_cast<const V2*>(o + (size_t)c * bz);
+        wi[u] = *reinterpret_cast<const V2*>(o + (size_t)(c + 1) * bz);
+      }
+#pragma unroll
+      for (int u = 0; u < UNZ; u++) {
+        const int rk = 2 * ((k + u) * (k + u + 1) / 2 + m);
+        T xr[G], xi[G];
+        V::ld(Y + (size_t)rk * NCT + cg * G, xr);
+        V::ld(Y + (size_t)(rk + 1) * NCT + cg * G, xi);
+#pragma unroll
+        for (int g = 0; g < G; g++) {
+          a0[g] += wr[u].x * xr[g] + wi[u].x * xi[g];
+          a1[g] += wr[u].y * xr[g] + wi[u].y * xi[g];
+        }
+      }
+    }
+    for (; k <= p; k++) {
+      const int c = 2 * (k - m);
+      const V2 wr = *reinterpret_cast<const V2*>(o + (size_t)c * bz);
+      const V2 wi = *reinterpret_cast<const V2*>(o + (size_t)(c + 1) * bz);
+      const int rk = 2 * (k * (k + 1) / 2 + m);
+      T xr[G], xi[G];
+      V::ld(Y + (size_t)rk * NCT + cg * G, xr);
+      V::ld(Y + (size_t)(rk + 1) * NCT + cg * G, xi);
+#pragma unroll
+      for (int g = 0; g < G; g++) {
+        a0[g] += wr.x * xr[g] + wi.x * xi[g];
+        a1[g] += wr.y * xr[g] + wi.y * xi[g];
+      }
+    }
+    const int cc = n * (n + 1) / 2 + m;
+    V::st(X + (size_t)(2 * cc) * NCT + cg * G, a0);
+    V::st(X + (size_t)(2 * cc + 1) * NCT + cg * G, a1);
+  }
+  __syncthreads();
+  rotate(X, Y, op.bk);
+  __syncthreads();
+  for (int j = 0; j < NCT; j++) {
+    const int col = t.col0 + j;
+    if (col >= t.ncols) break;
+    const TransPair pr = pairs[t.pair0 + col / C];
+    T* dp = dst + ((size_t)pr.dst * C + col % C) * D;
+    const T al = (T)pr.alpha;
+    for (int r = tid; r < dim; r += 256) atomicAdd(dp + r, al * Y[(size_t)r * NCT + j]);
+  }
+}
+
+int rot_cols_per_cta(int maxdim, int elem_bytes) {
+  (void)maxdim;
+  return elem_bytes == 4 ? 16 : 8;
+}
+
+template <class T>
+void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
+                          const RotOp* ops, const T* pool, int D, int C, int maxdim, const T* src, T* dst) {
+  if (ntask <= 0) return;
+  constexpr int NCT = sizeof(T) == 4 ? 16 : 8;
+  const size_t smem = sizeof(T) * 2 * (size_t)maxdim * NCT;
+  if (smem > 227 * 1024) throw CudaError{(int)cudaErrorInvalidValue};
+  auto kern = k_translate_rot<T, NCT>;
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kern<<<ntask, 256, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+template void launch_translate_rot<double>(cudaStream_t, int, const TransTask*, const TransPair*, const RotOp*,
+                                           const double*, int, int, int, const double*, double*);
+template void launch_translate_rot<float>(cudaStream_t, int, const TransTask*, const TransPair*, const RotOp*,
+                                          const float*, int, int, int, const float*, float*);
+
+}  // namespace efmm
+
+// CPU self-check of the factored operators (no device needed): largest
+// relative difference to the dense operators over every `stride`-th group of
+// the M2L offsets (|max| 2..3 in [-3,3]^3) and the 8 M2M and 8 L2L shifts at
+// order p and tolerance eps.  Returns the number of groups built.
+extern "C" int efmm_factored_selfcheck(int p, double eps, int stride, double* worst) {
+  using namespace efmm;
+  std::vector<int> kinds, orders;
+  std::vector<double> offs;
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = -3; k <= 3; k++) {
+        if (std::max(std::abs(i), std::max(std::abs(j), std::abs(k))) < 2) continue;
+        kinds.push_back(0);
+        orders.push_back(std::min(p, eps > 0 ? m2l_order(eps, i, j, k) : p));
+        offs.insert(offs.end(), {(double)i, (double)j, (double)k});
+      }
+  for (int kind = 1; kind <= 2; kind++)
+    for (int dg = 0; dg < 8; dg++) {
+      kinds.push_back(kind);
+      orders.push_back(p);
+      offs.insert(offs.end(), {(dg & 1) ? 0.25 : -0.25, ((dg >> 1) & 1) ? 0.25 : -0.25,
+                               ((dg >> 2) & 1) ? 0.25 : -0.25});
+    }
+  std::vector<RotOp> ops;
+  std::vector<double> pool;
+  build_factored_ops(p, kinds, orders, offs, ops, pool);
+  *worst = check_factored_ops(kinds, orders, offs, ops, pool, stride);
+  return (int)kinds.size();
+}

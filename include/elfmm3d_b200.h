@@ -161,6 +161,13 @@ int efmm_plan_evaluate_direct(efmm_plan *plan, double rlam, double rmu, const do
                               const double *sdl, double *u_src, double *e_src, double *u_tgt,
                               double *e_tgt);
 
+/* CPU self-check (no device): builds the factored translation operators
+ * (rotation, shift along z, rotation back) of the 316 M2L offsets and the
+ * 8 M2M and 8 L2L shifts at order p and tolerance eps and stores in *worst
+ * the largest relative difference to the dense operators over every
+ * stride-th of them.  Returns the number of operators built. */
+int efmm_factored_selfcheck(int p, double eps, int stride, double *worst);
+
 /* Number of this library's kernels launched so far in the process. */
 long long efmm_kernel_launches(void);
 
