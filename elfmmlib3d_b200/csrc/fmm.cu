@@ -488,7 +488,7 @@ k_p2m_weights(const P2MArgs a, int R, const int* __restrict__ wleaves, const lon
 // output tiles (GemmTask), 8 x 8 outputs per thread, K tiles of 16
 // double-buffered in shared memory; C is stored (each task owns its tile).
 template <class T>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 2 : 1)
 k_gemm_tn(const GemmTask* __restrict__ tasks, const T* __restrict__ A, const T* __restrict__ B,
           T* __restrict__ Cm) {
   using V2 = typename Vec2<T>::type;
@@ -873,7 +873,7 @@ k_l2t(const L2TArgs a) {
 // warp w owns point w, lane l the columns of right-hand sides l and l + 32;
 // FP64 throughout (the local expansions may be FP32 in the normalised
 // basis, converted while staged), then the Lame recombination of k_l2t.
-constexpr int LG_PTS = 8, LG_K = 16, LG_C = 256;
+constexpr int LG_PTS = 8, LG_K = 16, LG_C = 256, LG_CP = LG_C + 2;  // padded row: conflict-light staging
 
 struct LgTerm {
   int a, b, sg, im;  // shift in n, shift in m, sign, imaginary part
@@ -890,7 +890,7 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
   const int p = a.p, nc = ncoef(p), D = 2 * nc, C = 4 * R;
   cplx* Ys = reinterpret_cast<cplx*>(lg_smem);                     // [LG_PTS][nc]
   double* Gs = reinterpret_cast<double*>(Ys + LG_PTS * nc);         // [LG_K][LG_PTS][9]
-  double* Bs = Gs + LG_K * LG_PTS * 9;                              // [LG_K][LG_C]
+  double* Bs = Gs + LG_K * LG_PTS * 9;                              // [LG_K][LG_CP]
   const int box = a.leaves[chunk_leaf[blockIdx.x]];
   const int e0 = chunk_e0[blockIdx.x];
   const int col0 = blockIdx.y * LG_C;
@@ -981,7 +981,7 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
         b = (double)Lb[(size_t)gcol * D + row];
         if (wnorm) b *= wnorm[row];
       }
-      Bs[kk * LG_C + col] = b;
+      Bs[kk * LG_CP + col] = b;
     }
     __syncthreads();
 #pragma unroll 4
@@ -991,7 +991,7 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
       for (int v = 0; v < 9; v++) gv[v] = Gs[(kk * LG_PTS + warp) * 9 + v];
 #pragma unroll
       for (int h = 0; h < 2; h++) {
-        const double* br = Bs + kk * LG_C + 128 * h + 4 * lane;
+        const double* br = Bs + kk * LG_CP + 128 * h + 4 * lane;
         const double2 u0 = *reinterpret_cast<const double2*>(br);
         const double2 u1 = *reinterpret_cast<const double2*>(br + 2);
         bv[4 * h] = u0.x; bv[4 * h + 1] = u0.y; bv[4 * h + 2] = u1.x; bv[4 * h + 3] = u1.y;
@@ -1097,7 +1097,7 @@ template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
                      int R, const TB* local, const double* wnorm) {
   const int nc = ncoef(a.p);
-  size_t smem = sizeof(cplx) * LG_PTS * nc + sizeof(double) * (LG_K * LG_PTS * 9 + LG_K * LG_C);
+  size_t smem = sizeof(cplx) * LG_PTS * nc + sizeof(double) * (LG_K * LG_PTS * 9 + LG_K * LG_CP);
   if (smem > 227 * 1024) return false;
   if (nchunk <= 0 || R <= 0) return true;
   EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_gemm<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

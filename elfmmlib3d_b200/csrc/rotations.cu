@@ -365,7 +365,8 @@ double check_factored_ops(const std::vector<int>& kinds, const std::vector<int>&
 // ------------------------------------------------------------------ kernel
 // One CTA per tile of NCT columns of one group.  The columns are staged in
 // shared memory (rows x NCT), rotated (X -> Y), shifted (Y -> X), rotated
-// back (X -> Y) and added to the destinations.  The device pool stores every
+// back (X -> Y) and added to the destinations (ROT_THREADS threads: the
+// operator loads come from L2, so more warps hide more of their latency).  The device pool stores every
 // block column-major, so the 8 coefficients a warp works on read one
 // contiguous operator segment per k; a lane computes the re and im rows of
 // one coefficient for G consecutive columns (G = 4 FP32, 2 FP64).
@@ -399,8 +400,10 @@ __device__ __forceinline__ void coef_nm(int cc, int& n, int& m) {
   m = cc - n * (n + 1) / 2;
 }
 
+constexpr int ROT_THREADS = 512;
+
 template <class T, int NCT>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(ROT_THREADS)
 k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
                 const RotOp* __restrict__ ops, const T* __restrict__ pool, int D, int C,
                 const T* __restrict__ src, T* __restrict__ dst) {
@@ -426,7 +429,7 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
         sp[j] = src + ((size_t)pr.src * C + col % C) * D;
       }
     }
-    for (int q = tid; q < dim * 4; q += 256) {
+    for (int q = tid; q < dim * 4; q += ROT_THREADS) {
       const int r = q % dim, cg = q / dim;
       T v[G];
 #pragma unroll
@@ -438,7 +441,7 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
   const int sub = lane >> 2, cg = lane & 3;  // coefficient within the warp's 8, column group
   // rotation stage (degree blocks), coefficients in storage order
   auto rotate = [&](const T* in, T* out, long long base) {
-    for (int c0 = warp * 8; c0 < nc; c0 += 64) {
+    for (int c0 = warp * 8; c0 < nc; c0 += ROT_THREADS / 4) {
       const int cc = c0 + sub;
       if (cc >= nc) continue;
       int n, m;
@@ -484,7 +487,7 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
   rotate(X, Y, op.fw);
   __syncthreads();
   // shift along z: coefficients in order-major order (m, then n = m..p)
-  for (int q0 = warp * 8; q0 < nc; q0 += 64) {
+  for (int q0 = warp * 8; q0 < nc; q0 += ROT_THREADS / 4) {
     const int q = q0 + sub;
     if (q >= nc) continue;
     int m = 0, start = 0;
@@ -548,7 +551,7 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
     const TransPair pr = pairs[t.pair0 + col / C];
     T* dp = dst + ((size_t)pr.dst * C + col % C) * D;
     const T al = (T)pr.alpha;
-    for (int r = tid; r < dim; r += 256) atomicAdd(dp + r, al * Y[(size_t)r * NCT + j]);
+    for (int r = tid; r < dim; r += ROT_THREADS) atomicAdd(dp + r, al * Y[(size_t)r * NCT + j]);
   }
 }
 
@@ -566,7 +569,7 @@ void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, co
   if (smem > 227 * 1024) throw CudaError{(int)cudaErrorInvalidValue};
   auto kern = k_translate_rot<T, NCT>;
   EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  kern<<<ntask, 256, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst); count_launch();
+  kern<<<ntask, ROT_THREADS, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template void launch_translate_rot<double>(cudaStream_t, int, const TransTask*, const TransPair*, const RotOp*,
