@@ -55,6 +55,34 @@ __global__ void k_gather(int n, int w, const int* __restrict__ perm, const doubl
   size_t r = (size_t)blockIdx.y * w * n;  // right-hand side blockIdx.y
   for (int c = 0; c < w; c++) out[r + (size_t)w * i + c] = in[r + (size_t)w * j + c];
 }
+// M2L pairs of list 2: pass 0 counts per operator group, pass 1 places
+// (src box, dst box, 1/s) at the group's cursor
+__global__ void k_m2l_pairs(int nb, int pass, const int* __restrict__ level, const int* __restrict__ ijk,
+                            const int* __restrict__ scount, const int* __restrict__ tcount,
+                            const int* __restrict__ l2s, const int* __restrict__ l2i, const int* __restrict__ m2lg,
+                            double size, int* __restrict__ cnt, int* __restrict__ cursor,
+                            TransPair* __restrict__ out) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  if (level[b] < 2 || scount[b] + tcount[b] == 0) return;
+  const double inv_s = (double)(1ull << level[b]) / size;
+  for (int q = l2s[b]; q < l2s[b + 1]; q++) {
+    const int sb = l2i[q];
+    if (scount[sb] == 0) continue;
+    const int di = ijk[3 * b] - ijk[3 * sb], dj = ijk[3 * b + 1] - ijk[3 * sb + 1],
+              dk = ijk[3 * b + 2] - ijk[3 * sb + 2];
+    if (di < -3 || di > 3 || dj < -3 || dj > 3 || dk < -3 || dk > 3) continue;  // not a list-2 offset
+    const int g = m2lg[(di + 3) * 49 + (dj + 3) * 7 + (dk + 3)];
+    if (g < 0) continue;
+    if (pass == 0) {
+      atomicAdd(&cnt[g], 1);
+    } else {
+      const int pos = atomicAdd(&cursor[g], 1);
+      out[pos] = TransPair{sb, b, inv_s};
+    }
+  }
+}
+
 // user (R, n, 3) -> tree order, right-hand side innermost: out[(i*3+d)*R + r]
 __global__ void k_gather_rhs(int n, int R, const int* __restrict__ perm, const double* __restrict__ in,
                              double* __restrict__ out) {
@@ -121,6 +149,19 @@ __global__ void k_ops_normalised(const int* __restrict__ kinds, const long long*
   }
 }
 
+template <class T>
+static std::vector<T> d2h(const DevBuf<T>& b, size_t n, cudaStream_t st) {
+  std::vector<T> h(n);
+  if (n) EFMM_CUDA_TRY(cudaMemcpyAsync(h.data(), b.get(), n * sizeof(T), cudaMemcpyDeviceToHost, st));
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+  return h;
+}
+template <class T>
+static void h2d(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
+  b.resize(h.size());
+  if (!h.empty()) EFMM_CUDA_TRY(cudaMemcpyAsync(b.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+}
+
 // --------------------------------------------------------------- op pools
 static std::mutex g_ops_mu;
 static std::map<std::pair<int, std::pair<int, long long>>, OpPool*> g_ops;  // (device, (p, eps bits))
@@ -174,6 +215,10 @@ void Plan::ensure_ops() {
       descs.push_back(d);
     }
   P->descs = descs;
+  {
+    std::vector<int> g(P->m2l_group, P->m2l_group + 343);
+    h2d(P->m2lg_dev, g, st_);
+  }
   P->mats.resize(off);
   DevBuf<OpDesc> dd;
   dd.resize(descs.size());
@@ -209,19 +254,6 @@ Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
 }
 Plan::~Plan() {
   for (int i = 0; i < 10; i++) cudaEventDestroy(ev_[i]);
-}
-
-template <class T>
-static std::vector<T> d2h(const DevBuf<T>& b, size_t n, cudaStream_t st) {
-  std::vector<T> h(n);
-  if (n) EFMM_CUDA_TRY(cudaMemcpyAsync(h.data(), b.get(), n * sizeof(T), cudaMemcpyDeviceToHost, st));
-  EFMM_CUDA_TRY(cudaStreamSynchronize(st));
-  return h;
-}
-template <class T>
-static void h2d(DevBuf<T>& b, const std::vector<T>& h, cudaStream_t st) {
-  b.resize(h.size());
-  if (!h.empty()) EFMM_CUDA_TRY(cudaMemcpyAsync(b.get(), h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
 }
 
 int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const double* d_src, int nt,
@@ -280,6 +312,15 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
 }
 
 void Plan::build_worklists() {
+  // ELFMM3D_PROFILE_SETUP=1 prints the host time of each phase to stderr
+  static const bool prof = getenv("ELFMM3D_PROFILE_SETUP") != nullptr;
+  auto tp = std::chrono::steady_clock::now();
+  auto mark = [&](const char* what) {
+    if (!prof) return;
+    auto t = std::chrono::steady_clock::now();
+    fprintf(stderr, "build_worklists %-10s %8.2f ms\n", what, std::chrono::duration<double, std::milli>(t - tp).count());
+    tp = t;
+  };
   int nb = tr_.nboxes;
   auto level = d2h(tr_.level, nb, st_);
   auto ijk = d2h(tr_.ijk, 3 * (size_t)nb, st_);
@@ -298,6 +339,7 @@ void Plan::build_worklists() {
   csr(tr_.l3_start, tr_.l3_items, l3s, l3i);
   csr(tr_.l4_start, tr_.l4_items, l4s, l4i);
 
+  mark("d2h");
   // near field: per leaf with evaluation points, source boxes from
   // list1 U self U list3 U list4(ancestors-or-self)  (ITER pairing,
   // src/elfmm3dtria_iter_1.f:1188-1225, read from the target side)
@@ -350,6 +392,7 @@ void Plan::build_worklists() {
   h2d(near_start_, nstart, st_);
   h2d(near_items_, nitems, st_);
 
+  mark("near");
   // far field
   far_ = (p_ > 0) && (tr_.nlev >= 2);
   std::vector<int> p2m, l2t;
@@ -402,6 +445,7 @@ void Plan::build_worklists() {
   m2l_.clear();
   l2l_.clear();
   std::vector<TransPair> m2m_pairs, l2l_pairs, m2l_pairs;
+  mark("far-leaves");
   // M2M bottom-up: children at level lev -> parents at lev-1 (parents >= 2)
   for (int lev = tr_.nlev; lev >= 3; lev--) {
     std::vector<std::pair<int, TransPair>> gp;
@@ -414,24 +458,33 @@ void Plan::build_worklists() {
     }
     add_level(gp, m2m_pairs, m2m_);
   }
-  // M2L: list 2 of every box at level >= 2
+  mark("m2m");
+  // M2L: list 2 of every box at level >= 2, grouped by operator on the
+  // device (count per group, then fill; order within a group is arbitrary)
   {
-    std::vector<std::pair<int, TransPair>> gp;
-    for (int b = 0; b < nb; b++) {
-      if (level[b] < 2 || scount[b] + tcount[b] == 0) continue;
-      double s = tr_.size / (double)(1ull << level[b]);
-      for (int q = l2s[b]; q < l2s[b + 1]; q++) {
-        int sb = l2i[q];
-        if (scount[sb] == 0) continue;
-        int di = ijk[3 * b] - ijk[3 * sb], dj = ijk[3 * b + 1] - ijk[3 * sb + 1],
-            dk = ijk[3 * b + 2] - ijk[3 * sb + 2];
-        int g = m2lg[(di + 3) * 49 + (dj + 3) * 7 + (dk + 3)];
-        gp.push_back({g, TransPair{sb, b, 1.0 / s}});
-      }
-    }
-    m2l_pairs_h_ = gp.size();
-    add_level(gp, m2l_pairs, m2l_);
+    DevBuf<int>& cnt = m2l_cnt_;
+    cnt.resize(344);
+    cnt.zero(st_);
+    const int gb = (nb + 255) / 256;
+    k_m2l_pairs<<<gb, 256, 0, st_>>>(nb, 0, tr_.level.get(), tr_.ijk.get(), tr_.scount.get(), tr_.tcount.get(),
+                                     tr_.l2_start.get(), tr_.l2_items.get(), ops_->m2lg_dev.get(), tr_.size,
+                                     cnt.get(), nullptr, nullptr); count_launch();
+    std::vector<int> hc = d2h(cnt, 343, st_);
+    std::vector<int> start(344, 0);
+    for (int g = 0; g < 343; g++) start[g + 1] = start[g] + hc[g];
+    const int tot = start[343];
+    int s0 = (int)m2l_.segs.size();
+    for (int g = 0; g < 343; g++)
+      if (hc[g] > 0) m2l_.segs.push_back({g, start[g], hc[g]});
+    m2l_.lev.push_back({s0, (int)m2l_.segs.size() - s0});
+    h2d(m2l_cursor_, start, st_);
+    m2l_.pairs.resize(std::max(tot, 1));
+    k_m2l_pairs<<<gb, 256, 0, st_>>>(nb, 1, tr_.level.get(), tr_.ijk.get(), tr_.scount.get(), tr_.tcount.get(),
+                                     tr_.l2_start.get(), tr_.l2_items.get(), ops_->m2lg_dev.get(), tr_.size,
+                                     nullptr, m2l_cursor_.get(), m2l_.pairs.get()); count_launch();
+    m2l_pairs_h_ = tot;
   }
+  mark("m2l");
   // L2L top-down: parents at level lev (>= 2) -> children
   for (int lev = 2; lev < tr_.nlev; lev++) {
     std::vector<std::pair<int, TransPair>> gp;
@@ -446,9 +499,10 @@ void Plan::build_worklists() {
     }
     add_level(gp, l2l_pairs, l2l_);
   }
+  mark("l2l");
   h2d(m2m_.pairs, m2m_pairs, st_);
-  h2d(m2l_.pairs, m2l_pairs, st_);
   h2d(l2l_.pairs, l2l_pairs, st_);
+  mark("upload");
   int D = 2 * ncoef(p_);
   mpole_.resize((size_t)nb * 4 * D);
   local_.resize((size_t)nb * 4 * D);

@@ -27,6 +27,7 @@ struct OpPool {
   DevBuf<double> wnorm;   // w per real row (2 ncoef(p))
   DevBuf<int> kinds;      // operator kind per group (0 M2L, 1 M2M, 2 L2L)
   std::vector<OpDesc> descs;
+  DevBuf<int> m2lg_dev;  // m2l_group on the device
   // factored form (rotation, shift along z, rotation back) of every group,
   // FP64 factorial basis and FP32 normalised basis; made on first use
   bool rot_ready = false;
@@ -164,6 +165,7 @@ class Plan {
   template <class T>
   void run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst);
   size_t m2l_pairs_h_ = 0;
+  DevBuf<int> m2l_cnt_, m2l_cursor_;
   DevBuf<double> mpole_, local_;
   DevBuf<double> ssl_s_, sdl_s_, u_s_, e_s_, ut_s_, et_s_;
   DevBuf<TriRec> trir_;
