@@ -375,7 +375,7 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
 template <class T>
 __global__ void __launch_bounds__(256)
 k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ foff,
-               T* __restrict__ F) {
+               const long long* __restrict__ noff, double* __restrict__ nrec, T* __restrict__ F) {
   extern __shared__ __align__(16) unsigned char pf_smem[];
   const int p = a.p, nc = ncoef(p), D = 2 * nc;
   const int box = a.leaves[wleaves[blockIdx.x]];
@@ -397,6 +397,19 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
   for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
   const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
   const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+  if (lane == 0) {
+    // node record for the weights: position, normal, weight x area, triangle
+    const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+    const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+    const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                          e1[0] * e2[1] - e1[1] * e2[0]};
+    double* o = nrec + 8 * (noff[blockIdx.x] + node);
+    const double* nn = a.nrm + 3 * (size_t)it;
+    o[0] = y[0]; o[1] = y[1]; o[2] = y[2];
+    o[3] = nn[0]; o[4] = nn[1]; o[5] = nn[2];
+    o[6] = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+    o[7] = (double)it;
+  }
   for (int m = lane; m <= p; m += 32) {
     cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
     for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
@@ -440,28 +453,20 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
 template <class T>
 __global__ void __launch_bounds__(256)
 k_p2m_weights(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ woff,
-              T* __restrict__ W) {
+              const long long* __restrict__ noff, const double* __restrict__ nrec, T* __restrict__ W) {
   const int box = a.leaves[wleaves[blockIdx.x]];
-  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int tn = a.scount[box];
   const int nnode = 12 * tn, K = 4 * nnode, C = 4 * R;
-  Quad12 Q;
-  quad12(Q);
   const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu;
+  const double* nd = nrec + 8 * noff[blockIdx.x];
   T* out = W + woff[blockIdx.x];
   for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < (long long)nnode * C;
        q += (long long)gridDim.y * blockDim.x) {
     const int col = (int)(q / nnode), node = (int)(q % nnode);
     const int r = col >> 2, pass = col & 3;
-    const int it = t0 + node / 12, iq = node % 12;
-    const double* Tr = a.tri + 9 * (size_t)it;
-    double y[3];
-    for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
-    const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
-    const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
-    const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
-                          e1[0] * e2[1] - e1[1] * e2[0]};
-    const double w = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-    const double* nn = a.nrm + 3 * (size_t)it;
+    const double* o = nd + 8 * node;
+    const double y[3] = {o[0], o[1], o[2]}, nn[3] = {o[3], o[4], o[5]}, w = o[6];
+    const long long it = (long long)o[7];
     const long long off = r * a.rstride + it * a.tstride, ds = a.dstride;
     double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
     if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
@@ -478,9 +483,9 @@ k_p2m_weights(const P2MArgs a, int R, const int* __restrict__ wleaves, const lon
       wv[0] = w * (sly * c1 * inv2mu + dln * c2);
       for (int d = 0; d < 3; d++) wv[1 + d] = w * 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
     }
-    T* o = out + (size_t)col * K + 4 * node;
+    T* ow = out + (size_t)col * K + 4 * node;
 #pragma unroll
-    for (int k = 0; k < 4; k++) o[k] = (T)wv[k];
+    for (int k = 0; k < 4; k++) ow[k] = (T)wv[k];
   }
 }
 
@@ -1054,6 +1059,159 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
   }
 }
 
+// ------------------------------------------- L2T in two stages (product form)
+// Stage 1 writes, per leaf, the functionals G[row][9 point + v] of the nine
+// derivative sums (the same coefficients as k_l2t_gemm's G tile); stage 2 is
+// the FP64 product S[col][9 point + v] = sum_row G[row][.] L[col][row]
+// (k_gemm_tn); stage 3 applies the Lame recombination per (point, rhs).
+__global__ void __launch_bounds__(256)
+k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long* __restrict__ goff,
+               double* __restrict__ G) {
+  extern __shared__ __align__(16) unsigned char lf_smem[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc;
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
+  const int P = sn + tn;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int e = blockIdx.y * 8 + warp;
+  if (e >= P) return;
+  const bool is_src = e < sn;
+  const int pidx = is_src ? a.sstart[box] + e : a.tstart[box] + (e - sn);
+  const double* X = is_src ? a.src_pts + 3 * (size_t)pidx : a.tgt_pts + 3 * (size_t)pidx;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  cplx* Y = reinterpret_cast<cplx*>(lf_smem) + (size_t)warp * nc;
+  {
+    const double z[3] = {(X[0] - c[0]) * is, (X[1] - c[1]) * is, (X[2] - c[2]) * is};
+    const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+    for (int m = lane; m <= p; m += 32) {
+      cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+      for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+      Y[cidx(m, m)] = dm;
+      cplx ym2 = {0, 0}, ym1 = dm;
+      for (int n = m + 1; n <= p; n++) {
+        const double aa = (2.0 * n - 1.0) * z[2];
+        const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+        cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        Y[cidx(n, m)] = yn;
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+  }
+  __syncwarp();
+  double* out = G + goff[blockIdx.x] + 9 * (size_t)e;
+  const size_t lda = 9 * (size_t)P + ((9 * P) & 1);  // even: 16-byte rows for the product's vector loads
+  for (int row = lane; row < D; row += 32) {
+    const int cc = row >> 1, part = row & 1;
+    int N = 0;
+    while ((N + 1) * (N + 2) / 2 <= cc) N++;
+    const int M = cc - N * (N + 1) / 2;
+    const double sM = (M & 1) ? -1.0 : 1.0;
+#pragma unroll
+    for (int v = 0; v < 9; v++) {
+      const LgTerm t = c_lg_terms[v];
+      const int n = N - t.a;
+      double g = 0.0;
+      if (n >= 0) {
+        double yrd = 0, yid = 0, yrm = 0, yim = 0;
+        const int md = M - t.b, mm = -M - t.b;
+        if (md >= -n && md <= n) {
+          cplx y = hget(Y, n, md);
+          yrd = y.re; yid = y.im;
+        }
+        if (M > 0 && mm >= -n && mm <= n) {
+          cplx y = hget(Y, n, mm);
+          yrm = y.re; yim = y.im;
+        }
+        if (!t.im)
+          g = part == 0 ? yrd + sM * yrm : yid - sM * yim;
+        else
+          g = part == 0 ? -yid - sM * yim : yrd - sM * yrm;
+        g *= t.sg;
+      }
+      out[(size_t)row * lda + v] = g;
+    }
+  }
+}
+
+__global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wleaves,
+                             const long long* __restrict__ soff, const double* __restrict__ S) {
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
+  const int P = sn + tn;
+  const size_t ldc = 9 * (size_t)P + ((9 * P) & 1);
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
+  const double c1 = a.c1;
+  for (int q = threadIdx.x; q < P * R; q += blockDim.x) {
+    const int e = q % P, r = q / P;
+    const bool is_src = e < sn;
+    const int pidx = is_src ? a.sstart[box] + e : a.tstart[box] + (e - sn);
+    const double* X = is_src ? a.src_pts + 3 * (size_t)pidx : a.tgt_pts + 3 * (size_t)pidx;
+    const double x[3] = {X[0], X[1], X[2]};
+    double pot[4], g[4][3], H[4][3][3];
+    for (int pass = 0; pass < 4; pass++) {
+      const double* sv = S + soff[blockIdx.x] + (size_t)(4 * r + pass) * ldc + 9 * (size_t)e;
+      pot[pass] = sv[0];
+      g[pass][0] = sv[3] * is;
+      g[pass][1] = sv[4] * is;
+      g[pass][2] = sv[1] * is;
+      const double hzz = sv[2];
+      const double hxx = 0.5 * (sv[7] - hzz), hyy = 0.5 * (-sv[7] - hzz), hxy = 0.5 * sv[8];
+      const double hxz = sv[5], hyz = sv[6];
+      H[pass][0][0] = hxx * is2; H[pass][1][1] = hyy * is2; H[pass][2][2] = hzz * is2;
+      H[pass][0][1] = H[pass][1][0] = hxy * is2;
+      H[pass][0][2] = H[pass][2][0] = hxz * is2;
+      H[pass][1][2] = H[pass][2][1] = hyz * is2;
+    }
+    const size_t np = is_src ? a.nsrc : a.ntgt;
+    double u[3];
+    for (int i = 0; i < 3; i++) {
+      u[i] = (2.0 - c1) * pot[i] + g[3][i];
+      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+    }
+    double* U = (is_src ? a.u_src : a.u_tgt) + 3 * (np * r + pidx);
+    U[0] += u[0];
+    U[1] += u[1];
+    U[2] += u[2];
+    const bool dostrain = is_src ? a.dostrain_src : a.dostrain_tgt;
+    if (dostrain) {
+      double Gm[3][3];
+      for (int aa = 0; aa < 3; aa++)
+        for (int bb = 0; bb < 3; bb++) {
+          double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
+          for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+          Gm[aa][bb] = v;
+        }
+      double* E = (is_src ? a.e_src : a.e_tgt) + 6 * (np * r + pidx);
+      E[0] += Gm[0][0];
+      E[1] += Gm[1][1];
+      E[2] += Gm[2][2];
+      E[3] += 0.5 * (Gm[0][1] + Gm[1][0]);
+      E[4] += 0.5 * (Gm[0][2] + Gm[2][0]);
+      E[5] += 0.5 * (Gm[1][2] + Gm[2][1]);
+    }
+  }
+}
+
+void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
+                         const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
+                         int ntask, const GemmTask* tasks, const double* local) {
+  if (nwleaf <= 0) return;
+  const int nc = ncoef(a.p);
+  const int smem = (int)(sizeof(cplx) * 8 * nc);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_features, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_l2t_features<<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
+  const int gsm = (int)(sizeof(double) * 4 * 16 * 128);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+  k_gemm_tn<double><<<ntask, 256, gsm, st>>>(tasks, Gbuf, local, Sbuf); count_launch();
+  k_l2t_finish<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp) {
   if (nop <= 0) return;
@@ -1075,23 +1233,26 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs) {
 
 template <class T>
 void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
-                         const long long* foff, const long long* woff, int max_nodes, T* F, T* W, int ntask,
-                         const GemmTask* tasks, T* mpole) {
+                         const long long* foff, const long long* woff, const long long* noff, double* nrec,
+                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
   EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_p2m_features<T><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, F); count_launch();
-  k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, W); count_launch();
+  k_p2m_features<T><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
+  count_launch();
+  k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
   const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
   EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
   k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template void launch_p2m_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
-                                          const long long*, int, double*, double*, int, const GemmTask*, double*);
+                                          const long long*, const long long*, double*, int, double*, double*, int,
+                                          const GemmTask*, double*);
 template void launch_p2m_twostage<float>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
-                                         const long long*, int, float*, float*, int, const GemmTask*, float*);
+                                         const long long*, const long long*, double*, int, float*, float*, int,
+                                         const GemmTask*, float*);
 
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,

@@ -73,15 +73,23 @@ bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpo
 // rescaled by wnorm).  Returns false when the order is too high.
 // Two-stage P2M of R right-hand sides for one wave of leaves: node features
 // F (per leaf at foff: 4 x 12 x triangles rows of D), node weights W (per
-// leaf at woff: 4R columns of 4 x 12 x triangles), then the batched product
+// leaf at woff: 4R columns of 4 x 12 x triangles; node records of 8 doubles
+// per node at noff), then the batched product
 // into mpole (tasks cut by the caller).
 template <class T>
 void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
-                         const long long* foff, const long long* woff, int max_nodes, T* F, T* W, int ntask,
-                         const GemmTask* tasks, T* mpole);
+                         const long long* foff, const long long* woff, const long long* noff, double* nrec,
+                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole);
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
                      int R, const TB* local, const double* wnorm);
+// Two-stage L2T of R right-hand sides for one wave of leaves: functionals G
+// (per leaf at goff: D rows of 9 x points), the FP64 product into S (per leaf
+// at soff: 4R columns of 9 x points; tasks cut by the caller, B = local),
+// then the Lame recombination into the outputs.
+void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
+                         const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
+                         int ntask, const GemmTask* tasks, const double* local);
 template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                       const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,

@@ -409,6 +409,7 @@ void Plan::build_worklists() {
   for (int b : p2m) p2m_sc_h_.push_back(scount[b]);
   l2t_sc_h_.clear();
   l2t_tc_h_.clear();
+  l2t_h_ = l2t;
   for (int b : l2t) {
     l2t_sc_h_.push_back(scount[b]);
     l2t_tc_h_.push_back(tcount[b]);
@@ -825,7 +826,8 @@ void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
   const size_t nl = p2m_h_.size();
   while (i < nl) {
     std::vector<int> wl;
-    std::vector<long long> fo, wo;
+    std::vector<long long> fo, wo, no;
+    long long nodes = 0;
     std::vector<GemmTask> tasks;
     long long used = 0;
     int max_nodes = 0;
@@ -836,6 +838,8 @@ void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
       wl.push_back((int)i);
       fo.push_back(used);
       wo.push_back(used + K * D);
+      no.push_back(nodes);
+      nodes += 12LL * p2m_sc_h_[i];
       const int box = p2m_h_[i];
       for (int c0 = 0; c0 < C; c0 += 128)
         for (int r0 = 0; r0 < D; r0 += 128)
@@ -849,13 +853,62 @@ void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
     h2d(wave_foff_, fo, st_);
     h2d(wave_woff_, wo, st_);
     h2d(wave_tasks_, tasks, st_);
+    h2d(wave_noff_, no, st_);
+    wave_nrec_.resize(8 * (size_t)std::max(nodes, 1LL));
     T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
     launch_p2m_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
-                           max_nodes, scratch, scratch, (int)tasks.size(), wave_tasks_.get(), mpole);
+                           wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
+                           wave_tasks_.get(), mpole);
   }
 }
 template void Plan::p2m_twostage<double>(const P2MArgs&, int, double*);
 template void Plan::p2m_twostage<float>(const P2MArgs&, int, float*);
+
+// Two-stage L2T over waves of leaves whose functionals and sums fit a
+// scratch budget (at most 8 GB or a quarter of the free memory).
+void Plan::l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt) {
+  const int D = 2 * ncoef(p_), C = 4 * R;
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / 8;
+  size_t i = 0;
+  const size_t nl = l2t_h_.size();
+  while (i < nl) {
+    std::vector<int> wl;
+    std::vector<long long> go, so;
+    std::vector<GemmTask> tasks;
+    long long used = 0;
+    int max_pts = 0;
+    while (i < nl) {
+      const int P = (do_src ? l2t_sc_h_[i] : 0) + (do_tgt ? l2t_tc_h_[i] : 0);
+      if (P == 0) {
+        i++;
+        continue;
+      }
+      const int LD = 9 * P + ((9 * P) & 1);  // even leading dimension (16-byte vector loads)
+      const long long need = (long long)D * LD + (long long)C * LD;
+      if (!wl.empty() && used + need > (long long)budget) break;
+      wl.push_back((int)i);
+      go.push_back(used);
+      so.push_back(used + (long long)D * LD);
+      const int box = l2t_h_[i];
+      for (int c0 = 0; c0 < C; c0 += 128)
+        for (int r0 = 0; r0 < 9 * P; r0 += 128)
+          tasks.push_back({used, (long long)box * C * D, used + (long long)D * LD, 9 * P, C, D, LD, D, LD, r0, c0});
+      used += need;
+      max_pts = std::max(max_pts, P);
+      i++;
+    }
+    if (wl.empty()) break;
+    l2t_scratch_.resize((size_t)used);
+    h2d(wave_leaves_, wl, st_);
+    h2d(wave_foff_, go, st_);
+    h2d(wave_woff_, so, st_);
+    h2d(wave_tasks_, tasks, st_);
+    launch_l2t_twostage(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(), max_pts,
+                        l2t_scratch_.get(), l2t_scratch_.get(), (int)tasks.size(), wave_tasks_.get(), local_.get());
+  }
+}
 
 int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed) {
@@ -952,9 +1005,18 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     la.c1 = c1;
     la.u_src = u_s_.get(); la.e_src = e_s_.get(); la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
     la.C = C; la.nsrc = n; la.ntgt = nt;
-    // product form (chunks of 8 points of a leaf) once the columns fill its tiles
+    // two-stage product form once the columns fill its tiles
     bool done = false;
     if (C >= 32) {
+      if (mixed) {
+        local_.resize(nb * C * D);
+        k_f2d_local<<<1184, 256, 0, st_>>>(local_f_.size(), D, ops_->wnorm.get(), local_f_.get(), local_.get());
+        count_launch();
+      }
+      l2t_twostage(la, R, do_src, do_tgt);
+      done = true;
+    }
+    if (!done && C >= 32) {
       const int key = do_src | (do_tgt << 1);
       if (lchunk_key_ != key) {
         std::vector<int> cl, ce;

@@ -128,10 +128,14 @@ class Plan {
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA
   int nchunk_ = 0, chunk_key_ = -1;
   std::vector<int> l2t_sc_h_, l2t_tc_h_;  // per L2T leaf
+  std::vector<int> l2t_h_;                // L2T leaves
+  DevBuf<double> l2t_scratch_;            // functionals + sums of one wave of leaves
+  void l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt);
   std::vector<int> p2m_h_, p2m_sc_h_;     // P2M leaves and their triangle counts
   DevBuf<double> p2m_scratch_;            // node features + weights of one wave of leaves
   DevBuf<int> wave_leaves_;
-  DevBuf<long long> wave_foff_, wave_woff_;
+  DevBuf<long long> wave_foff_, wave_woff_, wave_noff_;
+  DevBuf<double> wave_nrec_;
   DevBuf<GemmTask> wave_tasks_;
   template <class T>
   void p2m_twostage(const P2MArgs& pa, int R, T* mpole);
