@@ -771,10 +771,19 @@ void Plan::flops_per_column(double* f) const {
   const long long nodes = 12LL * n_;
   f[0] = 2.0 * D * 4.0 * (double)nodes;  // rows x (charge + 3 dipole) per node
   const TransSched* S[3] = {&m2m_, &m2l_, &l2l_};
+  // flops of the form that runs: factored (two rotations and the shift along
+  // z, each sum_{j=1}^{p+1} (2j)^2 multiply-adds) or dense (dim^2)
+  const bool fact = factored_ && 2.0 * D * rot_cols_per_cta((int)D, 4) * 4 <= 227.0 * 1024;
   for (int k = 0; k < 3; k++)
     for (const TransSeg& g : S[k]->segs) {
-      double dim = ops_->dims[g.group];
-      f[1 + k] += 2.0 * dim * dim * g.npair;
+      if (fact) {
+        const double q = ops_->descs[g.group].p + 1;
+        const double rs = 4.0 * q * (q + 1) * (2 * q + 1) / 6.0;
+        f[1 + k] += 2.0 * 3.0 * rs * g.npair;
+      } else {
+        double dim = ops_->dims[g.group];
+        f[1 + k] += 2.0 * dim * dim * g.npair;
+      }
     }
   f[4] = 2.0 * D * 9.0 * (double)(n_ + nt_);  // 9 derivative sums per point
 }
