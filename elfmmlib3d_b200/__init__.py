@@ -48,7 +48,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
-           "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck"]
+           "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
+           "efmm_plan_evaluate_iter", "efmm_plan_stored_bytes"]
 
 
 class ElfmmError(RuntimeError):
@@ -83,6 +84,11 @@ def load():
     L.efmm_plan_evaluate_batch.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp,
                                            _vp, _vp, _vp, ctypes.c_int]
     L.efmm_plan_flops.argtypes = [_vp, _dp]
+    L.efmm_plan_stored_bytes.restype = ctypes.c_longlong
+    L.efmm_plan_stored_bytes.argtypes = [_vp]
+    L.efmm_plan_evaluate_iter.restype = ctypes.c_int
+    L.efmm_plan_evaluate_iter.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, _vp, _vp,
+                                          ctypes.c_int]
     L.efmm_plan_evaluate_direct_subset.restype = ctypes.c_int
     L.efmm_plan_evaluate_direct_subset.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp,
                                                    _vp, _vp, _vp]
@@ -320,7 +326,15 @@ class Plan:
             raise ElfmmError(ier, "set_geometry")
         self.n, self.nt = n, nt
 
-    def evaluate(self, rlam, rmu, ssl=None, sdl=None, u=None, e=None, ut=None, et=None, direct=False):
+    def evaluate(self, rlam, rmu, ssl=None, sdl=None, u=None, e=None, ut=None, et=None, direct=False, mode=0):
+        """mode 1: store the near-field interactions (ITER first call; geometry
+        set with iter=True), mode 2: reuse them."""
+        if mode:
+            ier = self._L.efmm_plan_evaluate_iter(self._h, float(rlam), float(rmu), self._ptr(ssl), self._ptr(sdl),
+                                                  self._ptr(u), self._ptr(e), self._ptr(ut), self._ptr(et), int(mode))
+            if ier:
+                raise ElfmmError(ier, "evaluate (iter)")
+            return
         f = self._L.efmm_plan_evaluate_direct if direct else self._L.efmm_plan_evaluate
         ier = f(self._h, float(rlam), float(rmu), self._ptr(ssl), self._ptr(sdl), self._ptr(u),
                 self._ptr(e), self._ptr(ut), self._ptr(et))
@@ -358,6 +372,10 @@ class Plan:
                                                        self._ptr(ssl), self._ptr(sdl), self._ptr(u), self._ptr(e))
         if ier:
             raise ElfmmError(ier, "evaluate_direct_subset")
+
+    def stored_bytes(self):
+        """Device bytes of the stored near field (ITER), 0 if none."""
+        return int(self._L.efmm_plan_stored_bytes(self._h))
 
     def flops_per_column(self):
         """Useful flops per expansion column: P2M, M2M, M2L, L2L, L2T."""

@@ -149,6 +149,18 @@ int efmm_plan_evaluate_batch(efmm_plan *plan, double rlam, double rmu, int nrhs,
  * side) of the current geometry: P2M, M2M, M2L, L2L, L2T. */
 void efmm_plan_flops(const efmm_plan *plan, double *f5);
 
+/* Device-resident ITER evaluation (the plan's geometry must have been set
+ * with iter != 0): mode 1 computes and stores the near-field interactions
+ * and evaluates, mode 2 evaluates with the stored interactions (same layers,
+ * outputs and Lame constants as the store, else 512).  Arguments as in
+ * efmm_plan_evaluate. */
+int efmm_plan_evaluate_iter(efmm_plan *plan, double rlam, double rmu, const double *ssl,
+                            const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                            double *e_tgt, int mode);
+
+/* Device bytes of the plan's stored near field (0 if none). */
+long long efmm_plan_stored_bytes(const efmm_plan *plan);
+
 /* Direct sum at the first nsub source points only (centroids 0..nsub-1,
  * self-aware), outputs u_src (nsub,3), e_src (nsub,3,3): the FP64 check of a
  * large evaluation on a subset. */
