@@ -101,6 +101,24 @@ def make_inputs(name, seed=1):
     return tri, nrm, cen, tgt, ssl, sdl, w["iprec"]
 
 
+def max_over_ranks(x, world, device=None):
+    """Largest x over the ranks of the process group (every rank calls it;
+    a single process returns x).  Device times are reported as this max."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(units_per_rank, t_max_ms, world):
+    """Whole-job throughput of independent replicas: all ranks' units over
+    the slowest rank's time."""
+    return world * units_per_rank / (t_max_ms * 1e-3)
+
+
 class ClockSampler:
     """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
 
@@ -237,14 +255,11 @@ def run_ours(args, rank, world, local_rank):
     info = P.info()
     tim = P.timings()
     setup = P.setup_timings()
-    t_max = ms
+    t_max = max_over_ranks(ms, world, dev)
     if world > 1:
         import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
         dist.barrier()
-    value = world * evals * args.steps / (t_max * 1e-3)
+    value = replica_value(evals * args.steps, t_max, world)
 
     # end to end through the Fortran ABI, pinned host buffers
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
@@ -255,12 +270,7 @@ def run_ours(args, rank, world, local_rank):
         ier, *_ = E.elfmm3dtriatarg(iprec, 1.0, 1.0, htri, hnrm, hcen, hssl, hsdl, htgt)
         assert ier == 0, ier
     e2e_s = time.perf_counter() - t0
-    e2e_t = e2e_s
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t = max_over_ranks(e2e_s, world, dev)
     e2e_value = world * evals * args.steps / e2e_t
     h2d = 8 * (9 * n + 3 * n + 3 * n + 3 * m + 6 * n)
     d2h = 8 * (3 * n + 9 * n + 3 * m + 9 * m)
@@ -341,14 +351,11 @@ def run_batch(args, rank, world, local_rank):
         torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = E.kernel_launches() - l0
-    t_max = ms
+    t_max = max_over_ranks(ms, world, dev)
     if world > 1:
         import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
         dist.barrier()
-    value = world * evals * args.steps / (t_max * 1e-3)
+    value = replica_value(evals * args.steps, t_max, world)
     info = P.info()
     fl = P.flops_per_column()
     setup = P.setup_timings()
@@ -367,12 +374,7 @@ def run_batch(args, rank, world, local_rank):
         ier, *_ = E.batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, out=hout)
         assert ier == 0, ier
     e2e_s = time.perf_counter() - t0
-    e2e_t = e2e_s
-    if world > 1:
-        import torch.distributed as dist
-        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_t = float(tt.item())
+    e2e_t = max_over_ranks(e2e_s, world, dev)
     e2e_value = world * evals * args.steps / e2e_t
     h2d = 8 * (9 * n + 3 * n + 3 * n + 3 * n * R)
     d2h = 8 * (3 * n * R + 9 * n * R)
@@ -503,14 +505,11 @@ def run_iter(args, rank, world, local_rank):
         torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = E.kernel_launches() - l0
-    t_max = ms
+    t_max = max_over_ranks(ms, world, dev)
     if world > 1:
         import torch.distributed as dist
-        tt = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
         dist.barrier()
-    value = world * evals / (t_max * 1e-3)
+    value = replica_value(evals, t_max, world)
     info = P.info()
     stored = P.stored_bytes()
     u_last = u.clone()
