@@ -26,6 +26,7 @@ import os
 import numpy as np
 
 __all__ = ["elfmm3dtria", "elfmm3dtriatarg", "el3dtriadirecttarg", "elfmm3dtriatargiter", "batch_host",
+           "elhfmm3dtriatargiter", "halfspace_self",
            "elfmm3dtriaiter", "iter_release", "iter_stored_bytes", "Plan", "load",
            "library_path", "device_count", "ElfmmError"]
 
@@ -49,7 +50,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_stored_bytes"]
+           "efmm_plan_evaluate_iter", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
 
 
 class ElfmmError(RuntimeError):
@@ -235,6 +236,43 @@ def batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma
     ier = L.efmm_batch_host(int(iprec), float(rlam), float(rmu), n, p(tri), p(nrm), p(src), m, p(tg), R, p(ssl),
                             p(sdl), p(pt), p(st), p(ptt) if m else None, p(stt) if m else None, int(precision))
     return ier, pt, st, ptt[:, :m], stt[:, :m]
+
+
+def elhfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, target=None,
+                         icomp_type=1, wsave=None, ifptfrctarg=1, ifstraintarg=1):
+    """Image part of the half-space (z <= 0) layer potentials at targets
+    (src/elhfmm3dtria_iter.f:46).  Returns (ier, lused, ptfrctarg (m,3),
+    straintarg (m,3,3))."""
+    L = load()
+    _need_gpu()
+    tri, nrm, src, ssl, sdl, n = _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    ws = wsave if wsave is not None else np.zeros(8)
+    ptt = np.zeros((max(m, 1), 3))
+    stt = np.zeros((max(m, 1), 3, 3))
+    ier = ctypes.c_int(0)
+    lused = ctypes.c_int(0)
+    L.elhfmm3dtriatargiter_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu),
+                            tri.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp), _byref_i(n), src.ctypes.data_as(_dp),
+                            _byref_i(sigma_sl is not None), ssl.ctypes.data_as(_dp), _byref_i(sigma_dl is not None),
+                            sdl.ctypes.data_as(_dp), _byref_i(m), tg.ctypes.data_as(_dp), _byref_i(ifptfrctarg),
+                            ptt.ctypes.data_as(_dp), _byref_i(ifstraintarg), stt.ctypes.data_as(_dp),
+                            _byref_i(icomp_type), ws.ctypes.data_as(_dp), _byref_i(ws.size), ctypes.byref(lused))
+    return ier.value, lused.value, ptt[:m], stt[:m]
+
+
+def halfspace_self(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None):
+    """Half-space self-evaluation at the centroids: the free-space (direct
+    arrival, on-surface) evaluation plus the image part with the centroids as
+    targets, the sum the reference's drivers form
+    (examples/elhfmm3dtria_self_iter_dr.f:331-385).  Returns (ier, ptfrc, strain)."""
+    ier, pt, st = elfmm3dtria(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl, sigma_dl)
+    if ier:
+        return ier, pt, st
+    ier, _, pti, sti = elhfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl, sigma_dl,
+                                            target=source)
+    return ier, pt + pti, st + sti
 
 
 ITER_LUSED = 8  # words of wsave the ITER handle occupies

@@ -5,6 +5,7 @@
 #include <mutex>
 #include <vector>
 #include "plan.h"
+#include "halfspace.h"
 #include "../../include/elfmm3d_b200.h"
 
 using namespace efmm;
@@ -376,6 +377,84 @@ extern "C" int efmm_batch_host(int iprec, double rlam, double rmu, int n, const 
   } catch (const std::bad_alloc&) {
     return IER_ALLOC;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Half-space image part (src/elhfmm3dtria_iter.f:46-51): direct GPU sum.
+// ---------------------------------------------------------------------------
+namespace {
+struct HsBufs {
+  DevBuf<double> tri, nrm, ssl, sdl, tgt, u, e6;
+  DevBuf<HsTri> work;
+};
+HsBufs* g_hs = nullptr;
+
+int hs_call(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n, int ifsingle,
+            const double* ssl, int ifdouble, const double* sdl, int nt, const double* tgt, int ifptfrctarg,
+            double* ptfrctarg, int ifstraintarg, double* straintarg, int icomp, int* lused) {
+  if (lused) *lused = 8;
+  if (n < 1 || nt < 0) return IER_BADARG;
+  if (iprec < -2 || iprec > 6) return IER_BADARG;
+  if (icomp == 0 || icomp == 4 || nt == 0 || !(ifptfrctarg || ifstraintarg)) return IER_OK;
+  if (icomp < 0 || icomp > 5) return IER_BADARG;
+  // the half-space is z <= 0: sources and targets must lie in it
+  for (int i = 0; i < 3 * n; i++)
+    if (tri[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < nt; i++)
+    if (tgt[3 * i + 2] > 0.0) return IER_BADARG;
+  std::lock_guard<std::mutex> lk(g_mu);
+  efmm_plan* p = shared_plan();
+  if (!p) return IER_NODEVICE;
+  try {
+    cudaSetDevice(p->device);
+    if (!g_hs) g_hs = new HsBufs();
+    HsBufs& B = *g_hs;
+    cudaStream_t st = p->stream;
+    up(B.tri, tri, 9 * (size_t)n, st);
+    up(B.nrm, nrm, 3 * (size_t)n, st);
+    if (ifsingle) up(B.ssl, ssl, 3 * (size_t)n, st);
+    if (ifdouble) up(B.sdl, sdl, 3 * (size_t)n, st);
+    up(B.tgt, tgt, 3 * (size_t)nt, st);
+    B.work.resize(n);
+    B.u.resize(3 * (size_t)nt);
+    B.e6.resize(6 * (size_t)nt);
+    launch_hs_image(st, n, B.tri.get(), B.nrm.get(), ifsingle ? B.ssl.get() : nullptr,
+                    ifdouble ? B.sdl.get() : nullptr, nt, B.tgt.get(), rlam, rmu, B.work.get(), B.u.get(),
+                    B.e6.get());
+    std::vector<double> e6(6 * (size_t)nt);
+    if (ifptfrctarg) down(ptfrctarg, B.u, 3 * (size_t)nt, st);
+    if (ifstraintarg) down(e6.data(), B.e6, 6 * (size_t)nt, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (ifstraintarg)
+      for (int i = 0; i < nt; i++) {
+        const double* s = &e6[6 * (size_t)i];
+        double* o = straintarg + 9 * (size_t)i;
+        o[0] = s[0]; o[4] = s[1]; o[8] = s[2];
+        o[1] = o[3] = s[3];
+        o[2] = o[6] = s[4];
+        o[5] = o[7] = s[5];
+      }
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+}  // namespace
+
+extern "C" void elhfmm3dtriatargiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
+                                      const double* triangle, const double* trinorm, const int* nparts,
+                                      const double* source, const int* ifsingle, const double* sigma_sl,
+                                      const int* ifdouble, const double* sigma_dl, const int* ntargs,
+                                      const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                      const int* ifstraintarg, double* straintarg, const int* icomp_type,
+                                      double* wsave, const int* lwsave, int* lused) {
+  (void)source;
+  (void)wsave;
+  (void)lwsave;
+  *ier = hs_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, *ifsingle, sigma_sl, *ifdouble, sigma_dl,
+                 *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, *icomp_type, lused);
 }
 
 // ---------------------------------------------------------------------------

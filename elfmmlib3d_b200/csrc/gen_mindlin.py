@@ -94,28 +94,21 @@ _pr = _Printer()
 
 def main():
     G = [image_force(k) for k in range(3)]  # G[k][i]
-    sl = []
-    for k in range(3):
-        sl += disp_strain(G[k])
-    dl = []
-    for p in range(3):
-        K = []
-        for i in range(3):
-            acc = 0
-            for q in range(3):
-                for k in range(3):
-                    for l in range(3):
-                        c = cijkl(p, q, k, l)
-                        if c != 0:
-                            acc += c * NN[q] * sp.diff(G[k][i], S[l])
-            K.append(acc)
-        dl += disp_strain(K)
+    f = sp.symbols('f1 f2 f3', real=True)
+    b = sp.symbols('b1 b2 b3', real=True)
+    sl = disp_strain([sum(f[k] * G[k][i] for k in range(3)) for i in range(3)])
+    dl = disp_strain([sum(cijkl(p, q, k, l) * b[p] * NN[q] * sp.diff(G[k][i], S[l])
+                          for p in range(3) for q in range(3) for k in range(3) for l in range(3)
+                          if cijkl(p, q, k, l) != 0) for i in range(3)])
     out = ['// mindlin_gen.cuh -- generated by gen_mindlin.py; do not edit.',
-           '// Image part of the half-space point-force (SL) and point-jump (DL)',
-           '// Green\'s functions: 27 doubles each, per source direction (force f = e_k',
-           '// or jump b = e_p): displacement (3) then strain (xx yy zz xy xz yz).',
+           '// Image part of the half-space Green\'s functions of a point force f',
+           '// (single layer) and of a point displacement jump b with normal n',
+           '// (double layer) at source s, seen at target (x, y, z): 9 doubles,',
+           '// displacement (3) then strain (xx yy zz xy xz yz).',
            '#pragma once', '#include "tri_index.cuh"', '', 'namespace efmm {', '']
-    for name, exprs, extra in (('mindlin_image_sl', sl, ''), ('mindlin_image_dl', dl, ', double n1, double n2, double n3')):
+    for name, exprs, extra in (('mindlin_image_sl', sl, ', double f1, double f2, double f3'),
+                               ('mindlin_image_dl', dl, ', double b1, double b2, double b3, double n1, double n2, '
+                                                        'double n3')):
         rep, red = sp.cse(exprs, symbols=sp.numbered_symbols('t'), optimizations='basic')
         out.append(f'EFMM_HD void {name}(double lam, double mu, double x, double y, double z, double s1, '
                    f'double s2, double s3{extra}, double* o) {{')

@@ -1,0 +1,151 @@
+// halfspace.cu -- image part of the Mindlin half-space layer potentials.
+//
+// elhfmm3dtriatargiter (src/elhfmm3dtria_iter.f:46) returns, at targets in
+// z < 0, the image part of the half-space single / double layer potentials
+// of piecewise-constant densities on flat triangles (the direct arrival is
+// the free-space evaluation, a separate call).  Here the image part is
+// summed directly over all (target, triangle) pairs on the GPU: the
+// integrand (mindlin_gen.cuh, generated by gen_mindlin.py) is smooth on the
+// triangle except near the reflected target, so each pair is integrated with
+// the 12-node degree-6 rule on sub-triangles refined by distance to the
+// reflected target (the reference refines adaptively too,
+// src/tria3adamar.f:16-548, with a depth cap).
+//
+// Not built: the image far field as expansions (the anti-image elastic FMM
+// and the Mindlin B/C plane-wave FMM of src/lfmm3dtriamindlin_iter_1.f); the
+// direct sum costs O(N M) pair integrals.
+#include "common.cuh"
+#include "mindlin_gen.cuh"
+#include "halfspace.h"
+
+namespace efmm {
+
+// sub-triangle accepted for the 12-node rule when the reflected target is
+// farther than HS_RATIO x its diameter (rule error ~ (1 / (2 HS_RATIO))^7)
+constexpr double HS_RATIO = 8.0;
+constexpr int HS_MAXDEPTH = 8;
+constexpr int HS_STACK = 3 * HS_MAXDEPTH + 1;
+constexpr int HS_TILE = 64;
+
+struct HsSub {
+  double v[9];
+  int depth;
+};
+
+__global__ void k_hs_prep(int n, const double* __restrict__ tri, const double* __restrict__ nrm,
+                          const double* __restrict__ ssl, const double* __restrict__ sdl, HsTri* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  HsTri t;
+  for (int c = 0; c < 9; c++) t.v[c] = tri[9 * (size_t)i + c];
+  for (int c = 0; c < 3; c++) {
+    t.n[c] = nrm[3 * (size_t)i + c];
+    t.sl[c] = ssl ? ssl[3 * (size_t)i + c] : 0.0;
+    t.dl[c] = sdl ? sdl[3 * (size_t)i + c] : 0.0;
+  }
+  out[i] = t;
+}
+
+__device__ void hs_pair(const HsTri& T, const double X[3], int dosl, int dodl, double lam, double mu,
+                        const Quad12& Q, double acc[9]) {
+  const double Xr[3] = {X[0], X[1], -X[2]};
+  HsSub stk[HS_STACK];
+  int top = 0;
+  for (int c = 0; c < 9; c++) stk[0].v[c] = T.v[c];
+  stk[0].depth = 0;
+  top = 1;
+  while (top > 0) {
+    const HsSub s = stk[--top];
+    const double* a = s.v;
+    const double* b = s.v + 3;
+    const double* c = s.v + 6;
+    double cen[3], diam = 0.0;
+    for (int d = 0; d < 3; d++) cen[d] = (a[d] + b[d] + c[d]) / 3.0;
+    {
+      double e0 = 0, e1 = 0, e2 = 0;
+      for (int d = 0; d < 3; d++) {
+        e0 += (b[d] - a[d]) * (b[d] - a[d]);
+        e1 += (c[d] - b[d]) * (c[d] - b[d]);
+        e2 += (a[d] - c[d]) * (a[d] - c[d]);
+      }
+      diam = sqrt(fmax(e0, fmax(e1, e2)));
+    }
+    double dist2 = 0;
+    for (int d = 0; d < 3; d++) dist2 += (Xr[d] - cen[d]) * (Xr[d] - cen[d]);
+    if (dist2 > HS_RATIO * HS_RATIO * diam * diam || s.depth >= HS_MAXDEPTH || top + 4 > HS_STACK) {
+      const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+      const double v[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+      const double cr[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+      const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      for (int q = 0; q < 12; q++) {
+        double y[3];
+        for (int d = 0; d < 3; d++) y[d] = Q.b[q][0] * a[d] + Q.b[q][1] * b[d] + Q.b[q][2] * c[d];
+        const double w = Q.w[q] * area;
+        double o[9];
+        if (dosl) {
+          mindlin_image_sl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], T.sl[0], T.sl[1], T.sl[2], o);
+          for (int k = 0; k < 9; k++) acc[k] += w * o[k];
+        }
+        if (dodl) {
+          mindlin_image_dl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], T.dl[0], T.dl[1], T.dl[2], T.n[0],
+                           T.n[1], T.n[2], o);
+          for (int k = 0; k < 9; k++) acc[k] += w * o[k];
+        }
+      }
+    } else {
+      double ab[3], bc[3], ca[3];
+      for (int d = 0; d < 3; d++) {
+        ab[d] = 0.5 * (a[d] + b[d]);
+        bc[d] = 0.5 * (b[d] + c[d]);
+        ca[d] = 0.5 * (c[d] + a[d]);
+      }
+      const double* kids[4][3] = {{a, ab, ca}, {ab, b, bc}, {ca, bc, c}, {ab, bc, ca}};
+      for (int k = 0; k < 4; k++) {
+        HsSub t;
+        for (int vtx = 0; vtx < 3; vtx++)
+          for (int d = 0; d < 3; d++) t.v[3 * vtx + d] = kids[k][vtx][d];
+        t.depth = s.depth + 1;
+        stk[top++] = t;
+      }
+    }
+  }
+}
+
+// One thread per target, triangles streamed through shared memory.
+__global__ void __launch_bounds__(128, 1)  // one CTA: let the generated kernel keep 255 registers
+k_hs_image(int n, const HsTri* __restrict__ tris, int m, const double* __restrict__ tgt, int dosl, int dodl,
+           double lam, double mu, double* __restrict__ u, double* __restrict__ e6) {
+  __shared__ HsTri tile[HS_TILE];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool ok = i < m;
+  double X[3] = {0, 0, 0};
+  if (ok)
+    for (int d = 0; d < 3; d++) X[d] = tgt[3 * (size_t)i + d];
+  Quad12 Q;
+  quad12(Q);
+  double acc[9];
+  for (int k = 0; k < 9; k++) acc[k] = 0.0;
+  for (int t0 = 0; t0 < n; t0 += HS_TILE) {
+    const int cnt = min(HS_TILE, n - t0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) tile[q] = tris[t0 + q];
+    __syncthreads();
+    if (ok)
+      for (int t = 0; t < cnt; t++) hs_pair(tile[t], X, dosl, dodl, lam, mu, Q, acc);
+  }
+  if (!ok) return;
+  for (int d = 0; d < 3; d++) u[3 * (size_t)i + d] = acc[d];
+  for (int d = 0; d < 6; d++) e6[6 * (size_t)i + d] = acc[3 + d];
+}
+
+void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nrm, const double* ssl,
+                     const double* sdl, int m, const double* tgt, double lam, double mu, HsTri* work, double* u,
+                     double* e6) {
+  if (n <= 0 || m <= 0) return;
+  k_hs_prep<<<(n + 127) / 128, 128, 0, st>>>(n, tri, nrm, ssl, sdl, work); count_launch();
+  k_hs_image<<<(m + 127) / 128, 128, 0, st>>>(n, work, m, tgt, ssl != nullptr, sdl != nullptr, lam, mu, u, e6);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace efmm

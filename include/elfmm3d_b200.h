@@ -99,6 +99,23 @@ int efmm_batch_host(int iprec, double rlam, double rmu, int n, const double *tri
                     int nrhs, const double *sigma_sl, const double *sigma_dl, double *ptfrc,
                     double *strain, double *ptfrctarg, double *straintarg, int precision);
 
+/* Replaces elhfmm3dtriatargiter (src/elhfmm3dtria_iter.f:46-51): the image
+ * part of the half-space (z <= 0, traction-free surface z = 0) single and
+ * double layer potentials at targets, Mindlin's solution (the direct
+ * arrival is the free-space evaluation, elfmm3dtriatarg_ / elfmm3dtria_).
+ * Here a direct GPU sum over all (target, triangle) pairs with quadrature
+ * refined towards the reflected target; iprec is checked but the result is
+ * accurate to the quadrature (~1e-9) at every iprec.  icomp_type 0 and 4 do
+ * nothing but set lused = 8 (nothing is stored); 1, 2, 3 and 5 evaluate.
+ * Sources or targets above z = 0 give ier 16. */
+void elhfmm3dtriatargiter_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                           const double *triangle, const double *trinorm, const int *nparts,
+                           const double *source, const int *ifsingle, const double *sigma_sl,
+                           const int *ifdouble, const double *sigma_dl, const int *ntargs,
+                           const double *target, const int *ifptfrctarg, double *ptfrctarg,
+                           const int *ifstraintarg, double *straintarg, const int *icomp_type,
+                           double *wsave, const int *lwsave, int *lused);
+
 /* Frees the device store named by an ITER handle (no counterpart in the
  * reference, whose store is the caller's wsave array).  512 if the handle
  * names no live store. */

@@ -1,0 +1,72 @@
+"""Half-space image part (elhfmm3dtriatargiter_, direct GPU sum): against the
+oracle's restatement of the reference's image kernels, and end to end
+against the traction-free condition on z = 0 with the free-space direct sum
+as the direct arrival."""
+import numpy as np
+import pytest
+
+from conftest import rel
+from elfmmlib3d_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _fault(nl=4, nw=3):
+    tri, nrm, cen, us = G.planar_fault(nl, nw, length=4.0, width=3.0, dip_deg=45.0, top_depth=1.0)
+    return tri, nrm, cen
+
+
+def test_image_matches_oracle(gpu):
+    from oracle import mindlin as M
+    tri, nrm, cen = _fault(3, 2)
+    rng = np.random.default_rng(2)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    extra = np.array([[0.3, 0.4, -0.5], [-1.2, 2.0, -3.0], [2.5, -0.5, -0.05]])
+    tg = np.vstack([cen, extra])
+    ier, lused, u, e = gpu.elhfmm3dtriatargiter(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, tg)
+    assert ier == 0 and lused == 8
+    uo, eo = M.image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg, level=2)
+    assert rel(u, uo) < 5e-8 and rel(e, eo) < 5e-8
+    # layers separately
+    _, _, u1, e1 = gpu.elhfmm3dtriatargiter(2, 1.3, 0.7, tri, nrm, cen, ssl, None, tg)
+    uo1, eo1 = M.image_direct(1.3, 0.7, tri, nrm, ssl, None, tg, level=2)
+    assert rel(u1, uo1) < 5e-8 and rel(e1, eo1) < 5e-8
+
+
+def test_total_field_traction_free_on_surface(gpu):
+    tri, nrm, cen = _fault(6, 4)
+    rng = np.random.default_rng(4)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    gx, gy = np.meshgrid(np.linspace(-3, 3, 7), np.linspace(-1, 4, 6))
+    surf = np.stack([gx.ravel(), gy.ravel(), np.zeros(gx.size)], axis=1)
+    lam, mu = 1.3, 0.7
+    _, _, ufree, efree = gpu.el3dtriadirecttarg(lam, mu, tri, nrm, cen, ssl, sdl, surf)
+    ier, _, uimg, eimg = gpu.elhfmm3dtriatargiter(2, lam, mu, tri, nrm, cen, ssl, sdl, surf)
+    assert ier == 0
+
+    def traction(e):
+        tr = np.trace(e, axis1=1, axis2=2)
+        sig = lam * tr[:, None, None] * np.eye(3)[None] + 2 * mu * e
+        return sig[:, :, 2]
+
+    t_free = traction(efree)
+    t_tot = traction(efree + eimg)
+    assert np.abs(t_tot).max() < 1e-7 * np.abs(t_free).max()
+
+
+def test_halfspace_self_and_errors(gpu):
+    tri, nrm, cen = _fault(3, 2)
+    rng = np.random.default_rng(6)
+    sdl = rng.normal(size=cen.shape)
+    ier, pt, st = gpu.halfspace_self(2, 1.0, 1.0, tri, nrm, cen, None, sdl)
+    assert ier == 0 and np.isfinite(pt).all() and np.isfinite(st).all()
+    ier, pf, sf = gpu.elfmm3dtria(2, 1.0, 1.0, tri, nrm, cen, None, sdl)
+    ier2, _, pi, si = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, cen)
+    assert ier == 0 and ier2 == 0
+    assert rel(pt, pf + pi) < 1e-14
+    # a target above the surface is rejected
+    bad = np.array([[0.0, 0.0, 0.5]])
+    assert gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, bad)[0] == 16
+    # icomp 4: nothing evaluated, lused = 8
+    ier, lused, u, _ = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, cen, icomp_type=4)
+    assert ier == 0 and lused == 8 and not u.any()
