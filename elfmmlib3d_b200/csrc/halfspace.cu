@@ -111,7 +111,11 @@ __device__ void hs_pair(const HsTri& T, const double X[3], int dosl, int dodl, d
   }
 }
 
-// One thread per target, triangles streamed through shared memory.
+// One thread per target and chunk of HS_CHUNK triangles (grid.y), the
+// triangles streamed through shared memory; partial sums are added to the
+// zeroed outputs.
+constexpr int HS_CHUNK = 512;
+
 __global__ void __launch_bounds__(128, 1)  // one CTA: let the generated kernel keep 255 registers
 k_hs_image(int n, const HsTri* __restrict__ tris, int m, const double* __restrict__ tgt, int dosl, int dodl,
            double lam, double mu, double* __restrict__ u, double* __restrict__ e6) {
@@ -125,8 +129,9 @@ k_hs_image(int n, const HsTri* __restrict__ tris, int m, const double* __restric
   quad12(Q);
   double acc[9];
   for (int k = 0; k < 9; k++) acc[k] = 0.0;
-  for (int t0 = 0; t0 < n; t0 += HS_TILE) {
-    const int cnt = min(HS_TILE, n - t0);
+  const int c0 = blockIdx.y * HS_CHUNK, c1 = min(n, c0 + HS_CHUNK);
+  for (int t0 = c0; t0 < c1; t0 += HS_TILE) {
+    const int cnt = min(HS_TILE, c1 - t0);
     __syncthreads();
     for (int q = threadIdx.x; q < cnt; q += blockDim.x) tile[q] = tris[t0 + q];
     __syncthreads();
@@ -134,8 +139,8 @@ k_hs_image(int n, const HsTri* __restrict__ tris, int m, const double* __restric
       for (int t = 0; t < cnt; t++) hs_pair(tile[t], X, dosl, dodl, lam, mu, Q, acc);
   }
   if (!ok) return;
-  for (int d = 0; d < 3; d++) u[3 * (size_t)i + d] = acc[d];
-  for (int d = 0; d < 6; d++) e6[6 * (size_t)i + d] = acc[3 + d];
+  for (int d = 0; d < 3; d++) atomicAdd(u + 3 * (size_t)i + d, acc[d]);
+  for (int d = 0; d < 6; d++) atomicAdd(e6 + 6 * (size_t)i + d, acc[3 + d]);
 }
 
 void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nrm, const double* ssl,
@@ -143,7 +148,10 @@ void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nr
                      double* e6) {
   if (n <= 0 || m <= 0) return;
   k_hs_prep<<<(n + 127) / 128, 128, 0, st>>>(n, tri, nrm, ssl, sdl, work); count_launch();
-  k_hs_image<<<(m + 127) / 128, 128, 0, st>>>(n, work, m, tgt, ssl != nullptr, sdl != nullptr, lam, mu, u, e6);
+  EFMM_CUDA_TRY(cudaMemsetAsync(u, 0, 3 * sizeof(double) * (size_t)m, st));
+  EFMM_CUDA_TRY(cudaMemsetAsync(e6, 0, 6 * sizeof(double) * (size_t)m, st));
+  dim3 grid((m + 127) / 128, (n + HS_CHUNK - 1) / HS_CHUNK);
+  k_hs_image<<<grid, 128, 0, st>>>(n, work, m, tgt, ssl != nullptr, sdl != nullptr, lam, mu, u, e6);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
