@@ -24,10 +24,13 @@ void launch_near_store(cudaStream_t st, const NearArgs& a, const long long* base
 void launch_near_replay(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K,
                         int dodisp, const double* ssl, const double* sdl, const double* store);
 // R <= 64 right-hand sides; densities (ntri_all, 3, R) tree order, outputs
-// (R, nsrc or ntgt, 3 or 6) tree order, ADDED to.
+// (R, nsrc or ntgt, 3 or 6) tree order, ADDED to.  With store != NULL the
+// pair blocks come from the ITER store (per leaf at sbase, sntri near
+// triangles) instead of being computed.
 void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int* chunk_leaf,
                        const int* chunk_e0, int R, int dostrain, const double* ssl, const double* sdl,
-                       int ntri_all, int nsrc, int ntgt);
+                       int ntri_all, int nsrc, int ntgt, const long long* sbase = nullptr,
+                       const int* sntri = nullptr, const double* store = nullptr);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
                        int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,

@@ -301,11 +301,15 @@ k_near_replay(const NearArgs a, const long long* __restrict__ base, const int* _
 // R <= 16 RB).  One CTA per (near leaf, chunk of NB_PTS evaluation points).
 constexpr int NB_PTS = 8, NB_TRI = 16, NB_THREADS = NB_PTS * NB_TRI;
 
-template <int RB>
+// REPLAY: the pair blocks are read from the stored near field (k_near_store
+// layout: per leaf at base[leaf], [point][near triangle][K]) instead of
+// computed -- the ITER store applied to many right-hand sides at once.
+template <int RB, bool REPLAY>
 __global__ void __launch_bounds__(NB_THREADS)
 k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __restrict__ chunk_e0,
              int R, int K, int dostrain, const double* __restrict__ ssl, const double* __restrict__ sdl,
-             int ntri_all, int nsrc, int ntgt) {
+             int ntri_all, int nsrc, int ntgt, const long long* __restrict__ sbase, const int* __restrict__ sntri,
+             const double* __restrict__ store) {
   constexpr int RW = 16 * RB;  // right-hand sides held per tile
   __shared__ TriRec tile[NB_TRI];
   extern __shared__ __align__(16) double nb_sm[];
@@ -335,13 +339,14 @@ k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __
 #pragma unroll
     for (int k = 0; k < RB; k++) acc[c][k] = 0.0;
   const int nl = a.dosl + a.dodl;
+  int pos = 0;  // running index of the leaf's near triangles (store layout)
   for (int b = a.nb_start[li]; b < a.nb_start[li + 1]; b++) {
     const int sb = a.nb_items[b];
     const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
     for (int k0 = 0; k0 < trn; k0 += NB_TRI) {
       const int cnt = min(NB_TRI, trn - k0);
       __syncthreads();
-      stage_tile(tile, a.trir + tr0 + k0, cnt);
+      if (!REPLAY) stage_tile(tile, a.trir + tr0 + k0, cnt);
       for (int q = tid; q < NB_TRI * 6 * RW; q += NB_THREADS) {
         int t = q / (6 * RW), j = (q / RW) % 6, r = q % RW;
         int layer = j / 3, d = j % 3;
@@ -353,7 +358,18 @@ k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __
         Sg[q] = v;
       }
       __syncthreads();
-      {
+      if (REPLAY) {
+        // the tile's blocks of the chunk's points: contiguous K-runs per point
+        const int nt = sntri[li];
+        const double* src = store + sbase[li];
+        for (int q = tid; q < NB_PTS * NB_TRI * K; q += NB_THREADS) {
+          const int pt = q / (NB_TRI * K), rem = q % (NB_TRI * K), t = rem / K, c = rem % K;
+          const int e = e0 + pt;
+          double v = 0.0;
+          if (e < nep && t < cnt) v = src[((size_t)e * nt + (pos + k0 + t)) * K + c];
+          Bk[q] = v;
+        }
+      } else {
         double* o = Bk + (pp * NB_TRI + tt) * K;
         if (ok1 && tt < cnt) {
           const int tidx = tr0 + k0 + tt;
@@ -386,6 +402,7 @@ k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __
         }
       }
     }
+    pos += trn;
   }
   (void)nl;
   const int e2 = e0 + pq;
@@ -439,7 +456,8 @@ void launch_near_replay(cudaStream_t st, const NearArgs& a, const long long* bas
 
 void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int* chunk_leaf,
                        const int* chunk_e0, int R, int dostrain, const double* ssl, const double* sdl,
-                       int ntri_all, int nsrc, int ntgt) {
+                       int ntri_all, int nsrc, int ntgt, const long long* sbase, const int* sntri,
+                       const double* store) {
   if (nchunk <= 0 || R <= 0) return;
   if (R > 64) throw CudaError{(int)cudaErrorInvalidValue};
   const int nl = a.dosl + a.dodl;
@@ -449,14 +467,23 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
   auto go = [&](auto kern) {
     EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     kern<<<nchunk, NB_THREADS, smem, st>>>(a, chunk_leaf, chunk_e0, R, K, dostrain, ssl, sdl, ntri_all, nsrc,
-                                           ntgt);
+                                           ntgt, sbase, sntri, store);
     count_launch();
   };
-  switch (RB) {
-    case 1: go(k_near_batch<1>); break;
-    case 2: go(k_near_batch<2>); break;
-    case 3: go(k_near_batch<3>); break;
-    default: go(k_near_batch<4>); break;
+  if (store) {
+    switch (RB) {
+      case 1: go(k_near_batch<1, true>); break;
+      case 2: go(k_near_batch<2, true>); break;
+      case 3: go(k_near_batch<3, true>); break;
+      default: go(k_near_batch<4, true>); break;
+    }
+  } else {
+    switch (RB) {
+      case 1: go(k_near_batch<1, false>); break;
+      case 2: go(k_near_batch<2, false>); break;
+      case 3: go(k_near_batch<3, false>); break;
+      default: go(k_near_batch<4, false>); break;
+    }
   }
   EFMM_CUDA_TRY(cudaGetLastError());
 }

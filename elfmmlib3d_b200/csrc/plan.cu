@@ -621,6 +621,33 @@ void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T
                         ops_->dim.get(), D, C, src, dst);
 }
 
+// Size and place the stored near field for the layers / outputs in flags
+// (bit 0 single layer, 1 double layer, 2 sources, 3 targets, 4 strain): K
+// doubles per (point, triangle) pair, per leaf [point][near triangle][K].
+int Plan::store_alloc(int flags, double rlam, double rmu) {
+  const int nl = (flags & 1) + ((flags >> 1) & 1), dstr = (flags >> 4) & 1;
+  const int do_src = (flags >> 2) & 1, do_tgt = (flags >> 3) & 1;
+  const int K = nl * 3 * (3 + 6 * dstr);
+  std::vector<long long> base(near_ntri_h_.size());
+  long long tot = 0;
+  for (size_t i = 0; i < near_ntri_h_.size(); i++) {
+    base[i] = tot;
+    long long nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+    tot += nep * near_ntri_h_[i] * K;
+  }
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  if ((double)tot * 8.0 > 0.9 * (double)freeb + (double)store_.cap * 8.0) return IER_ALLOC;
+  store_.resize((size_t)tot);
+  h2d(near_base_, base, st_);
+  store_K_ = K;
+  store_flags_ = flags;
+  store_lam_ = rlam;
+  store_mu_ = rmu;
+  store_valid_ = false;
+  return IER_OK;
+}
+
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
                    double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode, bool do_far) {
   int n = n_, nt = nt_;
@@ -632,26 +659,8 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   if (mode == 2 && (!store_valid_ || flags != store_flags_ || rlam != store_lam_ || rmu != store_mu_))
     return IER_HANDLE;
   if (mode == 1) {
-    // size and place the blocks: K doubles per (point, triangle) pair
-    const int nl = dosl + dodl, dstr = (ds_src || ds_tgt) ? 1 : 0;
-    const int K = nl * 3 * (3 + 6 * dstr);
-    std::vector<long long> base(near_ntri_h_.size());
-    long long tot = 0;
-    for (size_t i = 0; i < near_ntri_h_.size(); i++) {
-      base[i] = tot;
-      long long nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
-      tot += nep * near_ntri_h_[i] * K;
-    }
-    size_t freeb = 0, totb = 0;
-    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    if ((double)tot * 8.0 > 0.9 * (double)freeb + (double)store_.cap * 8.0) return IER_ALLOC;
-    store_.resize((size_t)tot);
-    h2d(near_base_, base, st_);
-    store_K_ = K;
-    store_flags_ = flags;
-    store_lam_ = rlam;
-    store_mu_ = rmu;
-    store_valid_ = false;
+    const int ier = store_alloc(flags, rlam, rmu);
+    if (ier) return ier;
   }
   long long launch0 = launches_total();
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
@@ -789,9 +798,21 @@ void Plan::flops_per_column(double* f) const {
 }
 
 int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
-                         double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision) {
-  if (R < 1 || precision < 0 || precision > 1) return IER_BADARG;
+                         double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
+                         int mode) {
+  if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
   const int n = n_, nt = nt_;
+  if (mode) {
+    const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+    const int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
+    const int flags = dosl | (dodl << 1) | (do_src << 2) | (do_tgt << 3) | ((d_e_src || d_e_tgt) ? 16 : 0);
+    if (mode == 2 && (!store_valid_ || flags != store_flags_ || rlam != store_lam_ || rmu != store_mu_))
+      return IER_HANDLE;
+    if (mode == 1) {
+      const int ier = store_alloc(flags, rlam, rmu);
+      if (ier) return ier;
+    }
+  }
   const int D = 2 * ncoef(p_);
   const size_t nb = tr_.nboxes;
   // right-hand sides per pass: at most 64 (near-field kernel), and the
@@ -811,7 +832,8 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
                          d_u_src ? d_u_src + 3 * (size_t)n * r0 : nullptr,
                          d_e_src ? d_e_src + 9 * (size_t)n * r0 : nullptr,
                          d_u_tgt ? d_u_tgt + 3 * (size_t)nt * r0 : nullptr,
-                         d_e_tgt ? d_e_tgt + 9 * (size_t)nt * r0 : nullptr, precision == 1);
+                         d_e_tgt ? d_e_tgt + 9 * (size_t)nt * r0 : nullptr, precision == 1,
+                         mode == 1 && r0 == 0 ? 1 : (mode ? 2 : 0));
     if (ier) return ier;
     tot += timings.total;
     near += timings.near;
@@ -920,7 +942,7 @@ void Plan::l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt) {
 }
 
 int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
-                     double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed) {
+                     double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed, int mode) {
   const int n = n_, nt = nt_;
   const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   const int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
@@ -1058,9 +1080,10 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
   }
   EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
-  // near field: frames only (densities enter the batched contraction)
+  // near field: frames only (densities enter the batched contraction; the
+  // stored operator, when replayed, replaces them)
   trir_.resize(n);
-  launch_tri_prep(st_, n, tri_s_.get(), nullptr, nullptr, nullptr, 0, 0, trir_.get());
+  if (mode != 2) launch_tri_prep(st_, n, tri_s_.get(), nullptr, nullptr, nullptr, 0, 0, trir_.get());
   const int key = do_src | (do_tgt << 1);
   if (chunk_key_ != key) {
     std::vector<int> cl, ce;
@@ -1087,9 +1110,16 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   na.do_src = do_src; na.do_tgt = do_tgt;
   na.rlam = rlam; na.rmu = rmu;
   na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
+  if (mode == 1) {
+    NearArgs sa = na;  // stored rows: displacement, and strain if any output wants it
+    sa.dostrain_src = sa.dostrain_tgt = (store_flags_ >> 4) & 1;
+    launch_near_store(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, 1, store_.get());
+    store_valid_ = true;
+  }
   if (dosl || dodl)
     launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, (ds_src || ds_tgt) ? 1 : 0,
-                      ssl_s_.get(), sdl_s_.get(), n, n, nt);
+                      ssl_s_.get(), sdl_s_.get(), n, n, nt, mode ? near_base_.get() : nullptr,
+                      mode ? near_ntri_.get() : nullptr, mode ? store_.get() : nullptr);
   EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
   if (do_src) {
     k_scatter_out<<<dim3((n + 255) / 256, R), 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src,

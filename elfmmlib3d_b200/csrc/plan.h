@@ -98,10 +98,12 @@ class Plan {
   // tree, lists and operators are shared; the near-field pair responses are
   // computed once and contracted with all right-hand sides.
   // precision 0: FP64 throughout; 1: mixed (P2M products and translations
-  // in FP32 with FP32 expansions, everything else FP64).
+  // in FP32 with FP32 expansions, everything else FP64).  mode as in
+  // evaluate: 1 stores the near-field operator (then replays it for all
+  // right-hand sides), 2 replays a stored one.
   int evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt,
-                     int precision = 0);
+                     int precision = 0, int mode = 0);
   // useful flops per expansion column of one pass: P2M, M2M, M2L, L2L, L2T
   void flops_per_column(double* f5) const;
   // all-pairs direct sum on the same geometry (no tree needed)
@@ -123,7 +125,8 @@ class Plan {
  private:
   void build_worklists();
   int batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
-                 double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed);
+                 double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed, int mode);
+  int store_alloc(int flags, double rlam, double rmu);
   DevBuf<float> mpole_f_, local_f_;
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA
   int nchunk_ = 0, chunk_key_ = -1;

@@ -175,6 +175,17 @@ int efmm_plan_evaluate_iter(efmm_plan *plan, double rlam, double rmu, const doub
                             const double *sdl, double *u_src, double *e_src, double *u_tgt,
                             double *e_tgt, int mode);
 
+/* Batched ITER evaluation: efmm_plan_evaluate_batch with the stored
+ * near-field interactions of efmm_plan_evaluate_iter (mode 1 stores them,
+ * mode 2 reuses them; the same store serves both entry points when the
+ * layers, outputs and Lame constants agree, else 512).  The replay is one
+ * sparse-block product of the stored pair responses with all right-hand
+ * sides (the ITER store of src/elfmm3dtria_iter_1.f:1240-1419 applied to
+ * nrhs density pairs at once). */
+int efmm_plan_evaluate_batch_iter(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
+                                  const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                                  double *e_tgt, int precision, int mode);
+
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 

@@ -147,3 +147,79 @@ def test_direct_subset_matches_full_direct(gpu):
     P.evaluate_direct_subset(1.3, 0.7, ns, d(ssl), d(sdl), u, e)
     assert rel(u.cpu().numpy(), full[0][:ns]) < 1e-14 and rel(e.cpu().numpy(), full[1][:ns]) < 1e-14
     P.close()
+
+
+def _batch_mode(P, d, R, ssl, sdl, n, m, mode, precision=0, rlam=1.3, strain=True):
+    torch = _t()
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device="cuda")
+    e = torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    ut = torch.zeros((R, m, 3), dtype=torch.float64, device="cuda")
+    et = torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    P.evaluate_batch(rlam, 0.7, R, d(ssl) if ssl is not None else None, d(sdl) if sdl is not None else None,
+                     u, e, ut, et, precision=precision, mode=mode)
+    return [u.cpu().numpy(), e.cpu().numpy() if strain else None, ut.cpu().numpy(),
+            et.cpu().numpy() if strain else None]
+
+
+@pytest.mark.parametrize("R", [3, 37, 70])
+def test_batch_iter_store_and_replay(gpu, R):
+    # mode 1 stores the near-field pair responses and contracts them with
+    # all right-hand sides; mode 2 replays them for new densities.  Both
+    # equal the analytic batched pass (R = 70 runs as two passes: store,
+    # then replay)
+    torch = _t()
+    tri, nrm, cen = G.sphere_triangles(3)
+    tg = G.box_targets(90, 41)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    P = gpu.Plan(0)
+    P.set_geometry(d(tri), d(nrm), d(cen), d(tg), iprec=2, iter=True)
+    n, m = len(cen), len(tg)
+    rng = np.random.default_rng(100 + R)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch_mode(P, d, R, ssl, sdl, n, m, 0)
+    b = _batch_mode(P, d, R, ssl, sdl, n, m, 1)
+    for x, y in zip(a, b):
+        assert rel(x, y) < SAME
+    assert P.stored_bytes() > 0
+    s2, d2 = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    c = _batch_mode(P, d, R, s2, d2, n, m, 2)
+    e = _batch_mode(P, d, R, s2, d2, n, m, 0)
+    for x, y in zip(c, e):
+        assert rel(x, y) < SAME
+    # mixed precision on the stored near field
+    f = _batch_mode(P, d, R, s2, d2, n, m, 2, precision=1)
+    assert rel(f[0], e[0]) < 0.5e-6 and rel(f[2], e[2]) < 0.5e-6
+    # the same store serves the single-density ITER call
+    u = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
+    ee = torch.zeros((n, 3, 3), dtype=torch.float64, device="cuda")
+    ut = torch.zeros((m, 3), dtype=torch.float64, device="cuda")
+    et = torch.zeros((m, 3, 3), dtype=torch.float64, device="cuda")
+    P.evaluate(1.3, 0.7, d(s2[0]), d(d2[0]), u, ee, ut, et, mode=2)
+    assert rel(u.cpu().numpy(), e[0][0]) < SAME and rel(et.cpu().numpy(), e[3][0]) < SAME
+    # other Lame constants than the store's: handle mismatch
+    with pytest.raises(gpu.ElfmmError) as ex:
+        _batch_mode(P, d, R, s2, d2, n, m, 2, rlam=1.4)
+    assert ex.value.ier == 512
+    P.close()
+
+
+def test_batch_iter_single_layer_displacement_only(gpu):
+    torch = _t()
+    tri, nrm, cen = G.sphere_triangles(2)
+    tg = G.box_targets(30, 43)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    P = gpu.Plan(0)
+    P.set_geometry(d(tri), d(nrm), d(cen), d(tg), iprec=1, iter=True)
+    n, m = len(cen), len(tg)
+    R = 17
+    rng = np.random.default_rng(5)
+    ssl = rng.normal(size=(R, n, 3))
+    _batch_mode(P, d, R, ssl, None, n, m, 1, strain=False)
+    s2 = rng.normal(size=(R, n, 3))
+    a = _batch_mode(P, d, R, s2, None, n, m, 2, strain=False)
+    b = _batch_mode(P, d, R, s2, None, n, m, 0, strain=False)
+    assert rel(a[0], b[0]) < SAME and rel(a[2], b[2]) < SAME
+    # a replay asking for strain the store does not hold is a mismatch
+    with pytest.raises(gpu.ElfmmError):
+        _batch_mode(P, d, R, s2, None, n, m, 2)
+    P.close()
