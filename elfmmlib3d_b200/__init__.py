@@ -50,7 +50,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
+           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_hs_image_direct", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
 
 
 class ElfmmError(RuntimeError):
@@ -87,6 +87,9 @@ def load():
     L.efmm_plan_flops.argtypes = [_vp, _dp]
     L.efmm_plan_stored_bytes.restype = ctypes.c_longlong
     L.efmm_plan_stored_bytes.argtypes = [_vp]
+    L.efmm_plan_evaluate_image.restype = ctypes.c_int
+    L.efmm_plan_evaluate_image.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp,
+                                           _vp, ctypes.c_int, ctypes.c_int]
     L.efmm_plan_evaluate_batch_iter.restype = ctypes.c_int
     L.efmm_plan_evaluate_batch_iter.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp,
                                                 _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
@@ -265,6 +268,29 @@ def elhfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=N
     return ier.value, lused.value, ptt[:m], stt[:m]
 
 
+def hs_image_direct(rlam, rmu, triangle, trinorm, sigma_sl=None, sigma_dl=None, target=None):
+    """Image part by direct summation (all pairs, refined quadrature): the
+    check of the image FMM.  Returns (ier, u (m,3), e (m,3,3))."""
+    L = load()
+    _need_gpu()
+    tri = _c(triangle, (-1, 3, 3))
+    n = tri.shape[0]
+    nrm = _c(trinorm, (n, 3))
+    ssl = _c(sigma_sl, (n, 3)) if sigma_sl is not None else None
+    sdl = _c(sigma_dl, (n, 3)) if sigma_dl is not None else None
+    tg = _c(target, (-1, 3))
+    m = tg.shape[0]
+    u = np.zeros((max(m, 1), 3))
+    e = np.zeros((max(m, 1), 3, 3))
+    f = L.efmm_hs_image_direct
+    f.restype = ctypes.c_int
+    ier = f(ctypes.c_int(2), ctypes.c_double(rlam), ctypes.c_double(rmu), tri.ctypes.data_as(_dp),
+            nrm.ctypes.data_as(_dp), ctypes.c_int(n), ssl.ctypes.data_as(_dp) if ssl is not None else None,
+            sdl.ctypes.data_as(_dp) if sdl is not None else None, ctypes.c_int(m), tg.ctypes.data_as(_dp),
+            u.ctypes.data_as(_dp), e.ctypes.data_as(_dp))
+    return ier, u[:m], e[:m]
+
+
 def halfspace_self(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None):
     """Half-space self-evaluation at the centroids: the free-space (direct
     arrival, on-surface) evaluation plus the image part with the centroids as
@@ -397,6 +423,16 @@ class Plan:
             ier = self._L.efmm_plan_evaluate_batch(*args)
         if ier:
             raise ElfmmError(ier, "evaluate_batch")
+
+    def evaluate_image(self, rlam, rmu, nrhs, ssl=None, sdl=None, ut=None, et=None, precision=0, mode=0):
+        """Half-space image part at the points x whose reflections (x1, x2,
+        -x3) were given as this plan's targets (set_geometry(..., mindlin=True)):
+        ssl/sdl (nrhs,n,3); outputs ut (nrhs,nt,3), et (nrhs,nt,3,3)."""
+        ier = self._L.efmm_plan_evaluate_image(self._h, float(rlam), float(rmu), int(nrhs), self._ptr(ssl),
+                                               self._ptr(sdl), self._ptr(ut), self._ptr(et), int(precision),
+                                               int(mode))
+        if ier:
+            raise ElfmmError(ier, "evaluate_image")
 
     def record(self, slot):
         """Record CUDA event `slot` (0..7) on the plan's stream."""

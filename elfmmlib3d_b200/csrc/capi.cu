@@ -104,6 +104,12 @@ extern "C" int efmm_plan_evaluate_batch_iter(efmm_plan* p, double rlam, double r
                                             mode);)
 }
 
+extern "C" int efmm_plan_evaluate_image(efmm_plan* p, double rlam, double rmu, int nrhs, const double* ssl,
+                                        const double* sdl, double* u_tgt, double* e_tgt, int precision, int mode) {
+  if (!p) return IER_BADARG;
+  EFMM_GUARD(return p->plan->evaluate_image(rlam, rmu, nrhs, ssl, sdl, u_tgt, e_tgt, precision, mode);)
+}
+
 extern "C" long long efmm_plan_stored_bytes(const efmm_plan* p) { return 8 * p->plan->stored_doubles(); }
 
 extern "C" void efmm_plan_flops(const efmm_plan* p, double* f5) { p->plan->flops_per_column(f5); }
@@ -450,6 +456,13 @@ int hs_call(int iprec, double rlam, double rmu, const double* tri, const double*
   }
 }
 }  // namespace
+
+extern "C" int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n,
+                                    const double* ssl, const double* sdl, int nt, const double* tgt, double* u,
+                                    double* e) {
+  return hs_call(iprec, rlam, rmu, tri, nrm, n, ssl != nullptr, ssl, sdl != nullptr, sdl, nt, tgt, u != nullptr,
+                 u, e != nullptr, e, 1, nullptr);
+}
 
 extern "C" void elhfmm3dtriatargiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
                                       const double* triangle, const double* trinorm, const int* nparts,

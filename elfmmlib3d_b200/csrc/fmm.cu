@@ -29,6 +29,8 @@ __global__ void k_build_ops(int nop, const OpDesc* __restrict__ ops, double* __r
   int p = o.p;
   if (o.kind == 0) {
     if (threadIdx.x == 0) irregular_harmonics(2 * p, o.d[0], o.d[1], o.d[2], tab);
+  } else if (o.kind == 3) {  // M2L of the half-space kernel U: T replaced by J
+    if (threadIdx.x == 0) u_harmonics(2 * p, o.d[0], o.d[1], o.d[2], tab);
   } else {
     if (threadIdx.x == 0) regular_harmonics(p, o.d[0], o.d[1], o.d[2], tab);
   }
@@ -39,7 +41,7 @@ __global__ void k_build_ops(int nop, const OpDesc* __restrict__ ops, double* __r
   for (long long q = threadIdx.x; q < tot; q += blockDim.x) {
     int r = (int)(q / nc), c = (int)(q % nc);
     double rr, ri, ir, ii;
-    op_entry(o.kind, tab, r, c, &rr, &ri, &ir, &ii);
+    op_entry(o.kind == 3 ? 0 : o.kind, tab, r, c, &rr, &ri, &ir, &ii);
     size_t r2 = 2 * (size_t)r, c2 = 2 * (size_t)c;
     M[r2 * dim + c2] = rr;
     M[r2 * dim + c2 + 1] = ri;
@@ -372,7 +374,10 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
 // product  mpole[box][col][row] = sum_k A[k][row] B[col][k]  (k_gemm_tn).
 // The features depend on the geometry only; each is computed once per node
 // instead of once per output tile.
-template <class T>
+// NF = 4: charge and dipole rows per node; NF = 9 adds the five second
+// derivatives (xx, yy, xy, xz, yz; zz = -xx - yy) that carry quadrupole
+// sources (the half-space image columns).
+template <class T, int NF>
 __global__ void __launch_bounds__(256)
 k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ foff,
                const long long* __restrict__ noff, double* __restrict__ nrec, T* __restrict__ F) {
@@ -425,7 +430,7 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
     }
   }
   __syncwarp();
-  T* out = F + foff[blockIdx.x] + (size_t)(4 * node) * D;
+  T* out = F + foff[blockIdx.x] + (size_t)(NF * node) * D;
   for (int cc = lane; cc < nc; cc += 32) {
     int fn = 0;
     while ((fn + 1) * (fn + 2) / 2 <= cc) fn++;
@@ -447,6 +452,111 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
     out[2 * D + 2 * cc + 1] = (T)(sr * 0.5 * is * (yb.re + yc.re));
     out[3 * D + 2 * cc] = (T)(sr * is * ya.re);
     out[3 * D + 2 * cc + 1] = (T)(-sr * is * ya.im);
+    if (NF == 9) {
+      // second derivatives from the ladder relations (conjugated rows):
+      //   xx = (Y^{m+2} - 2 Y^m + Y^{m-2}) / 4,  yy = -(Y^{m+2} + 2 Y^m + Y^{m-2}) / 4,
+      //   xy = (Y^{m+2} - Y^{m-2}) / 4i,  xz = (Y^{m+1} - Y^{m-1}) / 2,  yz = (Y^{m+1} + Y^{m-1}) / 2i
+      // (all of degree n - 2)
+      cplx y0 = {0, 0}, yp1 = {0, 0}, ym1 = {0, 0}, yp2 = {0, 0}, ym2 = {0, 0};
+      if (fn > 1) {
+        y0 = hget(Y, fn - 2, fm);
+        yp1 = hget(Y, fn - 2, fm + 1);
+        ym1 = hget(Y, fn - 2, fm - 1);
+        yp2 = hget(Y, fn - 2, fm + 2);
+        ym2 = hget(Y, fn - 2, fm - 2);
+      }
+      const double q = sr * is * is;
+      out[4 * D + 2 * cc] = (T)(q * 0.25 * (yp2.re - 2.0 * y0.re + ym2.re));
+      out[4 * D + 2 * cc + 1] = (T)(-q * 0.25 * (yp2.im - 2.0 * y0.im + ym2.im));
+      out[5 * D + 2 * cc] = (T)(-q * 0.25 * (yp2.re + 2.0 * y0.re + ym2.re));
+      out[5 * D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.im + 2.0 * y0.im + ym2.im));
+      out[6 * D + 2 * cc] = (T)(q * 0.25 * (yp2.im - ym2.im));
+      out[6 * D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.re - ym2.re));
+      out[7 * D + 2 * cc] = (T)(q * 0.5 * (yp1.re - ym1.re));
+      out[7 * D + 2 * cc + 1] = (T)(-q * 0.5 * (yp1.im - ym1.im));
+      out[8 * D + 2 * cc] = (T)(q * 0.5 * (yp1.im + ym1.im));
+      out[8 * D + 2 * cc + 1] = (T)(q * 0.5 * (yp1.re + ym1.re));
+    }
+  }
+}
+
+// Node weights of the half-space image columns, 7R per box: for right-hand
+// side r, columns 6r..6r+5 hold the anti-image passes 0..3 (the free-space
+// passes with the anti-image constants c1, c2 of P2MArgs) and the two 1/r
+// potentials Phi_a, Phi_c of the C piece; column 6R + r holds the U
+// potential W of the B piece.  Per node 9 rows: charge, dipole (3) and the
+// five second-derivative rows (xx - zz, yy - zz, 2xy, 2xz, 2yz of the
+// quadrupole tensor).  With f the single-layer density, T the double-layer
+// tensor lam (b.n) I + mu (b n^T + n b^T), h = -y_3 the source depth and
+// alpha = (lam + mu)/(lam + 2 mu) (sources in the gradient-of-source
+// convention of the product features):
+//   Phi_a: q = -(2 - alpha) f_3, D = -h alpha f - (2 - 2 alpha) T e_3, Q = -h alpha T
+//   Phi_c: D = -f, Q = -T
+//   W:     D = (f_1, f_2, -f_3), Q = diag-sign form of -(S T + T S)/2, S = diag(-1,-1,1)
+// (the B and C pieces of src/mindlinpieces.f:29-520 written as Laplace
+// potentials; their double layers by differentiation at the source).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ woff,
+                  const long long* __restrict__ noff, const double* __restrict__ nrec, T* __restrict__ W) {
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int tn = a.scount[box];
+  const int nnode = 12 * tn, K = 9 * nnode, C = 7 * R;
+  const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu, al = a.alpha, lam = a.lam, mu = a.mu;
+  const double* nd = nrec + 8 * noff[blockIdx.x];
+  T* out = W + woff[blockIdx.x];
+  for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < (long long)nnode * C;
+       q += (long long)gridDim.y * blockDim.x) {
+    const int col = (int)(q / nnode), node = (int)(q % nnode);
+    const int r = col < 6 * R ? col / 6 : col - 6 * R;
+    const int kind = col < 6 * R ? col % 6 : 6;
+    const double* o = nd + 8 * node;
+    const double y[3] = {o[0], o[1], o[2]}, nn[3] = {o[3], o[4], o[5]}, w = o[6];
+    const long long it = (long long)o[7];
+    const long long off = r * a.rstride + it * a.tstride, ds = a.dstride;
+    double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+    if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
+    if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
+    double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    double Qm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    const double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
+    double Tm[3][3];
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) Tm[k][l] = (k == l ? lam * dln : 0.0) + mu * (dl[k] * nn[l] + dl[l] * nn[k]);
+    const double h = -y[2];
+    if (kind < 3) {
+      wv[0] = sl[kind] * inv2mu;
+      for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * (nn[d] * dl[kind] + dl[d] * nn[kind]);
+    } else if (kind == 3) {
+      const double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
+      const double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+      const double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+      wv[0] = sly * c1 * inv2mu + dln * c2;
+      for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
+    } else if (kind == 4) {
+      wv[0] = -(2.0 - al) * sl[2];
+      for (int d = 0; d < 3; d++) wv[1 + d] = -h * al * sl[d] - (2.0 - 2.0 * al) * Tm[2][d];
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) Qm[k][l] = -h * al * Tm[k][l];
+    } else if (kind == 5) {
+      for (int d = 0; d < 3; d++) wv[1 + d] = -sl[d];
+      for (int k = 0; k < 3; k++)
+        for (int l = 0; l < 3; l++) Qm[k][l] = -Tm[k][l];
+    } else {
+      wv[1] = sl[0];
+      wv[2] = sl[1];
+      wv[3] = -sl[2];
+      Qm[0][0] = Tm[0][0]; Qm[1][1] = Tm[1][1]; Qm[2][2] = -Tm[2][2];
+      Qm[0][1] = Qm[1][0] = Tm[0][1];
+    }
+    wv[4] = Qm[0][0] - Qm[2][2];
+    wv[5] = Qm[1][1] - Qm[2][2];
+    wv[6] = 2.0 * Qm[0][1];
+    wv[7] = 2.0 * Qm[0][2];
+    wv[8] = 2.0 * Qm[1][2];
+    T* ow = out + (size_t)col * K + 9 * node;
+#pragma unroll
+    for (int k = 0; k < 9; k++) ow[k] = (T)(w * wv[k]);
   }
 }
 
@@ -1197,9 +1307,80 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
   }
 }
 
+// Half-space image recombination at the reflected targets xb = (x1, x2, -x3)
+// of the plan (columns as in k_p2m_weights_img, 7R per leaf in S).  In the
+// variables xb, with alpha = (lam + mu)/(lam + 2 mu), sc = (1 - alpha)/alpha:
+//   anti-image  u_A  = the free-space recombination with c1 = 2 - alpha
+//   B piece     u_B  = (sc / mu) grad W
+//   C piece     u_C  = (x3 / mu) P,  P = (d1 Phi_a, d2 Phi_a, -d3 Phi_a - (2 - alpha) Phi_c)
+// and the strain of u(x) = u(xb(x)) uses d/dx_j = s_j d/dxb_j, s = (1, 1, -1).
+__global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__ wleaves,
+                                 const long long* __restrict__ soff, const double* __restrict__ S) {
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int P = a.tcount[box];
+  const size_t ldc = 9 * (size_t)P + ((9 * P) & 1);
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
+  const double c1 = a.c1, al = a.alpha, imu = 1.0 / a.mu, sc = (1.0 - al) / al;
+  for (int q = threadIdx.x; q < P * R; q += blockDim.x) {
+    const int e = q % P, r = q / P;
+    const int pidx = a.tstart[box] + e;
+    const double* X = a.tgt_pts + 3 * (size_t)pidx;
+    const double x[3] = {X[0], X[1], X[2]};
+    double pot[7], g[7][3], H[7][3][3];
+    for (int cidx7 = 0; cidx7 < 7; cidx7++) {
+      const int col = cidx7 < 6 ? 6 * r + cidx7 : 6 * R + r;
+      const double* sv = S + soff[blockIdx.x] + (size_t)col * ldc + 9 * (size_t)e;
+      pot[cidx7] = sv[0];
+      g[cidx7][0] = sv[3] * is;
+      g[cidx7][1] = sv[4] * is;
+      g[cidx7][2] = sv[1] * is;
+      const double hzz = sv[2];
+      const double hxx = 0.5 * (sv[7] - hzz), hyy = 0.5 * (-sv[7] - hzz), hxy = 0.5 * sv[8];
+      const double hxz = sv[5], hyz = sv[6];
+      H[cidx7][0][0] = hxx * is2; H[cidx7][1][1] = hyy * is2; H[cidx7][2][2] = hzz * is2;
+      H[cidx7][0][1] = H[cidx7][1][0] = hxy * is2;
+      H[cidx7][0][2] = H[cidx7][2][0] = hxz * is2;
+      H[cidx7][1][2] = H[cidx7][2][1] = hyz * is2;
+    }
+    // columns: 0..3 anti-image passes, 4 Phi_a, 5 Phi_c, 6 W
+    const double x3 = -x[2];
+    const double Pv[3] = {g[4][0], g[4][1], -g[4][2] - (2.0 - al) * pot[5]};
+    double u[3], Gm[3][3];
+    for (int i = 0; i < 3; i++) {
+      u[i] = (2.0 - c1) * pot[i] + g[3][i];
+      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+      u[i] += sc * imu * g[6][i] + x3 * imu * Pv[i];
+    }
+    for (int aa = 0; aa < 3; aa++)
+      for (int bb = 0; bb < 3; bb++) {
+        double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
+        for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+        v += sc * imu * H[6][aa][bb];
+        const double dP = aa < 2 ? H[4][aa][bb] : -H[4][2][bb] - (2.0 - al) * g[5][bb];
+        v += imu * ((bb == 2 ? -Pv[aa] : 0.0) + x3 * dP);
+        Gm[aa][bb] = v;  // d u_a / d xb_b
+      }
+    double* U = a.u_tgt + 3 * (a.ntgt * r + pidx);
+    U[0] += u[0];
+    U[1] += u[1];
+    U[2] += u[2];
+    if (a.dostrain_tgt) {
+      // d u_a / d x_b = s_b Gm[a][b]
+      double* E = a.e_tgt + 6 * (a.ntgt * r + pidx);
+      E[0] += Gm[0][0];
+      E[1] += Gm[1][1];
+      E[2] -= Gm[2][2];
+      E[3] += 0.5 * (Gm[0][1] + Gm[1][0]);
+      E[4] += 0.5 * (-Gm[0][2] + Gm[2][0]);
+      E[5] += 0.5 * (-Gm[1][2] + Gm[2][1]);
+    }
+  }
+}
+
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
-                         int ntask, const GemmTask* tasks, const double* local) {
+                         int ntask, const GemmTask* tasks, const double* local, bool image) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
@@ -1208,9 +1389,36 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
   const int gsm = (int)(sizeof(double) * 4 * 16 * 128);
   EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
   k_gemm_tn<double><<<ntask, 256, gsm, st>>>(tasks, Gbuf, local, Sbuf); count_launch();
-  k_l2t_finish<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf); count_launch();
+  if (image)
+    k_l2t_finish_img<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
+  else
+    k_l2t_finish<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
+  count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+
+template <class T>
+void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
+                             const long long* foff, const long long* woff, const long long* noff, double* nrec,
+                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole) {
+  if (nwleaf <= 0) return;
+  const int nc = ncoef(a.p);
+  const int smem = (int)(sizeof(cplx) * 8 * nc);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_p2m_features<T, 9><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
+  count_launch();
+  k_p2m_weights_img<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
+  const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+  k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+template void launch_p2m_img_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*,
+                                              const long long*, const long long*, const long long*, double*, int,
+                                              double*, double*, int, const GemmTask*, double*);
+template void launch_p2m_img_twostage<float>(cudaStream_t, const P2MArgs&, int, int, const int*,
+                                             const long long*, const long long*, const long long*, double*, int,
+                                             float*, float*, int, const GemmTask*, float*);
 
 // ---------------------------------------------------------------- launchers
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp) {
@@ -1238,8 +1446,8 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_p2m_features<T><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_p2m_features<T, 4><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
   const int gsm = (int)(sizeof(T) * 4 * 16 * 128);

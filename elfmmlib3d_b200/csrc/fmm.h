@@ -6,7 +6,8 @@
 namespace efmm {
 
 // One translation operator: kind 0 = M2L (d = offset in box units),
-// 1 = M2M, 2 = L2L (d = child centre - parent centre in parent units).
+// 1 = M2M, 2 = L2L (d = child centre - parent centre in parent units),
+// 3 = M2L of the half-space kernel U = z log(r + z) - r (d as for kind 0).
 struct OpDesc {
   int kind, p;
   double d[3];
@@ -44,6 +45,9 @@ struct P2MArgs {
   int C = 4;
   long long rstride = 0, tstride = 3, dstride = 1;
   const double* wnorm = nullptr;  // product form: rows scaled by wnorm[row] if set
+  // half-space image columns: alpha = (lam + mu)/(lam + 2 mu) and the Lame
+  // constants of the double-layer tensor
+  double alpha = 0, lam = 0, mu = 0;
 };
 
 struct L2TArgs {
@@ -59,6 +63,7 @@ struct L2TArgs {
   // outputs at r * (3 or 6) * (number of sources or targets)
   int C = 4;
   long long nsrc = 0, ntgt = 0;
+  double alpha = 0, mu = 0;  // half-space image recombination
 };
 
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);
@@ -87,9 +92,19 @@ bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const i
 // (per leaf at goff: D rows of 9 x points), the FP64 product into S (per leaf
 // at soff: 4R columns of 9 x points; tasks cut by the caller, B = local),
 // then the Lame recombination into the outputs.
+// image = true: the half-space image columns (7R per leaf, targets only)
+// and their recombination (k_l2t_finish_img).
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
-                         int ntask, const GemmTask* tasks, const double* local);
+                         int ntask, const GemmTask* tasks, const double* local, bool image = false);
+// Two-stage P2M of the half-space image columns (7R per box, tasks cut by
+// the caller): node features with second-derivative rows (9 x 12 x
+// triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12
+// x triangles per leaf at woff), batched product into mpole.
+template <class T>
+void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
+                             const long long* foff, const long long* woff, const long long* noff, double* nrec,
+                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole);
 template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                       const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,

@@ -100,15 +100,25 @@ def main():
     dl = disp_strain([sum(cijkl(p, q, k, l) * b[p] * NN[q] * sp.diff(G[k][i], S[l])
                           for p in range(3) for q in range(3) for k in range(3) for l in range(3)
                           if cijkl(p, q, k, l) != 0) for i in range(3)])
+    # unit-density blocks (27 doubles: per direction k of the force or jump,
+    # displacement then strain): the stored near-field form
+    sl_blk = sum((disp_strain(G[k]) for k in range(3)), [])
+    dl_blk = sum((disp_strain([sum(cijkl(p, q, k, l) * NN[q] * sp.diff(G[k][i], S[l])
+                                   for q in range(3) for k in range(3) for l in range(3)
+                                   if cijkl(p, q, k, l) != 0) for i in range(3)]) for p in range(3)), [])
     out = ['// mindlin_gen.cuh -- generated by gen_mindlin.py; do not edit.',
            '// Image part of the half-space Green\'s functions of a point force f',
            '// (single layer) and of a point displacement jump b with normal n',
            '// (double layer) at source s, seen at target (x, y, z): 9 doubles,',
-           '// displacement (3) then strain (xx yy zz xy xz yz).',
+           '// displacement (3) then strain (xx yy zz xy xz yz).  The _blk forms',
+           '// return the responses to the three unit forces / unit jumps, 27 doubles',
+           '// (direction-major, 9 each).',
            '#pragma once', '#include "tri_index.cuh"', '', 'namespace efmm {', '']
     for name, exprs, extra in (('mindlin_image_sl', sl, ', double f1, double f2, double f3'),
                                ('mindlin_image_dl', dl, ', double b1, double b2, double b3, double n1, double n2, '
-                                                        'double n3')):
+                                                        'double n3'),
+                               ('mindlin_image_sl_blk', sl_blk, ''),
+                               ('mindlin_image_dl_blk', dl_blk, ', double n1, double n2, double n3')):
         rep, red = sp.cse(exprs, symbols=sp.numbered_symbols('t'), optimizations='basic')
         out.append(f'EFMM_HD void {name}(double lam, double mu, double x, double y, double z, double s1, '
                    f'double s2, double s3{extra}, double* o) {{')

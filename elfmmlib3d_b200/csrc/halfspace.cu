@@ -11,9 +11,9 @@
 // reflected target (the reference refines adaptively too,
 // src/tria3adamar.f:16-548, with a depth cap).
 //
-// Not built: the image far field as expansions (the anti-image elastic FMM
-// and the Mindlin B/C plane-wave FMM of src/lfmm3dtriamindlin_iter_1.f); the
-// direct sum costs O(N M) pair integrals.
+// This direct sum (O(N M) pair integrals) is the check of the image FMM
+// (image.cu); the FMM's near field uses the same refined quadrature
+// (k_hs_store).
 #include "common.cuh"
 #include "mindlin_gen.cuh"
 #include "halfspace.h"
@@ -141,6 +141,128 @@ k_hs_image(int n, const HsTri* __restrict__ tris, int m, const double* __restric
   if (!ok) return;
   for (int d = 0; d < 3; d++) atomicAdd(u + 3 * (size_t)i + d, acc[d]);
   for (int d = 0; d < 6; d++) atomicAdd(e6 + 6 * (size_t)i + d, acc[3 + d]);
+}
+
+// Unit-density blocks of one (target, triangle) pair with the refinement of
+// hs_pair: acc[0..26] single layer (unit force e_k at 9k), acc[27..53]
+// double layer (unit jump e_p at 27 + 9p); displacement then strain.
+__device__ void hs_pair_blk(const double* tv, const double nrm[3], const double X[3], int dosl, int dodl,
+                            double lam, double mu, const Quad12& Q, double* acc) {
+  const double Xr[3] = {X[0], X[1], -X[2]};
+  HsSub stk[HS_STACK];
+  for (int c = 0; c < 9; c++) stk[0].v[c] = tv[c];
+  stk[0].depth = 0;
+  int top = 1;
+  while (top > 0) {
+    const HsSub s = stk[--top];
+    const double* a = s.v;
+    const double* b = s.v + 3;
+    const double* c = s.v + 6;
+    double cen[3], diam;
+    for (int d = 0; d < 3; d++) cen[d] = (a[d] + b[d] + c[d]) / 3.0;
+    {
+      double e0 = 0, e1 = 0, e2 = 0;
+      for (int d = 0; d < 3; d++) {
+        e0 += (b[d] - a[d]) * (b[d] - a[d]);
+        e1 += (c[d] - b[d]) * (c[d] - b[d]);
+        e2 += (a[d] - c[d]) * (a[d] - c[d]);
+      }
+      diam = sqrt(fmax(e0, fmax(e1, e2)));
+    }
+    double dist2 = 0;
+    for (int d = 0; d < 3; d++) dist2 += (Xr[d] - cen[d]) * (Xr[d] - cen[d]);
+    if (dist2 > HS_RATIO * HS_RATIO * diam * diam || s.depth >= HS_MAXDEPTH || top + 4 > HS_STACK) {
+      const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+      const double v[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+      const double cr[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+      const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      for (int q = 0; q < 12; q++) {
+        double y[3];
+        for (int d = 0; d < 3; d++) y[d] = Q.b[q][0] * a[d] + Q.b[q][1] * b[d] + Q.b[q][2] * c[d];
+        const double w = Q.w[q] * area;
+        double o[27];
+        if (dosl) {
+          mindlin_image_sl_blk(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], o);
+          for (int k = 0; k < 27; k++) acc[k] += w * o[k];
+        }
+        if (dodl) {
+          mindlin_image_dl_blk(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], nrm[0], nrm[1], nrm[2], o);
+          for (int k = 0; k < 27; k++) acc[27 + k] += w * o[k];
+        }
+      }
+    } else {
+      double ab[3], bc[3], ca[3];
+      for (int d = 0; d < 3; d++) {
+        ab[d] = 0.5 * (a[d] + b[d]);
+        bc[d] = 0.5 * (b[d] + c[d]);
+        ca[d] = 0.5 * (c[d] + a[d]);
+      }
+      const double* kids[4][3] = {{a, ab, ca}, {ab, b, bc}, {ca, bc, c}, {ab, bc, ca}};
+      for (int k = 0; k < 4; k++) {
+        HsSub t;
+        for (int vtx = 0; vtx < 3; vtx++)
+          for (int d = 0; d < 3; d++) t.v[3 * vtx + d] = kids[k][vtx][d];
+        t.depth = s.depth + 1;
+        stk[top++] = t;
+      }
+    }
+  }
+}
+
+constexpr int HSS_PTS = 8;  // targets per CTA (the batched near-field chunks)
+
+__global__ void __launch_bounds__(128, 1)
+k_hs_store(const HsStoreArgs a, const int* __restrict__ chunk_leaf, const int* __restrict__ chunk_e0,
+           double* __restrict__ store) {
+  const int li = chunk_leaf[blockIdx.x], e0 = chunk_e0[blockIdx.x];
+  const int leaf = a.leaves[li];
+  const int tn = a.box_tgt_count[leaf], t0 = a.box_tgt_start[leaf];
+  const int ne = min(HSS_PTS, tn - e0);
+  const int nt = a.ntri[li];
+  double* out = store + a.base[li];
+  Quad12 Q;
+  quad12(Q);
+  for (int q = threadIdx.x; q < ne * nt; q += blockDim.x) {
+    const int e = e0 + q / nt, t = q % nt;
+    // triangle of near position t: the concatenated ranges of the paired boxes
+    int tri = -1, pos = 0;
+    for (int b = a.nb_start[li]; b < a.nb_start[li + 1]; b++) {
+      const int sb = a.nb_items[b], cnt = a.box_src_count[sb];
+      if (t < pos + cnt) {
+        tri = a.box_src_start[sb] + (t - pos);
+        break;
+      }
+      pos += cnt;
+    }
+    if (tri < 0) continue;
+    const double* xb = a.tgt + 3 * (size_t)(t0 + e);
+    const double X[3] = {xb[0], xb[1], -xb[2]};
+    double acc[54];
+    for (int k = 0; k < 54; k++) acc[k] = 0.0;
+    hs_pair_blk(a.tri + 9 * (size_t)tri, a.nrm + 3 * (size_t)tri, X, a.dosl, a.dodl, a.lam, a.mu, Q, acc);
+    double* o = out + ((size_t)e * nt + t) * a.K;
+    int w = 0;
+    for (int layer = 0; layer < 2; layer++) {
+      if ((layer == 0 && !a.dosl) || (layer == 1 && !a.dodl)) continue;
+      for (int c = 0; c < 3; c++) {
+        const double* blk = acc + 27 * layer + 9 * c;
+        o[w] = blk[0]; o[w + 1] = blk[1]; o[w + 2] = blk[2];
+        w += 3;
+        if (a.dstr) {
+          for (int k = 0; k < 6; k++) o[w + k] = blk[3 + k];
+          w += 6;
+        }
+      }
+    }
+  }
+}
+
+void launch_hs_store(cudaStream_t st, const HsStoreArgs& a, int nchunk, const int* chunk_leaf,
+                     const int* chunk_e0, double* store) {
+  if (nchunk <= 0) return;
+  k_hs_store<<<nchunk, 128, 0, st>>>(a, chunk_leaf, chunk_e0, store);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
 }
 
 void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nrm, const double* ssl,

@@ -16,4 +16,24 @@ void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nr
                      const double* sdl, int m, const double* tgt, double lam, double mu, HsTri* work, double* u,
                      double* e6);
 
+// Near field of the image FMM: the unit-density image responses of every
+// (target, near triangle) pair of each near leaf, written in the stored
+// near-field layout (per leaf at base[leaf]: [target][near triangle][K],
+// K = layers x 3 directions x (3 displacement + 6 strain if dstr)), so that
+// the batched replay contracts them with any number of right-hand sides.
+// Targets are the reflected points (x1, x2, -x3) in tree order; triangles,
+// normals tree order.
+struct HsStoreArgs {
+  const int *leaves, *nb_start, *nb_items;
+  const int *box_src_start, *box_src_count, *box_tgt_start, *box_tgt_count;
+  const double *tri, *nrm, *tgt;
+  const long long* base;
+  const int* ntri;
+  int dosl, dodl, dstr, K;
+  double lam, mu;
+};
+// One CTA per chunk of (near leaf, first of 8 targets).
+void launch_hs_store(cudaStream_t st, const HsStoreArgs& a, int nchunk, const int* chunk_leaf,
+                     const int* chunk_e0, double* store);
+
 }  // namespace efmm

@@ -80,6 +80,61 @@ EFMM_HD void irregular_harmonics(int N, double x, double y, double z, cplx* T) {
   }
 }
 
+// Harmonic table of the half-space kernel U(x) = z log(r + z) - r (z > 0 or
+// off the negative z axis), the function whose derivatives give the B piece
+// of Mindlin's image solution (src/mindlinpieces.f:29).  With the operators
+// that make the irregular harmonics, T_n^m = (-d_z)^{n-m} (d_x + i d_y)^m (1/r),
+// J_n^m = (-d_z)^{n-m} (d_x + i d_y)^m U.  Because d_z^2 U = 1/r,
+// J_n^m = T_{n-2}^m for n - m >= 2; the two outer diagonals are
+//   J_m^m     = (d_x + i d_y)^m U                = w^m G^m U,
+//   J_{m+1}^m = -(d_x + i d_y)^m log(r + z)      = -w^m G^m log(r + z),
+// w = x + iy, G = (1/r) d/dr at fixed z (radial functions only), with
+// G U = -1/(r+z), G log(r+z) = 1/(r (r+z)) and G(r^-a (r+z)^-b) =
+// -a r^-(a+2) (r+z)^-b - b r^-(a+1) (r+z)^-(b+1): positive coefficients
+// with one overall sign, so the sums do not cancel.  Replacing T by J in
+// the M2L coefficients gives the M2L operator of U.  0 <= m <= n <= N <= UH_MAX.
+constexpr int UH_MAX = 120;
+EFMM_HD void u_harmonics(int N, double x, double y, double z, cplx* J) {
+  if (N >= 2) irregular_harmonics(N - 2, x, y, z, J);  // T_{n}^m into slot of n for now
+  // shift the irregular table up by two degrees (n from N-2 down to 0)
+  for (int n = N; n >= 2; n--)
+    for (int m = 0; m <= n - 2; m++) J[cidx(n, m)] = J[cidx(n - 2, m)];
+  const double r = sqrt(x * x + y * y + z * z);
+  const double u = 1.0 / r, rho = r / (r + z);  // rho = v / u, v = 1/(r+z)
+  // g_M = u^{2M-1} sum_b c_b rho^b (b = 1..M);  h_M = u^{2M} sum_b d_b rho^b
+  double c[UH_MAX + 2], d[UH_MAX + 2];
+  for (int b = 0; b <= N + 1 && b < UH_MAX + 2; b++) c[b] = d[b] = 0.0;
+  c[1] = -1.0;
+  d[1] = 1.0;
+  cplx wm = {1.0, 0.0};
+  const cplx w = {x, y};
+  for (int M = 0; M <= N; M++) {
+    double gM, hM;
+    if (M == 0) {
+      gM = z * log(r + z) - r;
+      hM = log(r + z);
+    } else {
+      double sg = 0.0, sh = 0.0, rp = 1.0;
+      for (int b = 1; b <= M; b++) {
+        rp *= rho;
+        sg += c[b] * rp;
+        sh += d[b] * rp;
+      }
+      gM = sg * pow(u, 2 * M - 1);
+      hM = sh * pow(u, 2 * M);
+      // advance: c'_b = -(2M-1-b) c_b - (b-1) c_{b-1};  d'_b = -(2M-b) d_b - (b-1) d_{b-1}
+      for (int b = M + 1; b >= 1; b--) {
+        const double cb = b <= M ? c[b] : 0.0, db = b <= M ? d[b] : 0.0;
+        c[b] = -(2.0 * M - 1.0 - b) * cb - (b - 1.0) * c[b - 1];
+        d[b] = -(2.0 * M - b) * db - (b - 1.0) * d[b - 1];
+      }
+    }
+    J[cidx(M, M)] = cscale(gM, wm);
+    if (M + 1 <= N) J[cidx(M + 1, M)] = cscale(-hM, wm);
+    wm = cmul(wm, w);
+  }
+}
+
 // Access with negative orders through X_n^{-m} = (-1)^m conj(X_n^m).
 EFMM_HD cplx hget(const cplx* X, int n, int m) {
   if (n < 0 || m > n || -m > n) return {0.0, 0.0};

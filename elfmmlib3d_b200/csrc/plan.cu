@@ -9,6 +9,7 @@
 #include <chrono>
 #include <cmath>
 #include "plan.h"
+#include "halfspace.h"
 
 namespace efmm {
 
@@ -286,6 +287,8 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
     return (float)std::chrono::duration<double, std::milli>(b - a).count();
   };
   auto t0 = now();
+  mindlin_ = mindlin;
+  img_sched_ = false;
   int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_);
   if (ier) return ier;
   auto t1 = now();
@@ -510,11 +513,11 @@ void Plan::build_worklists() {
   EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
 }
 
-void Plan::cut_tasks(TransSched& S, int C) {
+void Plan::cut_tasks(TransSched& S, int C, const std::vector<int>* dimsp) {
   if (S.C == C) return;
   std::vector<TransTask> tasks;
   S.lev_tasks.clear();
-  const std::vector<int>& dims = ops_->dims;
+  const std::vector<int>& dims = dimsp ? *dimsp : ops_->dims;
   for (auto& r : S.lev) {
     int t0 = (int)tasks.size();
     for (int q = r.first; q < r.first + r.second; q++) {
@@ -1174,6 +1177,476 @@ int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const do
   EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
   cudaEventElapsedTime(&timings.near, ev_[0], ev_[1]);
   timings.total = timings.near;
+  return IER_OK;
+}
+
+// ------------------------------------------------------ half-space image
+// The image part of the half-space layer potentials (src/elhfmm3dtria_iter.f:
+// 544-840 composes it from an anti-image elastic FMM, a Mindlin B/C FMM and
+// an image near field).  Here one plan on (sources, reflected targets) runs
+// all of it: per right-hand side seven expansion columns, the four
+// anti-image passes (free-space passes with c1 = 2 - alpha and the
+// double-layer charge constant (2 lam + 3 mu)/(lam + 2 mu)), the 1/r
+// potentials Phi_a and Phi_c of the C piece, and the potential W of
+// U = R3 log(R + R3) - R for the B piece, whose M2L uses its own dense
+// operators (kind 3).  The image sources lie below z = 0 and the reflected
+// targets above it, so every M2L pair has a target box at or above its
+// source box, where U is regular.
+
+// M2L pairs of the image plan: target boxes holding targets only, sources
+// below or level with them; ukind selects the U operators (alpha = box side,
+// U grows like r) instead of the Laplace ones (alpha = 1 / box side).
+__global__ void k_m2l_pairs_img(int nb, int pass, int ukind, const int* __restrict__ level,
+                                const int* __restrict__ ijk, const int* __restrict__ scount,
+                                const int* __restrict__ tcount, const int* __restrict__ l2s,
+                                const int* __restrict__ l2i, const int* __restrict__ grp, double size,
+                                int* __restrict__ cnt, int* __restrict__ cursor, TransPair* __restrict__ out,
+                                int* __restrict__ bad) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= nb) return;
+  if (level[b] < 2 || tcount[b] == 0) return;
+  const double s = size / (double)(1ull << level[b]);
+  for (int q = l2s[b]; q < l2s[b + 1]; q++) {
+    const int sb = l2i[q];
+    if (scount[sb] == 0) continue;
+    const int di = ijk[3 * b] - ijk[3 * sb], dj = ijk[3 * b + 1] - ijk[3 * sb + 1],
+              dk = ijk[3 * b + 2] - ijk[3 * sb + 2];
+    if (di < -3 || di > 3 || dj < -3 || dj > 3 || dk < -3 || dk > 3) continue;
+    if (dk < 0) {  // a source box above a target box: not a half-space configuration
+      if (pass == 0) atomicAdd(bad, 1);
+      continue;
+    }
+    const int g = grp[(di + 3) * 49 + (dj + 3) * 7 + (dk + 3)];
+    if (g < 0) continue;
+    if (pass == 0) {
+      atomicAdd(&cnt[g], 1);
+    } else {
+      const int pos = atomicAdd(&cursor[g], 1);
+      out[pos] = TransPair{sb, b, ukind ? s : 1.0 / s};
+    }
+  }
+}
+
+void Plan::ensure_uops() {
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  OpPool* P = ops_;
+  if (P->u_ready) return;
+  std::vector<OpDesc> descs;
+  long long off = 0;
+  for (int q = 0; q < 343; q++) P->m2lu_group[q] = -1;
+  P->udims.clear();
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = 0; k <= 3; k++) {
+        const int mx = std::max(abs(i), std::max(abs(j), abs(k)));
+        if (mx < 2) continue;
+        OpDesc d;
+        d.kind = 3;
+        d.p = std::min(p_, m2l_order(eps_, i, j, k));
+        d.d[0] = i; d.d[1] = j; d.d[2] = k;
+        d.off = off;
+        const int dim = 2 * ncoef(d.p);
+        off += (long long)dim * dim;
+        P->m2lu_group[(i + 3) * 49 + (j + 3) * 7 + (k + 3)] = (int)descs.size();
+        P->udims.push_back(dim);
+        descs.push_back(d);
+      }
+  P->umats.resize(off);
+  DevBuf<OpDesc> dd;
+  dd.resize(descs.size());
+  EFMM_CUDA_TRY(cudaMemcpyAsync(dd.get(), descs.data(), descs.size() * sizeof(OpDesc), cudaMemcpyHostToDevice,
+                                st_));
+  launch_build_ops(st_, (int)descs.size(), dd.get(), P->umats.get(), p_);
+  std::vector<long long> offs;
+  std::vector<int> kinds;
+  for (auto& d : descs) {
+    offs.push_back(d.off);
+    kinds.push_back(3);
+  }
+  h2d(P->uoff, offs, st_);
+  h2d(P->udim, P->udims, st_);
+  h2d(P->ukinds, kinds, st_);
+  std::vector<int> g(P->m2lu_group, P->m2lu_group + 343);
+  h2d(P->m2lug_dev, g, st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  P->u_ready = true;
+}
+
+void Plan::ensure_mats_f() {
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  if (ops_->mats_f.size() != ops_->mats.size()) {
+    ops_->mats_f.resize(ops_->mats.size());
+    k_ops_normalised<<<(int)ops_->dims.size(), 256, 0, st_>>>(ops_->kinds.get(), ops_->off.get(), ops_->dim.get(),
+                                                              ops_->wnorm.get(), ops_->mats.get(),
+                                                              ops_->mats_f.get());
+    count_launch();
+  }
+  if (ops_->u_ready && ops_->umats_f.size() != ops_->umats.size()) {
+    ops_->umats_f.resize(ops_->umats.size());
+    k_ops_normalised<<<(int)ops_->udims.size(), 256, 0, st_>>>(ops_->ukinds.get(), ops_->uoff.get(),
+                                                               ops_->udim.get(), ops_->wnorm.get(),
+                                                               ops_->umats.get(), ops_->umats_f.get());
+    count_launch();
+  }
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+}
+
+int Plan::build_image_sched() {
+  const int nb = tr_.nboxes;
+  const int gb = (nb + 255) / 256;
+  DevBuf<int> bad;
+  bad.resize(1);
+  bad.zero(st_);
+  for (int uk = 0; uk < 2; uk++) {
+    TransSched& S = uk ? m2lu_ : m2lv_img_;
+    const int* grp = uk ? ops_->m2lug_dev.get() : ops_->m2lg_dev.get();
+    S.clear();
+    DevBuf<int>& cnt = m2l_cnt_;
+    cnt.resize(344);
+    cnt.zero(st_);
+    k_m2l_pairs_img<<<gb, 256, 0, st_>>>(nb, 0, uk, tr_.level.get(), tr_.ijk.get(), tr_.scount.get(),
+                                         tr_.tcount.get(), tr_.l2_start.get(), tr_.l2_items.get(), grp, tr_.size,
+                                         cnt.get(), nullptr, nullptr, bad.get());
+    count_launch();
+    std::vector<int> hc = d2h(cnt, 343, st_);
+    std::vector<int> start(344, 0);
+    for (int g = 0; g < 343; g++) start[g + 1] = start[g] + hc[g];
+    const int tot = start[343];
+    for (int g = 0; g < 343; g++)
+      if (hc[g] > 0) S.segs.push_back({g, start[g], hc[g]});
+    S.lev.push_back({0, (int)S.segs.size()});
+    h2d(m2l_cursor_, start, st_);
+    S.pairs.resize(std::max(tot, 1));
+    k_m2l_pairs_img<<<gb, 256, 0, st_>>>(nb, 1, uk, tr_.level.get(), tr_.ijk.get(), tr_.scount.get(),
+                                         tr_.tcount.get(), tr_.l2_start.get(), tr_.l2_items.get(), grp, tr_.size,
+                                         nullptr, m2l_cursor_.get(), S.pairs.get(), bad.get());
+    count_launch();
+  }
+  std::vector<int> hb = d2h(bad, 1, st_);
+  if (hb[0] != 0) return IER_BADARG;
+  img_sched_ = true;
+  return IER_OK;
+}
+
+template <class T>
+void Plan::run_dense(TransSched& S, int C, const T* mats, const T* src, T* dst) {
+  const int D = 2 * ncoef(p_);
+  cut_tasks(S, C, &ops_->udims);
+  for (auto& r : S.lev_tasks)
+    launch_translate<T>(st_, r.second, S.tasks.get() + r.first, S.pairs.get(), mats, ops_->uoff.get(),
+                        ops_->udim.get(), D, C, src, dst);
+}
+
+void Plan::build_chunks(int do_src, int do_tgt) {
+  const int key = do_src | (do_tgt << 1);
+  if (chunk_key_ == key) return;
+  std::vector<int> cl, ce;
+  for (size_t i = 0; i < near_sc_h_.size(); i++) {
+    int nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+    for (int e0 = 0; e0 < nep; e0 += 8) {
+      cl.push_back((int)i);
+      ce.push_back(e0);
+    }
+  }
+  h2d(chunk_leaf_, cl, st_);
+  h2d(chunk_e0_, ce, st_);
+  nchunk_ = (int)cl.size();
+  chunk_key_ = key;
+}
+
+// Two-stage P2M of the image columns over waves of leaves (budget as in
+// p2m_twostage): 9 feature rows per node, 7R columns (6R Laplace, R of U).
+template <class T>
+void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
+  const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R;
+  const size_t nb = tr_.nboxes;
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  const size_t budget_bytes = std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double));
+  const size_t budget = budget_bytes / sizeof(T);
+  size_t i = 0;
+  const size_t nl = p2m_h_.size();
+  while (i < nl) {
+    std::vector<int> wl;
+    std::vector<long long> fo, wo, no;
+    std::vector<GemmTask> tasks;
+    long long nodes = 0, used = 0;
+    int max_nodes = 0;
+    while (i < nl) {
+      const long long K = 108LL * p2m_sc_h_[i];
+      const long long need = K * D + K * (Cv + Cu);
+      if (!wl.empty() && used + need > (long long)budget) break;
+      wl.push_back((int)i);
+      fo.push_back(used);
+      wo.push_back(used + K * D);
+      no.push_back(nodes);
+      nodes += 12LL * p2m_sc_h_[i];
+      const long long box = p2m_h_[i];
+      for (int c0 = 0; c0 < Cv; c0 += 128)
+        for (int r0 = 0; r0 < D; r0 += 128)
+          tasks.push_back({used, used + K * D, box * Cv * D, D, Cv, (int)K, D, (int)K, D, r0, c0});
+      for (int c0 = 0; c0 < Cu; c0 += 128)
+        for (int r0 = 0; r0 < D; r0 += 128)
+          tasks.push_back({used, used + K * D + (long long)Cv * K, (long long)(nb * Cv * D) + box * Cu * D, D, Cu,
+                           (int)K, D, (int)K, D, r0, c0});
+      used += need;
+      max_nodes = std::max(max_nodes, 12 * p2m_sc_h_[i]);
+      i++;
+    }
+    p2m_scratch_.resize(((size_t)used * sizeof(T) + sizeof(double) - 1) / sizeof(double));
+    h2d(wave_leaves_, wl, st_);
+    h2d(wave_foff_, fo, st_);
+    h2d(wave_woff_, wo, st_);
+    h2d(wave_tasks_, tasks, st_);
+    h2d(wave_noff_, no, st_);
+    wave_nrec_.resize(8 * (size_t)std::max(nodes, 1LL));
+    T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
+    launch_p2m_img_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
+                               wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
+                               wave_tasks_.get(), mpole);
+  }
+}
+
+// Two-stage L2T of the image columns at the targets (waves as in l2t_twostage).
+void Plan::l2t_img_twostage(const L2TArgs& la, int R, const double* local) {
+  const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R, C = Cv + Cu;
+  const size_t nb = tr_.nboxes;
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / 8;
+  size_t i = 0;
+  const size_t nl = l2t_h_.size();
+  while (i < nl) {
+    std::vector<int> wl;
+    std::vector<long long> go, so;
+    std::vector<GemmTask> tasks;
+    long long used = 0;
+    int max_pts = 0;
+    while (i < nl) {
+      const int P = l2t_tc_h_[i];
+      if (P == 0) {
+        i++;
+        continue;
+      }
+      const int LD = 9 * P + ((9 * P) & 1);
+      const long long need = (long long)D * LD + (long long)C * LD;
+      if (!wl.empty() && used + need > (long long)budget) break;
+      wl.push_back((int)i);
+      go.push_back(used);
+      so.push_back(used + (long long)D * LD);
+      const long long box = l2t_h_[i];
+      for (int c0 = 0; c0 < Cv; c0 += 128)
+        for (int r0 = 0; r0 < 9 * P; r0 += 128)
+          tasks.push_back({used, box * Cv * D, used + (long long)D * LD, 9 * P, Cv, D, LD, D, LD, r0, c0});
+      for (int c0 = 0; c0 < Cu; c0 += 128)
+        for (int r0 = 0; r0 < 9 * P; r0 += 128)
+          tasks.push_back({used, (long long)(nb * Cv * D) + box * Cu * D, used + (long long)D * LD + (long long)Cv * LD,
+                           9 * P, Cu, D, LD, D, LD, r0, c0});
+      used += need;
+      max_pts = std::max(max_pts, P);
+      i++;
+    }
+    if (wl.empty()) break;
+    l2t_scratch_.resize((size_t)used);
+    h2d(wave_leaves_, wl, st_);
+    h2d(wave_foff_, go, st_);
+    h2d(wave_woff_, so, st_);
+    h2d(wave_tasks_, tasks, st_);
+    launch_l2t_twostage(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(), max_pts,
+                        l2t_scratch_.get(), l2t_scratch_.get(), (int)tasks.size(), wave_tasks_.get(), local, true);
+  }
+}
+
+int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                         double* d_u_tgt, double* d_e_tgt, int precision, int mode) {
+  if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
+  if (!mindlin_ || rmu <= 0 || rlam + 2 * rmu <= 0) return IER_BADARG;
+  const int nt = nt_;
+  if (nt == 0 || !(d_u_tgt || d_e_tgt)) return IER_OK;
+  if (!(d_ssl || d_sdl)) {
+    if (d_u_tgt) EFMM_CUDA_TRY(cudaMemsetAsync(d_u_tgt, 0, 24 * (size_t)nt * R, st_));
+    if (d_e_tgt) EFMM_CUDA_TRY(cudaMemsetAsync(d_e_tgt, 0, 72 * (size_t)nt * R, st_));
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+    return IER_OK;
+  }
+  const int flags = (d_ssl ? 1 : 0) | (d_sdl ? 2 : 0) | 8 | (d_e_tgt ? 16 : 0) | 32;
+  if (mode == 2 && (!store_valid_ || flags != store_flags_ || rlam != store_lam_ || rmu != store_mu_))
+    return IER_HANDLE;
+  if (mode != 2) {
+    const int ier = store_alloc(flags, rlam, rmu);
+    if (ier) return ier;
+  }
+  if (far_) {
+    ensure_uops();
+    if (!img_sched_) {
+      const int ier = build_image_sched();
+      if (ier) return ier;
+    }
+    if (precision == 1) ensure_mats_f();
+  }
+  const int n = n_, D = 2 * ncoef(p_);
+  const size_t nb = tr_.nboxes;
+  int Rc = std::min(R, 64);
+  if (far_) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const double have = 0.5 * (double)freeb + 8.0 * (double)(img_mp_.cap + img_lc_.cap);
+    while (Rc > 1 && 3.0 * 8.0 * nb * 7 * Rc * D > have) Rc /= 2;
+  }
+  float tot = 0;
+  for (int r0 = 0; r0 < R; r0 += Rc) {
+    const int rc = std::min(Rc, R - r0);
+    const int ier = image_pass(rlam, rmu, rc, d_ssl ? d_ssl + 3 * (size_t)n * r0 : nullptr,
+                               d_sdl ? d_sdl + 3 * (size_t)n * r0 : nullptr,
+                               d_u_tgt ? d_u_tgt + 3 * (size_t)nt * r0 : nullptr,
+                               d_e_tgt ? d_e_tgt + 9 * (size_t)nt * r0 : nullptr, precision == 1,
+                               mode != 2 && r0 == 0);
+    if (ier) return ier;
+    tot += timings.total;
+  }
+  timings.total = tot;
+  if (mode == 0) store_valid_ = false;  // the blocks served this call only
+  return IER_OK;
+}
+
+int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl, double* d_u_tgt,
+                     double* d_e_tgt, bool mixed, bool store_now) {
+  const int n = n_, nt = nt_;
+  const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+  const int dstr = d_e_tgt ? 1 : 0;
+  const int D = 2 * ncoef(p_);
+  const size_t nb = tr_.nboxes;
+  long long launch0 = launches_total();
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  ssl_s_.resize(3 * (size_t)n * R);
+  sdl_s_.resize(3 * (size_t)n * R);
+  const int gb = (int)(((long long)n * R + 255) / 256);
+  if (dosl) { k_gather_rhs<<<gb, 256, 0, st_>>>(n, R, tr_.iz.get(), d_ssl, ssl_s_.get()); count_launch(); }
+  if (dodl) { k_gather_rhs<<<gb, 256, 0, st_>>>(n, R, tr_.iz.get(), d_sdl, sdl_s_.get()); count_launch(); }
+  ut_s_.resize(3 * (size_t)nt * R);
+  et_s_.resize(6 * (size_t)nt * R);
+  ut_s_.zero(st_);
+  et_s_.zero(st_);
+  const double al = (rlam + rmu) / (rlam + 2 * rmu);
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  const int Cv = 6 * R, Cu = R;
+  if (far_) {
+    const size_t tot = nb * (size_t)(Cv + Cu) * D;
+    P2MArgs pa;
+    pa.leaves = p2m_leaves_.get();
+    pa.level = tr_.level.get(); pa.ijk = tr_.ijk.get();
+    pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
+    for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
+    pa.size = tr_.size;
+    pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
+    pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
+    // anti-image: Kelvin kernel with c1 = 2 - alpha, double-layer charge constant (2 lam + 3 mu)/(lam + 2 mu)
+    pa.c1 = 2.0 - al; pa.c2 = (2 * rlam + 3 * rmu) / (rlam + 2 * rmu); pa.inv2mu = 0.5 / rmu;
+    pa.alpha = al; pa.lam = rlam; pa.mu = rmu;
+    pa.C = Cv + Cu; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
+    if (mixed) {
+      img_mp_f_.resize(tot);
+      img_lc_f_.resize(tot);
+      img_mp_f_.zero(st_);
+      img_lc_f_.zero(st_);
+      float* mp = img_mp_f_.get();
+      float* lc = img_lc_f_.get();
+      pa.wnorm = ops_->wnorm.get();
+      p2m_img_twostage<float>(pa, R, mp);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      run_translations(m2m_, Cv, ops_->mats_f.get(), mp, mp);
+      run_translations(m2m_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      run_translations(m2lv_img_, Cv, ops_->mats_f.get(), mp, lc);
+      run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      run_translations(l2l_, Cv, ops_->mats_f.get(), lc, lc);
+      run_translations(l2l_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
+      img_lc_.resize(tot);
+      k_f2d_local<<<1184, 256, 0, st_>>>(tot, D, ops_->wnorm.get(), lc, img_lc_.get());
+      count_launch();
+    } else {
+      img_mp_.resize(tot);
+      img_lc_.resize(tot);
+      img_mp_.zero(st_);
+      img_lc_.zero(st_);
+      double* mp = img_mp_.get();
+      double* lc = img_lc_.get();
+      p2m_img_twostage<double>(pa, R, mp);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      run_translations(m2m_, Cv, ops_->mats.get(), mp, mp);
+      run_translations(m2m_, Cu, ops_->mats.get(), mp + nb * Cv * D, mp + nb * Cv * D);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      run_translations(m2lv_img_, Cv, ops_->mats.get(), mp, lc);
+      run_dense(m2lu_, Cu, ops_->umats.get(), mp + nb * Cv * D, lc + nb * Cv * D);
+      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      run_translations(l2l_, Cv, ops_->mats.get(), lc, lc);
+      run_translations(l2l_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
+    }
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
+    L2TArgs la;
+    la.leaves = l2t_leaves_.get();
+    la.level = tr_.level.get(); la.ijk = tr_.ijk.get();
+    la.sstart = tr_.sstart.get(); la.scount = tr_.scount.get();
+    la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
+    for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
+    la.size = tr_.size;
+    la.local = img_lc_.get();
+    la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
+    la.p = p_; la.do_src = 0; la.do_tgt = 1;
+    la.dostrain_src = 0; la.dostrain_tgt = dstr;
+    la.c1 = 2.0 - al; la.alpha = al; la.mu = rmu;
+    la.u_src = nullptr; la.e_src = nullptr; la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
+    la.C = Cv + Cu; la.nsrc = n; la.ntgt = nt;
+    l2t_img_twostage(la, R, img_lc_.get());
+  } else {
+    for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
+  // near field: refined quadrature of the whole image kernel, stored, then
+  // contracted with the right-hand sides
+  build_chunks(0, 1);
+  if (store_now) {
+    HsStoreArgs ha;
+    ha.leaves = near_leaves_.get(); ha.nb_start = near_start_.get(); ha.nb_items = near_items_.get();
+    ha.box_src_start = tr_.sstart.get(); ha.box_src_count = tr_.scount.get();
+    ha.box_tgt_start = tr_.tstart.get(); ha.box_tgt_count = tr_.tcount.get();
+    ha.tri = tri_s_.get(); ha.nrm = nrm_s_.get(); ha.tgt = tgt_s_.get();
+    ha.base = near_base_.get(); ha.ntri = near_ntri_.get();
+    ha.dosl = dosl; ha.dodl = dodl; ha.dstr = dstr; ha.K = store_K_;
+    ha.lam = rlam; ha.mu = rmu;
+    launch_hs_store(st_, ha, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), store_.get());
+    store_valid_ = true;
+  }
+  NearArgs na;
+  na.nleaf = nnear_;
+  na.leaves = near_leaves_.get(); na.nb_start = near_start_.get(); na.nb_items = near_items_.get();
+  na.box_src_start = tr_.sstart.get(); na.box_src_count = tr_.scount.get();
+  na.box_tgt_start = tr_.tstart.get(); na.box_tgt_count = tr_.tcount.get();
+  na.trir = trir_.get();
+  na.src_pts = src_s_.get(); na.tgt_pts = tgt_s_.get();
+  na.dosl = dosl; na.dodl = dodl; na.dostrain_src = 0; na.dostrain_tgt = dstr;
+  na.do_src = 0; na.do_tgt = 1;
+  na.rlam = rlam; na.rmu = rmu;
+  na.u_src = nullptr; na.e_src = nullptr; na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
+  launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, dstr, ssl_s_.get(), sdl_s_.get(), n, n,
+                    nt, near_base_.get(), near_ntri_.get(), store_.get());
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
+  k_scatter_out<<<dim3((nt + 255) / 256, R), 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(), d_u_tgt,
+                                                             d_e_tgt);
+  count_launch();
+  EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+  EFMM_CUDA_TRY(cudaGetLastError());
+  EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
+  cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
+  cudaEventElapsedTime(&timings.prep, ev_[0], ev_[1]);
+  cudaEventElapsedTime(&timings.p2m, ev_[1], ev_[2]);
+  cudaEventElapsedTime(&timings.m2m, ev_[2], ev_[3]);
+  cudaEventElapsedTime(&timings.m2l, ev_[3], ev_[4]);
+  cudaEventElapsedTime(&timings.l2l, ev_[4], ev_[5]);
+  cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
+  cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
+  launches_ = (int)(launches_total() - launch0);
   return IER_OK;
 }
 

@@ -39,6 +39,16 @@ struct OpPool {
   int m2l_group[343];
   int m2m_group[8], l2l_group[8];
   std::vector<int> dims;
+  // M2L operators of the half-space kernel U (kind 3), offsets with a
+  // non-negative z component only (targets above the image sources); made
+  // on first use, dense
+  bool u_ready = false;
+  DevBuf<double> umats;
+  DevBuf<float> umats_f;
+  DevBuf<long long> uoff;
+  DevBuf<int> udim, ukinds, m2lug_dev;
+  std::vector<int> udims;
+  int m2lu_group[343];
 };
 
 struct Timings {  // milliseconds of the last evaluate(), CUDA events
@@ -104,6 +114,18 @@ class Plan {
   int evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                      double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt,
                      int precision = 0, int mode = 0);
+  // Half-space image part (Mindlin) of the layer potentials on triangles in
+  // z <= 0, at the original targets x (R, nt, 3) / (R, nt, 3, 3), user
+  // order.  The plan's geometry must have been set with mindlin = true and
+  // the REFLECTED targets (x1, x2, -x3) as its targets.  Far field: the
+  // anti-image passes and the two 1/r potentials of the C piece through the
+  // Laplace translations, the U potential of the B piece through its own
+  // dense M2L (kind 3); near field: refined quadrature of the whole image
+  // kernel over the near lists, stored and contracted with all right-hand
+  // sides.  precision and mode as in evaluate_batch (mode 0 computes the
+  // near-field blocks for this call only).
+  int evaluate_image(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                     double* d_u_tgt, double* d_e_tgt, int precision = 0, int mode = 0);
   // useful flops per expansion column of one pass: P2M, M2M, M2L, L2L, L2T
   void flops_per_column(double* f5) const;
   // all-pairs direct sum on the same geometry (no tree needed)
@@ -127,6 +149,21 @@ class Plan {
   int batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                  double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, bool mixed, int mode);
   int store_alloc(int flags, double rlam, double rmu);
+  int image_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl, double* d_u_tgt,
+                 double* d_e_tgt, bool mixed, bool store_now);
+  void ensure_uops();
+  void ensure_mats_f();
+  int build_image_sched();
+  void build_chunks(int do_src, int do_tgt);
+  bool mindlin_ = false, img_sched_ = false;
+  TransSched m2lv_img_, m2lu_;
+  template <class T>
+  void p2m_img_twostage(const P2MArgs& pa, int R, T* mpole);
+  void l2t_img_twostage(const L2TArgs& la, int R, const double* local);
+  template <class T>
+  void run_dense(TransSched& S, int C, const T* mats, const T* src, T* dst);
+  DevBuf<double> img_mp_, img_lc_;
+  DevBuf<float> img_mp_f_, img_lc_f_;
   DevBuf<float> mpole_f_, local_f_;
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA
   int nchunk_ = 0, chunk_key_ = -1;
@@ -165,7 +202,7 @@ class Plan {
   double store_lam_ = 0, store_mu_ = 0;
   long long near_pairs_ = 0;
   TransSched m2m_, m2l_, l2l_;
-  void cut_tasks(TransSched& S, int C);
+  void cut_tasks(TransSched& S, int C, const std::vector<int>* dims = nullptr);
   void cut_rot_tasks(TransSched& S, int C, int W);
   void ensure_factored();
   bool factored_ = true;  // translations in factored form when they fit

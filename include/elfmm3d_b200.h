@@ -186,6 +186,25 @@ int efmm_plan_evaluate_batch_iter(efmm_plan *plan, double rlam, double rmu, int 
                                   const double *sdl, double *u_src, double *e_src, double *u_tgt,
                                   double *e_tgt, int precision, int mode);
 
+/* Half-space image part as an FMM (replaces the direct image sum of
+ * elhfmm3dtriatargiter, src/elhfmm3dtria_iter.f:544-840: anti-image elastic
+ * FMM, Mindlin B/C FMM, image near field).  The plan's geometry must have
+ * been set with mindlin != 0 and, as targets, the reflections (x1, x2, -x3)
+ * of the points x (z <= 0) where the field is wanted; sources in z <= 0.
+ * ssl/sdl (nrhs,n,3) device, NULL disables a layer; outputs at the points
+ * x: u_tgt (nrhs,nt,3), e_tgt (nrhs,nt,3,3).  precision 0 FP64, 1 mixed
+ * (FP32 expansions and translations); mode 0 plain, 1 store the image
+ * near-field blocks and use them, 2 reuse them (512 on mismatch). */
+int efmm_plan_evaluate_image(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
+                             const double *sdl, double *u_tgt, double *e_tgt, int precision, int mode);
+
+/* The image part by direct summation over all (target, triangle) pairs with
+ * the refined quadrature of the image near field (host arrays as in
+ * elhfmm3dtriatargiter; u (nt,3), e (nt,3,3), NULL skips an output): the
+ * O(n nt) check of the image FMM. */
+int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, const double *nrm, int n,
+                         const double *ssl, const double *sdl, int nt, const double *tgt, double *u, double *e);
+
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 
