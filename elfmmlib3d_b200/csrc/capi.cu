@@ -6,6 +6,7 @@
 #include <vector>
 #include "plan.h"
 #include "halfspace.h"
+#include "harmonics.cuh"
 #include "../../include/elfmm3d_b200.h"
 
 using namespace efmm;
@@ -685,4 +686,55 @@ extern "C" long long efmm_iter_stored_bytes(const double* wsave, int lwsave) {
   IterSlot* S = iter_find(wsave, lwsave);
   if (!S) return -1;
   return 8 * S->p->plan->stored_doubles();
+}
+
+// Host check of the M2L of the half-space kernel U = z log(r + z) - r built
+// from u_harmonics (the device operators use the same code): nsrc unit-box
+// sources around 0 with random charges, targets in the unit box around the
+// offset X; the local expansion of order p (multipole moments through the J
+// table) against the direct sum of U.  Returns the largest relative error.
+extern "C" double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, unsigned seed) {
+  using namespace efmm;
+  if (p < 1 || p > 54 || nsrc < 1) return -1.0;
+  unsigned long long st = seed * 6364136223846793005ull + 1442695040888963407ull;
+  auto uni = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return ((st >> 11) * (1.0 / 9007199254740992.0)) - 0.5;
+  };
+  const int nc = ncoef(p);
+  std::vector<cplx> Y(nc), M(nc, cplx{0, 0}), L(nc, cplx{0, 0}), J(ncoef(2 * p));
+  std::vector<double> q(nsrc), xs(3 * (size_t)nsrc);
+  for (int i = 0; i < nsrc; i++) {
+    q[i] = 2 * uni();
+    for (int d = 0; d < 3; d++) xs[3 * i + d] = uni();
+    regular_harmonics(p, xs[3 * i], xs[3 * i + 1], xs[3 * i + 2], Y.data());
+    for (int c = 0; c < nc; c++) M[c] = cadd(M[c], cscale(q[i], cconj(Y[c])));
+  }
+  u_harmonics(2 * p, X0, X1, X2, J.data());
+  for (int n = 0; n <= p; n++)
+    for (int m = 0; m <= n; m++) {
+      cplx acc = {0, 0};
+      for (int k = 0; k <= p; k++)
+        for (int l = -k; l <= k; l++) acc = cadd(acc, cmul(m2l_coef(J.data(), n, m, k, l), hget(M.data(), k, l)));
+      L[cidx(n, m)] = acc;
+    }
+  double worst = 0.0;
+  for (int t = 0; t < 8; t++) {
+    const double z[3] = {uni(), uni(), uni()};
+    regular_harmonics(p, z[0], z[1], z[2], Y.data());
+    double val = 0.0;
+    for (int n = 0; n <= p; n++)
+      for (int m = -n; m <= n; m++) {
+        const cplx a = hget(L.data(), n, m), y = cconj(hget(Y.data(), n, m));
+        val += a.re * y.re - a.im * y.im;
+      }
+    double ref = 0.0;
+    for (int i = 0; i < nsrc; i++) {
+      const double r[3] = {X0 + z[0] - xs[3 * i], X1 + z[1] - xs[3 * i + 1], X2 + z[2] - xs[3 * i + 2]};
+      const double rr = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      ref += q[i] * (r[2] * log(rr + r[2]) - rr);
+    }
+    worst = std::max(worst, fabs(val - ref) / fabs(ref));
+  }
+  return worst;
 }

@@ -205,6 +205,12 @@ int efmm_plan_evaluate_image(efmm_plan *plan, double rlam, double rmu, int nrhs,
 int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, const double *nrm, int n,
                          const double *ssl, const double *sdl, int nt, const double *tgt, double *u, double *e);
 
+/* Host check (no GPU) of the image FMM's M2L for the kernel
+ * U = z log(r + z) - r (src/mindlinpieces.f:29): order-p local expansion at
+ * offset X (box units, X2 >= 0) of nsrc random unit-box sources against
+ * their direct sum; returns the largest relative error (-1 on bad input). */
+double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, unsigned seed);
+
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 

@@ -16,3 +16,18 @@ def test_factored_equals_dense(lib, p, eps, stride):
     n = f(p, eps, stride, ctypes.byref(worst))
     assert n == 316 + 16
     assert worst.value < 1e-12
+
+
+def test_u_kernel_m2l_selfcheck(lib):
+    # M2L of the half-space kernel U = z log(r + z) - r through its J table
+    # (the device operators' code, run on the host): errors fall with the
+    # order as for 1/r, at offsets above, level with and far from the sources
+    import ctypes
+    f = lib.load().efmm_u_m2l_selfcheck
+    f.restype = ctypes.c_double
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_uint]
+    for X in [(2.0, 1.0, 1.0), (0.0, 0.0, 2.0), (3.0, -2.0, 0.0), (-1.0, 3.0, 3.0)]:
+        e8 = f(8, *X, 20, 3)
+        e20 = f(20, *X, 20, 3)
+        assert 0 <= e20 < 1e-6 and e20 < e8, (X, e8, e20)
+    assert f(0, 2.0, 0, 0, 5, 1) == -1.0
