@@ -465,20 +465,6 @@ extern "C" int efmm_hs_image_direct(int iprec, double rlam, double rmu, const do
                  u, e != nullptr, e, 1, nullptr);
 }
 
-extern "C" void elhfmm3dtriatargiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
-                                      const double* triangle, const double* trinorm, const int* nparts,
-                                      const double* source, const int* ifsingle, const double* sigma_sl,
-                                      const int* ifdouble, const double* sigma_dl, const int* ntargs,
-                                      const double* target, const int* ifptfrctarg, double* ptfrctarg,
-                                      const int* ifstraintarg, double* straintarg, const int* icomp_type,
-                                      double* wsave, const int* lwsave, int* lused) {
-  (void)source;
-  (void)wsave;
-  (void)lwsave;
-  *ier = hs_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, *ifsingle, sigma_sl, *ifdouble, sigma_dl,
-                 *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, *icomp_type, lused);
-}
-
 // ---------------------------------------------------------------------------
 // ITER entry point (src/elfmm3dtria_iter_1.f:160-165).  The reference keeps
 // the near-field operator in the caller's wsave array.  Here the operator
@@ -666,6 +652,123 @@ extern "C" void elfmm3dtriaiter_(int* ier, const int* iprec, const double* rlam,
   *ier = iter_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
                    sigma_dl, *ifptfrc, ptfrc, *ifstrain, strain, 0, nullptr, 0, nullptr, 0, nullptr,
                    *icomp_type, wsave, *lwsave, lused);
+}
+
+
+// ---------------------------------------------------------------------------
+// Half-space image part (elhfmm3dtriatargiter, src/elhfmm3dtria_iter.f:46-51)
+// through the image FMM (Plan::evaluate_image) on the sources and the
+// reflected targets.  icomp_type 1 evaluates, 2 evaluates and stores the
+// image near-field blocks behind a wsave handle (as elfmm3dtriatargiter),
+// 3 reuses them with new densities on the same geometry, 0 and 4 only return
+// lused, 5 behaves as 2.  Sources and targets must lie in z <= 0.
+// ---------------------------------------------------------------------------
+namespace {
+int hs_fmm_call(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n, const double* src,
+                int ifsingle, const double* ssl, int ifdouble, const double* sdl, int nt, const double* tgt,
+                int ifptfrctarg, double* ptfrctarg, int ifstraintarg, double* straintarg, int icomp,
+                double* wsave, int lwsave, int* lused) {
+  if (lused) *lused = ITER_LUSED;
+  if (n < 1 || nt < 0) return IER_BADARG;
+  if (iprec < -2 || iprec > 6) return IER_BADARG;
+  if (icomp < 0 || icomp > 5) return IER_BADARG;
+  if (icomp == 0 || icomp == 4 || nt == 0 || !(ifptfrctarg || ifstraintarg)) return IER_OK;
+  for (int i = 0; i < 3 * n; i++)
+    if (tri[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < nt; i++)
+    if (tgt[3 * i + 2] > 0.0) return IER_BADARG;
+  const bool storing = (icomp == 2 || icomp == 3 || icomp == 5) && lwsave >= ITER_LUSED && wsave;
+  const int mode = !storing ? 0 : (icomp == 3 ? 2 : 1);
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int flags = iter_flags(ifsingle, ifdouble, 0, 0, nt, ifptfrctarg, ifstraintarg) | 64;
+  const double cks = geometry_checksum(tri, nrm, src, n, tgt, nt);
+  IterSlot* S = nullptr;
+  efmm_plan* p = nullptr;
+  HostCall* B = nullptr;
+  if (mode == 0) {
+    p = shared_plan();
+    if (!p) return IER_NODEVICE;
+    if (!g_bufs) g_bufs = new HostCall();
+    B = g_bufs;
+  } else {
+    S = iter_find(wsave, lwsave);
+    if (mode == 2) {
+      if (!S || S->n != n || S->nt != nt || S->iprec != iprec || S->checksum != cks || S->flags != flags ||
+          wsave[3] != n || wsave[4] != nt || wsave[5] != iprec || wsave[6] != cks || wsave[7] != flags)
+        return IER_HANDLE;
+    } else {
+      S = iter_acquire(S);
+      if (!S) return IER_NODEVICE;
+      S->id = 0;  // invalid until this store completes
+    }
+    S->last_use = ++g_iter_clock;
+    p = S->p;
+    B = &S->bufs;
+  }
+  try {
+    cudaSetDevice(p->device);
+    cudaStream_t st = p->stream;
+    if (mode != 2) {
+      std::vector<double> refl(3 * (size_t)nt);
+      for (int i = 0; i < nt; i++) {
+        refl[3 * i] = tgt[3 * i];
+        refl[3 * i + 1] = tgt[3 * i + 1];
+        refl[3 * i + 2] = -tgt[3 * i + 2];
+      }
+      up(B->tri, tri, 9 * (size_t)n, st);
+      up(B->nrm, nrm, 3 * (size_t)n, st);
+      up(B->src, src, 3 * (size_t)n, st);
+      up(B->tgt, refl.data(), 3 * (size_t)nt, st);
+      const int ier = p->plan->set_geometry(n, B->tri.get(), B->nrm.get(), B->src.get(), nt, B->tgt.get(), iprec,
+                                            true, true);
+      if (ier) return ier;
+    }
+    if (ifsingle) up(B->ssl, ssl, 3 * (size_t)n, st);
+    if (ifdouble) up(B->sdl, sdl, 3 * (size_t)n, st);
+    B->ut.resize(3 * (size_t)nt);
+    B->et.resize(9 * (size_t)nt);
+    const int ier = p->plan->evaluate_image(rlam, rmu, 1, ifsingle ? B->ssl.get() : nullptr,
+                                            ifdouble ? B->sdl.get() : nullptr, B->ut.get(),
+                                            ifstraintarg ? B->et.get() : nullptr, 0, mode);
+    if (ier) return ier;
+    if (ifptfrctarg) down(ptfrctarg, B->ut, 3 * (size_t)nt, st);
+    if (ifstraintarg) down(straintarg, B->et, 9 * (size_t)nt, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (mode == 1) {
+      S->id = g_iter_next_id++;
+      S->n = n;
+      S->nt = nt;
+      S->iprec = iprec;
+      S->checksum = cks;
+      S->flags = flags;
+      wsave[0] = ITER_MAGIC;
+      wsave[1] = ITER_VERSION;
+      wsave[2] = (double)S->id;
+      wsave[3] = n;
+      wsave[4] = nt;
+      wsave[5] = iprec;
+      wsave[6] = cks;
+      wsave[7] = flags;
+    }
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+}  // namespace
+
+extern "C" void elhfmm3dtriatargiter_(int* ier, const int* iprec, const double* rlam, const double* rmu,
+                                      const double* triangle, const double* trinorm, const int* nparts,
+                                      const double* source, const int* ifsingle, const double* sigma_sl,
+                                      const int* ifdouble, const double* sigma_dl, const int* ntargs,
+                                      const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                      const int* ifstraintarg, double* straintarg, const int* icomp_type,
+                                      double* wsave, const int* lwsave, int* lused) {
+  *ier = hs_fmm_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
+                     sigma_dl, *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, *icomp_type,
+                     wsave, *lwsave, lused);
 }
 
 extern "C" int efmm_iter_release(const double* wsave, int lwsave) {

@@ -1,7 +1,8 @@
-"""Half-space image part (elhfmm3dtriatargiter_, direct GPU sum): against the
-oracle's restatement of the reference's image kernels, and end to end
-against the traction-free condition on z = 0 with the free-space direct sum
-as the direct arrival."""
+"""Half-space image part (elhfmm3dtriatargiter_, the image FMM; and the
+direct GPU image sum efmm_hs_image_direct): against the oracle's restatement
+of the reference's image kernels, end to end against the traction-free
+condition on z = 0 with the free-space direct sum as the direct arrival, and
+the ITER store/replay of the image near field."""
 import numpy as np
 import pytest
 
@@ -70,3 +71,43 @@ def test_halfspace_self_and_errors(gpu):
     # icomp 4: nothing evaluated, lused = 8
     ier, lused, u, _ = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, cen, icomp_type=4)
     assert ier == 0 and lused == 8 and not u.any()
+
+
+def test_direct_image_matches_oracle(gpu):
+    from oracle import mindlin as M
+    tri, nrm, cen = _fault(3, 2)
+    rng = np.random.default_rng(12)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    tg = np.vstack([cen, [[0.3, 0.4, 0.0], [2.5, -0.5, -0.05]]])
+    ier, u, e = gpu.hs_image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg)
+    assert ier == 0
+    uo, eo = M.image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg, level=2)
+    assert rel(u, uo) < 5e-8 and rel(e, eo) < 5e-8
+
+
+def test_image_iter_store_and_replay(gpu):
+    # icomp 2 stores the image near-field blocks behind the wsave handle, 3
+    # reuses them with new densities: equal to plain calls; a handle of
+    # another geometry is rejected
+    tri, nrm, cen, _ = G.planar_fault(40, 20)
+    rng = np.random.default_rng(14)
+    sdl = rng.normal(size=cen.shape)
+    w = np.zeros(8)
+    ier, lused, u2, e2 = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, cen, icomp_type=2, wsave=w)
+    assert ier == 0 and lused == 8 and w[0] != 0
+    ier, _, u1, e1 = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, sdl, cen, icomp_type=1)
+    assert ier == 0 and rel(u2, u1) < 1e-12 and rel(e2, e1) < 1e-12
+    assert gpu.iter_stored_bytes(w) > 0
+    s2 = rng.normal(size=cen.shape)
+    ier, _, u3, e3 = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, s2, cen, icomp_type=3, wsave=w)
+    ier1, _, u4, e4 = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, s2, cen, icomp_type=1)
+    assert ier == 0 and ier1 == 0 and rel(u3, u4) < 1e-12 and rel(e3, e4) < 1e-12
+    # against the direct image sum: at iprec 2 (eps 5e-7) the 12-node rule of
+    # the multipole moments on triangles a third of a leaf (the reference's
+    # rule) bounds the double-layer strain at a few 1e-6
+    ier, ud, ed = gpu.hs_image_direct(1.0, 1.0, tri, nrm, None, s2, cen)
+    assert ier == 0 and rel(u3, ud) < 2e-6 and rel(e3, ed) < 5e-6
+    # replay with a different target set: handle mismatch
+    ier, *_ = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, s2, cen[:10], icomp_type=3, wsave=w)
+    assert ier == 512
+    assert gpu.iter_release(w) == 0
