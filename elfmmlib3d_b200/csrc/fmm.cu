@@ -430,7 +430,11 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
     }
   }
   __syncwarp();
-  T* out = F + foff[blockIdx.x] + (size_t)(NF * node) * D;
+  // rows: charge/dipole rows of every node first (4 node + f), then (NF = 9)
+  // the five second-derivative rows (4 nnode + 5 node + f - 4), so that
+  // columns without quadrupole sources multiply the first block only
+  T* out = F + foff[blockIdx.x] + (size_t)(4 * node) * D;
+  T* outq = F + foff[blockIdx.x] + (size_t)(4 * nnode + 5 * node) * D;
   for (int cc = lane; cc < nc; cc += 32) {
     int fn = 0;
     while ((fn + 1) * (fn + 2) / 2 <= cc) fn++;
@@ -466,35 +470,79 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
         ym2 = hget(Y, fn - 2, fm - 2);
       }
       const double q = sr * is * is;
-      out[4 * D + 2 * cc] = (T)(q * 0.25 * (yp2.re - 2.0 * y0.re + ym2.re));
-      out[4 * D + 2 * cc + 1] = (T)(-q * 0.25 * (yp2.im - 2.0 * y0.im + ym2.im));
-      out[5 * D + 2 * cc] = (T)(-q * 0.25 * (yp2.re + 2.0 * y0.re + ym2.re));
-      out[5 * D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.im + 2.0 * y0.im + ym2.im));
-      out[6 * D + 2 * cc] = (T)(q * 0.25 * (yp2.im - ym2.im));
-      out[6 * D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.re - ym2.re));
-      out[7 * D + 2 * cc] = (T)(q * 0.5 * (yp1.re - ym1.re));
-      out[7 * D + 2 * cc + 1] = (T)(-q * 0.5 * (yp1.im - ym1.im));
-      out[8 * D + 2 * cc] = (T)(q * 0.5 * (yp1.im + ym1.im));
-      out[8 * D + 2 * cc + 1] = (T)(q * 0.5 * (yp1.re + ym1.re));
+      outq[2 * cc] = (T)(q * 0.25 * (yp2.re - 2.0 * y0.re + ym2.re));
+      outq[2 * cc + 1] = (T)(-q * 0.25 * (yp2.im - 2.0 * y0.im + ym2.im));
+      outq[D + 2 * cc] = (T)(-q * 0.25 * (yp2.re + 2.0 * y0.re + ym2.re));
+      outq[D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.im + 2.0 * y0.im + ym2.im));
+      outq[2 * D + 2 * cc] = (T)(q * 0.25 * (yp2.im - ym2.im));
+      outq[2 * D + 2 * cc + 1] = (T)(q * 0.25 * (yp2.re - ym2.re));
+      outq[3 * D + 2 * cc] = (T)(q * 0.5 * (yp1.re - ym1.re));
+      outq[3 * D + 2 * cc + 1] = (T)(-q * 0.5 * (yp1.im - ym1.im));
+      outq[4 * D + 2 * cc] = (T)(q * 0.5 * (yp1.im + ym1.im));
+      outq[4 * D + 2 * cc + 1] = (T)(q * 0.5 * (yp1.re + ym1.re));
     }
   }
 }
 
-// Node weights of the half-space image columns, 7R per box: for right-hand
-// side r, columns 6r..6r+5 hold the anti-image passes 0..3 (the free-space
-// passes with the anti-image constants c1, c2 of P2MArgs) and the two 1/r
-// potentials Phi_a, Phi_c of the C piece; column 6R + r holds the U
-// potential W of the B piece.  Per node 9 rows: charge, dipole (3) and the
-// five second-derivative rows (xx - zz, yy - zz, 2xy, 2xz, 2yz of the
+// Node weights of the half-space image columns, 7R per box, column
+// kind * R + r for right-hand side r: kinds 0..3 the anti-image passes (the
+// free-space passes with the anti-image constants c1, c2 of P2MArgs), 4 and 5
+// the two 1/r potentials Phi_a, Phi_c of the C piece, 6 the U potential W of
+// the B piece.  Per node 9 weights: charge, dipole (3) and the five
+// second-derivative weights (xx - zz, yy - zz, 2xy, 2xz, 2yz of the
 // quadrupole tensor).  With f the single-layer density, T the double-layer
 // tensor lam (b.n) I + mu (b n^T + n b^T), h = -y_3 the source depth and
 // alpha = (lam + mu)/(lam + 2 mu) (sources in the gradient-of-source
-// convention of the product features):
+// convention of the features):
 //   Phi_a: q = -(2 - alpha) f_3, D = -h alpha f - (2 - 2 alpha) T e_3, Q = -h alpha T
 //   Phi_c: D = -f, Q = -T
-//   W:     D = (f_1, f_2, -f_3), Q = diag-sign form of -(S T + T S)/2, S = diag(-1,-1,1)
-// (the B and C pieces of src/mindlinpieces.f:29-520 written as Laplace
+//   W:     D = (f_1, f_2, -f_3), Q = -(S T + T S)/2, S = diag(-1, -1, 1)
+// (the B and C pieces of src/mindlinpieces.f:29-520 written as Laplace-type
 // potentials; their double layers by differentiation at the source).
+__device__ void img_node_weights(int kind, const double sl[3], const double dl[3], const double nn[3],
+                                 const double y[3], const P2MArgs& a, double wv[9]) {
+  const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu, al = a.alpha, lam = a.lam, mu = a.mu;
+  for (int k = 0; k < 9; k++) wv[k] = 0.0;
+  double Qm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+  const double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
+  double Tm[3][3];
+  for (int k = 0; k < 3; k++)
+    for (int l = 0; l < 3; l++) Tm[k][l] = (k == l ? lam * dln : 0.0) + mu * (dl[k] * nn[l] + dl[l] * nn[k]);
+  const double h = -y[2];
+  if (kind < 3) {
+    wv[0] = sl[kind] * inv2mu;
+    for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * (nn[d] * dl[kind] + dl[d] * nn[kind]);
+  } else if (kind == 3) {
+    const double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
+    const double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+    const double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+    wv[0] = sly * c1 * inv2mu + dln * c2;
+    for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
+  } else if (kind == 4) {
+    wv[0] = -(2.0 - al) * sl[2];
+    for (int d = 0; d < 3; d++) wv[1 + d] = -h * al * sl[d] - (2.0 - 2.0 * al) * Tm[2][d];
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) Qm[k][l] = -h * al * Tm[k][l];
+  } else if (kind == 5) {
+    for (int d = 0; d < 3; d++) wv[1 + d] = -sl[d];
+    for (int k = 0; k < 3; k++)
+      for (int l = 0; l < 3; l++) Qm[k][l] = -Tm[k][l];
+  } else {
+    wv[1] = sl[0];
+    wv[2] = sl[1];
+    wv[3] = -sl[2];
+    Qm[0][0] = Tm[0][0]; Qm[1][1] = Tm[1][1]; Qm[2][2] = -Tm[2][2];
+    Qm[0][1] = Qm[1][0] = Tm[0][1];
+  }
+  wv[4] = Qm[0][0] - Qm[2][2];
+  wv[5] = Qm[1][1] - Qm[2][2];
+  wv[6] = 2.0 * Qm[0][1];
+  wv[7] = 2.0 * Qm[0][2];
+  wv[8] = 2.0 * Qm[1][2];
+}
+
+// Weights matrix per leaf: column col of ldb K = 9 nnode, rows in the
+// feature order (4 node + f, then 4 nnode + 5 node + f - 4).
 template <class T>
 __global__ void __launch_bounds__(256)
 k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ woff,
@@ -502,14 +550,12 @@ k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const
   const int box = a.leaves[wleaves[blockIdx.x]];
   const int tn = a.scount[box];
   const int nnode = 12 * tn, K = 9 * nnode, C = 7 * R;
-  const double c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu, al = a.alpha, lam = a.lam, mu = a.mu;
   const double* nd = nrec + 8 * noff[blockIdx.x];
   T* out = W + woff[blockIdx.x];
   for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < (long long)nnode * C;
        q += (long long)gridDim.y * blockDim.x) {
     const int col = (int)(q / nnode), node = (int)(q % nnode);
-    const int r = col < 6 * R ? col / 6 : col - 6 * R;
-    const int kind = col < 6 * R ? col % 6 : 6;
+    const int kind = col / R, r = col % R;
     const double* o = nd + 8 * node;
     const double y[3] = {o[0], o[1], o[2]}, nn[3] = {o[3], o[4], o[5]}, w = o[6];
     const long long it = (long long)o[7];
@@ -517,46 +563,154 @@ k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const
     double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
     if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
     if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
-    double wv[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    double Qm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-    const double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
-    double Tm[3][3];
-    for (int k = 0; k < 3; k++)
-      for (int l = 0; l < 3; l++) Tm[k][l] = (k == l ? lam * dln : 0.0) + mu * (dl[k] * nn[l] + dl[l] * nn[k]);
-    const double h = -y[2];
-    if (kind < 3) {
-      wv[0] = sl[kind] * inv2mu;
-      for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * (nn[d] * dl[kind] + dl[d] * nn[kind]);
-    } else if (kind == 3) {
-      const double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
-      const double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
-      const double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
-      wv[0] = sly * c1 * inv2mu + dln * c2;
-      for (int d = 0; d < 3; d++) wv[1 + d] = 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
-    } else if (kind == 4) {
-      wv[0] = -(2.0 - al) * sl[2];
-      for (int d = 0; d < 3; d++) wv[1 + d] = -h * al * sl[d] - (2.0 - 2.0 * al) * Tm[2][d];
-      for (int k = 0; k < 3; k++)
-        for (int l = 0; l < 3; l++) Qm[k][l] = -h * al * Tm[k][l];
-    } else if (kind == 5) {
-      for (int d = 0; d < 3; d++) wv[1 + d] = -sl[d];
-      for (int k = 0; k < 3; k++)
-        for (int l = 0; l < 3; l++) Qm[k][l] = -Tm[k][l];
-    } else {
-      wv[1] = sl[0];
-      wv[2] = sl[1];
-      wv[3] = -sl[2];
-      Qm[0][0] = Tm[0][0]; Qm[1][1] = Tm[1][1]; Qm[2][2] = -Tm[2][2];
-      Qm[0][1] = Qm[1][0] = Tm[0][1];
-    }
-    wv[4] = Qm[0][0] - Qm[2][2];
-    wv[5] = Qm[1][1] - Qm[2][2];
-    wv[6] = 2.0 * Qm[0][1];
-    wv[7] = 2.0 * Qm[0][2];
-    wv[8] = 2.0 * Qm[1][2];
-    T* ow = out + (size_t)col * K + 9 * node;
+    double wv[9];
+    img_node_weights(kind, sl, dl, nn, y, a, wv);
+    T* ow = out + (size_t)col * K;
 #pragma unroll
-    for (int k = 0; k < 9; k++) ow[k] = (T)(w * wv[k]);
+    for (int k = 0; k < 4; k++) ow[4 * node + k] = (T)(w * wv[k]);
+    if (kind >= 4) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) ow[4 * nnode + 5 * node + k] = (T)(w * wv[4 + k]);
+    }
+  }
+}
+
+// Direct image P2M (few right-hand sides): one CTA per (leaf, right-hand
+// side r = blockIdx.y), nodes in batches of P2M_NODES (one warp each builds
+// the regular harmonics), every thread accumulating 7 columns of its
+// coefficients from the charge, dipole and second-derivative terms.  T =
+// float writes the normalised basis (x wnorm).
+template <class T>
+__global__ void __launch_bounds__(P2M_THREADS)
+k_p2m_img(const P2MArgs a, int R, long long ubase, T* __restrict__ mpole) {
+  extern __shared__ double sm[];
+  const int box = a.leaves[blockIdx.x];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc;
+  cplx* Ys = reinterpret_cast<cplx*>(sm);             // [P2M_NODES][nc]
+  double* qd = sm + 2 * (size_t)P2M_NODES * nc;       // [P2M_NODES][7][9]
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int nnode = 12 * tn;
+  constexpr int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
+  double acc[CMAX][7][2];
+#pragma unroll
+  for (int i = 0; i < CMAX; i++)
+#pragma unroll
+    for (int q = 0; q < 7; q++) acc[i][q][0] = acc[i][q][1] = 0.0;
+  Quad12 Q;
+  quad12(Q);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int r = blockIdx.y;
+  for (int b0 = 0; b0 < nnode; b0 += P2M_NODES) {
+    __syncthreads();
+    const int node = b0 + warp;
+    if (node < nnode) {
+      const int it = t0 + node / 12, iq = node % 12;
+      const double* Tr = a.tri + 9 * (size_t)it;
+      double y[3];
+      for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
+      const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+      const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+      const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                            e1[0] * e2[1] - e1[1] * e2[0]};
+      const double w = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
+      cplx* Y = Ys + (size_t)warp * nc;
+      const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+      for (int m = lane; m <= p; m += 32) {
+        cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+        for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+        Y[cidx(m, m)] = dm;
+        cplx ym2 = {0, 0}, ym1 = dm;
+        for (int n = m + 1; n <= p; n++) {
+          const double aa = (2.0 * n - 1.0) * z[2];
+          const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+          cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+          Y[cidx(n, m)] = yn;
+          ym2 = ym1;
+          ym1 = yn;
+        }
+      }
+      if (lane < 7) {
+        const long long off = r * a.rstride + it * a.tstride, ds = a.dstride;
+        const double* nn = a.nrm + 3 * (size_t)it;
+        double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+        if (a.dosl) { sl[0] = a.ssl[off]; sl[1] = a.ssl[off + ds]; sl[2] = a.ssl[off + 2 * ds]; }
+        if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
+        const double nv[3] = {nn[0], nn[1], nn[2]};
+        double wv[9];
+        img_node_weights(lane, sl, dl, nv, y, a, wv);
+        for (int k = 0; k < 9; k++) qd[(warp * 7 + lane) * 9 + k] = w * wv[k];
+      }
+    }
+    __syncthreads();
+    const int nb = min(P2M_NODES, nnode - b0);
+#pragma unroll
+    for (int i = 0; i < CMAX; i++) {
+      const int cc = threadIdx.x + i * P2M_THREADS;
+      if (cc >= nc) break;
+      int n = 0;
+      while ((n + 1) * (n + 2) / 2 <= cc) n++;
+      const int m = cc - n * (n + 1) / 2;
+      for (int k = 0; k < nb; k++) {
+        const cplx* Y = Ys + (size_t)k * nc;
+        // conjugated feature values (re, im) of rows: Y, d_x, d_y, d_z, xx, yy, xy, xz, yz
+        double fr[9], fi[9];
+        const cplx y = Y[cc];
+        fr[0] = y.re; fi[0] = -y.im;
+        cplx ya = {0, 0}, yb = {0, 0}, yc = {0, 0};
+        if (n > 0) {
+          ya = hget(Y, n - 1, m);
+          yb = hget(Y, n - 1, m + 1);
+          yc = hget(Y, n - 1, m - 1);
+        }
+        fr[1] = 0.5 * is * (yb.re - yc.re); fi[1] = -0.5 * is * (yb.im - yc.im);
+        fr[2] = 0.5 * is * (yb.im + yc.im); fi[2] = 0.5 * is * (yb.re + yc.re);
+        fr[3] = is * ya.re; fi[3] = -is * ya.im;
+        cplx y0 = {0, 0}, yp1 = {0, 0}, ym1 = {0, 0}, yp2 = {0, 0}, ym2 = {0, 0};
+        if (n > 1) {
+          y0 = hget(Y, n - 2, m);
+          yp1 = hget(Y, n - 2, m + 1);
+          ym1 = hget(Y, n - 2, m - 1);
+          yp2 = hget(Y, n - 2, m + 2);
+          ym2 = hget(Y, n - 2, m - 2);
+        }
+        const double q2 = is * is;
+        fr[4] = q2 * 0.25 * (yp2.re - 2.0 * y0.re + ym2.re); fi[4] = -q2 * 0.25 * (yp2.im - 2.0 * y0.im + ym2.im);
+        fr[5] = -q2 * 0.25 * (yp2.re + 2.0 * y0.re + ym2.re); fi[5] = q2 * 0.25 * (yp2.im + 2.0 * y0.im + ym2.im);
+        fr[6] = q2 * 0.25 * (yp2.im - ym2.im); fi[6] = q2 * 0.25 * (yp2.re - ym2.re);
+        fr[7] = q2 * 0.5 * (yp1.re - ym1.re); fi[7] = -q2 * 0.5 * (yp1.im - ym1.im);
+        fr[8] = q2 * 0.5 * (yp1.im + ym1.im); fi[8] = q2 * 0.5 * (yp1.re + ym1.re);
+        const double* o = qd + (size_t)k * 63;
+#pragma unroll
+        for (int q = 0; q < 7; q++) {
+          double ar = 0.0, ai = 0.0;
+#pragma unroll
+          for (int f = 0; f < 9; f++) {
+            ar += o[9 * q + f] * fr[f];
+            ai += o[9 * q + f] * fi[f];
+          }
+          acc[i][q][0] += ar;
+          acc[i][q][1] += ai;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < CMAX; i++) {
+    const int cc = threadIdx.x + i * P2M_THREADS;
+    if (cc >= nc) break;
+    const double sr = a.wnorm ? a.wnorm[2 * cc] : 1.0;
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+      T* M = q < 6 ? mpole + ((size_t)box * 6 * R + (size_t)q * R + r) * D
+                   : mpole + ubase + ((size_t)box * R + r) * D;
+      M[2 * cc] = (T)(sr * acc[i][q][0]);
+      M[2 * cc + 1] = (T)(sr * acc[i][q][1]);
+    }
   }
 }
 
@@ -1329,7 +1483,7 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
     const double x[3] = {X[0], X[1], X[2]};
     double pot[7], g[7][3], H[7][3][3];
     for (int cidx7 = 0; cidx7 < 7; cidx7++) {
-      const int col = cidx7 < 6 ? 6 * r + cidx7 : 6 * R + r;
+      const int col = cidx7 * R + r;
       const double* sv = S + soff[blockIdx.x] + (size_t)col * ldc + 9 * (size_t)e;
       pot[cidx7] = sv[0];
       g[cidx7][0] = sv[3] * is;
@@ -1413,6 +1567,17 @@ void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwlea
   k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+template <class T>
+void launch_p2m_img(cudaStream_t st, int nleaf, const P2MArgs& a, int R, long long ubase, T* mpole) {
+  if (nleaf <= 0 || R <= 0) return;
+  const size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 63 * P2M_NODES);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_img<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_p2m_img<T><<<dim3(nleaf, R), P2M_THREADS, smem, st>>>(a, R, ubase, mpole);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+template void launch_p2m_img<double>(cudaStream_t, int, const P2MArgs&, int, long long, double*);
+template void launch_p2m_img<float>(cudaStream_t, int, const P2MArgs&, int, long long, float*);
 template void launch_p2m_img_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*,
                                               const long long*, const long long*, const long long*, double*, int,
                                               double*, double*, int, const GemmTask*, double*);

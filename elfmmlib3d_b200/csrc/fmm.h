@@ -101,6 +101,11 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
 // the caller): node features with second-derivative rows (9 x 12 x
 // triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12
 // x triangles per leaf at woff), batched product into mpole.
+// Direct P2M of the image columns (one CTA per leaf and right-hand side):
+// columns kind * R + r of 6R per box (kinds 0..5) and the U column at
+// mpole + ubase + (box R + r) D.  For few right-hand sides.
+template <class T>
+void launch_p2m_img(cudaStream_t st, int nleaf, const P2MArgs& a, int R, long long ubase, T* mpole);
 template <class T>
 void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                              const long long* foff, const long long* woff, const long long* noff, double* nrec,

@@ -1373,7 +1373,10 @@ void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
     long long nodes = 0, used = 0;
     int max_nodes = 0;
     while (i < nl) {
-      const long long K = 108LL * p2m_sc_h_[i];
+      // features: 4 charge/dipole rows per node, then 5 second-derivative
+      // rows per node; the anti-image columns (4R, no quadrupole sources)
+      // multiply the first block only
+      const long long K = 108LL * p2m_sc_h_[i], K4 = 48LL * p2m_sc_h_[i];
       const long long need = K * D + K * (Cv + Cu);
       if (!wl.empty() && used + need > (long long)budget) break;
       wl.push_back((int)i);
@@ -1381,14 +1384,19 @@ void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
       wo.push_back(used + K * D);
       no.push_back(nodes);
       nodes += 12LL * p2m_sc_h_[i];
-      const long long box = p2m_h_[i];
-      for (int c0 = 0; c0 < Cv; c0 += 128)
+      const long long box = p2m_h_[i], wb = used + K * D;
+      const int CA = 4 * R, CP = 2 * R;
+      for (int c0 = 0; c0 < CA; c0 += 128)
         for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, used + K * D, box * Cv * D, D, Cv, (int)K, D, (int)K, D, r0, c0});
+          tasks.push_back({used, wb, box * Cv * D, D, CA, (int)K4, D, (int)K, D, r0, c0});
+      for (int c0 = 0; c0 < CP; c0 += 128)
+        for (int r0 = 0; r0 < D; r0 += 128)
+          tasks.push_back({used, wb + (long long)CA * K, box * Cv * D + (long long)CA * D, D, CP, (int)K, D, (int)K, D,
+                           r0, c0});
       for (int c0 = 0; c0 < Cu; c0 += 128)
         for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, used + K * D + (long long)Cv * K, (long long)(nb * Cv * D) + box * Cu * D, D, Cu,
-                           (int)K, D, (int)K, D, r0, c0});
+          tasks.push_back({used, wb + (long long)Cv * K, (long long)(nb * Cv * D) + box * Cu * D, D, Cu, (int)K, D,
+                           (int)K, D, r0, c0});
       used += need;
       max_nodes = std::max(max_nodes, 12 * p2m_sc_h_[i]);
       i++;
@@ -1552,7 +1560,10 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       float* mp = img_mp_f_.get();
       float* lc = img_lc_f_.get();
       pa.wnorm = ops_->wnorm.get();
-      p2m_img_twostage<float>(pa, R, mp);
+      if (7 * R < 32)
+        launch_p2m_img<float>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
+      else
+        p2m_img_twostage<float>(pa, R, mp);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, Cv, ops_->mats_f.get(), mp, mp);
       run_translations(m2m_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
@@ -1572,7 +1583,10 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       img_lc_.zero(st_);
       double* mp = img_mp_.get();
       double* lc = img_lc_.get();
-      p2m_img_twostage<double>(pa, R, mp);
+      if (7 * R < 32)
+        launch_p2m_img<double>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
+      else
+        p2m_img_twostage<double>(pa, R, mp);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, Cv, ops_->mats.get(), mp, mp);
       run_translations(m2m_, Cu, ops_->mats.get(), mp + nb * Cv * D, mp + nb * Cv * D);
