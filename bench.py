@@ -63,6 +63,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOADS = {
+    "hs-fault-100k-r64": dict(kind="hsbatch", nl=250, nw=200, nrhs=64, iprec=3),
+    "hs-fault-10k-r32": dict(kind="hsbatch", nl=100, nw=50, nrhs=32, iprec=3),
     "fault-100k-r64": dict(kind="batch", nl=250, nw=200, nrhs=64, iprec=3),
     "fault-10k-r32": dict(kind="batch", nl=100, nw=50, nrhs=32, iprec=3),
     "fault-200k-iter": dict(kind="iter", nl=500, nw=200, calls=10, iprec=2),
@@ -83,7 +85,7 @@ def make_fault(name, seed=1):
 def make_inputs(name, seed=1):
     from elfmmlib3d_b200 import geometry as G
     w = WORKLOADS[name]
-    if w["kind"] == "batch":
+    if w["kind"] in ("batch", "hsbatch"):
         tri, nrm, cen, sdl, iprec = make_fault(name, seed)
         return tri, nrm, cen, np.zeros((0, 3)), None, sdl[0], iprec
     if w["kind"] == "iter":
@@ -456,6 +458,188 @@ def run_batch(args, rank, world, local_rank):
     }
 
 
+def run_hsbatch(args, rank, world, local_rank):
+    """The half-space batched workload: the direct arrival (free-space plan on
+    the centroids) plus the image part (image plan on the reflected
+    centroids), both with their near fields stored on the first call of the
+    sequence and replayed for every batch of 64 slip vectors; mixed precision
+    timed as `value`, the plain FP64 form (one ITER call pair per right-hand
+    side) and the batched FP64 form beside it; errors against the direct
+    sums (free space + image) on 2,000 centroids."""
+    import torch
+    import elfmmlib3d_b200 as E
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    tri, nrm, cen, sdl, iprec = make_fault(args.workload, seed=1 + rank)
+    R, n = sdl.shape[0], len(cen)
+    evals = n * n * R
+
+    def d(a):
+        return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    dtri, dnrm, dcen, dsdl = map(d, (tri, nrm, cen, sdl))
+    dcenr = d(cen * np.array([1.0, 1.0, -1.0]))
+    F, I = E.Plan(local_rank), E.Plan(local_rank)
+    F.set_geometry(dtri, dnrm, dcen, None, iprec=iprec, iter=True)
+    I.set_geometry(dtri, dnrm, dcen, dcenr, iprec=iprec, iter=True, mindlin=True)
+    uf = torch.zeros((R, n, 3), dtype=torch.float64, device=dev)
+    ef = torch.zeros((R, n, 3, 3), dtype=torch.float64, device=dev)
+    ui, ei = torch.zeros_like(uf), torch.zeros_like(ef)
+
+    def step(precision=1, mode=2):
+        F.evaluate_batch(1.0, 1.0, R, None, dsdl, uf, ef, precision=precision, mode=mode)
+        I.evaluate_image(1.0, 1.0, R, None, dsdl, ui, ei, precision=precision, mode=mode)
+
+    t0 = time.perf_counter()
+    step(mode=1)  # first call of the sequence: near fields stored
+    store_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        step()
+    l0 = E.kernel_launches()
+    stages = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        torch.cuda.nvtx.range_push("timed")  # profiler captures select this range
+        ev0.record()
+        for _ in range(args.steps):
+            step()
+            stages.append((F.timings(), I.timings()))
+        ev1.record()
+        ev1.synchronize()
+        torch.cuda.nvtx.range_pop()
+    ms = ev0.elapsed_time(ev1)
+    launches = E.kernel_launches() - l0
+    t_max = max_over_ranks(ms, world, dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    value = replica_value(evals * args.steps, t_max, world)
+    tf = {k: float(np.mean([s_[0][k] for s_ in stages])) for k in stages[0][0]}
+    ti = {k: float(np.mean([s_[1][k] for s_ in stages])) for k in stages[0][1]}
+    u_mixed, e_mixed = (uf + ui).clone(), (ef + ei).clone()
+
+    # end to end through the plan API: slip vectors from pinned host memory,
+    # total displacement + strain back to pinned host memory, every step
+    hsdl = torch.from_numpy(np.ascontiguousarray(sdl)).pin_memory()
+    hu = torch.empty((R, n, 3), dtype=torch.float64).pin_memory()
+    he = torch.empty((R, n, 3, 3), dtype=torch.float64).pin_memory()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        dsdl.copy_(hsdl)
+        step()
+        torch.add(uf, ui, out=uf)
+        torch.add(ef, ei, out=ef)
+        hu.copy_(uf)
+        he.copy_(ef)
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = max_over_ranks(e2e_s, world, dev)
+    e2e_value = world * evals * args.steps / e2e_t
+    h2d = 8 * 3 * n * R
+    d2h = 8 * (3 * n * R + 9 * n * R)
+
+    # plain FP64: one ITER call pair (direct arrival + image) per right-hand side
+    u1 = torch.zeros((R, n, 3), dtype=torch.float64, device=dev)
+    e1 = torch.zeros((R, n, 3, 3), dtype=torch.float64, device=dev)
+    ui1 = torch.zeros((1, n, 3), dtype=torch.float64, device=dev)
+    ei1 = torch.zeros((1, n, 3, 3), dtype=torch.float64, device=dev)
+    F.evaluate(1.0, 1.0, None, dsdl[0], u1[0], e1[0], mode=2)
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record()
+    for r in range(R):
+        F.evaluate(1.0, 1.0, None, dsdl[r], u1[r], e1[r], mode=2)
+        I.evaluate_image(1.0, 1.0, 1, None, dsdl[r:r + 1], ui1, ei1, precision=0, mode=2)
+        u1[r] += ui1[0]
+        e1[r] += ei1[0]
+    pe1.record()
+    pe1.synchronize()
+    plain_ms = pe0.elapsed_time(pe1)
+    be0, be1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    step(0)
+    be0.record()
+    step(0)
+    be1.record()
+    be1.synchronize()
+    b64_ms = be0.elapsed_time(be1)
+    u64, e64 = (uf + ui).clone(), (ef + ei).clone()
+    # errors against the direct sums (free space + image) on 2,000 centroids
+    ns = min(2000, n)
+    ud = torch.zeros((ns, 3), dtype=torch.float64, device=dev)
+    ed = torch.zeros((ns, 3, 3), dtype=torch.float64, device=dev)
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    errs = {"plain_fp64": [0.0, 0.0], "batched_fp64": [0.0, 0.0], "mixed_batched": [0.0, 0.0]}
+    for r in (0, R - 1):
+        F.evaluate_direct_subset(1.0, 1.0, ns, None, dsdl[r], ud, ed)
+        ier, uid, eid = E.hs_image_direct(1.0, 1.0, tri, nrm, None, sdl[r], cen[:ns])
+        assert ier == 0, ier
+        udt = ud + torch.from_numpy(uid).to(dev)
+        edt = ed + torch.from_numpy(eid).to(dev)
+        for key, (uu, ee) in (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)),
+                              ("mixed_batched", (u_mixed, e_mixed))):
+            errs[key][0] = max(errs[key][0], rel(uu[r, :ns], udt))
+            errs[key][1] = max(errs[key][1], rel(ee[r, :ns], edt))
+    if rank != 0:
+        return None
+    # roofline: the P2M products (k_gemm_tn<float>) of both plans, the
+    # largest kernel; flops counted from the product shapes, time = the P2M
+    # stages (features and weights included: a lower bound)
+    D = 2 * (F.info()["p"] + 1) * (F.info()["p"] + 2) // 2
+    gem_flops = 2.0 * D * (4 * R) * (48 * n) + 2.0 * D * ((4 * R) * (48 * n) + (3 * R) * (108 * n))
+    p2m_ms = tf["p2m"] + ti["p2m"]
+    achieved = gem_flops / (p2m_ms * 1e-3) / 1e12
+    peak32 = gemm_peak(torch, dev, torch.float32)
+    roof = {"kernel": "k_gemm_tn<float> (P2M products, free-space and image plans)", "bound": "fp32",
+            "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
+            "peak_source": "measured cuBLAS SGEMM 8192^3 (FP32 pipe, TF32 off) in this run; "
+                           "MEASURED_PEAKS.json has no FP32 entry",
+            "algorithmic": f"P2M product flops {gem_flops:.4g} per step (features x weights, D = {D}) over the "
+                           f"P2M stage time {p2m_ms:.1f} ms (features + weights + product)"}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
+        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
+               "sample": f"oracle free-space direct sum (the direct arrival only; the image part is not in "
+                         f"the sample), {npts} centroids x {n} triangles x 1 right-hand side ({dt:.1f} s)"}
+    plain_value = evals / (plain_ms * 1e-3)
+    b64_value = evals / (b64_ms * 1e-3)
+    fi = F.info()
+    ii = I.info()
+    return {
+        "metric": "triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)",
+        "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "triangles": n, "rhs": R, "targets": "centroids", "iprec": iprec,
+                   "green": "Mindlin half space (free space + image)", "evals_per_step": evals,
+                   "parallelism": f"replicas{world}",
+                   "l2_policy": "expansions (FP32, several GB) and stored near field (~49 GB) > L2 (126 MB)",
+                   "step": "free-space batch + image batch, near fields replayed (stored on the first call, "
+                           f"{store_s * 1e3:.0f} ms, untimed)",
+                   "forms": {"mixed_batched": value / world, "batched_fp64": b64_value,
+                             "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
+                             "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms},
+                   "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
+                   "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
+                   "stage_ms_free": tf, "stage_ms_image": ti,
+                   "tree_free": {k: fi[k] for k in ("nboxes", "nlev", "p", "nbox")},
+                   "tree_image": {k: ii[k] for k in ("nboxes", "nlev", "p", "nbox")},
+                   "stored_bytes": {"free": F.stored_bytes(), "image": I.stored_bytes()}},
+        "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "timing": "host wall clock: pinned slip vectors to the device, both plans, total displacement + "
+                          "strain back to pinned host memory, every step"},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
+
+
 def run_iter(args, rank, world, local_rank):
     """The ITER workload: store on the first call, reuse on the others."""
     import torch
@@ -585,7 +769,8 @@ def run_reference(args, rank):
         return None
     tri, nrm, cen, tgt, ssl, sdl, iprec = make_inputs(args.workload)
     n = len(cen)
-    batch = WORKLOADS[args.workload]["kind"] == "batch"
+    batch = WORKLOADS[args.workload]["kind"] in ("batch", "hsbatch")
+    hs = WORKLOADS[args.workload]["kind"] == "hsbatch"
     for _ in range(args.warmup):
         cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
     t0 = time.perf_counter()
@@ -602,10 +787,13 @@ def run_reference(args, rank):
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, "triangles": n, "targets": len(tgt), "iprec": iprec,
-                   **({"rhs": WORKLOADS[args.workload]["nrhs"], "green": "free space"} if batch else {})},
+                   **({"rhs": WORKLOADS[args.workload]["nrhs"],
+                       "green": "Mindlin half space" if hs else "free space"} if batch else {})},
         "cpu_baseline": {"value": value, "unit": "triangle-evals/s", "cores": os.cpu_count(), "kind": "port",
                          "sample": f"oracle direct sum (el3dtriadirecttarg restated), {args.ref_sample} "
-                                   f"evaluation points x {n} triangles per step"},
+                                   f"evaluation points x {n} triangles per step"
+                                   + (" (the direct arrival only; the image part is not in the sample)" if hs
+                                      else "")},
         "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -616,7 +804,7 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="fault-100k-r64", choices=list(WORKLOADS))
+    ap.add_argument("--workload", default="hs-fault-100k-r64", choices=list(WORKLOADS))
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--ref-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -635,6 +823,8 @@ def main():
             dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         if WORKLOADS[args.workload]["kind"] == "batch":
             out = run_batch(args, rank, world, local_rank)
+        elif WORKLOADS[args.workload]["kind"] == "hsbatch":
+            out = run_hsbatch(args, rank, world, local_rank)
         elif WORKLOADS[args.workload]["kind"] == "iter":
             out = run_iter(args, rank, world, local_rank)
         else:
