@@ -115,5 +115,15 @@ void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const 
                       const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,
                       const T* src, T* dst);
 void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs = 1);
+// The FP32 product of k_gemm_tn<float> on the tensor cores (tc_gemm.cu):
+// tcgen05.mma kind::tf32 with the 3-term head/tail split (FP32 accuracy).
+// *err is set when a bounded wait runs out (the tile is then not stored).
+void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
+                    int* err);
+// Per-device error flag of the tensor-core products; tc_take_error reads
+// and clears it (blocking).
+int* tc_err_ptr();
+bool tc_take_error();
+bool tc_enabled();
 
 }  // namespace efmm

@@ -1,0 +1,378 @@
+// tc_gemm.cu -- batched FP32 products on the 5th-generation tensor cores.
+//
+// The same contraction as k_gemm_tn<float> (fmm.cu):
+//   C[col][row] = sum_k A[k][row] * B[col][k]
+// over 128 x 128 output tiles (GemmTask), computed with tcgen05.mma
+// kind::tf32 and FP32 accumulation in tensor memory.  FP32 accuracy comes
+// from the 3-term split of each operand into a TF32 head and a TF32 tail
+// (x = hi + lo, hi = x rounded to TF32): A B ~ Ahi Bhi + Ahi Blo + Alo Bhi,
+// the dropped Alo Blo term being 2^-22 relative.
+//
+// One CTA (256 threads) per tile.  Each K tile of 32 is staged from global
+// memory through registers into shared memory in the canonical no-swizzle
+// K-major UMMA layout (core matrices of 8 rows x 4 k, 16 bytes per row; A is
+// transposed on the way: a lane loads 4 k of one row, the lanes of a warp
+// 32 consecutive rows), split into head and tail on the way, two
+// stages deep; one thread issues the 12 MMAs of a K tile into one of two
+// 128 x 128 TMEM accumulators and commits them to the stage's mbarrier; the
+// threads then drain the previous tile's accumulator with tcgen05.ld (warp
+// w: lanes 32 (w % 4).., columns 64 (w / 4)..) into FP32 registers while the
+// tensor cores work on the current one.  Every wait is bounded: a wait that
+// runs out sets *err, waits (bounded) for the MMAs in flight, frees the TMEM
+// and returns without storing.
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cmath>
+#include <vector>
+#include <cstdlib>
+#include "common.cuh"
+#include "fmm.h"
+
+namespace efmm {
+
+namespace {
+
+constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_THREADS = 256;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;          // one operand part, 16 KB
+constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;         // A hi, A lo, B hi, B lo
+constexpr int TC_SMEM = 2 * TC_STAGE_BYTES + 1024 + 64;   // two stages, alignment, barriers
+// A and B (K-major): element (row, k) at (k % 4) * 4 + (row % 8) * 16 + (k / 4) * 128 + (row / 8) * 1024
+constexpr uint32_t TC_LBO = 128, TC_SBO = 1024;
+constexpr long long TC_WAIT_CYCLES = 4000000000LL;       // about 2 s at 2 GHz
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// no-swizzle shared-memory matrix descriptor (version 1)
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+
+// instruction descriptor: F32 accumulate, TF32 A and B (both K-major), M = 128, N = 128
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) |
+                              ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+
+__device__ __forceinline__ float tf32_head(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait for phase `parity` of the barrier; false when it ran out
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity))
+    if (clock64() - t0 > TC_WAIT_CYCLES) return false;
+  return true;
+}
+
+__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accum)
+      : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+struct Quad {
+  float v[4];
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
+          float* __restrict__ Cm, int* __restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  // 1024-byte aligned operand region
+  const uint32_t raw = smem_u32(tc_smem_raw);
+  unsigned char* sm = tc_smem_raw + ((1024 - (raw & 1023)) & 1023);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + 2 * TC_STAGE_BYTES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(sm + 2 * TC_STAGE_BYTES + 16);
+  const GemmTask t = tasks[blockIdx.x];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * TC_BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const float* Ab = A + t.a_off;
+  const float* Bb = B + t.b_off;
+  const int nkt = (t.K + TC_BK - 1) / TC_BK;
+  // staging roles (4 quads of A and 4 of B per thread and K tile)
+  Quad qa[4], qb[4];
+  auto load = [&](int kt) {
+    const int k0 = kt * TC_BK;
+#pragma unroll
+    for (int it = 0; it < 4; it++) {
+      const int b = it * 8 + warp;
+      // A: row 32 (b % 4) + lane, k chunk b / 4 (k = 4 (b / 4) .. + 3): the
+      // lanes of a warp read 32 consecutive rows of each k
+      const int m = 32 * (b & 3) + lane, ka = 4 * (b >> 2);
+      const int gm = t.row0 + m, gk = k0 + ka;
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        qa[it].v[j] = (gk + j < t.K && gm < t.M) ? Ab[(size_t)(gk + j) * t.lda + gm] : 0.0f;
+      // B: n = 8 (b % 16) + lane % 8, k chunk 4 (b / 16) + lane / 8
+      const int n = 8 * (b & 15) + (lane & 7), kc = 4 * (b >> 4) + (lane >> 3);
+      const int gn = t.col0 + n, gk2 = k0 + 4 * kc;
+#pragma unroll
+      for (int j = 0; j < 4; j++)
+        qb[it].v[j] = (gn < t.N && gk2 + j < t.K) ? Bb[(size_t)gn * t.ldb + gk2 + j] : 0.0f;
+    }
+  };
+  auto store = [&](int s) {
+    unsigned char* st = sm + s * TC_STAGE_BYTES;
+#pragma unroll
+    for (int it = 0; it < 4; it++) {
+      const int b = it * 8 + warp;
+      const int m = 32 * (b & 3) + lane, ca = b >> 2;
+      const uint32_t offa = (m & 7) * 16 + ca * TC_LBO + (m >> 3) * TC_SBO;
+      float4 hi, lo;
+      hi.x = tf32_head(qa[it].v[0]); lo.x = qa[it].v[0] - hi.x;
+      hi.y = tf32_head(qa[it].v[1]); lo.y = qa[it].v[1] - hi.y;
+      hi.z = tf32_head(qa[it].v[2]); lo.z = qa[it].v[2] - hi.z;
+      hi.w = tf32_head(qa[it].v[3]); lo.w = qa[it].v[3] - hi.w;
+      *reinterpret_cast<float4*>(st + offa) = hi;
+      *reinterpret_cast<float4*>(st + TC_TILE_BYTES + offa) = lo;
+      const int n = 8 * (b & 15) + (lane & 7), kc = 4 * (b >> 4) + (lane >> 3);
+      const uint32_t offb = (n & 7) * 16 + kc * TC_LBO + (n >> 3) * TC_SBO;
+      hi.x = tf32_head(qb[it].v[0]); lo.x = qb[it].v[0] - hi.x;
+      hi.y = tf32_head(qb[it].v[1]); lo.y = qb[it].v[1] - hi.y;
+      hi.z = tf32_head(qb[it].v[2]); lo.z = qb[it].v[2] - hi.z;
+      hi.w = tf32_head(qb[it].v[3]); lo.w = qb[it].v[3] - hi.w;
+      *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + offb) = hi;
+      *reinterpret_cast<float4*>(st + 3 * TC_TILE_BYTES + offb) = lo;
+    }
+  };
+
+  // The tensor cores accumulate with truncation, so a long accumulation in
+  // tensor memory drifts (relative error ~ K x 2^-27); each K tile is
+  // therefore accumulated afresh in one of two TMEM accumulators and added
+  // into FP32 registers (round to nearest), which keeps the product as
+  // accurate as an FP32 dot product.  Accumulator (t & 1) holds tile t.
+  const int quarter = warp & 3, half = warp >> 2;
+  float acc[64];
+#pragma unroll
+  for (int j = 0; j < 64; j++) acc[j] = 0.0f;
+  auto drain = [&](int u) {  // add the accumulator of tile u into acc
+    const uint32_t col0 = (uint32_t)(u & 1) * TC_BN + 64 * half;
+#pragma unroll
+    for (int c16 = 0; c16 < 4; c16++) {
+      const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += __uint_as_float(r[j]);
+    }
+  };
+  bool ok = true;
+  if (nkt > 0) load(0);
+  for (int kt = 0; kt < nkt; kt++) {
+    const int s = kt & 1;
+    store(s);  // stage s is free: tile kt - 2 finished before tile kt - 1 was drained
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(sm + s * TC_STAGE_BYTES);
+      const uint32_t ahi = base, alo = base + TC_TILE_BYTES, bhi = base + 2 * TC_TILE_BYTES,
+                     blo = base + 3 * TC_TILE_BYTES;
+      const uint32_t dacc = tmem + (uint32_t)s * TC_BN;
+#pragma unroll
+      for (int i = 0; i < TC_BK / 8; i++) {
+        const uint64_t dah = umma_desc(ahi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dal = umma_desc(alo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dbh = umma_desc(bhi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dbl = umma_desc(blo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        mma_tf32(dacc, dal, dbh, i > 0 ? 1u : 0u);
+        mma_tf32(dacc, dah, dbl, 1u);
+        mma_tf32(dacc, dah, dbh, 1u);
+      }
+      mma_commit(smem_u32(&bars[s]));
+    }
+    if (kt + 1 < nkt) load(kt + 1);
+    if (kt >= 1) {
+      const int u = kt - 1;
+      ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+      ok = __syncthreads_and(ok);  // one decision for the whole CTA
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      drain(u);
+    }
+  }
+  if (ok && nkt > 0) {
+    const int u = nkt - 1;
+    ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+    ok = __syncthreads_and(ok);
+    if (ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      drain(u);
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    // give the MMAs in flight another bounded wait before freeing their accumulators
+    for (int u = (nkt >= 2 ? nkt - 2 : 0); u < nkt; u++) mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+  } else {
+    const int row = t.row0 + 32 * quarter + lane;
+    if (row < t.M) {
+      float* Cp = Cm + t.c_off + row;
+#pragma unroll
+      for (int j = 0; j < 64; j++) {
+        const int col = t.col0 + 64 * half + j;
+        if (col < t.N) Cp[(size_t)col * t.ldc] = acc[j];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN) : "memory");
+}
+
+namespace {
+__device__ int g_tc_err;
+int* g_tc_err_addr[64] = {};
+}  // namespace
+
+int* tc_err_ptr() {
+  int dev = 0;
+  EFMM_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) throw CudaError{(int)cudaErrorInvalidDevice};
+  if (!g_tc_err_addr[dev]) {
+    void* p = nullptr;
+    EFMM_CUDA_TRY(cudaGetSymbolAddress(&p, g_tc_err));
+    g_tc_err_addr[dev] = static_cast<int*>(p);
+  }
+  return g_tc_err_addr[dev];
+}
+
+bool tc_take_error() {
+  int* p = tc_err_ptr();
+  int h = 0;
+  EFMM_CUDA_TRY(cudaMemcpy(&h, p, sizeof(int), cudaMemcpyDeviceToHost));
+  if (h) EFMM_CUDA_TRY(cudaMemset(p, 0, sizeof(int)));
+  return h != 0;
+}
+
+// ELFMM3D_TC=0 keeps the FP32 products on the CUDA cores (k_gemm_tn<float>)
+bool tc_enabled() {
+  static const bool on = [] {
+    const char* e = getenv("ELFMM3D_TC");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+
+void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
+                    int* err) {
+  if (ntask <= 0) return;
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
+  k_gemm_tc<<<ntask, TC_THREADS, TC_SMEM, st>>>(tasks, A, B, C, err);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+}  // namespace efmm
+
+// Device check of the tensor-core product against an FP64 host product:
+// random A (K x M, lda = M + 3), B (N x K, ldb = K + 1) in [-1, 1), C = the
+// tiles of k_gemm_tc.  Returns 0 and the relative l2 error in *rel (and
+// *timeout != 0 if a bounded wait ran out).
+extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double* rel, int* timeout) {
+  using namespace efmm;
+  if (M < 1 || N < 1 || K < 0 || M > 4096 || N > 4096 || K > 65536) return 16;
+  const int lda = M + 3, ldb = K + 1, ldc = M + 1;
+  std::vector<float> hA((size_t)K * lda), hB((size_t)N * ldb), hC((size_t)N * ldc, -7.0f);
+  unsigned long long st = seed * 6364136223846793005ull + 1;
+  auto uni = [&]() {
+    st = st * 6364136223846793005ull + 1442695040888963407ull;
+    return (float)(((st >> 11) * (1.0 / 9007199254740992.0)) * 2.0 - 1.0);
+  };
+  for (auto& v : hA) v = uni();
+  for (auto& v : hB) v = uni();
+  std::vector<GemmTask> tasks;
+  for (int c0 = 0; c0 < N; c0 += 128)
+    for (int r0 = 0; r0 < M; r0 += 128) tasks.push_back({0, 0, 0, M, N, K, lda, ldb, ldc, r0, c0});
+  float *dA = nullptr, *dB = nullptr, *dC = nullptr;
+  int* dErr = nullptr;
+  GemmTask* dT = nullptr;
+  auto fail = [&]() {
+    cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dErr); cudaFree(dT);
+    return 256;
+  };
+  if (cudaMalloc(&dA, hA.size() * 4 + 16) || cudaMalloc(&dB, hB.size() * 4 + 16) ||
+      cudaMalloc(&dC, hC.size() * 4) || cudaMalloc(&dErr, 4) || cudaMalloc(&dT, tasks.size() * sizeof(GemmTask)))
+    return fail();
+  cudaMemcpy(dA, hA.data(), hA.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dB, hB.data(), hB.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dC, hC.data(), hC.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dT, tasks.data(), tasks.size() * sizeof(GemmTask), cudaMemcpyHostToDevice);
+  cudaMemset(dErr, 0, 4);
+  try {
+    launch_gemm_tc(0, (int)tasks.size(), dT, dA, dB, dC, dErr);
+  } catch (const CudaError&) {
+    return fail();
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) return fail();
+  cudaMemcpy(hC.data(), dC, hC.size() * 4, cudaMemcpyDeviceToHost);
+  int herr = 0;
+  cudaMemcpy(&herr, dErr, 4, cudaMemcpyDeviceToHost);
+  double num = 0, den = 0;
+  for (int c = 0; c < N; c++)
+    for (int r = 0; r < M; r++) {
+      double ref = 0;
+      for (int k = 0; k < K; k++) ref += (double)hA[(size_t)k * lda + r] * (double)hB[(size_t)c * ldb + k];
+      const double d = (double)hC[(size_t)c * ldc + r] - ref;
+      num += d * d;
+      den += ref * ref;
+    }
+  *rel = den > 0 ? sqrt(num / den) : sqrt(num);
+  *timeout = herr;
+  cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dErr); cudaFree(dT);
+  return 0;
+}

@@ -211,6 +211,12 @@ int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, 
  * their direct sum; returns the largest relative error (-1 on bad input). */
 double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, unsigned seed);
 
+/* Device check of the tensor-core FP32 product (tcgen05.mma kind::tf32,
+ * 3-term split) that carries the batched P2M: random A (K x M) and B
+ * (N x K) against an FP64 host product; *rel = relative l2 error, *timeout
+ * != 0 if a bounded wait in the kernel ran out.  Returns 0 or an ier. */
+int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
+
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 

@@ -1,0 +1,33 @@
+"""The tensor-core FP32 product (tcgen05.mma kind::tf32 with the 3-term
+head/tail split) against an FP64 host product: FP32-level accuracy on full
+tiles, ragged edges (M, N not multiples of 128, K not a multiple of 32) and
+an empty K."""
+import ctypes
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(gpu, M, N, K, seed):
+    f = gpu.load().efmm_tc_gemm_selfcheck
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_double),
+                  ctypes.POINTER(ctypes.c_int)]
+    rel, to = ctypes.c_double(), ctypes.c_int()
+    ier = f(M, N, K, seed, ctypes.byref(rel), ctypes.byref(to))
+    return ier, rel.value, to.value
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 128, 32), (256, 128, 512), (300, 200, 1000), (1640, 256, 4000), (5, 7, 3)])
+def test_tc_product_fp32_accuracy(gpu, M, N, K):
+    ier, rel, to = _check(gpu, M, N, K, 11)
+    print(f"tc product {M}x{N}x{K}: rel {rel:.2e}")
+    assert ier == 0 and to == 0
+    # FP32 products of K terms in [-1, 1): FP32 rounding ~ 1e-7
+    assert rel < 2e-6
+
+
+def test_tc_product_empty_k(gpu):
+    ier, rel, to = _check(gpu, 130, 10, 0, 3)
+    assert ier == 0 and to == 0 and rel == 0.0
