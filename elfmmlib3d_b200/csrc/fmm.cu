@@ -1551,6 +1551,23 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
+// The batched product of the two-stage P2M: FP32 on the tensor cores
+// (tc_gemm.cu) unless ELFMM3D_TC=0, FP64 (and FP32 when disabled) on the
+// CUDA cores.
+template <class T>
+void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C) {
+  if (ntask <= 0) return;
+  if (sizeof(T) == 4 && tc_enabled()) {
+    launch_gemm_tc(st, ntask, tasks, reinterpret_cast<const float*>(F), reinterpret_cast<const float*>(W),
+                   reinterpret_cast<float*>(C), tc_err_ptr());
+    return;
+  }
+  const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+  k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, C);
+  count_launch();
+}
+
 template <class T>
 void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                              const long long* foff, const long long* woff, const long long* noff, double* nrec,
@@ -1562,9 +1579,7 @@ void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwlea
   k_p2m_features<T, 9><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights_img<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
-  const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
-  k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
+  gemm_product<T>(st, ntask, tasks, F, W, mpole);
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template <class T>
@@ -1615,9 +1630,7 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
   k_p2m_features<T, 4><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
-  const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
-  k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, mpole); count_launch();
+  gemm_product<T>(st, ntask, tasks, F, W, mpole);
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template void launch_p2m_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,

@@ -1144,6 +1144,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
   cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
   launches_ = (int)(launches_total() - launch0);
+  if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
   return IER_OK;
 }
 
@@ -1661,6 +1662,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
   cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
   launches_ = (int)(launches_total() - launch0);
+  if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
   return IER_OK;
 }
 
