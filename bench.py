@@ -506,7 +506,7 @@ def run_hsbatch(args, rank, world, local_rank):
         ev0.record()
         for _ in range(args.steps):
             step()
-            stages.append((F.timings(), I.timings()))
+            stages.append((F.timings(), I.timings(), F.product_stats(), I.product_stats()))
         ev1.record()
         ev1.synchronize()
         torch.cuda.nvtx.range_pop()
@@ -585,20 +585,26 @@ def run_hsbatch(args, rank, world, local_rank):
             errs[key][1] = max(errs[key][1], rel(ee[r, :ns], edt))
     if rank != 0:
         return None
-    # roofline: the P2M products (k_gemm_tn<float>) of both plans, the
-    # largest kernel; flops counted from the product shapes, time = the P2M
-    # stages (features and weights included: a lower bound)
-    D = 2 * (F.info()["p"] + 1) * (F.info()["p"] + 2) // 2
-    gem_flops = 2.0 * D * (4 * R) * (48 * n) + 2.0 * D * ((4 * R) * (48 * n) + (3 * R) * (108 * n))
-    p2m_ms = tf["p2m"] + ti["p2m"]
-    achieved = gem_flops / (p2m_ms * 1e-3) / 1e12
-    peak32 = gemm_peak(torch, dev, torch.float32)
-    roof = {"kernel": "k_gemm_tn<float> (P2M products, free-space and image plans)", "bound": "fp32",
-            "achieved": achieved, "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
-            "peak_source": "measured cuBLAS SGEMM 8192^3 (FP32 pipe, TF32 off) in this run; "
-                           "MEASURED_PEAKS.json has no FP32 entry",
-            "algorithmic": f"P2M product flops {gem_flops:.4g} per step (features x weights, D = {D}) over the "
-                           f"P2M stage time {p2m_ms:.1f} ms (features + weights + product)"}
+    # roofline: the P2M products of both plans (k_gemm_tc, the largest
+    # kernel), timed with CUDA events around each product launch on the
+    # plans' streams; useful FP32 flops from the product shapes, tensor-pipe
+    # flops = 3 x useful (the head/tail split issues three TF32 MMAs)
+    prod_ms = float(np.mean([s_[2][0] + s_[3][0] for s_ in stages]))
+    prod_flops = float(np.mean([s_[2][1] + s_[3][1] for s_ in stages]))
+    useful = prod_flops / (prod_ms * 1e-3) / 1e12
+    achieved = 3.0 * useful
+    peak = None
+    try:
+        peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("bf16_tflops") / 2.0
+        peak_source = "MEASURED_PEAKS.json bf16_tflops (burst) / 2: the dense TF32 rate is half the BF16 rate"
+    except (OSError, ValueError, TypeError):
+        peak_source = "MEASURED_PEAKS.json absent"
+    roof = {"kernel": "k_gemm_tc (P2M products, tcgen05.mma kind::tf32, free-space and image plans)",
+            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": (achieved / peak) if peak else None, "traffic": None, "peak_source": peak_source,
+            "useful_fp32_tflops": useful,
+            "algorithmic": f"{prod_flops:.4g} useful FP32 flop per step (P2M features x weights) in "
+                           f"{prod_ms:.1f} ms of product launches; 3 TF32 MMAs per FP32 product"}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)

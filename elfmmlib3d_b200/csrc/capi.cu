@@ -144,6 +144,11 @@ extern "C" void efmm_plan_timings(const efmm_plan* p, float* ms) {
   ms[4] = t.m2l; ms[5] = t.l2l; ms[6] = t.l2t; ms[7] = t.near;
 }
 
+extern "C" void efmm_plan_product_stats(const efmm_plan* p, double* out2) {
+  out2[0] = p->plan->product_ms();
+  out2[1] = p->plan->product_flops();
+}
+
 extern "C" void efmm_plan_setup_timings(const efmm_plan* p, float* ms) {
   const Timings& t = p->plan->timings;
   ms[0] = t.geo_tree; ms[1] = t.geo_lists; ms[2] = t.geo_work; ms[3] = t.geo_ops;

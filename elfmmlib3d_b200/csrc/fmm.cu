@@ -1568,10 +1568,14 @@ void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F,
   count_launch();
 }
 
+template void gemm_product<double>(cudaStream_t, int, const GemmTask*, const double*, const double*, double*);
+template void gemm_product<float>(cudaStream_t, int, const GemmTask*, const float*, const float*, float*);
+
 template <class T>
 void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                              const long long* foff, const long long* woff, const long long* noff, double* nrec,
-                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole) {
+                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole,
+                             bool do_product) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
@@ -1579,7 +1583,7 @@ void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwlea
   k_p2m_features<T, 9><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights_img<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
-  gemm_product<T>(st, ntask, tasks, F, W, mpole);
+  if (do_product) gemm_product<T>(st, ntask, tasks, F, W, mpole);
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template <class T>
@@ -1595,10 +1599,10 @@ template void launch_p2m_img<double>(cudaStream_t, int, const P2MArgs&, int, lon
 template void launch_p2m_img<float>(cudaStream_t, int, const P2MArgs&, int, long long, float*);
 template void launch_p2m_img_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*,
                                               const long long*, const long long*, const long long*, double*, int,
-                                              double*, double*, int, const GemmTask*, double*);
+                                              double*, double*, int, const GemmTask*, double*, bool);
 template void launch_p2m_img_twostage<float>(cudaStream_t, const P2MArgs&, int, int, const int*,
                                              const long long*, const long long*, const long long*, double*, int,
-                                             float*, float*, int, const GemmTask*, float*);
+                                             float*, float*, int, const GemmTask*, float*, bool);
 
 // ---------------------------------------------------------------- launchers
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp) {
@@ -1622,7 +1626,8 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs) {
 template <class T>
 void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* foff, const long long* woff, const long long* noff, double* nrec,
-                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole) {
+                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole,
+                         bool do_product) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
@@ -1630,15 +1635,15 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
   k_p2m_features<T, 4><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
-  gemm_product<T>(st, ntask, tasks, F, W, mpole);
+  if (do_product) gemm_product<T>(st, ntask, tasks, F, W, mpole);
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 template void launch_p2m_twostage<double>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
                                           const long long*, const long long*, double*, int, double*, double*, int,
-                                          const GemmTask*, double*);
+                                          const GemmTask*, double*, bool);
 template void launch_p2m_twostage<float>(cudaStream_t, const P2MArgs&, int, int, const int*, const long long*,
                                          const long long*, const long long*, double*, int, float*, float*, int,
-                                         const GemmTask*, float*);
+                                         const GemmTask*, float*, bool);
 
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,

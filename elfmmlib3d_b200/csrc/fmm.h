@@ -84,7 +84,11 @@ bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpo
 template <class T>
 void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* foff, const long long* woff, const long long* noff, double* nrec,
-                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole);
+                         int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole,
+                         bool do_product = true);
+// The product stage alone (FP32: tensor cores unless ELFMM3D_TC=0).
+template <class T>
+void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C);
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
                      int R, const TB* local, const double* wnorm);
@@ -109,7 +113,8 @@ void launch_p2m_img(cudaStream_t st, int nleaf, const P2MArgs& a, int R, long lo
 template <class T>
 void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,
                              const long long* foff, const long long* woff, const long long* noff, double* nrec,
-                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole);
+                             int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole,
+                             bool do_product = true);
 template <class T>
 void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                       const T* mats, const long long* mat_off, const int* mat_dim, int D, int C,

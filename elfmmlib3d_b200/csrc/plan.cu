@@ -255,6 +255,37 @@ Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
 }
 Plan::~Plan() {
   for (int i = 0; i < 10; i++) cudaEventDestroy(ev_[i]);
+  for (cudaEvent_t e : pev_) cudaEventDestroy(e);
+}
+
+void Plan::product_begin() { npev_ = 0; }
+
+template <class T>
+void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, const GemmTask* dtasks, const T* F,
+                         const T* W, T* C) {
+  if (npev_ + 2 > (int)pev_.size()) {
+    cudaEvent_t a, b;
+    EFMM_CUDA_TRY(cudaEventCreate(&a));
+    EFMM_CUDA_TRY(cudaEventCreate(&b));
+    pev_.push_back(a);
+    pev_.push_back(b);
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_], st_));
+  gemm_product<T>(st_, ntask, dtasks, F, W, C);
+  EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_ + 1], st_));
+  npev_ += 2;
+  for (const GemmTask& t : tasks)
+    product_flops_ += 2.0 * std::min(128, t.M - t.row0) * std::min(128, t.N - t.col0) * (double)t.K;
+}
+
+// after the pass's final synchronisation
+void Plan::product_collect() {
+  for (int i = 0; i + 1 < npev_; i += 2) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, pev_[i], pev_[i + 1]);
+    product_ms_ += ms;
+  }
+  npev_ = 0;
 }
 
 int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const double* d_src, int nt,
@@ -828,6 +859,7 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
     while (Rc > 1 && 16.0 * nb * 4 * Rc * D > have) Rc /= 2;
   }
   float tot = 0, near = 0, far = 0;
+  product_ms_ = product_flops_ = 0;
   for (int r0 = 0; r0 < R; r0 += Rc) {
     const int rc = std::min(Rc, R - r0);
     int ier = batch_pass(rlam, rmu, rc, d_ssl ? d_ssl + 3 * (size_t)n * r0 : nullptr,
@@ -892,7 +924,8 @@ void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
     T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
     launch_p2m_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
                            wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
-                           wave_tasks_.get(), mpole);
+                           wave_tasks_.get(), mpole, false);
+    product_timed<T>((int)tasks.size(), tasks, wave_tasks_.get(), scratch, scratch, mpole);
   }
 }
 template void Plan::p2m_twostage<double>(const P2MArgs&, int, double*);
@@ -953,6 +986,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   const int D = 2 * ncoef(p_);
   const size_t nb = tr_.nboxes;
   long long launch0 = launches_total();
+  product_begin();
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
   ssl_s_.resize(3 * (size_t)n * R);
   sdl_s_.resize(3 * (size_t)n * R);
@@ -1144,6 +1178,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
   cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
   launches_ = (int)(launches_total() - launch0);
+  product_collect();
   if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
   return IER_OK;
 }
@@ -1412,7 +1447,8 @@ void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
     T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
     launch_p2m_img_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
                                wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
-                               wave_tasks_.get(), mpole);
+                               wave_tasks_.get(), mpole, false);
+    product_timed<T>((int)tasks.size(), tasks, wave_tasks_.get(), scratch, scratch, mpole);
   }
 }
 
@@ -1503,6 +1539,7 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
     while (Rc > 1 && 3.0 * 8.0 * nb * 7 * Rc * D > have) Rc /= 2;
   }
   float tot = 0;
+  product_ms_ = product_flops_ = 0;
   for (int r0 = 0; r0 < R; r0 += Rc) {
     const int rc = std::min(Rc, R - r0);
     const int ier = image_pass(rlam, rmu, rc, d_ssl ? d_ssl + 3 * (size_t)n * r0 : nullptr,
@@ -1526,6 +1563,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   const int D = 2 * ncoef(p_);
   const size_t nb = tr_.nboxes;
   long long launch0 = launches_total();
+  product_begin();
   EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
   ssl_s_.resize(3 * (size_t)n * R);
   sdl_s_.resize(3 * (size_t)n * R);
@@ -1662,6 +1700,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   cudaEventElapsedTime(&timings.l2t, ev_[5], ev_[6]);
   cudaEventElapsedTime(&timings.near, ev_[6], ev_[7]);
   launches_ = (int)(launches_total() - launch0);
+  product_collect();
   if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
   return IER_OK;
 }

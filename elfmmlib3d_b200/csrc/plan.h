@@ -142,6 +142,10 @@ class Plan {
   long long near_pairs() const { return near_pairs_; }
   long long m2l_pairs() const { return (long long)m2l_pairs_h_; }
   int kernel_launches() const { return launches_; }
+  // P2M product stage of the last evaluate_batch / evaluate_image: device ms
+  // (CUDA events around each product launch) and useful flops
+  double product_ms() const { return product_ms_; }
+  double product_flops() const { return product_flops_; }
   bool far_enabled() const { return far_; }
 
  private:
@@ -163,6 +167,16 @@ class Plan {
   template <class T>
   void run_dense(TransSched& S, int C, const T* mats, const T* src, T* dst);
   DevBuf<double> img_mp_, img_lc_;
+  // event pairs around the P2M product launches of one pass
+  std::vector<cudaEvent_t> pev_;
+  int npev_ = 0;
+  double product_ms_ = 0, product_flops_ = 0;
+  void product_begin();
+  void product_end();
+  void product_collect();
+  template <class T>
+  void product_timed(int ntask, const std::vector<GemmTask>& tasks, const GemmTask* dtasks, const T* F, const T* W,
+                     T* C);
   DevBuf<float> img_mp_f_, img_lc_f_;
   DevBuf<float> mpole_f_, local_f_;
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA

@@ -270,6 +270,11 @@ int efmm_direct_noalloc(double rlam, double rmu, int n, const double *tri, const
  * m2l, l2l, l2t, near. */
 void efmm_plan_timings(const efmm_plan *plan, float *ms8);
 
+/* The batched P2M product stage of the last evaluate_batch / evaluate_image
+ * (the largest kernel of the mixed form): out2[0] device ms (CUDA events
+ * around each product launch), out2[1] its useful FP32 flops. */
+void efmm_plan_product_stats(const efmm_plan *plan, double *out2);
+
 /* Host wall-clock ms of the last set_geometry: tree, lists, work lists
  * (with the tree-order gathers), translation operators. */
 void efmm_plan_setup_timings(const efmm_plan *plan, float *ms4);
