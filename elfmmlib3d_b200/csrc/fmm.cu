@@ -1328,9 +1328,12 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
 // derivative sums (the same coefficients as k_l2t_gemm's G tile); stage 2 is
 // the FP64 product S[col][9 point + v] = sum_row G[row][.] L[col][row]
 // (k_gemm_tn); stage 3 applies the Lame recombination per (point, rhs).
+// T = float: the functionals of the normalised basis (x wnorm), multiplied
+// with the FP32 normalised local expansions on the tensor cores.
+template <class T>
 __global__ void __launch_bounds__(256)
 k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long* __restrict__ goff,
-               double* __restrict__ G) {
+               T* __restrict__ G) {
   extern __shared__ __align__(16) unsigned char lf_smem[];
   const int p = a.p, nc = ncoef(p), D = 2 * nc;
   const int box = a.leaves[wleaves[blockIdx.x]];
@@ -1366,7 +1369,7 @@ k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long
     }
   }
   __syncwarp();
-  double* out = G + goff[blockIdx.x] + 9 * (size_t)e;
+  T* out = G + goff[blockIdx.x] + 9 * (size_t)e;
   const size_t lda = 9 * (size_t)P + ((9 * P) & 1);  // even: 16-byte rows for the product's vector loads
   for (int row = lane; row < D; row += 32) {
     const int cc = row >> 1, part = row & 1;
@@ -1396,13 +1399,14 @@ k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long
           g = part == 0 ? -yid - sM * yim : yrd - sM * yrm;
         g *= t.sg;
       }
-      out[(size_t)row * lda + v] = g;
+      out[(size_t)row * lda + v] = (T)(a.wnorm ? g * a.wnorm[row] : g);
     }
   }
 }
 
+template <class TS>
 __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wleaves,
-                             const long long* __restrict__ soff, const double* __restrict__ S) {
+                             const long long* __restrict__ soff, const TS* __restrict__ S) {
   const int box = a.leaves[wleaves[blockIdx.x]];
   const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
   const int P = sn + tn;
@@ -1418,7 +1422,7 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
     const double x[3] = {X[0], X[1], X[2]};
     double pot[4], g[4][3], H[4][3][3];
     for (int pass = 0; pass < 4; pass++) {
-      const double* sv = S + soff[blockIdx.x] + (size_t)(4 * r + pass) * ldc + 9 * (size_t)e;
+      const TS* sv = S + soff[blockIdx.x] + (size_t)(4 * r + pass) * ldc + 9 * (size_t)e;
       pot[pass] = sv[0];
       g[pass][0] = sv[3] * is;
       g[pass][1] = sv[4] * is;
@@ -1468,8 +1472,9 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
 //   B piece     u_B  = (sc / mu) grad W
 //   C piece     u_C  = (x3 / mu) P,  P = (d1 Phi_a, d2 Phi_a, -d3 Phi_a - (2 - alpha) Phi_c)
 // and the strain of u(x) = u(xb(x)) uses d/dx_j = s_j d/dxb_j, s = (1, 1, -1).
+template <class TS>
 __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__ wleaves,
-                                 const long long* __restrict__ soff, const double* __restrict__ S) {
+                                 const long long* __restrict__ soff, const TS* __restrict__ S) {
   const int box = a.leaves[wleaves[blockIdx.x]];
   const int P = a.tcount[box];
   const size_t ldc = 9 * (size_t)P + ((9 * P) & 1);
@@ -1484,7 +1489,7 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
     double pot[7], g[7][3], H[7][3][3];
     for (int cidx7 = 0; cidx7 < 7; cidx7++) {
       const int col = cidx7 * R + r;
-      const double* sv = S + soff[blockIdx.x] + (size_t)col * ldc + 9 * (size_t)e;
+      const TS* sv = S + soff[blockIdx.x] + (size_t)col * ldc + 9 * (size_t)e;
       pot[cidx7] = sv[0];
       g[cidx7][0] = sv[3] * is;
       g[cidx7][1] = sv[4] * is;
@@ -1532,24 +1537,29 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
   }
 }
 
+template <class T>
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
-                         const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
-                         int ntask, const GemmTask* tasks, const double* local, bool image) {
+                         const long long* goff, const long long* soff, int max_pts, T* Gbuf, T* Sbuf,
+                         int ntask, const GemmTask* tasks, const T* local, bool image) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_features, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_l2t_features<<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
-  const int gsm = (int)(sizeof(double) * 4 * 16 * 128);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
-  k_gemm_tn<double><<<ntask, 256, gsm, st>>>(tasks, Gbuf, local, Sbuf); count_launch();
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_features<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
+  gemm_product<T>(st, ntask, tasks, Gbuf, local, Sbuf);
   if (image)
-    k_l2t_finish_img<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
+    k_l2t_finish_img<T><<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
   else
-    k_l2t_finish<<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
+    k_l2t_finish<T><<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+template void launch_l2t_twostage<double>(cudaStream_t, const L2TArgs&, int, int, const int*, const long long*,
+                                          const long long*, int, double*, double*, int, const GemmTask*,
+                                          const double*, bool);
+template void launch_l2t_twostage<float>(cudaStream_t, const L2TArgs&, int, int, const int*, const long long*,
+                                         const long long*, int, float*, float*, int, const GemmTask*,
+                                         const float*, bool);
 
 // The batched product of the two-stage P2M: FP32 on the tensor cores
 // (tc_gemm.cu) unless ELFMM3D_TC=0, FP64 (and FP32 when disabled) on the

@@ -64,6 +64,7 @@ struct L2TArgs {
   int C = 4;
   long long nsrc = 0, ntgt = 0;
   double alpha = 0, mu = 0;  // half-space image recombination
+  const double* wnorm = nullptr;  // two-stage L2T in FP32: functionals x wnorm[row]
 };
 
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);
@@ -98,9 +99,12 @@ bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const i
 // then the Lame recombination into the outputs.
 // image = true: the half-space image columns (7R per leaf, targets only)
 // and their recombination (k_l2t_finish_img).
+// T = float: normalised-basis functionals (L2TArgs.wnorm) and FP32
+// normalised local expansions, the product on the tensor cores.
+template <class T>
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
-                         const long long* goff, const long long* soff, int max_pts, double* Gbuf, double* Sbuf,
-                         int ntask, const GemmTask* tasks, const double* local, bool image = false);
+                         const long long* goff, const long long* soff, int max_pts, T* Gbuf, T* Sbuf,
+                         int ntask, const GemmTask* tasks, const T* local, bool image = false);
 // Two-stage P2M of the half-space image columns (7R per box, tasks cut by
 // the caller): node features with second-derivative rows (9 x 12 x
 // triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12

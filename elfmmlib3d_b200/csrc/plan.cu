@@ -933,11 +933,16 @@ template void Plan::p2m_twostage<float>(const P2MArgs&, int, float*);
 
 // Two-stage L2T over waves of leaves whose functionals and sums fit a
 // scratch budget (at most 8 GB or a quarter of the free memory).
-void Plan::l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt) {
+// mixed: FP32 normalised locals (local_f_) against normalised functionals,
+// the product on the tensor cores
+void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool mixed) {
   const int D = 2 * ncoef(p_), C = 4 * R;
+  L2TArgs la = la0;
+  la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
+  const size_t esz = mixed ? sizeof(float) : sizeof(double);
   size_t freeb = 0, totb = 0;
   EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / 8;
+  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
   size_t i = 0;
   const size_t nl = l2t_h_.size();
   while (i < nl) {
@@ -967,13 +972,20 @@ void Plan::l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt) {
       i++;
     }
     if (wl.empty()) break;
-    l2t_scratch_.resize((size_t)used);
+    l2t_scratch_.resize(((size_t)used * esz + sizeof(double) - 1) / sizeof(double));
     h2d(wave_leaves_, wl, st_);
     h2d(wave_foff_, go, st_);
     h2d(wave_woff_, so, st_);
     h2d(wave_tasks_, tasks, st_);
-    launch_l2t_twostage(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(), max_pts,
-                        l2t_scratch_.get(), l2t_scratch_.get(), (int)tasks.size(), wave_tasks_.get(), local_.get());
+    if (mixed) {
+      float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
+      launch_l2t_twostage<float>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
+                                 max_pts, sc, sc, (int)tasks.size(), wave_tasks_.get(), local_f_.get());
+    } else {
+      launch_l2t_twostage<double>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(),
+                                  wave_woff_.get(), max_pts, l2t_scratch_.get(), l2t_scratch_.get(),
+                                  (int)tasks.size(), wave_tasks_.get(), local_.get());
+    }
   }
 }
 
@@ -1076,12 +1088,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     // two-stage product form once the columns fill its tiles
     bool done = false;
     if (C >= 32) {
-      if (mixed) {
-        local_.resize(nb * C * D);
-        k_f2d_local<<<1184, 256, 0, st_>>>(local_f_.size(), D, ops_->wnorm.get(), local_f_.get(), local_.get());
-        count_launch();
-      }
-      l2t_twostage(la, R, do_src, do_tgt);
+      l2t_twostage(la, R, do_src, do_tgt, mixed);
       done = true;
     }
     if (!done && C >= 32) {
@@ -1360,6 +1367,36 @@ int Plan::build_image_sched() {
   }
   std::vector<int> hb = d2h(bad, 1, st_);
   if (hb[0] != 0) return IER_BADARG;
+  // L2L into boxes that hold targets only (the boxes below the surface hold
+  // the image sources and are never evaluated)
+  {
+    auto nkids = d2h(tr_.nkids, nb, st_);
+    auto kids = d2h(tr_.kids, 8 * (size_t)nb, st_);
+    auto tcount = d2h(tr_.tcount, nb, st_);
+    auto ijk = d2h(tr_.ijk, 3 * (size_t)nb, st_);
+    l2l_img_.clear();
+    std::vector<TransPair> pairs;
+    for (int lev = 2; lev < tr_.nlev; lev++) {
+      std::vector<std::vector<TransPair>> byg(8);
+      const int lo = tr_.laddr[lev].first, cnt = tr_.laddr[lev].second;
+      for (int b = lo; b < lo + cnt; b++)
+        for (int q = 0; q < nkids[b]; q++) {
+          const int k = kids[8 * b + q];
+          if (tcount[k] == 0) continue;
+          const int dg = ((ijk[3 * k] - 1) & 1) + 2 * ((ijk[3 * k + 1] - 1) & 1) + 4 * ((ijk[3 * k + 2] - 1) & 1);
+          byg[dg].push_back(TransPair{b, k, 1.0});
+        }
+      const int s0 = (int)l2l_img_.segs.size();
+      for (int dg = 0; dg < 8; dg++) {
+        if (byg[dg].empty()) continue;
+        l2l_img_.segs.push_back({ops_->l2l_group[dg], (int)pairs.size(), (int)byg[dg].size()});
+        pairs.insert(pairs.end(), byg[dg].begin(), byg[dg].end());
+      }
+      l2l_img_.lev.push_back({s0, (int)l2l_img_.segs.size() - s0});
+    }
+    if (pairs.empty()) pairs.push_back(TransPair{0, 0, 0.0});
+    h2d(l2l_img_.pairs, pairs, st_);
+  }
   img_sched_ = true;
   return IER_OK;
 }
@@ -1453,12 +1490,16 @@ void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
 }
 
 // Two-stage L2T of the image columns at the targets (waves as in l2t_twostage).
-void Plan::l2t_img_twostage(const L2TArgs& la, int R, const double* local) {
+void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, const float* local_f) {
   const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R, C = Cv + Cu;
   const size_t nb = tr_.nboxes;
+  const bool mixed = local_f != nullptr;
+  L2TArgs la = la0;
+  la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
+  const size_t esz = mixed ? sizeof(float) : sizeof(double);
   size_t freeb = 0, totb = 0;
   EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / 8;
+  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
   size_t i = 0;
   const size_t nl = l2t_h_.size();
   while (i < nl) {
@@ -1492,13 +1533,20 @@ void Plan::l2t_img_twostage(const L2TArgs& la, int R, const double* local) {
       i++;
     }
     if (wl.empty()) break;
-    l2t_scratch_.resize((size_t)used);
+    l2t_scratch_.resize(((size_t)used * esz + sizeof(double) - 1) / sizeof(double));
     h2d(wave_leaves_, wl, st_);
     h2d(wave_foff_, go, st_);
     h2d(wave_woff_, so, st_);
     h2d(wave_tasks_, tasks, st_);
-    launch_l2t_twostage(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(), max_pts,
-                        l2t_scratch_.get(), l2t_scratch_.get(), (int)tasks.size(), wave_tasks_.get(), local, true);
+    if (mixed) {
+      float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
+      launch_l2t_twostage<float>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
+                                 max_pts, sc, sc, (int)tasks.size(), wave_tasks_.get(), local_f, true);
+    } else {
+      launch_l2t_twostage<double>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(),
+                                  wave_woff_.get(), max_pts, l2t_scratch_.get(), l2t_scratch_.get(),
+                                  (int)tasks.size(), wave_tasks_.get(), local, true);
+    }
   }
 }
 
@@ -1610,11 +1658,8 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       run_translations(m2lv_img_, Cv, ops_->mats_f.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
-      run_translations(l2l_, Cv, ops_->mats_f.get(), lc, lc);
-      run_translations(l2l_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
-      img_lc_.resize(tot);
-      k_f2d_local<<<1184, 256, 0, st_>>>(tot, D, ops_->wnorm.get(), lc, img_lc_.get());
-      count_launch();
+      run_translations(l2l_img_, Cv, ops_->mats_f.get(), lc, lc);
+      run_translations(l2l_img_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     } else {
       img_mp_.resize(tot);
       img_lc_.resize(tot);
@@ -1633,8 +1678,8 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       run_translations(m2lv_img_, Cv, ops_->mats.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats.get(), mp + nb * Cv * D, lc + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
-      run_translations(l2l_, Cv, ops_->mats.get(), lc, lc);
-      run_translations(l2l_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
+      run_translations(l2l_img_, Cv, ops_->mats.get(), lc, lc);
+      run_translations(l2l_img_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     }
     EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
     L2TArgs la;
@@ -1644,14 +1689,14 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
     for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
     la.size = tr_.size;
-    la.local = img_lc_.get();
+    la.local = mixed ? nullptr : img_lc_.get();
     la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
     la.p = p_; la.do_src = 0; la.do_tgt = 1;
     la.dostrain_src = 0; la.dostrain_tgt = dstr;
     la.c1 = 2.0 - al; la.alpha = al; la.mu = rmu;
     la.u_src = nullptr; la.e_src = nullptr; la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
     la.C = Cv + Cu; la.nsrc = n; la.ntgt = nt;
-    l2t_img_twostage(la, R, img_lc_.get());
+    l2t_img_twostage(la, R, mixed ? nullptr : img_lc_.get(), mixed ? img_lc_f_.get() : nullptr);
   } else {
     for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
   }

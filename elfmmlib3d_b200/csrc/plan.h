@@ -160,10 +160,10 @@ class Plan {
   int build_image_sched();
   void build_chunks(int do_src, int do_tgt);
   bool mindlin_ = false, img_sched_ = false;
-  TransSched m2lv_img_, m2lu_;
+  TransSched m2lv_img_, m2lu_, l2l_img_;
   template <class T>
   void p2m_img_twostage(const P2MArgs& pa, int R, T* mpole);
-  void l2t_img_twostage(const L2TArgs& la, int R, const double* local);
+  void l2t_img_twostage(const L2TArgs& la, int R, const double* local, const float* local_f);
   template <class T>
   void run_dense(TransSched& S, int C, const T* mats, const T* src, T* dst);
   DevBuf<double> img_mp_, img_lc_;
@@ -184,7 +184,7 @@ class Plan {
   std::vector<int> l2t_sc_h_, l2t_tc_h_;  // per L2T leaf
   std::vector<int> l2t_h_;                // L2T leaves
   DevBuf<double> l2t_scratch_;            // functionals + sums of one wave of leaves
-  void l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt);
+  void l2t_twostage(const L2TArgs& la, int R, int do_src, int do_tgt, bool mixed = false);
   std::vector<int> p2m_h_, p2m_sc_h_;     // P2M leaves and their triangle counts
   DevBuf<double> p2m_scratch_;            // node features + weights of one wave of leaves
   DevBuf<int> wave_leaves_;
