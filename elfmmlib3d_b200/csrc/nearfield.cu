@@ -426,6 +426,98 @@ k_near_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __
   }
 }
 
+// Batched replay of the stored near field, specialised on the layer count
+// NLAY (1: one layer, 2: both) and strain STR: compile-time block size
+// K = 3 NLAY (3 + 6 STR), only the enabled layers' densities staged, every
+// inner loop unrolled.  Same tiling as k_near_batch (CTA per 8 points of a
+// leaf, 16 triangles per tile, 9 x RB outputs per thread).
+template <int RB, int NLAY, int STR>
+__global__ void __launch_bounds__(NB_THREADS)
+k_near_replay_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const int* __restrict__ chunk_e0, int R,
+                    const double* __restrict__ sg0, const double* __restrict__ sg1, int nsrc, int ntgt,
+                    const long long* __restrict__ sbase, const int* __restrict__ sntri,
+                    const double* __restrict__ store) {
+  constexpr int RW = 16 * RB, NJ = 3 * NLAY, KB = 3 + 6 * STR, K = NJ * KB;
+  extern __shared__ __align__(16) double rb_sm[];
+  double* Bk = rb_sm;                     // [NB_PTS][NB_TRI][K]
+  double* Sg = Bk + NB_PTS * NB_TRI * K;  // [NB_TRI][NJ][RW]
+  const int li = chunk_leaf[blockIdx.x], e0 = chunk_e0[blockIdx.x];
+  const int leaf = a.leaves[li];
+  const int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int t0 = a.box_tgt_start[leaf], tn = a.do_tgt ? a.box_tgt_count[leaf] : 0;
+  const int nep = sn + tn;
+  const int tid = threadIdx.x;
+  const int rr = tid % 16, pq = tid / 16;
+  const int nt = sntri[li];
+  const double* src = store + sbase[li];
+  double acc[KB][RB];
+#pragma unroll
+  for (int c = 0; c < KB; c++)
+#pragma unroll
+    for (int k = 0; k < RB; k++) acc[c][k] = 0.0;
+  int pos = 0;
+  for (int b = a.nb_start[li]; b < a.nb_start[li + 1]; b++) {
+    const int sb = a.nb_items[b];
+    const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+    for (int k0 = 0; k0 < trn; k0 += NB_TRI) {
+      const int cnt = min(NB_TRI, trn - k0);
+      __syncthreads();
+      for (int q = tid; q < NB_TRI * NJ * RW; q += NB_THREADS) {
+        const int t = q / (NJ * RW), j = (q / RW) % NJ, r = q % RW;
+        const double* sg = (NLAY == 2 && j >= 3) ? sg1 : sg0;
+        double v = 0.0;
+        if (t < cnt && r < R) v = sg[((size_t)(tr0 + k0 + t) * 3 + (j % 3)) * R + r];
+        Sg[q] = v;
+      }
+      for (int q = tid; q < NB_PTS * NB_TRI * K; q += NB_THREADS) {
+        const int pt = q / (NB_TRI * K), rem = q % (NB_TRI * K), t = rem / K, c = rem % K;
+        const int e = e0 + pt;
+        double v = 0.0;
+        if (e < nep && t < cnt) v = src[((size_t)e * nt + (pos + k0 + t)) * K + c];
+        Bk[q] = v;
+      }
+      __syncthreads();
+      const double* Bp = Bk + pq * NB_TRI * K;
+#pragma unroll 2
+      for (int t = 0; t < cnt; t++) {
+        const double* Bt = Bp + t * K;
+#pragma unroll
+        for (int j = 0; j < NJ; j++) {
+          double sv[RB];
+#pragma unroll
+          for (int k = 0; k < RB; k++) sv[k] = Sg[(t * NJ + j) * RW + rr + 16 * k];
+#pragma unroll
+          for (int c = 0; c < KB; c++) {
+            const double bv = Bt[j * KB + c];
+#pragma unroll
+            for (int k = 0; k < RB; k++) acc[c][k] += bv * sv[k];
+          }
+        }
+      }
+    }
+    pos += trn;
+  }
+  const int e2 = e0 + pq;
+  if (e2 >= nep) return;
+  const bool src2 = e2 < sn;
+  const int pid2 = src2 ? s0 + e2 : t0 + (e2 - sn);
+  const size_t np = src2 ? (size_t)nsrc : (size_t)ntgt;
+  const bool ds2 = src2 ? a.dostrain_src : a.dostrain_tgt;
+#pragma unroll
+  for (int k = 0; k < RB; k++) {
+    const int r = rr + 16 * k;
+    if (r >= R) continue;
+    double* U = (src2 ? a.u_src : a.u_tgt) + 3 * (np * r + pid2);
+#pragma unroll
+    for (int c = 0; c < 3; c++) U[c] += acc[c][k];
+    if (STR && ds2) {
+      double* E = (src2 ? a.e_src : a.e_tgt) + 6 * (np * r + pid2);
+#pragma unroll
+      for (int c = 0; c < 6; c++) E[c] += acc[3 + c][k];
+    }
+  }
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out) {
@@ -471,12 +563,27 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
     count_launch();
   };
   if (store) {
+    const int nlay = nl, str = dostrain;
+    const double* g0 = a.dosl ? ssl : sdl;
+    const double* g1 = sdl;
+    const int smem2 = (int)(sizeof(double) * (NB_PTS * NB_TRI * K + NB_TRI * 3 * nlay * 16 * RB));
+    auto go2 = [&](auto kern) {
+      EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2));
+      kern<<<nchunk, NB_THREADS, smem2, st>>>(a, chunk_leaf, chunk_e0, R, g0, g1, nsrc, ntgt, sbase, sntri, store);
+      count_launch();
+    };
+#define EFMM_RB(RBV)                                                         \
+  if (nlay == 1 && !str) go2(k_near_replay_batch<RBV, 1, 0>);                \
+  else if (nlay == 1) go2(k_near_replay_batch<RBV, 1, 1>);                   \
+  else if (!str) go2(k_near_replay_batch<RBV, 2, 0>);                        \
+  else go2(k_near_replay_batch<RBV, 2, 1>);
     switch (RB) {
-      case 1: go(k_near_batch<1, true>); break;
-      case 2: go(k_near_batch<2, true>); break;
-      case 3: go(k_near_batch<3, true>); break;
-      default: go(k_near_batch<4, true>); break;
+      case 1: EFMM_RB(1) break;
+      case 2: EFMM_RB(2) break;
+      case 3: EFMM_RB(3) break;
+      default: EFMM_RB(4) break;
     }
+#undef EFMM_RB
   } else {
     switch (RB) {
       case 1: go(k_near_batch<1, false>); break;
