@@ -137,6 +137,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   const int nkt = (t.K + TC_BK - 1) / TC_BK;
   // staging roles (4 quads of A and 4 of B per thread and K tile)
   Quad qa[4], qb[4];
+  const bool bvec = ((t.b_off & 3) == 0) && ((t.ldb & 3) == 0);  // 16-byte rows of B
   auto load = [&](int kt) {
     const int k0 = kt * TC_BK;
 #pragma unroll
@@ -152,9 +153,14 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
       // B: n = 8 (b % 16) + lane % 8, k chunk 4 (b / 16) + lane / 8
       const int n = 8 * (b & 15) + (lane & 7), kc = 4 * (b >> 4) + (lane >> 3);
       const int gn = t.col0 + n, gk2 = k0 + 4 * kc;
+      if (bvec && gn < t.N && gk2 + 3 < t.K) {
+        const float4 v = *reinterpret_cast<const float4*>(Bb + (size_t)gn * t.ldb + gk2);
+        qb[it].v[0] = v.x; qb[it].v[1] = v.y; qb[it].v[2] = v.z; qb[it].v[3] = v.w;
+      } else {
 #pragma unroll
-      for (int j = 0; j < 4; j++)
-        qb[it].v[j] = (gn < t.N && gk2 + j < t.K) ? Bb[(size_t)gn * t.ldb + gk2 + j] : 0.0f;
+        for (int j = 0; j < 4; j++)
+          qb[it].v[j] = (gn < t.N && gk2 + j < t.K) ? Bb[(size_t)gn * t.ldb + gk2 + j] : 0.0f;
+      }
     }
   };
   auto store = [&](int s) {
