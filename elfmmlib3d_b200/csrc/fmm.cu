@@ -1465,6 +1465,159 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
   }
 }
 
+// Image displacement and strain at the original target from the value,
+// gradient and Hessian of the 7 columns at the reflected target x (columns:
+// 0..3 anti-image passes, 4 Phi_a, 5 Phi_c, 6 W); ADDED to U (3) and, if
+// E is set, E (6).
+__device__ __forceinline__ void img_recombine(const double x[3], const double pot[7], const double g[7][3],
+                                              const double H[7][3][3], double c1, double al, double imu, double sc,
+                                              double* U, double* E) {
+  const double x3 = -x[2];
+  const double Pv[3] = {g[4][0], g[4][1], -g[4][2] - (2.0 - al) * pot[5]};
+  double u[3], Gm[3][3];
+  for (int i = 0; i < 3; i++) {
+    u[i] = (2.0 - c1) * pot[i] + g[3][i];
+    for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+    u[i] += sc * imu * g[6][i] + x3 * imu * Pv[i];
+  }
+  U[0] += u[0];
+  U[1] += u[1];
+  U[2] += u[2];
+  if (!E) return;
+  for (int aa = 0; aa < 3; aa++)
+    for (int bb = 0; bb < 3; bb++) {
+      double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
+      for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+      v += sc * imu * H[6][aa][bb];
+      const double dP = aa < 2 ? H[4][aa][bb] : -H[4][2][bb] - (2.0 - al) * g[5][bb];
+      v += imu * ((bb == 2 ? -Pv[aa] : 0.0) + x3 * dP);
+      Gm[aa][bb] = v;  // d u_a / d xb_b
+    }
+  // d u_a / d x_b = s_b Gm[a][b], s = (1, 1, -1)
+  E[0] += Gm[0][0];
+  E[1] += Gm[1][1];
+  E[2] -= Gm[2][2];
+  E[3] += 0.5 * (Gm[0][1] + Gm[1][0]);
+  E[4] += 0.5 * (-Gm[0][2] + Gm[2][0]);
+  E[5] += 0.5 * (-Gm[1][2] + Gm[2][1]);
+}
+
+// Direct image L2T (few right-hand sides): one CTA per (leaf, right-hand
+// side r = blockIdx.y), the leaf's 7 local expansions in shared memory, a
+// warp per target point (lanes over the (n, m) terms, warp-shuffle sums),
+// then img_recombine.  local: columns kind * R + r of 6R per box, the U
+// column at local + ubase + (box R + r) D.
+__global__ void __launch_bounds__(L2T_WARPS * 32)
+k_l2t_img(const L2TArgs a, int R, long long ubase) {
+  extern __shared__ double lim_sm[];
+  const int box = a.leaves[blockIdx.x];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc;
+  const int r = blockIdx.y;
+  double* Ls = lim_sm;                                            // [7][D]
+  cplx* Yall = reinterpret_cast<cplx*>(lim_sm + 7 * (size_t)D);  // [warps][nc]
+  for (int q = threadIdx.x; q < 7 * D; q += blockDim.x) {
+    const int col = q / D, row = q % D;
+    const double* L = col < 6 ? a.local + ((size_t)box * 6 * R + (size_t)col * R + r) * D
+                              : a.local + ubase + ((size_t)box * R + r) * D;
+    Ls[q] = L[row];
+  }
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  cplx* Y = Yall + (size_t)warp * nc;
+  const int tn = a.tcount[box], t0 = a.tstart[box];
+  const double al = a.alpha, imu = 1.0 / a.mu, sc = (1.0 - al) / al;
+  for (int e = warp; e < tn; e += nw) {
+    const int pidx = t0 + e;
+    const double* X = a.tgt_pts + 3 * (size_t)pidx;
+    const double x[3] = {X[0], X[1], X[2]};
+    const double z[3] = {(x[0] - c[0]) * is, (x[1] - c[1]) * is, (x[2] - c[2]) * is};
+    __syncwarp();
+    const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+    for (int m = lane; m <= p; m += 32) {
+      cplx dm = {1.0, 0.0}, wv = {-0.5 * z[0], -0.5 * z[1]};
+      for (int k = 1; k <= m; k++) dm = cscale(1.0 / k, cmul(dm, wv));
+      Y[cidx(m, m)] = dm;
+      cplx ym2 = {0, 0}, ym1 = dm;
+      for (int n = m + 1; n <= p; n++) {
+        const double aa = (2.0 * n - 1.0) * z[2];
+        const double inv = 1.0 / ((double)(n - m) * (double)(n + m));
+        cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        Y[cidx(n, m)] = yn;
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+    __syncwarp();
+    double S[7][9];
+#pragma unroll
+    for (int q = 0; q < 7; q++)
+#pragma unroll
+      for (int v = 0; v < 9; v++) S[q][v] = 0.0;
+    const int tot = (p + 1) * (p + 1);
+    for (int idx = lane; idx < tot; idx += 32) {
+      int n = (int)sqrt((double)idx);
+      while (n * n > idx) n--;
+      while ((n + 1) * (n + 1) <= idx) n++;
+      const int m = idx - n * n - n;
+      const cplx yc = cconj(hget(Y, n, m));
+#pragma unroll
+      for (int q = 0; q < 7; q++) {
+        const double* Lq = Ls + (size_t)q * D;
+        auto Lg = [&](int nn, int mm) -> cplx {
+          if (nn > p || mm > nn || -mm > nn) return cplx{0.0, 0.0};
+          if (mm >= 0) return cplx{Lq[2 * cidx(nn, mm)], Lq[2 * cidx(nn, mm) + 1]};
+          const double re = Lq[2 * cidx(nn, -mm)], im = Lq[2 * cidx(nn, -mm) + 1];
+          return ((-mm) & 1) ? cplx{-re, im} : cplx{re, -im};
+        };
+        const cplx c0 = Lg(n, m);
+        S[q][0] += c0.re * yc.re - c0.im * yc.im;
+        if (n + 1 <= p) {
+          const cplx c1 = Lg(n + 1, m);
+          S[q][1] += c1.re * yc.re - c1.im * yc.im;
+          const cplx c2 = Lg(n + 1, m + 1);
+          S[q][3] -= c2.re * yc.re - c2.im * yc.im;
+          S[q][4] -= c2.re * yc.im + c2.im * yc.re;
+        }
+        if (n + 2 <= p) {
+          const cplx c3 = Lg(n + 2, m);
+          S[q][2] += c3.re * yc.re - c3.im * yc.im;
+          const cplx c4 = Lg(n + 2, m + 1);
+          S[q][5] -= c4.re * yc.re - c4.im * yc.im;
+          S[q][6] -= c4.re * yc.im + c4.im * yc.re;
+          const cplx c5 = Lg(n + 2, m + 2);
+          S[q][7] += c5.re * yc.re - c5.im * yc.im;
+          S[q][8] += c5.re * yc.im + c5.im * yc.re;
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 7; q++)
+#pragma unroll
+      for (int v = 0; v < 9; v++) S[q][v] = warp_sum(S[q][v]);
+    if (lane == 0) {
+      double pot[7], g[7][3], H[7][3][3];
+      for (int q = 0; q < 7; q++) {
+        pot[q] = S[q][0];
+        g[q][0] = S[q][3] * is;
+        g[q][1] = S[q][4] * is;
+        g[q][2] = S[q][1] * is;
+        const double hzz = S[q][2];
+        const double hxx = 0.5 * (S[q][7] - hzz), hyy = 0.5 * (-S[q][7] - hzz), hxy = 0.5 * S[q][8];
+        H[q][0][0] = hxx * is2; H[q][1][1] = hyy * is2; H[q][2][2] = hzz * is2;
+        H[q][0][1] = H[q][1][0] = hxy * is2;
+        H[q][0][2] = H[q][2][0] = S[q][5] * is2;
+        H[q][1][2] = H[q][2][1] = S[q][6] * is2;
+      }
+      img_recombine(x, pot, g, H, a.c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
+                    a.dostrain_tgt ? a.e_tgt + 6 * (a.ntgt * r + pidx) : nullptr);
+    }
+  }
+}
+
 // Half-space image recombination at the reflected targets xb = (x1, x2, -x3)
 // of the plan (columns as in k_p2m_weights_img, 7R per leaf in S).  In the
 // variables xb, with alpha = (lam + mu)/(lam + 2 mu), sc = (1 - alpha)/alpha:
@@ -1502,39 +1655,20 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
       H[cidx7][0][2] = H[cidx7][2][0] = hxz * is2;
       H[cidx7][1][2] = H[cidx7][2][1] = hyz * is2;
     }
-    // columns: 0..3 anti-image passes, 4 Phi_a, 5 Phi_c, 6 W
-    const double x3 = -x[2];
-    const double Pv[3] = {g[4][0], g[4][1], -g[4][2] - (2.0 - al) * pot[5]};
-    double u[3], Gm[3][3];
-    for (int i = 0; i < 3; i++) {
-      u[i] = (2.0 - c1) * pot[i] + g[3][i];
-      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
-      u[i] += sc * imu * g[6][i] + x3 * imu * Pv[i];
-    }
-    for (int aa = 0; aa < 3; aa++)
-      for (int bb = 0; bb < 3; bb++) {
-        double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
-        for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
-        v += sc * imu * H[6][aa][bb];
-        const double dP = aa < 2 ? H[4][aa][bb] : -H[4][2][bb] - (2.0 - al) * g[5][bb];
-        v += imu * ((bb == 2 ? -Pv[aa] : 0.0) + x3 * dP);
-        Gm[aa][bb] = v;  // d u_a / d xb_b
-      }
-    double* U = a.u_tgt + 3 * (a.ntgt * r + pidx);
-    U[0] += u[0];
-    U[1] += u[1];
-    U[2] += u[2];
-    if (a.dostrain_tgt) {
-      // d u_a / d x_b = s_b Gm[a][b]
-      double* E = a.e_tgt + 6 * (a.ntgt * r + pidx);
-      E[0] += Gm[0][0];
-      E[1] += Gm[1][1];
-      E[2] -= Gm[2][2];
-      E[3] += 0.5 * (Gm[0][1] + Gm[1][0]);
-      E[4] += 0.5 * (-Gm[0][2] + Gm[2][0]);
-      E[5] += 0.5 * (-Gm[1][2] + Gm[2][1]);
-    }
+    img_recombine(x, pot, g, H, c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
+                  a.dostrain_tgt ? a.e_tgt + 6 * (a.ntgt * r + pidx) : nullptr);
   }
+}
+
+bool launch_l2t_img(cudaStream_t st, int nleaf, const L2TArgs& a, int R, long long ubase) {
+  const size_t smem = sizeof(double) * 7 * 2 * (size_t)ncoef(a.p) + sizeof(cplx) * L2T_WARPS * ncoef(a.p);
+  if (smem > 227 * 1024) return false;  // high orders: the two-stage form
+  if (nleaf <= 0 || R <= 0) return true;
+  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_img, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_l2t_img<<<dim3(nleaf, R), L2T_WARPS * 32, smem, st>>>(a, R, ubase);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+  return true;
 }
 
 template <class T>

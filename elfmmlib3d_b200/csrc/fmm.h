@@ -87,6 +87,11 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
                          const long long* foff, const long long* woff, const long long* noff, double* nrec,
                          int max_nodes, T* F, T* W, int ntask, const GemmTask* tasks, T* mpole,
                          bool do_product = true);
+// Direct L2T of the image columns for few right-hand sides (one CTA per
+// leaf and right-hand side, FP64 locals: columns kind * R + r of 6R per box,
+// the U column at local + ubase + (box R + r) D).
+// Returns false (nothing launched) when the order is too high for its tiles.
+bool launch_l2t_img(cudaStream_t st, int nleaf, const L2TArgs& a, int R, long long ubase);
 // The product stage alone (FP32: tensor cores unless ELFMM3D_TC=0).
 template <class T>
 void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C);

@@ -1396,6 +1396,19 @@ int Plan::build_image_sched() {
     }
     if (pairs.empty()) pairs.push_back(TransPair{0, 0, 0.0});
     h2d(l2l_img_.pairs, pairs, st_);
+    // the U column (C = R) runs M2M and L2L on its own copies of the
+    // schedules, so that each copy keeps the tasks cut for one column count
+    l2l_img_u_.clear();
+    l2l_img_u_.segs = l2l_img_.segs;
+    l2l_img_u_.lev = l2l_img_.lev;
+    h2d(l2l_img_u_.pairs, pairs, st_);
+    m2m_u_.clear();
+    m2m_u_.segs = m2m_.segs;
+    m2m_u_.lev = m2m_.lev;
+    size_t np = 0;
+    for (const TransSeg& g : m2m_.segs) np = std::max(np, (size_t)(g.pair0 + g.npair));
+    std::vector<TransPair> mp = d2h(m2m_.pairs, std::max<size_t>(np, 1), st_);
+    h2d(m2m_u_.pairs, mp, st_);
   }
   img_sched_ = true;
   return IER_OK;
@@ -1653,13 +1666,13 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         p2m_img_twostage<float>(pa, R, mp);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, Cv, ops_->mats_f.get(), mp, mp);
-      run_translations(m2m_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
+      run_translations(m2m_u_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
       run_translations(m2lv_img_, Cv, ops_->mats_f.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
       run_translations(l2l_img_, Cv, ops_->mats_f.get(), lc, lc);
-      run_translations(l2l_img_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
+      run_translations(l2l_img_u_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     } else {
       img_mp_.resize(tot);
       img_lc_.resize(tot);
@@ -1673,13 +1686,13 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         p2m_img_twostage<double>(pa, R, mp);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
       run_translations(m2m_, Cv, ops_->mats.get(), mp, mp);
-      run_translations(m2m_, Cu, ops_->mats.get(), mp + nb * Cv * D, mp + nb * Cv * D);
+      run_translations(m2m_u_, Cu, ops_->mats.get(), mp + nb * Cv * D, mp + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
       run_translations(m2lv_img_, Cv, ops_->mats.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats.get(), mp + nb * Cv * D, lc + nb * Cv * D);
       EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
       run_translations(l2l_img_, Cv, ops_->mats.get(), lc, lc);
-      run_translations(l2l_img_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
+      run_translations(l2l_img_u_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     }
     EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
     L2TArgs la;
@@ -1696,7 +1709,18 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     la.c1 = 2.0 - al; la.alpha = al; la.mu = rmu;
     la.u_src = nullptr; la.e_src = nullptr; la.u_tgt = ut_s_.get(); la.e_tgt = et_s_.get();
     la.C = Cv + Cu; la.nsrc = n; la.ntgt = nt;
-    l2t_img_twostage(la, R, mixed ? nullptr : img_lc_.get(), mixed ? img_lc_f_.get() : nullptr);
+    bool done = false;
+    if (7 * R < 32) {
+      // few right-hand sides: the direct kernel on FP64 locals
+      if (mixed) {
+        img_lc_.resize(tot);
+        k_f2d_local<<<1184, 256, 0, st_>>>(tot, D, ops_->wnorm.get(), img_lc_f_.get(), img_lc_.get());
+        count_launch();
+      }
+      la.local = img_lc_.get();
+      done = launch_l2t_img(st_, nl2t_, la, R, (long long)(nb * Cv * D));
+    }
+    if (!done) l2t_img_twostage(la, R, mixed ? nullptr : img_lc_.get(), mixed ? img_lc_f_.get() : nullptr);
   } else {
     for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
   }

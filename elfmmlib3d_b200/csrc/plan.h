@@ -160,7 +160,7 @@ class Plan {
   int build_image_sched();
   void build_chunks(int do_src, int do_tgt);
   bool mindlin_ = false, img_sched_ = false;
-  TransSched m2lv_img_, m2lu_, l2l_img_;
+  TransSched m2lv_img_, m2lu_, l2l_img_, l2l_img_u_, m2m_u_;
   template <class T>
   void p2m_img_twostage(const P2MArgs& pa, int R, T* mpole);
   void l2t_img_twostage(const L2TArgs& la, int R, const double* local, const float* local_f);
