@@ -1407,7 +1407,7 @@ int Plan::build_image_sched() {
     m2m_u_.lev = m2m_.lev;
     size_t np = 0;
     for (const TransSeg& g : m2m_.segs) np = std::max(np, (size_t)(g.pair0 + g.npair));
-    std::vector<TransPair> mp = d2h(m2m_.pairs, std::max<size_t>(np, 1), st_);
+    std::vector<TransPair> mp = np ? d2h(m2m_.pairs, np, st_) : std::vector<TransPair>(1, TransPair{0, 0, 0.0});
     h2d(m2m_u_.pairs, mp, st_);
   }
   img_sched_ = true;
