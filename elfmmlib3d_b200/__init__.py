@@ -50,7 +50,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
+           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
 
 
 class ElfmmError(RuntimeError):
@@ -87,6 +87,12 @@ def load():
     L.efmm_plan_flops.argtypes = [_vp, _dp]
     L.efmm_plan_stored_bytes.restype = ctypes.c_longlong
     L.efmm_plan_stored_bytes.argtypes = [_vp]
+    L.efmm_plan_evaluate_batch_graph.restype = ctypes.c_int
+    L.efmm_plan_evaluate_batch_graph.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp,
+                                                 _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
+    L.efmm_plan_evaluate_image_graph.restype = ctypes.c_int
+    L.efmm_plan_evaluate_image_graph.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp,
+                                                 _vp, _vp, ctypes.c_int]
     L.efmm_plan_evaluate_image.restype = ctypes.c_int
     L.efmm_plan_evaluate_image.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp,
                                            _vp, ctypes.c_int, ctypes.c_int]
@@ -409,28 +415,38 @@ class Plan:
             raise ElfmmError(ier, "evaluate")
 
     def evaluate_batch(self, rlam, rmu, nrhs, ssl=None, sdl=None, u=None, e=None, ut=None, et=None,
-                       precision=0, mode=0):
+                       precision=0, mode=0, graph=False):
         """nrhs right-hand sides in one pass: ssl/sdl (nrhs,n,3); outputs
         (nrhs,n,3), (nrhs,n,3,3), (nrhs,nt,3), (nrhs,nt,3,3).  precision 0 =
         FP64, 1 = mixed (FP32 expansions and translations).  mode 1 stores the
         near-field interactions (geometry set with iter=True), mode 2 reuses
-        them."""
+        them.  graph=True replays repeated calls (same buffers) as one CUDA
+        graph (mode 0 or 2)."""
         args = (self._h, float(rlam), float(rmu), int(nrhs), self._ptr(ssl), self._ptr(sdl), self._ptr(u),
                 self._ptr(e), self._ptr(ut), self._ptr(et), int(precision))
-        if mode:
+        if graph:
+            ier = self._L.efmm_plan_evaluate_batch_graph(*args, int(mode))
+        elif mode:
             ier = self._L.efmm_plan_evaluate_batch_iter(*args, int(mode))
         else:
             ier = self._L.efmm_plan_evaluate_batch(*args)
         if ier:
             raise ElfmmError(ier, "evaluate_batch")
 
-    def evaluate_image(self, rlam, rmu, nrhs, ssl=None, sdl=None, ut=None, et=None, precision=0, mode=0):
+    def evaluate_image(self, rlam, rmu, nrhs, ssl=None, sdl=None, ut=None, et=None, precision=0, mode=0,
+                       graph=False):
         """Half-space image part at the points x whose reflections (x1, x2,
         -x3) were given as this plan's targets (set_geometry(..., mindlin=True)):
-        ssl/sdl (nrhs,n,3); outputs ut (nrhs,nt,3), et (nrhs,nt,3,3)."""
-        ier = self._L.efmm_plan_evaluate_image(self._h, float(rlam), float(rmu), int(nrhs), self._ptr(ssl),
-                                               self._ptr(sdl), self._ptr(ut), self._ptr(et), int(precision),
-                                               int(mode))
+        ssl/sdl (nrhs,n,3); outputs ut (nrhs,nt,3), et (nrhs,nt,3,3).
+        graph=True replays repeated mode-2 calls (same buffers) as one CUDA graph."""
+        if graph:
+            ier = self._L.efmm_plan_evaluate_image_graph(self._h, float(rlam), float(rmu), int(nrhs),
+                                                         self._ptr(ssl), self._ptr(sdl), self._ptr(ut),
+                                                         self._ptr(et), int(precision))
+        else:
+            ier = self._L.efmm_plan_evaluate_image(self._h, float(rlam), float(rmu), int(nrhs), self._ptr(ssl),
+                                                   self._ptr(sdl), self._ptr(ut), self._ptr(et), int(precision),
+                                                   int(mode))
         if ier:
             raise ElfmmError(ier, "evaluate_image")
 

@@ -111,6 +111,20 @@ extern "C" int efmm_plan_evaluate_image(efmm_plan* p, double rlam, double rmu, i
   EFMM_GUARD(return p->plan->evaluate_image(rlam, rmu, nrhs, ssl, sdl, u_tgt, e_tgt, precision, mode);)
 }
 
+extern "C" int efmm_plan_evaluate_batch_graph(efmm_plan* p, double rlam, double rmu, int nrhs, const double* ssl,
+                                              const double* sdl, double* u_src, double* e_src, double* u_tgt,
+                                              double* e_tgt, int precision, int mode) {
+  if (!p) return IER_BADARG;
+  EFMM_GUARD(return p->plan->evaluate_batch_graph(rlam, rmu, nrhs, ssl, sdl, u_src, e_src, u_tgt, e_tgt, precision,
+                                                  mode);)
+}
+
+extern "C" int efmm_plan_evaluate_image_graph(efmm_plan* p, double rlam, double rmu, int nrhs, const double* ssl,
+                                              const double* sdl, double* u_tgt, double* e_tgt, int precision) {
+  if (!p) return IER_BADARG;
+  EFMM_GUARD(return p->plan->evaluate_image_graph(rlam, rmu, nrhs, ssl, sdl, u_tgt, e_tgt, precision);)
+}
+
 extern "C" long long efmm_plan_stored_bytes(const efmm_plan* p) { return 8 * p->plan->stored_doubles(); }
 
 extern "C" void efmm_plan_flops(const efmm_plan* p, double* f5) { p->plan->flops_per_column(f5); }

@@ -1,5 +1,7 @@
 // plan.cu -- host orchestration: geometry -> tree -> work lists -> kernels.
 #include <algorithm>
+#include <functional>
+#include <cstdint>
 #include <map>
 #include <mutex>
 #include <vector>
@@ -254,15 +256,31 @@ Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
   for (int i = 0; i < 10; i++) EFMM_CUDA_TRY(cudaEventCreate(&ev_[i]));
 }
 Plan::~Plan() {
+  graph_reset();
   for (int i = 0; i < 10; i++) cudaEventDestroy(ev_[i]);
   for (cudaEvent_t e : pev_) cudaEventDestroy(e);
 }
 
 void Plan::product_begin() { npev_ = 0; }
 
+void WaveSet::upload(const std::vector<int>& wl, const std::vector<long long>& o1, const std::vector<long long>& o2,
+                     const std::vector<long long>& o3, const std::vector<GemmTask>& t, cudaStream_t st) {
+  h2d(leaves, wl, st);
+  h2d(off1, o1, st);
+  h2d(off2, o2, st);
+  h2d(off3, o3.empty() ? std::vector<long long>(1, 0) : o3, st);
+  h2d(tasks, t, st);
+  htasks = t;
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st));  // the host vectors may go away
+}
+
 template <class T>
-void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, const GemmTask* dtasks, const T* F,
-                         const T* W, T* C) {
+void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, long long t0, const GemmTask* dtasks,
+                         const T* F, const T* W, T* C) {
+  if (capturing_) {
+    gemm_product<T>(st_, ntask, dtasks, F, W, C);
+    return;
+  }
   if (npev_ + 2 > (int)pev_.size()) {
     cudaEvent_t a, b;
     EFMM_CUDA_TRY(cudaEventCreate(&a));
@@ -274,8 +292,10 @@ void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, const Ge
   gemm_product<T>(st_, ntask, dtasks, F, W, C);
   EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_ + 1], st_));
   npev_ += 2;
-  for (const GemmTask& t : tasks)
+  for (long long q = t0; q < t0 + ntask; q++) {
+    const GemmTask& t = tasks[q];
     product_flops_ += 2.0 * std::min(128, t.M - t.row0) * std::min(128, t.N - t.col0) * (double)t.K;
+  }
 }
 
 // after the pass's final synchronisation
@@ -320,6 +340,9 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   auto t0 = now();
   mindlin_ = mindlin;
   img_sched_ = false;
+  p2m_waves_.clear();  // the leaf lists change with the geometry
+  l2t_waves_.clear();
+  graph_reset();
   int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_);
   if (ier) return ier;
   auto t1 = now();
@@ -852,12 +875,15 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
   // right-hand sides per pass: at most 64 (near-field kernel), and the
   // expansions (2 x boxes x 4 rc x D doubles) within half the free memory
   int Rc = std::min(R, 64);
-  if (far_) {
+  if (capturing_) {
+    Rc = rc_last_;  // the warm pass before the capture sized the chunks
+  } else if (far_) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
     double have = 0.5 * (double)freeb + 8.0 * (double)(mpole_.cap + local_.cap);
     while (Rc > 1 && 16.0 * nb * 4 * Rc * D > have) Rc /= 2;
   }
+  rc_last_ = Rc;
   float tot = 0, near = 0, far = 0;
   product_ms_ = product_flops_ = 0;
   for (int r0 = 0; r0 < R; r0 += Rc) {
@@ -879,53 +905,68 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
 }
 
 // Two-stage P2M over waves of leaves whose node features and weights fit a
-// scratch budget (at most 8 GB or a quarter of the free memory).
+// scratch budget (at most 8 GB or a quarter of the free memory).  The waves
+// (leaves, offsets, product tasks) are built and uploaded once per column
+// count and element type; later passes (and graph captures) only launch.
 template <class T>
 void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
   const int D = 2 * ncoef(p_), C = 4 * R;
-  size_t freeb = 0, totb = 0;
-  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget_bytes =
-      std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double));
-  const size_t budget = budget_bytes / sizeof(T);  // elements
-  size_t i = 0;
-  const size_t nl = p2m_h_.size();
-  while (i < nl) {
+  WaveSet& W = p2m_waves_;
+  const long long key = ((long long)R << 8) | (sizeof(T) << 2) | 0;
+  if (W.key != key) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget =
+        std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double)) / sizeof(T);
+    W.clear();
     std::vector<int> wl;
     std::vector<long long> fo, wo, no;
-    long long nodes = 0;
     std::vector<GemmTask> tasks;
-    long long used = 0;
-    int max_nodes = 0;
+    size_t i = 0;
+    const size_t nl = p2m_h_.size();
     while (i < nl) {
-      const long long K = 48LL * p2m_sc_h_[i];
-      const long long need = K * D + K * C;
-      if (!wl.empty() && used + need > (long long)budget) break;
-      wl.push_back((int)i);
-      fo.push_back(used);
-      wo.push_back(used + K * D);
-      no.push_back(nodes);
-      nodes += 12LL * p2m_sc_h_[i];
-      const int box = p2m_h_[i];
-      for (int c0 = 0; c0 < C; c0 += 128)
-        for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, used + K * D, (long long)box * C * D, D, C, (int)K, D, (int)K, D, r0, c0});
-      used += need;
-      max_nodes = std::max(max_nodes, 12 * p2m_sc_h_[i]);
-      i++;
+      WaveSet::Wave w{0, (long long)wl.size(), 0, (long long)tasks.size(), 0, 0, 0};
+      long long used = 0, nodes = 0;
+      while (i < nl) {
+        const long long K = 48LL * p2m_sc_h_[i];
+        const long long need = K * D + K * C;
+        if (w.nwl > 0 && used + need > (long long)budget) break;
+        wl.push_back((int)i);
+        fo.push_back(used);
+        wo.push_back(used + K * D);
+        no.push_back(nodes);
+        nodes += 12LL * p2m_sc_h_[i];
+        const int box = p2m_h_[i];
+        for (int c0 = 0; c0 < C; c0 += 128)
+          for (int r0 = 0; r0 < D; r0 += 128)
+            tasks.push_back({used, used + K * D, (long long)box * C * D, D, C, (int)K, D, (int)K, D, r0, c0});
+        used += need;
+        w.maxn = std::max(w.maxn, 12 * p2m_sc_h_[i]);
+        w.nwl++;
+        i++;
+      }
+      w.ntask = (int)(tasks.size() - w.t0);
+      w.used = used;
+      w.nodes = nodes;
+      W.w.push_back(w);
     }
-    p2m_scratch_.resize(((size_t)used * sizeof(T) + sizeof(double) - 1) / sizeof(double));
-    h2d(wave_leaves_, wl, st_);
-    h2d(wave_foff_, fo, st_);
-    h2d(wave_woff_, wo, st_);
-    h2d(wave_tasks_, tasks, st_);
-    h2d(wave_noff_, no, st_);
-    wave_nrec_.resize(8 * (size_t)std::max(nodes, 1LL));
-    T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
-    launch_p2m_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
-                           wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
-                           wave_tasks_.get(), mpole, false);
-    product_timed<T>((int)tasks.size(), tasks, wave_tasks_.get(), scratch, scratch, mpole);
+    W.upload(wl, fo, wo, no, tasks, st_);
+    W.key = key;
+  }
+  size_t maxu = 1;
+  long long maxnodes = 1;
+  for (const auto& w : W.w) {
+    maxu = std::max(maxu, (size_t)w.used);
+    maxnodes = std::max(maxnodes, w.nodes);
+  }
+  p2m_scratch_.resize((maxu * sizeof(T) + sizeof(double) - 1) / sizeof(double));
+  wave_nrec_.resize(8 * (size_t)maxnodes);
+  T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
+  for (const auto& w : W.w) {
+    launch_p2m_twostage<T>(st_, pa, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0, W.off2.get() + w.wl0,
+                           W.off3.get() + w.wl0, wave_nrec_.get(), w.maxn, scratch, scratch, w.ntask,
+                           W.tasks.get() + w.t0, mpole, false);
+    product_timed<T>(w.ntask, W.htasks, w.t0, W.tasks.get() + w.t0, scratch, scratch, mpole);
   }
 }
 template void Plan::p2m_twostage<double>(const P2MArgs&, int, double*);
@@ -940,51 +981,63 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
   L2TArgs la = la0;
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
-  size_t freeb = 0, totb = 0;
-  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
-  size_t i = 0;
-  const size_t nl = l2t_h_.size();
-  while (i < nl) {
+  WaveSet& W = l2t_waves_;
+  const long long key = ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1;
+  if (W.key != key) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    W.clear();
     std::vector<int> wl;
     std::vector<long long> go, so;
     std::vector<GemmTask> tasks;
-    long long used = 0;
-    int max_pts = 0;
+    size_t i = 0;
+    const size_t nl = l2t_h_.size();
     while (i < nl) {
-      const int P = (do_src ? l2t_sc_h_[i] : 0) + (do_tgt ? l2t_tc_h_[i] : 0);
-      if (P == 0) {
+      WaveSet::Wave w{0, (long long)wl.size(), 0, (long long)tasks.size(), 0, 0, 0};
+      long long used = 0;
+      while (i < nl) {
+        const int P = (do_src ? l2t_sc_h_[i] : 0) + (do_tgt ? l2t_tc_h_[i] : 0);
+        if (P == 0) {
+          i++;
+          continue;
+        }
+        const int LD = 9 * P + ((9 * P) & 1);  // even leading dimension (16-byte vector loads)
+        const long long need = (long long)D * LD + (long long)C * LD;
+        if (w.nwl > 0 && used + need > (long long)budget) break;
+        wl.push_back((int)i);
+        go.push_back(used);
+        so.push_back(used + (long long)D * LD);
+        const int box = l2t_h_[i];
+        for (int c0 = 0; c0 < C; c0 += 128)
+          for (int r0 = 0; r0 < 9 * P; r0 += 128)
+            tasks.push_back({used, (long long)box * C * D, used + (long long)D * LD, 9 * P, C, D, LD, D, LD, r0, c0});
+        used += need;
+        w.maxn = std::max(w.maxn, P);
+        w.nwl++;
         i++;
-        continue;
       }
-      const int LD = 9 * P + ((9 * P) & 1);  // even leading dimension (16-byte vector loads)
-      const long long need = (long long)D * LD + (long long)C * LD;
-      if (!wl.empty() && used + need > (long long)budget) break;
-      wl.push_back((int)i);
-      go.push_back(used);
-      so.push_back(used + (long long)D * LD);
-      const int box = l2t_h_[i];
-      for (int c0 = 0; c0 < C; c0 += 128)
-        for (int r0 = 0; r0 < 9 * P; r0 += 128)
-          tasks.push_back({used, (long long)box * C * D, used + (long long)D * LD, 9 * P, C, D, LD, D, LD, r0, c0});
-      used += need;
-      max_pts = std::max(max_pts, P);
-      i++;
+      if (w.nwl == 0) break;
+      w.ntask = (int)(tasks.size() - w.t0);
+      w.used = used;
+      W.w.push_back(w);
     }
-    if (wl.empty()) break;
-    l2t_scratch_.resize(((size_t)used * esz + sizeof(double) - 1) / sizeof(double));
-    h2d(wave_leaves_, wl, st_);
-    h2d(wave_foff_, go, st_);
-    h2d(wave_woff_, so, st_);
-    h2d(wave_tasks_, tasks, st_);
+    W.upload(wl, go, so, {}, tasks, st_);
+    W.key = key;
+  }
+  size_t maxu = 1;
+  for (const auto& w : W.w) maxu = std::max(maxu, (size_t)w.used);
+  l2t_scratch_.resize((maxu * esz + sizeof(double) - 1) / sizeof(double));
+  for (const auto& w : W.w) {
     if (mixed) {
       float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
-      launch_l2t_twostage<float>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
-                                 max_pts, sc, sc, (int)tasks.size(), wave_tasks_.get(), local_f_.get());
+      launch_l2t_twostage<float>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                                 W.off2.get() + w.wl0, w.maxn, sc, sc, w.ntask, W.tasks.get() + w.t0,
+                                 local_f_.get());
     } else {
-      launch_l2t_twostage<double>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(),
-                                  wave_woff_.get(), max_pts, l2t_scratch_.get(), l2t_scratch_.get(),
-                                  (int)tasks.size(), wave_tasks_.get(), local_.get());
+      launch_l2t_twostage<double>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                                  W.off2.get() + w.wl0, w.maxn, l2t_scratch_.get(), l2t_scratch_.get(), w.ntask,
+                                  W.tasks.get() + w.t0, local_.get());
     }
   }
 }
@@ -999,7 +1052,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   const size_t nb = tr_.nboxes;
   long long launch0 = launches_total();
   product_begin();
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  rec(0);
   ssl_s_.resize(3 * (size_t)n * R);
   sdl_s_.resize(3 * (size_t)n * R);
   const int gb = (int)(((long long)n * R + 255) / 256);
@@ -1014,7 +1067,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   ut_s_.zero(st_);
   et_s_.zero(st_);
   const double c1 = (rlam + rmu) / (rlam + 2 * rmu), c2 = rmu / (rlam + 2 * rmu);
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  rec(1);
   const int C = 4 * R;
   if (far_ && (do_src || do_tgt)) {
     if (mixed) {
@@ -1051,11 +1104,11 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     if (mixed) {
       pa.wnorm = ops_->wnorm.get();  // multipoles in the normalised basis
       p2m_twostage<float>(pa, R, mpole_f_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      rec(2);
       run_translations(m2m_, C, ops_->mats_f.get(), mpole_f_.get(), mpole_f_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      rec(3);
       run_translations(m2l_, C, ops_->mats_f.get(), mpole_f_.get(), local_f_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      rec(4);
       run_translations(l2l_, C, ops_->mats_f.get(), local_f_.get(), local_f_.get());
     } else {
       // product form once the columns fill its tiles
@@ -1063,14 +1116,14 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         launch_p2m(st_, np2m_, pa, R);
       else
         p2m_twostage<double>(pa, R, mpole_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      rec(2);
       run_translations(m2m_, C, ops_->mats.get(), mpole_.get(), mpole_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      rec(3);
       run_translations(m2l_, C, ops_->mats.get(), mpole_.get(), local_.get());
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      rec(4);
       run_translations(l2l_, C, ops_->mats.get(), local_.get(), local_.get());
     }
-    EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
+    rec(5);
     L2TArgs la;
     la.leaves = l2t_leaves_.get();
     la.level = tr_.level.get(); la.ijk = tr_.ijk.get();
@@ -1121,9 +1174,9 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       launch_l2t(st_, nl2t_, la, R);
     }
   } else {
-    for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+    for (int i = 2; i <= 5; i++) rec(i);
   }
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
+  rec(6);
   // near field: frames only (densities enter the batched contraction; the
   // stored operator, when replayed, replaces them)
   trir_.resize(n);
@@ -1164,7 +1217,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, (ds_src || ds_tgt) ? 1 : 0,
                       ssl_s_.get(), sdl_s_.get(), n, n, nt, mode ? near_base_.get() : nullptr,
                       mode ? near_ntri_.get() : nullptr, mode ? store_.get() : nullptr);
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
+  rec(7);
   if (do_src) {
     k_scatter_out<<<dim3((n + 255) / 256, R), 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src,
                                                               d_e_src); count_launch();
@@ -1173,8 +1226,9 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     k_scatter_out<<<dim3((nt + 255) / 256, R), 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(),
                                                                d_u_tgt, d_e_tgt); count_launch();
   }
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+  rec(8);
   EFMM_CUDA_TRY(cudaGetLastError());
+  if (capturing_) return IER_OK;  // the graph is launched and timed by its caller
   EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
   cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
   cudaEventElapsedTime(&timings.prep, ev_[0], ev_[1]);
@@ -1221,6 +1275,89 @@ int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const do
   cudaEventElapsedTime(&timings.near, ev_[0], ev_[1]);
   timings.total = timings.near;
   return IER_OK;
+}
+
+// ---------------------------------------------------------- CUDA graphs
+// A repeated evaluation on the same geometry, buffers and parameters is
+// captured once into a CUDA graph and then replayed with one launch: the
+// first call runs the pass normally (allocations, operator and schedule
+// caches, wave lists), the second identical pass is captured, and every
+// later call with the same key launches the graph.  During the capture no
+// host synchronisation, allocation or upload happens (the caches are warm;
+// event timing and error checks are skipped and done around the launch).
+void Plan::rec(int i) {
+  if (!capturing_) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+}
+
+void Plan::graph_reset() {
+  if (gexec_) cudaGraphExecDestroy(gexec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  gexec_ = nullptr;
+  graph_ = nullptr;
+  gkey_.clear();
+}
+
+int Plan::run_graph(const std::vector<double>& key, const std::function<int()>& pass) {
+  if (gexec_ && key == gkey_) {
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+    EFMM_CUDA_TRY(cudaGraphLaunch(gexec_, st_));
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+    count_launch((int)graph_launches_);
+    EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
+    cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
+    launches_ = (int)graph_launches_;
+    if (tc_take_error()) return IER_CUDA;
+    return IER_OK;
+  }
+  graph_reset();
+  int ier = pass();  // warm pass: caches and buffers in place
+  if (ier) return ier;
+  const long long l0 = launches_total();
+  capturing_ = true;
+  EFMM_CUDA_TRY(cudaStreamBeginCapture(st_, cudaStreamCaptureModeThreadLocal));
+  cudaGraph_t g = nullptr;
+  try {
+    ier = pass();
+  } catch (...) {
+    capturing_ = false;
+    cudaStreamEndCapture(st_, &g);
+    if (g) cudaGraphDestroy(g);
+    throw;
+  }
+  capturing_ = false;
+  const cudaError_t e = cudaStreamEndCapture(st_, &g);
+  graph_launches_ = launches_total() - l0;
+  count_launch(-(int)graph_launches_);  // captured, not launched
+  if (ier || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    return ier ? ier : IER_CUDA;
+  }
+  graph_ = g;
+  EFMM_CUDA_TRY(cudaGraphInstantiate(&gexec_, graph_, 0));
+  gkey_ = key;
+  return run_graph(key, pass);
+}
+
+int Plan::evaluate_batch_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                               double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
+                               int mode) {
+  if (mode != 0 && mode != 2) return IER_BADARG;
+  const std::vector<double> key = {1.0, rlam, rmu, (double)R, (double)(uintptr_t)d_ssl, (double)(uintptr_t)d_sdl,
+                                   (double)(uintptr_t)d_u_src, (double)(uintptr_t)d_e_src,
+                                   (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision,
+                                   (double)mode};
+  return run_graph(key, [&]() {
+    return evaluate_batch(rlam, rmu, R, d_ssl, d_sdl, d_u_src, d_e_src, d_u_tgt, d_e_tgt, precision, mode);
+  });
+}
+
+int Plan::evaluate_image_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                               double* d_u_tgt, double* d_e_tgt, int precision) {
+  const std::vector<double> key = {2.0, rlam, rmu, (double)R, (double)(uintptr_t)d_ssl, (double)(uintptr_t)d_sdl,
+                                   (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision};
+  return run_graph(key, [&]() {
+    return evaluate_image(rlam, rmu, R, d_ssl, d_sdl, d_u_tgt, d_e_tgt, precision, 2);
+  });
 }
 
 // ------------------------------------------------------ half-space image
@@ -1317,6 +1454,8 @@ void Plan::ensure_uops() {
 
 void Plan::ensure_mats_f() {
   std::lock_guard<std::mutex> lk(g_ops_mu);
+  if (ops_->mats_f.size() == ops_->mats.size() && (!ops_->u_ready || ops_->umats_f.size() == ops_->umats.size()))
+    return;
   if (ops_->mats_f.size() != ops_->mats.size()) {
     ops_->mats_f.resize(ops_->mats.size());
     k_ops_normalised<<<(int)ops_->dims.size(), 256, 0, st_>>>(ops_->kinds.get(), ops_->off.get(), ops_->dim.get(),
@@ -1441,68 +1580,85 @@ void Plan::build_chunks(int do_src, int do_tgt) {
 }
 
 // Two-stage P2M of the image columns over waves of leaves (budget as in
-// p2m_twostage): 9 feature rows per node, 7R columns (6R Laplace, R of U).
+// p2m_twostage, waves cached likewise): 9 feature rows per node, 7R columns
+// (6R Laplace, R of U).
 template <class T>
 void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
   const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R;
   const size_t nb = tr_.nboxes;
-  size_t freeb = 0, totb = 0;
-  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget_bytes = std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double));
-  const size_t budget = budget_bytes / sizeof(T);
-  size_t i = 0;
-  const size_t nl = p2m_h_.size();
-  while (i < nl) {
+  WaveSet& W = p2m_waves_;
+  const long long key = ((long long)R << 8) | (sizeof(T) << 2) | 2;
+  if (W.key != key) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget =
+        std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double)) / sizeof(T);
+    W.clear();
     std::vector<int> wl;
     std::vector<long long> fo, wo, no;
     std::vector<GemmTask> tasks;
-    long long nodes = 0, used = 0;
-    int max_nodes = 0;
+    size_t i = 0;
+    const size_t nl = p2m_h_.size();
     while (i < nl) {
-      // features: 4 charge/dipole rows per node, then 5 second-derivative
-      // rows per node; the anti-image columns (4R, no quadrupole sources)
-      // multiply the first block only
-      const long long K = 108LL * p2m_sc_h_[i], K4 = 48LL * p2m_sc_h_[i];
-      const long long need = K * D + K * (Cv + Cu);
-      if (!wl.empty() && used + need > (long long)budget) break;
-      wl.push_back((int)i);
-      fo.push_back(used);
-      wo.push_back(used + K * D);
-      no.push_back(nodes);
-      nodes += 12LL * p2m_sc_h_[i];
-      const long long box = p2m_h_[i], wb = used + K * D;
-      const int CA = 4 * R, CP = 2 * R;
-      for (int c0 = 0; c0 < CA; c0 += 128)
-        for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, wb, box * Cv * D, D, CA, (int)K4, D, (int)K, D, r0, c0});
-      for (int c0 = 0; c0 < CP; c0 += 128)
-        for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, wb + (long long)CA * K, box * Cv * D + (long long)CA * D, D, CP, (int)K, D, (int)K, D,
-                           r0, c0});
-      for (int c0 = 0; c0 < Cu; c0 += 128)
-        for (int r0 = 0; r0 < D; r0 += 128)
-          tasks.push_back({used, wb + (long long)Cv * K, (long long)(nb * Cv * D) + box * Cu * D, D, Cu, (int)K, D,
-                           (int)K, D, r0, c0});
-      used += need;
-      max_nodes = std::max(max_nodes, 12 * p2m_sc_h_[i]);
-      i++;
+      WaveSet::Wave w{0, (long long)wl.size(), 0, (long long)tasks.size(), 0, 0, 0};
+      long long used = 0, nodes = 0;
+      while (i < nl) {
+        // features: 4 charge/dipole rows per node, then 5 second-derivative
+        // rows per node; the anti-image columns (4R, no quadrupole sources)
+        // multiply the first block only
+        const long long K = 108LL * p2m_sc_h_[i], K4 = 48LL * p2m_sc_h_[i];
+        const long long need = K * D + K * (Cv + Cu);
+        if (w.nwl > 0 && used + need > (long long)budget) break;
+        wl.push_back((int)i);
+        fo.push_back(used);
+        wo.push_back(used + K * D);
+        no.push_back(nodes);
+        nodes += 12LL * p2m_sc_h_[i];
+        const long long box = p2m_h_[i], wb = used + K * D;
+        const int CA = 4 * R, CP = 2 * R;
+        for (int c0 = 0; c0 < CA; c0 += 128)
+          for (int r0 = 0; r0 < D; r0 += 128)
+            tasks.push_back({used, wb, box * Cv * D, D, CA, (int)K4, D, (int)K, D, r0, c0});
+        for (int c0 = 0; c0 < CP; c0 += 128)
+          for (int r0 = 0; r0 < D; r0 += 128)
+            tasks.push_back({used, wb + (long long)CA * K, box * Cv * D + (long long)CA * D, D, CP, (int)K, D,
+                             (int)K, D, r0, c0});
+        for (int c0 = 0; c0 < Cu; c0 += 128)
+          for (int r0 = 0; r0 < D; r0 += 128)
+            tasks.push_back({used, wb + (long long)Cv * K, (long long)(nb * Cv * D) + box * Cu * D, D, Cu, (int)K,
+                             D, (int)K, D, r0, c0});
+        used += need;
+        w.maxn = std::max(w.maxn, 12 * p2m_sc_h_[i]);
+        w.nwl++;
+        i++;
+      }
+      w.ntask = (int)(tasks.size() - w.t0);
+      w.used = used;
+      w.nodes = nodes;
+      W.w.push_back(w);
     }
-    p2m_scratch_.resize(((size_t)used * sizeof(T) + sizeof(double) - 1) / sizeof(double));
-    h2d(wave_leaves_, wl, st_);
-    h2d(wave_foff_, fo, st_);
-    h2d(wave_woff_, wo, st_);
-    h2d(wave_tasks_, tasks, st_);
-    h2d(wave_noff_, no, st_);
-    wave_nrec_.resize(8 * (size_t)std::max(nodes, 1LL));
-    T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
-    launch_p2m_img_twostage<T>(st_, pa, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
-                               wave_noff_.get(), wave_nrec_.get(), max_nodes, scratch, scratch, (int)tasks.size(),
-                               wave_tasks_.get(), mpole, false);
-    product_timed<T>((int)tasks.size(), tasks, wave_tasks_.get(), scratch, scratch, mpole);
+    W.upload(wl, fo, wo, no, tasks, st_);
+    W.key = key;
+  }
+  size_t maxu = 1;
+  long long maxnodes = 1;
+  for (const auto& w : W.w) {
+    maxu = std::max(maxu, (size_t)w.used);
+    maxnodes = std::max(maxnodes, w.nodes);
+  }
+  p2m_scratch_.resize((maxu * sizeof(T) + sizeof(double) - 1) / sizeof(double));
+  wave_nrec_.resize(8 * (size_t)maxnodes);
+  T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
+  for (const auto& w : W.w) {
+    launch_p2m_img_twostage<T>(st_, pa, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                               W.off2.get() + w.wl0, W.off3.get() + w.wl0, wave_nrec_.get(), w.maxn, scratch,
+                               scratch, w.ntask, W.tasks.get() + w.t0, mpole, false);
+    product_timed<T>(w.ntask, W.htasks, w.t0, W.tasks.get() + w.t0, scratch, scratch, mpole);
   }
 }
 
-// Two-stage L2T of the image columns at the targets (waves as in l2t_twostage).
+// Two-stage L2T of the image columns at the targets (waves cached as in
+// l2t_twostage).
 void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, const float* local_f) {
   const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R, C = Cv + Cu;
   const size_t nb = tr_.nboxes;
@@ -1510,55 +1666,66 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
   L2TArgs la = la0;
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
-  size_t freeb = 0, totb = 0;
-  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-  const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
-  size_t i = 0;
-  const size_t nl = l2t_h_.size();
-  while (i < nl) {
+  WaveSet& W = l2t_waves_;
+  const long long key = ((long long)R << 8) | (esz << 4) | 3;
+  if (W.key != key) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    W.clear();
     std::vector<int> wl;
     std::vector<long long> go, so;
     std::vector<GemmTask> tasks;
-    long long used = 0;
-    int max_pts = 0;
+    size_t i = 0;
+    const size_t nl = l2t_h_.size();
     while (i < nl) {
-      const int P = l2t_tc_h_[i];
-      if (P == 0) {
+      WaveSet::Wave w{0, (long long)wl.size(), 0, (long long)tasks.size(), 0, 0, 0};
+      long long used = 0;
+      while (i < nl) {
+        const int P = l2t_tc_h_[i];
+        if (P == 0) {
+          i++;
+          continue;
+        }
+        const int LD = 9 * P + ((9 * P) & 1);
+        const long long need = (long long)D * LD + (long long)C * LD;
+        if (w.nwl > 0 && used + need > (long long)budget) break;
+        wl.push_back((int)i);
+        go.push_back(used);
+        so.push_back(used + (long long)D * LD);
+        const long long box = l2t_h_[i];
+        for (int c0 = 0; c0 < Cv; c0 += 128)
+          for (int r0 = 0; r0 < 9 * P; r0 += 128)
+            tasks.push_back({used, box * Cv * D, used + (long long)D * LD, 9 * P, Cv, D, LD, D, LD, r0, c0});
+        for (int c0 = 0; c0 < Cu; c0 += 128)
+          for (int r0 = 0; r0 < 9 * P; r0 += 128)
+            tasks.push_back({used, (long long)(nb * Cv * D) + box * Cu * D,
+                             used + (long long)D * LD + (long long)Cv * LD, 9 * P, Cu, D, LD, D, LD, r0, c0});
+        used += need;
+        w.maxn = std::max(w.maxn, P);
+        w.nwl++;
         i++;
-        continue;
       }
-      const int LD = 9 * P + ((9 * P) & 1);
-      const long long need = (long long)D * LD + (long long)C * LD;
-      if (!wl.empty() && used + need > (long long)budget) break;
-      wl.push_back((int)i);
-      go.push_back(used);
-      so.push_back(used + (long long)D * LD);
-      const long long box = l2t_h_[i];
-      for (int c0 = 0; c0 < Cv; c0 += 128)
-        for (int r0 = 0; r0 < 9 * P; r0 += 128)
-          tasks.push_back({used, box * Cv * D, used + (long long)D * LD, 9 * P, Cv, D, LD, D, LD, r0, c0});
-      for (int c0 = 0; c0 < Cu; c0 += 128)
-        for (int r0 = 0; r0 < 9 * P; r0 += 128)
-          tasks.push_back({used, (long long)(nb * Cv * D) + box * Cu * D, used + (long long)D * LD + (long long)Cv * LD,
-                           9 * P, Cu, D, LD, D, LD, r0, c0});
-      used += need;
-      max_pts = std::max(max_pts, P);
-      i++;
+      if (w.nwl == 0) break;
+      w.ntask = (int)(tasks.size() - w.t0);
+      w.used = used;
+      W.w.push_back(w);
     }
-    if (wl.empty()) break;
-    l2t_scratch_.resize(((size_t)used * esz + sizeof(double) - 1) / sizeof(double));
-    h2d(wave_leaves_, wl, st_);
-    h2d(wave_foff_, go, st_);
-    h2d(wave_woff_, so, st_);
-    h2d(wave_tasks_, tasks, st_);
+    W.upload(wl, go, so, {}, tasks, st_);
+    W.key = key;
+  }
+  size_t maxu = 1;
+  for (const auto& w : W.w) maxu = std::max(maxu, (size_t)w.used);
+  l2t_scratch_.resize((maxu * esz + sizeof(double) - 1) / sizeof(double));
+  for (const auto& w : W.w) {
     if (mixed) {
       float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
-      launch_l2t_twostage<float>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(), wave_woff_.get(),
-                                 max_pts, sc, sc, (int)tasks.size(), wave_tasks_.get(), local_f, true);
+      launch_l2t_twostage<float>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                                 W.off2.get() + w.wl0, w.maxn, sc, sc, w.ntask, W.tasks.get() + w.t0, local_f, true);
     } else {
-      launch_l2t_twostage<double>(st_, la, R, (int)wl.size(), wave_leaves_.get(), wave_foff_.get(),
-                                  wave_woff_.get(), max_pts, l2t_scratch_.get(), l2t_scratch_.get(),
-                                  (int)tasks.size(), wave_tasks_.get(), local, true);
+      launch_l2t_twostage<double>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                                  W.off2.get() + w.wl0, w.maxn, l2t_scratch_.get(), l2t_scratch_.get(), w.ntask,
+                                  W.tasks.get() + w.t0, local, true);
     }
   }
 }
@@ -1593,12 +1760,15 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
   const int n = n_, D = 2 * ncoef(p_);
   const size_t nb = tr_.nboxes;
   int Rc = std::min(R, 64);
-  if (far_) {
+  if (capturing_) {
+    Rc = rc_last_;
+  } else if (far_) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
     const double have = 0.5 * (double)freeb + 8.0 * (double)(img_mp_.cap + img_lc_.cap);
     while (Rc > 1 && 3.0 * 8.0 * nb * 7 * Rc * D > have) Rc /= 2;
   }
+  rc_last_ = Rc;
   float tot = 0;
   product_ms_ = product_flops_ = 0;
   for (int r0 = 0; r0 < R; r0 += Rc) {
@@ -1625,7 +1795,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   const size_t nb = tr_.nboxes;
   long long launch0 = launches_total();
   product_begin();
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+  rec(0);
   ssl_s_.resize(3 * (size_t)n * R);
   sdl_s_.resize(3 * (size_t)n * R);
   const int gb = (int)(((long long)n * R + 255) / 256);
@@ -1636,7 +1806,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   ut_s_.zero(st_);
   et_s_.zero(st_);
   const double al = (rlam + rmu) / (rlam + 2 * rmu);
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+  rec(1);
   const int Cv = 6 * R, Cu = R;
   if (far_) {
     const size_t tot = nb * (size_t)(Cv + Cu) * D;
@@ -1664,13 +1834,13 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         launch_p2m_img<float>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
       else
         p2m_img_twostage<float>(pa, R, mp);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      rec(2);
       run_translations(m2m_, Cv, ops_->mats_f.get(), mp, mp);
       run_translations(m2m_u_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      rec(3);
       run_translations(m2lv_img_, Cv, ops_->mats_f.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      rec(4);
       run_translations(l2l_img_, Cv, ops_->mats_f.get(), lc, lc);
       run_translations(l2l_img_u_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     } else {
@@ -1684,17 +1854,17 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         launch_p2m_img<double>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
       else
         p2m_img_twostage<double>(pa, R, mp);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
+      rec(2);
       run_translations(m2m_, Cv, ops_->mats.get(), mp, mp);
       run_translations(m2m_u_, Cu, ops_->mats.get(), mp + nb * Cv * D, mp + nb * Cv * D);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[3], st_));
+      rec(3);
       run_translations(m2lv_img_, Cv, ops_->mats.get(), mp, lc);
       run_dense(m2lu_, Cu, ops_->umats.get(), mp + nb * Cv * D, lc + nb * Cv * D);
-      EFMM_CUDA_TRY(cudaEventRecord(ev_[4], st_));
+      rec(4);
       run_translations(l2l_img_, Cv, ops_->mats.get(), lc, lc);
       run_translations(l2l_img_u_, Cu, ops_->mats.get(), lc + nb * Cv * D, lc + nb * Cv * D);
     }
-    EFMM_CUDA_TRY(cudaEventRecord(ev_[5], st_));
+    rec(5);
     L2TArgs la;
     la.leaves = l2t_leaves_.get();
     la.level = tr_.level.get(); la.ijk = tr_.ijk.get();
@@ -1722,9 +1892,9 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     }
     if (!done) l2t_img_twostage(la, R, mixed ? nullptr : img_lc_.get(), mixed ? img_lc_f_.get() : nullptr);
   } else {
-    for (int i = 2; i <= 5; i++) EFMM_CUDA_TRY(cudaEventRecord(ev_[i], st_));
+    for (int i = 2; i <= 5; i++) rec(i);
   }
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
+  rec(6);
   // near field: refined quadrature of the whole image kernel, stored, then
   // contracted with the right-hand sides
   build_chunks(0, 1);
@@ -1753,12 +1923,13 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   na.u_src = nullptr; na.e_src = nullptr; na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
   launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, dstr, ssl_s_.get(), sdl_s_.get(), n, n,
                     nt, near_base_.get(), near_ntri_.get(), store_.get());
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[7], st_));
+  rec(7);
   k_scatter_out<<<dim3((nt + 255) / 256, R), 256, 0, st_>>>(nt, tr_.izt.get(), ut_s_.get(), et_s_.get(), d_u_tgt,
                                                              d_e_tgt);
   count_launch();
-  EFMM_CUDA_TRY(cudaEventRecord(ev_[8], st_));
+  rec(8);
   EFMM_CUDA_TRY(cudaGetLastError());
+  if (capturing_) return IER_OK;  // the graph is launched and timed by its caller
   EFMM_CUDA_TRY(cudaEventSynchronize(ev_[8]));
   cudaEventElapsedTime(&timings.total, ev_[0], ev_[8]);
   cudaEventElapsedTime(&timings.prep, ev_[0], ev_[1]);

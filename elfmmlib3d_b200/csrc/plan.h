@@ -1,6 +1,7 @@
 // plan.h -- host orchestration of one elastostatic layer-potential evaluation.
 #pragma once
 #include <vector>
+#include <functional>
 #include <utility>
 #include "devbuf.h"
 #include "tree.h"
@@ -86,6 +87,33 @@ struct TransSched {
   }
 };
 
+// Waves of leaves for the two-stage P2M / L2T products: per wave the leaf
+// range, its product tasks and scratch extent, uploaded once per key (kind,
+// column count, element type) and reused by every later pass.
+struct WaveSet {
+  struct Wave {
+    int nwl;
+    long long wl0;
+    int ntask;
+    long long t0;
+    int maxn;
+    long long used, nodes;
+  };
+  long long key = -1;
+  std::vector<Wave> w;
+  std::vector<GemmTask> htasks;
+  DevBuf<int> leaves;
+  DevBuf<long long> off1, off2, off3;
+  DevBuf<GemmTask> tasks;
+  void clear() {
+    key = -1;
+    w.clear();
+    htasks.clear();
+  }
+  void upload(const std::vector<int>& wl, const std::vector<long long>& o1, const std::vector<long long>& o2,
+              const std::vector<long long>& o3, const std::vector<GemmTask>& t, cudaStream_t st);
+};
+
 class Plan {
  public:
   Plan(int device, cudaStream_t stream);
@@ -126,6 +154,16 @@ class Plan {
   // near-field blocks for this call only).
   int evaluate_image(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                      double* d_u_tgt, double* d_e_tgt, int precision = 0, int mode = 0);
+  // The same calls replayed as one CUDA graph: the first call with a new
+  // key (parameters and device pointers) runs the pass, captures a second
+  // identical pass and launches the graph; later calls with the same key
+  // only launch it.  Batch: mode 0 or 2 (the store made by an earlier mode-1
+  // call); image: mode 2.  New data must be written into the same buffers.
+  int evaluate_batch_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                           double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
+                           int mode);
+  int evaluate_image_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
+                           double* d_u_tgt, double* d_e_tgt, int precision);
   // useful flops per expansion column of one pass: P2M, M2M, M2L, L2L, L2T
   void flops_per_column(double* f5) const;
   // all-pairs direct sum on the same geometry (no tree needed)
@@ -175,8 +213,18 @@ class Plan {
   void product_end();
   void product_collect();
   template <class T>
-  void product_timed(int ntask, const std::vector<GemmTask>& tasks, const GemmTask* dtasks, const T* F, const T* W,
-                     T* C);
+  void product_timed(int ntask, const std::vector<GemmTask>& tasks, long long t0, const GemmTask* dtasks, const T* F,
+                     const T* W, T* C);
+  WaveSet p2m_waves_, l2t_waves_;
+  bool capturing_ = false;
+  int rc_last_ = 64;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t gexec_ = nullptr;
+  std::vector<double> gkey_;
+  long long graph_launches_ = 0;
+  void rec(int i);
+  void graph_reset();
+  int run_graph(const std::vector<double>& key, const std::function<int()>& pass);
   DevBuf<float> img_mp_f_, img_lc_f_;
   DevBuf<float> mpole_f_, local_f_;
   DevBuf<int> chunk_leaf_, chunk_e0_;  // (near leaf, first point) per batched near-field CTA

@@ -217,6 +217,22 @@ double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, un
  * != 0 if a bounded wait in the kernel ran out.  Returns 0 or an ier. */
 int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
 
+/* Repeated batched evaluations as one CUDA graph (no counterpart in the
+ * reference): the same arguments as efmm_plan_evaluate_batch_iter /
+ * efmm_plan_evaluate_image.  The first call with new arguments (parameters
+ * and device pointers) runs the pass, captures a second identical pass and
+ * launches it; later calls with the same arguments launch the captured
+ * graph only, so new densities must be written into the same buffers.
+ * Batch: mode 0 (analytic near field) or 2 (a store made by an earlier
+ * mode-1 call); image: the stored near field of an earlier mode-1 call.
+ * The first call should not run while another capture on the plan's stream
+ * is in progress.  A new geometry drops the graph. */
+int efmm_plan_evaluate_batch_graph(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
+                                   const double *sdl, double *u_src, double *e_src, double *u_tgt,
+                                   double *e_tgt, int precision, int mode);
+int efmm_plan_evaluate_image_graph(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
+                                   const double *sdl, double *u_tgt, double *e_tgt, int precision);
+
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 
