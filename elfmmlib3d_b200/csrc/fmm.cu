@@ -575,6 +575,550 @@ k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const
   }
 }
 
+// ------------------------------- P2M factored through unit-density multipoles
+// The node weights of every column are linear in the six density components
+// of the node's triangle (sl_0..2, dl_0..2), with coefficients that depend on
+// the geometry only.  The P2M of a leaf therefore factors as
+//   mpole[box][kind, r] = sum_{t in box} sum_s H[kind][t][s] sigma_s(t, r),
+// where H[kind][t][s] (D coefficients) is the multipole of triangle t with
+// unit density component s in column kind.  Stage 1 (k_p2m_unit) builds H
+// once per triangle, independent of the right-hand sides; stage 2 is the
+// batched product of H (K = 6 x triangles per leaf) with the densities
+// (k_p2m_sigma gathers them, N = R).  Per triangle, H follows from 26 node
+// moments of the features F (rows as in k_p2m_features):
+//   M0[row] = sum_nodes w F[row],  M1_e[row] = sum_nodes w y_e F[row]
+// (w: quadrature weight x area, y: node position), by the combinations of
+// the weights in k_p2m_weights / img_node_weights:
+//   kinds p = 0..2: H[sl_p] = inv2mu M0[0],
+//                   H[dl_e] = (delta_ep n.M0[1..3] + n_p M0[1 + e]) / 2
+//   kind 3:         H[sl_e] = c1 inv2mu M1_e[0],
+//                   H[dl_e] = c2 n_e M0[0] + c1 (sum_d n_d M1_e[1 + d] + sum_j n_j M1_j[1 + e]) / 2
+//   kind 4:         H[sl_e] = alpha M1_3[1 + e] - delta_e3 (2 - alpha) M0[0],
+//                   H[dl_e] = -(2 - 2 alpha) Te_3.M0[1..3] + alpha qv(Te).M1_3[4..8]
+//   kind 5:         H[sl_e] = -M0[1 + e],  H[dl_e] = -qv(Te).M0[4..8]
+//   kind 6:         H[sl] = (M0[1], M0[2], -M0[3]),  H[dl_e] = qvU(Te).M0[4..8]
+// with Te[k][l] = lam delta_kl n_e + mu (delta_ke n_l + delta_le n_k) the
+// double-layer tensor of a unit jump e, qv(T) = (T00 - T22, T11 - T22, 2 T01,
+// 2 T02, 2 T12) and qvU(T) = (T00 + T22, T11 + T22, 2 T01, 0, 0).  NK = 4:
+// the four free-space (or anti-image) columns; NK = 7 adds the image columns.
+constexpr int UNIT_TB = 16;  // triangles per CTA
+
+// Largest CTA of k_p2m_unit (register budget of the moments: at most 128
+// per thread in FP32, 240 in FP64; CTAs of whole warp quadruples, so that
+// every sub-partition's register file holds its share); the launch uses the
+// fewest such threads that cover the coefficients in the same number of rounds
+template <class T>
+__host__ __device__ constexpr int unit_threads() { return sizeof(T) == 4 ? 512 : 256; }
+
+// Shared-memory layout of the node harmonics in k_p2m_unit: row n = -2..p
+// holds m = -2..n+4 (zero outside 0 <= |m| <= n; Y_n^{-m} = (-1)^m conj Y_n^m
+// for m = 1, 2), so every ladder neighbour of (n, m) is a plain load.
+__host__ __device__ constexpr int unit_yoff(int n, int m) { return (n + 6) * (n + 7) / 2 + m - 8; }
+__host__ __device__ constexpr int unit_ylen(int p) { return unit_yoff(p + 1, -2); }
+
+// Unit-density columns H[kind][s] of one coefficient from its (scaled)
+// moments: put(kind, s, re, im) for s = 0..2 (single layer), 3..5 (double
+// layer); nv the triangle normal.  Kinds reading the first moments come
+// first so that their registers free up early.
+template <class T, int NK, class Put>
+__device__ __forceinline__ void unit_combine(Put& put, const T* m0r, const T* m0i, const T (*m1r)[4],
+                                             const T (*m1i)[4], const T* mqr, const T* mqi, const T* nv3, T tc1,
+                                             T tc2, T ti2, T tal, T tlam, T tmu) {
+  for (int e = 0; e < 3; e++) put(3, e, tc1 * ti2 * m1r[e][0], tc1 * ti2 * m1i[e][0]);
+  for (int e = 0; e < 3; e++) {
+    T vr = tc2 * nv3[e] * m0r[0], vi = tc2 * nv3[e] * m0i[0];
+    for (int d = 0; d < 3; d++) {
+      vr += (T)0.5 * tc1 * (nv3[d] * m1r[e][1 + d] + nv3[d] * m1r[d][1 + e]);
+      vi += (T)0.5 * tc1 * (nv3[d] * m1i[e][1 + d] + nv3[d] * m1i[d][1 + e]);
+    }
+    put(3, 3 + e, vr, vi);
+  }
+  // Te: the double-layer tensor of a unit jump in direction e,
+  // qv(Te) = (T00 - T22, T11 - T22, 2 T01, 2 T02, 2 T12), qvU(Te) = (T00 + T22, T11 + T22, 2 T01)
+  auto tens = [&](int e, int k, int l) {
+    return (k == l ? tlam * nv3[e] : (T)0) + tmu * ((k == e ? nv3[l] : (T)0) + (l == e ? nv3[k] : (T)0));
+  };
+  if constexpr (NK == 7) {
+    for (int e = 0; e < 3; e++) {
+      put(4, e, tal * m1r[2][1 + e] - (e == 2 ? ((T)2 - tal) * m0r[0] : (T)0),
+          tal * m1i[2][1 + e] - (e == 2 ? ((T)2 - tal) * m0i[0] : (T)0));
+      const T qv[5] = {tens(e, 0, 0) - tens(e, 2, 2), tens(e, 1, 1) - tens(e, 2, 2), 2 * tens(e, 0, 1),
+                       2 * tens(e, 0, 2), 2 * tens(e, 1, 2)};
+      T r4 = 0, i4 = 0;
+      for (int d = 0; d < 3; d++) {
+        r4 -= ((T)2 - 2 * tal) * tens(e, 2, d) * m0r[1 + d];
+        i4 -= ((T)2 - 2 * tal) * tens(e, 2, d) * m0i[1 + d];
+      }
+      for (int f = 0; f < 5; f++) {
+        r4 += tal * qv[f] * mqr[f];
+        i4 += tal * qv[f] * mqi[f];
+      }
+      put(4, 3 + e, r4, i4);
+    }
+  }
+  const T ndr = nv3[0] * m0r[1] + nv3[1] * m0r[2] + nv3[2] * m0r[3];
+  const T ndi = nv3[0] * m0i[1] + nv3[1] * m0i[2] + nv3[2] * m0i[3];
+#pragma unroll
+  for (int pk = 0; pk < 3; pk++) {
+    for (int e = 0; e < 3; e++) put(pk, e, e == pk ? ti2 * m0r[0] : (T)0, e == pk ? ti2 * m0i[0] : (T)0);
+    for (int e = 0; e < 3; e++)
+      put(pk, 3 + e, (T)0.5 * ((e == pk ? ndr : (T)0) + nv3[pk] * m0r[1 + e]),
+          (T)0.5 * ((e == pk ? ndi : (T)0) + nv3[pk] * m0i[1 + e]));
+  }
+  if constexpr (NK == 7) {
+    for (int e = 0; e < 3; e++) {
+      const T qv[5] = {tens(e, 0, 0) - tens(e, 2, 2), tens(e, 1, 1) - tens(e, 2, 2), 2 * tens(e, 0, 1),
+                       2 * tens(e, 0, 2), 2 * tens(e, 1, 2)};
+      const T qu[3] = {tens(e, 0, 0) + tens(e, 2, 2), tens(e, 1, 1) + tens(e, 2, 2), 2 * tens(e, 0, 1)};
+      T r5 = 0, i5 = 0, r6 = 0, i6 = 0;
+      for (int f = 0; f < 5; f++) {
+        r5 -= qv[f] * m0r[4 + f];
+        i5 -= qv[f] * m0i[4 + f];
+      }
+      for (int f = 0; f < 3; f++) {
+        r6 += qu[f] * m0r[4 + f];
+        i6 += qu[f] * m0i[4 + f];
+      }
+      put(5, 3 + e, r5, i5);
+      put(6, 3 + e, r6, i6);
+      put(5, e, -m0r[1 + e], -m0i[1 + e]);
+    }
+    put(6, 0, m0r[1], m0i[1]);
+    put(6, 1, m0r[2], m0i[2]);
+    put(6, 2, -m0r[3], -m0i[3]);
+  }
+}
+
+template <class T, int NK, int NT>
+__global__ void __launch_bounds__(NT, 1)
+k_p2m_unit(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ hoff, int sbase,
+           int ns, T* __restrict__ H) {
+  constexpr int NF = NK == 7 ? 9 : 4;
+  extern __shared__ __align__(16) unsigned char pu_smem[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc, NY = unit_ylen(p);
+  cplx* Ys = reinterpret_cast<cplx*>(pu_smem);    // [12][NY] node harmonics (extended rows)
+  double* rtab = reinterpret_cast<double*>(Ys + 12 * NY);  // [nc]: 1/m! at (m, m), 1/((n-m)(n+m)) at n > m
+  int* nmtab = reinterpret_cast<int*>(rtab + nc);          // [nc]: n | m << 16
+  double* sct = reinterpret_cast<double*>(nmtab + nc + (nc & 1));  // [18]: row scales (re, im)
+  T* geo = reinterpret_cast<T*>(sct + 18);                          // [12][4]: w, w y
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int tl0 = blockIdx.y * UNIT_TB, tl1 = min(tn, tl0 + UNIT_TB);
+  if (tl0 >= tn) return;
+  const int tid = threadIdx.x, NTr = blockDim.x;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, q2 = is * is;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  for (int i = tid; i < 12 * NY; i += NTr) Ys[i] = {0.0, 0.0};
+  for (int i = tid; i < nc; i += NTr) {
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= i) n++;
+    const int m = i - n * (n + 1) / 2;
+    double f = 1.0;
+    for (int k = 2; k <= m; k++) f /= k;
+    rtab[i] = n > m ? 1.0 / ((double)(n - m) * (double)(n + m)) : f;
+    nmtab[i] = n | (m << 16);
+  }
+  Quad12 Q;
+  quad12(Q);
+  const double lam = a.lam, mu = a.mu, al = a.alpha, c1 = a.c1, c2 = a.c2, inv2mu = a.inv2mu;
+  const long long kstride = (long long)ns * tn * D;  // one kind of the leaf
+  T* Hb = H + hoff[blockIdx.x];
+  // scales of the feature rows (re, im) applied to the moments: the node
+  // loop accumulates the unscaled ladder combinations below
+  if (tid == 0) {
+    const double sr9[9] = {1.0, 0.5 * is, 0.5 * is, is, 0.25 * q2, -0.25 * q2, 0.25 * q2, 0.5 * q2, 0.5 * q2};
+    const double si9[9] = {-1.0, -0.5 * is, 0.5 * is, -is, -0.25 * q2, 0.25 * q2, 0.25 * q2, -0.5 * q2, 0.5 * q2};
+    for (int f = 0; f < 9; f++) {
+      sct[f] = sr9[f];
+      sct[9 + f] = si9[f];
+    }
+  }
+  const double* scr = sct;
+  const double* sci = sct + 9;
+  for (int tl = tl0; tl < tl1; tl++) {
+    const int it = t0 + tl;
+    const double* Tr = a.tri + 9 * (size_t)it;
+    __syncthreads();  // the previous triangle's harmonics have been read (and the tables written)
+    // column m of node j: Y_m^m = (-(z_x + i z_y)/2)^m / m!, then
+    // Y_n^m = ((2n - 1) z_3 Y_{n-1}^m - |z|^2 Y_{n-2}^m) / ((n - m)(n + m))
+    for (int task = tid; task < 12 * (p + 1); task += NTr) {
+      const int m = task / 12, j = task % 12;
+      double y[3];
+      for (int d = 0; d < 3; d++) y[d] = Q.b[j][0] * Tr[d] + Q.b[j][1] * Tr[3 + d] + Q.b[j][2] * Tr[6 + d];
+      const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
+      const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+      if (m == 0) {
+        const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+        const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                              e1[0] * e2[1] - e1[1] * e2[0]};
+        const double w = Q.w[j] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        T* gq = geo + 4 * j;
+        gq[0] = (T)w; gq[1] = (T)(w * y[0]); gq[2] = (T)(w * y[1]); gq[3] = (T)(w * y[2]);
+      }
+      cplx pw = {1.0, 0.0}, b = {-0.5 * z[0], -0.5 * z[1]};
+      for (int e = m; e; e >>= 1) {
+        if (e & 1) pw = cmul(pw, b);
+        if (e > 1) b = cmul(b, b);
+      }
+      cplx* Y = Ys + (size_t)j * NY;
+      cplx ym2 = {0, 0}, ym1 = cscale(rtab[cidx(m, m)], pw);
+      for (int n = m;;) {
+        Y[unit_yoff(n, m)] = ym1;
+        if (m == 1) Y[unit_yoff(n, -1)] = {-ym1.re, ym1.im};
+        if (m == 2) Y[unit_yoff(n, -2)] = {ym1.re, -ym1.im};
+        if (++n > p) break;
+        const double aa = (2.0 * n - 1.0) * z[2], inv = rtab[cidx(n, m)];
+        const cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+    __syncthreads();
+    const double* nv = a.nrm + 3 * (size_t)it;
+    const double nn[3] = {nv[0], nv[1], nv[2]};
+    for (int cc = tid; cc < nc; cc += NTr) {
+      const int nm = nmtab[cc], fn = nm & 0xFFFF, fm = nm >> 16;
+      const int o0 = unit_yoff(fn, fm), o1 = unit_yoff(fn - 1, fm), o2 = unit_yoff(fn - 2, fm);
+      const double srd = a.wnorm ? a.wnorm[2 * cc] : 1.0;
+      // moments (re, im) of the unscaled rows: M0 rows 0..NF-1, M1_e rows 0..3, M1_3 rows 4..8
+      T m0r[NF], m0i[NF], m1r[3][4], m1i[3][4], mqr[5], mqi[5];
+#pragma unroll
+      for (int f = 0; f < NF; f++) m0r[f] = m0i[f] = (T)0;
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int f = 0; f < 4; f++) m1r[e][f] = m1i[e][f] = (T)0;
+#pragma unroll
+      for (int f = 0; f < 5; f++) mqr[f] = mqi[f] = (T)0;
+#pragma unroll 1
+      for (int j = 0; j < 12; j++) {
+        const cplx* Y = Ys + (size_t)j * NY;
+        const T* gq = geo + 4 * j;
+        const T w = gq[0], wy[3] = {gq[1], gq[2], gq[3]};
+        // Y, d_x, d_y, d_z (and xx, yy, xy, xz, yz) by the ladder relations, unscaled
+        T fr[NF], fi[NF];
+        // (the ladder sums in T: the FP32 form rounds the harmonics first,
+        // scaled by the coefficient's basis normalisation so that they stay
+        // in range)
+        auto ld = [&](int o, T& re, T& im) {
+          const cplx v = Y[o];
+          re = (T)(srd * v.re);
+          im = (T)(srd * v.im);
+        };
+        T ar, ai, br, bi, cr, ci;
+        ld(o0, fr[0], fi[0]);
+        ld(o1, ar, ai);
+        ld(o1 + 1, br, bi);
+        ld(o1 - 1, cr, ci);
+        fr[1] = br - cr; fi[1] = bi - ci;
+        fr[2] = bi + ci; fi[2] = br + cr;
+        fr[3] = ar; fi[3] = ai;
+        if constexpr (NF == 9) {
+          T zr, zi, p1r, p1i, m1r_, m1i_, p2r, p2i, m2r, m2i;
+          ld(o2, zr, zi);
+          ld(o2 + 1, p1r, p1i);
+          ld(o2 - 1, m1r_, m1i_);
+          ld(o2 + 2, p2r, p2i);
+          ld(o2 - 2, m2r, m2i);
+          fr[4] = p2r - 2 * zr + m2r; fi[4] = p2i - 2 * zi + m2i;
+          fr[5] = p2r + 2 * zr + m2r; fi[5] = p2i + 2 * zi + m2i;
+          fr[6] = p2i - m2i; fi[6] = p2r - m2r;
+          fr[7] = p1r - m1r_; fi[7] = p1i - m1i_;
+          fr[8] = p1i + m1i_; fi[8] = p1r + m1r_;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          m0r[f] += w * fr[f];
+          m0i[f] += w * fi[f];
+        }
+#pragma unroll
+        for (int e = 0; e < 3; e++)
+#pragma unroll
+          for (int f = 0; f < 4; f++) {
+            m1r[e][f] += wy[e] * fr[f];
+            m1i[e][f] += wy[e] * fi[f];
+          }
+        if constexpr (NF == 9) {
+#pragma unroll
+          for (int f = 0; f < 5; f++) {
+            mqr[f] += wy[2] * fr[4 + f];
+            mqi[f] += wy[2] * fi[4 + f];
+          }
+        }
+      }
+      // the row scales (conjugation signs, 1/s per derivative, ladder factors)
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        m0r[f] = (T)(scr[f] * m0r[f]);
+        m0i[f] = (T)(sci[f] * m0i[f]);
+      }
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+          m1r[e][f] = (T)(scr[f] * m1r[e][f]);
+          m1i[e][f] = (T)(sci[f] * m1i[e][f]);
+        }
+#pragma unroll
+      for (int f = 0; f < 5; f++) {
+        mqr[f] = (T)(scr[4 + f] * mqr[f]);
+        mqi[f] = (T)(sci[4 + f] * mqi[f]);
+      }
+      // the combinations in T
+      T* o = Hb + (size_t)(ns * tl) * D + 2 * cc;
+      // column s (0..2 single layer, 3..5 double layer) of kind q, if carried
+      auto put = [&](int q, int sidx, T vr, T vi) {
+        const int sl = sidx - sbase;
+        if (sl < 0 || sl >= ns) return;
+        T* oo = o + q * kstride + (size_t)sl * D;
+        oo[0] = vr;
+        oo[1] = vi;
+      };
+      const T nv3[3] = {(T)nn[0], (T)nn[1], (T)nn[2]};
+      unit_combine<T, NK>(put, m0r, m0i, m1r, m1i, mqr, mqi, nv3, (T)c1, (T)c2, (T)inv2mu, (T)al, (T)lam, (T)mu);
+    }
+  }
+}
+
+// FP32 form of k_p2m_unit (the mixed-precision P2M).  The node harmonics
+// are computed in FP64 and stored in FP32 in the normalised basis
+// Yh_n^m = Y_n^m sqrt((n + m)! (n - m)!) (bounded by |z|^n, no underflow);
+// a coefficient (n, m) reads its ladder neighbours (n', m') times
+// sqrt((n + m)! (n - m)! / ((n' + m')! (n' - m')!)), which yields the
+// features of the normalised basis directly.  Two harmonic buffers: the
+// recurrences of triangle t + 1 run while the moments of triangle t
+// accumulate (one barrier per triangle).
+constexpr int UNITF_THREADS = 512;
+
+__host__ __device__ inline size_t unitf_smem(int p) {
+  const size_t nc = (size_t)(p + 1) * (p + 2) / 2;
+  return 2 * 12 * (size_t)unit_ylen(p) * sizeof(float2) + 2 * nc * sizeof(double) + 2 * 12 * 4 * sizeof(float) +
+         18 * sizeof(float);
+}
+
+template <int NK>
+__global__ void __launch_bounds__(UNITF_THREADS, 1)
+k_p2m_unit_f(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ hoff, int sbase,
+             int ns, float* __restrict__ H) {
+  constexpr int NF = NK == 7 ? 9 : 4;
+  extern __shared__ __align__(16) unsigned char pf_smem2[];
+  const int p = a.p, nc = ncoef(p), D = 2 * nc, NY = unit_ylen(p);
+  float2* Yb = reinterpret_cast<float2*>(pf_smem2);                  // [2][12][NY]
+  double* rtab = reinterpret_cast<double*>(Yb + 2 * 12 * NY);        // [nc]: 1/m!, 1/((n-m)(n+m))
+  double* wtab = rtab + nc;                                          // [nc]: sqrt((n+m)!(n-m)!)
+  float* geo = reinterpret_cast<float*>(wtab + nc);                  // [2][12][4]: w, w y
+  float* sct = geo + 2 * 12 * 4;                                     // [18]: row scales (re, im)
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int tl0 = blockIdx.y * UNIT_TB, tl1 = min(tn, tl0 + UNIT_TB);
+  if (tl0 >= tn) return;
+  const int tid = threadIdx.x, NTr = blockDim.x;
+  const int lev = a.level[box];
+  const double s = a.size / (double)(1ull << lev), is = 1.0 / s, q2 = is * is;
+  double c[3];
+  for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  for (int i = tid; i < 2 * 12 * NY; i += NTr) Yb[i] = make_float2(0.f, 0.f);
+  for (int i = tid; i < nc; i += NTr) {
+    int n = 0;
+    while ((n + 1) * (n + 2) / 2 <= i) n++;
+    const int m = i - n * (n + 1) / 2;
+    double f = 1.0;
+    for (int k = 2; k <= m; k++) f /= k;
+    rtab[i] = n > m ? 1.0 / ((double)(n - m) * (double)(n + m)) : f;
+    wtab[i] = a.wnorm[2 * i];
+  }
+  if (tid == 0) {
+    const double sr9[9] = {1.0, 0.5 * is, 0.5 * is, is, 0.25 * q2, -0.25 * q2, 0.25 * q2, 0.5 * q2, 0.5 * q2};
+    const double si9[9] = {-1.0, -0.5 * is, 0.5 * is, -is, -0.25 * q2, 0.25 * q2, 0.25 * q2, -0.5 * q2, 0.5 * q2};
+    for (int f = 0; f < 9; f++) {
+      sct[f] = (float)sr9[f];
+      sct[9 + f] = (float)si9[f];
+    }
+  }
+  Quad12 Q;
+  quad12(Q);
+  const float lam = (float)a.lam, mu = (float)a.mu, al = (float)a.alpha, c1 = (float)a.c1, c2 = (float)a.c2,
+              inv2mu = (float)a.inv2mu;
+  const long long kstride = (long long)ns * tn * D;  // one kind of the leaf
+  float* Hb = H + hoff[blockIdx.x];
+  // harmonics of the 12 nodes of triangle tl into buffer b: task (m, j) =
+  // column m of node j, Y_m^m = (-(z_x + i z_y)/2)^m / m! then the recurrence
+  // Y_n^m = ((2n - 1) z_3 Y_{n-1}^m - |z|^2 Y_{n-2}^m) / ((n - m)(n + m))
+  // (tasks from the last thread down: the threads with one coefficient round
+  // less take the longest columns)
+  auto harmonics = [&](int tl, int b) {
+    const double* Tr = a.tri + 9 * (size_t)(t0 + tl);
+    for (int task = NTr - 1 - tid; task < 12 * (p + 1); task += NTr) {
+      const int m = task / 12, j = task % 12;
+      double y[3];
+      for (int d = 0; d < 3; d++) y[d] = Q.b[j][0] * Tr[d] + Q.b[j][1] * Tr[3 + d] + Q.b[j][2] * Tr[6 + d];
+      const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
+      const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
+      if (m == 0) {
+        const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+        const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                              e1[0] * e2[1] - e1[1] * e2[0]};
+        const double w = Q.w[j] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        float* gq = geo + (b * 12 + j) * 4;
+        gq[0] = (float)w; gq[1] = (float)(w * y[0]); gq[2] = (float)(w * y[1]); gq[3] = (float)(w * y[2]);
+      }
+      cplx pw = {1.0, 0.0}, bb = {-0.5 * z[0], -0.5 * z[1]};
+      for (int e = m; e; e >>= 1) {
+        if (e & 1) pw = cmul(pw, bb);
+        if (e > 1) bb = cmul(bb, bb);
+      }
+      float2* Y = Yb + (size_t)(b * 12 + j) * NY;
+      cplx ym2 = {0, 0}, ym1 = cscale(rtab[cidx(m, m)], pw);
+      for (int n = m;;) {
+        const double wn = wtab[cidx(n, m)];
+        const float2 v = make_float2((float)(wn * ym1.re), (float)(wn * ym1.im));
+        Y[unit_yoff(n, m)] = v;
+        if (m == 1) Y[unit_yoff(n, -1)] = make_float2(-v.x, v.y);
+        if (m == 2) Y[unit_yoff(n, -2)] = make_float2(v.x, -v.y);
+        if (++n > p) break;
+        const double aa = (2.0 * n - 1.0) * z[2], inv = rtab[cidx(n, m)];
+        const cplx yn = {(aa * ym1.re - r2 * ym2.re) * inv, (aa * ym1.im - r2 * ym2.im) * inv};
+        ym2 = ym1;
+        ym1 = yn;
+      }
+    }
+  };
+  __syncthreads();  // zeroed buffers and tables
+  harmonics(tl0, 0);
+  __syncthreads();
+  for (int tl = tl0; tl < tl1; tl++) {
+    const int b = (tl - tl0) & 1;
+    if (tl + 1 < tl1) harmonics(tl + 1, b ^ 1);
+    const double* nvp = a.nrm + 3 * (size_t)(t0 + tl);
+    const float nv3[3] = {(float)nvp[0], (float)nvp[1], (float)nvp[2]};
+    for (int cc = tid; cc < nc; cc += NTr) {
+      int fn = (int)((sqrtf(8.0f * cc + 1.0f) - 1.0f) * 0.5f);
+      while ((fn + 1) * (fn + 2) / 2 <= cc) fn++;
+      while (fn * (fn + 1) / 2 > cc) fn--;
+      const int fm = cc - fn * (fn + 1) / 2;
+      const float np_ = (float)(fn + fm), nm_ = (float)(fn - fm);
+      // normalisation ratios of the ladder neighbours (0 where the neighbour is outside the table)
+      auto rt = [](float x) { return sqrtf(fmaxf(x, 0.0f)); };
+      const float rA = rt(np_ * nm_), rB = rt(nm_ * (nm_ - 1)), rC = rt(np_ * (np_ - 1));
+      const float rZ = rt(np_ * (np_ - 1) * nm_ * (nm_ - 1)), rP1 = rt(np_ * nm_ * (nm_ - 1) * (nm_ - 2));
+      const float rM1 = rt(np_ * (np_ - 1) * (np_ - 2) * nm_), rP2 = rt(nm_ * (nm_ - 1) * (nm_ - 2) * (nm_ - 3));
+      const float rM2 = rt(np_ * (np_ - 1) * (np_ - 2) * (np_ - 3));
+      const int o0 = unit_yoff(fn, fm), o1 = unit_yoff(fn - 1, fm), o2 = unit_yoff(fn - 2, fm);
+      float m0r[NF], m0i[NF], m1r[3][4], m1i[3][4], mqr[5], mqi[5];
+#pragma unroll
+      for (int f = 0; f < NF; f++) m0r[f] = m0i[f] = 0.f;
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int f = 0; f < 4; f++) m1r[e][f] = m1i[e][f] = 0.f;
+#pragma unroll
+      for (int f = 0; f < 5; f++) mqr[f] = mqi[f] = 0.f;
+#pragma unroll 1
+      for (int j = 0; j < 12; j++) {
+        const float2* Y = Yb + (size_t)(b * 12 + j) * NY;
+        const float* gq = geo + (b * 12 + j) * 4;
+        const float w = gq[0], wy[3] = {gq[1], gq[2], gq[3]};
+        float fr[NF], fi[NF];
+        const float2 v0 = Y[o0], A = Y[o1], B = Y[o1 + 1], C = Y[o1 - 1];
+        fr[0] = v0.x; fi[0] = v0.y;
+        fr[1] = rB * B.x - rC * C.x; fi[1] = rB * B.y - rC * C.y;
+        fr[2] = rB * B.y + rC * C.y; fi[2] = rB * B.x + rC * C.x;
+        fr[3] = rA * A.x; fi[3] = rA * A.y;
+        if constexpr (NF == 9) {
+          const float2 Z = Y[o2], P1 = Y[o2 + 1], M1 = Y[o2 - 1], P2 = Y[o2 + 2], M2 = Y[o2 - 2];
+          const float zr = 2 * rZ * Z.x, zi = 2 * rZ * Z.y;
+          fr[4] = rP2 * P2.x - zr + rM2 * M2.x; fi[4] = rP2 * P2.y - zi + rM2 * M2.y;
+          fr[5] = rP2 * P2.x + zr + rM2 * M2.x; fi[5] = rP2 * P2.y + zi + rM2 * M2.y;
+          fr[6] = rP2 * P2.y - rM2 * M2.y; fi[6] = rP2 * P2.x - rM2 * M2.x;
+          fr[7] = rP1 * P1.x - rM1 * M1.x; fi[7] = rP1 * P1.y - rM1 * M1.y;
+          fr[8] = rP1 * P1.y + rM1 * M1.y; fi[8] = rP1 * P1.x + rM1 * M1.x;
+        }
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          m0r[f] += w * fr[f];
+          m0i[f] += w * fi[f];
+        }
+#pragma unroll
+        for (int e = 0; e < 3; e++)
+#pragma unroll
+          for (int f = 0; f < 4; f++) {
+            m1r[e][f] += wy[e] * fr[f];
+            m1i[e][f] += wy[e] * fi[f];
+          }
+        if constexpr (NF == 9) {
+#pragma unroll
+          for (int f = 0; f < 5; f++) {
+            mqr[f] += wy[2] * fr[4 + f];
+            mqi[f] += wy[2] * fi[4 + f];
+          }
+        }
+      }
+      const float* scr = sct;
+      const float* sci = sct + 9;
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        m0r[f] *= scr[f];
+        m0i[f] *= sci[f];
+      }
+#pragma unroll
+      for (int e = 0; e < 3; e++)
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+          m1r[e][f] *= scr[f];
+          m1i[e][f] *= sci[f];
+        }
+#pragma unroll
+      for (int f = 0; f < 5; f++) {
+        mqr[f] *= scr[4 + f];
+        mqi[f] *= sci[4 + f];
+      }
+      float* o = Hb + (size_t)(ns * tl) * D + 2 * cc;
+      auto put = [&](int q, int sidx, float vr, float vi) {
+        const int sl = sidx - sbase;
+        if (sl < 0 || sl >= ns) return;
+        float* oo = o + q * kstride + (size_t)sl * D;
+        oo[0] = vr;
+        oo[1] = vi;
+      };
+      unit_combine<float, NK>(put, m0r, m0i, m1r, m1i, mqr, mqi, nv3, c1, c2, inv2mu, al, lam, mu);
+    }
+    __syncthreads();  // buffer b is free, buffer b ^ 1 complete
+  }
+}
+
+// Densities of the leaves as the B operand of the factored P2M product:
+// per leaf at soff, R rows of Kp = ns tn rounded up to 4, entry ns t + j =
+// density component sbase + j of triangle t (components 0..2 single layer,
+// 3..5 double layer).
+template <class T>
+__global__ void __launch_bounds__(256)
+k_p2m_sigma(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ soff,
+            int sbase, int ns, T* __restrict__ S) {
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int K = ns * tn, Kp = (K + 3) & ~3;
+  T* out = S + soff[blockIdx.x];
+  for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < (long long)R * Kp;
+       q += (long long)gridDim.y * blockDim.x) {
+    const int r = (int)(q / Kp), k = (int)(q % Kp);
+    double v = 0.0;
+    if (k < K) {
+      const int tl = k / ns, sc = sbase + k % ns;
+      const long long off = r * a.rstride + (long long)(t0 + tl) * a.tstride + (sc % 3) * a.dstride;
+      if (sc < 3) {
+        if (a.dosl) v = a.ssl[off];
+      } else if (a.dodl) {
+        v = a.sdl[off];
+      }
+    }
+    out[q] = (T)v;
+  }
+}
+
 // Direct image P2M (few right-hand sides): one CTA per (leaf, right-hand
 // side r = blockIdx.y), nodes in batches of P2M_NODES (one warp each builds
 // the regular harmonics), every thread accumulating 7 columns of its
@@ -1695,15 +2239,72 @@ template void launch_l2t_twostage<float>(cudaStream_t, const L2TArgs&, int, int,
                                          const long long*, int, float*, float*, int, const GemmTask*,
                                          const float*, bool);
 
+// Stage 1 of the factored P2M for one wave of leaves: unit-density
+// multipoles H (nk = 4 or 7 kinds, per leaf at hoff: [kind][ns tn][D]) and
+// the density operand S (per leaf at soff: R rows of ns tn rounded up to 4).
+// FP32 (T = float) runs k_p2m_unit_f and needs the basis normalisation.
+// False (nothing launched) when the order is too high for the kernel's
+// shared memory.
+template <class T>
+bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S) {
+  const int nc = ncoef(a.p);
+  const bool fp32 = sizeof(T) == 4;
+  const size_t smem = p2m_unit_smem(a.p, fp32);
+  if (smem > 227 * 1024 || (fp32 && !a.wnorm)) return false;
+  if (nwleaf <= 0) return true;
+  const dim3 grid(nwleaf, (maxtn + UNIT_TB - 1) / UNIT_TB);
+  // the fewest threads (whole warp quadruples) that cover the coefficients in ceil(nc / NT) rounds
+  const int NT = fp32 ? UNITF_THREADS : unit_threads<T>();
+  const int rounds = (nc + NT - 1) / NT;
+  const int nthr = std::max(128, std::min(NT, (((nc + rounds - 1) / rounds) + 127) / 128 * 128));
+  if constexpr (sizeof(T) == 4) {
+    float* Hf = reinterpret_cast<float*>(H);
+    if (nk == 7) {
+      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_unit_f<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_p2m_unit_f<7><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
+    } else {
+      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_unit_f<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_p2m_unit_f<4><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
+    }
+  } else {
+    constexpr int NTD = unit_threads<T>();
+    if (nk == 7) {
+      EFMM_CUDA_TRY(
+          cudaFuncSetAttribute(k_p2m_unit<T, 7, NTD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_p2m_unit<T, 7, NTD><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, H);
+    } else {
+      EFMM_CUDA_TRY(
+          cudaFuncSetAttribute(k_p2m_unit<T, 4, NTD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_p2m_unit<T, 4, NTD><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, H);
+    }
+  }
+  count_launch();
+  k_p2m_sigma<T><<<dim3(nwleaf, 8), 256, 0, st>>>(a, R, wleaves, soff, sbase, ns, S);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+  return true;
+}
+size_t p2m_unit_smem(int p, bool fp32) {
+  if (fp32) return unitf_smem(p);
+  const size_t nc = ncoef(p);
+  return 12 * (size_t)unit_ylen(p) * sizeof(cplx) + nc * sizeof(double) + (nc + 1) * sizeof(int) +
+         (18 + 12 * 4) * sizeof(double);
+}
+template bool launch_p2m_unit<double>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
+                                      const long long*, const long long*, int, int, double*, double*);
+template bool launch_p2m_unit<float>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
+                                     const long long*, const long long*, int, int, float*, float*);
+
 // The batched product of the two-stage P2M: FP32 on the tensor cores
 // (tc_gemm.cu) unless ELFMM3D_TC=0, FP64 (and FP32 when disabled) on the
 // CUDA cores.
 template <class T>
-void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C) {
+void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C, int bn) {
   if (ntask <= 0) return;
   if (sizeof(T) == 4 && tc_enabled()) {
     launch_gemm_tc(st, ntask, tasks, reinterpret_cast<const float*>(F), reinterpret_cast<const float*>(W),
-                   reinterpret_cast<float*>(C), tc_err_ptr());
+                   reinterpret_cast<float*>(C), tc_err_ptr(), bn);
     return;
   }
   const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
@@ -1712,8 +2313,8 @@ void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F,
   count_launch();
 }
 
-template void gemm_product<double>(cudaStream_t, int, const GemmTask*, const double*, const double*, double*);
-template void gemm_product<float>(cudaStream_t, int, const GemmTask*, const float*, const float*, float*);
+template void gemm_product<double>(cudaStream_t, int, const GemmTask*, const double*, const double*, double*, int);
+template void gemm_product<float>(cudaStream_t, int, const GemmTask*, const float*, const float*, float*, int);
 
 template <class T>
 void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, const int* wleaves,

@@ -92,9 +92,11 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
 // the U column at local + ubase + (box R + r) D).
 // Returns false (nothing launched) when the order is too high for its tiles.
 bool launch_l2t_img(cudaStream_t st, int nleaf, const L2TArgs& a, int R, long long ubase);
-// The product stage alone (FP32: tensor cores unless ELFMM3D_TC=0).
+// The product stage alone (FP32: tensor cores unless ELFMM3D_TC=0).  Tasks
+// cover 128 x 128 output tiles; bn = 64 runs the tensor-core tiles 64 columns
+// wide (every task then has at most 64 columns).
 template <class T>
-void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C);
+void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F, const T* W, T* C, int bn = 128);
 template <class TB>
 bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const int* chunk_e0, const L2TArgs& a,
                      int R, const TB* local, const double* wnorm);
@@ -114,6 +116,19 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
 // the caller): node features with second-derivative rows (9 x 12 x
 // triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12
 // x triangles per leaf at woff), batched product into mpole.
+// Stage 1 of the P2M factored through unit-density multipoles, for one wave
+// of leaves (at most maxtn triangles each): H (nk = 4 free-space or
+// anti-image kinds, 7 with the image columns; per leaf at hoff,
+// [kind][ns x triangles][D], geometry only) for the ns density components
+// sbase.. (0..2 single layer, 3..5 double layer), and the density operand S
+// (per leaf at soff, R rows of ns x triangles rounded up to a multiple of 4).
+// Stage 2 is gemm_product with K = ns x triangles, N = R.  False (nothing
+// launched) when the order is too high for its shared memory
+// (p2m_unit_smem(p, T is float) > 227 KB).
+template <class T>
+bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S);
+size_t p2m_unit_smem(int p, bool fp32);
 // Direct P2M of the image columns (one CTA per leaf and right-hand side):
 // columns kind * R + r of 6R per box (kinds 0..5) and the U column at
 // mpole + ubase + (box R + r) D.  For few right-hand sides.
@@ -132,8 +147,9 @@ void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs = 1);
 // The FP32 product of k_gemm_tn<float> on the tensor cores (tc_gemm.cu):
 // tcgen05.mma kind::tf32 with the 3-term head/tail split (FP32 accuracy).
 // *err is set when a bounded wait runs out (the tile is then not stored).
+// bn: output tile width (64 or 128 columns).
 void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
-                    int* err);
+                    int* err, int bn = 128);
 // Per-device error flag of the tensor-core products; tc_take_error reads
 // and clears it (blocking).
 int* tc_err_ptr();

@@ -253,6 +253,8 @@ void Plan::ensure_ops() {
 Plan::Plan(int device, cudaStream_t stream) : dev_(device), st_(stream) {
   const char* tr = getenv("ELFMM3D_TRANSLATIONS");  // "dense": per-offset dense operators
   factored_ = !(tr && strcmp(tr, "dense") == 0);
+  const char* pm = getenv("ELFMM3D_P2M");  // "nodes": batched P2M as node-feature products
+  p2m_unit_ = !(pm && strcmp(pm, "nodes") == 0);
   for (int i = 0; i < 10; i++) EFMM_CUDA_TRY(cudaEventCreate(&ev_[i]));
 }
 Plan::~Plan() {
@@ -276,9 +278,9 @@ void WaveSet::upload(const std::vector<int>& wl, const std::vector<long long>& o
 
 template <class T>
 void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, long long t0, const GemmTask* dtasks,
-                         const T* F, const T* W, T* C) {
+                         const T* F, const T* W, T* C, int bn) {
   if (capturing_) {
-    gemm_product<T>(st_, ntask, dtasks, F, W, C);
+    gemm_product<T>(st_, ntask, dtasks, F, W, C, bn);
     return;
   }
   if (npev_ + 2 > (int)pev_.size()) {
@@ -289,7 +291,7 @@ void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, long lon
     pev_.push_back(b);
   }
   EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_], st_));
-  gemm_product<T>(st_, ntask, dtasks, F, W, C);
+  gemm_product<T>(st_, ntask, dtasks, F, W, C, bn);
   EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_ + 1], st_));
   npev_ += 2;
   for (long long q = t0; q < t0 + ntask; q++) {
@@ -972,6 +974,91 @@ void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
 template void Plan::p2m_twostage<double>(const P2MArgs&, int, double*);
 template void Plan::p2m_twostage<float>(const P2MArgs&, int, float*);
 
+// P2M factored through unit-density multipoles over waves of leaves (budget
+// as in p2m_twostage): per leaf the unit multipoles H of its triangles
+// ([kind][ns tn][D], nk kinds, ns = 3 or 6 density components: those of the
+// layers present) and the densities S (R rows of ns tn rounded up to 4),
+// then one product task per (leaf, kind, 128-row tile): K = ns tn, N = R
+// (64-column tensor-core tiles when R <= 64).  Column layouts: the
+// free-space plan writes columns 4 r + kind of 4R per box; the image plan
+// columns kind R + r of 6R (kinds 0..5) and the U column at nb 6R D + box R D.
+template <class T>
+bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
+  const int D = 2 * ncoef(p_), nk = image ? 7 : 4;
+  const long long nb = tr_.nboxes;
+  if (p2m_unit_smem(p_, sizeof(T) == 4) > (size_t)227 * 1024) return false;
+  // density components carried: single layer 0..2, double layer 3..5
+  const int sbase = pa.dosl ? 0 : 3, ns = (pa.dosl && pa.dodl) ? 6 : 3;
+  WaveSet& W = p2m_waves_;
+  const long long key = ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) | (sizeof(T) << 2) | (image ? 3 : 1);
+  if (W.key != key) {
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    const size_t budget =
+        std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double)) / sizeof(T);
+    W.clear();
+    std::vector<int> wl;
+    std::vector<long long> ho, so;
+    std::vector<GemmTask> tasks;
+    size_t i = 0;
+    const size_t nl = p2m_h_.size();
+    while (i < nl) {
+      WaveSet::Wave w{0, (long long)wl.size(), 0, (long long)tasks.size(), 0, 0, 0};
+      long long used = 0;
+      while (i < nl) {
+        const int tn = p2m_sc_h_[i];
+        const long long K = (long long)ns * tn, Kp = (K + 3) & ~3LL, hk = K * D;
+        const long long need = nk * hk + R * Kp;
+        if (w.nwl > 0 && used + need > (long long)budget) break;
+        wl.push_back((int)i);
+        ho.push_back(used);
+        so.push_back(used + nk * hk);
+        const long long box = p2m_h_[i];
+        for (int q = 0; q < nk; q++) {
+          long long coff;
+          int ldc;
+          if (!image) {
+            coff = box * 4 * R * D + (long long)q * D;
+            ldc = 4 * D;
+          } else if (q < 6) {
+            coff = box * 6 * R * D + (long long)q * R * D;
+            ldc = D;
+          } else {
+            coff = nb * 6 * R * D + box * R * D;
+            ldc = D;
+          }
+          for (int c0 = 0; c0 < R; c0 += 128)
+            for (int r0 = 0; r0 < D; r0 += 128)
+              tasks.push_back({used + q * hk, used + nk * hk, coff, D, R, (int)K, D, (int)Kp, ldc, r0, c0});
+        }
+        used += need;
+        w.maxn = std::max(w.maxn, tn);
+        w.nwl++;
+        i++;
+      }
+      w.ntask = (int)(tasks.size() - w.t0);
+      w.used = used;
+      W.w.push_back(w);
+    }
+    W.upload(wl, ho, so, {}, tasks, st_);
+    W.key = key;
+  }
+  size_t maxu = 1;
+  for (const auto& w : W.w) maxu = std::max(maxu, (size_t)w.used);
+  p2m_scratch_.resize((maxu * sizeof(T) + sizeof(double) - 1) / sizeof(double));
+  T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
+  const int bn = R <= 64 ? 64 : 128;
+  for (const auto& w : W.w) {
+    if (!launch_p2m_unit<T>(st_, pa, R, nk, w.nwl, w.maxn, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
+                            W.off2.get() + w.wl0, sbase, ns, scratch, scratch))
+      return false;
+    product_timed<T>(w.ntask, W.htasks, w.t0, W.tasks.get() + w.t0, scratch, scratch, mpole, bn);
+  }
+  return true;
+}
+template bool Plan::p2m_factored<double>(const P2MArgs&, int, double*, bool);
+template bool Plan::p2m_factored<float>(const P2MArgs&, int, float*, bool);
+
 // Two-stage L2T over waves of leaves whose functionals and sums fit a
 // scratch budget (at most 8 GB or a quarter of the free memory).
 // mixed: FP32 normalised locals (local_f_) against normalised functionals,
@@ -1103,7 +1190,8 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.C = C; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
     if (mixed) {
       pa.wnorm = ops_->wnorm.get();  // multipoles in the normalised basis
-      p2m_twostage<float>(pa, R, mpole_f_.get());
+      if (!(p2m_unit_ && p2m_factored<float>(pa, R, mpole_f_.get(), false)))
+        p2m_twostage<float>(pa, R, mpole_f_.get());
       rec(2);
       run_translations(m2m_, C, ops_->mats_f.get(), mpole_f_.get(), mpole_f_.get());
       rec(3);
@@ -1114,7 +1202,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       // product form once the columns fill its tiles
       if (C < 32)
         launch_p2m(st_, np2m_, pa, R);
-      else
+      else if (!(p2m_unit_ && p2m_factored<double>(pa, R, mpole_.get(), false)))
         p2m_twostage<double>(pa, R, mpole_.get());
       rec(2);
       run_translations(m2m_, C, ops_->mats.get(), mpole_.get(), mpole_.get());
@@ -1832,7 +1920,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       pa.wnorm = ops_->wnorm.get();
       if (7 * R < 32)
         launch_p2m_img<float>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
-      else
+      else if (!(p2m_unit_ && p2m_factored<float>(pa, R, mp, true)))
         p2m_img_twostage<float>(pa, R, mp);
       rec(2);
       run_translations(m2m_, Cv, ops_->mats_f.get(), mp, mp);
@@ -1852,7 +1940,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       double* lc = img_lc_.get();
       if (7 * R < 32)
         launch_p2m_img<double>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
-      else
+      else if (!(p2m_unit_ && p2m_factored<double>(pa, R, mp, true)))
         p2m_img_twostage<double>(pa, R, mp);
       rec(2);
       run_translations(m2m_, Cv, ops_->mats.get(), mp, mp);

@@ -214,7 +214,7 @@ class Plan {
   void product_collect();
   template <class T>
   void product_timed(int ntask, const std::vector<GemmTask>& tasks, long long t0, const GemmTask* dtasks, const T* F,
-                     const T* W, T* C);
+                     const T* W, T* C, int bn = 128);
   WaveSet p2m_waves_, l2t_waves_;
   bool capturing_ = false;
   int rc_last_ = 64;
@@ -241,6 +241,10 @@ class Plan {
   DevBuf<GemmTask> wave_tasks_;
   template <class T>
   void p2m_twostage(const P2MArgs& pa, int R, T* mpole);
+  // P2M through unit-density multipoles (free-space 4 kinds, or the image
+  // plan's 7); false when the order is too high for its kernel
+  template <class T>
+  bool p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image);
   DevBuf<int> lchunk_leaf_, lchunk_e0_;   // (L2T leaf index, first point) per product-form L2T CTA
   int nlchunk_ = 0, lchunk_key_ = -1;
   void ensure_ops();
@@ -268,6 +272,7 @@ class Plan {
   void cut_rot_tasks(TransSched& S, int C, int W);
   void ensure_factored();
   bool factored_ = true;  // translations in factored form when they fit
+  bool p2m_unit_ = true;  // batched P2M through unit-density multipoles (else node products)
   template <class T>
   void run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst);
   size_t m2l_pairs_h_ = 0;

@@ -32,10 +32,13 @@ namespace efmm {
 
 namespace {
 
-constexpr int TC_BM = 128, TC_BN = 128, TC_BK = 32, TC_THREADS = 256;
-constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;          // one operand part, 16 KB
-constexpr int TC_STAGE_BYTES = 4 * TC_TILE_BYTES;         // A hi, A lo, B hi, B lo
-constexpr int TC_SMEM = 2 * TC_STAGE_BYTES + 1024 + 64;   // two stages, alignment, barriers
+constexpr int TC_BM = 128, TC_BK = 32, TC_THREADS = 256;
+constexpr int TC_TILE_BYTES = TC_BM * TC_BK * 4;          // one A part, 16 KB
+// per stage: A hi, A lo (16 KB each), B hi, B lo (BN x 32 x 4 bytes each)
+template <int BN>
+__host__ __device__ constexpr int tc_stage_bytes() { return 2 * TC_TILE_BYTES + 2 * BN * TC_BK * 4; }
+template <int BN>
+__host__ __device__ constexpr int tc_smem() { return 2 * tc_stage_bytes<BN>() + 1024 + 64; }  // two stages, alignment, barriers
 // A and B (K-major): element (row, k) at (k % 4) * 4 + (row % 8) * 16 + (k / 4) * 128 + (row / 8) * 1024
 constexpr uint32_t TC_LBO = 128, TC_SBO = 1024;
 constexpr long long TC_WAIT_CYCLES = 4000000000LL;       // about 2 s at 2 GHz
@@ -50,9 +53,12 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint3
          ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
 }
 
-// instruction descriptor: F32 accumulate, TF32 A and B (both K-major), M = 128, N = 128
-constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) |
-                              ((uint32_t)(TC_BN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+// instruction descriptor: F32 accumulate, TF32 A and B (both K-major), M = 128, N = BN
+template <int BN>
+__host__ __device__ constexpr uint32_t tc_idesc() {
+  return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) | ((uint32_t)(BN >> 3) << 17) |
+         ((uint32_t)(TC_BM >> 4) << 24);
+}
 
 __device__ __forceinline__ float tf32_head(float x) {
   uint32_t r;
@@ -84,12 +90,13 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
   return true;
 }
 
-__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t accum) {
+__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accum) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(TC_IDESC), "r"(accum)
+      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
       : "memory");
 }
 
@@ -104,9 +111,15 @@ struct Quad {
 
 }  // namespace
 
+template <int BN>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
           float* __restrict__ Cm, int* __restrict__ err) {
+  constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
+  constexpr int RG = BN / 8;       // 8-row groups of B
+  constexpr int NB = BN / 32;      // B quads per thread and K tile
+  constexpr int NHALF = BN / 2;    // accumulator columns drained per warp
+  constexpr uint32_t IDESC = tc_idesc<BN>();
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   // 1024-byte aligned operand region
   const uint32_t raw = smem_u32(tc_smem_raw);
@@ -118,7 +131,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * TC_BN)
+                 "r"(2 * BN)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -136,7 +149,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   const float* Bb = B + t.b_off;
   const int nkt = (t.K + TC_BK - 1) / TC_BK;
   // staging roles (4 quads of A and 4 of B per thread and K tile)
-  Quad qa[4], qb[4];
+  Quad qa[4], qb[NB];
   const bool bvec = ((t.b_off & 3) == 0) && ((t.ldb & 3) == 0);  // 16-byte rows of B
   auto load = [&](int kt) {
     const int k0 = kt * TC_BK;
@@ -150,8 +163,12 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
 #pragma unroll
       for (int j = 0; j < 4; j++)
         qa[it].v[j] = (gk + j < t.K && gm < t.M) ? Ab[(size_t)(gk + j) * t.lda + gm] : 0.0f;
-      // B: n = 8 (b % 16) + lane % 8, k chunk 4 (b / 16) + lane / 8
-      const int n = 8 * (b & 15) + (lane & 7), kc = 4 * (b >> 4) + (lane >> 3);
+    }
+#pragma unroll
+    for (int it = 0; it < NB; it++) {
+      const int b = it * 8 + warp;
+      // B: n = 8 (b % RG) + lane % 8, k chunk 4 (b / RG) + lane / 8
+      const int n = 8 * (b % RG) + (lane & 7), kc = 4 * (b / RG) + (lane >> 3);
       const int gn = t.col0 + n, gk2 = k0 + 4 * kc;
       if (bvec && gn < t.N && gk2 + 3 < t.K) {
         const float4 v = *reinterpret_cast<const float4*>(Bb + (size_t)gn * t.ldb + gk2);
@@ -177,14 +194,19 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
       hi.w = tf32_head(qa[it].v[3]); lo.w = qa[it].v[3] - hi.w;
       *reinterpret_cast<float4*>(st + offa) = hi;
       *reinterpret_cast<float4*>(st + TC_TILE_BYTES + offa) = lo;
-      const int n = 8 * (b & 15) + (lane & 7), kc = 4 * (b >> 4) + (lane >> 3);
+    }
+#pragma unroll
+    for (int it = 0; it < NB; it++) {
+      const int b = it * 8 + warp;
+      float4 hi, lo;
+      const int n = 8 * (b % RG) + (lane & 7), kc = 4 * (b / RG) + (lane >> 3);
       const uint32_t offb = (n & 7) * 16 + kc * TC_LBO + (n >> 3) * TC_SBO;
       hi.x = tf32_head(qb[it].v[0]); lo.x = qb[it].v[0] - hi.x;
       hi.y = tf32_head(qb[it].v[1]); lo.y = qb[it].v[1] - hi.y;
       hi.z = tf32_head(qb[it].v[2]); lo.z = qb[it].v[2] - hi.z;
       hi.w = tf32_head(qb[it].v[3]); lo.w = qb[it].v[3] - hi.w;
       *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + offb) = hi;
-      *reinterpret_cast<float4*>(st + 3 * TC_TILE_BYTES + offb) = lo;
+      *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + TC_BTILE + offb) = lo;
     }
   };
 
@@ -194,13 +216,13 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   // into FP32 registers (round to nearest), which keeps the product as
   // accurate as an FP32 dot product.  Accumulator (t & 1) holds tile t.
   const int quarter = warp & 3, half = warp >> 2;
-  float acc[64];
+  float acc[NHALF];
 #pragma unroll
-  for (int j = 0; j < 64; j++) acc[j] = 0.0f;
+  for (int j = 0; j < NHALF; j++) acc[j] = 0.0f;
   auto drain = [&](int u) {  // add the accumulator of tile u into acc
-    const uint32_t col0 = (uint32_t)(u & 1) * TC_BN + 64 * half;
+    const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
 #pragma unroll
-    for (int c16 = 0; c16 < 4; c16++) {
+    for (int c16 = 0; c16 < NHALF / 16; c16++) {
       const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
       uint32_t r[16];
       asm volatile(
@@ -226,17 +248,17 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t base = smem_u32(sm + s * TC_STAGE_BYTES);
       const uint32_t ahi = base, alo = base + TC_TILE_BYTES, bhi = base + 2 * TC_TILE_BYTES,
-                     blo = base + 3 * TC_TILE_BYTES;
-      const uint32_t dacc = tmem + (uint32_t)s * TC_BN;
+                     blo = bhi + TC_BTILE;
+      const uint32_t dacc = tmem + (uint32_t)s * BN;
 #pragma unroll
       for (int i = 0; i < TC_BK / 8; i++) {
         const uint64_t dah = umma_desc(ahi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
         const uint64_t dal = umma_desc(alo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
         const uint64_t dbh = umma_desc(bhi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
         const uint64_t dbl = umma_desc(blo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        mma_tf32(dacc, dal, dbh, i > 0 ? 1u : 0u);
-        mma_tf32(dacc, dah, dbl, 1u);
-        mma_tf32(dacc, dah, dbh, 1u);
+        mma_tf32(dacc, dal, dbh, IDESC, i > 0 ? 1u : 0u);
+        mma_tf32(dacc, dah, dbl, IDESC, 1u);
+        mma_tf32(dacc, dah, dbh, IDESC, 1u);
       }
       mma_commit(smem_u32(&bars[s]));
     }
@@ -268,8 +290,8 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
     if (row < t.M) {
       float* Cp = Cm + t.c_off + row;
 #pragma unroll
-      for (int j = 0; j < 64; j++) {
-        const int col = t.col0 + 64 * half + j;
+      for (int j = 0; j < NHALF; j++) {
+        const int col = t.col0 + NHALF * half + j;
         if (col < t.N) Cp[(size_t)col * t.ldc] = acc[j];
       }
     }
@@ -277,7 +299,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TC_BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
 }
 
 namespace {
@@ -315,10 +337,16 @@ bool tc_enabled() {
 }
 
 void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
-                    int* err) {
+                    int* err, int bn) {
   if (ntask <= 0) return;
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM));
-  k_gemm_tc<<<ntask, TC_THREADS, TC_SMEM, st>>>(tasks, A, B, C, err);
+  if (bn == 64) {
+    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<64>()));
+    k_gemm_tc<64><<<ntask, TC_THREADS, tc_smem<64>(), st>>>(tasks, A, B, C, err);
+  } else {
+    EFMM_CUDA_TRY(
+        cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()));
+    k_gemm_tc<128><<<ntask, TC_THREADS, tc_smem<128>(), st>>>(tasks, A, B, C, err);
+  }
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -329,9 +357,11 @@ void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const flo
 // random A (K x M, lda = M + 3), B (N x K, ldb = K + 1) in [-1, 1), C = the
 // tiles of k_gemm_tc.  Returns 0 and the relative l2 error in *rel (and
 // *timeout != 0 if a bounded wait ran out).
-extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double* rel, int* timeout) {
+extern "C" int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, unsigned seed, double* rel,
+                                           int* timeout) {
   using namespace efmm;
   if (M < 1 || N < 1 || K < 0 || M > 4096 || N > 4096 || K > 65536) return 16;
+  if (bn != 64 && bn != 128) return 16;
   const int lda = M + 3, ldb = K + 1, ldc = M + 1;
   std::vector<float> hA((size_t)K * lda), hB((size_t)N * ldb), hC((size_t)N * ldc, -7.0f);
   unsigned long long st = seed * 6364136223846793005ull + 1;
@@ -342,7 +372,7 @@ extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double
   for (auto& v : hA) v = uni();
   for (auto& v : hB) v = uni();
   std::vector<GemmTask> tasks;
-  for (int c0 = 0; c0 < N; c0 += 128)
+  for (int c0 = 0; c0 < N; c0 += bn)
     for (int r0 = 0; r0 < M; r0 += 128) tasks.push_back({0, 0, 0, M, N, K, lda, ldb, ldc, r0, c0});
   float *dA = nullptr, *dB = nullptr, *dC = nullptr;
   int* dErr = nullptr;
@@ -360,7 +390,7 @@ extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double
   cudaMemcpy(dT, tasks.data(), tasks.size() * sizeof(GemmTask), cudaMemcpyHostToDevice);
   cudaMemset(dErr, 0, 4);
   try {
-    launch_gemm_tc(0, (int)tasks.size(), dT, dA, dB, dC, dErr);
+    launch_gemm_tc(0, (int)tasks.size(), dT, dA, dB, dC, dErr, bn);
   } catch (const CudaError&) {
     return fail();
   }
@@ -381,4 +411,8 @@ extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double
   *timeout = herr;
   cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dErr); cudaFree(dT);
   return 0;
+}
+
+extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double* rel, int* timeout) {
+  return efmm_tc_gemm_selfcheck_tile(M, N, K, 128, seed, rel, timeout);
 }

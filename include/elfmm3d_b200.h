@@ -216,6 +216,9 @@ double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, un
  * (N x K) against an FP64 host product; *rel = relative l2 error, *timeout
  * != 0 if a bounded wait in the kernel ran out.  Returns 0 or an ier. */
 int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
+/* The same check with output tiles bn = 64 or 128 columns wide (the 64-wide
+ * tiles carry the factored P2M product, N = number of right-hand sides). */
+int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, unsigned seed, double *rel, int *timeout);
 
 /* Repeated batched evaluations as one CUDA graph (no counterpart in the
  * reference): the same arguments as efmm_plan_evaluate_batch_iter /

@@ -223,3 +223,36 @@ def test_batch_iter_single_layer_displacement_only(gpu):
     with pytest.raises(gpu.ElfmmError):
         _batch_mode(P, d, R, s2, None, n, m, 2)
     P.close()
+
+
+@pytest.mark.parametrize("R", [8, 64])
+def test_batch_p2m_unit_multipoles_match_node_products(gpu, monkeypatch, R):
+    # the batched P2M through per-triangle unit-density multipoles equals the
+    # node-feature product form (ELFMM3D_P2M=nodes): the same FP64 sums
+    # regrouped, and the mixed form within FP32 rounding
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=3, ntarg=80, iprec=3, seed=23)
+    monkeypatch.setenv("ELFMM3D_P2M", "nodes")
+    Pn = gpu.Plan(0)
+    monkeypatch.delenv("ELFMM3D_P2M")
+    Pn.set_geometry(d(tri), d(nrm), d(cen), d(tg), iprec=3)
+    n, m = len(cen), len(tg)
+    rng = np.random.default_rng(29)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    a = _batch(P, d, R, ssl, sdl, n, m)
+    b = _batch(Pn, d, R, ssl, sdl, n, m)
+    for x, y in zip(a, b):
+        assert rel(x, y) < SAME
+    torch = _t()
+    outs = []
+    for Q in (P, Pn):
+        o = [torch.zeros((R, n, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, m, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda")]
+        Q.evaluate_batch(1.3, 0.7, R, d(ssl), d(sdl), *o, precision=1)
+        outs.append([t.cpu().numpy() for t in o])
+    for x, y, z in zip(outs[0], outs[1], a):
+        print(f"unit vs nodes (mixed): {rel(x, y):.2e}   unit mixed vs FP64: {rel(x, z):.2e}")
+        assert rel(x, y) < 1e-6 and rel(x, z) < 1e-6
+    P.close()
+    Pn.close()

@@ -91,6 +91,30 @@ def test_image_fmm_iprec3_and_forms(gpu):
     P.close()
 
 
+def test_image_p2m_unit_multipoles_match_node_products(gpu, monkeypatch):
+    # image plan: the seven columns (anti-image, C piece, U piece) through
+    # per-triangle unit-density multipoles equal the node-feature products
+    P, tri, nrm, cen, tg, d = _setup(gpu, nl=40, nw=20, iprec=3, seed=4)
+    monkeypatch.setenv("ELFMM3D_P2M", "nodes")
+    Pn, *_ = _setup(gpu, nl=40, nw=20, iprec=3, seed=4)
+    monkeypatch.delenv("ELFMM3D_P2M")
+    m = len(tg)
+    rng = np.random.default_rng(6)
+    R = 12
+    ssl, sdl = rng.normal(size=(R,) + cen.shape), rng.normal(size=(R,) + cen.shape)
+    u, e = _image(P, d, R, ssl, sdl, m)
+    un, en = _image(Pn, d, R, ssl, sdl, m)
+    print(f"unit vs nodes (FP64): u {rel(u, un):.2e}  strain {rel(e, en):.2e}")
+    assert rel(u, un) < 1e-12 and rel(e, en) < 1e-12
+    um, em = _image(P, d, R, ssl, sdl, m, precision=1)
+    unm, enm = _image(Pn, d, R, ssl, sdl, m, precision=1)
+    print(f"unit vs nodes (mixed): u {rel(um, unm):.2e}  strain {rel(em, enm):.2e}")
+    assert rel(um, unm) < 1e-6 and rel(em, enm) < 1e-6
+    assert rel(um, u) < 1e-6 and rel(em, e) < 1e-6
+    P.close()
+    Pn.close()
+
+
 def test_image_fmm_traction_free_surface(gpu):
     # the total field (free-space FMM + image FMM) has zero traction on z = 0
     torch = _t()
