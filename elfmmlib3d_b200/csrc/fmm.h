@@ -147,8 +147,11 @@ void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs = 1);
 // The FP32 product of k_gemm_tn<float> on the tensor cores (tc_gemm.cu):
 // tcgen05.mma kind::tf32 with the 3-term head/tail split (FP32 accuracy).
 // *err is set when a bounded wait runs out (the tile is then not stored).
-// bn: output tile width (64 or 128 columns).
+// bn: output tile width (64 or 128 columns).  The double-output form adds
+// the tensor cores' K-tile sums in FP64.
 void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
+                    int* err, int bn = 128);
+void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, double* C,
                     int* err, int bn = 128);
 // Per-device error flag of the tensor-core products; tc_take_error reads
 // and clears it (blocking).

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "fmm.h"
 
 namespace efmm {
 
@@ -31,6 +32,19 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
                        const int* chunk_e0, int R, int dostrain, const double* ssl, const double* sdl,
                        int ntri_all, int nsrc, int ntgt, const long long* sbase = nullptr,
                        const int* sntri = nullptr, const double* store = nullptr);
+// Mixed-precision replay of the stored near field on the tensor cores: the
+// FP64 store converted once to FP32 in the product layout (per leaf at the
+// store's offsets: A[NJ t + j][KB e + c], lda = KB x points, self pairs
+// zero), then per call the near densities gathered per leaf (S at soff, rows
+// of NJ x ntri rounded up to 4), the product tasks (per leaf and 128-row
+// tile: C at coff, ldc = KB x points, FP64 sums), the results ADDED to the
+// outputs, and the self pairs added in FP64 from the FP64 store at base.
+void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K, int KB,
+                          const double* store, float* out);
+void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0, const double* g1,
+                    const long long* soff, const int* ntri, float* S, int ntask, const GemmTask* tasks,
+                    const float* A, const long long* coff, double* C, int nsrc, int ntgt, const long long* base,
+                    const double* store);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
                        int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,

@@ -518,6 +518,149 @@ k_near_replay_batch(const NearArgs a, const int* __restrict__ chunk_leaf, const 
   }
 }
 
+// ------------------------------------- stored near field on the tensor cores
+// Mixed-precision replay of the ITER store as one dense product per leaf:
+// out[row][r] = sum_k A[k][row] S[r][k] with k = NJ t + j (near triangle t,
+// density component j of the NJ = 3 x layers stored) and row = KB e + c
+// (evaluation point e, output c of KB = 3 (+ 6 strain)).  A is the FP64
+// store converted once to FP32 in this layout (same per-leaf offsets, lda =
+// KB x points); S the leaf's near densities gathered per right-hand side;
+// the product runs on the tensor cores (gemm_product<float>) and the
+// results are added to the FP64 outputs.
+
+// Position of the leaf's own triangles in its near list (-1 if absent):
+// the self pairs (source point e, near triangle self + e) are applied in
+// FP64 from the FP64 store (k_near_self64), not through the FP32 copy.
+__device__ __forceinline__ int near_self_pos(const NearArgs& a, int i, int leaf) {
+  int pos = 0;
+  for (int b = a.nb_start[i]; b < a.nb_start[i + 1]; b++) {
+    const int sb = a.nb_items[b];
+    if (sb == leaf) return pos;
+    pos += a.box_src_count[sb];
+  }
+  return -1;
+}
+
+// FP64 store [point][near triangle][K] -> FP32 [NJ t + j][KB e + c], per leaf
+// (self pairs zero).
+__global__ void __launch_bounds__(256)
+k_near_store_tc(const NearArgs a, const long long* __restrict__ base, const int* __restrict__ ntri, int K, int KB,
+                const double* __restrict__ store, float* __restrict__ out) {
+  const int i = blockIdx.x, leaf = a.leaves[i];
+  const int sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int nep = sn + (a.do_tgt ? a.box_tgt_count[leaf] : 0);
+  const long long nt = ntri[i], M = (long long)KB * nep, NJ = K / KB, tot = nep * nt * K;
+  const int self = near_self_pos(a, i, leaf);
+  const double* src = store + base[i];
+  float* dst = out + base[i];
+  for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.y * blockDim.x) {
+    const long long e = q / (nt * K), rem = q % (nt * K), t = rem / K, jc = rem % K;
+    const long long j = jc / KB, c = jc % KB;
+    const bool is_self = e < sn && self >= 0 && t == self + e;
+    dst[(t * NJ + j) * M + e * KB + c] = is_self ? 0.0f : (float)src[q];
+  }
+}
+
+// The self pairs of the mixed replay in FP64: per source point of the leaf
+// (thread) and right-hand side (blockIdx.y), the FP64 stored block times the
+// FP64 densities of the point's own triangle, ADDED to the outputs.
+__global__ void __launch_bounds__(128)
+k_near_self64(const NearArgs a, int R, int K, int KB, const double* __restrict__ g0, const double* __restrict__ g1,
+              const long long* __restrict__ base, const int* __restrict__ ntri, const double* __restrict__ store,
+              int nsrc) {
+  const int i = blockIdx.x, r = blockIdx.y, leaf = a.leaves[i];
+  const int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int self = near_self_pos(a, i, leaf);
+  if (self < 0) return;
+  const long long nt = ntri[i];
+  const int NJ = K / KB;
+  for (int e = threadIdx.x; e < sn; e += blockDim.x) {
+    const int pid = s0 + e;
+    const double* blk = store + base[i] + ((long long)e * nt + self + e) * K;
+    double out[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int j = 0; j < NJ; j++) {
+      const double sv = (j >= 3 ? g1 : g0)[((size_t)pid * 3 + (j % 3)) * R + r];
+      for (int c = 0; c < KB; c++) out[c] += blk[j * KB + c] * sv;
+    }
+    double* U = a.u_src + 3 * ((size_t)nsrc * r + pid);
+    for (int c = 0; c < 3; c++) U[c] += out[c];
+    if (KB == 9 && a.dostrain_src) {
+      double* E = a.e_src + 6 * ((size_t)nsrc * r + pid);
+      for (int c = 0; c < 6; c++) E[c] += out[3 + c];
+    }
+  }
+}
+
+// Near densities of each leaf as the B operand: S[r][NJ t + j] at soff[leaf]
+// (row length ntri NJ rounded up to 4), from sigma[(tri 3 + comp) R + r]
+// (g0: the first layer stored, g1: the double layer when both are).
+__global__ void __launch_bounds__(256)
+k_near_sigma_tc(const NearArgs a, int R, int NJ, const double* __restrict__ g0, const double* __restrict__ g1,
+                const long long* __restrict__ soff, const int* __restrict__ ntri, float* __restrict__ S) {
+  const int i = blockIdx.x;
+  const int K = NJ * ntri[i], Kp = (K + 3) & ~3;
+  float* o = S + soff[i];
+  int pos = 0;
+  for (int b = a.nb_start[i]; b < a.nb_start[i + 1]; b++) {
+    const int sb = a.nb_items[b];
+    const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+    for (int q = threadIdx.x; q < trn * NJ * R; q += blockDim.x) {
+      const int r = q / (trn * NJ), k = q % (trn * NJ), t = k / NJ, j = k % NJ;
+      const double* sg = j >= 3 ? g1 : g0;
+      o[(size_t)r * Kp + (size_t)(pos + t) * NJ + j] = (float)sg[((size_t)(tr0 + t) * 3 + (j % 3)) * R + r];
+    }
+    pos += trn;
+  }
+}
+
+// Add the products C[r][KB e + c] (per leaf at coff) to the outputs.
+__global__ void __launch_bounds__(256)
+k_near_scatter_tc(const NearArgs a, int R, int KB, const long long* __restrict__ coff, const double* __restrict__ C,
+                  int nsrc, int ntgt) {
+  const int i = blockIdx.x, r = blockIdx.y, leaf = a.leaves[i];
+  const int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int t0 = a.box_tgt_start[leaf], tn = a.do_tgt ? a.box_tgt_count[leaf] : 0;
+  const int M = KB * (sn + tn);
+  const double* Cr = C + coff[i] + (size_t)r * M;
+  for (int row = threadIdx.x; row < M; row += blockDim.x) {
+    const int e = row / KB, c = row % KB;
+    const bool src = e < sn;
+    const int pid = src ? s0 + e : t0 + (e - sn);
+    const size_t np = src ? (size_t)nsrc : (size_t)ntgt;
+    const double v = Cr[row];
+    if (c < 3) {
+      (src ? a.u_src : a.u_tgt)[3 * (np * r + pid) + c] += v;
+    } else if (src ? a.dostrain_src : a.dostrain_tgt) {
+      (src ? a.e_src : a.e_tgt)[6 * (np * r + pid) + (c - 3)] += v;
+    }
+  }
+}
+
+void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K, int KB,
+                          const double* store, float* out) {
+  if (a.nleaf <= 0) return;
+  k_near_store_tc<<<dim3(a.nleaf, 64), 256, 0, st>>>(a, base, ntri, K, KB, store, out);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0, const double* g1,
+                    const long long* soff, const int* ntri, float* S, int ntask, const GemmTask* tasks,
+                    const float* A, const long long* coff, double* C, int nsrc, int ntgt, const long long* base,
+                    const double* store) {
+  if (a.nleaf <= 0 || R <= 0) return;
+  k_near_sigma_tc<<<a.nleaf, 256, 0, st>>>(a, R, NJ, g0, g1, soff, ntri, S);
+  count_launch();
+  launch_gemm_tc(st, ntask, tasks, A, S, C, tc_err_ptr(), R <= 64 ? 64 : 128);
+  k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
+  count_launch();
+  if (a.do_src) {
+    k_near_self64<<<dim3(a.nleaf, R), 128, 0, st>>>(a, R, NJ * KB, KB, g0, g1, base, ntri, store, nsrc);
+    count_launch();
+  }
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
 // ---------------------------------------------------------------- launchers
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,
                      const double* sdl, int dosl, int dodl, TriRec* out) {

@@ -432,6 +432,8 @@ void Plan::build_worklists() {
   }
   h2d(near_ntri_, near_ntri_h_, st_);
   store_valid_ = false;
+  store_gen_++;
+  ntc_key_ = -1;
   chunk_key_ = -1;
   near_pairs_ = 0;
   {
@@ -699,12 +701,76 @@ int Plan::store_alloc(int flags, double rlam, double rmu) {
   if ((double)tot * 8.0 > 0.9 * (double)freeb + (double)store_.cap * 8.0) return IER_ALLOC;
   store_.resize((size_t)tot);
   h2d(near_base_, base, st_);
+  near_base_h_ = base;
   store_K_ = K;
   store_flags_ = flags;
   store_lam_ = rlam;
   store_mu_ = rmu;
   store_valid_ = false;
+  store_gen_++;
+  ntc_key_ = -1;
   return IER_OK;
+}
+
+// The FP32 product-layout copy of the stored near field (converted once per
+// store; false: not enough memory, the tensor cores are off, or no store --
+// the caller then replays the FP64 store).
+bool Plan::near_tc_ready(const NearArgs& na) {
+  if (!tc_enabled() || !store_valid_ || store_K_ <= 0) return false;
+  if (store_tc_gen_ == store_gen_) return true;
+  if (capturing_) return false;
+  const size_t tot = store_.size();
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  if ((double)tot * 4.0 > 0.8 * (double)freeb + 4.0 * (double)store_f_.cap) return false;
+  store_f_.resize(tot);
+  NearArgs sa = na;
+  sa.do_src = (store_flags_ >> 2) & 1;
+  sa.do_tgt = (store_flags_ >> 3) & 1;
+  const int KB = 3 + 6 * ((store_flags_ >> 4) & 1);
+  launch_near_store_tc(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, KB, store_.get(), store_f_.get());
+  store_tc_gen_ = store_gen_;
+  return true;
+}
+
+// Mixed replay of the stored near field for R <= 128 right-hand sides: per
+// leaf the product of its FP32 blocks (KB x points rows, NJ x near triangles
+// columns) with its near densities, on the tensor cores with FP64 sums, and
+// the self pairs in FP64; the per-leaf tasks are cut once per (R, store
+// layout).
+void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt) {
+  const int KB = 3 + 6 * ((store_flags_ >> 4) & 1), NJ = store_K_ / KB;
+  const int do_src = (store_flags_ >> 2) & 1, do_tgt = (store_flags_ >> 3) & 1;
+  const long long key = ((long long)R << 8) | store_flags_;
+  if (ntc_key_ != key) {
+    std::vector<long long> so, co;
+    std::vector<GemmTask> tasks;
+    long long stot = 0, ctot = 0;
+    for (size_t i = 0; i < near_ntri_h_.size(); i++) {
+      const long long nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+      const long long M = KB * nep, K = (long long)NJ * near_ntri_h_[i], Kp = (K + 3) & ~3LL;
+      so.push_back(stot);
+      co.push_back(ctot);
+      for (int c0 = 0; c0 < R; c0 += 128)
+        for (long long r0 = 0; r0 < M; r0 += 128)
+          tasks.push_back({near_base_h_[i], stot, ctot, (int)M, R, (int)K, (int)M, (int)Kp, (int)M, (int)r0, c0});
+      stot += R * Kp;
+      ctot += R * M;
+    }
+    h2d(ntc_soff_, so, st_);
+    h2d(ntc_coff_, co, st_);
+    h2d(ntc_tasks_, tasks, st_);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st_));  // the host vectors go away
+    ntc_ntask_ = (int)tasks.size();
+    ntc_stot_ = stot;
+    ntc_ctot_ = ctot;
+    ntc_key_ = key;
+  }
+  ntc_scratch_.resize((size_t)ntc_stot_);
+  ntc_cbuf_.resize((size_t)ntc_ctot_);
+  launch_near_tc(st_, na, R, NJ, KB, g0, g1, ntc_soff_.get(), near_ntri_.get(), ntc_scratch_.get(), ntc_ntask_,
+                 ntc_tasks_.get(), store_f_.get(), ntc_coff_.get(), ntc_cbuf_.get(), n, nt, near_base_.get(),
+                 store_.get());
 }
 
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
@@ -803,6 +869,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     if (mode == 1) {
       launch_near_store(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, 1, store_.get());
       store_valid_ = true;
+      store_gen_++;
     }
     NearArgs ra = na;  // outputs as requested by this call
     ra.dostrain_src = sa.dostrain_src;
@@ -1300,11 +1367,16 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     sa.dostrain_src = sa.dostrain_tgt = (store_flags_ >> 4) & 1;
     launch_near_store(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, 1, store_.get());
     store_valid_ = true;
+    store_gen_++;
   }
-  if (dosl || dodl)
-    launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, (ds_src || ds_tgt) ? 1 : 0,
-                      ssl_s_.get(), sdl_s_.get(), n, n, nt, mode ? near_base_.get() : nullptr,
-                      mode ? near_ntri_.get() : nullptr, mode ? store_.get() : nullptr);
+  if (dosl || dodl) {
+    if (mixed && mode && near_tc_ready(na))
+      near_tc(na, R, dosl ? ssl_s_.get() : sdl_s_.get(), sdl_s_.get(), n, nt);
+    else
+      launch_near_batch(st_, na, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), R, (ds_src || ds_tgt) ? 1 : 0,
+                        ssl_s_.get(), sdl_s_.get(), n, n, nt, mode ? near_base_.get() : nullptr,
+                        mode ? near_ntri_.get() : nullptr, mode ? store_.get() : nullptr);
+  }
   rec(7);
   if (do_src) {
     k_scatter_out<<<dim3((n + 255) / 256, R), 256, 0, st_>>>(n, tr_.iz.get(), u_s_.get(), e_s_.get(), d_u_src,
@@ -1870,7 +1942,10 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
     tot += timings.total;
   }
   timings.total = tot;
-  if (mode == 0) store_valid_ = false;  // the blocks served this call only
+  if (mode == 0) {
+    store_valid_ = false;  // the blocks served this call only
+    store_gen_++;
+  }
   return IER_OK;
 }
 
@@ -1997,6 +2072,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     ha.lam = rlam; ha.mu = rmu;
     launch_hs_store(st_, ha, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), store_.get());
     store_valid_ = true;
+    store_gen_++;
   }
   NearArgs na;
   na.nleaf = nnear_;

@@ -262,6 +262,18 @@ class Plan {
   std::vector<int> near_sc_h_, near_tc_h_, near_ntri_h_;  // per near leaf
   DevBuf<int> near_ntri_;
   DevBuf<long long> near_base_;
+  std::vector<long long> near_base_h_;
+  // FP32 product-layout copy of the stored near field for mixed replays on
+  // the tensor cores (built from store generation store_tc_gen_), the
+  // per-leaf product tasks and the density / product scratch
+  DevBuf<float> store_f_, ntc_scratch_;
+  DevBuf<double> ntc_cbuf_;
+  DevBuf<long long> ntc_soff_, ntc_coff_;
+  DevBuf<GemmTask> ntc_tasks_;
+  long long store_gen_ = 0, store_tc_gen_ = -1, ntc_key_ = -1, ntc_stot_ = 0, ntc_ctot_ = 0;
+  int ntc_ntask_ = 0;
+  bool near_tc_ready(const NearArgs& na);
+  void near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt);
   DevBuf<double> store_;
   bool store_valid_ = false;
   int store_flags_ = 0, store_K_ = 0;

@@ -111,10 +111,12 @@ struct Quad {
 
 }  // namespace
 
-template <int BN>
+// TC: the accumulation (and output) type, float or double (the K-tile sums
+// of the tensor cores added in FP64: the near-field replay)
+template <int BN, class TC>
 __global__ void __launch_bounds__(TC_THREADS, 1)
 k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
-          float* __restrict__ Cm, int* __restrict__ err) {
+          TC* __restrict__ Cm, int* __restrict__ err) {
   constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
   constexpr int RG = BN / 8;       // 8-row groups of B
   constexpr int NB = BN / 32;      // B quads per thread and K tile
@@ -216,9 +218,9 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   // into FP32 registers (round to nearest), which keeps the product as
   // accurate as an FP32 dot product.  Accumulator (t & 1) holds tile t.
   const int quarter = warp & 3, half = warp >> 2;
-  float acc[NHALF];
+  TC acc[NHALF];
 #pragma unroll
-  for (int j = 0; j < NHALF; j++) acc[j] = 0.0f;
+  for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
   auto drain = [&](int u) {  // add the accumulator of tile u into acc
     const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
 #pragma unroll
@@ -233,7 +235,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
           : "r"(addr));
       asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += __uint_as_float(r[j]);
+      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += (TC)__uint_as_float(r[j]);
     }
   };
   bool ok = true;
@@ -288,7 +290,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   } else {
     const int row = t.row0 + 32 * quarter + lane;
     if (row < t.M) {
-      float* Cp = Cm + t.c_off + row;
+      TC* Cp = Cm + t.c_off + row;
 #pragma unroll
       for (int j = 0; j < NHALF; j++) {
         const int col = t.col0 + NHALF * half + j;
@@ -336,19 +338,31 @@ bool tc_enabled() {
   return on;
 }
 
-void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
-                    int* err, int bn) {
+template <class TC>
+static void launch_gemm_tc_t(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B,
+                             TC* C, int* err, int bn) {
   if (ntask <= 0) return;
   if (bn == 64) {
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tc<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<64>()));
-    k_gemm_tc<64><<<ntask, TC_THREADS, tc_smem<64>(), st>>>(tasks, A, B, C, err);
+    EFMM_CUDA_TRY(
+        cudaFuncSetAttribute(k_gemm_tc<64, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<64>()));
+    k_gemm_tc<64, TC><<<ntask, TC_THREADS, tc_smem<64>(), st>>>(tasks, A, B, C, err);
   } else {
     EFMM_CUDA_TRY(
-        cudaFuncSetAttribute(k_gemm_tc<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()));
-    k_gemm_tc<128><<<ntask, TC_THREADS, tc_smem<128>(), st>>>(tasks, A, B, C, err);
+        cudaFuncSetAttribute(k_gemm_tc<128, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()));
+    k_gemm_tc<128, TC><<<ntask, TC_THREADS, tc_smem<128>(), st>>>(tasks, A, B, C, err);
   }
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, float* C,
+                    int* err, int bn) {
+  launch_gemm_tc_t<float>(st, ntask, tasks, A, B, C, err, bn);
+}
+
+void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B, double* C,
+                    int* err, int bn) {
+  launch_gemm_tc_t<double>(st, ntask, tasks, A, B, C, err, bn);
 }
 
 }  // namespace efmm

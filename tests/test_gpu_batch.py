@@ -186,9 +186,13 @@ def test_batch_iter_store_and_replay(gpu, R):
     e = _batch_mode(P, d, R, s2, d2, n, m, 0)
     for x, y in zip(c, e):
         assert rel(x, y) < SAME
-    # mixed precision on the stored near field
+    # mixed precision on the stored near field (its FP32 copy replayed on
+    # the tensor cores): all four outputs within the FP32 tolerance
     f = _batch_mode(P, d, R, s2, d2, n, m, 2, precision=1)
-    assert rel(f[0], e[0]) < 0.5e-6 and rel(f[2], e[2]) < 0.5e-6
+    errs = [rel(x, y) for x, y in zip(f, e)]
+    print("mixed replay vs FP64:", " ".join(f"{v:.2e}" for v in errs))
+    assert errs[0] < 0.5e-6 and errs[2] < 0.5e-6 and errs[1] < 0.5e-5 and errs[3] < 0.5e-5
+    assert max(errs) > 1e-13  # the FP32 path ran
     # the same store serves the single-density ITER call
     u = torch.zeros((n, 3), dtype=torch.float64, device="cuda")
     ee = torch.zeros((n, 3, 3), dtype=torch.float64, device="cuda")
@@ -219,6 +223,9 @@ def test_batch_iter_single_layer_displacement_only(gpu):
     a = _batch_mode(P, d, R, s2, None, n, m, 2, strain=False)
     b = _batch_mode(P, d, R, s2, None, n, m, 0, strain=False)
     assert rel(a[0], b[0]) < SAME and rel(a[2], b[2]) < SAME
+    # single-layer store without strain rows (KB = 3) replayed in FP32
+    c = _batch_mode(P, d, R, s2, None, n, m, 2, strain=False, precision=1)
+    assert rel(c[0], b[0]) < 1e-5 and rel(c[2], b[2]) < 1e-5 and rel(c[0], b[0]) > 1e-13
     # a replay asking for strain the store does not hold is a mismatch
     with pytest.raises(gpu.ElfmmError):
         _batch_mode(P, d, R, s2, None, n, m, 2)
