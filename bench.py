@@ -513,6 +513,11 @@ def run_hsbatch(args, rank, world, local_rank):
         F.evaluate_batch(1.0, 1.0, R, None, dsdl, uf, ef, precision=precision, mode=mode, graph=graph)
         I.evaluate_image(1.0, 1.0, R, None, dsdl, ui, ei, precision=precision, mode=mode, graph=graph)
 
+    # mixed form's truncation floor (the library default): orders for
+    # max(eps(iprec), 5e-8), no truncation finer than the FP32 rounding
+    mixed_floor = 5e-8
+    p_mixed = F.set_mixed_floor(mixed_floor)
+    I.set_mixed_floor(mixed_floor)
     t0 = time.perf_counter()
     step(mode=1)  # first call of the sequence: near fields stored
     store_s = time.perf_counter() - t0
@@ -579,6 +584,24 @@ def run_hsbatch(args, rank, world, local_rank):
     h2d = 8 * 3 * n * R
     d2h = 8 * (3 * n * R + 9 * n * R)
 
+    # the mixed form at the iprec orders (no truncation floor), beside the
+    # headline: plain passes timed with events
+    F.set_mixed_floor(0.0)
+    I.set_mixed_floor(0.0)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record()
+    for _ in range(args.steps):
+        step()
+    pe1.record()
+    pe1.synchronize()
+    mixed_iprec_ms = pe0.elapsed_time(pe1) / args.steps
+    u_mi, e_mi = (uf + ui).clone(), (ef + ei).clone()
+    F.set_mixed_floor(mixed_floor)
+    I.set_mixed_floor(mixed_floor)
+
     # plain FP64: one ITER call pair (direct arrival + image) per right-hand side
     u1 = torch.zeros((R, n, 3), dtype=torch.float64, device=dev)
     e1 = torch.zeros((R, n, 3, 3), dtype=torch.float64, device=dev)
@@ -609,7 +632,8 @@ def run_hsbatch(args, rank, world, local_rank):
     ud = torch.zeros((ns, 3), dtype=torch.float64, device=dev)
     ed = torch.zeros((ns, 3, 3), dtype=torch.float64, device=dev)
     rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-    errs = {"plain_fp64": [0.0, 0.0], "batched_fp64": [0.0, 0.0], "mixed_batched": [0.0, 0.0]}
+    errs = {"plain_fp64": [0.0, 0.0], "batched_fp64": [0.0, 0.0], "mixed_batched": [0.0, 0.0],
+            "mixed_batched_iprec_orders": [0.0, 0.0]}
     for r in (0, R - 1):
         F.evaluate_direct_subset(1.0, 1.0, ns, None, dsdl[r], ud, ed)
         ier, uid, eid = E.hs_image_direct(1.0, 1.0, tri, nrm, None, sdl[r], cen[:ns])
@@ -617,7 +641,8 @@ def run_hsbatch(args, rank, world, local_rank):
         udt = ud + torch.from_numpy(uid).to(dev)
         edt = ed + torch.from_numpy(eid).to(dev)
         for key, (uu, ee) in (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)),
-                              ("mixed_batched", (u_mixed, e_mixed))):
+                              ("mixed_batched", (u_mixed, e_mixed)),
+                              ("mixed_batched_iprec_orders", (u_mi, e_mi))):
             errs[key][0] = max(errs[key][0], rel(uu[r, :ns], udt))
             errs[key][1] = max(errs[key][1], rel(ee[r, :ns], edt))
     if rank != 0:
@@ -669,7 +694,13 @@ def run_hsbatch(args, rank, world, local_rank):
                    "ms_per_step_without_graph": nograph_ms,
                    "forms": {"mixed_batched": value / world, "batched_fp64": b64_value,
                              "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
-                             "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms},
+                             "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms,
+                             "mixed_batched_iprec_orders": evals / (mixed_iprec_ms * 1e-3),
+                             "mixed_iprec_orders_ms": mixed_iprec_ms},
+                   "orders": {"iprec": fi["p"], "mixed": p_mixed, "mixed_floor": mixed_floor,
+                              "rule": "mixed form: expansions and translations truncated at max(eps(iprec), "
+                                      "floor), no finer than its FP32 rounding; plain and batched FP64 forms "
+                                      "at eps(iprec)"},
                    "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
                    "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
                    "stage_ms_free": tf, "stage_ms_image": ti,

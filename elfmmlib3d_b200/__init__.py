@@ -50,7 +50,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "elhfmm3dtriatargiter_"]
+           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "elhfmm3dtriatargiter_"]
 
 
 class ElfmmError(RuntimeError):
@@ -87,6 +87,8 @@ def load():
     L.efmm_plan_flops.argtypes = [_vp, _dp]
     L.efmm_plan_stored_bytes.restype = ctypes.c_longlong
     L.efmm_plan_stored_bytes.argtypes = [_vp]
+    L.efmm_plan_set_mixed_floor.restype = ctypes.c_int
+    L.efmm_plan_set_mixed_floor.argtypes = [_vp, ctypes.c_double, _vp]
     L.efmm_plan_evaluate_batch_graph.restype = ctypes.c_int
     L.efmm_plan_evaluate_batch_graph.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp,
                                                  _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
@@ -480,6 +482,16 @@ class Plan:
     def stored_bytes(self):
         """Device bytes of the stored near field (ITER), 0 if none."""
         return int(self._L.efmm_plan_stored_bytes(self._h))
+
+    def set_mixed_floor(self, eps):
+        """Truncation floor of the mixed form (precision=1): its orders follow
+        max(eps(iprec), eps); eps <= 0 keeps the iprec orders.  Returns the
+        mixed form's expansion order."""
+        order = ctypes.c_int()
+        ier = self._L.efmm_plan_set_mixed_floor(self._h, float(eps), ctypes.byref(order))
+        if ier:
+            raise ElfmmError(ier, "set_mixed_floor")
+        return order.value
 
     def flops_per_column(self):
         """Useful flops per expansion column: P2M, M2M, M2L, L2L, L2T."""

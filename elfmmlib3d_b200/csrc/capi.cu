@@ -127,6 +127,11 @@ extern "C" int efmm_plan_evaluate_image_graph(efmm_plan* p, double rlam, double 
 
 extern "C" long long efmm_plan_stored_bytes(const efmm_plan* p) { return 8 * p->plan->stored_doubles(); }
 
+extern "C" int efmm_plan_set_mixed_floor(efmm_plan* p, double eps, int* order) {
+  if (!p) return IER_BADARG;
+  EFMM_GUARD(p->plan->set_mixed_floor(eps); if (order) *order = p->plan->mixed_order(); return IER_OK;)
+}
+
 extern "C" void efmm_plan_flops(const efmm_plan* p, double* f5) { p->plan->flops_per_column(f5); }
 
 extern "C" int efmm_plan_evaluate_direct(efmm_plan* p, double rlam, double rmu, const double* ssl,

@@ -320,6 +320,8 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   eps_ = iprec_eps(iprec);
   nbox_ = iprec_nbox(iprec, n, nt, iter);
   p_ = eps_ > 0 ? order_for_eps(eps_, 1.5) : 0;
+  eps_mixed_ = mixed_floor_ > 0 ? std::max(eps_, mixed_floor_) : eps_;
+  p_mixed_ = eps_mixed_ > 0 ? std::min(p_, order_for_eps(eps_mixed_, 1.5)) : p_;
   // Expansion orders above 54 (iprec 5, eps 5e-16) exceed the P2M register
   // tiling; at that tolerance the near-field-only evaluation (one box) is used.
   if (p_ > 54) {
@@ -572,7 +574,7 @@ void Plan::build_worklists() {
 }
 
 void Plan::cut_tasks(TransSched& S, int C, const std::vector<int>* dimsp) {
-  if (S.C == C) return;
+  if (S.C == C && S.pool == ops_) return;
   std::vector<TransTask> tasks;
   S.lev_tasks.clear();
   const std::vector<int>& dims = dimsp ? *dimsp : ops_->dims;
@@ -589,10 +591,11 @@ void Plan::cut_tasks(TransSched& S, int C, const std::vector<int>* dimsp) {
   }
   h2d(S.tasks, tasks, st_);
   S.C = C;
+  S.pool = ops_;
 }
 
 void Plan::cut_rot_tasks(TransSched& S, int C, int W) {
-  if (S.rC == C && S.rW == W) return;
+  if (S.rC == C && S.rW == W && S.rpool == ops_) return;
   std::vector<TransTask> tasks;
   S.lev_rtasks.clear();
   S.lev_rdim.clear();
@@ -619,6 +622,7 @@ void Plan::cut_rot_tasks(TransSched& S, int C, int W) {
   h2d(S.rtasks, tasks, st_);
   S.rC = C;
   S.rW = W;
+  S.rpool = ops_;
 }
 
 // factored operators of the pool: host construction once per (device, p, eps)
@@ -923,10 +927,45 @@ void Plan::flops_per_column(double* f) const {
   f[4] = 2.0 * D * 9.0 * (double)(n_ + nt_);  // 9 derivative sums per point
 }
 
+void Plan::set_mixed_floor(double eps) {
+  mixed_floor_ = eps;
+  eps_mixed_ = mixed_floor_ > 0 ? std::max(eps_, mixed_floor_) : eps_;
+  p_mixed_ = eps_mixed_ > 0 ? std::min(p_, order_for_eps(eps_mixed_, 1.5)) : p_;
+  graph_reset();  // a captured pass holds the previous orders
+}
+
+// The mixed form's orders for the duration of a mixed call: order p_mixed_
+// and the operator pool of (p_mixed_, eps_mixed_) in place of the iprec
+// ones (restored on exit); nothing changes when they coincide.
+struct MixedOrders {
+  Plan* P;
+  int p0 = 0;
+  double e0 = 0;
+  OpPool* o0 = nullptr;
+  bool on = false;
+  MixedOrders(Plan* P_, bool mixed) : P(P_) {
+    if (!mixed || !P->far_ || P->p_mixed_ >= P->p_) return;
+    p0 = P->p_;
+    e0 = P->eps_;
+    o0 = P->ops_;
+    on = true;
+    P->p_ = P->p_mixed_;
+    P->eps_ = P->eps_mixed_;
+    P->ensure_ops();
+  }
+  ~MixedOrders() {
+    if (!on) return;
+    P->p_ = p0;
+    P->eps_ = e0;
+    P->ops_ = o0;
+  }
+};
+
 int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
                          int mode) {
   if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
+  MixedOrders orders(this, precision == 1);
   const int n = n_, nt = nt_;
   if (mode) {
     const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
@@ -981,7 +1020,7 @@ template <class T>
 void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
   const int D = 2 * ncoef(p_), C = 4 * R;
   WaveSet& W = p2m_waves_;
-  const long long key = ((long long)R << 8) | (sizeof(T) << 2) | 0;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (sizeof(T) << 2) | 0;
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1057,7 +1096,7 @@ bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
   // density components carried: single layer 0..2, double layer 3..5
   const int sbase = pa.dosl ? 0 : 3, ns = (pa.dosl && pa.dodl) ? 6 : 3;
   WaveSet& W = p2m_waves_;
-  const long long key = ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) | (sizeof(T) << 2) | (image ? 3 : 1);
+  const long long key = ((long long)p_ << 40) | ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) | (sizeof(T) << 2) | (image ? 3 : 1);
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1136,7 +1175,7 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
   WaveSet& W = l2t_waves_;
-  const long long key = ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1;
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1747,7 +1786,7 @@ void Plan::p2m_img_twostage(const P2MArgs& pa, int R, T* mpole) {
   const int D = 2 * ncoef(p_), Cv = 6 * R, Cu = R;
   const size_t nb = tr_.nboxes;
   WaveSet& W = p2m_waves_;
-  const long long key = ((long long)R << 8) | (sizeof(T) << 2) | 2;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (sizeof(T) << 2) | 2;
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1827,7 +1866,7 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
   WaveSet& W = l2t_waves_;
-  const long long key = ((long long)R << 8) | (esz << 4) | 3;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | 3;
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1909,6 +1948,7 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
     const int ier = store_alloc(flags, rlam, rmu);
     if (ier) return ier;
   }
+  MixedOrders orders(this, precision == 1);
   if (far_) {
     ensure_uops();
     if (!img_sched_) {

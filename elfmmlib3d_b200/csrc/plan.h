@@ -69,10 +69,12 @@ struct TransSched {
   std::vector<TransSeg> segs;
   std::vector<std::pair<int, int>> lev;  // segment ranges in execution order
   int C = -1;
+  const void* pool = nullptr;  // operator pool the tasks were cut for
   DevBuf<TransTask> tasks;
   std::vector<std::pair<int, int>> lev_tasks;  // task ranges in execution order
-  // column tiles of the factored kernel (cut for C and tile width)
+  // column tiles of the factored kernel (cut for C, tile width and pool)
   int rC = -1, rW = -1;
+  const void* rpool = nullptr;
   DevBuf<TransTask> rtasks;
   std::vector<std::pair<int, int>> lev_rtasks;  // task ranges in execution order,
   std::vector<int> lev_rdim;                     // each with its largest operator size
@@ -80,6 +82,7 @@ struct TransSched {
     segs.clear();
     lev.clear();
     C = -1;
+    pool = rpool = nullptr;
     lev_tasks.clear();
     rC = rW = -1;
     lev_rtasks.clear();
@@ -131,6 +134,9 @@ class Plan {
                double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode = 0, bool do_far = true);
   long long stored_doubles() const { return store_valid_ ? (long long)store_.size() : 0; }
   bool store_valid() const { return store_valid_; }
+  // tolerance floor of the mixed form's orders (<= 0: the iprec orders)
+  void set_mixed_floor(double eps);
+  int mixed_order() const { return p_mixed_; }
   // R right-hand sides at once: densities (R, n, 3) user order, outputs
   // (R, n, 3) / (R, n, 3, 3) / (R, nt, 3) / (R, nt, 3, 3) user order.  The
   // tree, lists and operators are shared; the near-field pair responses are
@@ -252,6 +258,12 @@ class Plan {
   cudaStream_t st_;
   int n_ = 0, nt_ = 0, iprec_ = 2, nbox_ = 40, p_ = 0;
   double eps_ = 0.5e-6;
+  // Mixed form (precision 1): expansion and translation orders for
+  // max(eps_, mixed_floor_) -- no truncation finer than the FP32 rounding
+  // of the result; mixed_floor_ <= 0 keeps the iprec orders.
+  double mixed_floor_ = 0.5e-7, eps_mixed_ = 0.5e-6;
+  int p_mixed_ = 0;
+  friend struct MixedOrders;
   bool far_ = false;
   Tree tr_;
   DevBuf<double> tri_s_, nrm_s_, src_s_, tgt_s_;

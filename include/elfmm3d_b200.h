@@ -239,6 +239,14 @@ int efmm_plan_evaluate_image_graph(efmm_plan *plan, double rlam, double rmu, int
 /* Device bytes of the plan's stored near field (0 if none). */
 long long efmm_plan_stored_bytes(const efmm_plan *plan);
 
+/* Orders of the mixed form (precision 1; no counterpart in the reference):
+ * its expansions and translations are truncated at max(eps(iprec), eps)
+ * -- by default eps = 5e-8, about the FP32 rounding of the result, so that
+ * no truncation is finer than the arithmetic; eps <= 0 keeps the iprec
+ * orders.  *order (if not NULL) receives the mixed form's expansion order.
+ * Applies to later calls on the plan's current geometry. */
+int efmm_plan_set_mixed_floor(efmm_plan *plan, double eps, int *order);
+
 /* Direct sum at the first nsub source points only (centroids 0..nsub-1,
  * self-aware), outputs u_src (nsub,3), e_src (nsub,3,3): the FP64 check of a
  * large evaluation on a subset. */

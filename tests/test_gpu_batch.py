@@ -263,3 +263,34 @@ def test_batch_p2m_unit_multipoles_match_node_products(gpu, monkeypatch, R):
         assert rel(x, y) < 1e-6 and rel(x, z) < 1e-6
     P.close()
     Pn.close()
+
+
+def test_mixed_form_orders_floor(gpu):
+    # the mixed form truncates no finer than its FP32 rounding (default
+    # floor 5e-8): at iprec 3 its order drops below the iprec order and its
+    # error against the FP64 form stays at the FP32 level; floor 0 restores
+    # the iprec orders
+    P, tri, nrm, cen, tg, d = _plan(gpu, level=3, ntarg=100, iprec=3, seed=31)
+    n, m = len(cen), len(tg)
+    R = 8
+    rng = np.random.default_rng(37)
+    ssl, sdl = rng.normal(size=(R, n, 3)), rng.normal(size=(R, n, 3))
+    ref = _batch(P, d, R, ssl, sdl, n, m)
+    p_iprec = P.info()["p"]
+    torch = _t()
+    outs = {}
+    for floor in (5e-8, 0.0):
+        pm = P.set_mixed_floor(floor)
+        assert (pm < p_iprec) if floor > 0 else (pm == p_iprec)
+        o = [torch.zeros((R, n, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, m, 3), dtype=torch.float64, device="cuda"),
+             torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda")]
+        P.evaluate_batch(1.3, 0.7, R, d(ssl), d(sdl), *o, precision=1)
+        outs[floor] = [t.cpu().numpy() for t in o]
+        errs = [rel(x, y) for x, y in zip(outs[floor], ref)]
+        print(f"floor {floor:g}: order {pm} (iprec {p_iprec}), mixed vs FP64:", " ".join(f"{v:.2e}" for v in errs))
+        assert errs[0] < 1e-6 and errs[2] < 1e-6 and errs[1] < 1e-5 and errs[3] < 1e-5
+    # the FP64 form keeps the iprec orders whatever the mixed floor
+    assert rel(_batch(P, d, R, ssl, sdl, n, m)[0], ref[0]) < SAME
+    P.close()
