@@ -13,6 +13,8 @@
 #include <cmath>
 #include <random>
 #include <thread>
+#include <cstdlib>
+#include <cstring>
 #include "common.cuh"
 #include "harmonics.cuh"
 #include "fmm.h"
@@ -555,6 +557,185 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
   }
 }
 
+// FP32 factored translations with one warp per degree block (rotations) or
+// order block (shift along z), in place: the 16 columns of the task stay in
+// one shared buffer X[row][16]; a warp owns whole blocks (lane l: output
+// rows 2l, 2l + 1 of the block, all 16 columns in registers), reads its
+// block's operator columns from global memory (one coalesced 8-byte load per
+// lane and k) and the input rows of X as broadcasts, and writes its rows
+// back after the block's reads (__syncwarp).  Blocks are spread over the
+// warps by size (longest first).  For orders p <= 31 (blocks of <= 64 rows);
+// half the shared memory of k_translate_rot, two CTAs of 12 warps per SM.
+constexpr int ROTW_THREADS = 384, ROTW_NCT = 16, ROTW_PMAX = 31, ROTW_NW = ROTW_THREADS / 32;
+
+// Warp of degree block n at order p (order block p - n of the shift): the
+// blocks, (2n + 2)^2 entries each, spread largest first onto the least
+// loaded warp; fixed per order, built at compile time.
+struct RotwOwners {
+  unsigned char o[ROTW_PMAX + 1][ROTW_PMAX + 1];
+};
+constexpr RotwOwners make_rotw_owners() {
+  RotwOwners r{};
+  for (int p = 0; p <= ROTW_PMAX; p++) {
+    int load[ROTW_NW] = {};
+    for (int n = p; n >= 0; n--) {
+      int best = 0;
+      for (int w = 1; w < ROTW_NW; w++)
+        if (load[w] < load[best]) best = w;
+      r.o[p][n] = (unsigned char)best;
+      load[best] += (n + 1) * (n + 1);
+    }
+  }
+  return r;
+}
+__constant__ RotwOwners c_rotw_owners = make_rotw_owners();
+// shared memory: X [dim][16] floats, then the source column offsets [16] (8-byte aligned)
+__host__ __device__ inline size_t rotw_cbase_off(int dim) { return sizeof(float) * (size_t)dim * ROTW_NCT; }
+
+__global__ void __launch_bounds__(ROTW_THREADS, 2)
+k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
+                  const RotOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
+                  const float* __restrict__ src, float* __restrict__ dst) {
+  constexpr int NCT = ROTW_NCT, G = NCT / 4;
+  extern __shared__ __align__(16) unsigned char rw_smem[];
+  const TransTask t = tasks[blockIdx.x];
+  const RotOp op = ops[t.group];
+  const int p = op.p, dim = (p + 1) * (p + 2);
+  float* X = reinterpret_cast<float*>(rw_smem);                                   // [dim][NCT]
+  long long* cbase = reinterpret_cast<long long*>(rw_smem + rotw_cbase_off(dim));  // [NCT]: source columns
+  const unsigned char* owner = c_rotw_owners.o[p];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid < NCT) {
+    const int col = t.col0 + tid;
+    long long b = -1;
+    if (col < t.ncols) {
+      const TransPair pr = pairs[t.pair0 + col / C];
+      b = ((long long)pr.src * C + col % C) * D;
+    }
+    cbase[tid] = b;
+  }
+  __syncthreads();
+  for (int q = tid; q < dim * 4; q += ROTW_THREADS) {
+    const int r = q % dim, cg = q / dim;
+    float v[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+      const long long b = cbase[cg * G + g];
+      v[g] = b >= 0 ? src[b + r] : 0.0f;
+    }
+    *reinterpret_cast<float4*>(X + (size_t)r * NCT + cg * G) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  __syncthreads();
+  auto put_rows = [&](int ra, int rb, const float* a0, const float* a1) {
+#pragma unroll
+    for (int q = 0; q < NCT / 4; q++) {
+      *reinterpret_cast<float4*>(X + (size_t)ra * NCT + 4 * q) =
+          make_float4(a0[4 * q], a0[4 * q + 1], a0[4 * q + 2], a0[4 * q + 3]);
+      *reinterpret_cast<float4*>(X + (size_t)rb * NCT + 4 * q) =
+          make_float4(a1[4 * q], a1[4 * q + 1], a1[4 * q + 2], a1[4 * q + 3]);
+    }
+  };
+  auto rotate = [&](long long base) {
+    for (int n = 0; n <= p; n++) {
+      if (owner[n] != warp) continue;
+      const int bb = 2 * n + 2, r0 = n * (n + 1);
+      const bool act = 2 * lane < bb;
+      const float* o = pool + base + rot_block_off(n) + 2 * lane;  // column-major: (row, k) at k bb + row
+      float a0[NCT], a1[NCT];
+#pragma unroll
+      for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
+      constexpr int UNR = 2;
+      int k = 0;
+      for (; k + UNR <= bb; k += UNR) {
+        float2 w[UNR];
+#pragma unroll
+        for (int u = 0; u < UNR; u++)
+          w[u] = act ? *reinterpret_cast<const float2*>(o + (size_t)(k + u) * bb) : make_float2(0.f, 0.f);
+#pragma unroll
+        for (int u = 0; u < UNR; u++) {
+          const float4* xr = reinterpret_cast<const float4*>(X + (size_t)(r0 + k + u) * NCT);
+#pragma unroll
+          for (int q = 0; q < NCT / 4; q++) {
+            const float4 x = xr[q];
+            a0[4 * q] += w[u].x * x.x; a0[4 * q + 1] += w[u].x * x.y;
+            a0[4 * q + 2] += w[u].x * x.z; a0[4 * q + 3] += w[u].x * x.w;
+            a1[4 * q] += w[u].y * x.x; a1[4 * q + 1] += w[u].y * x.y;
+            a1[4 * q + 2] += w[u].y * x.z; a1[4 * q + 3] += w[u].y * x.w;
+          }
+        }
+      }
+      for (; k < bb; k++) {
+        const float2 w = act ? *reinterpret_cast<const float2*>(o + (size_t)k * bb) : make_float2(0.f, 0.f);
+        const float4* xr = reinterpret_cast<const float4*>(X + (size_t)(r0 + k) * NCT);
+#pragma unroll
+        for (int q = 0; q < NCT / 4; q++) {
+          const float4 x = xr[q];
+          a0[4 * q] += w.x * x.x; a0[4 * q + 1] += w.x * x.y; a0[4 * q + 2] += w.x * x.z; a0[4 * q + 3] += w.x * x.w;
+          a1[4 * q] += w.y * x.x; a1[4 * q + 1] += w.y * x.y; a1[4 * q + 2] += w.y * x.z; a1[4 * q + 3] += w.y * x.w;
+        }
+      }
+      __syncwarp();
+      if (act) put_rows(r0 + 2 * lane, r0 + 2 * lane + 1, a0, a1);
+      __syncwarp();
+    }
+  };
+  rotate(op.fw);
+  __syncthreads();
+  // shift along z: order block m (rows (n, m), n = m..p), owned like degree block p - m
+  for (int m = 0; m <= p; m++) {
+    if (owner[p - m] != warp) continue;
+    const int bz = 2 * (p - m + 1);
+    const bool act = 2 * lane < bz;
+    const float* o = pool + op.z + z_block_off(p, m) + 2 * lane;  // column-major: (row, col) at col bz + row
+    float a0[NCT], a1[NCT];
+#pragma unroll
+    for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
+    for (int k = m; k <= p; k++) {
+      const int c2 = 2 * (k - m);
+      const float2 wr = act ? *reinterpret_cast<const float2*>(o + (size_t)c2 * bz) : make_float2(0.f, 0.f);
+      const float2 wi = act ? *reinterpret_cast<const float2*>(o + (size_t)(c2 + 1) * bz) : make_float2(0.f, 0.f);
+      const int rk = 2 * (k * (k + 1) / 2 + m);
+      const float4* xre = reinterpret_cast<const float4*>(X + (size_t)rk * NCT);
+      const float4* xim = reinterpret_cast<const float4*>(X + (size_t)(rk + 1) * NCT);
+#pragma unroll
+      for (int q = 0; q < NCT / 4; q++) {
+        const float4 xr = xre[q], xi = xim[q];
+        a0[4 * q] += wr.x * xr.x + wi.x * xi.x; a0[4 * q + 1] += wr.x * xr.y + wi.x * xi.y;
+        a0[4 * q + 2] += wr.x * xr.z + wi.x * xi.z; a0[4 * q + 3] += wr.x * xr.w + wi.x * xi.w;
+        a1[4 * q] += wr.y * xr.x + wi.y * xi.x; a1[4 * q + 1] += wr.y * xr.y + wi.y * xi.y;
+        a1[4 * q + 2] += wr.y * xr.z + wi.y * xi.z; a1[4 * q + 3] += wr.y * xr.w + wi.y * xi.w;
+      }
+    }
+    __syncwarp();
+    if (act) {
+      const int n = m + lane, cc = n * (n + 1) / 2 + m;
+      put_rows(2 * cc, 2 * cc + 1, a0, a1);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  rotate(op.bk);
+  __syncthreads();
+  for (int j = 0; j < NCT; j++) {
+    const int col = t.col0 + j;
+    if (col >= t.ncols) break;
+    const TransPair pr = pairs[t.pair0 + col / C];
+    float* dp = dst + ((size_t)pr.dst * C + col % C) * D;
+    const float al = (float)pr.alpha;
+    for (int r = tid; r < dim; r += ROTW_THREADS) atomicAdd(dp + r, al * X[(size_t)r * NCT + j]);
+  }
+}
+
+// The warp-block kernel for launches of orders pmin..31 (smaller orders
+// have fewer blocks than warps: the coefficient-tile kernel serves them).
+bool rot_warp_blocks_ok(int maxdim) {
+  static const int pmin = [] {
+    const char* e = getenv("ELFMM3D_ROTW_PMIN");
+    return e ? atoi(e) : 20;
+  }();
+  return maxdim <= (ROTW_PMAX + 1) * (ROTW_PMAX + 2) && maxdim >= (pmin + 1) * (pmin + 2);
+}
+
 int rot_cols_per_cta(int maxdim, int elem_bytes) {
   (void)maxdim;
   return elem_bytes == 4 ? 16 : 8;
@@ -564,6 +745,22 @@ template <class T>
 void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                           const RotOp* ops, const T* pool, int D, int C, int maxdim, const T* src, T* dst) {
   if (ntask <= 0) return;
+  static const bool warp_blocks = [] {
+    const char* e = getenv("ELFMM3D_ROT");
+    return !(e && strcmp(e, "tiles") == 0);
+  }();
+  if constexpr (sizeof(T) == 4) {
+    if (warp_blocks && rot_warp_blocks_ok(maxdim)) {
+      const size_t smem = rotw_cbase_off(maxdim) + sizeof(long long) * ROTW_NCT;
+      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_translate_rot_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k_translate_rot_w<<<ntask, ROTW_THREADS, smem, st>>>(tasks, pairs, ops, reinterpret_cast<const float*>(pool),
+                                                             D, C, reinterpret_cast<const float*>(src),
+                                                             reinterpret_cast<float*>(dst));
+      count_launch();
+      EFMM_CUDA_TRY(cudaGetLastError());
+      return;
+    }
+  }
   constexpr int NCT = sizeof(T) == 4 ? 16 : 8;
   const size_t smem = sizeof(T) * 2 * (size_t)maxdim * NCT;
   if (smem > 227 * 1024) throw CudaError{(int)cudaErrorInvalidValue};
