@@ -664,12 +664,31 @@ def run_hsbatch(args, rank, world, local_rank):
         peak_source += f" (its bf16_tflops is {bf16})"
     except (OSError, ValueError, TypeError):
         pass
-    roof = {"kernel": "k_gemm_tc (P2M products, tcgen05.mma kind::tf32, free-space and image plans)",
-            "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": (achieved / peak) if peak else None, "traffic": None, "peak_source": peak_source,
-            "useful_fp32_tflops": useful,
-            "algorithmic": f"{prod_flops:.4g} useful FP32 flop per step (P2M features x weights) in "
-                           f"{prod_ms:.1f} ms of product launches; 3 TF32 MMAs per FP32 product"}
+    roof_tc = {"kernel": "k_gemm_tc (P2M products, tcgen05.mma kind::tf32, free-space and image plans)",
+               "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+               "frac": (achieved / peak) if peak else None, "traffic": None, "peak_source": peak_source,
+               "useful_fp32_tflops": useful,
+               "algorithmic": f"{prod_flops:.4g} useful FP32 flop per step (unit multipoles x densities) in "
+                              f"{prod_ms:.1f} ms of product launches; 3 TF32 MMAs per FP32 product"}
+    # the dominant kernels of the step (ncu launch shares): the factored
+    # translations (k_translate_rot_w / k_translate_rot, FP32 FMA pipe),
+    # flops counted per pair and column as they run, time = the M2M + M2L +
+    # L2L stage events of both plans, against the measured SGEMM rate
+    trf = F.translation_flops(R, 1)
+    tri_ = I.translation_flops(R, 1)
+    tr_flops = sum(trf.values()) + sum(tri_.values())
+    tr_ms = float(np.mean([sum(s_[0][k] + s_[1][k] for k in ("m2m", "m2l", "l2l")) for s_ in stages]))
+    peak32 = gemm_peak(torch, dev, torch.float32)
+    tr_ach = tr_flops / (tr_ms * 1e-3) / 1e12
+    roof = {"kernel": "k_translate_rot_w + k_translate_rot (factored M2M / M2L / L2L, FP32, both plans; "
+                      "the largest share of the step's launch time)",
+            "bound": "fp32", "achieved": tr_ach, "peak": peak32, "unit": "TFLOP/s",
+            "frac": tr_ach / peak32 if peak32 else None, "traffic": None,
+            "peak_source": "measured cuBLAS SGEMM 8192^3 with TF32 off (best of 5) in this run; the FP32 FMA "
+                           "pipe (MEASURED_PEAKS.json has no FP32 entry)",
+            "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
+                           f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages",
+            "flops_by_stage": {"free": trf, "image": tri_}}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
         ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
@@ -713,6 +732,7 @@ def run_hsbatch(args, rank, world, local_rank):
                           "strain back to pinned host memory, every step"},
         "gpu_launches": launches,
         "roofline": roof,
+        "roofline_tc": roof_tc,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }

@@ -50,7 +50,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "elhfmm3dtriatargiter_"]
+           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_"]
 
 
 class ElfmmError(RuntimeError):
@@ -89,6 +89,8 @@ def load():
     L.efmm_plan_stored_bytes.argtypes = [_vp]
     L.efmm_plan_set_mixed_floor.restype = ctypes.c_int
     L.efmm_plan_set_mixed_floor.argtypes = [_vp, ctypes.c_double, _vp]
+    L.efmm_plan_translation_flops.restype = ctypes.c_int
+    L.efmm_plan_translation_flops.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _dp]
     L.efmm_plan_evaluate_batch_graph.restype = ctypes.c_int
     L.efmm_plan_evaluate_batch_graph.argtypes = [_vp, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp, _vp,
                                                  _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
@@ -492,6 +494,15 @@ class Plan:
         if ier:
             raise ElfmmError(ier, "set_mixed_floor")
         return order.value
+
+    def translation_flops(self, nrhs, precision=1):
+        """Flops of one pass's translation launches (M2M, M2L, L2L) for nrhs
+        right-hand sides at the orders of the given form."""
+        a = (ctypes.c_double * 3)()
+        ier = self._L.efmm_plan_translation_flops(self._h, int(nrhs), int(precision), a)
+        if ier:
+            raise ElfmmError(ier, "translation_flops")
+        return dict(zip(["m2m", "m2l", "l2l"], list(a)))
 
     def flops_per_column(self):
         """Useful flops per expansion column: P2M, M2M, M2L, L2L, L2T."""

@@ -134,6 +134,11 @@ extern "C" int efmm_plan_set_mixed_floor(efmm_plan* p, double eps, int* order) {
 
 extern "C" void efmm_plan_flops(const efmm_plan* p, double* f5) { p->plan->flops_per_column(f5); }
 
+extern "C" int efmm_plan_translation_flops(efmm_plan* p, int nrhs, int precision, double* f3) {
+  if (!p || nrhs < 1 || !f3) return IER_BADARG;
+  EFMM_GUARD(p->plan->translation_flops(nrhs, precision == 1, f3); return IER_OK;)
+}
+
 extern "C" int efmm_plan_evaluate_direct(efmm_plan* p, double rlam, double rmu, const double* ssl,
                                          const double* sdl, double* u_src, double* e_src,
                                          double* u_tgt, double* e_tgt) {

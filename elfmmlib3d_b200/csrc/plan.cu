@@ -961,6 +961,42 @@ struct MixedOrders {
   }
 };
 
+void Plan::translation_flops(int R, bool mixed, double* f) {
+  for (int i = 0; i < 3; i++) f[i] = 0;
+  if (!far_) return;
+  MixedOrders orders(this, mixed);
+  ensure_ops();
+  const double D = 2.0 * ncoef(p_);
+  const bool fact = factored_ && 2.0 * D * rot_cols_per_cta((int)D, 4) * 4 <= 227.0 * 1024;
+  auto add = [&](const TransSched& S, int k, double cols) {
+    for (const TransSeg& g : S.segs) {
+      if (fact) {
+        const double q = ops_->descs[g.group].p + 1;
+        f[k] += 2.0 * 3.0 * (4.0 * q * (q + 1) * (2 * q + 1) / 6.0) * g.npair * cols;
+      } else {
+        const double dim = ops_->dims[g.group];
+        f[k] += 2.0 * dim * dim * g.npair * cols;
+      }
+    }
+  };
+  if (!mindlin_) {
+    add(m2m_, 0, 4.0 * R);
+    add(m2l_, 1, 4.0 * R);
+    add(l2l_, 2, 4.0 * R);
+    return;
+  }
+  ensure_uops();
+  add(m2m_, 0, 6.0 * R);
+  add(m2m_u_, 0, 1.0 * R);
+  add(m2lv_img_, 1, 6.0 * R);
+  for (const TransSeg& g : m2lu_.segs) {
+    const double dim = ops_->udims[g.group];
+    f[1] += 2.0 * dim * dim * g.npair * R;
+  }
+  add(l2l_img_, 2, 6.0 * R);
+  add(l2l_img_u_, 2, 1.0 * R);
+}
+
 int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
                          int mode) {

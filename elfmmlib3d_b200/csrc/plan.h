@@ -172,6 +172,12 @@ class Plan {
                            double* d_u_tgt, double* d_e_tgt, int precision);
   // useful flops per expansion column of one pass: P2M, M2M, M2L, L2L, L2T
   void flops_per_column(double* f5) const;
+  // Flops of one pass's translation launches for R right-hand sides at the
+  // orders of the given form (mixed: the mixed form's orders and pool):
+  // f3 = M2M, M2L, L2L (factored form: two rotations and the z shift per
+  // pair and column; dense: 2 dim^2); image: the image plan's schedules
+  // (6R Laplace columns, R columns of U with its dense M2L).
+  void translation_flops(int R, bool mixed, double* f3);
   // all-pairs direct sum on the same geometry (no tree needed)
   // nsub > 0: only the first nsub source points (centroids), no targets
   int evaluate_direct(double rlam, double rmu, const double* d_ssl, const double* d_sdl,

@@ -371,12 +371,14 @@ void launch_gemm_tc(cudaStream_t st, int ntask, const GemmTask* tasks, const flo
 // random A (K x M, lda = M + 3), B (N x K, ldb = K + 1) in [-1, 1), C = the
 // tiles of k_gemm_tc.  Returns 0 and the relative l2 error in *rel (and
 // *timeout != 0 if a bounded wait ran out).
-extern "C" int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, unsigned seed, double* rel,
+extern "C" int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, int aligned, unsigned seed, double* rel,
                                            int* timeout) {
   using namespace efmm;
   if (M < 1 || N < 1 || K < 0 || M > 4096 || N > 4096 || K > 65536) return 16;
   if (bn != 64 && bn != 128) return 16;
-  const int lda = M + 3, ldb = K + 1, ldc = M + 1;
+  // aligned: rows of A and B start on 16-byte boundaries (vector loads of
+  // B); else odd leading dimensions (scalar loads)
+  const int lda = aligned ? (M + 3) / 4 * 4 : M + 3, ldb = aligned ? (K + 3) / 4 * 4 : K + 1, ldc = M + 1;
   std::vector<float> hA((size_t)K * lda), hB((size_t)N * ldb), hC((size_t)N * ldc, -7.0f);
   unsigned long long st = seed * 6364136223846793005ull + 1;
   auto uni = [&]() {
@@ -428,5 +430,5 @@ extern "C" int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, unsigned
 }
 
 extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double* rel, int* timeout) {
-  return efmm_tc_gemm_selfcheck_tile(M, N, K, 128, seed, rel, timeout);
+  return efmm_tc_gemm_selfcheck_tile(M, N, K, 128, 0, seed, rel, timeout);
 }

@@ -217,8 +217,11 @@ double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, un
  * != 0 if a bounded wait in the kernel ran out.  Returns 0 or an ier. */
 int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
 /* The same check with output tiles bn = 64 or 128 columns wide (the 64-wide
- * tiles carry the factored P2M product, N = number of right-hand sides). */
-int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, unsigned seed, double *rel, int *timeout);
+ * tiles carry the factored P2M product, N = number of right-hand sides);
+ * aligned != 0: leading dimensions rounded up to multiples of 4 (16-byte
+ * rows, vector loads), else odd ones. */
+int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, int aligned, unsigned seed, double *rel,
+                                int *timeout);
 
 /* Repeated batched evaluations as one CUDA graph (no counterpart in the
  * reference): the same arguments as efmm_plan_evaluate_batch_iter /
@@ -246,6 +249,13 @@ long long efmm_plan_stored_bytes(const efmm_plan *plan);
  * orders.  *order (if not NULL) receives the mixed form's expansion order.
  * Applies to later calls on the plan's current geometry. */
 int efmm_plan_set_mixed_floor(efmm_plan *plan, double eps, int *order);
+
+/* Flops of one pass's translation launches (M2M, M2L, L2L into f3) for
+ * nrhs right-hand sides at the orders of the form `precision` selects
+ * (1: the mixed form's), counted as the kernels run them (factored: two
+ * rotations and the shift along z per pair and column).  Measurement
+ * support, no counterpart in the reference. */
+int efmm_plan_translation_flops(efmm_plan *plan, int nrhs, int precision, double *f3);
 
 /* Direct sum at the first nsub source points only (centroids 0..nsub-1,
  * self-aware), outputs u_src (nsub,3), e_src (nsub,3,3): the FP64 check of a

@@ -9,13 +9,13 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _check(gpu, M, N, K, seed, bn=128):
+def _check(gpu, M, N, K, seed, bn=128, aligned=0):
     f = gpu.load().efmm_tc_gemm_selfcheck_tile
     f.restype = ctypes.c_int
-    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
                   ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     rel, to = ctypes.c_double(), ctypes.c_int()
-    ier = f(M, N, K, bn, seed, ctypes.byref(rel), ctypes.byref(to))
+    ier = f(M, N, K, bn, aligned, seed, ctypes.byref(rel), ctypes.byref(to))
     return ier, rel.value, to.value
 
 
@@ -37,4 +37,13 @@ def test_tc_product_empty_k(gpu):
 def test_tc_product_64_wide_tiles(gpu, M, N, K):
     ier, rel, to = _check(gpu, M, N, K, 5, bn=64)
     print(f"tc product (64-wide tiles) {M}x{N}x{K}: rel {rel:.2e}")
+    assert ier == 0 and to == 0 and rel < 2e-6
+
+
+@pytest.mark.parametrize("bn", [64, 128])
+@pytest.mark.parametrize("M,N,K", [(128, 64, 32), (1640, 64, 1250), (300, 50, 77), (992, 130, 4000)])
+def test_tc_product_aligned_rows(gpu, M, N, K, bn):
+    # 16-byte rows: vector loads of B, zero fill at the edges
+    ier, rel, to = _check(gpu, M, N, K, 9, bn=bn, aligned=1)
+    print(f"tc product (aligned, {bn}-wide) {M}x{N}x{K}: rel {rel:.2e}")
     assert ier == 0 and to == 0 and rel < 2e-6
