@@ -114,7 +114,7 @@ struct Quad {
 // TC: the accumulation (and output) type, float or double (the K-tile sums
 // of the tensor cores added in FP64: the near-field replay)
 template <int BN, class TC>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, BN == 64 ? 2 : 1)
 k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
           TC* __restrict__ Cm, int* __restrict__ err) {
   constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
@@ -243,6 +243,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   for (int kt = 0; kt < nkt; kt++) {
     const int s = kt & 1;
     store(s);  // stage s is free: tile kt - 2 finished before tile kt - 1 was drained
+    if (kt + 1 < nkt) load(kt + 1);  // in flight while the tensor cores work on tile kt
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -264,7 +265,6 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
       }
       mma_commit(smem_u32(&bars[s]));
     }
-    if (kt + 1 < nkt) load(kt + 1);
     if (kt >= 1) {
       const int u = kt - 1;
       ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
