@@ -510,6 +510,7 @@ def run_hsbatch(args, rank, world, local_rank):
     ui, ei = torch.zeros_like(uf), torch.zeros_like(ef)
 
     def step(precision=1, mode=2, graph=False):
+        graph = graph and not args.no_graph
         F.evaluate_batch(1.0, 1.0, R, None, dsdl, uf, ef, precision=precision, mode=mode, graph=graph)
         I.evaluate_image(1.0, 1.0, R, None, dsdl, ui, ei, precision=precision, mode=mode, graph=graph)
 
@@ -709,7 +710,9 @@ def run_hsbatch(args, rank, world, local_rank):
                    "parallelism": f"replicas{world}",
                    "l2_policy": "expansions (FP32, several GB) and stored near field (~49 GB) > L2 (126 MB)",
                    "step": "free-space batch + image batch, near fields replayed (stored on the first call, "
-                           f"{store_s * 1e3:.0f} ms, untimed), each plan's pass replayed as one CUDA graph",
+                           f"{store_s * 1e3:.0f} ms, untimed), "
+                           + ("plain passes (--no-graph)" if args.no_graph else
+                              "each plan's pass replayed as one CUDA graph"),
                    "ms_per_step_without_graph": nograph_ms,
                    "forms": {"mixed_batched": value / world, "batched_fp64": b64_value,
                              "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
@@ -1053,6 +1056,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=16)
     ap.add_argument("--ref-sample", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-graph", action="store_true",
+                    help="half-space batch: time plain passes instead of CUDA-graph replays (profiling)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
