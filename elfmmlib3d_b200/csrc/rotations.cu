@@ -589,8 +589,14 @@ constexpr RotwOwners make_rotw_owners() {
   return r;
 }
 __constant__ RotwOwners c_rotw_owners = make_rotw_owners();
-// shared memory: X [dim][16] floats, then the source column offsets [16] (8-byte aligned)
+// shared memory: X [dim][16] floats, the source column offsets [16], then
+// per warp two operator buffers of ROTW_CH columns of <= 64 rows
+constexpr int ROTW_CH = 8;
 __host__ __device__ inline size_t rotw_cbase_off(int dim) { return sizeof(float) * (size_t)dim * ROTW_NCT; }
+__host__ __device__ inline size_t rotw_wbuf_off(int dim) { return rotw_cbase_off(dim) + 8 * ROTW_NCT; }
+__host__ __device__ inline size_t rotw_smem(int dim) {
+  return rotw_wbuf_off(dim) + sizeof(float) * (size_t)ROTW_NW * 2 * ROTW_CH * 64;
+}
 
 __global__ void __launch_bounds__(ROTW_THREADS, 2)
 k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
@@ -635,47 +641,78 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
           make_float4(a1[4 * q], a1[4 * q + 1], a1[4 * q + 2], a1[4 * q + 3]);
     }
   };
+  // the warp's operator columns, ROTW_CH at a time, copied asynchronously
+  // into its two shared buffers (one chunk ahead of the products); a block's
+  // columns are contiguous (column-major, ld = rows <= 64)
+  float* wbuf = reinterpret_cast<float*>(rw_smem + rotw_wbuf_off(dim)) + (size_t)warp * 2 * ROTW_CH * 64;
+  auto fetch = [&](const float* blk, int ld, int ncol, int chunk) {
+    const int c0 = chunk * ROTW_CH, nbytes = 4 * min(ROTW_CH, ncol - c0) * ld;
+    const float* g = blk + (size_t)c0 * ld;
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(wbuf + (chunk & 1) * ROTW_CH * 64));
+    for (int b = 16 * lane; b < nbytes; b += 16 * 32) {
+      const int nb = min(16, nbytes - b);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(d + b), "l"(reinterpret_cast<const char*>(g) + b),
+                   "r"(nb)
+                   : "memory");
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // one block product: rows 2 lane, 2 lane + 1 of the block (if < nrow),
+  // columns kk < ncol of the operator (ld = nrow); the operator column pairs
+  // of input row k are (2k, 2k + 1) for the shift (pair = true), else k
+  auto block = [&](const float* blk, int nrow, int ncol, bool pair, auto xrow, float* a0, float* a1) {
+    const bool act = 2 * lane < nrow;
+    const int nch = (ncol + ROTW_CH - 1) / ROTW_CH;
+    fetch(blk, nrow, ncol, 0);
+    for (int ch = 0; ch < nch; ch++) {
+      if (ch + 1 < nch)
+        fetch(blk, nrow, ncol, ch + 1);
+      else
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+      __syncwarp();
+      const float* wb = wbuf + (ch & 1) * ROTW_CH * 64 + 2 * lane;
+      const int cend = min(ROTW_CH, ncol - ch * ROTW_CH);
+      if (!pair) {
+        for (int u = 0; u < cend; u++) {
+          const float2 w = act ? *reinterpret_cast<const float2*>(wb + u * nrow) : make_float2(0.f, 0.f);
+          const float4* xr = reinterpret_cast<const float4*>(X + (size_t)xrow(ch * ROTW_CH + u) * NCT);
+#pragma unroll
+          for (int q = 0; q < NCT / 4; q++) {
+            const float4 x = xr[q];
+            a0[4 * q] += w.x * x.x; a0[4 * q + 1] += w.x * x.y; a0[4 * q + 2] += w.x * x.z; a0[4 * q + 3] += w.x * x.w;
+            a1[4 * q] += w.y * x.x; a1[4 * q + 1] += w.y * x.y; a1[4 * q + 2] += w.y * x.z; a1[4 * q + 3] += w.y * x.w;
+          }
+        }
+      } else {
+        for (int u = 0; u < cend; u += 2) {
+          const float2 wr = act ? *reinterpret_cast<const float2*>(wb + u * nrow) : make_float2(0.f, 0.f);
+          const float2 wi = act ? *reinterpret_cast<const float2*>(wb + (u + 1) * nrow) : make_float2(0.f, 0.f);
+          const int rk = xrow((ch * ROTW_CH + u) >> 1);
+          const float4* xre = reinterpret_cast<const float4*>(X + (size_t)rk * NCT);
+          const float4* xim = reinterpret_cast<const float4*>(X + (size_t)(rk + 1) * NCT);
+#pragma unroll
+          for (int q = 0; q < NCT / 4; q++) {
+            const float4 xr = xre[q], xi = xim[q];
+            a0[4 * q] += wr.x * xr.x + wi.x * xi.x; a0[4 * q + 1] += wr.x * xr.y + wi.x * xi.y;
+            a0[4 * q + 2] += wr.x * xr.z + wi.x * xi.z; a0[4 * q + 3] += wr.x * xr.w + wi.x * xi.w;
+            a1[4 * q] += wr.y * xr.x + wi.y * xi.x; a1[4 * q + 1] += wr.y * xr.y + wi.y * xi.y;
+            a1[4 * q + 2] += wr.y * xr.z + wi.y * xi.z; a1[4 * q + 3] += wr.y * xr.w + wi.y * xi.w;
+          }
+        }
+      }
+      __syncwarp();  // buffer (ch & 1) is refilled by the fetch of chunk ch + 2
+    }
+  };
   auto rotate = [&](long long base) {
     for (int n = 0; n <= p; n++) {
       if (owner[n] != warp) continue;
       const int bb = 2 * n + 2, r0 = n * (n + 1);
-      const bool act = 2 * lane < bb;
-      const float* o = pool + base + rot_block_off(n) + 2 * lane;  // column-major: (row, k) at k bb + row
       float a0[NCT], a1[NCT];
 #pragma unroll
       for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
-      constexpr int UNR = 2;
-      int k = 0;
-      for (; k + UNR <= bb; k += UNR) {
-        float2 w[UNR];
-#pragma unroll
-        for (int u = 0; u < UNR; u++)
-          w[u] = act ? *reinterpret_cast<const float2*>(o + (size_t)(k + u) * bb) : make_float2(0.f, 0.f);
-#pragma unroll
-        for (int u = 0; u < UNR; u++) {
-          const float4* xr = reinterpret_cast<const float4*>(X + (size_t)(r0 + k + u) * NCT);
-#pragma unroll
-          for (int q = 0; q < NCT / 4; q++) {
-            const float4 x = xr[q];
-            a0[4 * q] += w[u].x * x.x; a0[4 * q + 1] += w[u].x * x.y;
-            a0[4 * q + 2] += w[u].x * x.z; a0[4 * q + 3] += w[u].x * x.w;
-            a1[4 * q] += w[u].y * x.x; a1[4 * q + 1] += w[u].y * x.y;
-            a1[4 * q + 2] += w[u].y * x.z; a1[4 * q + 3] += w[u].y * x.w;
-          }
-        }
-      }
-      for (; k < bb; k++) {
-        const float2 w = act ? *reinterpret_cast<const float2*>(o + (size_t)k * bb) : make_float2(0.f, 0.f);
-        const float4* xr = reinterpret_cast<const float4*>(X + (size_t)(r0 + k) * NCT);
-#pragma unroll
-        for (int q = 0; q < NCT / 4; q++) {
-          const float4 x = xr[q];
-          a0[4 * q] += w.x * x.x; a0[4 * q + 1] += w.x * x.y; a0[4 * q + 2] += w.x * x.z; a0[4 * q + 3] += w.x * x.w;
-          a1[4 * q] += w.y * x.x; a1[4 * q + 1] += w.y * x.y; a1[4 * q + 2] += w.y * x.z; a1[4 * q + 3] += w.y * x.w;
-        }
-      }
-      __syncwarp();
-      if (act) put_rows(r0 + 2 * lane, r0 + 2 * lane + 1, a0, a1);
+      block(pool + base + rot_block_off(n), bb, bb, false, [&](int k) { return r0 + k; }, a0, a1);
+      if (2 * lane < bb) put_rows(r0 + 2 * lane, r0 + 2 * lane + 1, a0, a1);
       __syncwarp();
     }
   };
@@ -685,29 +722,12 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
   for (int m = 0; m <= p; m++) {
     if (owner[p - m] != warp) continue;
     const int bz = 2 * (p - m + 1);
-    const bool act = 2 * lane < bz;
-    const float* o = pool + op.z + z_block_off(p, m) + 2 * lane;  // column-major: (row, col) at col bz + row
     float a0[NCT], a1[NCT];
 #pragma unroll
     for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
-    for (int k = m; k <= p; k++) {
-      const int c2 = 2 * (k - m);
-      const float2 wr = act ? *reinterpret_cast<const float2*>(o + (size_t)c2 * bz) : make_float2(0.f, 0.f);
-      const float2 wi = act ? *reinterpret_cast<const float2*>(o + (size_t)(c2 + 1) * bz) : make_float2(0.f, 0.f);
-      const int rk = 2 * (k * (k + 1) / 2 + m);
-      const float4* xre = reinterpret_cast<const float4*>(X + (size_t)rk * NCT);
-      const float4* xim = reinterpret_cast<const float4*>(X + (size_t)(rk + 1) * NCT);
-#pragma unroll
-      for (int q = 0; q < NCT / 4; q++) {
-        const float4 xr = xre[q], xi = xim[q];
-        a0[4 * q] += wr.x * xr.x + wi.x * xi.x; a0[4 * q + 1] += wr.x * xr.y + wi.x * xi.y;
-        a0[4 * q + 2] += wr.x * xr.z + wi.x * xi.z; a0[4 * q + 3] += wr.x * xr.w + wi.x * xi.w;
-        a1[4 * q] += wr.y * xr.x + wi.y * xi.x; a1[4 * q + 1] += wr.y * xr.y + wi.y * xi.y;
-        a1[4 * q + 2] += wr.y * xr.z + wi.y * xi.z; a1[4 * q + 3] += wr.y * xr.w + wi.y * xi.w;
-      }
-    }
-    __syncwarp();
-    if (act) {
+    block(pool + op.z + z_block_off(p, m), bz, bz, true,
+          [&](int kq) { const int k = m + kq; return 2 * (k * (k + 1) / 2 + m); }, a0, a1);
+    if (2 * lane < bz) {
       const int n = m + lane, cc = n * (n + 1) / 2 + m;
       put_rows(2 * cc, 2 * cc + 1, a0, a1);
     }
@@ -751,7 +771,7 @@ void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, co
   }();
   if constexpr (sizeof(T) == 4) {
     if (warp_blocks && rot_warp_blocks_ok(maxdim)) {
-      const size_t smem = rotw_cbase_off(maxdim) + sizeof(long long) * ROTW_NCT;
+      const size_t smem = rotw_smem(maxdim);
       EFMM_CUDA_TRY(cudaFuncSetAttribute(k_translate_rot_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
       k_translate_rot_w<<<ntask, ROTW_THREADS, smem, st>>>(tasks, pairs, ops, reinterpret_cast<const float*>(pool),
                                                              D, C, reinterpret_cast<const float*>(src),

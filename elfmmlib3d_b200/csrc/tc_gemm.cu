@@ -114,7 +114,7 @@ struct Quad {
 // TC: the accumulation (and output) type, float or double (the K-tile sums
 // of the tensor cores added in FP64: the near-field replay)
 template <int BN, class TC>
-__global__ void __launch_bounds__(TC_THREADS, BN == 64 ? 2 : 1)
+__global__ void __launch_bounds__(TC_THREADS, 1)
 k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
           TC* __restrict__ Cm, int* __restrict__ err) {
   constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
