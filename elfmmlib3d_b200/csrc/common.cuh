@@ -63,6 +63,15 @@ struct __align__(16) TriRec {
 static_assert(sizeof(TriRec) == 192, "TriRec layout");
 
 // Number of this library's kernels launched so far (all devices, all plans).
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`, never
+// lowering it: plans driven from several host threads launch the same kernels
+// with different sizes, and a lower limit set by one thread between another
+// thread's setting and its launch would make that launch fail.
+cudaError_t smem_raise_fn(const void* kern, int bytes);
+template <class F>
+inline cudaError_t smem_raise(F* kern, int bytes) {
+  return smem_raise_fn(reinterpret_cast<const void*>(kern), bytes);
+}
 long long launches_total();
 void count_launch(int k = 1);
 

@@ -2208,7 +2208,7 @@ bool launch_l2t_img(cudaStream_t st, int nleaf, const L2TArgs& a, int R, long lo
   const size_t smem = sizeof(double) * 7 * 2 * (size_t)ncoef(a.p) + sizeof(cplx) * L2T_WARPS * ncoef(a.p);
   if (smem > 227 * 1024) return false;  // high orders: the two-stage form
   if (nleaf <= 0 || R <= 0) return true;
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_img, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EFMM_CUDA_TRY(smem_raise(k_l2t_img, (int)smem));
   k_l2t_img<<<dim3(nleaf, R), L2T_WARPS * 32, smem, st>>>(a, R, ubase);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
@@ -2222,7 +2222,7 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_features<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  EFMM_CUDA_TRY(smem_raise(k_l2t_features<T>, (int)(smem)));
   k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
   gemm_product<T>(st, ntask, tasks, Gbuf, local, Sbuf);
   if (image)
@@ -2261,21 +2261,19 @@ bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwlea
   if constexpr (sizeof(T) == 4) {
     float* Hf = reinterpret_cast<float*>(H);
     if (nk == 7) {
-      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_unit_f<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EFMM_CUDA_TRY(smem_raise(k_p2m_unit_f<7>, (int)smem));
       k_p2m_unit_f<7><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
     } else {
-      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_unit_f<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EFMM_CUDA_TRY(smem_raise(k_p2m_unit_f<4>, (int)smem));
       k_p2m_unit_f<4><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
     }
   } else {
     constexpr int NTD = unit_threads<T>();
     if (nk == 7) {
-      EFMM_CUDA_TRY(
-          cudaFuncSetAttribute(k_p2m_unit<T, 7, NTD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EFMM_CUDA_TRY(smem_raise(k_p2m_unit<T, 7, NTD>, (int)smem));
       k_p2m_unit<T, 7, NTD><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, H);
     } else {
-      EFMM_CUDA_TRY(
-          cudaFuncSetAttribute(k_p2m_unit<T, 4, NTD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EFMM_CUDA_TRY(smem_raise(k_p2m_unit<T, 4, NTD>, (int)smem));
       k_p2m_unit<T, 4, NTD><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, H);
     }
   }
@@ -2308,7 +2306,7 @@ void gemm_product(cudaStream_t st, int ntask, const GemmTask* tasks, const T* F,
     return;
   }
   const int gsm = (int)(sizeof(T) * 4 * 16 * 128);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_gemm_tn<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, gsm));
+  EFMM_CUDA_TRY(smem_raise(k_gemm_tn<T>, (int)(gsm)));
   k_gemm_tn<T><<<ntask, 256, gsm, st>>>(tasks, F, W, C);
   count_launch();
 }
@@ -2324,7 +2322,7 @@ void launch_p2m_img_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwlea
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T, 9>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  EFMM_CUDA_TRY(smem_raise(k_p2m_features<T, 9>, (int)(smem)));
   k_p2m_features<T, 9><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights_img<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
@@ -2335,7 +2333,7 @@ template <class T>
 void launch_p2m_img(cudaStream_t st, int nleaf, const P2MArgs& a, int R, long long ubase, T* mpole) {
   if (nleaf <= 0 || R <= 0) return;
   const size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 63 * P2M_NODES);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_img<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EFMM_CUDA_TRY(smem_raise(k_p2m_img<T>, (int)smem));
   k_p2m_img<T><<<dim3(nleaf, R), P2M_THREADS, smem, st>>>(a, R, ubase, mpole);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
@@ -2354,7 +2352,7 @@ void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats,
   if (nop <= 0) return;
   size_t smem = sizeof(cplx) * (size_t)ncoef(2 * maxp);
   if (smem > 48 * 1024)
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_build_ops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EFMM_CUDA_TRY(smem_raise(k_build_ops, (int)smem));
   k_build_ops<<<nop, 256, smem, st>>>(nop, ops, mats); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -2363,7 +2361,7 @@ void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs) {
   if (nleaf <= 0) return;
   size_t smem = sizeof(double) * (2 * (size_t)P2M_NODES * ncoef(a.p) + 16 * P2M_NODES);
   if (smem > 48 * 1024)
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EFMM_CUDA_TRY(smem_raise(k_p2m, (int)smem));
   k_p2m<<<dim3(nleaf, nrhs), P2M_THREADS, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -2376,7 +2374,7 @@ void launch_p2m_twostage(cudaStream_t st, const P2MArgs& a, int R, int nwleaf, c
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_features<T, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  EFMM_CUDA_TRY(smem_raise(k_p2m_features<T, 4>, (int)(smem)));
   k_p2m_features<T, 4><<<dim3(nwleaf, (max_nodes + 7) / 8), 256, smem, st>>>(a, wleaves, foff, noff, nrec, F);
   count_launch();
   k_p2m_weights<T><<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, wleaves, woff, noff, nrec, W); count_launch();
@@ -2397,7 +2395,7 @@ bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const i
   size_t smem = sizeof(cplx) * LG_PTS * nc + sizeof(double) * (LG_K * LG_PTS * 9 + LG_K * LG_CP);
   if (smem > 227 * 1024) return false;
   if (nchunk <= 0 || R <= 0) return true;
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t_gemm<TB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EFMM_CUDA_TRY(smem_raise(k_l2t_gemm<TB>, (int)smem));
   dim3 grid(nchunk, (4 * R + LG_C - 1) / LG_C);
   k_l2t_gemm<TB><<<grid, 256, smem, st>>>(a, chunk_leaf, chunk_e0, R, local, wnorm); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
@@ -2416,7 +2414,7 @@ bool launch_p2m_gemm(cudaStream_t st, int nleaf, const P2MArgs& a, int R, T* mpo
   smem = (smem + 15) / 16 * 16;
   if (smem > 227 * 1024) return false;  // high orders: the caller uses k_p2m
   if (nleaf <= 0 || R <= 0) return true;
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(k_p2m_gemm<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EFMM_CUDA_TRY(smem_raise(k_p2m_gemm<T>, (int)smem));
   dim3 grid(nleaf, (D + PG_R - 1) / PG_R, (C + PG_C - 1) / PG_C);
   k_p2m_gemm<T><<<grid, 256, smem, st>>>(a, R, mpole); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
@@ -2435,7 +2433,7 @@ void launch_translate(cudaStream_t st, int ntask, const TransTask* tasks, const 
   int dev = 0;
   EFMM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev >= 64 || !attr_set[dev]) {
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_translate<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EFMM_CUDA_TRY(smem_raise(k_translate<T>, (int)(smem)));
     if (dev < 64) attr_set[dev] = true;
   }
   k_translate<T><<<ntask, 256, smem, st>>>(tasks, pairs, mats, mat_off, mat_dim, D, C, src, dst); count_launch();
@@ -2455,7 +2453,7 @@ void launch_l2t(cudaStream_t st, int nleaf, const L2TArgs& a, int nrhs) {
   while (nw > 1 && need(nw) > 220 * 1024) nw /= 2;
   size_t smem = need(nw);
   if (smem > 48 * 1024)
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(k_l2t, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EFMM_CUDA_TRY(smem_raise(k_l2t, (int)smem));
   k_l2t<<<dim3(nleaf, nrhs), nw * 32, smem, st>>>(a); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }

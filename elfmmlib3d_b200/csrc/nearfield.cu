@@ -700,7 +700,7 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
   const int RB = (R + 15) / 16;
   const int smem = (int)(sizeof(double) * (NB_PTS * NB_TRI * K + NB_TRI * 6 * 16 * RB));
   auto go = [&](auto kern) {
-    EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    EFMM_CUDA_TRY(smem_raise(kern, (int)(smem)));
     kern<<<nchunk, NB_THREADS, smem, st>>>(a, chunk_leaf, chunk_e0, R, K, dostrain, ssl, sdl, ntri_all, nsrc,
                                            ntgt, sbase, sntri, store);
     count_launch();
@@ -711,7 +711,7 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
     const double* g1 = sdl;
     const int smem2 = (int)(sizeof(double) * (NB_PTS * NB_TRI * K + NB_TRI * 3 * nlay * 16 * RB));
     auto go2 = [&](auto kern) {
-      EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem2));
+      EFMM_CUDA_TRY(smem_raise(kern, (int)(smem2)));
       kern<<<nchunk, NB_THREADS, smem2, st>>>(a, chunk_leaf, chunk_e0, R, g0, g1, nsrc, ntgt, sbase, sntri, store);
       count_launch();
     };

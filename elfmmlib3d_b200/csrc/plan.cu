@@ -17,6 +17,20 @@ namespace efmm {
 
 static std::atomic<long long> g_launches{0};
 long long launches_total() { return g_launches.load(); }
+
+cudaError_t smem_raise_fn(const void* kern, int bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, int> limit;  // (device, kernel) -> limit set
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  int& cur = limit[std::make_pair(dev, kern)];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
 void count_launch(int k) { g_launches += k; }
 
 double iprec_eps(int iprec) {

@@ -772,7 +772,7 @@ void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, co
   if constexpr (sizeof(T) == 4) {
     if (warp_blocks && rot_warp_blocks_ok(maxdim)) {
       const size_t smem = rotw_smem(maxdim);
-      EFMM_CUDA_TRY(cudaFuncSetAttribute(k_translate_rot_w, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      EFMM_CUDA_TRY(smem_raise(k_translate_rot_w, (int)smem));
       k_translate_rot_w<<<ntask, ROTW_THREADS, smem, st>>>(tasks, pairs, ops, reinterpret_cast<const float*>(pool),
                                                              D, C, reinterpret_cast<const float*>(src),
                                                              reinterpret_cast<float*>(dst));
@@ -785,7 +785,7 @@ void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, co
   const size_t smem = sizeof(T) * 2 * (size_t)maxdim * NCT;
   if (smem > 227 * 1024) throw CudaError{(int)cudaErrorInvalidValue};
   auto kern = k_translate_rot<T, NCT>;
-  EFMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  EFMM_CUDA_TRY(smem_raise(kern, (int)smem));
   kern<<<ntask, ROT_THREADS, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst); count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }

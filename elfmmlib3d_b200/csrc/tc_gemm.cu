@@ -343,12 +343,10 @@ static void launch_gemm_tc_t(cudaStream_t st, int ntask, const GemmTask* tasks, 
                              TC* C, int* err, int bn) {
   if (ntask <= 0) return;
   if (bn == 64) {
-    EFMM_CUDA_TRY(
-        cudaFuncSetAttribute(k_gemm_tc<64, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<64>()));
+    EFMM_CUDA_TRY(smem_raise(k_gemm_tc<64, TC>, (int)(tc_smem<64>())));
     k_gemm_tc<64, TC><<<ntask, TC_THREADS, tc_smem<64>(), st>>>(tasks, A, B, C, err);
   } else {
-    EFMM_CUDA_TRY(
-        cudaFuncSetAttribute(k_gemm_tc<128, TC>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem<128>()));
+    EFMM_CUDA_TRY(smem_raise(k_gemm_tc<128, TC>, (int)(tc_smem<128>())));
     k_gemm_tc<128, TC><<<ntask, TC_THREADS, tc_smem<128>(), st>>>(tasks, A, B, C, err);
   }
   count_launch();
