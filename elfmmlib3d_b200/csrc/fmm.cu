@@ -603,10 +603,11 @@ k_p2m_weights_img(const P2MArgs a, int R, const int* __restrict__ wleaves, const
 // the four free-space (or anti-image) columns; NK = 7 adds the image columns.
 constexpr int UNIT_TB = 16;  // triangles per CTA
 
-// Largest CTA of k_p2m_unit (register budget of the moments: at most 128
-// per thread in FP32, 240 in FP64; CTAs of whole warp quadruples, so that
-// every sub-partition's register file holds its share); the launch uses the
-// fewest such threads that cover the coefficients in the same number of rounds
+// Largest CTA of k_p2m_unit (the FP64 form; register budget of the moments
+// about 240 per thread; CTAs of whole warp quadruples, so that every
+// sub-partition's register file holds its share); the launch uses the fewest
+// such threads that cover the coefficients in the same number of rounds.
+// The FP32 form runs k_p2m_unit_f.
 template <class T>
 __host__ __device__ constexpr int unit_threads() { return sizeof(T) == 4 ? 512 : 256; }
 
@@ -800,9 +801,8 @@ k_p2m_unit(const P2MArgs a, const int* __restrict__ wleaves, const long long* __
         const T w = gq[0], wy[3] = {gq[1], gq[2], gq[3]};
         // Y, d_x, d_y, d_z (and xx, yy, xy, xz, yz) by the ladder relations, unscaled
         T fr[NF], fi[NF];
-        // (the ladder sums in T: the FP32 form rounds the harmonics first,
-        // scaled by the coefficient's basis normalisation so that they stay
-        // in range)
+        // (the ladder sums in T, the harmonics scaled by the coefficient's
+        // basis normalisation when one is given)
         auto ld = [&](int o, T& re, T& im) {
           const cplx v = Y[o];
           re = (T)(srd * v.re);
