@@ -1590,7 +1590,9 @@ int Plan::run_graph(const std::vector<double>& key, const std::function<int()>& 
 int Plan::evaluate_batch_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                                double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
                                int mode) {
-  if (mode != 0 && mode != 2) return IER_BADARG;
+  // one pass per call (R <= 64): the passes of a chunked call would re-cut
+  // their cached work lists inside the capture
+  if ((mode != 0 && mode != 2) || R < 1 || R > 64) return IER_BADARG;
   const std::vector<double> key = {1.0, rlam, rmu, (double)R, (double)(uintptr_t)d_ssl, (double)(uintptr_t)d_sdl,
                                    (double)(uintptr_t)d_u_src, (double)(uintptr_t)d_e_src,
                                    (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision,
@@ -1602,6 +1604,7 @@ int Plan::evaluate_batch_graph(double rlam, double rmu, int R, const double* d_s
 
 int Plan::evaluate_image_graph(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
                                double* d_u_tgt, double* d_e_tgt, int precision) {
+  if (R < 1 || R > 64) return IER_BADARG;  // one pass per call, as above
   const std::vector<double> key = {2.0, rlam, rmu, (double)R, (double)(uintptr_t)d_ssl, (double)(uintptr_t)d_sdl,
                                    (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision};
   return run_graph(key, [&]() {

@@ -231,6 +231,7 @@ int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, int aligned, unsign
  * graph only, so new densities must be written into the same buffers.
  * Batch: mode 0 (analytic near field) or 2 (a store made by an earlier
  * mode-1 call); image: the stored near field of an earlier mode-1 call.
+ * nrhs <= 64 (one pass per call; else IER 16).
  * The first call should not run while another capture on the plan's stream
  * is in progress.  A new geometry drops the graph. */
 int efmm_plan_evaluate_batch_graph(efmm_plan *plan, double rlam, double rmu, int nrhs, const double *ssl,
