@@ -47,3 +47,22 @@ def test_graph_batch_and_image_replay(gpu):
     assert rel(u.cpu().numpy(), u0.cpu().numpy()) < 1e-12 and rel(e.cpu().numpy(), e0.cpu().numpy()) < 1e-12
     for P in (F, I, F2):
         P.close()
+
+
+def test_graph_rejects_chunked_calls(gpu):
+    # more than 64 right-hand sides run as several passes: not replayed
+    # (IER 16), the plain call serves them
+    import torch
+    tri, nrm, cen, _ = G.planar_fault(10, 5)
+    n, R = len(cen), 70
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    F = gpu.Plan(0)
+    F.set_geometry(d(tri), d(nrm), d(cen), None, iprec=2)
+    sdl = d(np.random.default_rng(2).normal(size=(R, n, 3)))
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device="cuda")
+    with pytest.raises(gpu.ElfmmError) as ex:
+        F.evaluate_batch(1.0, 1.0, R, None, sdl, u, None, precision=1, graph=True)
+    assert ex.value.ier == 16
+    F.evaluate_batch(1.0, 1.0, R, None, sdl, u, None, precision=1)
+    assert float(u.abs().sum()) > 0
+    F.close()
