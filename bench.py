@@ -236,6 +236,56 @@ def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     return nsample * n / dt, dt, cores, nsample
 
 
+def cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample):
+    """Oracle half-space self-evaluation at the first nsample centroids
+    against all triangles: the direct arrival (free-space direct sum) plus
+    the image part (the oracle's C image quadrature, refined by distance to
+    the reflected target), all host cores.  Returns (evals/s, seconds,
+    cores, points)."""
+    from oracle import oracle as O
+    O.lib()
+    n = len(cen)
+    nsample = min(nsample, n)
+    t0 = time.perf_counter()
+    O.direct(1.0, 1.0, tri, cen, ssl, sdl, None, rows=(0, nsample), trows=(0, 0))
+    O.image_direct(1.0, 1.0, tri, nrm, ssl, sdl, cen[:nsample], level=-1)
+    dt = time.perf_counter() - t0
+    return nsample * n / dt, dt, os.cpu_count(), nsample
+
+
+def uneven_sample_problems(probs):
+    """The problems of an uneven batch that the CPU samples cover: about 16,
+    evenly spaced in the batch (sizes drawn independently of position)."""
+    return probs[::max(1, len(probs) // 16)]
+
+
+def cpu_oracle_uneven_sample(probs, nsample):
+    """cpu_oracle_hs_sample on the first nsample centroids of each problem of
+    uneven_sample_problems.  Returns (evals/s, seconds, cores, points)."""
+    ev, dt, npts = 0.0, 0.0, 0
+    for tri, nrm, cen, ssl, sdl in uneven_sample_problems(probs):
+        e, d, cores, k = cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample)
+        ev += e * d
+        dt += d
+        npts += k
+    return ev / dt, dt, os.cpu_count(), npts
+
+
+def make_uneven_problems(w, rank=0):
+    """The uneven batch: w["nprob"] half-space faults, strike U[0, 360),
+    dip U[15, 90], top depth U[0.5, 5], triangle count log-uniform in
+    [nmin, nmax], one slip vector N(0,1) per triangle (double layer)."""
+    from elfmmlib3d_b200.batch import fault_problem
+    rng = np.random.default_rng(7 + rank)
+    probs = []
+    for i in range(w["nprob"]):
+        ntri = int(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"]))))
+        tri, nrm, cen, slip = fault_problem(ntri, rng.uniform(0.0, 360.0), rng.uniform(15.0, 90.0),
+                                            rng.uniform(0.5, 5.0), seed=100000 * rank + i)
+        probs.append((tri, nrm, cen, None, slip))
+    return probs
+
+
 # FP64 operations per near-field (point, triangle) pair of the analytic
 # kernel: ncu thread-instruction counts of k_near_leaf on the sphere-5120 case,
 # (dadd + dmul + 2 dfma) / pairs = (0.984e9 + 1.749e9 + 2 * 3.029e9) / 3.194e6
@@ -696,10 +746,11 @@ def run_hsbatch(args, rank, world, local_rank):
             "flops_by_stage": {"free": trf, "image": tri_}}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
+        ev, dt, cores, npts = cpu_oracle_hs_sample(tri, nrm, cen, None, sdl[0], args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
-               "sample": f"oracle free-space direct sum (the direct arrival only; the image part is not in "
-                         f"the sample), {npts} centroids x {n} triangles x 1 right-hand side ({dt:.1f} s)"}
+               "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
+                         f"distance refinement), {npts} centroids x {n} triangles x 1 right-hand side "
+                         f"({dt:.1f} s)"}
     plain_value = evals / (plain_ms * 1e-3)
     b64_value = evals / (b64_ms * 1e-3)
     fi = F.info()
@@ -989,10 +1040,10 @@ def run_hsiter(args, rank, world, local_rank):
             "algorithmic": f"stored near field read once per call: {stored[0] / 1e9:.2f} GB"}
     cpu = None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, slips[0], args.cpu_sample)
+        ev, dt, cores, npts = cpu_oracle_hs_sample(tri, nrm, cen, None, slips[0], args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
-               "sample": f"oracle free-space direct sum (the direct arrival only), {npts} centroids x {n} "
-                         f"triangles ({dt:.1f} s)"}
+               "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
+                         f"distance refinement), {npts} centroids x {n} triangles ({dt:.1f} s)"}
     return {
         "metric": "triangle-evals/s over the ITER call sequence (store once, reuse)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": ncall, "warmup": max(args.warmup, 2),
@@ -1017,35 +1068,64 @@ def run_hsiter(args, rank, world, local_rank):
 
 
 def run_reference(args, rank):
+    """The reference arm: the oracle's CPU restatement of the reference's
+    path on all host cores, each step a bounded sample of the workload
+    (ref_sample evaluation points against all triangles).  Half-space
+    workloads time the direct arrival plus the image part."""
     if rank != 0:
         return None
-    tri, nrm, cen, tgt, ssl, sdl, iprec = make_inputs(args.workload)
-    n = len(cen)
-    batch = WORKLOADS[args.workload]["kind"] in ("batch", "hsbatch")
-    hs = WORKLOADS[args.workload]["kind"] == "hsbatch"
+    w = WORKLOADS[args.workload]
+    kind = w["kind"]
+    batch = kind in ("batch", "hsbatch")
+    hs = kind in ("hsbatch", "hsiter", "uneven")
+    if kind == "uneven":
+        probs = make_uneven_problems(w)
+        n = int(sum(len(p[2]) for p in probs))
+        cfg = {"problems": len(probs), "triangles_total": n, "iprec": w["iprec"]}
+        sample = lambda: cpu_oracle_uneven_sample(probs, args.ref_sample)
+        desc = (f"oracle half-space self-evaluation (free-space direct sum + image quadrature with distance "
+                f"refinement) at {args.ref_sample} centroids of each of {len(uneven_sample_problems(probs))} "
+                f"evenly spaced problems, against all of their problem's triangles, per step")
+        metric = "triangle-evals/s (batched uneven half-space geometries, mixed precision)"
+    else:
+        tri, nrm, cen, tgt, ssl, sdl, iprec = make_inputs(args.workload)
+        n = len(cen)
+        cfg = {"triangles": n, "targets": len(tgt), "iprec": iprec}
+        if batch:
+            cfg.update({"rhs": w["nrhs"], "green": "Mindlin half space" if hs else "free space"})
+        if hs:
+            sample = lambda: cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, args.ref_sample)
+            desc = (f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
+                    f"distance refinement), {args.ref_sample} centroids x {n} triangles per step")
+        else:
+            sample = lambda: cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
+            desc = (f"oracle direct sum (el3dtriadirecttarg restated), {args.ref_sample} evaluation points x "
+                    f"{n} triangles per step")
+        if batch:
+            metric = "triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)"
+        elif kind in ("iter", "hsiter"):
+            metric = "triangle-evals/s over the ITER call sequence (store once, reuse)"
+        else:
+            metric = "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)"
     for _ in range(args.warmup):
-        cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
+        sample()
+    evs, secs = 0.0, 0.0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.ref_sample)
+        ev, dt, cores, npts = sample()
+        evs += ev * dt
+        secs += dt
     tot = time.perf_counter() - t0
-    value = args.steps * args.ref_sample * n / tot
-    metric = ("triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)" if batch
-              else "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)")
+    value = evs / secs
     return {
         "impl": "reference",
         "metric": metric,
         "value": value, "unit": "triangle-evals/s", "n_gpus": 0, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "triangles": n, "targets": len(tgt), "iprec": iprec,
-                   **({"rhs": WORKLOADS[args.workload]["nrhs"],
-                       "green": "Mindlin half space" if hs else "free space"} if batch else {})},
+        "config": {"workload": args.workload, **cfg},
         "cpu_baseline": {"value": value, "unit": "triangle-evals/s", "cores": os.cpu_count(), "kind": "port",
-                         "sample": f"oracle direct sum (el3dtriadirecttarg restated), {args.ref_sample} "
-                                   f"evaluation points x {n} triangles per step"
-                                   + (" (the direct arrival only; the image part is not in the sample)" if hs
-                                      else "")},
+                         "sample": desc},
         "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -1061,17 +1141,11 @@ def run_uneven(args, rank, world, local_rank):
     the host.  Errors against the FP64 direct sums on 200 centroids of every
     8th problem (untimed)."""
     import torch
-    from elfmmlib3d_b200.batch import halfspace_many, fault_problem
+    from elfmmlib3d_b200.batch import halfspace_many
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     w = WORKLOADS[args.workload]
-    rng = np.random.default_rng(7 + rank)
-    probs = []
-    for i in range(w["nprob"]):
-        ntri = int(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"]))))
-        tri, nrm, cen, slip = fault_problem(ntri, rng.uniform(0.0, 360.0), rng.uniform(15.0, 90.0),
-                                            rng.uniform(0.5, 5.0), seed=100000 * rank + i)
-        probs.append((tri, nrm, cen, None, slip))
+    probs = make_uneven_problems(w, rank)
     sizes = np.array([len(p[2]) for p in probs])
     evals = float(np.sum(sizes.astype(np.float64) ** 2))
     workers = 4
@@ -1094,6 +1168,13 @@ def run_uneven(args, rank, world, local_rank):
     errs = np.array(cinfo["errors"])
     if rank != 0:
         return None
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        ev, dt, cores, npts = cpu_oracle_uneven_sample(probs, args.cpu_sample)
+        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
+               "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
+                         f"distance refinement) at {npts} centroids of {len(uneven_sample_problems(probs))} "
+                         f"evenly spaced problems, against all of their problem's triangles ({dt:.1f} s)"}
     return {
         "metric": "triangle-evals/s (batched uneven half-space geometries, mixed precision)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -1117,7 +1198,7 @@ def run_uneven(args, rank, world, local_rank):
                           "problem"},
         "gpu_launches": launches // max(1, args.steps),
         "roofline": None,
-        "cpu_baseline": None,
+        "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }
 
@@ -1129,8 +1210,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="hs-fault-100k-r64", choices=list(WORKLOADS))
-    ap.add_argument("--cpu-sample", type=int, default=16)
-    ap.add_argument("--ref-sample", type=int, default=4)
+    # CPU samples: one evaluation point per host thread by default, so that
+    # every core has work (the oracle shares the points among its threads)
+    ncpu = min(256, max(8, os.cpu_count() or 8))
+    ap.add_argument("--cpu-sample", type=int, default=ncpu)
+    ap.add_argument("--ref-sample", type=int, default=ncpu)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-graph", action="store_true",
                     help="half-space batch: time plain passes instead of CUDA-graph replays (profiling)")

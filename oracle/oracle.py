@@ -116,6 +116,31 @@ def direct(rlam, rmu, triangles, centroids, sigma_sl=None, sigma_dl=None, target
     return pt, st, ptt[:m].copy(), stt
 
 
+def image_direct(rlam, rmu, triangles, normals, sigma_sl, sigma_dl, targets, level=-1):
+    """Image part of the half-space potentials (image.c; the image of
+    src/el3greenh.f:643-787 integrated over every triangle), at targets in
+    z < 0: returns (u (m,3), strain (m,3,3)).  level >= 0: 4**level uniform
+    sub-triangles per triangle (as mindlin.image_direct); level < 0:
+    refinement by distance to the reflected target.  None disables a layer."""
+    tri = c64(triangles).reshape(-1, 3, 3)
+    n = tri.shape[0]
+    nrm = c64(normals).reshape(n, 3)
+    tg = c64(targets).reshape(-1, 3)
+    m = tg.shape[0]
+    ssl = c64(sigma_sl).reshape(n, 3) if sigma_sl is not None else None
+    sdl = c64(sigma_dl).reshape(n, 3) if sigma_dl is not None else None
+    u = np.zeros((m, 3))
+    e = np.zeros((m, 3, 3))
+    f = lib().oracle_image_direct
+    f.restype = ctypes.c_int
+    ier = f(ctypes.c_double(rlam), ctypes.c_double(rmu), ctypes.c_int(n), _d(tri), _d(nrm),
+            _d(ssl) if ssl is not None else None, _d(sdl) if sdl is not None else None, ctypes.c_int(m),
+            _d(tg), ctypes.c_int(int(level)), _d(u), _d(e))
+    if ier:
+        raise ValueError(f"oracle_image_direct ier={ier}")
+    return u, e
+
+
 class Tree:
     """Bit-exact restatement of d3tstrcr (d3tstrcr.f:31).  All ids are 1-based."""
 
