@@ -111,3 +111,19 @@ def test_image_iter_store_and_replay(gpu):
     ier, *_ = gpu.elhfmm3dtriatargiter(2, 1.0, 1.0, tri, nrm, cen, None, s2, cen[:10], icomp_type=3, wsave=w)
     assert ier == 512
     assert gpu.iter_release(w) == 0
+
+
+def test_direct_image_matches_c_oracle_same_refinement(gpu, oracle):
+    # the oracle's C image sum with the same quadrature (12-node rule on
+    # sub-triangles refined until the reflected target is 8 diameters away)
+    # leaves only rounding between the two: 1e-9 here, where the uniform
+    # 16-sub-triangle numpy sum above differs from both by 2e-8 (strain)
+    tri, nrm, cen = _fault(3, 2)
+    rng = np.random.default_rng(12)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    tg = np.vstack([cen, [[0.3, 0.4, 0.0], [2.5, -0.5, -0.05]]])
+    for a, b in ((ssl, sdl), (ssl, None), (None, sdl)):
+        ier, u, e = gpu.hs_image_direct(1.3, 0.7, tri, nrm, a, b, tg)
+        assert ier == 0
+        uo, eo = oracle.image_direct(1.3, 0.7, tri, nrm, a, b, tg, level=-1)
+        assert rel(u, uo) < 1e-9 and rel(e, eo) < 1e-9
