@@ -50,7 +50,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
-           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_"]
+           "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_",
+           "elhfmm3dtria_total_"]
 
 
 class ElfmmError(RuntimeError):
@@ -299,6 +300,34 @@ def hs_image_direct(rlam, rmu, triangle, trinorm, sigma_sl=None, sigma_dl=None, 
             sdl.ctypes.data_as(_dp) if sdl is not None else None, ctypes.c_int(m), tg.ctypes.data_as(_dp),
             u.ctypes.data_as(_dp), e.ctypes.data_as(_dp))
     return ier, u[:m], e[:m]
+
+
+def elhfmm3dtria_total(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None,
+                       target=None, ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1):
+    """Half-space (z <= 0) total field, direct arrival + image part, at the
+    n centroids (on-surface) and at optional targets, in one call: the sum
+    the reference's drivers form from elfmm3dtriatarg and
+    elhfmm3dtriatargiter (examples/elhfmm3dtria_self_iter_dr.f:331-385).
+    Returns (ier, ptfrc (n,3), strain (n,3,3), ptfrctarg (m,3),
+    straintarg (m,3,3))."""
+    L = load()
+    _need_gpu()
+    tri, nrm, src, ssl, sdl, n = _ref_args(triangle, trinorm, source, sigma_sl, sigma_dl)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    pt = np.zeros((n, 3))
+    st = np.zeros((n, 3, 3))
+    ptt = np.zeros((max(m, 1), 3))
+    stt = np.zeros((max(m, 1), 3, 3))
+    ier = ctypes.c_int(0)
+    L.elhfmm3dtria_total_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu),
+                          tri.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp), _byref_i(n),
+                          src.ctypes.data_as(_dp), _byref_i(sigma_sl is not None), ssl.ctypes.data_as(_dp),
+                          _byref_i(sigma_dl is not None), sdl.ctypes.data_as(_dp), _byref_i(ifptfrc),
+                          pt.ctypes.data_as(_dp), _byref_i(ifstrain), st.ctypes.data_as(_dp), _byref_i(m),
+                          tg.ctypes.data_as(_dp), _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp),
+                          _byref_i(ifstraintarg), stt.ctypes.data_as(_dp))
+    return ier.value, pt, st, ptt[:m], stt[:m]
 
 
 def halfspace_self(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None):

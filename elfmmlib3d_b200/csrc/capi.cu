@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points (include/elfmm3d_b200.h).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -798,6 +799,67 @@ extern "C" void elhfmm3dtriatargiter_(int* ier, const int* iprec, const double* 
   *ier = hs_fmm_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
                      sigma_dl, *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, *icomp_type,
                      wsave, *lwsave, lused);
+}
+
+// ---------------------------------------------------------------------------
+// Half-space total field: the direct arrival (free-space evaluation at the
+// centroids, on-surface, and at the targets) plus the image part at the same
+// points, the sum the reference's drivers form from two calls
+// (examples/elhfmm3dtria_self_iter_dr.f:331-385).  The image part of the
+// centroids and the targets is one image-FMM pass over both point sets.
+// Sources and targets must lie in z <= 0 (ier 16, nothing evaluated).
+// ---------------------------------------------------------------------------
+namespace {
+int hs_total_call(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n, const double* src,
+                  int ifsingle, const double* ssl, int ifdouble, const double* sdl, int ifptfrc, double* ptfrc,
+                  int ifstrain, double* strain, int nt, const double* tgt, int ifptfrctarg, double* ptfrctarg,
+                  int ifstraintarg, double* straintarg) {
+  if (n < 1 || nt < 0) return IER_BADARG;
+  if (iprec < -2 || iprec > 6) return IER_BADARG;
+  for (int i = 0; i < 3 * n; i++)
+    if (tri[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < n; i++)
+    if (src[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < nt; i++)
+    if (tgt[3 * i + 2] > 0.0) return IER_BADARG;
+  const bool on_src = ifptfrc || ifstrain;
+  const bool on_tgt = nt > 0 && (ifptfrctarg || ifstraintarg);
+  if (!on_src && !on_tgt) return IER_OK;
+  int ier = host_call(iprec, rlam, rmu, tri, nrm, n, src, ifsingle, ssl, ifdouble, sdl, ifptfrc, ptfrc, ifstrain,
+                      strain, nt, tgt, ifptfrctarg, ptfrctarg, ifstraintarg, straintarg, false);
+  if (ier) return ier;
+  const int ns = on_src ? n : 0;
+  const int m = ns + (on_tgt ? nt : 0);
+  std::vector<double> pts(3 * (size_t)m), ui(3 * (size_t)m), ei(9 * (size_t)m);
+  if (on_src) std::copy(src, src + 3 * (size_t)n, pts.begin());
+  if (on_tgt) std::copy(tgt, tgt + 3 * (size_t)nt, pts.begin() + 3 * (size_t)ns);
+  const int want_u = (on_src && ifptfrc) || (on_tgt && ifptfrctarg);
+  const int want_e = (on_src && ifstrain) || (on_tgt && ifstraintarg);
+  ier = hs_fmm_call(iprec, rlam, rmu, tri, nrm, n, src, ifsingle, ssl, ifdouble, sdl, m, pts.data(), want_u,
+                    ui.data(), want_e, ei.data(), 1, nullptr, 0, nullptr);
+  if (ier) return ier;
+  if (ifptfrc)
+    for (size_t k = 0; k < 3 * (size_t)n; k++) ptfrc[k] += ui[k];
+  if (ifstrain)
+    for (size_t k = 0; k < 9 * (size_t)n; k++) strain[k] += ei[k];
+  if (on_tgt && ifptfrctarg)
+    for (size_t k = 0; k < 3 * (size_t)nt; k++) ptfrctarg[k] += ui[3 * (size_t)ns + k];
+  if (on_tgt && ifstraintarg)
+    for (size_t k = 0; k < 9 * (size_t)nt; k++) straintarg[k] += ei[9 * (size_t)ns + k];
+  return IER_OK;
+}
+}  // namespace
+
+extern "C" void elhfmm3dtria_total_(int* ier, const int* iprec, const double* rlam, const double* rmu,
+                                    const double* triangle, const double* trinorm, const int* nparts,
+                                    const double* source, const int* ifsingle, const double* sigma_sl,
+                                    const int* ifdouble, const double* sigma_dl, const int* ifptfrc, double* ptfrc,
+                                    const int* ifstrain, double* strain, const int* ntargs, const double* target,
+                                    const int* ifptfrctarg, double* ptfrctarg, const int* ifstraintarg,
+                                    double* straintarg) {
+  *ier = hs_total_call(*iprec, *rlam, *rmu, triangle, trinorm, *nparts, source, *ifsingle, sigma_sl, *ifdouble,
+                       sigma_dl, *ifptfrc, ptfrc, *ifstrain, strain, *ntargs, target, *ifptfrctarg, ptfrctarg,
+                       *ifstraintarg, straintarg);
 }
 
 extern "C" int efmm_iter_release(const double* wsave, int lwsave) {

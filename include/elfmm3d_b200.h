@@ -103,11 +103,14 @@ int efmm_batch_host(int iprec, double rlam, double rmu, int n, const double *tri
  * part of the half-space (z <= 0, traction-free surface z = 0) single and
  * double layer potentials at targets, Mindlin's solution (the direct
  * arrival is the free-space evaluation, elfmm3dtriatarg_ / elfmm3dtria_).
- * Here a direct GPU sum over all (target, triangle) pairs with quadrature
- * refined towards the reflected target; iprec is checked but the result is
- * accurate to the quadrature (~1e-9) at every iprec.  icomp_type 0 and 4 do
- * nothing but set lused = 8 (nothing is stored); 1, 2, 3 and 5 evaluate.
- * Sources or targets above z = 0 give ier 16. */
+ * Evaluated by the image FMM (anti-image and Mindlin B/C far field, image
+ * near field by refined quadrature) on the sources and the reflected
+ * targets, to the accuracy of iprec.  icomp_type 1 evaluates; 2 evaluates
+ * and stores the image near field on the device behind the 8-word handle in
+ * wsave (lwsave >= 8; shorter: a plain evaluation); 3 reuses that store
+ * with new densities on the same geometry (512 for a handle that does not
+ * match); 5 behaves as 2; 0 and 4 only set lused = 8.  Sources or targets
+ * above z = 0 give ier 16. */
 void elhfmm3dtriatargiter_(int *ier, const int *iprec, const double *rlam, const double *rmu,
                            const double *triangle, const double *trinorm, const int *nparts,
                            const double *source, const int *ifsingle, const double *sigma_sl,
@@ -115,6 +118,22 @@ void elhfmm3dtriatargiter_(int *ier, const int *iprec, const double *rlam, const
                            const double *target, const int *ifptfrctarg, double *ptfrctarg,
                            const int *ifstraintarg, double *straintarg, const int *icomp_type,
                            double *wsave, const int *lwsave, int *lused);
+
+/* Half-space total field (no single counterpart in the reference, whose
+ * drivers add the two calls, examples/elhfmm3dtria_self_iter_dr.f:331-385):
+ * the direct arrival (elfmm3dtriatarg_, on-surface at the centroids) plus
+ * the image part (elhfmm3dtriatargiter_, icomp_type 1) at the centroids
+ * (ptfrc, strain) and at the targets (ptfrctarg, straintarg), arguments as
+ * in elfmm3dtriatarg_.  The image part of both point sets is one image-FMM
+ * pass.  Sources, centroids or targets above z = 0 give ier 16 (nothing
+ * evaluated). */
+void elhfmm3dtria_total_(int *ier, const int *iprec, const double *rlam, const double *rmu,
+                         const double *triangle, const double *trinorm, const int *nparts,
+                         const double *source, const int *ifsingle, const double *sigma_sl,
+                         const int *ifdouble, const double *sigma_dl, const int *ifptfrc, double *ptfrc,
+                         const int *ifstrain, double *strain, const int *ntargs, const double *target,
+                         const int *ifptfrctarg, double *ptfrctarg, const int *ifstraintarg,
+                         double *straintarg);
 
 /* Frees the device store named by an ITER handle (no counterpart in the
  * reference, whose store is the caller's wsave array).  512 if the handle

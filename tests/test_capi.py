@@ -70,3 +70,27 @@ def test_iprec_tables():
             if jf * hf < eps:
                 return j
     assert [p_for(e) for e in (.5e-3, .5e-6, .5e-9, .5e-12)] == [14, 26, 39, 51]
+
+
+def test_halfspace_total_checks_arguments_before_the_device(lib):
+    """elhfmm3dtria_total_ rejects points above z = 0 with ier 16 before it
+    touches a device; valid input without a device gives 1024."""
+    if lib.device_count() > 0:
+        pytest.skip("a GPU is visible")
+    L = ctypes.CDLL(lib.library_path())
+    dp = ctypes.POINTER(ctypes.c_double)
+    tri = np.array([0, 0, -1, 1, 0, -1, 0, 1, -1], float)
+    nrm = np.array([0, 0, 1.0])
+    src = np.array([1 / 3, 1 / 3, -1.0])
+    sig = np.array([1.0, 0, 0])
+    out = np.zeros(18)
+    i = lambda v: ctypes.byref(ctypes.c_int(v))
+    d = lambda v: ctypes.byref(ctypes.c_double(v))
+    for tgt, want in ((np.array([0.2, 0.2, 0.5]), 16), (np.array([0.2, 0.2, -0.5]), 1024)):
+        ier = ctypes.c_int(-5)
+        L.elhfmm3dtria_total_(ctypes.byref(ier), i(2), d(1.0), d(1.0), tri.ctypes.data_as(dp),
+                              nrm.ctypes.data_as(dp), i(1), src.ctypes.data_as(dp), i(0), sig.ctypes.data_as(dp),
+                              i(1), sig.ctypes.data_as(dp), i(1), out.ctypes.data_as(dp), i(1),
+                              out.ctypes.data_as(dp), i(1), tgt.ctypes.data_as(dp), i(1), out.ctypes.data_as(dp),
+                              i(1), out.ctypes.data_as(dp))
+        assert ier.value == want

@@ -127,3 +127,24 @@ def test_direct_image_matches_c_oracle_same_refinement(gpu, oracle):
         assert ier == 0
         uo, eo = oracle.image_direct(1.3, 0.7, tri, nrm, a, b, tg, level=-1)
         assert rel(u, uo) < 1e-9 and rel(e, eo) < 1e-9
+
+
+def test_halfspace_total_is_the_two_call_sum(gpu):
+    # elhfmm3dtria_total_ = the free-space call (centroids on-surface, and
+    # targets) + the image call at the centroids and the targets together
+    tri, nrm, cen = _fault(4, 3)
+    rng = np.random.default_rng(16)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    tg = np.array([[0.3, 0.4, -0.5], [-1.2, 2.0, -3.0], [2.5, -0.5, 0.0]])
+    ier, pt, st, ptt, stt = gpu.elhfmm3dtria_total(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, tg)
+    assert ier == 0
+    ier1, pf, sf, pft, sft = gpu.elfmm3dtriatarg(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, tg)
+    ier2, _, pi, si = gpu.elhfmm3dtriatargiter(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, np.vstack([cen, tg]))
+    assert ier1 == 0 and ier2 == 0
+    n = len(cen)
+    assert rel(pt, pf + pi[:n]) < 1e-13 and rel(st, sf + si[:n]) < 1e-13
+    assert rel(ptt, pft + pi[n:]) < 1e-13 and rel(stt, sft + si[n:]) < 1e-13
+    # displacement only, no targets; a target above the surface is rejected
+    ier, pt2, st2, _, _ = gpu.elhfmm3dtria_total(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, ifstrain=0)
+    assert ier == 0 and not st2.any() and rel(pt2, pt) < 1e-5
+    assert gpu.elhfmm3dtria_total(2, 1.3, 0.7, tri, nrm, cen, ssl, sdl, [[0.0, 0.0, 0.1]])[0] == 16
