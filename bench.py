@@ -71,6 +71,11 @@ WORKLOADS = {
     "hs-fault-200k-iter": dict(kind="hsiter", nl=500, nw=200, calls=10, iprec=2),
     "sphere-1.3M": dict(kind="single", level=8, ntarg=1_000_000, targets="shell", iprec=2),
     "sphere-5120": dict(kind="single", level=4, ntarg=1_000, targets="box", iprec=2),
+    # the same sphere and shell targets in the mixed form (FP32 far field,
+    # FP64 near-singular parts), errors against the FP64 direct sums at
+    # iprec 1, 2, 3 (eps .5e-3, .5e-6, .5e-9)
+    "sphere-1.3M-mixed": dict(kind="single_mixed", level=8, ntarg=1_000_000, targets="shell", iprec=2,
+                              err_iprecs=(1, 2, 3)),
     # batched uneven geometries: independent half-space faults, random
     # strike / dip / depth, triangle counts log-uniform in [1,000, 50,000]
     "hs-uneven-256": dict(kind="uneven", nprob=256, nmin=1000, nmax=50000, iprec=3),
@@ -388,6 +393,151 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
     }
     return out
+
+
+SINGLE_MIXED_METRIC = ("triangle-evals/s (free-space SLP+DLP displacement+strain, mixed precision, errors vs FP64 "
+                       "direct sums at iprec 1/2/3)")
+
+
+def run_single_mixed(args, rank, world, local_rank):
+    """One right-hand side on the sphere with off-surface targets in the
+    mixed form (evaluate_batch with nrhs 1, precision 1): a step =
+    set_geometry + the mixed pass, as the FP64 sphere workload's step.
+    Beside it: the FP64 pass at the same iprec, and the mixed form's
+    relative error against the FP64 direct sums at each of err_iprecs on
+    2,000 centroids and 2,000 targets (untimed)."""
+    import torch
+    import elfmmlib3d_b200 as E
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+    w = WORKLOADS[args.workload]
+    tri, nrm, cen, tgt, ssl, sdl, iprec = make_inputs(args.workload, seed=1 + rank)
+    n, m = len(cen), len(tgt)
+    evals = (n + m) * n
+
+    def d(a):
+        return torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    dtri, dnrm, dcen, dtgt, dssl, dsdl = map(d, (tri, nrm, cen, tgt, ssl, sdl))
+    z = lambda *shape: torch.zeros(shape, dtype=torch.float64, device=dev)
+    u, e, ut, et = z(1, n, 3), z(1, n, 3, 3), z(1, m, 3), z(1, m, 3, 3)
+    P = E.Plan(local_rank)
+
+    def step(ip=iprec):
+        P.set_geometry(dtri, dnrm, dcen, dtgt, iprec=ip)
+        P.evaluate_batch(1.0, 1.0, 1, dssl[None], dsdl[None], u, e, ut, et, precision=1)
+
+    for _ in range(args.warmup):
+        step()
+    l0 = E.kernel_launches()
+    stage = []
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local_rank) as clk:
+        P.record(0)
+        for _ in range(args.steps):
+            step()
+            stage.append(P.timings())
+        P.record(1)
+        ms = P.elapsed(0, 1)
+    torch.cuda.synchronize()
+    launches = E.kernel_launches() - l0
+    t_max = max_over_ranks(ms, world, dev)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    value = replica_value(evals * args.steps, t_max, world)
+    info = P.info()
+    tim = {k: float(np.mean([s_[k] for s_ in stage])) for k in stage[0]}
+    tr_flops = float(sum(P.translation_flops(1, precision=1).values()))
+    tr_ms = tim["m2m"] + tim["m2l"] + tim["l2l"]
+
+    # end to end from pinned host buffers through the C ABI (efmm_batch_host)
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    htri, hnrm, hcen, htgt = map(pin, (tri, nrm, cen, tgt))
+    hssl, hsdl = pin(ssl[None]), pin(sdl[None])
+    hout = (pin(np.zeros((1, n, 3))), pin(np.zeros((1, n, 3, 3))), pin(np.zeros((1, m, 3))),
+            pin(np.zeros((1, m, 3, 3))))
+    ier, *_ = E.batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, hssl, hsdl, htgt, precision=1, out=hout)
+    assert ier == 0, ier
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ier, *_ = E.batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, hssl, hsdl, htgt, precision=1, out=hout)
+        assert ier == 0, ier
+    e2e_t = max_over_ranks(time.perf_counter() - t0, world, dev)
+    e2e_value = world * evals * args.steps / e2e_t
+    h2d = 8 * (9 * n + 3 * n + 3 * n + 3 * m + 6 * n)
+    d2h = 8 * (3 * n + 9 * n + 3 * m + 9 * m)
+
+    # the FP64 pass at the same iprec
+    u64, e64, ut64, et64 = z(n, 3), z(n, 3, 3), z(m, 3), z(m, 3, 3)
+    P.set_geometry(dtri, dnrm, dcen, dtgt, iprec=iprec)
+    P.evaluate(1.0, 1.0, dssl, dsdl, u64, e64, ut64, et64)
+    P.record(0)
+    P.set_geometry(dtri, dnrm, dcen, dtgt, iprec=iprec)
+    P.evaluate(1.0, 1.0, dssl, dsdl, u64, e64, ut64, et64)
+    P.record(1)
+    fp64_ms = P.elapsed(0, 1)
+
+    # errors against the FP64 direct sums: the first ns centroids (on-surface)
+    # and the first nk targets (a second plan holding only those targets)
+    ns, nk = min(2000, n), min(2000, m)
+    ud, ed = z(ns, 3), z(ns, 3, 3)
+    P.evaluate_direct_subset(1.0, 1.0, ns, dssl, dsdl, ud, ed)
+    Q = E.Plan(local_rank)
+    Q.set_geometry(dtri, dnrm, dcen, dtgt[:nk].contiguous(), iprec=iprec)
+    utd, etd = z(nk, 3), z(nk, 3, 3)
+    Q.evaluate(1.0, 1.0, dssl, dsdl, None, None, utd, etd, direct=True)
+    Q.close()
+    rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
+    errs = {}
+    for ip in w["err_iprecs"]:
+        step(ip)
+        errs[f"mixed_iprec{ip}"] = {"u": rel(u[0, :ns], ud), "strain": rel(e[0, :ns], ed),
+                                    "u_targets": rel(ut[0, :nk], utd), "strain_targets": rel(et[0, :nk], etd),
+                                    "order_iprec": P.info()["p"],
+                                    "order_mixed": P.set_mixed_floor(0.5e-7)}  # the default floor
+    errs[f"fp64_iprec{iprec}"] = {"u": rel(u64[:ns], ud), "strain": rel(e64[:ns], ed),
+                                  "u_targets": rel(ut64[:nk], utd), "strain_targets": rel(et64[:nk], etd)}
+    P.close()
+    if rank != 0:
+        return None
+    achieved = tr_flops / (tr_ms * 1e-3) / 1e12
+    peak32 = gemm_peak(torch, dev, torch.float32)
+    roof = {"kernel": "translations (k_translate_rot_w / k_translate_rot<float>: M2M + M2L + L2L)",
+            "bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
+            "frac": achieved / peak32 if peak32 else None, "traffic": None,
+            "peak_source": "measured cuBLAS SGEMM 8192^3 with TF32 off (best of 5) in this run; the FP32 FMA "
+                           "pipe (MEASURED_PEAKS.json has no FP32 entry)",
+            "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
+                           f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages"}
+    cpu = None
+    if not args.no_cpu_baseline and world == 1:
+        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.cpu_sample)
+        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
+               "sample": f"oracle direct sum, {npts} evaluation points x {n} triangles ({dt:.1f} s)"}
+    return {
+        "metric": SINGLE_MIXED_METRIC,
+        "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": args.workload, "triangles": n, "targets": m, "iprec": iprec,
+                   "evals_per_step": evals, "parallelism": f"replicas{world}",
+                   "l2_policy": "inputs + expansions > L2 (126 MB)",
+                   "step": "set_geometry + mixed pass (one right-hand side, single and double layer)",
+                   "fp64_ms_per_step": fp64_ms, "fp64_value": evals / (fp64_ms * 1e-3),
+                   "rel_err_vs_direct": errs,
+                   "rel_err_sample": f"{ns} centroids (on-surface) and {nk} targets",
+                   "stage_ms": tim, "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")}},
+        "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
+                "d2h_bytes_per_step": d2h,
+                "timing": "host wall clock around blocking efmm_batch_host calls (pinned host arrays)"},
+        "gpu_launches": launches // max(1, args.steps),
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clk.summary(),
+    }
 
 
 def run_batch(args, rank, world, local_rank):
@@ -1105,6 +1255,8 @@ def run_reference(args, rank):
             metric = "triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)"
         elif kind in ("iter", "hsiter"):
             metric = "triangle-evals/s over the ITER call sequence (store once, reuse)"
+        elif kind == "single_mixed":
+            metric = SINGLE_MIXED_METRIC
         else:
             metric = "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)"
     for _ in range(args.warmup):
@@ -1241,6 +1393,8 @@ def main():
             out = run_hsiter(args, rank, world, local_rank)
         elif WORKLOADS[args.workload]["kind"] == "uneven":
             out = run_uneven(args, rank, world, local_rank)
+        elif WORKLOADS[args.workload]["kind"] == "single_mixed":
+            out = run_single_mixed(args, rank, world, local_rank)
         else:
             out = run_ours(args, rank, world, local_rank)
         if world > 1:
