@@ -35,7 +35,7 @@ def test_two_replicas_max_and_value():
     import torch.multiprocessing as mp
     world = 2
     port = _free_port()
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:  # no fork of a threaded process
         out = m.dict()
         mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
