@@ -152,3 +152,19 @@ def test_image_fmm_rejects_non_halfspace_plan(gpu):
         _image(P, d, 1, None, np.ones((1,) + cen.shape), len(cen))
     assert ex.value.ier == 16
     P.close()
+
+
+def test_image_fmm_matches_c_oracle(gpu, oracle):
+    # the image FMM at iprec 3 against the oracle's C image sum (its own
+    # kernels and refinement, independent of the product's direct sum) on
+    # every 40th centroid and all off-surface and surface targets
+    P, tri, nrm, cen, tg, d = _setup(gpu, nl=40, nw=20, iprec=3, seed=3)
+    rng = np.random.default_rng(9)
+    ssl, sdl = rng.normal(size=cen.shape), rng.normal(size=cen.shape)
+    u, e = _image(P, d, 1, ssl[None], sdl[None], len(tg))
+    P.close()
+    sub = np.concatenate([np.arange(0, len(cen), 40), np.arange(len(cen), len(tg))])
+    uo, eo = oracle.image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg[sub], level=-1)
+    eu, ee = rel(u[0][sub], uo), rel(e[0][sub], eo)
+    print(f"iprec 3 image FMM vs C oracle: u {eu:.2e}  strain {ee:.2e}")
+    assert eu < 5e-7 and ee < 5e-7
