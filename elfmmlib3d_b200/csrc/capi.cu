@@ -8,6 +8,7 @@
 #include "plan.h"
 #include "halfspace.h"
 #include "harmonics.cuh"
+#include "mindlin_gen.cuh"
 #include "../../include/elfmm3d_b200.h"
 
 using namespace efmm;
@@ -880,6 +881,23 @@ extern "C" long long efmm_iter_stored_bytes(const double* wsave, int lwsave) {
   IterSlot* S = iter_find(wsave, lwsave);
   if (!S) return -1;
   return 8 * S->p->plan->stored_doubles();
+}
+
+// Host evaluation of the generated image kernels (mindlin_gen.cuh) that the
+// image near field and the direct image sum integrate: the responses at
+// target x to the three unit point forces (layer 0) or to the three unit
+// displacement jumps with normal nrm (layer 1) at source s, 27 doubles (per
+// direction: displacement, strain xx yy zz xy xz yz).
+extern "C" int efmm_mindlin_image_kernel(int layer, double lam, double mu, const double* x, const double* s,
+                                         const double* nrm, double* out) {
+  if (!x || !s || !out || (layer == 1 && !nrm)) return IER_BADARG;
+  if (layer == 0)
+    mindlin_image_sl_blk(lam, mu, x[0], x[1], x[2], s[0], s[1], s[2], out);
+  else if (layer == 1)
+    mindlin_image_dl_blk(lam, mu, x[0], x[1], x[2], s[0], s[1], s[2], nrm[0], nrm[1], nrm[2], out);
+  else
+    return IER_BADARG;
+  return IER_OK;
 }
 
 // Host check of the M2L of the half-space kernel U = z log(r + z) - r built

@@ -230,6 +230,17 @@ int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, 
  * their direct sum; returns the largest relative error (-1 on bad input). */
 double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, unsigned seed);
 
+/* Host evaluation of the image kernels that the half-space image near field
+ * and direct image sum integrate (no counterpart in the reference, whose
+ * kernels are src/el3greenh.f:643-787 with src/mindlinpieces.f): responses
+ * at target x (3) to the three unit point forces (layer 0) or the three
+ * unit displacement jumps with normal nrm (layer 1) at source s (3), both in
+ * z < 0; out[27] = per direction displacement (3) then strain (xx yy zz xy
+ * xz yz), no 1/(4 pi).  For checks of the kernels; no device is used.
+ * Returns 0, or 16 for a bad layer or a NULL pointer. */
+int efmm_mindlin_image_kernel(int layer, double lam, double mu, const double *x, const double *s,
+                              const double *nrm, double *out);
+
 /* Device check of the tensor-core FP32 product (tcgen05.mma kind::tf32,
  * 3-term split) that carries the batched P2M: random A (K x M) and B
  * (N x K) against an FP64 host product; *rel = relative l2 error, *timeout

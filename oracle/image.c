@@ -151,3 +151,17 @@ int oracle_image_direct(double lam, double mu, int n, const double* tri, const d
   }
   return 0;
 }
+
+/* One kernel evaluation (layer 0: the three unit point forces, 1: the three
+ * unit jumps with normal nrm) at target x from source s: out[27] as in
+ * image_gen.h.  Returns 0, or 4 for a bad layer. */
+int oracle_image_kernel(int layer, double lam, double mu, const double* x, const double* s, const double* nrm,
+                        double* out) {
+  if (layer == 0)
+    oracle_image_sl(lam, mu, x[0], x[1], x[2], s[0], s[1], s[2], out);
+  else if (layer == 1)
+    oracle_image_dl(lam, mu, x[0], x[1], x[2], s[0], s[1], s[2], nrm[0], nrm[1], nrm[2], out);
+  else
+    return 4;
+  return 0;
+}
