@@ -51,7 +51,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_evaluate_batch", "efmm_plan_flops",
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
            "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_",
-           "elhfmm3dtria_total_", "efmm_mindlin_image_kernel"]
+           "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
+           "efmm_pair_eval_host"]
 
 
 class ElfmmError(RuntimeError):

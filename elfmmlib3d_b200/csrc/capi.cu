@@ -883,6 +883,28 @@ extern "C" long long efmm_iter_stored_bytes(const double* wsave, int lwsave) {
   return 8 * S->p->plan->stored_doubles();
 }
 
+// Host evaluation of one (triangle, point) pair of the free-space analytic
+// near field: the closed-form integrals and assembly of tri_integrals.cuh
+// that the device near field runs, with the densities rotated into the
+// triangle frame as the device does.  u[3] and e6[6] (xx yy zz xy xz yz) are
+// overwritten.
+extern "C" int efmm_pair_eval_host(double rlam, double rmu, const double* tri, const double* ssl, const double* sdl,
+                                   const double* x, int self, double* u, double* e6) {
+  if (!tri || !x || !u || !e6 || (!ssl && !sdl)) return IER_BADARG;
+  TriFrame f;
+  tri_frame(tri, f);
+  const double* ax[3] = {f.e1, f.e2, f.e3};
+  double sl[3] = {0, 0, 0}, dl[3] = {0, 0, 0};
+  for (int c = 0; c < 3; c++) {
+    if (ssl) sl[c] = ax[c][0] * ssl[0] + ax[c][1] * ssl[1] + ax[c][2] * ssl[2];
+    if (sdl) dl[c] = ax[c][0] * sdl[0] + ax[c][1] * sdl[1] + ax[c][2] * sdl[2];
+  }
+  for (int c = 0; c < 3; c++) u[c] = 0.0;
+  for (int c = 0; c < 6; c++) e6[c] = 0.0;
+  pair_eval(f, sl, dl, ssl != nullptr, sdl != nullptr, true, x, self != 0, rlam, rmu, u, e6);
+  return IER_OK;
+}
+
 // Host evaluation of the generated image kernels (mindlin_gen.cuh) that the
 // image near field and the direct image sum integrate: the responses at
 // target x to the three unit point forces (layer 0) or to the three unit

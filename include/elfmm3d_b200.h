@@ -230,6 +230,18 @@ int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, 
  * their direct sum; returns the largest relative error (-1 on bad input). */
 double efmm_u_m2l_selfcheck(int p, double X0, double X1, double X2, int nsrc, unsigned seed);
 
+/* Host evaluation of one (triangle, point) interaction of the free-space
+ * analytic near field, the closed-form triangle integrals the device near
+ * field runs (the role of elust3triadirecttarg_one / eltst3triadirecttarg_one,
+ * src/elfmm3dtria.f:1689-2015, 2368-2911): displacement u[3] and strain
+ * e6[6] (xx yy zz xy xz yz) at x of the single layer ssl[3] and/or double
+ * layer sdl[3] (global components; NULL disables one; the double layer's
+ * normal is the vertex-order normal) on triangle tri[9]; self = 1 when x is
+ * the triangle's own centroid (principal value / finite part).  For checks;
+ * no device is used.  Returns 0, or 16 for NULL arguments. */
+int efmm_pair_eval_host(double rlam, double rmu, const double *tri, const double *ssl, const double *sdl,
+                        const double *x, int self, double *u, double *e6);
+
 /* Host evaluation of the image kernels that the half-space image near field
  * and direct image sum integrate (no counterpart in the reference, whose
  * kernels are src/el3greenh.f:643-787 with src/mindlinpieces.f): responses
