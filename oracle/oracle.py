@@ -1,4 +1,4 @@
-"""ctypes front end for the CPU oracle (oracle.c).
+"""ctypes front end for the CPU oracle (oracle.c, image.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, ``__graft_entry__.smoke()`` and the
 CPU legs of ``bench.py``; never by the product package.  Array layouts follow the
@@ -24,10 +24,17 @@ def build():
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
 
 
+def _stale():
+    if not os.path.exists(_SO):
+        return True
+    t = os.path.getmtime(_SO)
+    return any(os.path.getmtime(os.path.join(_HERE, f)) > t for f in ("oracle.c", "image.c", "image_gen.h"))
+
+
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(_SO):
+        if _stale():
             build()
         _lib = ctypes.CDLL(_SO)
         _lib.oracle_tree_build.restype = ctypes.c_int
