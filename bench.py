@@ -225,6 +225,20 @@ def gemm_peak(torch, dev, dtype):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def host_threads():
+    """Host threads this process can run at once: its CPU affinity, capped
+    by a cgroup CPU quota when one is set."""
+    n = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as fh:
+            quota, period = fh.read().split()[:2]
+        if quota != "max":
+            n = min(n, max(1, int(quota) // int(period)))
+    except (OSError, ValueError):
+        pass
+    return n
+
+
 def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     """Oracle direct sum for nsample evaluation points against all triangles,
     all host cores.  Returns (evals/s, seconds, cores, points)."""
@@ -237,8 +251,7 @@ def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
         half = nsample
     O.direct(1.0, 1.0, tri, cen, ssl, sdl, tgt, rows=(0, half), trows=(0, nsample - half))
     dt = time.perf_counter() - t0
-    cores = os.cpu_count()
-    return nsample * n / dt, dt, cores, nsample
+    return nsample * n / dt, dt, host_threads(), nsample
 
 
 def cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample):
@@ -255,7 +268,7 @@ def cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample):
     O.direct(1.0, 1.0, tri, cen, ssl, sdl, None, rows=(0, nsample), trows=(0, 0))
     O.image_direct(1.0, 1.0, tri, nrm, ssl, sdl, cen[:nsample], level=-1)
     dt = time.perf_counter() - t0
-    return nsample * n / dt, dt, os.cpu_count(), nsample
+    return nsample * n / dt, dt, host_threads(), nsample
 
 
 def uneven_sample_problems(probs):
@@ -273,7 +286,7 @@ def cpu_oracle_uneven_sample(probs, nsample):
         ev += e * d
         dt += d
         npts += k
-    return ev / dt, dt, os.cpu_count(), npts
+    return ev / dt, dt, host_threads(), npts
 
 
 def make_uneven_problems(w, rank=0):
@@ -1276,7 +1289,7 @@ def run_reference(args, rank):
         "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": args.workload, **cfg},
-        "cpu_baseline": {"value": value, "unit": "triangle-evals/s", "cores": os.cpu_count(), "kind": "port",
+        "cpu_baseline": {"value": value, "unit": "triangle-evals/s", "cores": host_threads(), "kind": "port",
                          "sample": desc},
         "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -1364,7 +1377,7 @@ def main():
     ap.add_argument("--workload", default="hs-fault-100k-r64", choices=list(WORKLOADS))
     # CPU samples: one evaluation point per host thread by default, so that
     # every core has work (the oracle shares the points among its threads)
-    ncpu = min(256, max(8, os.cpu_count() or 8))
+    ncpu = min(256, max(8, host_threads()))
     ap.add_argument("--cpu-sample", type=int, default=ncpu)
     ap.add_argument("--ref-sample", type=int, default=ncpu)
     ap.add_argument("--no-cpu-baseline", action="store_true")
