@@ -7,9 +7,11 @@
 // acceptable.  For them efmm_direct_noalloc evaluates the same O(N^2) analytic
 // direct sum as el3dtriadirecttarg_, with the caller providing inputs and
 // outputs in device memory and all intermediate data held in fixed-size
-// scratch arrays at file scope below.  Those arrays (about 11 MB) exist on
-// every GPU that loads this library, for the life of the process, whether or
-// not the entry point is used.
+// scratch arrays at file scope below.  Those arrays (about 11 MB) stay on a GPU
+// for the life of the process once this file's module is loaded there.  Under
+// CUDA's lazy module loading (the default since CUDA 12) that happens at the
+// first call on the device, which therefore must come before the caller's pool
+// reserves the free memory (a call with one triangle is enough).
 #include <mutex>
 #include "common.cuh"
 #include "kernels.h"
@@ -27,7 +29,9 @@ static __device__ __align__(256) double g_noalloc_e[6 * NOALLOC_MAX_PTS];
 
 // Device addresses of the scratch arrays, looked up once per device.  In host
 // code the array names above stand for host-side shadows, not device
-// addresses, so the kernels must be given these looked-up pointers.
+// addresses, so the kernels must be given these looked-up pointers.  They
+// belong to the device's primary context: after cudaDeviceReset they are
+// stale, and the entry point must not be used again in that process.
 struct NoallocPtrs {
   TriRec* tri;
   double* u;
@@ -77,8 +81,10 @@ using namespace efmm;
 // See include/elfmm3d_b200.h.  Enqueues on `stream` and returns; the outputs
 // are complete when the stream reaches that point.  The first call on a device
 // looks up the scratch addresses for that device (make it before any stream
-// capture).  Calls that overlap on the GPU (different streams or host
-// threads, same device) share the scratch and race.
+// capture and before a memory pool reserves the free memory).  Calls that
+// overlap on the GPU (different streams or host threads, same device) share
+// the scratch and race.  A launch error left pending by earlier work of the
+// calling thread is not consumed: the call returns IER_CUDA without running.
 extern "C" int efmm_direct_noalloc(double rlam, double rmu, int n, const double* tri,
                                    const double* src, const double* ssl, const double* sdl, int nt,
                                    const double* tgt, double* u_src, double* e_src, double* u_tgt,
@@ -93,6 +99,7 @@ extern "C" int efmm_direct_noalloc(double rlam, double rmu, int n, const double*
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return IER_NODEVICE;
+  if (cudaPeekAtLastError() != cudaSuccess) return IER_CUDA;
   NoallocPtrs S;
   int ier = noalloc_setup(dev, S);
   if (ier) return ier;

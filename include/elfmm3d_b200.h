@@ -335,13 +335,16 @@ float efmm_plan_elapsed(efmm_plan *plan, int a, int b);
  * tri (n,3,3), src (n,3), ssl/sdl (n,3; NULL disables a layer), tgt (nt,3);
  * outputs u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3), NULL
  * disables one.  Intermediates live in fixed file-scope device arrays
- * (about 11 MB, present on every GPU that loads the library until exit):
- * at most 32768 triangles and 65536 evaluation points (n + nt) per call;
- * larger sizes return 16 with a message on stderr.  Enqueues on `stream`
- * (a cudaStream_t, NULL = legacy default stream) and returns; the first call
- * on a device looks up the scratch addresses for that device and should come
- * before any stream capture.  Calls that overlap on the GPU share the scratch
- * and race. */
+ * (about 11 MB per GPU, held until exit once loaded): at most 32768
+ * triangles and 65536 evaluation points (n + nt) per call; larger sizes
+ * return 16 with a message on stderr.  Enqueues on `stream` (a cudaStream_t,
+ * NULL = legacy default stream) and returns.  The first call on a device
+ * loads the scratch (CUDA loads modules lazily by default) and looks up its
+ * address: make it (n = 1 is enough) before a memory pool reserves the
+ * device's free memory and before any stream capture.  Calls that overlap on
+ * the GPU share the scratch and race.  Not usable after cudaDeviceReset in
+ * the same process.  A launch error already pending in the calling thread
+ * makes the call return 256 without running and without clearing it. */
 int efmm_direct_noalloc(double rlam, double rmu, int n, const double *tri, const double *src,
                         const double *ssl, const double *sdl, int nt, const double *tgt,
                         double *u_src, double *e_src, double *u_tgt, double *e_tgt, void *stream);
