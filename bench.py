@@ -6,42 +6,47 @@ side) interaction (elhfmm3dtria_self_iter_dr.f:270 counts points x triangles;
 times the number of right-hand sides for the batched forms).
 
 Workloads (seeded synthetic inputs, no datasets):
-  fault-100k-r64 : [default] planar fault 40 x 20 dipping 45 degrees, top edge
-                   at depth 1, 250 x 200 cells x 2 = 100,000 right triangles,
-                   64 displacement-jump right-hand sides i.i.d. N(0,1) (double
-                   layer), lambda = mu = 1, displacement + strain at the
-                   centroids, free space, iprec 3.  The 64-RHS fault shape of
-                   the half-space configuration, evaluated with the free-space
-                   Green's function (the half-space image path is not built).
-                   A step = set_geometry + one batched evaluation of all 64
-                   right-hand sides in the mixed-precision form (P2M products,
-                   expansions and translations FP32 in the normalised basis;
-                   near field and local evaluation FP64).  The plain FP64 form
-                   (64 single evaluations, each with its own set_geometry) and
-                   the batched FP64 form are timed beside it, and the relative
-                   l2 error of every form against the FP64 direct sum on 2,000
-                   centroids is measured in the same run.
-  fault-10k-r32  : the same fault at 100 x 50 cells (10,000 triangles), 32
-                   right-hand sides: the small case for profiler captures.
-  fault-200k-iter: the ITER call sequence of the half-space self-evaluation
-                   configuration on the same fault at 500 x 200 cells
-                   (200,000 triangles), free space, iprec 2: slip = cos^2
-                   taper along strike x down dip + 5 % N(0,1) noise (new noise
-                   per call), displacement + strain at the centroids.  A step
-                   = one call; the timed region is the whole sequence: tree +
-                   store + evaluate on the first call, 9 calls reusing the
-                   stored near field.  The plain form (10 full calls) is timed
-                   beside it.
-  sphere-1.3M    : unit icosphere refined 8x (1,310,720 flat triangles) plus
+  hs-fault-100k-r64 : [default] the Mindlin half-space multi-RHS configuration:
+                   planar fault 40 x 20 dipping 45 degrees, top edge at depth
+                   1, 250 x 200 cells x 2 = 100,000 right triangles, 64 slip
+                   (displacement-jump) right-hand sides i.i.d. N(0,1),
+                   lambda = mu = 1, displacement + strain at the centroids,
+                   iprec 3.  Direct arrival (free-space plan) + image part
+                   (image plan on the reflected centroids), both near fields
+                   stored on the first call and replayed as block products;
+                   a step = one mixed-precision pass of all 64 right-hand
+                   sides through both plans, each replayed as a CUDA graph.
+                   Beside it: the plain FP64 form (one ITER call pair per
+                   right-hand side), the batched FP64 form, errors of every
+                   form against the FP64 direct sums on 2,000 centroids and
+                   against the oracle at the CPU sample's centroids.
+  hs-fault-10k-r32 : the same at 100 x 50 cells, 32 right-hand sides (the
+                   small case for profiler captures).
+  fault-100k-r64 / fault-10k-r32 : the same faults and right-hand sides in
+                   free space (one plan).
+  fault-200k-iter  : the ITER call sequence of the half-space self-evaluation
+                   configuration on the free-space kernel: 500 x 200 cells
+                   (200,000 triangles), iprec 2, slip = cos^2 taper + 5 %
+                   N(0,1) noise (new noise per call); the timed region is the
+                   whole sequence (tree + store on the first call, 9 reuses).
+  hs-fault-200k-iter : the same sequence in the half space (direct arrival +
+                   image part through both ITER stores).
+  sphere-1.3M      : unit icosphere refined 8x (1,310,720 flat triangles) plus
                    1,000,000 targets uniform in the shell 1.05 < |x| < 3,
-                   single + double layer N(0,1), iprec 2, one right-hand side,
-                   plain FP64 (step = set_geometry + evaluate).
-  sphere-5120    : icosphere level 4 (5,120 triangles) plus 1,000 targets
+                   single + double layer N(0,1), iprec 2, plain FP64.
+  sphere-1.3M-mixed : the same in the mixed form, errors against the FP64
+                   direct sums at iprec 1, 2, 3.
+  sphere-5120      : icosphere level 4 (5,120 triangles) plus 1,000 targets
                    uniform in [-2,2]^3 with |x| > 1.1, iprec 2, plain FP64.
+  hs-uneven-256 / hs-uneven-32 : independent half-space faults (random
+                   strike / dip / depth, triangle counts log-uniform), one
+                   slip right-hand side each, mixed form.
 
 Inputs are resident in device memory for `value`; `e2e` runs the same step
-through the C ABI from pinned host buffers (efmm_batch_host for the batched
-workload, elfmm3dtriatarg_ for the single ones), host copies included.
+through the C ABI from pinned host buffers (elhfmm3dtria_batch_host for the
+half-space batch, efmm_batch_host for the free-space batch and the mixed
+sphere, elfmm3dtriatarg_ for the single ones, the ITER entry points for the
+call sequences), host copies included.
 
 --impl reference times the CPU stand-in for the reference (the oracle's direct
 restatement of el3dtriadirecttarg; the Fortran reference cannot be compiled on
@@ -241,7 +246,10 @@ def host_threads():
 
 def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     """Oracle direct sum for nsample evaluation points against all triangles,
-    all host cores.  Returns (evals/s, seconds, cores, points)."""
+    all host cores: the first half of the sample on the centroids, the rest
+    on the targets.  Returns (evals/s, seconds, cores, points, outputs), the
+    outputs (u, strain at the first `rows` centroids; ut, et at the first
+    `trows` targets) kept for the GPU forms' errors against the oracle."""
     from oracle import oracle as O
     O.lib()
     n = len(cen)
@@ -249,9 +257,12 @@ def cpu_oracle_sample(tri, cen, tgt, ssl, sdl, nsample, seed=0):
     t0 = time.perf_counter()
     if len(tgt) == 0:
         half = nsample
-    O.direct(1.0, 1.0, tri, cen, ssl, sdl, tgt, rows=(0, half), trows=(0, nsample - half))
+    half = min(half, n)
+    nt = min(nsample - half, len(tgt))
+    pt, st, ptt, stt = O.direct(1.0, 1.0, tri, cen, ssl, sdl, tgt, rows=(0, half), trows=(0, nt))
     dt = time.perf_counter() - t0
-    return nsample * n / dt, dt, host_threads(), nsample
+    ref = {"rows": half, "trows": nt, "u": pt[:half], "e": st[:half], "ut": ptt[:nt], "et": stt[:nt]}
+    return (half + nt) * n / dt, dt, host_threads(), half + nt, ref
 
 
 def cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample):
@@ -265,10 +276,11 @@ def cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample):
     n = len(cen)
     nsample = min(nsample, n)
     t0 = time.perf_counter()
-    O.direct(1.0, 1.0, tri, cen, ssl, sdl, None, rows=(0, nsample), trows=(0, 0))
-    O.image_direct(1.0, 1.0, tri, nrm, ssl, sdl, cen[:nsample], level=-1)
+    pt, st, _, _ = O.direct(1.0, 1.0, tri, cen, ssl, sdl, None, rows=(0, nsample), trows=(0, 0))
+    ui, ei = O.image_direct(1.0, 1.0, tri, nrm, ssl, sdl, cen[:nsample], level=-1)
     dt = time.perf_counter() - t0
-    return nsample * n / dt, dt, host_threads(), nsample
+    ref = {"rows": nsample, "trows": 0, "u": pt[:nsample] + ui, "e": st[:nsample] + ei}
+    return nsample * n / dt, dt, host_threads(), nsample, ref
 
 
 def uneven_sample_problems(probs):
@@ -279,14 +291,37 @@ def uneven_sample_problems(probs):
 
 def cpu_oracle_uneven_sample(probs, nsample):
     """cpu_oracle_hs_sample on the first nsample centroids of each problem of
-    uneven_sample_problems.  Returns (evals/s, seconds, cores, points)."""
-    ev, dt, npts = 0.0, 0.0, 0
+    uneven_sample_problems.  Returns (evals/s, seconds, cores, points, the
+    oracle outputs of each sampled problem)."""
+    ev, dt, npts, refs = 0.0, 0.0, 0, []
     for tri, nrm, cen, ssl, sdl in uneven_sample_problems(probs):
-        e, d, cores, k = cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample)
+        e, d, cores, k, ref = cpu_oracle_hs_sample(tri, nrm, cen, ssl, sdl, nsample)
         ev += e * d
         dt += d
         npts += k
-    return ev / dt, dt, host_threads(), npts
+        refs.append(ref)
+    return ev / dt, dt, host_threads(), npts, refs
+
+
+def oracle_errors(ref, u=None, e=None, ut=None, et=None):
+    """Relative l2 errors of GPU outputs (numpy or torch, evaluation points
+    in the order of the oracle sample) against the oracle's outputs at the
+    sampled points: the first ref["rows"] centroids and ref["trows"] targets."""
+    def rel(a, b):
+        a = a.detach().cpu().numpy() if hasattr(a, "detach") else np.asarray(a)
+        b = np.asarray(b)
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b)) if np.linalg.norm(b) > 0 else None
+    out = {}
+    r, t = ref["rows"], ref.get("trows", 0)
+    if u is not None and r:
+        out["u"] = rel(u[:r], ref["u"])
+    if e is not None and r:
+        out["strain"] = rel(e[:r], ref["e"])
+    if ut is not None and t:
+        out["u_targets"] = rel(ut[:t], ref["ut"])
+    if et is not None and t:
+        out["strain_targets"] = rel(et[:t], ref["et"])
+    return out
 
 
 def make_uneven_problems(w, rank=0):
@@ -383,11 +418,12 @@ def run_ours(args, rank, world, local_rank):
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
             "peak_source": "measured cuBLAS DGEMM 8192^3 in this run (FP64 has no entry in MEASURED_PEAKS.json)",
             "algorithmic": f"{NEAR_FLOPS_PER_PAIR:.0f} FP64 flop/pair x {info['near_pairs']} pairs"}
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.cpu_sample)
+        ev, dt, cores, npts, ref = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle direct sum, {npts} evaluation points x {n} triangles ({dt:.1f} s)"}
+        oerr = oracle_errors(ref, u, e, ut, et)
     out = {
         "metric": "triangle-evals/s (free-space SLP+DLP displacement+strain, FP64 FMM at iprec 2)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -397,7 +433,9 @@ def run_ours(args, rank, world, local_rank):
                    "evals_per_step": evals, "parallelism": f"replicas{world}",
                    "l2_policy": "inputs + expansions > L2 (126 MB)",
                    "stage_ms": tim, "setup_ms": setup, "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")},
-                   "near_pairs": info["near_pairs"], "m2l_pairs": info["m2l_pairs"]},
+                   "near_pairs": info["near_pairs"], "m2l_pairs": info["m2l_pairs"],
+                   "rel_err_vs_oracle": oerr,
+                   "rel_err_vs_oracle_sample": "the cpu_baseline sample's points (oracle FP64 direct sum)"},
         "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h, "timing": "host wall clock around blocking C-ABI calls"},
         "gpu_launches": launches,
@@ -504,15 +542,26 @@ def run_single_mixed(args, rank, world, local_rank):
     Q.evaluate(1.0, 1.0, dssl, dsdl, None, None, utd, etd, direct=True)
     Q.close()
     rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
-    errs = {}
+    # the oracle's FP64 direct sum at the CPU sample's points (also the timed
+    # CPU baseline): errors of every form against it
+    cpu, ref = None, None
+    if not args.no_cpu_baseline and world == 1:
+        ev, dt, cores, npts, ref = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.cpu_sample)
+        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
+               "sample": f"oracle direct sum, {npts} evaluation points x {n} triangles ({dt:.1f} s)"}
+    errs, oerr = {}, {}
     for ip in w["err_iprecs"]:
         step(ip)
         errs[f"mixed_iprec{ip}"] = {"u": rel(u[0, :ns], ud), "strain": rel(e[0, :ns], ed),
                                     "u_targets": rel(ut[0, :nk], utd), "strain_targets": rel(et[0, :nk], etd),
                                     "order_iprec": P.info()["p"],
                                     "order_mixed": P.set_mixed_floor(0.5e-7)}  # the default floor
+        if ref is not None:
+            oerr[f"mixed_iprec{ip}"] = oracle_errors(ref, u[0], e[0], ut[0], et[0])
     errs[f"fp64_iprec{iprec}"] = {"u": rel(u64[:ns], ud), "strain": rel(e64[:ns], ed),
                                   "u_targets": rel(ut64[:nk], utd), "strain_targets": rel(et64[:nk], etd)}
+    if ref is not None:
+        oerr[f"fp64_iprec{iprec}"] = oracle_errors(ref, u64, e64, ut64, et64)
     P.close()
     if rank != 0:
         return None
@@ -525,11 +574,6 @@ def run_single_mixed(args, rank, world, local_rank):
                            "pipe (MEASURED_PEAKS.json has no FP32 entry)",
             "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
                            f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages"}
-    cpu = None
-    if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, tgt, ssl, sdl, args.cpu_sample)
-        cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
-               "sample": f"oracle direct sum, {npts} evaluation points x {n} triangles ({dt:.1f} s)"}
     return {
         "metric": SINGLE_MIXED_METRIC,
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -542,6 +586,9 @@ def run_single_mixed(args, rank, world, local_rank):
                    "fp64_ms_per_step": fp64_ms, "fp64_value": evals / (fp64_ms * 1e-3),
                    "rel_err_vs_direct": errs,
                    "rel_err_sample": f"{ns} centroids (on-surface) and {nk} targets",
+                   "rel_err_vs_oracle": oerr or None,
+                   "rel_err_vs_oracle_sample": "the cpu_baseline sample's centroids and targets (oracle FP64 "
+                                               "direct sum)",
                    "stage_ms": tim, "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")}},
         "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
@@ -666,12 +713,14 @@ def run_batch(args, rank, world, local_rank):
             "algorithmic": f"factored translations (rotation, shift along z, rotation back): "
                            f"{tr_flops:.4g} flop per step over {info['m2l_pairs']} M2L pairs x {C} columns"}
     stage_tf = {k: fl[k] * C / (tim[k] * 1e-3) / 1e12 for k in ("p2m", "m2m", "m2l", "l2l", "l2t") if tim[k] > 0}
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
+        ev, dt, cores, npts, ref = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, sdl[0], args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle direct sum, {npts} centroids x {n} triangles x 1 right-hand side "
                          f"({dt:.1f} s)"}
+        oerr = {k: oracle_errors(ref, uu[0], ee[0]) for k, (uu, ee) in
+                (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)), ("mixed_batched", (u_mixed, e_mixed)))}
     plain_value = evals / (plain_ms * 1e-3)
     b64_value = evals / (b64_ms * 1e-3)
     return {
@@ -687,6 +736,9 @@ def run_batch(args, rank, world, local_rank):
                              "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms},
                    "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
                    "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
+                   "rel_err_vs_oracle": oerr,
+                   "rel_err_vs_oracle_sample": "right-hand side 0 at the cpu_baseline sample's centroids "
+                                               "(oracle FP64 direct sum)",
                    "stage_ms": tim, "stage_tflops": stage_tf, "setup_ms": setup,
                    "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")},
                    "near_pairs": info["near_pairs"], "m2l_pairs": info["m2l_pairs"]},
@@ -781,27 +833,6 @@ def run_hsbatch(args, rank, world, local_rank):
     ti = {k: float(np.mean([s_[1][k] for s_ in stages])) for k in stages[0][1]}
     u_mixed, e_mixed = (uf + ui).clone(), (ef + ei).clone()
 
-    # end to end through the plan API: slip vectors from pinned host memory,
-    # total displacement + strain back to pinned host memory, every step
-    hsdl = torch.from_numpy(np.ascontiguousarray(sdl)).pin_memory()
-    hu = torch.empty((R, n, 3), dtype=torch.float64).pin_memory()
-    he = torch.empty((R, n, 3, 3), dtype=torch.float64).pin_memory()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        dsdl.copy_(hsdl)
-        step(graph=True)
-        torch.add(uf, ui, out=uf)
-        torch.add(ef, ei, out=ef)
-        hu.copy_(uf)
-        he.copy_(ef)
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - t0
-    e2e_t = max_over_ranks(e2e_s, world, dev)
-    e2e_value = world * evals * args.steps / e2e_t
-    h2d = 8 * 3 * n * R
-    d2h = 8 * (3 * n * R + 9 * n * R)
-
     # the mixed form at the iprec orders (no truncation floor), beside the
     # headline: plain passes timed with events
     F.set_mixed_floor(0.0)
@@ -863,6 +894,45 @@ def run_hsbatch(args, rank, world, local_rank):
                               ("mixed_batched_iprec_orders", (u_mi, e_mi))):
             errs[key][0] = max(errs[key][0], rel(uu[r, :ns], udt))
             errs[key][1] = max(errs[key][1], rel(ee[r, :ns], edt))
+    trf = F.translation_flops(R, 1)
+    tri_ = I.translation_flops(R, 1)
+    fi, ii = F.info(), I.info()
+    stored = {"free": F.stored_bytes(), "image": I.stored_bytes()}
+    F.close()  # the C-ABI call below holds its own plans and stores
+    I.close()
+    del uf, ef, ui, ei
+    torch.cuda.empty_cache()
+
+    # end to end through the C ABI (elhfmm3dtria_batch_host): the 64 slip
+    # vectors from pinned host memory, both plans' passes (stored near
+    # fields replayed, each pass one CUDA graph), the total displacement and
+    # strain back to pinned host memory, every step; the store call
+    # (icomp_type 2) and one replay before the timed calls are untimed
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy()
+    htri, hnrm, hcen, hsdl = map(pin, (tri, nrm, cen, sdl))
+    hout = (pin(np.zeros((R, n, 3))), pin(np.zeros((R, n, 3, 3))))
+    ws = np.zeros(8)
+    t0 = time.perf_counter()
+    ier, _, _ = E.hs_batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, icomp_type=2,
+                                wsave=ws, out=hout)
+    assert ier == 0, ier
+    e2e_store_s = time.perf_counter() - t0
+    ier, _, _ = E.hs_batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, icomp_type=3,
+                                wsave=ws, out=hout)
+    assert ier == 0, ier
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ier, _, _ = E.hs_batch_host(iprec, 1.0, 1.0, htri, hnrm, hcen, None, hsdl, precision=1, icomp_type=3,
+                                    wsave=ws, out=hout)
+        assert ier == 0, ier
+    e2e_s = time.perf_counter() - t0
+    E.iter_release(ws)
+    e2e_t = max_over_ranks(e2e_s, world, dev)
+    e2e_value = world * evals * args.steps / e2e_t
+    h2d = 8 * 3 * n * R
+    d2h = 8 * (3 * n * R + 9 * n * R)
+    e2e_vs_value = {"u": rel(torch.from_numpy(hout[0]).to(dev), u_mixed),
+                    "strain": rel(torch.from_numpy(hout[1]).to(dev), e_mixed)}
     if rank != 0:
         return None
     # roofline: the P2M products of both plans (k_gemm_tc, the largest
@@ -892,8 +962,6 @@ def run_hsbatch(args, rank, world, local_rank):
     # translations (k_translate_rot_w / k_translate_rot, FP32 FMA pipe),
     # flops counted per pair and column as they run, time = the M2M + M2L +
     # L2L stage events of both plans, against the measured SGEMM rate
-    trf = F.translation_flops(R, 1)
-    tri_ = I.translation_flops(R, 1)
     tr_flops = sum(trf.values()) + sum(tri_.values())
     tr_ms = float(np.mean([sum(s_[0][k] + s_[1][k] for k in ("m2m", "m2l", "l2l")) for s_ in stages]))
     peak32 = gemm_peak(torch, dev, torch.float32)
@@ -907,17 +975,19 @@ def run_hsbatch(args, rank, world, local_rank):
             "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
                            f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages",
             "flops_by_stage": {"free": trf, "image": tri_}}
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_hs_sample(tri, nrm, cen, None, sdl[0], args.cpu_sample)
+        ev, dt, cores, npts, ref = cpu_oracle_hs_sample(tri, nrm, cen, None, sdl[0], args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
                          f"distance refinement), {npts} centroids x {n} triangles x 1 right-hand side "
                          f"({dt:.1f} s)"}
+        oerr = {k: oracle_errors(ref, uu[0], ee[0]) for k, (uu, ee) in
+                (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)), ("mixed_batched", (u_mixed, e_mixed)),
+                 ("mixed_batched_iprec_orders", (u_mi, e_mi)))}
+        oerr["e2e_c_abi"] = oracle_errors(ref, hout[0][0], hout[1][0])
     plain_value = evals / (plain_ms * 1e-3)
     b64_value = evals / (b64_ms * 1e-3)
-    fi = F.info()
-    ii = I.info()
     return {
         "metric": "triangle-evals/s at <=1e-6 rel err (mixed-precision batched form; plain FP64 beside it)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -943,14 +1013,19 @@ def run_hsbatch(args, rank, world, local_rank):
                                       "at eps(iprec)"},
                    "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
                    "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
+                   "rel_err_vs_oracle": oerr,
+                   "rel_err_vs_oracle_sample": "right-hand side 0 at the cpu_baseline sample's centroids (oracle "
+                                               "FP64 free-space direct sum + image quadrature)",
                    "stage_ms_free": tf, "stage_ms_image": ti,
                    "tree_free": {k: fi[k] for k in ("nboxes", "nlev", "p", "nbox")},
                    "tree_image": {k: ii[k] for k in ("nboxes", "nlev", "p", "nbox")},
-                   "stored_bytes": {"free": F.stored_bytes(), "image": I.stored_bytes()}},
+                   "stored_bytes": stored},
         "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
-                "timing": "host wall clock: pinned slip vectors to the device, both plans, total displacement + "
-                          "strain back to pinned host memory, every step"},
+                "timing": "host wall clock around blocking elhfmm3dtria_batch_host calls (icomp_type 3: pinned "
+                          "slip vectors to the device, both plans' stored-near-field passes as CUDA graphs, the "
+                          "total displacement + strain back to pinned host memory)",
+                "store_call_s": e2e_store_s, "outputs_vs_value_step": e2e_vs_value},
         "gpu_launches": launches,
         "roofline": roof,
         "roofline_tc": roof_tc,
@@ -1015,7 +1090,7 @@ def run_iter(args, rank, world, local_rank):
     value = replica_value(evals, t_max, world)
     info = P.info()
     stored = P.stored_bytes()
-    u_last = u.clone()
+    u_last, e_last = u.clone(), e.clone()
     # error of the last call against the FP64 direct sum on 2,000 centroids
     ns = min(2000, n)
     ud = torch.zeros((ns, 3), dtype=torch.float64, device=dev)
@@ -1056,11 +1131,13 @@ def run_iter(args, rank, world, local_rank):
             "frac": (gbs / peak) if peak else None, "traffic": None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peak else "MEASURED_PEAKS.json absent",
             "algorithmic": f"stored near field read once per call: {stored / 1e9:.2f} GB"}
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, slips[0], args.cpu_sample)
+        ev, dt, cores, npts, ref = cpu_oracle_sample(tri, cen, np.zeros((0, 3)), None, slips[ncall - 1],
+                                                     args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle direct sum, {npts} centroids x {n} triangles ({dt:.1f} s)"}
+        oerr = oracle_errors(ref, u_last, e_last)
     return {
         "metric": "triangle-evals/s over the ITER call sequence (store once, reuse)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": ncall, "warmup": max(args.warmup, 2),
@@ -1072,6 +1149,8 @@ def run_iter(args, rank, world, local_rank):
                    "first_call_ms": store_tim["total"], "replay_call_ms": rep_tot, "replay_near_ms": rep_near,
                    "plain_call_ms": plain_call_ms, "sequence_over_plain": plain_call_ms * ncall / t_max,
                    "rel_err_vs_direct_last_call": err, "stored_bytes": stored,
+                   "rel_err_vs_oracle_last_call": oerr,
+                   "rel_err_vs_oracle_sample": "the cpu_baseline sample's centroids (oracle FP64 direct sum)",
                    "tree": {k: info[k] for k in ("nboxes", "nlev", "p", "nbox")}, "near_pairs": info["near_pairs"]},
         "e2e": {"value": world * evals / e2e_s, "unit": "triangle-evals/s",
                 "h2d_bytes_per_step": 8 * (9 * n + 3 * n + 3 * n + 3 * n), "d2h_bytes_per_step": 8 * (3 * n + 9 * n),
@@ -1201,12 +1280,13 @@ def run_hsiter(args, rank, world, local_rank):
             "unit": "GB/s", "frac": (gbs / peak) if peak else None, "traffic": None,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs" if peak else "MEASURED_PEAKS.json absent",
             "algorithmic": f"stored near field read once per call: {stored[0] / 1e9:.2f} GB"}
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_hs_sample(tri, nrm, cen, None, slips[0], args.cpu_sample)
+        ev, dt, cores, npts, ref = cpu_oracle_hs_sample(tri, nrm, cen, None, slips[ncall - 1], args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
                          f"distance refinement), {npts} centroids x {n} triangles ({dt:.1f} s)"}
+        oerr = oracle_errors(ref, ut, et)
     return {
         "metric": "triangle-evals/s over the ITER call sequence (store once, reuse)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": ncall, "warmup": max(args.warmup, 2),
@@ -1217,6 +1297,9 @@ def run_hsiter(args, rank, world, local_rank):
                    "parallelism": f"replicas{world}",
                    "l2_policy": f"stored near fields {sum(stored) / 1e9:.1f} GB > L2 (126 MB)",
                    "first_call_s": first_s, "replay_call_ms": {"free": rep_f, "image": rep_i},
+                   "rel_err_vs_oracle_last_call": oerr,
+                   "rel_err_vs_oracle_sample": "the cpu_baseline sample's centroids (oracle FP64 free-space direct "
+                                               "sum + image quadrature)",
                    "plain_call_ms": plain_call_ms, "sequence_over_plain": plain_call_ms * ncall / t_max,
                    "rel_err_vs_direct_last_call": err, "stored_bytes": {"free": stored[0], "image": stored[1]}},
         "e2e": {"value": world * evals / e2e_s, "unit": "triangle-evals/s",
@@ -1277,7 +1360,7 @@ def run_reference(args, rank):
     evs, secs = 0.0, 0.0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        ev, dt, cores, npts = sample()
+        ev, dt, cores, npts = sample()[:4]
         evs += ev * dt
         secs += dt
     tot = time.perf_counter() - t0
@@ -1333,13 +1416,20 @@ def run_uneven(args, rank, world, local_rank):
     errs = np.array(cinfo["errors"])
     if rank != 0:
         return None
-    cpu = None
+    cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
-        ev, dt, cores, npts = cpu_oracle_uneven_sample(probs, args.cpu_sample)
+        ev, dt, cores, npts, refs = cpu_oracle_uneven_sample(probs, args.cpu_sample)
         cpu = {"value": ev, "unit": "triangle-evals/s", "cores": cores, "kind": "port",
                "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
                          f"distance refinement) at {npts} centroids of {len(uneven_sample_problems(probs))} "
                          f"evenly spaced problems, against all of their problem's triangles ({dt:.1f} s)"}
+        # per-problem errors of the mixed form against the oracle at those centroids
+        sp = uneven_sample_problems(probs)
+        res, _ = halfspace_many(sp, iprec=w["iprec"], precision=1, workers=workers, device=local_rank)
+        per = [oracle_errors(ref, uu, ee) for ref, (uu, ee) in zip(refs, res)]
+        oerr = {"problems": len(per), "triangles": [int(len(p_[2])) for p_ in sp],
+                "u": [x.get("u") for x in per], "strain": [x.get("strain") for x in per],
+                "u_max": max(x.get("u") or 0.0 for x in per), "strain_max": max(x.get("strain") or 0.0 for x in per)}
     return {
         "metric": "triangle-evals/s (batched uneven half-space geometries, mixed precision)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -1356,6 +1446,8 @@ def run_uneven(args, rank, world, local_rank):
                                          "u_median": float(np.median(errs[:, 0])),
                                          "strain_max": float(errs[:, 1].max()),
                                          "strain_median": float(np.median(errs[:, 1]))},
+                   "rel_err_vs_oracle": oerr,
+                   "rel_err_vs_oracle_sample": "per sampled problem, the cpu_baseline sample's centroids",
                    "parallelism": f"replicas{world}"},
         "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": int(sizes.sum() * 8 * (9 + 3 + 3 + 3)),
                 "d2h_bytes_per_step": int(sizes.sum() * 8 * 12),

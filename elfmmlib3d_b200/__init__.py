@@ -52,7 +52,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
            "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_",
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
-           "efmm_pair_eval_host"]
+           "efmm_pair_eval_host", "elhfmm3dtria_batch_host"]
 
 
 class ElfmmError(RuntimeError):
@@ -125,6 +125,10 @@ def load():
     L.efmm_batch_host.restype = ctypes.c_int
     L.efmm_batch_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp, _dp,
                                   ctypes.c_int, _dp, ctypes.c_int, _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
+    L.elhfmm3dtria_batch_host.restype = ctypes.c_int
+    L.elhfmm3dtria_batch_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp,
+                                          _dp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp,
+                                          ctypes.c_int]
     L.efmm_iter_release.restype = ctypes.c_int
     L.efmm_iter_release.argtypes = [_dp, ctypes.c_int]
     L.efmm_iter_stored_bytes.restype = ctypes.c_longlong
@@ -254,6 +258,32 @@ def batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma
     ier = L.efmm_batch_host(int(iprec), float(rlam), float(rmu), n, p(tri), p(nrm), p(src), m, p(tg), R, p(ssl),
                             p(sdl), p(pt), p(st), p(ptt) if m else None, p(stt) if m else None, int(precision))
     return ier, pt, st, ptt[:, :m], stt[:, :m]
+
+
+def hs_batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, precision=1,
+                  icomp_type=1, wsave=None, out=None):
+    """Half-space self-evaluation (direct arrival + image part) of nrhs
+    right-hand sides from host arrays through elhfmm3dtria_batch_host:
+    sigma_sl/sigma_dl (nrhs,n,3).  icomp_type 1 evaluates, 2 also stores both
+    near fields behind ``wsave`` (8 doubles), 3 replays them with new
+    densities.  Returns (ier, ptfrc (nrhs,n,3), strain (nrhs,n,3,3)).
+    ``out`` may pass preallocated (e.g. pinned) output arrays."""
+    L = load()
+    _need_gpu()
+    tri = _c(triangle, (-1, 3, 3))
+    n = tri.shape[0]
+    nrm, src = _c(trinorm, (n, 3)), _c(source, (n, 3))
+    ssl = _c(sigma_sl, (-1, n, 3)) if sigma_sl is not None else None
+    sdl = _c(sigma_dl, (-1, n, 3)) if sigma_dl is not None else None
+    R = (ssl if ssl is not None else sdl).shape[0]
+    if out is None:
+        out = (np.zeros((R, n, 3)), np.zeros((R, n, 3, 3)))
+    pt, st = out
+    ws = wsave if wsave is not None else np.zeros(8)
+    p = lambda a: a.ctypes.data_as(_dp) if a is not None else None
+    ier = L.elhfmm3dtria_batch_host(int(iprec), float(rlam), float(rmu), n, p(tri), p(nrm), p(src), R, p(ssl),
+                                    p(sdl), p(pt), p(st), int(precision), int(icomp_type), p(ws), len(ws))
+    return ier, pt, st
 
 
 def elhfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, target=None,

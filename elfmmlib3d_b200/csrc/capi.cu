@@ -863,8 +863,174 @@ extern "C" void elhfmm3dtria_total_(int* ier, const int* iprec, const double* rl
                        *ifstraintarg, straintarg);
 }
 
+// ---------------------------------------------------------------------------
+// Half-space self-evaluation of many right-hand sides from host arrays (no
+// counterpart in the reference: its multi-slip use is a loop of
+// elfmm3dtriatargiter + elhfmm3dtriatargiter call pairs, icomp_type 2 then 3,
+// examples/elhfmm3dtria_self_iter_dr.f:222-385).  One slot holds the two
+// plans (direct arrival on the centroids; image part on the reflected
+// centroids, Mindlin root) and their device buffers; icomp_type 2 stores both
+// near fields behind an 8-word handle in wsave, 3 replays them with new
+// densities, each plan's pass replayed as one CUDA graph (nrhs <= 64).  One
+// store is live at a time: a new store invalidates the previous handle.
+// ---------------------------------------------------------------------------
+namespace {
+__global__ void k_add_into(size_t n, double* __restrict__ a, const double* __restrict__ b) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    a[i] += b[i];
+}
+
+constexpr double HSB_MAGIC = 1162626642.0;  // "ELFR"
+
+struct HsBatchSlot {
+  efmm_plan* f = nullptr;
+  efmm_plan* img = nullptr;
+  DevBuf<double> tri, nrm, src, refl, ssl, sdl, uf, ef, ui, ei;
+  long long id = 0;
+  int n = 0, R = 0, iprec = 0, precision = 0, flags = 0;
+  double checksum = 0;
+};
+HsBatchSlot* g_hsb = nullptr;
+long long g_hsb_next = 1;
+
+int hs_batch_host(int iprec, double rlam, double rmu, int n, const double* tri, const double* nrm,
+                  const double* src, int R, const double* ssl, const double* sdl, double* u, double* e,
+                  int precision, int icomp, double* wsave, int lwsave) {
+  if (n < 1 || R < 1 || (!ssl && !sdl) || (!u && !e)) return IER_BADARG;
+  if (iprec < -2 || iprec > 6 || precision < 0 || precision > 1) return IER_BADARG;
+  if (icomp < 1 || icomp > 3) return IER_BADARG;
+  if (icomp != 1 && (!wsave || lwsave < ITER_LUSED)) return IER_BADARG;
+  for (int i = 0; i < 3 * n; i++)
+    if (tri[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < n; i++)
+    if (src[3 * i + 2] > 0.0) return IER_BADARG;
+  std::lock_guard<std::mutex> lk(g_mu);
+  const int flags = (ssl ? 1 : 0) | (sdl ? 2 : 0) | (u ? 4 : 0) | (e ? 8 : 0) | (precision << 4);
+  const double cks = geometry_checksum(tri, nrm, src, n, nullptr, 0);
+  if (icomp == 3) {
+    const HsBatchSlot* S = g_hsb;
+    if (!S || S->id == 0 || wsave[0] != HSB_MAGIC || wsave[1] != ITER_VERSION || wsave[2] != (double)S->id ||
+        S->n != n || S->R != R || S->iprec != iprec || S->checksum != cks || S->flags != flags ||
+        wsave[3] != n || wsave[4] != R || wsave[5] != iprec || wsave[6] != cks || wsave[7] != flags)
+      return IER_HANDLE;
+  }
+  if (!g_hsb) {
+    HsBatchSlot* S = new HsBatchSlot();
+    S->f = efmm_plan_create(env_device());
+    S->img = efmm_plan_create(env_device());
+    if (!S->f || !S->img) {
+      efmm_plan_destroy(S->f);
+      efmm_plan_destroy(S->img);
+      delete S;
+      return IER_NODEVICE;
+    }
+    g_hsb = S;
+  }
+  HsBatchSlot& S = *g_hsb;
+  if (icomp != 3) S.id = 0;  // invalid until this store completes
+  try {
+    cudaSetDevice(S.f->device);
+    cudaStream_t st = S.f->stream;
+    const size_t N3 = 3 * (size_t)n * R, N9 = 9 * (size_t)n * R;
+    if (icomp != 3) {
+      std::vector<double> refl(src, src + 3 * (size_t)n);
+      for (int i = 0; i < n; i++) refl[3 * i + 2] = -refl[3 * i + 2];
+      up(S.tri, tri, 9 * (size_t)n, st);
+      up(S.nrm, nrm, 3 * (size_t)n, st);
+      up(S.src, src, 3 * (size_t)n, st);
+      up(S.refl, refl.data(), 3 * (size_t)n, st);
+      EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+      const bool iter = icomp == 2;
+      int ier = S.f->plan->set_geometry(n, S.tri.get(), S.nrm.get(), S.src.get(), 0, nullptr, iprec, iter, false);
+      if (ier) return ier;
+      ier = S.img->plan->set_geometry(n, S.tri.get(), S.nrm.get(), S.src.get(), n, S.refl.get(), iprec, iter, true);
+      if (ier) return ier;
+      S.uf.resize(N3);
+      S.ef.resize(N9);
+      S.ui.resize(N3);
+      S.ei.resize(N9);
+    }
+    if (ssl) up(S.ssl, ssl, N3, st);
+    if (sdl) up(S.sdl, sdl, N3, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    const double* dssl = ssl ? S.ssl.get() : nullptr;
+    const double* dsdl = sdl ? S.sdl.get() : nullptr;
+    double* duf = S.uf.get();  // the image pass needs the displacement buffer for strain-only calls too
+    double* def = e ? S.ef.get() : nullptr;
+    double* dui = S.ui.get();
+    double* dei = e ? S.ei.get() : nullptr;
+    const int mode = icomp == 1 ? 0 : (icomp == 2 ? 1 : 2);
+    int ier;
+    if (mode == 2 && R <= 64) {
+      ier = S.f->plan->evaluate_batch_graph(rlam, rmu, R, dssl, dsdl, duf, def, nullptr, nullptr, precision, 2);
+      if (!ier) ier = S.img->plan->evaluate_image_graph(rlam, rmu, R, dssl, dsdl, dui, dei, precision);
+    } else {
+      ier = S.f->plan->evaluate_batch(rlam, rmu, R, dssl, dsdl, duf, def, nullptr, nullptr, precision, mode);
+      if (!ier) ier = S.img->plan->evaluate_image(rlam, rmu, R, dssl, dsdl, dui, dei, precision, mode);
+    }
+    if (ier) return ier;
+    EFMM_CUDA_TRY(cudaStreamSynchronize(S.img->stream));
+    if (u) {
+      k_add_into<<<592, 256, 0, st>>>(N3, duf, dui);
+      count_launch();
+      down(u, S.uf, N3, st);
+    }
+    if (e) {
+      k_add_into<<<592, 256, 0, st>>>(N9, def, dei);
+      count_launch();
+      down(e, S.ef, N9, st);
+    }
+    EFMM_CUDA_TRY(cudaGetLastError());
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (icomp == 2) {
+      S.id = g_hsb_next++;
+      S.n = n;
+      S.R = R;
+      S.iprec = iprec;
+      S.precision = precision;
+      S.checksum = cks;
+      S.flags = flags;
+      wsave[0] = HSB_MAGIC;
+      wsave[1] = ITER_VERSION;
+      wsave[2] = (double)S.id;
+      wsave[3] = n;
+      wsave[4] = R;
+      wsave[5] = iprec;
+      wsave[6] = cks;
+      wsave[7] = flags;
+    }
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+}  // namespace
+
+extern "C" int elhfmm3dtria_batch_host(int iprec, double rlam, double rmu, int n, const double* triangle,
+                                       const double* trinorm, const double* source, int nrhs,
+                                       const double* sigma_sl, const double* sigma_dl, double* ptfrc,
+                                       double* strain, int precision, int icomp_type, double* wsave,
+                                       int lwsave) {
+  return hs_batch_host(iprec, rlam, rmu, n, triangle, trinorm, source, nrhs, sigma_sl, sigma_dl, ptfrc, strain,
+                       precision, icomp_type, wsave, lwsave);
+}
+
 extern "C" int efmm_iter_release(const double* wsave, int lwsave) {
   std::lock_guard<std::mutex> lk(g_mu);
+  if (wsave && lwsave >= ITER_LUSED && wsave[0] == HSB_MAGIC) {  // an elhfmm3dtria_batch_host store
+    if (!g_hsb || g_hsb->id == 0 || wsave[2] != (double)g_hsb->id) return IER_HANDLE;
+    HsBatchSlot* S = g_hsb;
+    g_hsb = nullptr;
+    cudaSetDevice(S->f->device);
+    efmm_plan* f = S->f;
+    efmm_plan* img = S->img;
+    delete S;  // frees the slot's device buffers
+    efmm_plan_destroy(f);
+    efmm_plan_destroy(img);
+    return IER_OK;
+  }
   IterSlot* S = iter_find(wsave, lwsave);
   if (!S) return IER_HANDLE;
   for (size_t i = 0; i < g_iter.size(); i++)

@@ -99,6 +99,26 @@ int efmm_batch_host(int iprec, double rlam, double rmu, int n, const double *tri
                     int nrhs, const double *sigma_sl, const double *sigma_dl, double *ptfrc,
                     double *strain, double *ptfrctarg, double *straintarg, int precision);
 
+/* Half-space self-evaluation of nrhs right-hand sides from host arrays (no
+ * single counterpart in the reference: it replaces the loop of
+ * elfmm3dtriatargiter + elhfmm3dtriatargiter call pairs over slip vectors,
+ * icomp_type 2 then 3, and the drivers' sum of direct arrival and image,
+ * examples/elhfmm3dtria_self_iter_dr.f:222-385).  Geometry as in
+ * elfmm3dtria_ (z <= 0), sigma_sl/sigma_dl (3,n,nrhs) column-major (NULL
+ * disables a layer); outputs the total displacement ptfrc (3,n,nrhs) and
+ * strain (3,3,n,nrhs) at the centroids (NULL disables one).  precision 0
+ * FP64, 1 mixed.  icomp_type 1 evaluates; 2 evaluates and stores both near
+ * fields on the device behind the 8-word handle in wsave (lwsave >= 8);
+ * 3 replays them with new densities (same geometry, iprec, nrhs, precision,
+ * layers and outputs, else 512), each of the two passes replayed as one
+ * CUDA graph for nrhs <= 64.  One store is live at a time: a new store
+ * invalidates the previous handle.  Blocking; returns ier. */
+int elhfmm3dtria_batch_host(int iprec, double rlam, double rmu, int n, const double *triangle,
+                            const double *trinorm, const double *source, int nrhs,
+                            const double *sigma_sl, const double *sigma_dl, double *ptfrc,
+                            double *strain, int precision, int icomp_type, double *wsave,
+                            int lwsave);
+
 /* Replaces elhfmm3dtriatargiter (src/elhfmm3dtria_iter.f:46-51): the image
  * part of the half-space (z <= 0, traction-free surface z = 0) single and
  * double layer potentials at targets, Mindlin's solution (the direct
@@ -136,8 +156,9 @@ void elhfmm3dtria_total_(int *ier, const int *iprec, const double *rlam, const d
                          double *straintarg);
 
 /* Frees the device store named by an ITER handle (no counterpart in the
- * reference, whose store is the caller's wsave array).  512 if the handle
- * names no live store. */
+ * reference, whose store is the caller's wsave array), including the two
+ * plans of an elhfmm3dtria_batch_host store.  512 if the handle names no
+ * live store. */
 int efmm_iter_release(const double *wsave, int lwsave);
 
 /* Device bytes held by the store an ITER handle names; -1 if none. */

@@ -10,9 +10,17 @@
   golden_fault100.npz oracle direct sum on a flat 10x5 fault (100 triangles,
                       coplanar neighbours, targets collinear with edges) + 20
                       targets.
+  golden_c1_sphere5120.npz  the free-space configuration at its own size:
+                      icosphere level 4 (5,120 triangles), 1,000 targets
+                      uniform in [-2,2]^3 with |x| > 1.1, lambda = mu = 1,
+                      single and double layer N(0,1) (seed 1); the oracle
+                      direct sum at 256 sampled centroids and 256 sampled
+                      targets (the geometry is regenerated from
+                      elfmmlib3d_b200.geometry and checked by its SHA-256).
 
-Run from the repository root:  python tests/golden/make_golden.py
+Run from the repository root:  python tests/golden/make_golden.py [c1]
 """
+import hashlib
 import os
 import sys
 
@@ -61,6 +69,30 @@ def quad_tables(v, x0, y0, z0):
     return out
 
 
+def c1():
+    """Oracle direct sum on the free-space configuration (sphere 5,120 +
+    1,000 box targets) at sampled points.  The oracle evaluates a
+    contiguous range of centroids, so the triangles are permuted to put the
+    sampled ones first (the sum over triangles does not depend on their
+    order)."""
+    tri, nrm, cen = G.sphere_triangles(4)
+    tg = G.box_targets(1000, 2)
+    rng = np.random.default_rng(1)
+    ssl = rng.normal(size=cen.shape)
+    sdl = rng.normal(size=cen.shape)
+    pick = np.random.default_rng(11)
+    ic = np.sort(pick.choice(len(cen), 256, replace=False))
+    it = np.sort(pick.choice(len(tg), 256, replace=False))
+    order = np.concatenate([ic, np.setdiff1d(np.arange(len(cen)), ic)])
+    pt, st, _, _ = O.direct(1.0, 1.0, tri[order], cen[order], ssl[order], sdl[order], None,
+                            rows=(0, len(ic)), trows=(0, 0))
+    _, _, ptt, stt = O.direct(1.0, 1.0, tri, cen, ssl, sdl, tg[it], rows=(0, 0))
+    np.savez_compressed(os.path.join(OUT, "golden_c1_sphere5120.npz"), rlam=1.0, rmu=1.0, ssl=ssl, sdl=sdl,
+                        tgt=tg, idx_c=ic, idx_t=it, u_c=pt[:len(ic)], e_c=st[:len(ic)], u_t=ptt, e_t=stt,
+                        tri_sha256=hashlib.sha256(np.ascontiguousarray(tri).tobytes()).hexdigest())
+    print("c1", flush=True)
+
+
 def main():
     rot, v = O.frame(TRI)
     targets = np.array([TRI[0] + rot @ xl for xl in LOCAL_TARGETS])
@@ -96,4 +128,8 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["c1"]:
+        c1()
+    else:
+        main()
+        c1()

@@ -167,4 +167,6 @@ def test_image_fmm_matches_c_oracle(gpu, oracle):
     uo, eo = oracle.image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg[sub], level=-1)
     eu, ee = rel(u[0][sub], uo), rel(e[0][sub], eo)
     print(f"iprec 3 image FMM vs C oracle: u {eu:.2e}  strain {ee:.2e}")
-    assert eu < 5e-7 and ee < 5e-7
+    # the FMM's own error at iprec 3 (2e-11 displacement, 5e-10 strain against
+    # the direct image sum, which equals the oracle's sum to rounding)
+    assert eu < 1e-9 and ee < 2e-9

@@ -168,3 +168,30 @@ def test_rigid_body_identity_large(gpu):
     assert rel(ptt[:500], exact_in) < TOL[2] and rel(pt, exact_on) < TOL[2]
     assert np.linalg.norm(ptt[500:]) < TOL[2] * np.linalg.norm(exact_in)
     assert np.abs(pt - exact_on).max() < 1e-4 * np.linalg.norm(b)
+
+
+def _c1_inputs():
+    import hashlib
+    g = golden("golden_c1_sphere5120.npz")
+    tri, nrm, cen = G.sphere_triangles(4)
+    assert hashlib.sha256(np.ascontiguousarray(tri).tobytes()).hexdigest() == str(g["tri_sha256"])
+    return g, tri, nrm, cen
+
+
+def test_c1_sphere5120_matches_oracle_fixture(gpu):
+    """The free-space configuration at its own size (5,120 triangles, 1,000
+    targets, iprec 2) through elfmm3dtriatarg_ against the oracle's FP64
+    direct sum at 256 sampled centroids and 256 sampled targets; and the GPU
+    direct sum (el3dtriadirecttarg_) against the same fixture."""
+    g, tri, nrm, cen = _c1_inputs()
+    ic, it = g["idx_c"], g["idx_t"]
+    ier, pt, st, ptt, stt = gpu.elfmm3dtriatarg(2, 1.0, 1.0, tri, nrm, cen, g["ssl"], g["sdl"], g["tgt"])
+    assert ier == 0
+    eu, ee = rel(pt[ic], g["u_c"]), rel(st[ic], g["e_c"])
+    eut, eet = rel(ptt[it], g["u_t"]), rel(stt[it], g["e_t"])
+    print(f"C1 FMM vs oracle: u {eu:.2e} strain {ee:.2e} u_t {eut:.2e} strain_t {eet:.2e}")
+    assert eu < DISP * TOL[2] and eut < DISP * TOL[2]
+    assert ee < 10 * TOL[2] and eet < 10 * TOL[2]
+    d = gpu.el3dtriadirecttarg(1.0, 1.0, tri, nrm, cen, g["ssl"], g["sdl"], g["tgt"])
+    assert rel(d[0][ic], g["u_c"]) < 1e-12 and rel(d[1][ic], g["e_c"]) < 1e-12
+    assert rel(d[2][it], g["u_t"]) < 1e-12 and rel(d[3][it], g["e_t"]) < 1e-12

@@ -88,3 +88,16 @@ def test_tree_invariants(oracle, mindlin):
             assert b + 1 in T.lists[4][j - 1].tolist()
     if mindlin:
         assert T.center[2] == 0.0
+
+
+def test_c1_fixture_geometry_regenerates():
+    """The C1 fixture stores the densities and targets; its triangles are
+    regenerated from the package's icosphere and checked by hash."""
+    import hashlib
+    from elfmmlib3d_b200 import geometry as G
+    from conftest import golden
+    g = golden("golden_c1_sphere5120.npz")
+    tri, nrm, cen = G.sphere_triangles(4)
+    assert hashlib.sha256(np.ascontiguousarray(tri).tobytes()).hexdigest() == str(g["tri_sha256"])
+    assert g["u_c"].shape == (256, 3) and g["e_t"].shape == (256, 3, 3)
+    assert np.all(np.linalg.norm(g["tgt"], axis=1) > 1.1)
