@@ -51,8 +51,11 @@ call sequences), host copies included.
 --impl reference times the CPU stand-in for the reference (the oracle's direct
 restatement of el3dtriadirecttarg; the Fortran reference cannot be compiled on
 this image) on a bounded sample of evaluation points, all host cores.
-Multi-GPU (torchrun): independent replicas, one per rank, no collectives on the
-data path; value = total evaluations / max-over-ranks time.
+Multi-GPU (torchrun, elfmmlib3d_b200.partition): the batched workloads split
+nrhs x N right-hand-side columns on one geometry into contiguous blocks, the
+uneven batch assigns nprob x N problems by a greedy n^2 balance, the
+single-problem workloads run one replica per rank; no collective on the data
+path; value = total evaluations / max-over-ranks time.
 """
 import argparse
 import json
@@ -88,13 +91,24 @@ WORKLOADS = {
 }
 
 
-def make_fault(name, seed=1):
+def make_fault(name, seed=1, cols=None):
+    """The fault of a batched workload and its slip right-hand sides: column
+    r (global index) is N(0,1) from seed 1000 seed + r; `cols` = [start,
+    stop) of the global columns this rank holds (default all of nrhs)."""
     from elfmmlib3d_b200 import geometry as G
     w = WORKLOADS[name]
     tri, nrm, cen, _ = G.planar_fault(w["nl"], w["nw"])
-    R = w["nrhs"]
-    sdl = np.stack([np.random.default_rng(seed * 1000 + r).normal(size=cen.shape) for r in range(R)])
+    a, b = cols if cols is not None else (0, w["nrhs"])
+    sdl = np.stack([np.random.default_rng(seed * 1000 + r).normal(size=cen.shape) for r in range(a, b)])
     return tri, nrm, cen, sdl, w["iprec"]
+
+
+def rank_columns(name, world, rank):
+    """This rank's block of the job's right-hand-side columns: the job is
+    nrhs x world columns on one geometry, split into contiguous blocks
+    (elfmmlib3d_b200.partition.rhs_columns), nrhs per rank."""
+    from elfmmlib3d_b200.partition import rhs_columns
+    return rhs_columns(WORKLOADS[name]["nrhs"] * world, world, rank)
 
 
 def make_inputs(name, seed=1):
@@ -324,17 +338,26 @@ def oracle_errors(ref, u=None, e=None, ut=None, et=None):
     return out
 
 
-def make_uneven_problems(w, rank=0):
-    """The uneven batch: w["nprob"] half-space faults, strike U[0, 360),
-    dip U[15, 90], top depth U[0.5, 5], triangle count log-uniform in
-    [nmin, nmax], one slip vector N(0,1) per triangle (double layer)."""
+def make_uneven_problems(w, world=1, rank=None):
+    """The uneven batch: w["nprob"] x world half-space faults, strike
+    U[0, 360), dip U[15, 90], top depth U[0.5, 5], triangle count
+    log-uniform in [nmin, nmax], one slip vector N(0,1) per triangle (double
+    layer).  rank given: only the problems that the greedy n^2 balance
+    (elfmmlib3d_b200.partition.balance_problems) assigns to that rank."""
     from elfmmlib3d_b200.batch import fault_problem
-    rng = np.random.default_rng(7 + rank)
-    probs = []
-    for i in range(w["nprob"]):
+    from elfmmlib3d_b200.partition import balance_problems
+    rng = np.random.default_rng(7)
+    spec = []
+    for i in range(w["nprob"] * world):
         ntri = int(np.exp(rng.uniform(np.log(w["nmin"]), np.log(w["nmax"]))))
-        tri, nrm, cen, slip = fault_problem(ntri, rng.uniform(0.0, 360.0), rng.uniform(15.0, 90.0),
-                                            rng.uniform(0.5, 5.0), seed=100000 * rank + i)
+        spec.append((ntri, rng.uniform(0.0, 360.0), rng.uniform(15.0, 90.0), rng.uniform(0.5, 5.0)))
+    mine = range(len(spec))
+    if rank is not None:
+        mine = balance_problems([float(s_[0]) ** 2 for s_ in spec], world)[rank]
+    probs = []
+    for i in mine:
+        ntri, strike, dip, depth = spec[i]
+        tri, nrm, cen, slip = fault_problem(ntri, strike, dip, depth, seed=i)
         probs.append((tri, nrm, cen, None, slip))
     return probs
 
@@ -607,7 +630,8 @@ def run_batch(args, rank, world, local_rank):
     import elfmmlib3d_b200 as E
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    tri, nrm, cen, sdl, iprec = make_fault(args.workload, seed=1 + rank)
+    cols = rank_columns(args.workload, world, rank)
+    tri, nrm, cen, sdl, iprec = make_fault(args.workload, cols=cols)
     R, n = sdl.shape[0], len(cen)
     evals = n * n * R
 
@@ -729,7 +753,10 @@ def run_batch(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": args.workload, "triangles": n, "rhs": R, "targets": 0, "iprec": iprec,
-                   "green": "free space", "evals_per_step": evals, "parallelism": f"replicas{world}",
+                   "green": "free space", "evals_per_step": evals,
+                   "parallelism": (f"rhs-columns{world}: {R * world} right-hand sides on one geometry, columns "
+                                   f"{cols[0]}..{cols[1] - 1} on rank {rank}, geometry and plans replicated, no "
+                                   "exchange") if world > 1 else "1 GPU",
                    "l2_policy": "expansions (2 x 3.5 GB FP32) and pair data > L2 (126 MB)",
                    "forms": {"mixed_batched": value / world, "batched_fp64": b64_value,
                              "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
@@ -763,7 +790,8 @@ def run_hsbatch(args, rank, world, local_rank):
     import elfmmlib3d_b200 as E
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
-    tri, nrm, cen, sdl, iprec = make_fault(args.workload, seed=1 + rank)
+    cols = rank_columns(args.workload, world, rank)
+    tri, nrm, cen, sdl, iprec = make_fault(args.workload, cols=cols)
     R, n = sdl.shape[0], len(cen)
     evals = n * n * R
 
@@ -995,7 +1023,9 @@ def run_hsbatch(args, rank, world, local_rank):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": args.workload, "triangles": n, "rhs": R, "targets": "centroids", "iprec": iprec,
                    "green": "Mindlin half space (free space + image)", "evals_per_step": evals,
-                   "parallelism": f"replicas{world}",
+                   "parallelism": (f"rhs-columns{world}: {R * world} right-hand sides on one geometry, columns "
+                                   f"{cols[0]}..{cols[1] - 1} on rank {rank}, geometry, plans and stored near "
+                                   "fields replicated, no exchange") if world > 1 else "1 GPU",
                    "l2_policy": "expansions (FP32, several GB) and stored near field (~49 GB) > L2 (126 MB)",
                    "step": "free-space batch + image batch, near fields replayed (stored on the first call, "
                            f"{store_s * 1e3:.0f} ms, untimed), "
@@ -1393,7 +1423,7 @@ def run_uneven(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     w = WORKLOADS[args.workload]
-    probs = make_uneven_problems(w, rank)
+    probs = make_uneven_problems(w, world, rank)
     sizes = np.array([len(p[2]) for p in probs])
     evals = float(np.sum(sizes.astype(np.float64) ** 2))
     workers = 4
@@ -1448,7 +1478,8 @@ def run_uneven(args, rank, world, local_rank):
                                          "strain_median": float(np.median(errs[:, 1]))},
                    "rel_err_vs_oracle": oerr,
                    "rel_err_vs_oracle_sample": "per sampled problem, the cpu_baseline sample's centroids",
-                   "parallelism": f"replicas{world}"},
+                   "parallelism": (f"problems{world}: {w['nprob']} x {world} problems, greedy n^2 balance "
+                                   "across ranks, no exchange") if world > 1 else "1 GPU"},
         "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": int(sizes.sum() * 8 * (9 + 3 + 3 + 3)),
                 "d2h_bytes_per_step": int(sizes.sum() * 8 * 12),
                 "timing": "host wall clock: geometry and slip vectors from host memory, results back, every "
