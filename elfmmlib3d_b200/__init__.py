@@ -52,7 +52,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_evaluate_direct_subset", "efmm_batch_host", "efmm_factored_selfcheck",
            "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_",
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
-           "efmm_pair_eval_host", "elhfmm3dtria_batch_host"]
+           "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
+           "efmm_tri_refine", "efmm_tri_build"]
 
 
 class ElfmmError(RuntimeError):
@@ -129,6 +130,14 @@ def load():
     L.elhfmm3dtria_batch_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp,
                                           _dp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp,
                                           ctypes.c_int]
+    L.efmm_tri_read.restype = ctypes.c_int
+    L.efmm_tri_read.argtypes = [ctypes.c_char_p, _dp, ctypes.c_int, _ip, _ip, ctypes.c_int, _ip]
+    L.efmm_tri_write.restype = ctypes.c_int
+    L.efmm_tri_write.argtypes = [ctypes.c_char_p, _dp, ctypes.c_int, _ip, ctypes.c_int]
+    L.efmm_tri_refine.restype = ctypes.c_int
+    L.efmm_tri_refine.argtypes = [_dp, ctypes.c_int, _ip, ctypes.c_int, _dp, _ip]
+    L.efmm_tri_build.restype = ctypes.c_int
+    L.efmm_tri_build.argtypes = [_dp, ctypes.c_int, ctypes.c_int, _ip, _dp, _dp, _dp, _dp]
     L.efmm_iter_release.restype = ctypes.c_int
     L.efmm_iter_release.argtypes = [_dp, ctypes.c_int]
     L.efmm_iter_stored_bytes.restype = ctypes.c_longlong
@@ -284,6 +293,68 @@ def hs_batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, si
     ier = L.elhfmm3dtria_batch_host(int(iprec), float(rlam), float(rmu), n, p(tri), p(nrm), p(src), R, p(ssl),
                                     p(sdl), p(pt), p(st), int(precision), int(icomp_type), p(ws), len(ws))
     return ier, pt, st
+
+
+def read_tri(path):
+    """Read a Cart3D .tri file (efmm_tri_read, the reference's atrireadchk,
+    src/trilib.f:59).  Returns (verts (nverts,3) float64, ifaces (nfaces,3)
+    int32, 1-based as in the file).  Raises OSError / ValueError."""
+    L = load()
+    nv, nf = ctypes.c_int(0), ctypes.c_int(0)
+    b = os.fsencode(path)
+    ier = L.efmm_tri_read(b, None, 0, ctypes.byref(nv), None, 0, ctypes.byref(nf))
+    if ier == 1:
+        raise OSError(f"read_tri: cannot open {path}")
+    if ier not in (0, 2, 3) or (ier == 0 and (nv.value or nf.value)):
+        raise ValueError(f"read_tri: malformed file {path} (ier={ier})")
+    verts = np.zeros((max(nv.value, 1), 3))
+    ifaces = np.zeros((max(nf.value, 1), 3), dtype=np.int32)
+    ier = L.efmm_tri_read(b, verts.ctypes.data_as(_dp), nv.value, ctypes.byref(nv),
+                          ifaces.ctypes.data_as(_ip), nf.value, ctypes.byref(nf))
+    if ier:
+        raise ValueError(f"read_tri: malformed file {path} (ier={ier})")
+    return verts[:nv.value], ifaces[:nf.value]
+
+
+def write_tri(path, verts, ifaces):
+    """Write a Cart3D .tri file (efmm_tri_write, the reference's atriwrite);
+    ifaces 1-based."""
+    v = _c(verts, (-1, 3))
+    f = np.ascontiguousarray(ifaces, dtype=np.int32).reshape(-1, 3)
+    ier = load().efmm_tri_write(os.fsencode(path), v.ctypes.data_as(_dp), v.shape[0], f.ctypes.data_as(_ip),
+                                f.shape[0])
+    if ier:
+        raise OSError(f"write_tri: cannot write {path} (ier={ier})")
+
+
+def refine_tri(verts, ifaces):
+    """Split every face in four at its edge midpoints (efmm_tri_refine, the
+    reference's matlab/atrirefine.m).  Returns (verts1, ifaces1)."""
+    v = _c(verts, (-1, 3))
+    f = np.ascontiguousarray(ifaces, dtype=np.int32).reshape(-1, 3)
+    nv, nf = v.shape[0], f.shape[0]
+    v1 = np.zeros((nv + 3 * nf, 3))
+    f1 = np.zeros((4 * nf, 3), dtype=np.int32)
+    ier = load().efmm_tri_refine(v.ctypes.data_as(_dp), nv, f.ctypes.data_as(_ip), nf, v1.ctypes.data_as(_dp),
+                                 f1.ctypes.data_as(_ip))
+    if ier:
+        raise ValueError(f"refine_tri: face index outside 1..{nv}")
+    return v1, f1
+
+
+def build_tri(verts, ifaces):
+    """Triangle arrays from vertex arrays (efmm_tri_build, the reference's
+    buildtri, src/trilib.f:192).  Returns (triangle (n,3,3), centroids (n,3),
+    trinorm (n,3), triarea (n,)): the arguments the FMM entry points take."""
+    v = _c(verts, (-1, 3))
+    f = np.ascontiguousarray(ifaces, dtype=np.int32).reshape(-1, 3)
+    n = f.shape[0]
+    tri, cen, nrm, area = np.zeros((n, 3, 3)), np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n)
+    ier = load().efmm_tri_build(v.ctypes.data_as(_dp), v.shape[0], n, f.ctypes.data_as(_ip), tri.ctypes.data_as(_dp),
+                                cen.ctypes.data_as(_dp), nrm.ctypes.data_as(_dp), area.ctypes.data_as(_dp))
+    if ier:
+        raise ValueError(f"build_tri: face index outside 1..{v.shape[0]}")
+    return tri, cen, nrm, area
 
 
 def elhfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, target=None,

@@ -395,6 +395,39 @@ void efmm_plan_info(const efmm_plan *plan, long long *info8);
 int efmm_plan_tree_export(const efmm_plan *plan, int *boxes, int *iz, int *iztarg, int *laddr,
                           double *center_size4, int *lstart, int *litems, long long *lcount5);
 
+/* ---- flat-triangle geometry I/O (host code) ----------------------------
+ * The Cart3D ".tri" format: "nverts nfaces", nverts vertices (3 reals),
+ * nfaces vertex-index triples (1-based), free format.  Arrays in the
+ * reference's layout: verts(3,nverts), ifaces(3,nfaces). */
+
+/* Replaces atrireadchk (src/trilib.f:59-88), which reads from a Fortran
+ * unit; here from a file name.  Reads the sizes into *nverts / *nfaces, then
+ * the arrays if they fit: ier 0 ok, 1 the file cannot be opened, 2 lv <
+ * nverts, 3 li < nfaces (the reference's codes; lv = li = 0 asks for the
+ * sizes), 4 malformed file (not a number, index outside 1..nverts). */
+int efmm_tri_read(const char *path, double *verts, int lv, int *nverts, int *ifaces, int li, int *nfaces);
+
+/* Replaces atriwrite (src/trilib.f:113-128): writes the file (vertices
+ * with 17 significant digits, so they read back bit for bit).  ier 0 / 1. */
+int efmm_tri_write(const char *path, const double *verts, int nverts, const int *ifaces, int nfaces);
+
+/* Replaces matlab/atrirefine.m: every face split into four at its edge
+ * midpoints.  verts1 (3, nverts + 3 nfaces): the vertices, then the
+ * midpoints of edges 1-2, 2-3, 3-1 of each face (three blocks in face order,
+ * shared edges not merged); ifaces1 (3, 4 nfaces): the corner triangles of
+ * vertex 1, 2, 3 of each face, then the middle triangles (four blocks).
+ * ier 16 on an index outside 1..nverts. */
+int efmm_tri_refine(const double *verts, int nverts, const int *ifaces, int nfaces, double *verts1,
+                    int *ifaces1);
+
+/* Replaces buildtri (src/trilib.f:192-240): triangle(3,3,ntri),
+ * centroids(3,ntri), unit normals trinorm(3,ntri) and areas triarea(ntri)
+ * (NULL skips one) from the vertex arrays; the normal and area formulas of
+ * triangle_norm / triangle_area (src/trilib.f:245-318).  ier 16 on an index
+ * outside 1..nverts. */
+int efmm_tri_build(const double *verts, int nverts, int ntri, const int *itrivert, double *triangle,
+                   double *centroids, double *trinorm, double *triarea);
+
 #ifdef __cplusplus
 }
 #endif
