@@ -640,10 +640,10 @@ void Plan::cut_rot_tasks(TransSched& S, int C, int W) {
 }
 
 // factored operators of the pool: host construction once per (device, p, eps)
-void Plan::ensure_factored() {
+void Plan::ensure_factored(bool tc) {
   std::lock_guard<std::mutex> lk(g_ops_mu);
   OpPool* P = ops_;
-  if (P->rot_ready) return;
+  if (P->rot_ready && (!tc || P->rot_tc_ready)) return;
   std::vector<int> kinds, orders;
   std::vector<double> offs;
   for (const OpDesc& d : P->descs) {
@@ -661,6 +661,16 @@ void Plan::ensure_factored() {
           std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
   std::vector<float> poolf;
   normalise_factored_ops(kinds, rops, pool, w, poolf);
+  if (tc && !P->rot_tc_ready) {
+    std::vector<RotTcOp> tops;
+    std::vector<float> tiles;
+    build_rot_tc_tiles(rops, poolf, tops, tiles);
+    h2d(P->rot_tc_ops, tops, st_);
+    h2d(P->rot_tc_tiles, tiles, st_);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+    P->rot_tc_ready = true;
+    if (P->rot_ready) return;
+  }
   // device layout: blocks column-major
   column_major_factored(rops, pool);
   {
@@ -675,9 +685,79 @@ void Plan::ensure_factored() {
   P->rot_ready = true;
 }
 
+// The tensor-core form serves the FP32 translations of pools of order <= 31
+// (blocks of at most 64 rows); ELFMM3D_ROT_TC=0 keeps them on the CUDA cores.
+bool Plan::rot_tc_usable() const {
+  static const bool on = [] {
+    const char* e = getenv("ELFMM3D_ROT_TC");
+    return !(e && e[0] == '0');
+  }();
+  return on && factored_ && tc_enabled() && p_ <= 31;
+}
+
+void Plan::cut_tc_tasks(TransSched& S, int C) {
+  if (S.tcC == C && S.tcpool == ops_) return;
+  // scratch budget per intermediate array (floats); a level whose columns
+  // need more runs as several batches
+  const long long budget = 1LL << 28;
+  std::vector<RotTcSeg> segs;
+  std::vector<RotTcTask> tasks;
+  S.tcb.clear();
+  for (auto& r : S.lev) {
+    long long ny = 0, nw = 0;
+    int t0 = (int)tasks.size();
+    for (int q = r.first; q < r.first + r.second; q++) {
+      const TransSeg& g = S.segs[q];
+      const int pg = ops_->descs[g.group].p;
+      const long long ncols = (long long)g.npair * C;
+      const long long sy = (long long)rot_tc_pad_rows(0, pg) * ncols, sw = (long long)rot_tc_pad_rows(1, pg) * ncols;
+      if ((ny + sy > budget || nw + sw > budget) && (int)tasks.size() > t0) {
+        S.tcb.push_back({t0, (int)tasks.size() - t0, ny, nw});
+        t0 = (int)tasks.size();
+        ny = nw = 0;
+      }
+      const int si = (int)segs.size();
+      segs.push_back({g.group, g.pair0, (int)ncols, 0, ny, nw});
+      for (long long c0 = 0; c0 < ncols; c0 += 128) tasks.push_back({si, (int)c0});
+      ny += sy;
+      nw += sw;
+    }
+    if ((int)tasks.size() > t0) S.tcb.push_back({t0, (int)tasks.size() - t0, ny, nw});
+  }
+  h2d(S.tcsegs, segs, st_);
+  h2d(S.tctasks, tasks, st_);
+  S.tcC = C;
+  S.tcpool = ops_;
+}
+
+void Plan::run_translations_tc(TransSched& S, int C, const float* src, float* dst) {
+  ensure_factored(true);
+  cut_tc_tasks(S, C);
+  long long ny = 0, nw = 0;
+  for (const auto& b : S.tcb) {
+    ny = std::max(ny, b.ny);
+    nw = std::max(nw, b.nw);
+  }
+  rot_y_.resize((size_t)std::max(ny, 1LL));  // grows only: no reallocation inside a captured pass
+  rot_w_.resize((size_t)std::max(nw, 1LL));
+  const int D = 2 * ncoef(p_);
+  int* err = tc_err_ptr();
+  for (const auto& b : S.tcb)
+    for (int stage = 0; stage < 3; stage++)
+      launch_rot_tc(st_, stage, b.ntask, S.tctasks.get() + b.task0, S.tcsegs.get(), S.pairs.get(),
+                    ops_->rot_tc_ops.get(), ops_->rot_tc_tiles.get(), D, C, src, rot_y_.get(), rot_w_.get(), dst,
+                    err);
+}
+
 template <class T>
 void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst) {
   int D = 2 * ncoef(p_);
+  if constexpr (sizeof(T) == 4) {
+    if (rot_tc_usable()) {
+      run_translations_tc(S, C, reinterpret_cast<const float*>(src), reinterpret_cast<float*>(dst));
+      return;
+    }
+  }
   // factored form when its column tiles fit in shared memory
   const int W = rot_cols_per_cta(D, (int)sizeof(T));
   const size_t smem = sizeof(T) * 2 * (size_t)D * W;

@@ -35,6 +35,11 @@ struct OpPool {
   DevBuf<RotOp> rot_ops;
   DevBuf<double> rot_d;
   DevBuf<float> rot_f;
+  // the FP32 factored operators as tensor-core tiles (orders <= 31); made on
+  // the first FP32 pass that uses them
+  bool rot_tc_ready = false;
+  DevBuf<RotTcOp> rot_tc_ops;
+  DevBuf<float> rot_tc_tiles;
   DevBuf<long long> off;
   DevBuf<int> dim;
   int m2l_group[343];
@@ -78,6 +83,18 @@ struct TransSched {
   DevBuf<TransTask> rtasks;
   std::vector<std::pair<int, int>> lev_rtasks;  // task ranges in execution order,
   std::vector<int> lev_rdim;                     // each with its largest operator size
+  // tensor-core form: segments with their intermediate bases, 128-column
+  // tasks, and per batch (levels split so that Y and W stay within budget)
+  // the task range and its Y / W extents (floats)
+  int tcC = -1;
+  const void* tcpool = nullptr;
+  DevBuf<RotTcSeg> tcsegs;
+  DevBuf<RotTcTask> tctasks;
+  struct TcBatch {
+    int task0, ntask;
+    long long ny, nw;
+  };
+  std::vector<TcBatch> tcb;
   void clear() {
     segs.clear();
     lev.clear();
@@ -87,6 +104,9 @@ struct TransSched {
     rC = rW = -1;
     lev_rtasks.clear();
     lev_rdim.clear();
+    tcC = -1;
+    tcpool = nullptr;
+    tcb.clear();
   }
 };
 
@@ -300,7 +320,12 @@ class Plan {
   TransSched m2m_, m2l_, l2l_;
   void cut_tasks(TransSched& S, int C, const std::vector<int>* dims = nullptr);
   void cut_rot_tasks(TransSched& S, int C, int W);
-  void ensure_factored();
+  void ensure_factored(bool tc = false);
+  // the FP32 translations of a schedule on the tensor cores (rot_tc.cu)
+  bool rot_tc_usable() const;
+  void cut_tc_tasks(TransSched& S, int C);
+  void run_translations_tc(TransSched& S, int C, const float* src, float* dst);
+  DevBuf<float> rot_y_, rot_w_;  // intermediates of the tensor-core translations
   bool factored_ = true;  // translations in factored form when they fit
   bool p2m_unit_ = true;  // batched P2M through unit-density multipoles (else node products)
   template <class T>

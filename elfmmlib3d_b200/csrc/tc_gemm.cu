@@ -27,6 +27,7 @@
 #include <cstdlib>
 #include "common.cuh"
 #include "fmm.h"
+#include "tc_common.cuh"
 
 namespace efmm {
 
@@ -41,69 +42,6 @@ template <int BN>
 __host__ __device__ constexpr int tc_smem() { return 2 * tc_stage_bytes<BN>() + 1024 + 64; }  // two stages, alignment, barriers
 // A and B (K-major): element (row, k) at (k % 4) * 4 + (row % 8) * 16 + (k / 4) * 128 + (row / 8) * 1024
 constexpr uint32_t TC_LBO = 128, TC_SBO = 1024;
-constexpr long long TC_WAIT_CYCLES = 4000000000LL;       // about 2 s at 2 GHz
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// no-swizzle shared-memory matrix descriptor (version 1)
-__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
-         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
-}
-
-// instruction descriptor: F32 accumulate, TF32 A and B (both K-major), M = 128, N = BN
-template <int BN>
-__host__ __device__ constexpr uint32_t tc_idesc() {
-  return (1u << 4) | (2u << 7) | (2u << 10) | (0u << 15) | (0u << 16) | ((uint32_t)(BN >> 3) << 17) |
-         ((uint32_t)(TC_BM >> 4) << 24);
-}
-
-__device__ __forceinline__ float tf32_head(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-
-// bounded wait for phase `parity` of the barrier; false when it ran out
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  const long long t0 = clock64();
-  while (!mbar_try(bar, parity))
-    if (clock64() - t0 > TC_WAIT_CYCLES) return false;
-  return true;
-}
-
-__device__ __forceinline__ void mma_tf32(uint32_t dtmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
-                                         uint32_t accum) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
-      ::"r"(dtmem), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
-      : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-               : "memory");
-}
 
 struct Quad {
   float v[4];
@@ -121,7 +59,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   constexpr int RG = BN / 8;       // 8-row groups of B
   constexpr int NB = BN / 32;      // B quads per thread and K tile
   constexpr int NHALF = BN / 2;    // accumulator columns drained per warp
-  constexpr uint32_t IDESC = tc_idesc<BN>();
+  constexpr uint32_t IDESC = tc_idesc_mn(TC_BM, BN);
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   // 1024-byte aligned operand region
   const uint32_t raw = smem_u32(tc_smem_raw);

@@ -395,6 +395,16 @@ void efmm_plan_info(const efmm_plan *plan, long long *info8);
 int efmm_plan_tree_export(const efmm_plan *plan, int *boxes, int *iz, int *iztarg, int *laddr,
                           double *center_size4, int *lstart, int *litems, long long *lcount5);
 
+/* Checks of the FP32 factored translations on the tensor cores (no
+ * counterpart in the reference): one M2L, one M2M and one L2L group of order
+ * p (1..31).  _selfcheck emulates the three stages on the host (tiles, their
+ * layout, the row maps between the stages, the 3-term split); _device runs
+ * them on the GPU for npair box pairs of C columns each.  Both return 0 and
+ * the relative l2 difference from the FP64 product of the same FP32
+ * operators in *rel (_device: *timeout != 0 if a bounded wait ran out). */
+int efmm_rot_tc_selfcheck(int p, unsigned seed, double *rel);
+int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double *rel, int *timeout);
+
 /* ---- flat-triangle geometry I/O (host code) ----------------------------
  * The Cart3D ".tri" format: "nverts nfaces", nverts vertices (3 reals),
  * nfaces vertex-index triples (1-based), free format.  Arrays in the
