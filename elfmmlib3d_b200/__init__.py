@@ -53,7 +53,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_plan_evaluate_iter", "efmm_plan_evaluate_batch_iter", "efmm_plan_evaluate_image", "efmm_plan_evaluate_batch_graph", "efmm_plan_evaluate_image_graph", "efmm_hs_image_direct", "efmm_u_m2l_selfcheck", "efmm_tc_gemm_selfcheck", "efmm_tc_gemm_selfcheck_tile", "efmm_plan_stored_bytes", "efmm_plan_set_mixed_floor", "efmm_plan_translation_flops", "elhfmm3dtriatargiter_",
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
-           "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device"]
+           "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
+           "efmm_hs_capped"]
 
 
 class ElfmmError(RuntimeError):
@@ -493,6 +494,14 @@ def elfmm3dtriaiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, 
     ier, lused, pt, st, _, _ = elfmm3dtriatargiter(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl,
                                                    sigma_dl, None, icomp_type, wsave, ifptfrc, ifstrain, 0, 0)
     return ier, lused, pt, st
+
+
+def hs_capped():
+    """Sub-triangles of the image quadrature kept at the adaptive depth cap
+    since the last call (and clears the count)."""
+    L = load()
+    L.efmm_hs_capped.restype = ctypes.c_int
+    return int(L.efmm_hs_capped())
 
 
 def iter_release(wsave):

@@ -465,8 +465,8 @@ int hs_call(int iprec, double rlam, double rmu, const double* tri, const double*
     B.u.resize(3 * (size_t)nt);
     B.e6.resize(6 * (size_t)nt);
     launch_hs_image(st, n, B.tri.get(), B.nrm.get(), ifsingle ? B.ssl.get() : nullptr,
-                    ifdouble ? B.sdl.get() : nullptr, nt, B.tgt.get(), rlam, rmu, B.work.get(), B.u.get(),
-                    B.e6.get());
+                    ifdouble ? B.sdl.get() : nullptr, nt, B.tgt.get(), rlam, rmu, hs_quad_eps(iprec), hs_ncap_ptr(),
+                    B.work.get(), B.u.get(), B.e6.get());
     std::vector<double> e6(6 * (size_t)nt);
     if (ifptfrctarg) down(ptfrctarg, B.u, 3 * (size_t)nt, st);
     if (ifstraintarg) down(e6.data(), B.e6, 6 * (size_t)nt, st);
@@ -488,6 +488,16 @@ int hs_call(int iprec, double rlam, double rmu, const double* tri, const double*
   }
 }
 }  // namespace
+
+// Sub-triangles of the image quadrature kept at the adaptive depth cap
+// without meeting the tolerance since the last call (on the current device).
+extern "C" int efmm_hs_capped(void) {
+  try {
+    return hs_take_ncap();
+  } catch (const efmm::CudaError&) {
+    return -1;
+  }
+}
 
 extern "C" int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double* tri, const double* nrm, int n,
                                     const double* ssl, const double* sdl, int nt, const double* tgt, double* u,

@@ -12,9 +12,14 @@ struct HsTri {
 // Image displacement u (m,3) and strain e6 (m,6: xx yy zz xy xz yz) at
 // targets tgt (m,3) of the single (ssl) and double (sdl, normals nrm)
 // layers on triangles tri (n,3,3); NULL disables a layer.  work: n records.
+// eps: relative tolerance of the adaptive integration of near-singular
+// sub-triangles (hs_quad_eps); *ncap (may be null) counts sub-triangles kept
+// at the depth cap without meeting it.
 void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nrm, const double* ssl,
-                     const double* sdl, int m, const double* tgt, double lam, double mu, HsTri* work, double* u,
-                     double* e6);
+                     const double* sdl, int m, const double* tgt, double lam, double mu, double eps, int* ncap,
+                     HsTri* work, double* u, double* e6);
+// tolerance of the image quadrature for iprec: min(1e-6, eps(iprec) / 10)
+double hs_quad_eps(int iprec);
 
 // Near field of the image FMM: the unit-density image responses of every
 // (target, near triangle) pair of each near leaf, written in the stored
@@ -31,7 +36,14 @@ struct HsStoreArgs {
   const int* ntri;
   int dosl, dodl, dstr, K;
   double lam, mu;
+  double eps = 1e-6;     // adaptive tolerance of near-singular sub-triangles
+  int* ncap = nullptr;   // sub-triangles kept at the depth cap (counter, may be null)
 };
+// The per-device counter of sub-triangles kept at the adaptive depth cap
+// (device address, for HsStoreArgs::ncap and launch_hs_image), and its value
+// read and cleared (blocking).
+int* hs_ncap_ptr();
+int hs_take_ncap();
 // One CTA per chunk of (near leaf, first of 8 targets).
 void launch_hs_store(cudaStream_t st, const HsStoreArgs& a, int nchunk, const int* chunk_leaf,
                      const int* chunk_e0, double* store);

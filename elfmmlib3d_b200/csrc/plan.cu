@@ -2243,6 +2243,8 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     ha.base = near_base_.get(); ha.ntri = near_ntri_.get();
     ha.dosl = dosl; ha.dodl = dodl; ha.dstr = dstr; ha.K = store_K_;
     ha.lam = rlam; ha.mu = rmu;
+    ha.eps = hs_quad_eps(iprec_);
+    ha.ncap = hs_ncap_ptr();
     launch_hs_store(st_, ha, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), store_.get());
     store_valid_ = true;
     store_gen_++;

@@ -239,11 +239,21 @@ int efmm_plan_evaluate_image(efmm_plan *plan, double rlam, double rmu, int nrhs,
                              const double *sdl, double *u_tgt, double *e_tgt, int precision, int mode);
 
 /* The image part by direct summation over all (target, triangle) pairs with
- * the refined quadrature of the image near field (host arrays as in
+ * the quadrature of the image near field (host arrays as in
  * elhfmm3dtriatargiter; u (nt,3), e (nt,3,3), NULL skips an output): the
- * O(n nt) check of the image FMM. */
+ * O(n nt) check of the image FMM.  The quadrature refines sub-triangles by
+ * distance to the reflected target and integrates the near-singular ones
+ * adaptively to relative tolerance min(1e-6, eps(iprec) / 10), the scheme
+ * of tria3adam (src/tria3adamar.f:33-395), with a depth cap. */
 int efmm_hs_image_direct(int iprec, double rlam, double rmu, const double *tri, const double *nrm, int n,
                          const double *ssl, const double *sdl, int nt, const double *tgt, double *u, double *e);
+
+/* Sub-triangles of the image quadrature (direct sum or image near-field
+ * store) kept at the adaptive depth cap without meeting the tolerance since
+ * the last call, on the current device (the reference reports the same
+ * event as ier 4 of tria3adam, src/tria3adamar.f:65-67); clears the count.
+ * -1 on a CUDA error. */
+int efmm_hs_capped(void);
 
 /* Host check (no GPU) of the image FMM's M2L for the kernel
  * U = z log(r + z) - r (src/mindlinpieces.f:29): order-p local expansion at

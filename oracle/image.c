@@ -16,11 +16,17 @@
  *   level >= 0  every triangle split into 4**level congruent sub-triangles
  *               (the numpy oracle mindlin.image_direct: the same sums, in
  *               another rounding order);
- *   level <  0  adaptive: a sub-triangle is split in four until the reflected
- *               target lies farther than 8 diameters from its centroid, at
- *               most 8 times.
+ *   level <  0  refined by distance: a sub-triangle is split in four until
+ *               the reflected target lies farther than 8 diameters from its
+ *               centroid, at most 8 times.
+ * and oracle_image_direct_adaptive integrates each pair and layer by the
+ * adaptive scheme of the reference's tria3adam (src/tria3adamar.f:33-395):
+ * the rule on a sub-triangle against the sum of the rule on its four
+ * children, a sub-triangle accepted when every output agrees to eps times
+ * the largest output of the parent estimate, depth-first with a depth cap.
  */
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "image_gen.h"
@@ -163,5 +169,122 @@ int oracle_image_kernel(int layer, double lam, double mu, const double* x, const
     oracle_image_dl(lam, mu, x[0], x[1], x[2], s[0], s[1], s[2], nrm[0], nrm[1], nrm[2], out);
   else
     return 4;
+  return 0;
+}
+
+/* the 12-node rule on sub-triangle (a, b, c) of one layer (0 force sl, 1
+ * jump dl with normal nrm): out[9] = displacement (3), strain (6) */
+static void image_rule(double lam, double mu, int layer, const double* nrm, const double* den, const double X[3],
+                       const double* a, const double* b, const double* c, double B[12][3], const double W[12],
+                       double out[9]) {
+  const double u[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]};
+  const double v[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+  const double cr[3] = {u[1] * v[2] - u[2] * v[1], u[2] * v[0] - u[0] * v[2], u[0] * v[1] - u[1] * v[0]};
+  const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+  for (int r = 0; r < 9; r++) out[r] = 0.0;
+  for (int q = 0; q < 12; q++) {
+    double y[3], o[27];
+    for (int d = 0; d < 3; d++) y[d] = B[q][0] * a[d] + B[q][1] * b[d] + B[q][2] * c[d];
+    const double w = W[q] * area;
+    if (layer == 0)
+      oracle_image_sl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], o);
+    else
+      oracle_image_dl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], nrm[0], nrm[1], nrm[2], o);
+    for (int k = 0; k < 3; k++)
+      for (int r = 0; r < 9; r++) out[r] += w * den[k] * o[9 * k + r];
+  }
+}
+
+enum { ADA_MAXDEPTH = 60, ADA_STACK = 3 * ADA_MAXDEPTH + 4 };
+
+typedef struct {
+  double v[9];
+  double val[9];
+  int depth;
+} AdaSub;
+
+/* one pair and layer, tria3adam's recursion; returns 1 if the depth cap
+ * was reached somewhere (that sub-triangle's estimate is kept) */
+static int image_pair_adaptive(double lam, double mu, int layer, const double* T, const double* nrm,
+                               const double* den, const double X[3], double eps, int maxdepth, double B[12][3],
+                               const double W[12], double acc[9]) {
+  AdaSub* stk = (AdaSub*)malloc(sizeof(AdaSub) * ADA_STACK);
+  int top = 1, capped = 0;
+  memcpy(stk[0].v, T, sizeof(double) * 9);
+  image_rule(lam, mu, layer, nrm, den, X, T, T + 3, T + 6, B, W, stk[0].val);
+  stk[0].depth = 0;
+  while (top > 0) {
+    AdaSub s = stk[--top];
+    if (s.depth >= maxdepth) {
+      for (int r = 0; r < 9; r++) acc[r] += s.val[r];
+      capped = 1;
+      continue;
+    }
+    const double *a = s.v, *b = s.v + 3, *c = s.v + 6;
+    double ab[3], bc[3], ca[3];
+    for (int d = 0; d < 3; d++) {
+      ab[d] = 0.5 * (a[d] + b[d]);
+      bc[d] = 0.5 * (b[d] + c[d]);
+      ca[d] = 0.5 * (c[d] + a[d]);
+    }
+    const double* kids[4][3] = {{a, ab, ca}, {ab, b, bc}, {ca, bc, c}, {ab, bc, ca}};
+    double kv[4][9], sum[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int k = 0; k < 4; k++) {
+      image_rule(lam, mu, layer, nrm, den, X, kids[k][0], kids[k][1], kids[k][2], B, W, kv[k]);
+      for (int r = 0; r < 9; r++) sum[r] += kv[k][r];
+    }
+    double dmax = 0.0;
+    for (int r = 0; r < 9; r++) dmax = fmax(dmax, fabs(s.val[r]));
+    int done = 1;
+    for (int r = 0; r < 9; r++)
+      if (fabs(sum[r] - s.val[r]) > eps * dmax) done = 0;
+    if (done || top + 4 > ADA_STACK) {
+      for (int r = 0; r < 9; r++) acc[r] += sum[r];
+      if (!done) capped = 1;
+      continue;
+    }
+    for (int k = 3; k >= 0; k--) {
+      AdaSub t;
+      for (int vtx = 0; vtx < 3; vtx++) memcpy(t.v + 3 * vtx, kids[k][vtx], sizeof(double) * 3);
+      memcpy(t.val, kv[k], sizeof(double) * 9);
+      t.depth = s.depth + 1;
+      stk[top++] = t;
+    }
+  }
+  free(stk);
+  return capped;
+}
+
+/* Image displacement u (m, 3) and strain e (m, 3, 3) as oracle_image_direct,
+ * every (target, triangle) pair and layer integrated adaptively to relative
+ * tolerance eps with at most maxdepth (<= 60) halvings.  *ncapped = pairs
+ * whose recursion reached the cap.  Returns 0, or 4 for bad arguments. */
+int oracle_image_direct_adaptive(double lam, double mu, int n, const double* tri, const double* nrm,
+                                 const double* ssl, const double* sdl, int m, const double* tgt, double eps,
+                                 int maxdepth, double* u, double* e, int* ncapped) {
+  if (maxdepth < 0 || maxdepth > ADA_MAXDEPTH || !(eps > 0)) return 4;
+  double B[12][3], W[12];
+  quad12(B, W);
+  int capped = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : capped)
+  for (int i = 0; i < m; i++) {
+    double acc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const double* X = tgt + 3 * (size_t)i;
+    for (int t = 0; t < n; t++) {
+      const double* T = tri + 9 * (size_t)t;
+      const double* nt = nrm + 3 * (size_t)t;
+      if (ssl) capped += image_pair_adaptive(lam, mu, 0, T, nt, ssl + 3 * (size_t)t, X, eps, maxdepth, B, W, acc);
+      if (sdl) capped += image_pair_adaptive(lam, mu, 1, T, nt, sdl + 3 * (size_t)t, X, eps, maxdepth, B, W, acc);
+    }
+    for (int d = 0; d < 3; d++) u[3 * (size_t)i + d] = acc[d];
+    double* E = e + 9 * (size_t)i;
+    E[0] = acc[3];
+    E[4] = acc[4];
+    E[8] = acc[5];
+    E[1] = E[3] = acc[6];
+    E[2] = E[6] = acc[7];
+    E[5] = E[7] = acc[8];
+  }
+  if (ncapped) *ncapped = capped;
   return 0;
 }

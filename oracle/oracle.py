@@ -148,6 +148,31 @@ def image_direct(rlam, rmu, triangles, normals, sigma_sl, sigma_dl, targets, lev
     return u, e
 
 
+def image_direct_adaptive(rlam, rmu, triangles, normals, sigma_sl, sigma_dl, targets, eps=1e-11, maxdepth=40):
+    """Image part as image_direct, every pair and layer integrated by the
+    adaptive scheme of the reference's tria3adam (src/tria3adamar.f:33-395)
+    to relative tolerance eps with at most maxdepth halvings.  Returns
+    (u (m,3), strain (m,3,3), pairs that reached the depth cap)."""
+    tri = c64(triangles).reshape(-1, 3, 3)
+    n = tri.shape[0]
+    nrm = c64(normals).reshape(n, 3)
+    tg = c64(targets).reshape(-1, 3)
+    m = tg.shape[0]
+    ssl = c64(sigma_sl).reshape(n, 3) if sigma_sl is not None else None
+    sdl = c64(sigma_dl).reshape(n, 3) if sigma_dl is not None else None
+    u = np.zeros((m, 3))
+    e = np.zeros((m, 3, 3))
+    capped = ctypes.c_int(0)
+    f = lib().oracle_image_direct_adaptive
+    f.restype = ctypes.c_int
+    ier = f(ctypes.c_double(rlam), ctypes.c_double(rmu), ctypes.c_int(n), _d(tri), _d(nrm),
+            _d(ssl) if ssl is not None else None, _d(sdl) if sdl is not None else None, ctypes.c_int(m),
+            _d(tg), ctypes.c_double(eps), ctypes.c_int(int(maxdepth)), _d(u), _d(e), ctypes.byref(capped))
+    if ier:
+        raise ValueError(f"oracle_image_direct_adaptive ier={ier}")
+    return u, e, capped.value
+
+
 class Tree:
     """Bit-exact restatement of d3tstrcr (d3tstrcr.f:31).  All ids are 1-based."""
 

@@ -41,3 +41,29 @@ def test_c_image_rejects_bad_level(oracle, fault):
     tri, nrm, tg, ssl, sdl = fault
     with pytest.raises(ValueError):
         oracle.image_direct(1.0, 1.0, tri, nrm, ssl, sdl, tg, level=13)
+
+
+def test_c_adaptive_converges_and_matches_refinement(oracle, fault):
+    """The oracle's tria3adam-style adaptive mode (src/tria3adamar.f:33-395):
+    tighter tolerances converge, and the result agrees with the distance
+    refinement; no pair reaches the depth cap."""
+    tri, nrm, tg, ssl, sdl = fault
+    ur, er = oracle.image_direct(1.3, 0.7, tri, nrm, ssl, sdl, tg, level=-1)
+    u6, e6, c6 = oracle.image_direct_adaptive(1.3, 0.7, tri, nrm, ssl, sdl, tg, eps=1e-6)
+    u12, e12, c12 = oracle.image_direct_adaptive(1.3, 0.7, tri, nrm, ssl, sdl, tg, eps=1e-12)
+    assert c6 == 0 and c12 == 0
+    assert rel(u6, u12) < 1e-7 and rel(e6, e12) < 1e-7
+    assert rel(ur, u12) < 1e-10 and rel(er, e12) < 1e-10
+
+
+def test_c_adaptive_surface_breaking_fault(oracle):
+    """A fault whose top edge lies on the surface, targets down to 1e-3 below
+    it: the adaptive sum converges (1e-9 against 1e-12) without the cap."""
+    tri, nrm, cen, _ = G.planar_fault(4, 2, length=4.0, width=2.0, dip_deg=60.0, top_depth=0.0)
+    rng = np.random.default_rng(5)
+    sdl = rng.normal(size=cen.shape)
+    tg = np.vstack([cen, [[0.3, 0.05, -1e-3], [1.1, -0.2, -0.02]]])
+    u9, e9, c9 = oracle.image_direct_adaptive(1.0, 1.0, tri, nrm, None, sdl, tg, eps=1e-9)
+    u12, e12, c12 = oracle.image_direct_adaptive(1.0, 1.0, tri, nrm, None, sdl, tg, eps=1e-12)
+    assert c9 == 0 and c12 == 0
+    assert rel(u9, u12) < 1e-8 and rel(e9, e12) < 1e-8
