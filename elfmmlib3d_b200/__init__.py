@@ -54,7 +54,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
-           "efmm_hs_capped"]
+           "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host"]
 
 
 class ElfmmError(RuntimeError):
@@ -504,6 +504,27 @@ def hs_capped():
     return int(L.efmm_hs_capped())
 
 
+def gcr_dense_host(A, B, tol=1e-10, maxit=50):
+    """The solver's iteration on the host for a dense matrix (efmm_gcr_dense_host):
+    A (n,n), B (nrhs,n).  Returns (X (nrhs,n), iterations, relative
+    residuals, ier per column)."""
+    L = load()
+    A = np.ascontiguousarray(A, dtype=np.float64)
+    B = np.ascontiguousarray(B, dtype=np.float64).reshape(-1, A.shape[0])
+    R, n = B.shape
+    X = np.zeros((R, n))
+    its = np.zeros(R, dtype=np.int32)
+    rel = np.zeros(R)
+    ier_c = np.zeros(R, dtype=np.int32)
+    L.efmm_gcr_dense_host.restype = ctypes.c_int
+    ier = L.efmm_gcr_dense_host(n, R, A.ctypes.data_as(_dp), B.ctypes.data_as(_dp), X.ctypes.data_as(_dp),
+                                ctypes.c_double(tol), int(maxit), its.ctypes.data_as(_ip), rel.ctypes.data_as(_dp),
+                                ier_c.ctypes.data_as(_ip))
+    if ier:
+        raise ElfmmError(ier, "gcr_dense_host")
+    return X, its, rel, ier_c
+
+
 def iter_release(wsave):
     """Free the device store an ITER handle names; returns ier (512 if none)."""
     return int(load().efmm_iter_release(wsave.ctypes.data_as(_dp), int(wsave.size)))
@@ -576,6 +597,30 @@ class Plan:
             ier = self._L.efmm_plan_evaluate_batch(*args)
         if ier:
             raise ElfmmError(ier, "evaluate_batch")
+
+    def solve(self, image, kind, rlam, rmu, nrhs, nrm, rhs, x, tol=1e-8, maxit=30, precision=0):
+        """Iterative solution over the operator (efmm_plan_solve, the minimal-
+        residual iteration of the reference's matlab/gmres_simple.m on the
+        device): rhs (nrhs,n,3) -> x (nrhs,n,3), CUDA tensors.  image: the
+        half-space image Plan or None.  kind 0: x = slip (double layer),
+        operator = traction on nrm at the centroids; kind 1: x = traction
+        (single layer), operator = displacement at the centroids.  Returns
+        (iterations, relative residuals, ier per column) as numpy arrays."""
+        R = int(nrhs)
+        its = np.zeros(R, dtype=np.int32)
+        rel = np.zeros(R)
+        ier_c = np.zeros(R, dtype=np.int32)
+        L = self._L
+        L.efmm_plan_solve.restype = ctypes.c_int
+        L.efmm_plan_solve.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _vp,
+                                      _vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _ip, _dp, _ip]
+        ier = L.efmm_plan_solve(self._h, image._h if image is not None else None, int(kind), float(rlam), float(rmu),
+                                R, self._ptr(nrm), self._ptr(rhs), self._ptr(x), float(tol), int(maxit),
+                                int(precision), its.ctypes.data_as(_ip), rel.ctypes.data_as(_dp),
+                                ier_c.ctypes.data_as(_ip))
+        if ier:
+            raise ElfmmError(ier, "solve")
+        return its, rel, ier_c
 
     def evaluate_image(self, rlam, rmu, nrhs, ssl=None, sdl=None, ut=None, et=None, precision=0, mode=0,
                        graph=False):

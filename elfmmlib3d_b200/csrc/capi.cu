@@ -7,6 +7,7 @@
 #include <vector>
 #include "plan.h"
 #include "halfspace.h"
+#include "solve.h"
 #include "harmonics.cuh"
 #include "mindlin_gen.cuh"
 #include "../../include/elfmm3d_b200.h"
@@ -128,6 +129,16 @@ extern "C" int efmm_plan_evaluate_image_graph(efmm_plan* p, double rlam, double 
 }
 
 extern "C" long long efmm_plan_stored_bytes(const efmm_plan* p) { return 8 * p->plan->stored_doubles(); }
+
+extern "C" int efmm_plan_solve(efmm_plan* free_plan, efmm_plan* image_plan, int kind, double rlam, double rmu,
+                               int nrhs, const double* nrm, const double* rhs, double* x, double tol, int maxit,
+                               int precision, int* iters, double* relres, int* ier_cols) {
+  efmm_plan* p = free_plan;
+  if (!p) return IER_BADARG;
+  if (image_plan && image_plan->device != p->device) return IER_BADARG;
+  EFMM_GUARD(return solve_layers(p->plan.get(), image_plan ? image_plan->plan.get() : nullptr, kind, rlam, rmu, nrhs,
+                                 nrm, rhs, x, tol, maxit, precision, iters, relres, ier_cols);)
+}
 
 extern "C" int efmm_plan_set_mixed_floor(efmm_plan* p, double eps, int* order) {
   if (!p) return IER_BADARG;

@@ -405,6 +405,31 @@ void efmm_plan_info(const efmm_plan *plan, long long *info8);
 int efmm_plan_tree_export(const efmm_plan *plan, int *boxes, int *iz, int *iztarg, int *laddr,
                           double *center_size4, int *lstart, int *litems, long long *lcount5);
 
+/* Iterative solution over the layer-potential operator (the reference's
+ * solver loop is MATLAB over a function handle, matlab/gmres_simple.m and
+ * matlab/Contents.m:32-33; this is its minimal-residual iteration on the
+ * device): nrhs right-hand sides rhs (nrhs,n,3) -> densities x (nrhs,n,3),
+ * device arrays, each column with its own coefficients.  free_plan: geometry
+ * set with iter = 1 and no targets; image_plan: NULL (free space) or the
+ * half-space image plan (iter = 1, mindlin = 1, targets = the reflected
+ * centroids (x1, x2, -x3)).  kind 0: x is a double-layer density (slip),
+ * the operator the traction (lam tr(e) I + 2 mu e) nrm at the centroids
+ * (nrm (n,3) device); kind 1: x is a single-layer density (traction), the
+ * operator the displacement at the centroids.  The first application stores
+ * the near fields if the plans hold none; later ones replay them (CUDA
+ * graphs for nrhs <= 64).  Stops a column at |r| < tol |b| (ier_cols 0),
+ * when |r| stops decreasing (8) or after maxit steps (4); iters and the
+ * final |r| / |b| per column (each may be NULL).  Returns ier. */
+int efmm_plan_solve(efmm_plan *free_plan, efmm_plan *image_plan, int kind, double rlam, double rmu, int nrhs,
+                    const double *nrm, const double *rhs, double *x, double tol, int maxit, int precision,
+                    int *iters, double *relres, int *ier_cols);
+
+/* The same iteration on the host for a dense row-major n x n matrix A and
+ * nrhs right-hand sides B (nrhs,n) -> X (nrhs,n): the CPU check of the
+ * algorithm (no device used). */
+int efmm_gcr_dense_host(int n, int nrhs, const double *A, const double *B, double *X, double tol, int maxit,
+                        int *iters, double *relres, int *ier_cols);
+
 /* Checks of the FP32 factored translations on the tensor cores (no
  * counterpart in the reference): one M2L, one M2M and one L2L group of order
  * p (1..31).  _selfcheck emulates the three stages on the host (tiles, their
