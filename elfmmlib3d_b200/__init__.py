@@ -54,7 +54,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
-           "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host"]
+           "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
+           "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump"]
 
 
 class ElfmmError(RuntimeError):
@@ -523,6 +524,17 @@ def gcr_dense_host(A, B, tol=1e-10, maxit=50):
     if ier:
         raise ElfmmError(ier, "gcr_dense_host")
     return X, its, rel, ier_c
+
+
+def tune_dump():
+    """The autotuner's keys and decisions, one line each:
+    "knob p nbox C prec kind decided ms0 ms1" (efmm_tune_dump)."""
+    L = load()
+    L.efmm_tune_dump.restype = ctypes.c_int
+    n = L.efmm_tune_dump(None, 0)
+    buf = ctypes.create_string_buffer(n + 1)
+    L.efmm_tune_dump(buf, n + 1)
+    return [l for l in buf.value.decode().splitlines() if l]
 
 
 def iter_release(wsave):

@@ -749,11 +749,34 @@ void Plan::run_translations_tc(TransSched& S, int C, const float* src, float* ds
                     err);
 }
 
+// The engine of each FP32 translation stage for this pass: the tuner's pick
+// for the key (stage, order, leaf capacity, columns, kind); a pass being
+// captured into a graph takes the decided engine (or the tensor cores while
+// undecided) and reports nothing.
+void Plan::tune_begin(int kind, int C) {
+  trans_tuning_ = !capturing_ && rot_tc_usable();
+  for (int s = 0; s < 3; s++) {
+    trans_key_[s] = TuneKey{s, ops_->p, nbox_, C, 1, kind};
+    if (!rot_tc_usable())
+      trans_cand_[s] = 1;
+    else
+      trans_cand_[s] = capturing_ ? tune_best(trans_key_[s], 0) : tune_pick(trans_key_[s], 2);
+  }
+}
+
+void Plan::tune_end() {
+  if (!trans_tuning_) return;
+  const float ms[3] = {timings.m2m, timings.m2l, timings.l2l};
+  for (int s = 0; s < 3; s++) tune_report(trans_key_[s], 2, trans_cand_[s], ms[s]);
+  trans_tuning_ = false;
+}
+
 template <class T>
 void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T* dst) {
   int D = 2 * ncoef(p_);
   if constexpr (sizeof(T) == 4) {
-    if (rot_tc_usable()) {
+    const int stage = (&S == &m2l_ || &S == &m2lv_img_) ? 1 : ((&S == &l2l_ || &S == &l2l_img_ || &S == &l2l_img_u_) ? 2 : 0);
+    if (rot_tc_usable() && trans_cand_[stage] == 0) {
       run_translations_tc(S, C, reinterpret_cast<const float*>(src), reinterpret_cast<float*>(dst));
       return;
     }
@@ -1426,6 +1449,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.C = C; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
     if (mixed) {
       pa.wnorm = ops_->wnorm.get();  // multipoles in the normalised basis
+      tune_begin(0, C);
       if (!(p2m_unit_ && p2m_factored<float>(pa, R, mpole_f_.get(), false)))
         p2m_twostage<float>(pa, R, mpole_f_.get());
       rec(2);
@@ -1570,6 +1594,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   launches_ = (int)(launches_total() - launch0);
   product_collect();
   if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
+  if (mixed) tune_end();
   return IER_OK;
 }
 
@@ -2166,6 +2191,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       float* mp = img_mp_f_.get();
       float* lc = img_lc_f_.get();
       pa.wnorm = ops_->wnorm.get();
+      tune_begin(1, Cv + Cu);
       if (7 * R < 32)
         launch_p2m_img<float>(st_, np2m_, pa, R, (long long)(nb * Cv * D), mp);
       else if (!(p2m_unit_ && p2m_factored<float>(pa, R, mp, true)))
@@ -2281,6 +2307,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
   launches_ = (int)(launches_total() - launch0);
   product_collect();
   if (mixed && tc_take_error()) return IER_CUDA;  // a tensor-core product gave up waiting
+  if (mixed) tune_end();
   return IER_OK;
 }
 

@@ -8,6 +8,7 @@
 #include "fmm.h"
 #include "kernels.h"
 #include "rotations.h"
+#include "tune.h"
 
 namespace efmm {
 
@@ -326,6 +327,14 @@ class Plan {
   void cut_tc_tasks(TransSched& S, int C);
   void run_translations_tc(TransSched& S, int C, const float* src, float* dst);
   DevBuf<float> rot_y_, rot_w_;  // intermediates of the tensor-core translations
+  // autotuned engine of the FP32 translations per stage (M2M, M2L, L2L):
+  // 0 tensor cores, 1 CUDA cores; chosen at the start of a mixed pass
+  // (tune_begin), reported with the stage times at its end (tune_end)
+  int trans_cand_[3] = {0, 0, 0};
+  TuneKey trans_key_[3];
+  bool trans_tuning_ = false;
+  void tune_begin(int kind, int C);
+  void tune_end();
   bool factored_ = true;  // translations in factored form when they fit
   bool p2m_unit_ = true;  // batched P2M through unit-density multipoles (else node products)
   template <class T>

@@ -430,6 +430,22 @@ int efmm_plan_solve(efmm_plan *free_plan, efmm_plan *image_plan, int kind, doubl
 int efmm_gcr_dense_host(int n, int nrhs, const double *A, const double *B, double *X, double tol, int maxit,
                         int *iters, double *relres, int *ier_cols);
 
+/* The autotuner (no counterpart in the reference, whose tuning is the fixed
+ * iprec tables, src/elfmm3dtria.f:702-722): per key (knob, expansion order,
+ * leaf capacity, expansion columns per box, precision, plan kind) the first
+ * passes time every candidate implementation of the knob's stage
+ * (TUNE_VISITS = 2 runs each, the faster kept) and later passes run the
+ * fastest.  Knobs 0, 1, 2: the FP32 translations of the M2M, M2L, L2L
+ * stages on the tensor cores (candidate 0) or the CUDA cores (1).  Decisions
+ * persist in the file named by ELFMM3D_TUNE_FILE when it is set.  pick
+ * returns the candidate to run; report records a timed run (ms); dump
+ * writes "knob p nbox C prec kind decided ms..." lines into buf (len bytes)
+ * and returns the full length. */
+int efmm_tune_pick(int knob, int p, int nbox, int C, int prec, int kind, int ncand);
+void efmm_tune_report(int knob, int p, int nbox, int C, int prec, int kind, int ncand, int cand, float ms);
+void efmm_tune_reset(void);
+int efmm_tune_dump(char *buf, int len);
+
 /* Checks of the FP32 factored translations on the tensor cores (no
  * counterpart in the reference): one M2L, one M2M and one L2L group of order
  * p (1..31).  _selfcheck emulates the three stages on the host (tiles, their
