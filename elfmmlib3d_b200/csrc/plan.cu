@@ -764,6 +764,29 @@ void Plan::tune_begin(int kind, int C) {
   }
 }
 
+void Plan::switch_precision(bool mixed) {
+  if (capturing_ || last_mixed_ == (int)mixed) return;
+  const bool had = last_mixed_ >= 0;
+  last_mixed_ = mixed ? 1 : 0;
+  if (!had) return;
+  graph_reset();
+  if (!mixed) {
+    store_f_.release();
+    store_tc_gen_ = -1;
+    mpole_f_.release();
+    local_f_.release();
+    img_mp_f_.release();
+    img_lc_f_.release();
+    rot_y_.release();
+    rot_w_.release();
+  } else {
+    mpole_.release();
+    local_.release();
+    img_mp_.release();
+    img_lc_.release();
+  }
+}
+
 void Plan::tune_end() {
   if (!trans_tuning_) return;
   const float ms[3] = {timings.m2m, timings.m2l, timings.l2l};
@@ -896,6 +919,7 @@ void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1
 
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
                    double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode, bool do_far) {
+  switch_precision(false);
   int n = n_, nt = nt_;
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
@@ -1118,6 +1142,7 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
                          int mode) {
   if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
+  switch_precision(precision == 1);
   MixedOrders orders(this, precision == 1);
   const int n = n_, nt = nt_;
   if (mode) {
@@ -2091,6 +2116,7 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
                          double* d_u_tgt, double* d_e_tgt, int precision, int mode) {
   if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
   if (!mindlin_ || rmu <= 0 || rlam + 2 * rmu <= 0) return IER_BADARG;
+  switch_precision(precision == 1);
   const int nt = nt_;
   if (nt == 0 || !(d_u_tgt || d_e_tgt)) return IER_OK;
   if (!(d_ssl || d_sdl)) {

@@ -335,6 +335,14 @@ class Plan {
   bool trans_tuning_ = false;
   void tune_begin(int kind, int C);
   void tune_end();
+  // A pass of the other precision than the last one releases the large
+  // buffers only the last one's form uses (FP32 expansions, the FP32 copy
+  // of the stored near field and the tensor-core intermediates; or the FP64
+  // expansions of many right-hand sides), so that the memory a form finds,
+  // and with it the size of its waves and right-hand-side chunks, does not
+  // depend on which form ran before.  Captured graphs are dropped with them.
+  int last_mixed_ = -1;
+  void switch_precision(bool mixed);
   bool factored_ = true;  // translations in factored form when they fit
   bool p2m_unit_ = true;  // batched P2M through unit-density multipoles (else node products)
   template <class T>
