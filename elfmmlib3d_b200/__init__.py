@@ -55,7 +55,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
-           "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump"]
+           "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant"]
 
 
 class ElfmmError(RuntimeError):

@@ -242,6 +242,246 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
 }
 
+// ----------------------------------------------------------------------
+// The same product with the operand tiles streamed by cp.async into a ring
+// of raw FP32 tiles in shared memory, RING tiles ahead of the tensor cores
+// (RING = 4 for 64-wide tiles, 3 for 128-wide), so that several K tiles of
+// loads are in flight per SM while the threads split the current tile into
+// its TF32 head and tail (shared memory to shared memory, into the canonical
+// layout of k_gemm_tc) and the previous tile's accumulator is drained.  The
+// raw A tile is [32 k][128 rows] (rows contiguous, as in A), the raw B tile
+// [BN columns][32 k] with its 16-byte chunks XOR-swizzled by the column, so
+// that the conversion's reads are free of bank conflicts.  Rows of A and B
+// that are 16-byte aligned and complete are copied in 16-byte pieces, other
+// elements one by one (zero-filled past the matrix).  Bounded waits and the
+// per-K-tile FP32 drain as in k_gemm_tc.
+template <int BN>
+__host__ __device__ constexpr int tc_ring_depth() { return BN == 64 ? 4 : 3; }
+template <int BN>
+__host__ __device__ constexpr int tc_raw_bytes() { return TC_BM * TC_BK * 4 + BN * TC_BK * 4; }
+template <int BN>
+__host__ __device__ constexpr int tc_ring_smem() {
+  return 2 * tc_stage_bytes<BN>() + tc_ring_depth<BN>() * tc_raw_bytes<BN>() + 1024 + 64;
+}
+
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int srcbytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(srcbytes) : "memory");
+}
+__device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, int srcbytes) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(dst), "l"(src), "r"(srcbytes) : "memory");
+}
+
+template <int BN, class TC>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
+               TC* __restrict__ Cm, int* __restrict__ err) {
+  constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
+  constexpr int RING = tc_ring_depth<BN>(), RAW = tc_raw_bytes<BN>(), RAW_A = TC_BM * TC_BK * 4;
+  constexpr int RG = BN / 8, NB = BN / 32, NHALF = BN / 2;
+  constexpr int NCA = TC_BM * TC_BK / 4 / TC_THREADS;  // A chunks of 16 bytes per thread and tile (4)
+  constexpr int NCB = BN * TC_BK / 4 / TC_THREADS;     // B chunks per thread and tile (2 or 4)
+  constexpr uint32_t IDESC = tc_idesc_mn(TC_BM, BN);
+  extern __shared__ __align__(1024) unsigned char tc_ring_raw[];
+  const uint32_t raw = smem_u32(tc_ring_raw);
+  unsigned char* sm = tc_ring_raw + ((1024 - (raw & 1023)) & 1023);
+  unsigned char* ring = sm + 2 * TC_STAGE_BYTES;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(ring + RING * RAW);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ring + RING * RAW + 16);
+  const GemmTask t = tasks[blockIdx.x];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                 "r"(2 * BN)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(smem_u32(&bars[0]), 1);
+    mbar_init(smem_u32(&bars[1]), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = *tmem_slot;
+
+  const float* Ab = A + t.a_off;
+  const float* Bb = B + t.b_off;
+  const int nkt = (t.K + TC_BK - 1) / TC_BK;
+  const bool avec = ((t.a_off & 3) == 0) && ((t.lda & 3) == 0);
+  const bool bvec = ((t.b_off & 3) == 0) && ((t.ldb & 3) == 0);
+  // copies of K tile kt into ring slot kt % RING (nothing past the last tile)
+  auto issue = [&](int kt) {
+    if (kt >= nkt) return;
+    const uint32_t slot = smem_u32(ring + (kt % RING) * RAW);
+    const int k0 = kt * TC_BK;
+#pragma unroll
+    for (int it = 0; it < NCA; it++) {
+      const int c = tid + TC_THREADS * it, k = c >> 5, mc = c & 31;
+      const int gk = k0 + k, gm = t.row0 + 4 * mc;
+      const uint32_t d = slot + (uint32_t)(k * TC_BM + 4 * mc) * 4;
+      const float* g = Ab + (size_t)gk * t.lda + gm;
+      if (avec && gk < t.K && gm + 3 < t.M) {
+        cp_async16(d, g, 16);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const bool ok = gk < t.K && gm + j < t.M;
+          cp_async4(d + 4 * j, ok ? (const void*)(g + j) : (const void*)Ab, ok ? 4 : 0);
+        }
+      }
+    }
+#pragma unroll
+    for (int it = 0; it < NCB; it++) {
+      const int c = tid + TC_THREADS * it, n = c >> 3, kc = c & 7;
+      const int gn = t.col0 + n, gk = k0 + 4 * kc;
+      const uint32_t d = slot + RAW_A + (uint32_t)(n * 128 + ((kc ^ (n & 7)) * 16));
+      const float* g = Bb + (size_t)gn * t.ldb + gk;
+      if (bvec && gn < t.N && gk + 3 < t.K) {
+        cp_async16(d, g, 16);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+          const bool ok = gn < t.N && gk + j < t.K;
+          cp_async4(d + 4 * j, ok ? (const void*)(g + j) : (const void*)Bb, ok ? 4 : 0);
+        }
+      }
+    }
+  };
+  // ring slot of tile kt -> head / tail in conversion stage s (canonical layout)
+  auto convert = [&](int kt, int s) {
+    const unsigned char* slot = ring + (kt % RING) * RAW;
+    const float* ra = reinterpret_cast<const float*>(slot);
+    unsigned char* st = sm + s * TC_STAGE_BYTES;
+#pragma unroll
+    for (int it = 0; it < 4; it++) {
+      const int b = it * 8 + warp;
+      const int m = 32 * (b & 3) + lane, ca = b >> 2;
+      float v[4];
+#pragma unroll
+      for (int j = 0; j < 4; j++) v[j] = ra[(4 * ca + j) * TC_BM + m];
+      const uint32_t offa = (m & 7) * 16 + ca * TC_LBO + (m >> 3) * TC_SBO;
+      float4 hi, lo;
+      hi.x = tf32_head(v[0]); lo.x = v[0] - hi.x;
+      hi.y = tf32_head(v[1]); lo.y = v[1] - hi.y;
+      hi.z = tf32_head(v[2]); lo.z = v[2] - hi.z;
+      hi.w = tf32_head(v[3]); lo.w = v[3] - hi.w;
+      *reinterpret_cast<float4*>(st + offa) = hi;
+      *reinterpret_cast<float4*>(st + TC_TILE_BYTES + offa) = lo;
+    }
+#pragma unroll
+    for (int it = 0; it < NB; it++) {
+      const int b = it * 8 + warp;
+      const int n = 8 * (b % RG) + (lane & 7), kc = 4 * (b / RG) + (lane >> 3);
+      const float4 v = *reinterpret_cast<const float4*>(slot + RAW_A + n * 128 + ((kc ^ (n & 7)) * 16));
+      const uint32_t offb = (n & 7) * 16 + kc * TC_LBO + (n >> 3) * TC_SBO;
+      float4 hi, lo;
+      hi.x = tf32_head(v.x); lo.x = v.x - hi.x;
+      hi.y = tf32_head(v.y); lo.y = v.y - hi.y;
+      hi.z = tf32_head(v.z); lo.z = v.z - hi.z;
+      hi.w = tf32_head(v.w); lo.w = v.w - hi.w;
+      *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + offb) = hi;
+      *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + TC_BTILE + offb) = lo;
+    }
+  };
+  const int quarter = warp & 3, half = warp >> 2;
+  TC acc[NHALF];
+#pragma unroll
+  for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
+  auto drain = [&](int u) {
+    const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
+#pragma unroll
+    for (int c16 = 0; c16 < NHALF / 16; c16++) {
+      const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
+      uint32_t r[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "r"(addr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += (TC)__uint_as_float(r[j]);
+    }
+  };
+  // the first RING - 1 tiles in flight (one commit group per tile, empty past the end)
+#pragma unroll
+  for (int q = 0; q < RING - 1; q++) {
+    issue(q);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  }
+  bool ok = true;
+  int issued = -1;  // last tile whose MMAs were issued
+  for (int kt = 0; kt < nkt; kt++) {
+    const int s = kt & 1;
+    asm volatile("cp.async.wait_group %0;" ::"n"(RING - 2) : "memory");
+    __syncthreads();  // tile kt landed for every thread; slot of tile kt - 1 converted
+    issue(kt + RING - 1);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    convert(kt, s);  // stage s is free: tile kt - 2 finished before tile kt - 1 was drained
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(sm + s * TC_STAGE_BYTES);
+      const uint32_t ahi = base, alo = base + TC_TILE_BYTES, bhi = base + 2 * TC_TILE_BYTES, blo = bhi + TC_BTILE;
+      const uint32_t dacc = tmem + (uint32_t)s * BN;
+#pragma unroll
+      for (int i = 0; i < TC_BK / 8; i++) {
+        const uint64_t dah = umma_desc(ahi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dal = umma_desc(alo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dbh = umma_desc(bhi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        const uint64_t dbl = umma_desc(blo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
+        mma_tf32(dacc, dal, dbh, IDESC, i > 0 ? 1u : 0u);
+        mma_tf32(dacc, dah, dbl, IDESC, 1u);
+        mma_tf32(dacc, dah, dbh, IDESC, 1u);
+      }
+      mma_commit(smem_u32(&bars[s]));
+    }
+    issued = kt;
+    if (kt >= 1) {
+      const int u = kt - 1;
+      ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+      ok = __syncthreads_and(ok);
+      if (!ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      drain(u);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy outlives the CTA
+  if (ok && nkt > 0) {
+    const int u = nkt - 1;
+    ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+    ok = __syncthreads_and(ok);
+    if (ok) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      drain(u);
+    }
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    for (int u = (issued >= 1 ? issued - 1 : 0); u <= issued; u++) mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+  } else {
+    const int row = t.row0 + 32 * quarter + lane;
+    if (row < t.M) {
+      TC* Cp = Cm + t.c_off + row;
+#pragma unroll
+      for (int j = 0; j < NHALF; j++) {
+        const int col = t.col0 + NHALF * half + j;
+        if (col < t.N) Cp[(size_t)col * t.ldc] = acc[j];
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+}
+
 namespace {
 __device__ int g_tc_err;
 int* g_tc_err_addr[64] = {};
@@ -276,10 +516,34 @@ bool tc_enabled() {
   return on;
 }
 
+// Which form of the product runs: 1 (default) the cp.async ring
+// (k_gemm_tc_ring), 0 the register-staged k_gemm_tc; ELFMM3D_TC_RING=0 or
+// efmm_tc_variant select the latter.
+static int g_tc_ring = -1;
+int tc_ring_variant() {
+  if (g_tc_ring < 0) {
+    const char* e = getenv("ELFMM3D_TC_RING");
+    g_tc_ring = (e && e[0] == '0') ? 0 : 1;
+  }
+  return g_tc_ring;
+}
+
 template <class TC>
 static void launch_gemm_tc_t(cudaStream_t st, int ntask, const GemmTask* tasks, const float* A, const float* B,
                              TC* C, int* err, int bn) {
   if (ntask <= 0) return;
+  if (tc_ring_variant()) {
+    if (bn == 64) {
+      EFMM_CUDA_TRY(smem_raise(k_gemm_tc_ring<64, TC>, (int)(tc_ring_smem<64>())));
+      k_gemm_tc_ring<64, TC><<<ntask, TC_THREADS, tc_ring_smem<64>(), st>>>(tasks, A, B, C, err);
+    } else {
+      EFMM_CUDA_TRY(smem_raise(k_gemm_tc_ring<128, TC>, (int)(tc_ring_smem<128>())));
+      k_gemm_tc_ring<128, TC><<<ntask, TC_THREADS, tc_ring_smem<128>(), st>>>(tasks, A, B, C, err);
+    }
+    count_launch();
+    EFMM_CUDA_TRY(cudaGetLastError());
+    return;
+  }
   if (bn == 64) {
     EFMM_CUDA_TRY(smem_raise(k_gemm_tc<64, TC>, (int)(tc_smem<64>())));
     k_gemm_tc<64, TC><<<ntask, TC_THREADS, tc_smem<64>(), st>>>(tasks, A, B, C, err);
@@ -363,6 +627,14 @@ extern "C" int efmm_tc_gemm_selfcheck_tile(int M, int N, int K, int bn, int alig
   *timeout = herr;
   cudaFree(dA); cudaFree(dB); cudaFree(dC); cudaFree(dErr); cudaFree(dT);
   return 0;
+}
+
+// Select the form of the tensor-core product for this process (1 the
+// cp.async ring, 0 register staging); returns the previous form.
+extern "C" int efmm_tc_variant(int ring) {
+  const int old = efmm::tc_ring_variant();
+  efmm::g_tc_ring = ring ? 1 : 0;
+  return old;
 }
 
 extern "C" int efmm_tc_gemm_selfcheck(int M, int N, int K, unsigned seed, double* rel, int* timeout) {

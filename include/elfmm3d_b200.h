@@ -430,6 +430,12 @@ int efmm_plan_solve(efmm_plan *free_plan, efmm_plan *image_plan, int kind, doubl
 int efmm_gcr_dense_host(int n, int nrhs, const double *A, const double *B, double *X, double tol, int maxit,
                         int *iters, double *relres, int *ier_cols);
 
+/* The form of the tensor-core FP32 product for this process: 1 (default)
+ * operands streamed by cp.async into a ring of raw tiles, 0 staged through
+ * registers (also ELFMM3D_TC_RING=0).  Returns the previous form.  No
+ * counterpart in the reference. */
+int efmm_tc_variant(int ring);
+
 /* The autotuner (no counterpart in the reference, whose tuning is the fixed
  * iprec tables, src/elfmm3dtria.f:702-722): per key (knob, expansion order,
  * leaf capacity, expansion columns per box, precision, plan kind) the first

@@ -1,12 +1,22 @@
 """The tensor-core FP32 product (tcgen05.mma kind::tf32 with the 3-term
 head/tail split) against an FP64 host product: FP32-level accuracy on full
 tiles, ragged edges (M, N not multiples of 128, K not a multiple of 32) and
-an empty K."""
+an empty K; in both forms of the kernel (operands streamed by cp.async into
+a ring of raw tiles, the default, and register staging)."""
 import ctypes
 
 import pytest
 
 pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(params=[1, 0], ids=["ring", "registers"], autouse=True)
+def variant(request, gpu):
+    f = gpu.load().efmm_tc_variant
+    f.restype = ctypes.c_int
+    old = f(request.param)
+    yield request.param
+    f(old)
 
 
 def _check(gpu, M, N, K, seed, bn=128, aligned=0):
