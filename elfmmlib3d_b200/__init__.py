@@ -55,7 +55,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
-           "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant"]
+           "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
+           "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host"]
 
 
 class ElfmmError(RuntimeError):
@@ -243,6 +244,63 @@ def el3dtriadirecttarg(rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigm
                           _byref_i(ifptfrctarg), ptt.ctypes.data_as(_dp), _byref_i(ifstraintarg),
                           stt.ctypes.data_as(_dp))
     return pt, st, ptt[:m], stt[:m]
+
+
+def _part_args(source, sigma_sl, sigma_dl, sigma_dv):
+    src = _c(source, (-1, 3))
+    n = src.shape[0]
+    z = np.zeros((n, 3))
+    ssl = _c(sigma_sl, (n, 3)) if sigma_sl is not None else z
+    sdl = _c(sigma_dl, (n, 3)) if sigma_dl is not None else z
+    sdv = _c(sigma_dv, (n, 3)) if sigma_dv is not None else z
+    return src, ssl, sdl, sdv, n
+
+
+def elfmm3dparttarg(iprec, rlam, rmu, source, sigma_sl=None, sigma_dl=None, sigma_dv=None, target=None,
+                    ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1, direct=False):
+    """Particle FMM in free space (src/elfmm3dpart.f:104; direct=True: the
+    O(N^2) el3dpartdirecttarg, :506): point forces sigma_sl (n,3), point
+    displacement discontinuities sigma_dl (n,3) with orientations sigma_dv
+    (n,3).  Returns (ier, ptfrc (n,3), strain (n,3,3), ptfrctarg (m,3),
+    straintarg (m,3,3))."""
+    L = load()
+    _need_gpu()
+    src, ssl, sdl, sdv, n = _part_args(source, sigma_sl, sigma_dl, sigma_dv)
+    tg = _c(target if target is not None else np.zeros((0, 3)), (-1, 3))
+    m = tg.shape[0]
+    pt, st = np.zeros((n, 3)), np.zeros((n, 3, 3))
+    ptt, stt = np.zeros((max(m, 1), 3)), np.zeros((max(m, 1), 3, 3))
+    d = lambda a: a.ctypes.data_as(_dp)
+    ier = ctypes.c_int(0)
+    if direct:
+        L.el3dpartdirecttarg_(_byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src), _byref_i(sigma_sl is not None),
+                              d(ssl), _byref_i(sigma_dl is not None), d(sdl), d(sdv), _byref_i(ifptfrc), d(pt),
+                              _byref_i(ifstrain), d(st), _byref_i(m), d(tg), _byref_i(ifptfrctarg), d(ptt),
+                              _byref_i(ifstraintarg), d(stt))
+    else:
+        L.elfmm3dparttarg_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src),
+                           _byref_i(sigma_sl is not None), d(ssl), _byref_i(sigma_dl is not None), d(sdl), d(sdv),
+                           _byref_i(ifptfrc), d(pt), _byref_i(ifstrain), d(st), _byref_i(m), d(tg),
+                           _byref_i(ifptfrctarg), d(ptt), _byref_i(ifstraintarg), d(stt))
+    return ier.value, pt, st, ptt[:m], stt[:m]
+
+
+def part_pair_host(rlam, rmu, x, y, sl=None, dl=None, nu=None):
+    """One (point, particle) pair of the particle near field on the host
+    (efmm_part_pair_host): (u (3,), strain (3,3))."""
+    L = load()
+    u, e6 = np.zeros(3), np.zeros(6)
+    p = lambda a: _c(a, (3,)).ctypes.data_as(_dp) if a is not None else None
+    L.efmm_part_pair_host.restype = ctypes.c_int
+    L.efmm_part_pair_host.argtypes = [ctypes.c_double, ctypes.c_double, _dp, _dp, _dp, _dp, _dp, _dp, _dp]
+    keep = [_c(a, (3,)) if a is not None else None for a in (x, y, sl, dl, nu)]
+    ier = L.efmm_part_pair_host(float(rlam), float(rmu), *[k.ctypes.data_as(_dp) if k is not None else None
+                                                           for k in keep], u.ctypes.data_as(_dp),
+                                e6.ctypes.data_as(_dp))
+    if ier:
+        raise ElfmmError(ier, "part_pair_host")
+    e = np.array([[e6[0], e6[3], e6[4]], [e6[3], e6[1], e6[5]], [e6[4], e6[5], e6[2]]])
+    return u, e
 
 
 def batch_host(iprec, rlam, rmu, triangle, trinorm, source, sigma_sl=None, sigma_dl=None, target=None,

@@ -355,6 +355,92 @@ int host_call(int iprec, double rlam, double rmu, const double* tri, const doubl
 }
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Particle FMM (src/elfmm3dpart.f:52-218, el3dpartdirecttarg :506): point
+// forces sigma_sl and point displacement discontinuities sigma_dl with
+// orientations sigma_dv at the sources; displacement and strain at the
+// sources (self-interaction excluded) and at targets.
+// ---------------------------------------------------------------------------
+namespace {
+int part_call(int iprec, double rlam, double rmu, int n, const double* src, int ifsingle, const double* ssl,
+              int ifdouble, const double* sdl, const double* sdv, int ifptfrc, double* ptfrc, int ifstrain,
+              double* strain, int nt, const double* tgt, int ifptfrctarg, double* ptfrctarg, int ifstraintarg,
+              double* straintarg, bool direct) {
+  if (n < 1 || nt < 0 || rmu <= 0) return IER_BADARG;
+  if (ifdouble && !sdv) return IER_BADARG;
+  std::lock_guard<std::mutex> lk(g_mu);
+  efmm_plan* p = shared_plan();
+  if (!p) return IER_NODEVICE;
+  try {
+    cudaSetDevice(p->device);
+    if (!g_bufs) g_bufs = new HostCall();
+    HostCall& B = *g_bufs;
+    cudaStream_t st = p->stream;
+    up(B.src, src, 3 * (size_t)n, st);
+    up(B.tgt, tgt, 3 * (size_t)nt, st);
+    if (ifdouble) up(B.nrm, sdv, 3 * (size_t)n, st);
+    if (ifsingle) up(B.ssl, ssl, 3 * (size_t)n, st);
+    if (ifdouble) up(B.sdl, sdl, 3 * (size_t)n, st);
+    B.u.resize(3 * (size_t)n);
+    B.e.resize(9 * (size_t)n);
+    B.ut.resize(3 * (size_t)std::max(nt, 1));
+    B.et.resize(9 * (size_t)std::max(nt, 1));
+    int ier = p->plan->set_geometry(n, nullptr, ifdouble ? B.nrm.get() : nullptr, B.src.get(), nt, B.tgt.get(),
+                                    iprec, false, false);
+    if (ier) return ier;
+    const bool src_out = ifptfrc || ifstrain, tgt_out = nt > 0 && (ifptfrctarg || ifstraintarg);
+    double* du = src_out ? B.u.get() : nullptr;
+    double* de = ifstrain ? B.e.get() : nullptr;
+    double* dut = tgt_out ? B.ut.get() : nullptr;
+    double* det = (nt > 0 && ifstraintarg) ? B.et.get() : nullptr;
+    const double* dssl = ifsingle ? B.ssl.get() : nullptr;
+    const double* dsdl = ifdouble ? B.sdl.get() : nullptr;
+    ier = direct ? p->plan->evaluate_direct(rlam, rmu, dssl, dsdl, du, de, dut, det)
+                 : p->plan->evaluate(rlam, rmu, dssl, dsdl, du, de, dut, det);
+    if (ier) return ier;
+    if (ifptfrc) down(ptfrc, B.u, 3 * (size_t)n, st);
+    if (ifstrain) down(strain, B.e, 9 * (size_t)n, st);
+    if (nt > 0 && ifptfrctarg) down(ptfrctarg, B.ut, 3 * (size_t)nt, st);
+    if (nt > 0 && ifstraintarg) down(straintarg, B.et, 9 * (size_t)nt, st);
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+    return IER_OK;
+  } catch (const efmm::CudaError&) {
+    return IER_CUDA;
+  } catch (const std::bad_alloc&) {
+    return IER_ALLOC;
+  }
+}
+}  // namespace
+
+extern "C" void elfmm3dparttarg_(int* ier, const int* iprec, const double* rlam, const double* rmu, const int* nparts,
+                                 const double* source, const int* ifsingle, const double* sigma_sl,
+                                 const int* ifdouble, const double* sigma_dl, const double* sigma_dv,
+                                 const int* ifptfrc, double* ptfrc, const int* ifstrain, double* strain,
+                                 const int* ntargs, const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                 const int* ifstraintarg, double* straintarg) {
+  *ier = part_call(*iprec, *rlam, *rmu, *nparts, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv,
+                   *ifptfrc, ptfrc, *ifstrain, strain, *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg,
+                   straintarg, false);
+}
+
+extern "C" void elfmm3dpart_(int* ier, const int* iprec, const double* rlam, const double* rmu, const int* nparts,
+                             const double* source, const int* ifsingle, const double* sigma_sl, const int* ifdouble,
+                             const double* sigma_dl, const double* sigma_dv, const int* ifptfrc, double* ptfrc,
+                             const int* ifstrain, double* strain) {
+  *ier = part_call(*iprec, *rlam, *rmu, *nparts, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv,
+                   *ifptfrc, ptfrc, *ifstrain, strain, 0, nullptr, 0, nullptr, 0, nullptr, false);
+}
+
+extern "C" void el3dpartdirecttarg_(const double* rlam, const double* rmu, const int* nsource, const double* source,
+                                    const int* ifsingle, const double* sigma_sl, const int* ifdouble,
+                                    const double* sigma_dl, const double* sigma_dv, const int* ifptfrc,
+                                    double* ptfrc, const int* ifstrain, double* strain, const int* ntarget,
+                                    const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                    const int* ifstraintarg, double* straintarg) {
+  part_call(2, *rlam, *rmu, *nsource, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv, *ifptfrc, ptfrc,
+            *ifstrain, strain, *ntarget, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, true);
+}
+
 extern "C" void elfmm3dtriatarg_(int* ier, const int* iprec, const double* rlam, const double* rmu,
                                  const double* triangle, const double* trinorm, const int* nparts,
                                  const double* source, const int* ifsingle, const double* sigma_sl,

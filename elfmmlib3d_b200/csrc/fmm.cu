@@ -66,7 +66,7 @@ k_p2m(const P2MArgs a) {
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
   int t0 = a.sstart[box], tn = a.scount[box];
-  int nnode = 12 * tn;
+  int nnode = a.points ? tn : 12 * tn;
   const int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
   double acc[CMAX][4][2];
 #pragma unroll
@@ -81,17 +81,25 @@ k_p2m(const P2MArgs a) {
     __syncthreads();
     int node = b0 + warp;
     if (node < nnode) {
-      int it = t0 + node / 12, iq = node % 12;
-      const double* T = a.tri + 9 * (size_t)it;
-      double y[3];
-      for (int d = 0; d < 3; d++)
-        y[d] = Q.b[iq][0] * T[d] + Q.b[iq][1] * T[3 + d] + Q.b[iq][2] * T[6 + d];
-      double e1[3] = {T[3] - T[0], T[4] - T[1], T[5] - T[2]};
-      double e2[3] = {T[6] - T[0], T[7] - T[1], T[8] - T[2]};
-      double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
-                      e1[0] * e2[1] - e1[1] * e2[0]};
-      double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-      double w = Q.w[iq] * area;
+      int it, iq = 0;
+      double y[3], w;
+      if (a.points) {  // a particle: one node of weight 1
+        it = t0 + node;
+        for (int d = 0; d < 3; d++) y[d] = a.pts[3 * (size_t)it + d];
+        w = 1.0;
+      } else {
+        it = t0 + node / 12;
+        iq = node % 12;
+        const double* T = a.tri + 9 * (size_t)it;
+        for (int d = 0; d < 3; d++)
+          y[d] = Q.b[iq][0] * T[d] + Q.b[iq][1] * T[3 + d] + Q.b[iq][2] * T[6 + d];
+        double e1[3] = {T[3] - T[0], T[4] - T[1], T[5] - T[2]};
+        double e2[3] = {T[6] - T[0], T[7] - T[1], T[8] - T[2]};
+        double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                        e1[0] * e2[1] - e1[1] * e2[0]};
+        double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+        w = Q.w[iq] * area;
+      }
       double z[3] = {(y[0] - c[0]) / s, (y[1] - c[1]) / s, (y[2] - c[2]) / s};
       // column chains of the regular harmonics, one order m per lane
       cplx* Y = Ys + (size_t)warp * nc;

@@ -48,6 +48,10 @@ struct P2MArgs {
   // half-space image columns: alpha = (lam + mu)/(lam + 2 mu) and the Lame
   // constants of the double-layer tensor
   double alpha = 0, lam = 0, mu = 0;
+  // particles (k_p2m only): one node per source at pts (tree order), weight
+  // 1, nrm = the dipole orientations (src/elfmm3dpart.f:319-420)
+  int points = 0;
+  const double* pts = nullptr;
 };
 
 struct L2TArgs {

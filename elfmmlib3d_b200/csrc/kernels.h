@@ -15,6 +15,8 @@ struct NearArgs {
   int dosl, dodl, dostrain_src, dostrain_tgt, do_src, do_tgt;
   double rlam, rmu;
   double *u_src, *e_src, *u_tgt, *e_tgt;
+  const double* part_sl = nullptr;  // particles: densities (n, 3) in tree order
+  const double* part_dl = nullptr;
 };
 
 void launch_tri_prep(cudaStream_t st, int n, const double* tri, const int* perm, const double* ssl,

@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include "plan.h"
+#include "particles.h"
 #include "halfspace.h"
 
 namespace efmm {
@@ -342,10 +343,21 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
     p_ = 0;
     nbox_ = n + nt;
   }
-  tri_u_.resize(9 * (size_t)n);
+  // no triangles: particles (points with dipole orientations d_nrm)
+  points_ = d_tri == nullptr;
+  if (points_ && mindlin) return IER_BADARG;
+  tri_u_.resize(points_ ? 1 : 9 * (size_t)n);
   src_u_.resize(3 * (size_t)n);
   tgt_u_.resize(3 * (size_t)nt);
-  EFMM_CUDA_TRY(cudaMemcpyAsync(tri_u_.get(), d_tri, 72 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+  if (!points_)
+    EFMM_CUDA_TRY(cudaMemcpyAsync(tri_u_.get(), d_tri, 72 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+  nu_u_.resize(3 * (size_t)n);
+  if (points_) {
+    if (d_nrm)
+      EFMM_CUDA_TRY(cudaMemcpyAsync(nu_u_.get(), d_nrm, 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
+    else
+      EFMM_CUDA_TRY(cudaMemsetAsync(nu_u_.get(), 0, 24 * (size_t)n, st_));
+  }
   EFMM_CUDA_TRY(cudaMemcpyAsync(src_u_.get(), d_src, 24 * (size_t)n, cudaMemcpyDeviceToDevice, st_));
   if (nt) EFMM_CUDA_TRY(cudaMemcpyAsync(tgt_u_.get(), d_tgt, 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
   auto now = [&]() {
@@ -367,12 +379,15 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   ier = build_lists(st_, tr_);
   if (ier) return ier;
   auto t2 = now();
-  tri_s_.resize(9 * (size_t)n);
+  tri_s_.resize(points_ ? 1 : 9 * (size_t)n);
   nrm_s_.resize(3 * (size_t)n);
   src_s_.resize(3 * (size_t)n);
   tgt_s_.resize(3 * (size_t)nt);
-  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 9, tr_.iz.get(), d_tri, tri_s_.get()); count_launch();
-  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_nrm, nrm_s_.get()); count_launch();
+  if (!points_) {
+    k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 9, tr_.iz.get(), d_tri, tri_s_.get()); count_launch();
+  }
+  k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), points_ ? nu_u_.get() : d_nrm, nrm_s_.get());
+  count_launch();
   k_gather<<<(n + 255) / 256, 256, 0, st_>>>(n, 3, tr_.iz.get(), d_src, src_s_.get()); count_launch();
   if (nt) { k_gather<<<(nt + 255) / 256, 256, 0, st_>>>(nt, 3, tr_.izt.get(), d_tgt, tgt_s_.get()); count_launch(); }
   build_worklists();
@@ -920,6 +935,7 @@ void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1
 int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d_sdl, double* d_u_src,
                    double* d_e_src, double* d_u_tgt, double* d_e_tgt, int mode, bool do_far) {
   switch_precision(false);
+  if (points_ && mode != 0) return IER_BADARG;  // particles: no stored near field
   int n = n_, nt = nt_;
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
   int do_src = (d_u_src || d_e_src) ? 1 : 0, do_tgt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? 1 : 0;
@@ -964,6 +980,8 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
     pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
     pa.mpole = mpole_.get();
+    pa.points = points_ ? 1 : 0;
+    pa.pts = src_s_.get();
     launch_p2m(st_, np2m_, pa);
     EFMM_CUDA_TRY(cudaEventRecord(ev_[2], st_));
     run_translations(m2m_, 4, ops_->mats.get(), mpole_.get(), mpole_.get());
@@ -992,7 +1010,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   EFMM_CUDA_TRY(cudaEventRecord(ev_[6], st_));
   // near field
   trir_.resize(n);
-  if (mode != 2)  // the stored operator replaces the triangle records
+  if (mode != 2 && !points_)  // the stored operator replaces the triangle records
     launch_tri_prep(st_, n, tri_s_.get(), nullptr, ssl_s_.get(), sdl_s_.get(), dosl, dodl, trir_.get());
   NearArgs na;
   na.nleaf = nnear_;
@@ -1005,7 +1023,11 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
   na.do_src = do_src; na.do_tgt = do_tgt;
   na.rlam = rlam; na.rmu = rmu;
   na.u_src = u_s_.get(); na.e_src = e_s_.get(); na.u_tgt = ut_s_.get(); na.e_tgt = et_s_.get();
-  if (mode == 0) {
+  if (points_) {
+    na.part_sl = dosl ? ssl_s_.get() : nullptr;
+    na.part_dl = dodl ? sdl_s_.get() : nullptr;
+    launch_near_points(st_, na, nrm_s_.get(), rlam, rmu);
+  } else if (mode == 0) {
     launch_near_leaf(st_, na);
   } else {
     // stored operator rows carry displacement and (if any output wants it) strain
@@ -1142,6 +1164,7 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
                          double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int precision,
                          int mode) {
   if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
+  if (points_) return IER_BADARG;  // particles: the single-right-hand-side FP64 form only
   switch_precision(precision == 1);
   MixedOrders orders(this, precision == 1);
   const int n = n_, nt = nt_;
@@ -1627,6 +1650,27 @@ int Plan::evaluate_direct(double rlam, double rmu, const double* d_ssl, const do
                           double* d_u_src, double* d_e_src, double* d_u_tgt, double* d_e_tgt, int nsub) {
   int n = n_, nt = nsub > 0 ? 0 : nt_;
   int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
+  if (points_) {  // particles: the point-pair direct sum, user order
+    const int ns = (d_u_src || d_e_src) ? (nsub > 0 ? std::min(nsub, n) : n) : 0;
+    const int ntt = (nt > 0 && (d_u_tgt || d_e_tgt)) ? nt : 0;
+    u_s_.resize(3 * (size_t)n);
+    e_s_.resize(6 * (size_t)n);
+    ut_s_.resize(3 * (size_t)std::max(nt, 1));
+    et_s_.resize(6 * (size_t)std::max(nt, 1));
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[0], st_));
+    launch_part_direct(st_, n, ns, src_u_.get(), d_ssl, d_sdl, nu_u_.get(), ntt, tgt_u_.get(), rlam, rmu, u_s_.get(),
+                       e_s_.get(), ut_s_.get(), et_s_.get());
+    EFMM_CUDA_TRY(cudaEventRecord(ev_[1], st_));
+    if (ns && d_u_src) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_src, u_s_.get(), 24 * (size_t)ns, cudaMemcpyDeviceToDevice, st_));
+    if (ns && d_e_src) { k_sym6to9<<<(ns + 255) / 256, 256, 0, st_>>>(ns, e_s_.get(), d_e_src); count_launch(); }
+    if (ntt && d_u_tgt) EFMM_CUDA_TRY(cudaMemcpyAsync(d_u_tgt, ut_s_.get(), 24 * (size_t)nt, cudaMemcpyDeviceToDevice, st_));
+    if (ntt && d_e_tgt) { k_sym6to9<<<(nt + 255) / 256, 256, 0, st_>>>(nt, et_s_.get(), d_e_tgt); count_launch(); }
+    EFMM_CUDA_TRY(cudaGetLastError());
+    EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+    cudaEventElapsedTime(&timings.near, ev_[0], ev_[1]);
+    timings.total = timings.near;
+    return IER_OK;
+  }
   trir_.resize(n);
   launch_tri_prep(st_, n, tri_u_.get(), nullptr, d_ssl, d_sdl, dosl, dodl, trir_.get());
   u_s_.resize(3 * (size_t)n);

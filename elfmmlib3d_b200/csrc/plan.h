@@ -207,6 +207,7 @@ class Plan {
   const Tree& tree() const { return tr_; }
   Timings timings;
   int n() const { return n_; }
+  bool points() const { return points_; }
   int nt() const { return nt_; }
   int order() const { return p_; }
   int nbox() const { return nbox_; }
@@ -343,6 +344,10 @@ class Plan {
   // depend on which form ran before.  Captured graphs are dropped with them.
   int last_mixed_ = -1;
   void switch_precision(bool mixed);
+  // particles (set_geometry with no triangles): sources are points, nrm the
+  // dipole orientations; the FP64 single-right-hand-side forms only
+  bool points_ = false;
+  DevBuf<double> nu_u_;  // dipole orientations, user order (direct sum)
   bool factored_ = true;  // translations in factored form when they fit
   bool p2m_unit_ = true;  // batched P2M through unit-density multipoles (else node products)
   template <class T>

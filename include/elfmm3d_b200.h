@@ -89,6 +89,41 @@ void elfmm3dtriaiter_(int *ier, const int *iprec, const double *rlam, const doub
                       double *ptfrc, const int *ifstrain, double *strain, const int *icomp_type,
                       double *wsave, const int *lwsave, int *lused);
 
+/* Replaces elfmm3dparttarg (src/elfmm3dpart.f:104-218): the particle FMM in
+ * free space.  Point forces sigma_sl(3,n) and point displacement
+ * discontinuities sigma_dl(3,n) with orientations sigma_dv(3,n) at
+ * source(3,n); displacement ptfrc(3,n) and strain(3,3,n) at the sources
+ * (self-interaction excluded) and at target(3,nt).  Same decomposition,
+ * tree and translations as the triangle FMM (one P2M node per source; near
+ * field by point pairs).  ier as elfmm3dtriatarg_. */
+void elfmm3dparttarg_(int *ier, const int *iprec, const double *rlam, const double *rmu, const int *nparts,
+                      const double *source, const int *ifsingle, const double *sigma_sl, const int *ifdouble,
+                      const double *sigma_dl, const double *sigma_dv, const int *ifptfrc, double *ptfrc,
+                      const int *ifstrain, double *strain, const int *ntargs, const double *target,
+                      const int *ifptfrctarg, double *ptfrctarg, const int *ifstraintarg, double *straintarg);
+
+/* Replaces elfmm3dpart (src/elfmm3dpart.f:52-102): as above, no targets. */
+void elfmm3dpart_(int *ier, const int *iprec, const double *rlam, const double *rmu, const int *nparts,
+                  const double *source, const int *ifsingle, const double *sigma_sl, const int *ifdouble,
+                  const double *sigma_dl, const double *sigma_dv, const int *ifptfrc, double *ptfrc,
+                  const int *ifstrain, double *strain);
+
+/* Replaces el3dpartdirecttarg (src/elfmm3dpart.f:506-712): the O(N^2)
+ * particle direct sum, on the GPU. */
+void el3dpartdirecttarg_(const double *rlam, const double *rmu, const int *nsource, const double *source,
+                         const int *ifsingle, const double *sigma_sl, const int *ifdouble, const double *sigma_dl,
+                         const double *sigma_dv, const int *ifptfrc, double *ptfrc, const int *ifstrain,
+                         double *strain, const int *ntarget, const double *target, const int *ifptfrctarg,
+                         double *ptfrctarg, const int *ifstraintarg, double *straintarg);
+
+/* Host evaluation of one (point, particle) pair of the particle near field
+ * (the decomposition the device uses): u[3], strain e6[6] (xx yy zz xy xz
+ * yz) at x of a point force sl and a point jump dl with orientation nu at y
+ * (either layer may be NULL).  No counterpart in the reference; the CPU
+ * check of the particle kernels. */
+int efmm_part_pair_host(double rlam, double rmu, const double *x, const double *y, const double *sl,
+                        const double *dl, const double *nu, double *u, double *e6);
+
 /* nrhs right-hand sides from host arrays (no counterpart in the reference):
  * geometry as in elfmm3dtriatarg_, sigma_sl/sigma_dl (3,n,nrhs) column-major
  * (NULL disables a layer), outputs ptfrc (3,n,nrhs), strain (3,3,n,nrhs),
