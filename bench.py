@@ -1426,7 +1426,7 @@ def run_uneven(args, rank, world, local_rank):
     probs = make_uneven_problems(w, world, rank)
     sizes = np.array([len(p[2]) for p in probs])
     evals = float(np.sum(sizes.astype(np.float64) ** 2))
-    workers = 4
+    workers = args.uneven_workers or max(4, min(16, host_threads()))
     for _ in range(max(1, args.warmup)):
         halfspace_many(probs[:8], iprec=w["iprec"], precision=1, workers=workers, device=local_rank)
     torch.cuda.synchronize()
@@ -1504,6 +1504,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=ncpu)
     ap.add_argument("--ref-sample", type=int, default=ncpu)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--uneven-workers", type=int, default=0,
+                    help="uneven batch: host worker threads (default: the host threads, 4 to 16)")
     ap.add_argument("--no-graph", action="store_true",
                     help="half-space batch: time plain passes instead of CUDA-graph replays (profiling)")
     args = ap.parse_args()
