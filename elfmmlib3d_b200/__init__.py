@@ -56,7 +56,8 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
            "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
-           "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host"]
+           "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host",
+           "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_"]
 
 
 class ElfmmError(RuntimeError):
@@ -257,12 +258,13 @@ def _part_args(source, sigma_sl, sigma_dl, sigma_dv):
 
 
 def elfmm3dparttarg(iprec, rlam, rmu, source, sigma_sl=None, sigma_dl=None, sigma_dv=None, target=None,
-                    ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1, direct=False):
+                    ifptfrc=1, ifstrain=1, ifptfrctarg=1, ifstraintarg=1, direct=False, halfspace=False):
     """Particle FMM in free space (src/elfmm3dpart.f:104; direct=True: the
-    O(N^2) el3dpartdirecttarg, :506): point forces sigma_sl (n,3), point
-    displacement discontinuities sigma_dl (n,3) with orientations sigma_dv
-    (n,3).  Returns (ier, ptfrc (n,3), strain (n,3,3), ptfrctarg (m,3),
-    straintarg (m,3,3))."""
+    O(N^2) el3dpartdirecttarg, :506) or, halfspace=True, in the Mindlin half
+    space z <= 0 (elhfmm3dparttarg / elh3dpartdirecttarg): point forces
+    sigma_sl (n,3), point displacement discontinuities sigma_dl (n,3) with
+    orientations sigma_dv (n,3).  Returns (ier, ptfrc (n,3), strain (n,3,3),
+    ptfrctarg (m,3), straintarg (m,3,3))."""
     L = load()
     _need_gpu()
     src, ssl, sdl, sdv, n = _part_args(source, sigma_sl, sigma_dl, sigma_dv)
@@ -273,12 +275,14 @@ def elfmm3dparttarg(iprec, rlam, rmu, source, sigma_sl=None, sigma_dl=None, sigm
     d = lambda a: a.ctypes.data_as(_dp)
     ier = ctypes.c_int(0)
     if direct:
-        L.el3dpartdirecttarg_(_byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src), _byref_i(sigma_sl is not None),
+        f = L.elh3dpartdirecttarg_ if halfspace else L.el3dpartdirecttarg_
+        f(_byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src), _byref_i(sigma_sl is not None),
                               d(ssl), _byref_i(sigma_dl is not None), d(sdl), d(sdv), _byref_i(ifptfrc), d(pt),
                               _byref_i(ifstrain), d(st), _byref_i(m), d(tg), _byref_i(ifptfrctarg), d(ptt),
                               _byref_i(ifstraintarg), d(stt))
     else:
-        L.elfmm3dparttarg_(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src),
+        f = L.elhfmm3dparttarg_ if halfspace else L.elfmm3dparttarg_
+        f(ctypes.byref(ier), _byref_i(iprec), _byref_d(rlam), _byref_d(rmu), _byref_i(n), d(src),
                            _byref_i(sigma_sl is not None), d(ssl), _byref_i(sigma_dl is not None), d(sdl), d(sdv),
                            _byref_i(ifptfrc), d(pt), _byref_i(ifstrain), d(st), _byref_i(m), d(tg),
                            _byref_i(ifptfrctarg), d(ptt), _byref_i(ifstraintarg), d(stt))

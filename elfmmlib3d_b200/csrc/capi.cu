@@ -412,6 +412,126 @@ int part_call(int iprec, double rlam, double rmu, int n, const double* src, int 
 }
 }  // namespace
 
+namespace {
+// The half-space particle FMM (src/elhfmm3dpart.f:47-498): the free-space
+// particle FMM (the direct arrival) plus the image part through the image
+// FMM with one P2M node per source and the image kernels at the points as
+// the near field, on the sources (self-interaction of the direct arrival
+// excluded; the image of a source acts on it) and on the targets.  Sources
+// and targets in z <= 0.  direct: the O(N^2) sums (elh3dpartdirecttarg).
+int hs_part_call(int iprec, double rlam, double rmu, int n, const double* src, int ifsingle, const double* ssl,
+                 int ifdouble, const double* sdl, const double* sdv, int ifptfrc, double* ptfrc, int ifstrain,
+                 double* strain, int nt, const double* tgt, int ifptfrctarg, double* ptfrctarg, int ifstraintarg,
+                 double* straintarg, bool direct) {
+  if (n < 1 || nt < 0) return IER_BADARG;
+  for (int i = 0; i < n; i++)
+    if (src[3 * i + 2] > 0.0) return IER_BADARG;
+  for (int i = 0; i < nt; i++)
+    if (tgt[3 * i + 2] > 0.0) return IER_BADARG;
+  int ier = part_call(iprec, rlam, rmu, n, src, ifsingle, ssl, ifdouble, sdl, sdv, ifptfrc, ptfrc, ifstrain, strain,
+                      nt, tgt, ifptfrctarg, ptfrctarg, ifstraintarg, straintarg, direct);
+  if (ier) return ier;
+  const bool on_src = ifptfrc || ifstrain, on_tgt = nt > 0 && (ifptfrctarg || ifstraintarg);
+  if (!on_src && !on_tgt) return IER_OK;
+  const int ns = on_src ? n : 0, m = ns + (on_tgt ? nt : 0);
+  std::vector<double> pts(3 * (size_t)m), ui(3 * (size_t)m), ei(9 * (size_t)m);
+  for (int i = 0; i < ns; i++)
+    for (int d = 0; d < 3; d++) pts[3 * i + d] = src[3 * i + d];
+  for (int i = 0; i < (on_tgt ? nt : 0); i++)
+    for (int d = 0; d < 3; d++) pts[3 * (size_t)(ns + i) + d] = tgt[3 * i + d];
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    efmm_plan* p = shared_plan();
+    if (!p) return IER_NODEVICE;
+    try {
+      cudaSetDevice(p->device);
+      HostCall& B = *g_bufs;  // made by part_call
+      cudaStream_t st = p->stream;
+      std::vector<double> refl(pts);
+      for (int i = 0; i < m; i++) refl[3 * i + 2] = -refl[3 * i + 2];
+      up(B.src, src, 3 * (size_t)n, st);
+      if (ifdouble) up(B.nrm, sdv, 3 * (size_t)n, st);
+      if (ifsingle) up(B.ssl, ssl, 3 * (size_t)n, st);
+      if (ifdouble) up(B.sdl, sdl, 3 * (size_t)n, st);
+      B.ut.resize(3 * (size_t)m);
+      B.et.resize(9 * (size_t)m);
+      const double* dssl = ifsingle ? B.ssl.get() : nullptr;
+      const double* dsdl = ifdouble ? B.sdl.get() : nullptr;
+      if (direct) {
+        up(B.tgt, pts.data(), 3 * (size_t)m, st);
+        B.u.resize(6 * (size_t)m);
+        launch_part_image(st, n, B.src.get(), dssl, dsdl, ifdouble ? B.nrm.get() : nullptr, m, B.tgt.get(), rlam, rmu,
+                          B.ut.get(), B.u.get());
+        std::vector<double> e6(6 * (size_t)m);
+        down(ui.data(), B.ut, 3 * (size_t)m, st);
+        down(e6.data(), B.u, 6 * (size_t)m, st);
+        EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+        for (int i = 0; i < m; i++) {
+          const double* q = &e6[6 * (size_t)i];
+          double* o = &ei[9 * (size_t)i];
+          o[0] = q[0]; o[4] = q[1]; o[8] = q[2];
+          o[1] = o[3] = q[3];
+          o[2] = o[6] = q[4];
+          o[5] = o[7] = q[5];
+        }
+      } else {
+        up(B.tgt, refl.data(), 3 * (size_t)m, st);
+        ier = p->plan->set_geometry(n, nullptr, ifdouble ? B.nrm.get() : nullptr, B.src.get(), m, B.tgt.get(), iprec,
+                                    false, true);
+        if (ier) return ier;
+        ier = p->plan->evaluate_image(rlam, rmu, 1, dssl, dsdl, B.ut.get(), B.et.get(), 0, 0);
+        if (ier) return ier;
+        down(ui.data(), B.ut, 3 * (size_t)m, st);
+        down(ei.data(), B.et, 9 * (size_t)m, st);
+        EFMM_CUDA_TRY(cudaStreamSynchronize(st));
+      }
+    } catch (const efmm::CudaError&) {
+      return IER_CUDA;
+    } catch (const std::bad_alloc&) {
+      return IER_ALLOC;
+    }
+  }
+  if (ifptfrc)
+    for (size_t k = 0; k < 3 * (size_t)n; k++) ptfrc[k] += ui[k];
+  if (ifstrain)
+    for (size_t k = 0; k < 9 * (size_t)n; k++) strain[k] += ei[k];
+  if (on_tgt && ifptfrctarg)
+    for (size_t k = 0; k < 3 * (size_t)nt; k++) ptfrctarg[k] += ui[3 * (size_t)ns + k];
+  if (on_tgt && ifstraintarg)
+    for (size_t k = 0; k < 9 * (size_t)nt; k++) straintarg[k] += ei[9 * (size_t)ns + k];
+  return IER_OK;
+}
+}  // namespace
+
+extern "C" void elhfmm3dparttarg_(int* ier, const int* iprec, const double* rlam, const double* rmu, const int* nparts,
+                                  const double* source, const int* ifsingle, const double* sigma_sl,
+                                  const int* ifdouble, const double* sigma_dl, const double* sigma_dv,
+                                  const int* ifptfrc, double* ptfrc, const int* ifstrain, double* strain,
+                                  const int* ntargs, const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                  const int* ifstraintarg, double* straintarg) {
+  *ier = hs_part_call(*iprec, *rlam, *rmu, *nparts, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv,
+                      *ifptfrc, ptfrc, *ifstrain, strain, *ntargs, target, *ifptfrctarg, ptfrctarg, *ifstraintarg,
+                      straintarg, false);
+}
+
+extern "C" void elhfmm3dpart_(int* ier, const int* iprec, const double* rlam, const double* rmu, const int* nparts,
+                              const double* source, const int* ifsingle, const double* sigma_sl, const int* ifdouble,
+                              const double* sigma_dl, const double* sigma_dv, const int* ifptfrc, double* ptfrc,
+                              const int* ifstrain, double* strain) {
+  *ier = hs_part_call(*iprec, *rlam, *rmu, *nparts, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv,
+                      *ifptfrc, ptfrc, *ifstrain, strain, 0, nullptr, 0, nullptr, 0, nullptr, false);
+}
+
+extern "C" void elh3dpartdirecttarg_(const double* rlam, const double* rmu, const int* nsource, const double* source,
+                                     const int* ifsingle, const double* sigma_sl, const int* ifdouble,
+                                     const double* sigma_dl, const double* sigma_dv, const int* ifptfrc,
+                                     double* ptfrc, const int* ifstrain, double* strain, const int* ntarget,
+                                     const double* target, const int* ifptfrctarg, double* ptfrctarg,
+                                     const int* ifstraintarg, double* straintarg) {
+  hs_part_call(2, *rlam, *rmu, *nsource, source, *ifsingle, sigma_sl, *ifdouble, sigma_dl, sigma_dv, *ifptfrc, ptfrc,
+               *ifstrain, strain, *ntarget, target, *ifptfrctarg, ptfrctarg, *ifstraintarg, straintarg, true);
+}
+
 extern "C" void elfmm3dparttarg_(int* ier, const int* iprec, const double* rlam, const double* rmu, const int* nparts,
                                  const double* source, const int* ifsingle, const double* sigma_sl,
                                  const int* ifdouble, const double* sigma_dl, const double* sigma_dv,

@@ -1145,7 +1145,7 @@ k_p2m_img(const P2MArgs a, int R, long long ubase, T* __restrict__ mpole) {
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
   const int t0 = a.sstart[box], tn = a.scount[box];
-  const int nnode = 12 * tn;
+  const int nnode = a.points ? tn : 12 * tn;
   constexpr int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
   double acc[CMAX][7][2];
 #pragma unroll
@@ -1160,15 +1160,23 @@ k_p2m_img(const P2MArgs a, int R, long long ubase, T* __restrict__ mpole) {
     __syncthreads();
     const int node = b0 + warp;
     if (node < nnode) {
-      const int it = t0 + node / 12, iq = node % 12;
-      const double* Tr = a.tri + 9 * (size_t)it;
-      double y[3];
-      for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
-      const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
-      const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
-      const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
-                            e1[0] * e2[1] - e1[1] * e2[0]};
-      const double w = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      int it;
+      double y[3], w;
+      if (a.points) {  // a particle: one node of weight 1
+        it = t0 + node;
+        for (int d = 0; d < 3; d++) y[d] = a.pts[3 * (size_t)it + d];
+        w = 1.0;
+      } else {
+        it = t0 + node / 12;
+        const int iq = node % 12;
+        const double* Tr = a.tri + 9 * (size_t)it;
+        for (int d = 0; d < 3; d++) y[d] = Q.b[iq][0] * Tr[d] + Q.b[iq][1] * Tr[3 + d] + Q.b[iq][2] * Tr[6 + d];
+        const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
+        const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
+        const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
+                              e1[0] * e2[1] - e1[1] * e2[0]};
+        w = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
+      }
       const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
       cplx* Y = Ys + (size_t)warp * nc;
       const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];

@@ -381,8 +381,15 @@ k_hs_store(const HsStoreArgs a, const int* __restrict__ chunk_leaf, const int* _
     const double X[3] = {xb[0], xb[1], -xb[2]};
     double acc[54];
     for (int k = 0; k < 54; k++) acc[k] = 0.0;
-    hs_pair_blk(a.tri + 9 * (size_t)tri, a.nrm + 3 * (size_t)tri, X, a.dosl, a.dodl, a.lam, a.mu, Q, a.eps, a.ncap,
-                acc);
+    if (a.points) {  // a particle: the kernel blocks at the point
+      const double* y = a.pts + 3 * (size_t)tri;
+      const double* nv = a.nrm + 3 * (size_t)tri;
+      if (a.dosl) mindlin_image_sl_blk(a.lam, a.mu, X[0], X[1], X[2], y[0], y[1], y[2], acc);
+      if (a.dodl) mindlin_image_dl_blk(a.lam, a.mu, X[0], X[1], X[2], y[0], y[1], y[2], nv[0], nv[1], nv[2], acc + 27);
+    } else {
+      hs_pair_blk(a.tri + 9 * (size_t)tri, a.nrm + 3 * (size_t)tri, X, a.dosl, a.dodl, a.lam, a.mu, Q, a.eps,
+                  a.ncap, acc);
+    }
     double* o = out + ((size_t)e * nt + t) * a.K;
     int w = 0;
     for (int layer = 0; layer < 2; layer++) {
@@ -430,6 +437,44 @@ void launch_hs_store(cudaStream_t st, const HsStoreArgs& a, int nchunk, const in
                      const int* chunk_e0, double* store) {
   if (nchunk <= 0) return;
   k_hs_store<<<nchunk, 128, 0, st>>>(a, chunk_leaf, chunk_e0, store);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+// The half-space particle direct sum of the image part: one thread per
+// target, all points (the reference's elh3dpartdirecttarg image terms).
+__global__ void __launch_bounds__(128, 1)
+k_part_image(int n, const double* __restrict__ src, const double* __restrict__ sl, const double* __restrict__ dl,
+             const double* __restrict__ nu, int m, const double* __restrict__ tgt, double lam, double mu,
+             double* __restrict__ u, double* __restrict__ e6) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const double X[3] = {tgt[3 * (size_t)i], tgt[3 * (size_t)i + 1], tgt[3 * (size_t)i + 2]};
+  double acc[9];
+  for (int k = 0; k < 9; k++) acc[k] = 0.0;
+  for (int j = 0; j < n; j++) {
+    const double* y = src + 3 * (size_t)j;
+    double o[9];
+    if (sl) {
+      mindlin_image_sl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], sl[3 * (size_t)j], sl[3 * (size_t)j + 1],
+                       sl[3 * (size_t)j + 2], o);
+      for (int k = 0; k < 9; k++) acc[k] += o[k];
+    }
+    if (dl) {
+      const double* nv = nu + 3 * (size_t)j;
+      mindlin_image_dl(lam, mu, X[0], X[1], X[2], y[0], y[1], y[2], dl[3 * (size_t)j], dl[3 * (size_t)j + 1],
+                       dl[3 * (size_t)j + 2], nv[0], nv[1], nv[2], o);
+      for (int k = 0; k < 9; k++) acc[k] += o[k];
+    }
+  }
+  for (int d = 0; d < 3; d++) u[3 * (size_t)i + d] = acc[d];
+  for (int d = 0; d < 6; d++) e6[6 * (size_t)i + d] = acc[3 + d];
+}
+
+void launch_part_image(cudaStream_t st, int n, const double* src, const double* sl, const double* dl,
+                       const double* nu, int m, const double* tgt, double lam, double mu, double* u, double* e6) {
+  if (n <= 0 || m <= 0) return;
+  k_part_image<<<(m + 127) / 128, 128, 0, st>>>(n, src, sl, dl, nu, m, tgt, lam, mu, u, e6);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }

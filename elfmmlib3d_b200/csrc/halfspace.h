@@ -20,6 +20,11 @@ void launch_hs_image(cudaStream_t st, int n, const double* tri, const double* nr
                      HsTri* work, double* u, double* e6);
 // tolerance of the image quadrature for iprec: min(1e-6, eps(iprec) / 10)
 double hs_quad_eps(int iprec);
+// The image part at targets (m,3) of point forces sl and point jumps dl
+// with orientations nu at the n points src (user order; null disables a
+// layer): u (m,3), e6 (m,6), overwritten.  The half-space particle direct sum.
+void launch_part_image(cudaStream_t st, int n, const double* src, const double* sl, const double* dl,
+                       const double* nu, int m, const double* tgt, double lam, double mu, double* u, double* e6);
 
 // Near field of the image FMM: the unit-density image responses of every
 // (target, near triangle) pair of each near leaf, written in the stored
@@ -38,6 +43,10 @@ struct HsStoreArgs {
   double lam, mu;
   double eps = 1e-6;     // adaptive tolerance of near-singular sub-triangles
   int* ncap = nullptr;   // sub-triangles kept at the depth cap (counter, may be null)
+  // particles: sources are the points pts (tree order), nrm their dipole
+  // orientations; a pair block is the image kernel at the point
+  int points = 0;
+  const double* pts = nullptr;
 };
 // The per-device counter of sub-triangles kept at the adaptive depth cap
 // (device address, for HsStoreArgs::ncap and launch_hs_image), and its value

@@ -345,7 +345,6 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   }
   // no triangles: particles (points with dipole orientations d_nrm)
   points_ = d_tri == nullptr;
-  if (points_ && mindlin) return IER_BADARG;
   tri_u_.resize(points_ ? 1 : 9 * (size_t)n);
   src_u_.resize(3 * (size_t)n);
   tgt_u_.resize(3 * (size_t)nt);
@@ -2160,6 +2159,7 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
                          double* d_u_tgt, double* d_e_tgt, int precision, int mode) {
   if (R < 1 || precision < 0 || precision > 1 || mode < 0 || mode > 2) return IER_BADARG;
   if (!mindlin_ || rmu <= 0 || rlam + 2 * rmu <= 0) return IER_BADARG;
+  if (points_ && (precision != 0 || 7 * R >= 32)) return IER_BADARG;  // particles: FP64, at most 4 right-hand sides
   switch_precision(precision == 1);
   const int nt = nt_;
   if (nt == 0 || !(d_u_tgt || d_e_tgt)) return IER_OK;
@@ -2253,6 +2253,8 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.c1 = 2.0 - al; pa.c2 = (2 * rlam + 3 * rmu) / (rlam + 2 * rmu); pa.inv2mu = 0.5 / rmu;
     pa.alpha = al; pa.lam = rlam; pa.mu = rmu;
     pa.C = Cv + Cu; pa.rstride = 1; pa.tstride = 3 * (long long)R; pa.dstride = R;
+    pa.points = points_ ? 1 : 0;
+    pa.pts = src_s_.get();
     if (mixed) {
       img_mp_f_.resize(tot);
       img_lc_f_.resize(tot);
@@ -2341,6 +2343,8 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     ha.lam = rlam; ha.mu = rmu;
     ha.eps = hs_quad_eps(iprec_);
     ha.ncap = hs_ncap_ptr();
+    ha.points = points_ ? 1 : 0;
+    ha.pts = src_s_.get();
     launch_hs_store(st_, ha, nchunk_, chunk_leaf_.get(), chunk_e0_.get(), store_.get());
     store_valid_ = true;
     store_gen_++;

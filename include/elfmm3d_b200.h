@@ -116,6 +116,32 @@ void el3dpartdirecttarg_(const double *rlam, const double *rmu, const int *nsour
                          double *strain, const int *ntarget, const double *target, const int *ifptfrctarg,
                          double *ptfrctarg, const int *ifstraintarg, double *straintarg);
 
+/* Replaces elhfmm3dparttarg (src/elhfmm3dpart.f:99-498): the particle FMM
+ * in the Mindlin half space z <= 0 (traction-free z = 0), arguments as
+ * elfmm3dparttarg_: the free-space particle FMM plus the image part (image
+ * FMM, one P2M node per source, the image kernels at the points as its near
+ * field).  Sources and targets in z <= 0, else ier 16. */
+void elhfmm3dparttarg_(int *ier, const int *iprec, const double *rlam, const double *rmu, const int *nparts,
+                       const double *source, const int *ifsingle, const double *sigma_sl, const int *ifdouble,
+                       const double *sigma_dl, const double *sigma_dv, const int *ifptfrc, double *ptfrc,
+                       const int *ifstrain, double *strain, const int *ntargs, const double *target,
+                       const int *ifptfrctarg, double *ptfrctarg, const int *ifstraintarg, double *straintarg);
+
+/* Replaces elhfmm3dpart (src/elhfmm3dpart.f:47-97): as above, no targets. */
+void elhfmm3dpart_(int *ier, const int *iprec, const double *rlam, const double *rmu, const int *nparts,
+                   const double *source, const int *ifsingle, const double *sigma_sl, const int *ifdouble,
+                   const double *sigma_dl, const double *sigma_dv, const int *ifptfrc, double *ptfrc,
+                   const int *ifstrain, double *strain);
+
+/* Replaces elh3dpartdirecttarg (listed in src/elfmm3dpart.f:33-36): the
+ * half-space particle direct sum (free-space pairs plus the image kernels
+ * of every source), on the GPU. */
+void elh3dpartdirecttarg_(const double *rlam, const double *rmu, const int *nsource, const double *source,
+                          const int *ifsingle, const double *sigma_sl, const int *ifdouble, const double *sigma_dl,
+                          const double *sigma_dv, const int *ifptfrc, double *ptfrc, const int *ifstrain,
+                          double *strain, const int *ntarget, const double *target, const int *ifptfrctarg,
+                          double *ptfrctarg, const int *ifstraintarg, double *straintarg);
+
 /* Host evaluation of one (point, particle) pair of the particle near field
  * (the decomposition the device uses): u[3], strain e6[6] (xx yy zz xy xz
  * yz) at x of a point force sl and a point jump dl with orientation nu at y

@@ -143,3 +143,47 @@ def test_particle_fmm_within_iprec_tolerance(gpu, iprec, layers):
     print(f"particles iprec {iprec} {layers}: {errs}")
     assert errs[0] < 2 * TOL[iprec] and errs[2] < 2 * TOL[iprec]
     assert errs[1] < 10 * TOL[iprec] and errs[3] < 10 * TOL[iprec]
+
+
+def _halfspace_cloud(n, m, seed):
+    src, tgt, sl, dl, dv = _cloud(n, m, seed)
+    src[:, 2] = -np.abs(src[:, 2]) - 0.05
+    tgt[:, 2] = -np.abs(tgt[:, 2]) - 0.01
+    return src, tgt, sl, dl, dv
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("iprec", [2, 3])
+def test_halfspace_particle_fmm_matches_direct(gpu, iprec):
+    src, tgt, sl, dl, dv = _halfspace_cloud(8000, 1500, 9 + iprec)
+    d = gpu.elfmm3dparttarg(iprec, 1.3, 0.7, src, sl, dl, dv, tgt, direct=True, halfspace=True)
+    ier, u, e, ut, et = gpu.elfmm3dparttarg(iprec, 1.3, 0.7, src, sl, dl, dv, tgt, halfspace=True)
+    assert ier == 0
+    errs = [rel(u, d[1]), rel(e, d[2]), rel(ut, d[3]), rel(et, d[4])]
+    print(f"half-space particles iprec {iprec}: {errs}")
+    assert errs[0] < 2 * TOL[iprec] and errs[2] < 2 * TOL[iprec]
+    assert errs[1] < 10 * TOL[iprec] and errs[3] < 10 * TOL[iprec]
+
+
+@pytest.mark.gpu
+def test_halfspace_particles_traction_free_surface(gpu):
+    """The total field of particles below the surface carries no traction
+    on z = 0 (lam tr(e) n + 2 mu e n with n = e_z), relative to the
+    free-space traction there."""
+    src, _, sl, dl, dv = _halfspace_cloud(400, 1, 3)
+    g = np.linspace(-1.5, 1.5, 9)
+    surf = np.array([[x, y, 0.0] for x in g for y in g])
+    ier, _, _, _, et = gpu.elfmm3dparttarg(3, 1.3, 0.7, src, sl, dl, dv, surf, ifptfrc=0, ifstrain=0,
+                                           halfspace=True)
+    assert ier == 0
+    _, _, _, _, ef = gpu.elfmm3dparttarg(3, 1.3, 0.7, src, sl, dl, dv, surf, ifptfrc=0, ifstrain=0)
+    tr = lambda E_: 1.3 * np.trace(E_, axis1=1, axis2=2)[:, None] * np.array([0, 0, 1.0]) + 2 * 0.7 * E_[:, :, 2]
+    assert np.abs(tr(et)).max() < 1e-7 * np.abs(tr(ef)).max()
+
+
+@pytest.mark.gpu
+def test_halfspace_particles_reject_points_above_the_surface(gpu):
+    src, tgt, sl, dl, dv = _halfspace_cloud(20, 3, 1)
+    src[0, 2] = 0.5
+    ier, *_ = gpu.elfmm3dparttarg(2, 1.0, 1.0, src, sl, None, None, tgt, halfspace=True)
+    assert ier == 16
