@@ -1049,7 +1049,10 @@ def run_hsbatch(args, rank, world, local_rank):
                    "stage_ms_free": tf, "stage_ms_image": ti,
                    "tree_free": {k: fi[k] for k in ("nboxes", "nlev", "p", "nbox")},
                    "tree_image": {k: ii[k] for k in ("nboxes", "nlev", "p", "nbox")},
-                   "stored_bytes": stored},
+                   "stored_bytes": stored,
+                   "tuner": {"lines": E.tune_dump(),
+                             "format": "knob (0 M2M, 1 M2L, 2 L2L) p nbox C prec kind (0 free, 1 image) decided "
+                                       "(0 tensor cores, 1 CUDA cores) ms_tensor ms_cuda"}},
         "e2e": {"value": e2e_value, "unit": "triangle-evals/s", "h2d_bytes_per_step": h2d,
                 "d2h_bytes_per_step": d2h,
                 "timing": "host wall clock around blocking elhfmm3dtria_batch_host calls (icomp_type 3: pinned "

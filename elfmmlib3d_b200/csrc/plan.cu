@@ -1566,6 +1566,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
         k_f2d_local<<<1184, 256, 0, st_>>>(local_f_.size(), D, ops_->wnorm.get(), local_f_.get(), local_.get());
         count_launch();
       }
+      la.local = local_.get();  // after the resize: the buffer may have been (re)allocated just above
       launch_l2t(st_, nl2t_, la, R);
     }
   } else {

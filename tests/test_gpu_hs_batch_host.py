@@ -5,8 +5,10 @@ through the free-space FMM plus the image part through the image FMM), the
 sum the reference's drivers form from an elfmm3dtriatarg and an
 elhfmm3dtriatargiter call (examples/elhfmm3dtria_self_iter_dr.f:331-385).
 The store call (icomp_type 2) and two replays with new densities
-(icomp_type 3, CUDA-graph replay) are checked; FP64 to 1e-10, the mixed form
-to its stated 1e-6 (displacement) / 1e-5 (strain)."""
+(icomp_type 3, CUDA-graph replay) are checked; FP64 to the FMM's own error
+at iprec 3 (the batched and the single-column passes take different routes
+to it: 2e-10 displacement, 6e-10 strain measured), the mixed form to its
+stated 1e-6 (displacement) / 1e-5 (strain)."""
 import numpy as np
 import pytest
 
@@ -26,7 +28,7 @@ def test_hs_batch_host_store_and_replay(gpu, precision):
     n, R = len(cen), 3
     rng = np.random.default_rng(5 + precision)
     ws = np.zeros(8)
-    tol_u, tol_e = (1e-10, 1e-10) if precision == 0 else (1e-6, 1e-5)
+    tol_u, tol_e = (2e-9, 5e-9) if precision == 0 else (1e-6, 1e-5)
     for call, icomp in enumerate((2, 3, 3)):
         sdl = rng.normal(size=(R, n, 3))
         ssl = rng.normal(size=(R, n, 3)) if precision == 0 else None
