@@ -1416,37 +1416,83 @@ def run_uneven(args, rank, world, local_rank):
     U[0, 360), dip U[15, 90], top depth U[0.5, 5] degrees / units, triangle
     count log-uniform in [nmin, nmax], one slip vector N(0,1) each), each a
     half-space self-evaluation at its centroids (direct arrival + image part)
-    in the mixed form, through `elfmmlib3d_b200.batch.halfspace_many` (worker
-    threads owning a plan pair each, problems from one queue, largest first).
-    A step = all problems, set-up (trees, lists) included, results back on
-    the host.  Errors against the FP64 direct sums on 200 centroids of every
-    8th problem (untimed)."""
+    in the mixed form.  Engine "forest" (default): all problems in one forest
+    (elfmmlib3d_b200.Forest: one free-space and one image plan over every
+    problem, each stage one launch over all problems' boxes); "plans": worker
+    threads owning a plan pair each (elfmmlib3d_b200.batch.halfspace_many).
+    A step = all problems, set-up (trees, lists) included.  value: inputs
+    resident on the device, CUDA events around each step; e2e: host arrays
+    in and out through elhfmm3dtria_many_host.  Errors of the timed results
+    against the FP64 direct sums on 200 centroids of every 8th problem and
+    against the oracle on the CPU sample (untimed)."""
     import torch
-    from elfmmlib3d_b200.batch import halfspace_many
+    import elfmmlib3d_b200 as E
+    from elfmmlib3d_b200.batch import halfspace_many, _check
     dev = torch.device("cuda", local_rank)
     torch.cuda.set_device(dev)
     w = WORKLOADS[args.workload]
     probs = make_uneven_problems(w, world, rank)
     sizes = np.array([len(p[2]) for p in probs])
+    counts = sizes.astype(np.int32)
+    off = np.concatenate([[0], np.cumsum(sizes)])
     evals = float(np.sum(sizes.astype(np.float64) ** 2))
+    engine = args.uneven_engine
     workers = args.uneven_workers or max(4, min(16, host_threads()))
+    h_tri = np.ascontiguousarray(np.concatenate([p[0].reshape(-1, 9) for p in probs]))
+    h_nrm = np.ascontiguousarray(np.concatenate([p[1] for p in probs]))
+    h_cen = np.ascontiguousarray(np.concatenate([p[2] for p in probs]))
+    h_sdl = np.ascontiguousarray(np.concatenate([p[4] for p in probs]))
+    d = lambda a: torch.tensor(a, dtype=torch.float64, device=dev)
+    tri, nrm, cen, sdl = d(h_tri), d(h_nrm), d(h_cen), d(h_sdl)
+    u = torch.zeros((len(h_cen), 3), dtype=torch.float64, device=dev)
+    e = torch.zeros((len(h_cen), 3, 3), dtype=torch.float64, device=dev)
+    F = E.Forest(local_rank) if engine == "forest" else None
+
+    def step():
+        if F is not None:
+            F.set_geometry(counts, tri, nrm, cen, iprec=w["iprec"])
+            F.evaluate(1.0, 1.0, None, sdl, u, e, precision=1)
+        else:
+            res, _ = halfspace_many(probs, iprec=w["iprec"], precision=1, workers=workers, device=local_rank,
+                                    engine="plans")
+            u.copy_(torch.from_numpy(np.concatenate([r[0] for r in res])))
+            e.copy_(torch.from_numpy(np.concatenate([r[1] for r in res])))
+
     for _ in range(max(1, args.warmup)):
-        halfspace_many(probs[:8], iprec=w["iprec"], precision=1, workers=workers, device=local_rank)
+        step()
     torch.cuda.synchronize()
-    l0 = __import__("elfmmlib3d_b200").kernel_launches()
+    l0 = E.kernel_launches()
     times = []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
-            _, info = halfspace_many(probs, iprec=w["iprec"], precision=1, workers=workers, device=local_rank)
-            times.append(info["seconds"])
-    launches = __import__("elfmmlib3d_b200").kernel_launches() - l0
+            torch.cuda.synchronize()
+            ev0.record()
+            step()
+            ev1.record()
+            torch.cuda.synchronize()
+            times.append(ev0.elapsed_time(ev1) * 1e-3)
+    launches = E.kernel_launches() - l0
     t = float(np.mean(times))
     t_max = max_over_ranks(t, world, dev)
     value = world * evals / t_max
-    sample = probs[::8]
-    _, cinfo = halfspace_many(sample, iprec=w["iprec"], precision=1, workers=workers, device=local_rank,
-                              check=200)
-    errs = np.array(cinfo["errors"])
+    uh, eh = u.cpu().numpy(), e.cpu().numpy()
+    res = [(uh[off[i]:off[i + 1]], eh[off[i]:off[i + 1]]) for i in range(len(probs))]
+    # e2e: host arrays through the C ABI, host wall clock
+    e2e_t = []
+    if engine == "forest":
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            ier, uu, ee = E.hs_many_host(w["iprec"], 1.0, 1.0, counts, h_tri, h_nrm, h_cen, None, h_sdl, precision=1)
+            e2e_t.append(time.perf_counter() - t0)
+            if ier:
+                raise E.ElfmmError(ier, "elhfmm3dtria_many_host")
+        e2e_err = float(max(np.linalg.norm(uu - uh) / np.linalg.norm(uh), np.linalg.norm(ee - eh) / np.linalg.norm(eh)))
+    if F is not None:
+        F.close()
+    checked = list(range(0, len(probs), 8))
+    errs = np.array([_check(probs[i], *res[i], min(200, int(sizes[i])), 1.0, 1.0, dev) for i in checked])
+    e2e_v = world * evals / max_over_ranks(float(np.mean(e2e_t)), world, dev) if e2e_t else value
     if rank != 0:
         return None
     cpu, oerr = None, None
@@ -1456,13 +1502,17 @@ def run_uneven(args, rank, world, local_rank):
                "sample": f"oracle half-space self-evaluation (free-space direct sum + image quadrature with "
                          f"distance refinement) at {npts} centroids of {len(uneven_sample_problems(probs))} "
                          f"evenly spaced problems, against all of their problem's triangles ({dt:.1f} s)"}
-        # per-problem errors of the mixed form against the oracle at those centroids
-        sp = uneven_sample_problems(probs)
-        res, _ = halfspace_many(sp, iprec=w["iprec"], precision=1, workers=workers, device=local_rank)
-        per = [oracle_errors(ref, uu, ee) for ref, (uu, ee) in zip(refs, res)]
-        oerr = {"problems": len(per), "triangles": [int(len(p_[2])) for p_ in sp],
+        # per-problem errors of the timed results against the oracle at those centroids
+        sidx = list(range(len(probs)))[::max(1, len(probs) // 16)]
+        per = [oracle_errors(ref, res[i][0], res[i][1]) for ref, i in zip(refs, sidx)]
+        oerr = {"problems": len(per), "triangles": [int(sizes[i]) for i in sidx],
                 "u": [x.get("u") for x in per], "strain": [x.get("strain") for x in per],
                 "u_max": max(x.get("u") or 0.0 for x in per), "strain_max": max(x.get("strain") or 0.0 for x in per)}
+    forest_step = ("one forest of all problems: the problems moved side by side in x and y, one per column of "
+                   "boxes of a common root; set_geometry of its free-space and image plan (trees, lists, "
+                   "work lists), the mixed pass of each over all problems' boxes (one right-hand side)")
+    plans_step = ("every problem: set_geometry of a free-space and an image plan, the mixed batch pass of each "
+                  "(one right-hand side), results to host; worker threads over one queue (largest first)")
     return {
         "metric": "triangle-evals/s (batched uneven half-space geometries, mixed precision)",
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -1470,11 +1520,11 @@ def run_uneven(args, rank, world, local_rank):
         "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": args.workload, "problems": len(probs), "triangles_total": int(sizes.sum()),
                    "triangles_min_median_max": [int(sizes.min()), int(np.median(sizes)), int(sizes.max())],
-                   "evals_per_step": evals, "iprec": w["iprec"], "workers": workers,
-                   "step": "every problem: set_geometry of a free-space and an image plan, the mixed batch "
-                           "pass of each (one right-hand side), results to host; worker threads over one "
-                           "queue (largest first)",
-                   "rel_err_vs_direct": {"problems_checked": len(sample), "centroids_each": 200,
+                   "evals_per_step": evals, "iprec": w["iprec"], "engine": engine,
+                   "workers": workers if engine == "plans" else None,
+                   "step": forest_step if engine == "forest" else plans_step,
+                   "l2": "inputs (geometry > 300 MB) larger than L2",
+                   "rel_err_vs_direct": {"problems_checked": len(checked), "centroids_each": 200,
                                          "u_max": float(errs[:, 0].max()),
                                          "u_median": float(np.median(errs[:, 0])),
                                          "strain_max": float(errs[:, 1].max()),
@@ -1483,10 +1533,12 @@ def run_uneven(args, rank, world, local_rank):
                    "rel_err_vs_oracle_sample": "per sampled problem, the cpu_baseline sample's centroids",
                    "parallelism": (f"problems{world}: {w['nprob']} x {world} problems, greedy n^2 balance "
                                    "across ranks, no exchange") if world > 1 else "1 GPU"},
-        "e2e": {"value": value, "unit": "triangle-evals/s", "h2d_bytes_per_step": int(sizes.sum() * 8 * (9 + 3 + 3 + 3)),
+        "e2e": {"value": e2e_v, "unit": "triangle-evals/s", "h2d_bytes_per_step": int(sizes.sum() * 8 * (9 + 3 + 3 + 3)),
                 "d2h_bytes_per_step": int(sizes.sum() * 8 * 12),
-                "timing": "host wall clock: geometry and slip vectors from host memory, results back, every "
-                          "problem"},
+                "timing": ("host wall clock around elhfmm3dtria_many_host: geometry and slip vectors from host "
+                           f"memory, results back (max relative difference from the device-resident step "
+                           f"{e2e_err:.1e})") if e2e_t else "the device-resident step (plans engine copies "
+                           "every problem from the host already)"},
         "gpu_launches": launches // max(1, args.steps),
         "roofline": None,
         "cpu_baseline": cpu,
@@ -1507,6 +1559,8 @@ def main():
     ap.add_argument("--cpu-sample", type=int, default=ncpu)
     ap.add_argument("--ref-sample", type=int, default=ncpu)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--uneven-engine", default="forest", choices=["forest", "plans"],
+                    help="uneven batch: one forest of all problems, or worker threads over per-problem plans")
     ap.add_argument("--uneven-workers", type=int, default=0,
                     help="uneven batch: host worker threads (default: the host threads, 4 to 16)")
     ap.add_argument("--no-graph", action="store_true",

@@ -57,7 +57,9 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
            "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
            "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host",
-           "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_"]
+           "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_", "efmm_plan_set_forest",
+           "efmm_forest_create", "efmm_forest_destroy", "efmm_forest_set_geometry", "efmm_forest_evaluate",
+           "efmm_forest_plan", "efmm_forest_layout", "elhfmm3dtria_many_host"]
 
 
 class ElfmmError(RuntimeError):
@@ -134,6 +136,23 @@ def load():
     L.elhfmm3dtria_batch_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _dp, _dp,
                                           _dp, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, _dp,
                                           ctypes.c_int]
+    L.efmm_plan_set_forest.restype = ctypes.c_int
+    L.efmm_plan_set_forest.argtypes = [_vp, _dp]
+    L.efmm_forest_create.restype = _vp
+    L.efmm_forest_create.argtypes = [ctypes.c_int]
+    L.efmm_forest_destroy.argtypes = [_vp]
+    L.efmm_forest_set_geometry.restype = ctypes.c_int
+    L.efmm_forest_set_geometry.argtypes = [_vp, ctypes.c_int, _ip, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int]
+    L.efmm_forest_evaluate.restype = ctypes.c_int
+    L.efmm_forest_evaluate.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, ctypes.c_int,
+                                       ctypes.c_int]
+    L.efmm_forest_plan.restype = _vp
+    L.efmm_forest_plan.argtypes = [_vp, ctypes.c_int]
+    L.efmm_forest_layout.restype = ctypes.c_int
+    L.efmm_forest_layout.argtypes = [ctypes.c_int, _dp, _dp, _dp]
+    L.elhfmm3dtria_many_host.restype = ctypes.c_int
+    L.elhfmm3dtria_many_host.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int, _ip, _dp,
+                                         _dp, _dp, _dp, _dp, _dp, _dp, ctypes.c_int]
     L.efmm_tri_read.restype = ctypes.c_int
     L.efmm_tri_read.argtypes = [ctypes.c_char_p, _dp, ctypes.c_int, _ip, _ip, ctypes.c_int, _ip]
     L.efmm_tri_write.restype = ctypes.c_int
@@ -813,9 +832,83 @@ class Plan:
         return dict(boxes=boxes, iz=iz[:self.n], iztarg=izt[:self.nt], laddr=laddr, center=cs[:3],
                     size=cs[3], lists=lists)
 
+    def set_forest(self, forest):
+        """Forest of independent problems for the following set_geometry
+        calls (efmm_plan_set_forest): (centre x, y, z, side, level), or None."""
+        f = None if forest is None else np.ascontiguousarray(forest, dtype=np.float64).reshape(5)
+        ier = self._L.efmm_plan_set_forest(self._h, f.ctypes.data_as(_dp) if f is not None else None)
+        if ier:
+            raise ElfmmError(ier, "set_forest")
+
+    @classmethod
+    def _view(cls, L, h, n, nt):
+        """A non-owning Plan over handle h (a forest's plan)."""
+        v = cls.__new__(cls)
+        v._L, v._h, v._owned, v.n, v.nt = L, h, False, n, nt
+        return v
+
+    def close(self):
+        if getattr(self, "_h", None) and getattr(self, "_owned", True):
+            self._L.efmm_plan_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def forest_layout(bb):
+    """The forest placement (efmm_forest_layout, host code): bb (nprob,6)
+    centroid boxes (min x, y, z, max x, y, z) -> (root (5,), shift (nprob,2))."""
+    L = load()
+    bb = _c(bb, (-1, 6))
+    root, shift = np.zeros(5), np.zeros((bb.shape[0], 2))
+    ier = L.efmm_forest_layout(bb.shape[0], bb.ctypes.data_as(_dp), root.ctypes.data_as(_dp),
+                               shift.ctypes.data_as(_dp))
+    if ier:
+        raise ElfmmError(ier, "forest_layout")
+    return root, shift
+
+
+class Forest:
+    """Many independent half-space problems in one pass (efmm_forest_*):
+    device arrays (torch CUDA tensors or addresses) concatenated in problem
+    order, counts = triangles per problem."""
+
+    def __init__(self, device=0):
+        L = load()
+        _need_gpu()
+        self._L = L
+        self._h = L.efmm_forest_create(int(device))
+        if not self._h:
+            raise ElfmmError(1024, f"cannot create forest on device {device}")
+        self.n = 0
+
+    def set_geometry(self, counts, tri, nrm, cen, iprec=2, iter=False):
+        c = np.ascontiguousarray(counts, dtype=np.int32)
+        ier = self._L.efmm_forest_set_geometry(self._h, len(c), c.ctypes.data_as(_ip), Plan._ptr(tri),
+                                               Plan._ptr(nrm), Plan._ptr(cen), int(iprec), int(iter))
+        if ier:
+            raise ElfmmError(ier, "forest set_geometry")
+        self.n = int(c.sum())
+
+    def evaluate(self, rlam, rmu, ssl=None, sdl=None, u=None, e=None, precision=1, mode=0):
+        """Half-space u (n,3), e (n,3,3) at every problem's centroids."""
+        ier = self._L.efmm_forest_evaluate(self._h, float(rlam), float(rmu), Plan._ptr(ssl), Plan._ptr(sdl),
+                                           Plan._ptr(u), Plan._ptr(e), int(precision), int(mode))
+        if ier:
+            raise ElfmmError(ier, "forest evaluate")
+
+    def plan(self, which):
+        """The free-space (0) or image (1) plan, as a non-owning Plan."""
+        h = self._L.efmm_forest_plan(self._h, int(which))
+        return Plan._view(self._L, h, self.n, 0 if which == 0 else self.n)
+
     def close(self):
         if getattr(self, "_h", None):
-            self._L.efmm_plan_destroy(self._h)
+            self._L.efmm_forest_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -823,3 +916,23 @@ class Plan:
             self.close()
         except Exception:
             pass
+
+
+def hs_many_host(iprec, rlam, rmu, counts, triangle, trinorm, centroids, sigma_sl=None, sigma_dl=None,
+                 precision=1):
+    """elhfmm3dtria_many_host: the half-space self-evaluation of many
+    independent problems from host arrays concatenated in problem order.
+    Returns (ier, u (n,3), strain (n,3,3))."""
+    L = load()
+    _need_gpu()
+    c = np.ascontiguousarray(counts, dtype=np.int32)
+    tri = _c(triangle, (-1, 3, 3))
+    n = tri.shape[0]
+    nrm, cen = _c(trinorm, (n, 3)), _c(centroids, (n, 3))
+    ssl = _c(sigma_sl, (n, 3)) if sigma_sl is not None else None
+    sdl = _c(sigma_dl, (n, 3)) if sigma_dl is not None else None
+    u, e = np.zeros((n, 3)), np.zeros((n, 3, 3))
+    p = lambda a: a.ctypes.data_as(_dp) if a is not None else None
+    ier = L.elhfmm3dtria_many_host(int(iprec), float(rlam), float(rmu), len(c), c.ctypes.data_as(_ip), p(tri),
+                                   p(nrm), p(cen), p(ssl), p(sdl), p(u), p(e), int(precision))
+    return ier, u, e

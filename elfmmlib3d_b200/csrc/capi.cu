@@ -6,6 +6,7 @@
 #include <mutex>
 #include <vector>
 #include "plan.h"
+#include "capi_plan.h"
 #include "halfspace.h"
 #include "solve.h"
 #include "harmonics.cuh"
@@ -14,12 +15,6 @@
 
 using namespace efmm;
 
-struct efmm_plan {
-  int device;
-  cudaStream_t stream;
-  std::unique_ptr<Plan> plan;
-  cudaEvent_t user_ev[8];
-};
 
 static int env_device() {
   const char* s = getenv("ELFMM3D_DEVICE");
@@ -91,6 +86,14 @@ extern "C" int efmm_plan_evaluate_direct_subset(efmm_plan* p, double rlam, doubl
                                                 double* e_src) {
   if (!p || nsub < 1) return IER_BADARG;
   EFMM_GUARD(return p->plan->evaluate_direct(rlam, rmu, ssl, sdl, u_src, e_src, nullptr, nullptr, nsub);)
+}
+
+extern "C" int efmm_plan_set_forest(efmm_plan* p, const double* forest) {
+  if (!p) return IER_BADARG;
+  if (forest && (!(forest[3] > 0.0) || forest[4] < 1.0 || forest[4] > 15.0 || forest[4] != (int)forest[4]))
+    return IER_BADARG;
+  p->plan->set_forest(forest);
+  return IER_OK;
 }
 
 extern "C" int efmm_plan_evaluate_batch(efmm_plan* p, double rlam, double rmu, int nrhs, const double* ssl,

@@ -372,7 +372,8 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   p2m_waves_.clear();  // the leaf lists change with the geometry
   l2t_waves_.clear();
   graph_reset();
-  int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_);
+  if (forest_on_ && mindlin && forest_[2] != 0.0) return IER_BADARG;  // the Mindlin root is centred on z = 0
+  int ier = build_tree(st_, n, d_src, nt, d_tgt, nbox_, mindlin ? 1 : 0, tr_, forest_on_ ? forest_ : nullptr);
   if (ier) return ier;
   auto t1 = now();
   ier = build_lists(st_, tr_);

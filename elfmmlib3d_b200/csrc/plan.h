@@ -145,6 +145,13 @@ class Plan {
   // geometry in user order, device pointers: tri (n,3,3), nrm (n,3), src (n,3), tgt (nt,3)
   int set_geometry(int n, const double* d_tri, const double* d_nrm, const double* d_src, int nt,
                    const double* d_tgt, int iprec, bool iter, bool mindlin);
+  // A forest of independent problems for the following set_geometry calls:
+  // f5 = {root centre x, y, z, root side, level} as build_tree's forest (the
+  // Mindlin root needs centre z = 0); null: one problem.
+  void set_forest(const double* f5) {
+    forest_on_ = f5 != nullptr;
+    for (int i = 0; i < 5; i++) forest_[i] = f5 ? f5[i] : 0.0;
+  }
   // densities in user order (device); outputs in user order (device):
   // u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3); null pointers disable them.
   // mode 0: analytic near field; 1: compute and store the near-field
@@ -232,6 +239,8 @@ class Plan {
   int build_image_sched();
   void build_chunks(int do_src, int do_tgt);
   bool mindlin_ = false, img_sched_ = false;
+  bool forest_on_ = false;
+  double forest_[5] = {0, 0, 0, 0, 0};
   TransSched m2lv_img_, m2lu_, l2l_img_, l2l_img_u_, m2m_u_;
   template <class T>
   void p2m_img_twostage(const P2MArgs& pa, int R, T* mpole);

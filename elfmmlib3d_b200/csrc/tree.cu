@@ -16,6 +16,13 @@
 // keep their place), and children are created from per-box digit counts.
 // Lists: 5 (colleagues) and 2 from the parent's colleagues' children, 1 and 3
 // from a depth-first walk below each leaf's colleagues, 4 as the dual of 3.
+//
+// Forest (no counterpart in the reference): many independent problems in one
+// tree.  The caller places problem k in its own column of boxes of level L
+// (grid position (i, j) of that level, all k) and gives the root cube; every
+// box above level L splits, and boxes of different columns are never
+// colleagues, so every list stays inside one problem and each problem sees
+// the FMM of the subtree below its column.
 #include <cub/cub.cuh>
 #include <vector>
 #include <algorithm>
@@ -60,11 +67,13 @@ __global__ void k_bbox(int n, const double* __restrict__ p, double* out /* 6: mi
   }
 }
 
-__global__ void k_split(int lo, int hi, int nbox, const int* __restrict__ scount,
+// every box of a level below `force` splits (the levels above a forest's
+// problems), others while they hold more than nbox sources or targets
+__global__ void k_split(int lo, int hi, int nbox, int force, const int* __restrict__ scount,
                         const int* __restrict__ tcount, int* __restrict__ split) {
   int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= hi) return;
-  split[b - lo] = (scount[b] > nbox || tcount[b] > nbox) ? 1 : 0;
+  split[b - lo] = (force || scount[b] > nbox || tcount[b] > nbox) ? 1 : 0;
 }
 
 // digit + key for every point; counts per (split box, digit)
@@ -179,8 +188,21 @@ __device__ bool touch(const TreeDev& T, int a, int b) {
   return true;
 }
 
+// Problem of box b in a forest: its grid column (i, j) at level T.flev, -1
+// above that level (boxes that hold several problems); 0 without a forest.
+__device__ __forceinline__ int fcol(const TreeDev& T, int b) {
+  if (T.flev < 0) return 0;
+  const int l = T.level[b];
+  if (l < T.flev) return -1;
+  const int sh = l - T.flev;
+  return ((T.ijk[3 * b] - 1) >> sh) + (((T.ijk[3 * b + 1] - 1) >> sh) << T.flev);
+}
+
 // lists 5 and 2 for boxes of one level.  coll: 27 slots per box.
-// mode 0: count list-2 entries; mode 1: write them at l2_off.
+// mode 0: count list-2 entries; mode 1: write them at l2_off.  In a forest,
+// boxes of different problems are neither colleagues nor in list 2, and the
+// boxes above the problems' level (colleagues among themselves, so that the
+// level below finds its colleagues) have no list 2.
 __global__ void k_list52(TreeDev T, int lo, int hi, int mode, int* __restrict__ l2cnt,
                          const int* __restrict__ l2off, int* __restrict__ l2items) {
   int b = lo + blockIdx.x * blockDim.x + threadIdx.x;
@@ -188,15 +210,19 @@ __global__ void k_list52(TreeDev T, int lo, int hi, int mode, int* __restrict__ 
   int dad = T.parent[b];
   int nc = 0, n2 = 0;
   int w = mode ? l2off[b] : 0;
+  const int fb = fcol(T, b);
   for (int i = 0; i <= T.ncoll[dad]; i++) {
     int c = (i == 0) ? dad : T.coll[27 * dad + i - 1];
     for (int q = 0; q < T.nkids[c]; q++) {
       int kid = T.kids[8 * c + q];
       if (kid == b) continue;
+      const int fk = fcol(T, kid);
       if (touch(T, kid, b)) {
+        if (fk != fb) continue;
         if (mode == 0) T.coll[27 * b + nc] = kid;
         nc++;
       } else {
+        if (fk != fb || fb < 0) continue;
         if (mode == 1) l2items[w + n2] = kid;
         n2++;
       }
@@ -341,26 +367,20 @@ __global__ void k_transpose_pairs(int np, const int2* __restrict__ in, int2* __r
   out[i] = make_int2(in[i].y, in[i].x);
 }
 
-int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double* d_tgt, int nbox,
-               int mindlin, Tree& tr) {
-  if (n < 1) return IER_BADARG;
-  TreeScratch& S = tr.scr;
-  DevBuf<char>& tmp = S.tmp;
-  tr.n = n;
-  tr.nt = nt;
-  // ---- root
-  DevBuf<double>& bb = S.bb;
+// The reference's root (src/d3tstrcr.f:31 d3tstrcr, src/d3tstrcr_mindlin.f:
+// 1380): centre and side of the bounding cube of sources and targets; the
+// Mindlin variant centres it on z = 0 with side >= 2 max|z|.
+static void bounding_root(cudaStream_t st, int n, const double* d_src, int nt, const double* d_tgt, int mindlin,
+                          DevBuf<double>& bb, double* c0, double& size) {
   bb.resize(6);
-  {
-    unsigned long long init[6];
-    for (int c = 0; c < 3; c++) {
-      init[c] = ~0ull;
-      init[3 + c] = 0ull;
-    }
-    EFMM_CUDA_TRY(cudaMemcpyAsync(bb.get(), init, sizeof(init), cudaMemcpyHostToDevice, st));
-    k_bbox<<<148, 256, 0, st>>>(n, d_src, bb.get()); count_launch();
-    if (nt > 0) { k_bbox<<<148, 256, 0, st>>>(nt, d_tgt, bb.get()); count_launch(); }
+  unsigned long long init[6];
+  for (int c = 0; c < 3; c++) {
+    init[c] = ~0ull;
+    init[3 + c] = 0ull;
   }
+  EFMM_CUDA_TRY(cudaMemcpyAsync(bb.get(), init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_bbox<<<148, 256, 0, st>>>(n, d_src, bb.get()); count_launch();
+  if (nt > 0) { k_bbox<<<148, 256, 0, st>>>(nt, d_tgt, bb.get()); count_launch(); }
   std::vector<unsigned long long> hb = to_host((unsigned long long*)bb.get(), 6, st);
   double mn[3], mx[3];
   for (int c = 0; c < 3; c++) {
@@ -373,15 +393,35 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     mn[c] = dec(hb[c]);
     mx[c] = dec(hb[3 + c]);
   }
-  double size = mx[0] - mn[0], sy = mx[1] - mn[1], sz = mx[2] - mn[2];
+  size = mx[0] - mn[0];
+  const double sy = mx[1] - mn[1], sz = mx[2] - mn[2];
   if (sy > size) size = sy;
   if (sz > size) size = sz;
-  for (int c = 0; c < 3; c++) tr.c0[c] = (mn[c] + mx[c]) / 2;
+  for (int c = 0; c < 3; c++) c0[c] = (mn[c] + mx[c]) / 2;
   if (mindlin) {
-    double distz = fabs(mn[2]) > fabs(mx[2]) ? fabs(mn[2]) : fabs(mx[2]);
-    tr.c0[2] = 0.0;
+    const double distz = fabs(mn[2]) > fabs(mx[2]) ? fabs(mn[2]) : fabs(mx[2]);
+    c0[2] = 0.0;
     if (2 * distz > size) size = 2 * distz;
   }
+}
+
+int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double* d_tgt, int nbox,
+               int mindlin, Tree& tr, const double* forest) {
+  if (n < 1) return IER_BADARG;
+  TreeScratch& S = tr.scr;
+  DevBuf<char>& tmp = S.tmp;
+  tr.n = n;
+  tr.nt = nt;
+  tr.flev = -1;
+  double size = 0.0;
+  if (forest) {
+    if (!(forest[3] > 0.0) || forest[4] < 1.0 || forest[4] > 15.0) return IER_BADARG;
+    for (int c = 0; c < 3; c++) tr.c0[c] = forest[c];
+    size = forest[3];
+    tr.flev = (int)forest[4];
+  }
+  // ---- root: the given cube of a forest, else the points' bounding cube
+  if (!forest) bounding_root(st, n, d_src, nt, d_tgt, mindlin, S.bb, tr.c0, size);
   tr.size = size;
 
   // ---- boxes (grown per level)
@@ -452,7 +492,8 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     off.resize(nl);
     cs.zero(st);
     ct.zero(st);
-    k_split<<<(nl + 255) / 256, 256, 0, st>>>(lo, hi, nbox, tr.scount.get(), tr.tcount.get(), split.get()); count_launch();
+    k_split<<<(nl + 255) / 256, 256, 0, st>>>(lo, hi, nbox, lev < tr.flev ? 1 : 0, tr.scount.get(),
+                                              tr.tcount.get(), split.get()); count_launch();
     double side = size / (double)(1ull << lev);
     k_digits<<<(n + 255) / 256, 256, 0, st>>>(n, d_src, tr.iz.get(), pbs.get(), tr.level.get(), lev, lo,
                                               split.get(), tr.ijk.get(), tr.sstart.get(), tr.c0[0],

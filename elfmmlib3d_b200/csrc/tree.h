@@ -13,6 +13,10 @@ struct TreeDev {
   int *coll, *ncoll;
   double c0[3];
   double size;
+  // forest of independent problems (flev >= 0): each column of boxes of
+  // level flev (one (i, j) grid position, every k) holds one problem, and
+  // only boxes of the same column below flev interact
+  int flev;
 };
 
 // Device scratch of the tree and list builds, kept between builds so that a
@@ -33,6 +37,7 @@ struct TreeScratch {
 struct Tree {
   int n = 0, nt = 0, nboxes = 0, nlev = 0;
   double c0[3] = {0, 0, 0}, size = 0;
+  int flev = -1;  // forest level (TreeDev::flev), -1: one problem
   DevBuf<int> level, ijk, parent, kids, nkids, sstart, scount, tstart, tcount;
   DevBuf<int> iz, izt;
   std::vector<std::pair<int, int>> laddr;  // (first box, count) per level
@@ -47,12 +52,16 @@ struct Tree {
     t.tstart = tstart.get(); t.tcount = tcount.get(); t.coll = coll.get(); t.ncoll = ncoll.get();
     for (int c = 0; c < 3; c++) t.c0[c] = c0[c];
     t.size = size;
+    t.flev = flev;
     return t;
   }
 };
 
+// forest (may be null): {c0x, c0y, c0z, size, level} -- the given root cube
+// instead of the points' bounding cube, every box above `level` split, and
+// the lists of build_lists restricted to the columns of that level.
 int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double* d_tgt, int nbox,
-               int mindlin, Tree& tr);
+               int mindlin, Tree& tr, const double* forest = nullptr);
 int build_lists(cudaStream_t st, Tree& tr);
 
 }  // namespace efmm

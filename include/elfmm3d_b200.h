@@ -243,6 +243,16 @@ int efmm_plan_set_geometry(efmm_plan *plan, int n, const double *tri, const doub
                            const double *src, int nt, const double *tgt, int iprec, int iter,
                            int mindlin);
 
+/* A forest of independent problems for the plan's following set_geometry
+ * calls (no counterpart in the reference): forest = {root centre x, y, z,
+ * root side, level L} -- the tree's root is this cube instead of the
+ * points' bounding cube, every box above level L splits, and boxes of
+ * different columns of level L (grid positions (i, j), any k) are never
+ * neighbours, so the problems placed one per column do not interact.  A
+ * Mindlin plan needs centre z = 0.  NULL: one problem (the default).  L in
+ * 1..15; ier 16 otherwise. */
+int efmm_plan_set_forest(efmm_plan *plan, const double *forest);
+
 /* Evaluate with device densities ssl/sdl (n,3; NULL disables a layer) into
  * device outputs u_src (n,3), e_src (n,3,3), u_tgt (nt,3), e_tgt (nt,3,3)
  * (NULL disables an output).  Blocks until the results are complete. */
@@ -522,6 +532,54 @@ int efmm_tune_dump(char *buf, int len);
  * operators in *rel (_device: *timeout != 0 if a bounded wait ran out). */
 int efmm_rot_tc_selfcheck(int p, unsigned seed, double *rel);
 int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double *rel, int *timeout);
+
+/* ---- many independent half-space problems in one pass -----------------
+ * (no counterpart in the reference, whose drivers evaluate one fault per
+ * call: the half-space self-evaluation of examples/elhfmm3dtria_self_iter_dr.f
+ * :331-385, direct arrival plus image part, for every problem).  The
+ * problems are moved side by side in x and y (z kept: the half-space kernels
+ * depend on x and y through differences only), one per column of boxes of a
+ * common root cube centred on z = 0, and one free-space plan and one image
+ * plan are built over all of them as a forest (efmm_plan_set_forest): every
+ * stage of both passes is one launch over the boxes of all problems. */
+typedef struct efmm_forest efmm_forest;
+
+efmm_forest *efmm_forest_create(int device);
+void efmm_forest_destroy(efmm_forest *forest);
+
+/* The problems' geometry, device arrays concatenated in problem order:
+ * counts (host, nprob) triangles per problem, tri (n,3,3), nrm (n,3),
+ * centroids cen (n,3), n = sum of counts, every vertex and centroid in
+ * z <= 0 (else ier 16).  iter != 0: the ITER leaf capacity (for mode 1/2
+ * evaluations).  Builds both plans. */
+int efmm_forest_set_geometry(efmm_forest *forest, int nprob, const int *counts, const double *tri,
+                             const double *nrm, const double *cen, int iprec, int iter);
+
+/* Half-space displacement u (n,3) and strain e (n,3,3) at every problem's
+ * centroids (device, problem order; NULL disables an output) of the
+ * densities ssl / sdl (n,3; NULL disables a layer), each problem on its own.
+ * precision 0 FP64, 1 mixed; mode 0, or 1 / 2 to store / replay both plans'
+ * near fields (geometry set with iter != 0).  Blocks. */
+int efmm_forest_evaluate(efmm_forest *forest, double rlam, double rmu, const double *ssl, const double *sdl,
+                         double *u, double *e, int precision, int mode);
+
+/* The forest's plans: which 0 the free-space (direct arrival) plan, 1 the
+ * image plan (for efmm_plan_info, efmm_plan_tree_export, timings). */
+efmm_plan *efmm_forest_plan(efmm_forest *forest, int which);
+
+/* The placement (host code, no device): from each problem's centroid
+ * bounding box bb (nprob,6: min x, y, z, max x, y, z) the root cube
+ * root5 = {centre x, y, z = 0, side, level L} and the x and y shift of each
+ * problem, shift (nprob,2), that moves its box to the centre of column
+ * k = i + 2^L j.  ier 16 on nprob < 1, bad boxes or a box above z = 0. */
+int efmm_forest_layout(int nprob, const double *bb, double *root5, double *shift);
+
+/* Host arrays in and out: the problems of efmm_forest_set_geometry and the
+ * outputs of efmm_forest_evaluate (mode 0) in one call, on a forest kept
+ * between calls. */
+int elhfmm3dtria_many_host(int iprec, double rlam, double rmu, int nprob, const int *counts, const double *tri,
+                           const double *nrm, const double *cen, const double *ssl, const double *sdl, double *u,
+                           double *e, int precision);
 
 /* ---- flat-triangle geometry I/O (host code) ----------------------------
  * The Cart3D ".tri" format: "nverts nfaces", nverts vertices (3 reals),

@@ -1,0 +1,135 @@
+"""Many independent half-space problems in one forest (efmm_forest_*,
+csrc/forest.cu): every problem's result against its own plans
+(elhfmm3dtria_total_, the reference drivers' direct arrival + image part,
+examples/elhfmm3dtria_self_iter_dr.f:331-385) and against the FP64 direct
+sums; the forest's lists never join two problems; the host-array entry point
+gives the device results; bad input is rejected."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _problems(k, seed, nmin=300, nmax=3000):
+    from elfmmlib3d_b200.batch import fault_problem
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(k):
+        ntri = int(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        tri, nrm, cen, slip = fault_problem(ntri, rng.uniform(0, 360), rng.uniform(15, 90), rng.uniform(0.5, 5),
+                                            seed=1000 * seed + i)
+        ssl = np.random.default_rng(i).normal(size=cen.shape) if i % 2 else None
+        out.append((tri, nrm, cen, ssl, slip))
+    return out
+
+
+def _forest(gpu, probs, iprec, precision):
+    import torch
+    dev = torch.device("cuda", 0)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
+    counts = [len(p[2]) for p in probs]
+    cat = lambda j, w: np.concatenate([np.asarray(p[j]).reshape(-1, w) for p in probs])
+    ssl = np.concatenate([p[3] if p[3] is not None else np.zeros_like(p[2]) for p in probs])
+    n = sum(counts)
+    u = torch.zeros((n, 3), dtype=torch.float64, device=dev)
+    e = torch.zeros((n, 3, 3), dtype=torch.float64, device=dev)
+    F = gpu.Forest(0)
+    F.set_geometry(counts, d(cat(0, 9)), d(cat(1, 3)), d(cat(2, 3)), iprec=iprec)
+    F.evaluate(1.3, 0.7, d(ssl), d(cat(4, 3)), u, e, precision=precision)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    uh, eh = u.cpu().numpy(), e.cpu().numpy()
+    return F, [(uh[off[i]:off[i + 1]], eh[off[i]:off[i + 1]]) for i in range(len(probs))]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_forest_matches_single_problem_plans(gpu, precision):
+    """FP64: each problem equals its own FMM up to the two trees' FMM
+    errors at iprec 3 (5e-10 each); mixed: within 2e-6."""
+    probs = _problems(7, 11)
+    F, res = _forest(gpu, probs, 3, precision)
+    F.close()
+    tol = 2e-8 if precision == 0 else 2e-6
+    worst = 0.0
+    for (tri, nrm, cen, ssl, sdl), (u, e) in zip(probs, res):
+        ier, ur, er, _, _ = gpu.elhfmm3dtria_total(3, 1.3, 0.7, tri, nrm, cen, ssl, sdl)
+        assert ier == 0
+        worst = max(worst, rel(u, ur), rel(e, er))
+    print(f"forest vs single-problem plans, precision {precision}: {worst:.2e}")
+    assert worst < tol
+
+
+def test_forest_matches_direct_sums(gpu):
+    import torch
+    from elfmmlib3d_b200.batch import _check
+    probs = _problems(5, 12)
+    F, res = _forest(gpu, probs, 3, 1)
+    F.close()
+    errs = [_check(p, u, e, 150, 1.3, 0.7, torch.device("cuda", 0)) for p, (u, e) in zip(probs, res)]
+    worst = max(max(x) for x in errs)
+    print(f"forest (mixed) vs FP64 direct sums: {worst:.2e}")
+    assert worst < 1e-6
+
+
+def test_forest_lists_stay_in_their_column(gpu):
+    """Lists 1-5 of both plans join only boxes of the same column of level L
+    (above L: colleagues only, no list 1-4 entries)."""
+    probs = _problems(6, 13, 200, 800)
+    F, _ = _forest(gpu, probs, 2, 1)
+    bb = np.array([np.concatenate([p[2].min(0), p[2].max(0)]) for p in probs])
+    root, _ = gpu.forest_layout(bb)
+    L = int(root[4])
+    for which in (0, 1):
+        T = F.plan(which).tree()
+        B = T["boxes"]
+        assert np.allclose(T["center"], root[:3]) and T["size"] == root[3]
+
+        def col(b):
+            lev = B[b, 0]
+            if lev < L:
+                return None
+            sh = lev - L
+            return ((B[b, 1] - 1) >> sh, (B[b, 2] - 1) >> sh)
+
+        nb = len(B)
+        for t in (1, 2, 3, 4, 5):
+            for b in range(nb):
+                for c in T["lists"][t][b]:
+                    cb, cc = col(b), col(int(c) - 1)
+                    if t == 5 and cb is None:
+                        assert cc is None
+                        continue
+                    assert cb is not None and cb == cc, (which, t, b, c)
+        # every box at level L or below lies in a column that holds one problem
+        cols = {col(b) for b in range(nb) if B[b, 0] >= L}
+        assert len(cols) == len(probs)
+    F.close()
+
+
+def test_forest_host_entry_matches_device(gpu):
+    probs = _problems(4, 14)
+    F, res = _forest(gpu, probs, 2, 1)
+    F.close()
+    counts = [len(p[2]) for p in probs]
+    cat = lambda j, w: np.concatenate([np.asarray(p[j]).reshape(-1, w) for p in probs])
+    ssl = np.concatenate([p[3] if p[3] is not None else np.zeros_like(p[2]) for p in probs])
+    ier, u, e = gpu.hs_many_host(2, 1.3, 0.7, counts, cat(0, 9), cat(1, 3), cat(2, 3), ssl, cat(4, 3), precision=1)
+    assert ier == 0
+    ud = np.concatenate([r[0] for r in res])
+    ed = np.concatenate([r[1] for r in res])
+    # the same computation up to the order of atomic sums in FP32
+    assert rel(u, ud) < 1e-6 and rel(e, ed) < 1e-6
+
+
+def test_forest_rejects_points_above_the_surface(gpu):
+    probs = _problems(3, 15, 100, 200)
+    tri, nrm, cen, ssl, sdl = probs[1]
+    probs[1] = (tri + np.array([0, 0, 10.0]), nrm, cen + np.array([0, 0, 10.0]), ssl, sdl)
+    counts = [len(p[2]) for p in probs]
+    cat = lambda j, w: np.concatenate([np.asarray(p[j]).reshape(-1, w) for p in probs])
+    ier, _, _ = gpu.hs_many_host(2, 1.0, 1.0, counts, cat(0, 9), cat(1, 3), cat(2, 3), None, cat(4, 3))
+    assert ier == 16
+    ier, _, _ = gpu.hs_many_host(2, 1.0, 1.0, [counts[0], 0, counts[1] + counts[2]], cat(0, 9), cat(1, 3),
+                                 cat(2, 3), None, cat(4, 3))
+    assert ier == 16
