@@ -1478,6 +1478,12 @@ def run_uneven(args, rank, world, local_rank):
     value = world * evals / t_max
     uh, eh = u.cpu().numpy(), e.cpu().numpy()
     res = [(uh[off[i]:off[i + 1]], eh[off[i]:off[i + 1]]) for i in range(len(probs))]
+    print(f"uneven: {t * 1e3:.1f} ms per step on the device ({evals / t:.3e} triangle-evals/s)", file=sys.stderr)
+    if F is not None:
+        F.close()  # the host entry point builds its own forest
+        F = None
+    del tri, nrm, cen, sdl, u, e
+    torch.cuda.empty_cache()
     # e2e: host arrays through the C ABI, host wall clock
     e2e_t = []
     if engine == "forest":
@@ -1488,8 +1494,6 @@ def run_uneven(args, rank, world, local_rank):
             if ier:
                 raise E.ElfmmError(ier, "elhfmm3dtria_many_host")
         e2e_err = float(max(np.linalg.norm(uu - uh) / np.linalg.norm(uh), np.linalg.norm(ee - eh) / np.linalg.norm(eh)))
-    if F is not None:
-        F.close()
     checked = list(range(0, len(probs), 8))
     errs = np.array([_check(probs[i], *res[i], min(200, int(sizes[i])), 1.0, 1.0, dev) for i in checked])
     e2e_v = world * evals / max_over_ranks(float(np.mean(e2e_t)), world, dev) if e2e_t else value

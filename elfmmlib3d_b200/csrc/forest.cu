@@ -105,7 +105,11 @@ int guard(efmm_forest* F, const std::function<int()>& body) {
   try {
     cudaSetDevice(F->device);
     return body();
-  } catch (const CudaError&) {
+  } catch (const CudaError& e) {
+    if (e.code == (int)cudaErrorMemoryAllocation) {
+      cudaGetLastError();  // the failed allocation leaves no sticky error
+      return IER_ALLOC;
+    }
     return IER_CUDA;
   } catch (const std::bad_alloc&) {
     return IER_ALLOC;

@@ -710,34 +710,23 @@ bool Plan::rot_tc_usable() const {
   return on && factored_ && tc_enabled() && p_ <= 31;
 }
 
-void Plan::cut_tc_tasks(TransSched& S, int C) {
+void Plan::cut_tc_tasks(TransSched& S, int C, bool one_launch) {
   if (S.tcC == C && S.tcpool == ops_) return;
-  // scratch budget per intermediate array (floats); a level whose columns
-  // need more runs as several batches
-  const long long budget = 1LL << 28;
   std::vector<RotTcSeg> segs;
   std::vector<RotTcTask> tasks;
   S.tcb.clear();
   for (auto& r : S.lev) {
-    long long ny = 0, nw = 0;
-    int t0 = (int)tasks.size();
+    if (S.tcb.empty() || !one_launch) S.tcb.push_back({(int)tasks.size(), 0, 0});
+    TransSched::TcBatch& b = S.tcb.back();
     for (int q = r.first; q < r.first + r.second; q++) {
       const TransSeg& g = S.segs[q];
-      const int pg = ops_->descs[g.group].p;
-      const long long ncols = (long long)g.npair * C;
-      const long long sy = (long long)rot_tc_pad_rows(0, pg) * ncols, sw = (long long)rot_tc_pad_rows(1, pg) * ncols;
-      if ((ny + sy > budget || nw + sw > budget) && (int)tasks.size() > t0) {
-        S.tcb.push_back({t0, (int)tasks.size() - t0, ny, nw});
-        t0 = (int)tasks.size();
-        ny = nw = 0;
-      }
+      const int pg = ops_->descs[g.group].p, ncols = g.npair * C;
       const int si = (int)segs.size();
-      segs.push_back({g.group, g.pair0, (int)ncols, 0, ny, nw});
-      for (long long c0 = 0; c0 < ncols; c0 += 128) tasks.push_back({si, (int)c0});
-      ny += sy;
-      nw += sw;
+      segs.push_back({g.group, g.pair0, ncols, 0});
+      for (int c0 = 0; c0 < ncols; c0 += RTC_COLS) tasks.push_back({si, c0});
+      b.pmax = std::max(b.pmax, pg);
     }
-    if ((int)tasks.size() > t0) S.tcb.push_back({t0, (int)tasks.size() - t0, ny, nw});
+    b.ntask = (int)tasks.size() - b.task0;
   }
   h2d(S.tcsegs, segs, st_);
   h2d(S.tctasks, tasks, st_);
@@ -745,23 +734,17 @@ void Plan::cut_tc_tasks(TransSched& S, int C) {
   S.tcpool = ops_;
 }
 
-void Plan::run_translations_tc(TransSched& S, int C, const float* src, float* dst) {
+// The FP32 translations of a schedule on the tensor cores (rot_tc.cu): one
+// launch per level (M2M, L2L: a level's sources are the previous level's
+// results), or one for all levels (M2L).
+void Plan::run_translations_tc(TransSched& S, int C, const float* src, float* dst, bool one_launch) {
   ensure_factored(true);
-  cut_tc_tasks(S, C);
-  long long ny = 0, nw = 0;
-  for (const auto& b : S.tcb) {
-    ny = std::max(ny, b.ny);
-    nw = std::max(nw, b.nw);
-  }
-  rot_y_.resize((size_t)std::max(ny, 1LL));  // grows only: no reallocation inside a captured pass
-  rot_w_.resize((size_t)std::max(nw, 1LL));
+  cut_tc_tasks(S, C, one_launch);
   const int D = 2 * ncoef(p_);
   int* err = tc_err_ptr();
   for (const auto& b : S.tcb)
-    for (int stage = 0; stage < 3; stage++)
-      launch_rot_tc(st_, stage, b.ntask, S.tctasks.get() + b.task0, S.tcsegs.get(), S.pairs.get(),
-                    ops_->rot_tc_ops.get(), ops_->rot_tc_tiles.get(), D, C, src, rot_y_.get(), rot_w_.get(), dst,
-                    err);
+    launch_rot_tc(st_, b.ntask, S.tctasks.get() + b.task0, S.tcsegs.get(), S.pairs.get(), ops_->rot_tc_ops.get(),
+                  ops_->rot_tc_tiles.get(), D, C, b.pmax, src, dst, err);
 }
 
 // The engine of each FP32 translation stage for this pass: the tuner's pick
@@ -792,8 +775,6 @@ void Plan::switch_precision(bool mixed) {
     local_f_.release();
     img_mp_f_.release();
     img_lc_f_.release();
-    rot_y_.release();
-    rot_w_.release();
   } else {
     mpole_.release();
     local_.release();
@@ -815,7 +796,7 @@ void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T
   if constexpr (sizeof(T) == 4) {
     const int stage = (&S == &m2l_ || &S == &m2lv_img_) ? 1 : ((&S == &l2l_ || &S == &l2l_img_ || &S == &l2l_img_u_) ? 2 : 0);
     if (rot_tc_usable() && trans_cand_[stage] == 0) {
-      run_translations_tc(S, C, reinterpret_cast<const float*>(src), reinterpret_cast<float*>(dst));
+      run_translations_tc(S, C, reinterpret_cast<const float*>(src), reinterpret_cast<float*>(dst), stage == 1);
       return;
     }
   }

@@ -84,16 +84,14 @@ struct TransSched {
   DevBuf<TransTask> rtasks;
   std::vector<std::pair<int, int>> lev_rtasks;  // task ranges in execution order,
   std::vector<int> lev_rdim;                     // each with its largest operator size
-  // tensor-core form: segments with their intermediate bases, 128-column
-  // tasks, and per batch (levels split so that Y and W stay within budget)
-  // the task range and its Y / W extents (floats)
+  // tensor-core form: segments, 32-column tasks, and per launch (a level,
+  // or all levels of an M2L stage) the task range and its largest order
   int tcC = -1;
   const void* tcpool = nullptr;
   DevBuf<RotTcSeg> tcsegs;
   DevBuf<RotTcTask> tctasks;
   struct TcBatch {
-    int task0, ntask;
-    long long ny, nw;
+    int task0, ntask, pmax;
   };
   std::vector<TcBatch> tcb;
   void clear() {
@@ -334,9 +332,8 @@ class Plan {
   void ensure_factored(bool tc = false);
   // the FP32 translations of a schedule on the tensor cores (rot_tc.cu)
   bool rot_tc_usable() const;
-  void cut_tc_tasks(TransSched& S, int C);
-  void run_translations_tc(TransSched& S, int C, const float* src, float* dst);
-  DevBuf<float> rot_y_, rot_w_;  // intermediates of the tensor-core translations
+  void cut_tc_tasks(TransSched& S, int C, bool one_launch);
+  void run_translations_tc(TransSched& S, int C, const float* src, float* dst, bool one_launch);
   // autotuned engine of the FP32 translations per stage (M2M, M2L, L2L):
   // 0 tensor cores, 1 CUDA cores; chosen at the start of a mixed pass
   // (tune_begin), reported with the stage times at its end (tune_end)

@@ -61,39 +61,36 @@ void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, co
 int rot_cols_per_cta(int maxdim, int elem_bytes);
 
 // ---- the FP32 factored translations on the tensor cores (rot_tc.cu) ----
-// A segment: the columns (npair x C) of one group's pairs, with the bases
-// (floats) of its rows in the two intermediate arrays Y and W, laid out
-// [row][column] (ncols per row).
+// A segment: the columns (npair x C) of one group's pairs.
 struct RotTcSeg {
   int group, pair0, ncols, pad;
-  long long ybase, wbase;
 };
-// A task: 128 consecutive columns of one segment.
+// A task: 32 consecutive columns of one segment (RTC_COLS).
 struct RotTcTask {
   int seg, col0;
 };
+constexpr int RTC_COLS = 32;
 // Per group: the order and, per stage (0 Fw, 1 Z, 2 Bk), the offset (floats)
-// of its first block tile; block tiles follow in block order, each the TF32
-// head then tail of the block in the canonical K-major layout (ceil16(rows)
-// x ceil8(rows) floats per part).
+// of its first block tile.  Block tiles follow in block order; a block of b
+// rows has ceil8(b) operator rows and K = ceil8(b) input rows, split into K
+// chunks of 32, each chunk the TF32 head then tail of the block's columns in
+// the chunk, in the canonical K-major layout (ceil8(b) x Kc floats per part).
 struct RotTcOp {
   int p, pad;
   long long tiles[3];
 };
-// Rows of block q of a stage at order p, and a stage's padded output rows
-// (each block rounded up to a multiple of 8): the row count of Y (stage 0)
-// and W (stage 1) per column.
+// Rows of block q of a stage at order p.
 int rot_tc_rows(int stage, int p, int q);
-int rot_tc_pad_rows(int stage, int p);
-size_t rot_tc_smem();
+// Shared memory of a launch whose groups have orders <= pmax.
+size_t rot_tc_smem(int pmax);
 // Operator tiles from the normalised FP32 pool in row-major block layout
 // (groups of order > 31 get no tiles: their blocks exceed 64 rows).
 void build_rot_tc_tiles(const std::vector<RotOp>& ops, const std::vector<float>& pool_rowmajor,
                         std::vector<RotTcOp>& tops, std::vector<float>& tiles);
-// One stage over ntask tasks: 0 reads the source expansions and writes Y,
-// 1 reads Y and writes W, 2 reads W and adds alpha x the result into dst.
-void launch_rot_tc(cudaStream_t st, int stage, int ntask, const RotTcTask* tasks, const RotTcSeg* segs,
-                   const TransPair* pairs, const RotTcOp* ops, const float* tiles, int D, int C, const float* src,
-                   float* ybuf, float* wbuf, float* dst, int* err);
+// The three factors of ntask tasks (groups of order <= pmax <= 31): alpha x
+// Bk Z Fw of each column of src is ADDED into its destination column of dst.
+void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const RotTcSeg* segs, const TransPair* pairs,
+                   const RotTcOp* ops, const float* tiles, int D, int C, int pmax, const float* src, float* dst,
+                   int* err);
 
 }  // namespace efmm

@@ -1,7 +1,8 @@
-"""The FP32 factored translations on the tensor cores (k_rot_tc, the three
-stages Fw, Z, Bk through the intermediates Y and W) against the factored
-product of the same FP32 operators in FP64 (host), through the C ABI; and
-the host emulation of the same stages (CPU, no device)."""
+"""The FP32 factored translations on the tensor cores (k_rot_tc: the three
+factors Fw, Z, Bk of 32 columns at a time in shared memory, M = 64 operator
+rows x N = 32 columns per MMA) against the factored product of the same FP32
+operators in FP64 (host), through the C ABI; and the host emulation of the
+kernel's arithmetic (tiles, padded rows, row maps; CPU, no device)."""
 import ctypes
 
 import pytest
