@@ -1448,10 +1448,15 @@ def run_uneven(args, rank, world, local_rank):
     e = torch.zeros((len(h_cen), 3, 3), dtype=torch.float64, device=dev)
     F = E.Forest(local_rank) if engine == "forest" else None
 
+    split = {}
+
     def step():
         if F is not None:
+            t0 = time.perf_counter()
             F.set_geometry(counts, tri, nrm, cen, iprec=w["iprec"])
+            t1 = time.perf_counter()
             F.evaluate(1.0, 1.0, None, sdl, u, e, precision=1)
+            split.update(set_geometry_ms=(t1 - t0) * 1e3, evaluate_ms=(time.perf_counter() - t1) * 1e3)
         else:
             res, _ = halfspace_many(probs, iprec=w["iprec"], precision=1, workers=workers, device=local_rank,
                                     engine="plans")
@@ -1476,6 +1481,12 @@ def run_uneven(args, rank, world, local_rank):
     t = float(np.mean(times))
     t_max = max_over_ranks(t, world, dev)
     value = world * evals / t_max
+    stages = None
+    if F is not None:
+        # device ms of the last step's passes by stage, host ms of its set-up by phase
+        stages = {name: {"evaluate": F.plan(k).timings(), "set_up": F.plan(k).setup_timings(),
+                         "info": F.plan(k).info()} for k, name in ((0, "free"), (1, "image"))}
+        stages["host_ms"] = dict(split)
     uh, eh = u.cpu().numpy(), e.cpu().numpy()
     res = [(uh[off[i]:off[i + 1]], eh[off[i]:off[i + 1]]) for i in range(len(probs))]
     print(f"uneven: {t * 1e3:.1f} ms per step on the device ({evals / t:.3e} triangle-evals/s)", file=sys.stderr)
@@ -1528,6 +1539,7 @@ def run_uneven(args, rank, world, local_rank):
                    "workers": workers if engine == "plans" else None,
                    "step": forest_step if engine == "forest" else plans_step,
                    "l2": "inputs (geometry > 300 MB) larger than L2",
+                   "stage_ms": stages,
                    "rel_err_vs_direct": {"problems_checked": len(checked), "centroids_each": 200,
                                          "u_max": float(errs[:, 0].max()),
                                          "u_median": float(np.median(errs[:, 0])),

@@ -44,13 +44,19 @@ namespace efmm {
 
 namespace {
 
-constexpr int RTC_NC = RTC_COLS, RTC_THREADS = 256, RTC_M = 64, RTC_KC = 32;
+constexpr int RTC_NC = RTC_COLS, RTC_M = 64, RTC_KC = 32;
 constexpr int RTC_APART = RTC_M * RTC_KC * 4;   // one part (head or tail) of an operator chunk: 8 KB
 constexpr int RTC_ASLOT = 2 * RTC_APART;        // 16 KB
 constexpr int RTC_BPART = RTC_NC * RTC_KC * 4;  // 4 KB
 constexpr int RTC_BSLOT = 2 * RTC_BPART;        // 8 KB
-constexpr int RTC_NA = 3;                       // operator ring slots
-constexpr int RTC_TMEM_COLS = 128;              // 2 blocks x 2 K chunks x 32 columns
+constexpr int RTC_NA = 3;                       // operator chunks in flight
+constexpr int RTC_NB = 4;                       // staged X chunks in flight
+constexpr int RTC_NACC = 4;                     // blocks in flight in TMEM (2 K chunks x 32 columns each)
+constexpr int RTC_TMEM_COLS = 256;
+// roles: warps 0-3 stage X (and load the sources), warps 4-7 drain TMEM
+// (warp 4 + i reads TMEM lanes 32 i .. 32 i + 31), warp 8 issues the MMAs,
+// warp 9 copies the operator chunks
+constexpr int RTC_THREADS = 320, RTC_CONV = 128, RTC_DRAIN = 128;
 
 __host__ __device__ inline int ceil8(int x) { return (x + 7) & ~7; }
 
@@ -73,22 +79,26 @@ __host__ __device__ inline long long rtc_tile_off(const RotTcOp& op, int s, int 
   return o + 2LL * ceil8(rtc_rows(s, op.p, q)) * RTC_KC * c;
 }
 
-// one task's columns: source and destination expansion offsets (-1 past the
-// segment), pair factor; the task's index, group and order
-struct RtcTaskInfo {
-  long long sbase[RTC_NC], dbase[RTC_NC];
-  float alpha[RTC_NC];
-  int ti, group, p, valid;
+// barriers: A full / empty per operator slot, B full / empty per staging
+// buffer, accumulator full / empty per TMEM block, X ready (the drains of a
+// stage done), teardown
+struct RtcBars {
+  uint64_t afull[RTC_NA], aempty[RTC_NA], bfull[RTC_NB], bempty[RTC_NB], cfull[RTC_NACC], cempty[RTC_NACC];
+  uint64_t xready, done;
+};
+// per-role tables (by task parity): source offsets of the staging warps,
+// destination offsets and pair factors of the draining warps
+struct RtcTables {
+  long long sbase[2][RTC_NC], dbase[2][RTC_NC];
+  float alpha[2][RTC_NC];
+  uint32_t tmem;
+  int abort_;
 };
 
 constexpr size_t rtc_smem_bytes(int xs) {
-  return 1024 + (size_t)RTC_NA * RTC_ASLOT + 2 * RTC_BSLOT + (size_t)RTC_NC * xs * 4 + 2 * sizeof(RtcTaskInfo) + 64;
+  return 1024 + (size_t)RTC_NA * RTC_ASLOT + (size_t)RTC_NB * RTC_BSLOT + (size_t)RTC_NC * xs * 4 + sizeof(RtcBars) +
+         sizeof(RtcTables);
 }
-
-// a unit: K chunk c of block q of stage s of the CTA's t-th task
-struct RtcUnit {
-  int t, s, q, c, valid;
-};
 
 __device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
   uint32_t r[16];
@@ -103,17 +113,79 @@ __device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
   for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
+}
+__device__ __forceinline__ void bar_named(int id, int n) { asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory"); }
+// named barrier that returns, to every participant, whether any of them passed true
+__device__ __forceinline__ bool bar_any(int id, int n, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred q, p;\n\t"
+      "setp.ne.u32 q, %1, 0;\n\t"
+      "bar.red.or.pred p, %2, %3, q;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(id), "r"(n)
+      : "memory");
+  return r != 0;
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// untiled bulk copy global -> shared, completion counted on an mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+// bounded wait for phase `parity`, giving up at once when another role has
+// given up (*abort_ set); false when it gave up
+__device__ __forceinline__ bool rtc_wait(uint32_t bar, uint32_t parity, volatile int* abort_) {
+  const long long t0 = clock64();
+  while (!mbar_try(bar, parity)) {
+    if (*abort_ || clock64() - t0 > TC_WAIT_CYCLES) {
+      *abort_ = 1;
+      return false;
+    }
+  }
+  return true;
+}
+
+// the task of this CTA's k-th turn: order, group, segment columns
+struct RtcTask {
+  int ti, p, group, pair0, ncols, col0;
+};
+__device__ __forceinline__ RtcTask rtc_task(int k, int ntask, const RotTcTask* tasks, const RotTcSeg* segs,
+                                            const RotTcOp* ops) {
+  RtcTask r;
+  r.ti = blockIdx.x + k * gridDim.x;
+  if (r.ti >= ntask) {
+    r.p = -1;
+    return r;
+  }
+  const RotTcTask t = tasks[r.ti];
+  const RotTcSeg sg = segs[t.seg];
+  r.group = sg.group;
+  r.p = ops[sg.group].p;
+  r.pair0 = sg.pair0;
+  r.ncols = sg.ncols;
+  r.col0 = t.col0;
+  return r;
 }
 
 }  // namespace
 
 size_t rot_tc_smem(int pmax) { return rtc_smem_bytes(rtc_xs(pmax)); }
 
+// The units of a task, in the order every role walks them: stages 0, 1, 2;
+// blocks 0..p; K chunks.  Units index the operator ring (u % RTC_NA) and the
+// staging buffers (u % RTC_NB), blocks the TMEM blocks (b % RTC_NACC), each
+// role counting its own.
 __global__ void __launch_bounds__(RTC_THREADS, 1)
 k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restrict__ segs,
          const TransPair* __restrict__ pairs, const RotTcOp* __restrict__ ops, const float* __restrict__ tiles, int D,
@@ -122,291 +194,295 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
   const uint32_t raw = smem_u32(rtc_raw);
   unsigned char* sm = rtc_raw + ((1024 - (raw & 1023)) & 1023);
   const uint32_t sA = smem_u32(sm), sB = sA + RTC_NA * RTC_ASLOT;
-  float* X = reinterpret_cast<float*>(sm + RTC_NA * RTC_ASLOT + 2 * RTC_BSLOT);
-  unsigned char* tbl = sm + RTC_NA * RTC_ASLOT + 2 * RTC_BSLOT + (size_t)RTC_NC * XS * 4;
-  RtcTaskInfo* info = reinterpret_cast<RtcTaskInfo*>(tbl);                      // [2], by task parity
-  uint64_t* bars = reinterpret_cast<uint64_t*>(tbl + 2 * sizeof(RtcTaskInfo));  // stg[2], blk[2]
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 4);
+  unsigned char* bstage = sm + RTC_NA * RTC_ASLOT;
+  float* X = reinterpret_cast<float*>(sm + RTC_NA * RTC_ASLOT + RTC_NB * RTC_BSLOT);
+  RtcBars* B = reinterpret_cast<RtcBars*>(sm + RTC_NA * RTC_ASLOT + RTC_NB * RTC_BSLOT + (size_t)RTC_NC * XS * 4);
+  RtcTables* T = reinterpret_cast<RtcTables*>(B + 1);
+  volatile int* abort_ = &T->abort_;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto bar = [](const uint64_t& b) { return smem_u32(&b); };
 
-  // the table of the CTA's k-th task
-  auto fill = [&](int k) {
-    RtcTaskInfo& I = info[k & 1];
-    const int ti = blockIdx.x + k * gridDim.x;
-    if (tid < RTC_NC) {
-      long long sb = -1, db = -1;
-      float al = 0.0f;
-      if (ti < ntask) {
-        const RotTcTask t = tasks[ti];
-        const RotTcSeg sg = segs[t.seg];
-        const int col = t.col0 + tid;
-        if (col < sg.ncols) {
-          const TransPair pr = pairs[sg.pair0 + col / C];
-          sb = ((long long)pr.src * C + col % C) * D;
-          db = ((long long)pr.dst * C + col % C) * D;
-          al = (float)pr.alpha;
-        }
-      }
-      I.sbase[tid] = sb;
-      I.dbase[tid] = db;
-      I.alpha[tid] = al;
+  if (tid == 0) {
+    for (int i = 0; i < RTC_NA; i++) {
+      mbar_init(bar(B->afull[i]), 1);
+      mbar_init(bar(B->aempty[i]), 1);
     }
-    if (tid == 0) {
-      I.ti = ti;
-      I.valid = ti < ntask;
-      if (ti < ntask) {
-        I.group = segs[tasks[ti].seg].group;
-        I.p = ops[I.group].p;
-      } else {
-        I.group = 0;
-        I.p = 0;
-      }
+    for (int i = 0; i < RTC_NB; i++) {
+      mbar_init(bar(B->bfull[i]), RTC_CONV);
+      mbar_init(bar(B->bempty[i]), 1);
     }
-  };
-  auto next_unit = [&](RtcUnit u) {
-    const int p = info[u.t & 1].p;
-    if (u.c + 1 < rtc_nchunk(u.s, p, u.q)) {
-      u.c++;
-      return u;
+    for (int i = 0; i < RTC_NACC; i++) {
+      mbar_init(bar(B->cfull[i]), 1);
+      mbar_init(bar(B->cempty[i]), RTC_DRAIN);
     }
-    u.c = 0;
-    if (u.q < p) {
-      u.q++;
-      return u;
-    }
-    u.q = 0;
-    if (u.s < 2) {
-      u.s++;
-      return u;
-    }
-    u.s = 0;
-    u.t++;
-    u.valid = info[u.t & 1].valid;
-    return u;
-  };
-  // source rows of degrees n0..n1 of a task into X (pairs of floats: source
-  // rows n(n+1) + 2j, X rows xpad(n) + 2j)
-  auto load_x = [&](const RtcTaskInfo& I, int n0, int n1) {
-    if (n1 < n0) return;
-    const int g0 = n0 * (n0 + 1) / 2, np = (n1 + 1) * (n1 + 2) / 2 - g0;
-    for (int idx = tid; idx < RTC_NC * np; idx += RTC_THREADS) {
-      const int col = idx / np, g = g0 + idx % np;
-      const long long sb = I.sbase[col];
-      if (sb < 0) continue;
-      int n = (int)((sqrtf(8.0f * g + 1.0f) - 1.0f) * 0.5f);
-      while (n * (n + 1) / 2 > g) n--;
-      while ((n + 1) * (n + 2) / 2 <= g) n++;
-      const int j = g - n * (n + 1) / 2;
-      cp_async8(smem_u32(X + (size_t)col * XS + xpad(n) + 2 * j), src + sb + 2 * g);
-    }
-  };
-  // operator chunk of unit u into ring slot `slot`
-  auto load_a = [&](const RtcUnit& u, int slot) {
-    const RotTcOp op = ops[info[u.t & 1].group];
-    const int Mr = ceil8(rtc_rows(u.s, op.p, u.q)), Kc = min(RTC_KC, Mr - RTC_KC * u.c);
-    const float* g = tiles + rtc_tile_off(op, u.s, u.q, u.c);
-    const int n16 = Mr * Kc / 4;
-    for (int i = tid; i < 2 * n16; i += RTC_THREADS) {
-      const int part = i >= n16, j = i - part * n16;
-      cp_async16(sA + slot * RTC_ASLOT + part * RTC_APART + j * 16, g + (size_t)part * Mr * Kc + 4 * j);
-    }
-  };
-  // X rows of unit u, split into head and tail, into staging buffer `buf`
-  // (N = 32 columns x K = Kc, canonical K-major)
-  auto convert = [&](const RtcUnit& u, int buf) {
-    const int p = info[u.t & 1].p, bb = rtc_rows(u.s, p, u.q), Kc = min(RTC_KC, ceil8(bb) - RTC_KC * u.c);
-    const int col = tid & 31, kq = tid >> 5, k0 = 4 * kq, kk = RTC_KC * u.c + k0;
-    if (k0 >= Kc) return;
-    const float* xc = X + (size_t)col * XS;
-    float v[4];
-    if (u.s != 1) {
-      const float4 w = *reinterpret_cast<const float4*>(xc + xpad(u.q) + kk);
-      v[0] = w.x; v[1] = w.y; v[2] = w.z; v[3] = w.w;
-      for (int e = 0; e < 4; e++)
-        if (kk + e >= bb) v[e] = 0.0f;
-    } else {
-      // order q: K index k -> degree q + k / 2, part k & 1
-      const int n = u.q + (kk >> 1);
-      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
-      if (kk < bb) a = *reinterpret_cast<const float2*>(xc + xpad(n) + 2 * u.q);
-      if (kk + 2 < bb) b = *reinterpret_cast<const float2*>(xc + xpad(n + 1) + 2 * u.q);
-      v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
-    }
-    float4 hi, lo;
-    hi.x = tf32_head(v[0]); lo.x = v[0] - hi.x;
-    hi.y = tf32_head(v[1]); lo.y = v[1] - hi.y;
-    hi.z = tf32_head(v[2]); lo.z = v[2] - hi.z;
-    hi.w = tf32_head(v[3]); lo.w = v[3] - hi.w;
-    unsigned char* b = sm + RTC_NA * RTC_ASLOT + buf * RTC_BSLOT + (col & 7) * 16 + kq * 128 + (col >> 3) * Kc * 32;
-    *reinterpret_cast<float4*>(b) = hi;
-    *reinterpret_cast<float4*>(b + RTC_BPART) = lo;
-  };
-  uint32_t tmem = 0;
-  // block (stage s, block q) of task slot ts, TMEM blocks bp: rows 16 w + lane
-  // of sub-partition w (the M = 64 layout: row r in lane 32 (r / 16) + r % 16)
-  auto drain = [&](int ts, int s, int q, int bp) {
-    const RtcTaskInfo& I = info[ts];
-    const int bb = rtc_rows(s, I.p, q), w4 = warp & 3, h = warp >> 2;
-    if (16 * w4 >= bb) return;  // warp-uniform: no rows of this block in the sub-partition
-    const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)(2 * bp) * 32 + 16 * h;
-    float v[16];
-    tmem_ld16(ta, v);
-    if (rtc_nchunk(s, I.p, q) > 1) {
-      float w[16];
-      tmem_ld16(ta + 32, w);
-#pragma unroll
-      for (int j = 0; j < 16; j++) v[j] += w[j];
-    }
-    const int i = 16 * w4 + lane;
-    if (lane >= 16 || i >= bb) return;
-    if (s == 2) {
-      const int row = q * (q + 1) + i;
-#pragma unroll
-      for (int j = 0; j < 16; j++) {
-        const long long db = I.dbase[16 * h + j];
-        if (db >= 0) atomicAdd(dst + db + row, I.alpha[16 * h + j] * v[j]);
-      }
-    } else {
-      const int xrow = s == 0 ? xpad(q) + i : xpad(q + (i >> 1)) + 2 * q + (i & 1);
-#pragma unroll
-      for (int j = 0; j < 16; j++) X[(size_t)(16 * h + j) * XS + xrow] = v[j];
-    }
-  };
-
-  if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+    mbar_init(bar(B->xready), RTC_DRAIN);
+    mbar_init(bar(B->done), 1);
+    T->abort_ = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 8) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&T->tmem)),
                  "r"(RTC_TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
-  if (tid == 0) {
-    for (int b = 0; b < 4; b++) mbar_init(smem_u32(&bars[b]), 1);
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  fill(0);
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  tmem = *tmem_slot;
-  const uint32_t stg[2] = {smem_u32(&bars[0]), smem_u32(&bars[1])};
-  const uint32_t blk[2] = {smem_u32(&bars[2]), smem_u32(&bars[3])};
-  const uint32_t idesc = tc_idesc_mn(RTC_M, RTC_NC);
+  const uint32_t tmem = T->tmem;
 
-  RtcUnit cur{0, 0, 0, 0, info[0].valid};
-  RtcUnit pf1 = cur, pf2 = cur;
-  if (cur.valid) {
-    load_x(info[0], 0, info[0].p);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    load_a(cur, 0);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    pf1 = next_unit(cur);
-    load_a(pf1, 1);
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    pf2 = next_unit(pf1);
-  }
-  long long un = 0;  // units issued so far (staging buffer un & 1, ring slot un % 3)
-  int bseq = 0;      // blocks committed so far (TMEM blocks and blk barrier bseq & 1)
-  bool pend = false;
-  int pts = 0, pss = 0, pq = 0, pseq = 0;  // the committed block not yet drained
-  bool ok = true;
-  auto drain_pending = [&]() {
-    ok = mbar_wait(blk[pseq & 1], (pseq >> 1) & 1);
-    ok = __syncthreads_and(ok);
-    if (!ok) return;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    drain(pts, pss, pq, pseq & 1);
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    pend = false;
-  };
-  while (cur.valid) {
-    const bool task_start = cur.s == 0 && cur.q == 0 && cur.c == 0;
-    const bool stage_start = cur.q == 0 && cur.c == 0;
-    if (task_start)
+  if (warp < 4) {
+    // ---- staging warps: X rows of each unit, split, into a staging buffer
+    const int ct = tid;  // 0..127
+    // the source offsets of task k's columns (table k & 1)
+    auto fill_src = [&](int k, const RtcTask& tk) {
+      if (ct < RTC_NC) {
+        long long sb = -1;
+        const int col = tk.col0 + ct;
+        if (tk.p >= 0 && col < tk.ncols) {
+          const TransPair pr = pairs[tk.pair0 + col / C];
+          sb = ((long long)pr.src * C + col % C) * D;
+        }
+        T->sbase[k & 1][ct] = sb;
+      }
+    };
+    // source rows of degrees n0..n1 into X (pairs of floats: source rows
+    // n(n+1) + 2j, X rows xpad(n) + 2j)
+    auto load_x = [&](int k, int n0, int n1) {
+      if (n1 < n0) return;
+      const int g0 = n0 * (n0 + 1) / 2, np = (n1 + 1) * (n1 + 2) / 2 - g0;
+      for (int idx = ct; idx < RTC_NC * np; idx += RTC_CONV) {
+        const int col = idx / np, g = g0 + idx % np;
+        const long long sb = T->sbase[k & 1][col];
+        if (sb < 0) continue;
+        int n = (int)((sqrtf(8.0f * g + 1.0f) - 1.0f) * 0.5f);
+        while (n * (n + 1) / 2 > g) n--;
+        while ((n + 1) * (n + 2) / 2 <= g) n++;
+        const int j = g - n * (n + 1) / 2;
+        cp_async8(smem_u32(X + (size_t)col * XS + xpad(n) + 2 * j), src + sb + 2 * g);
+      }
+      asm volatile("cp.async.commit_group;" ::: "memory");
+    };
+    RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
+    fill_src(0, tk);
+    bar_named(1, RTC_CONV);
+    load_x(0, 0, tk.p);
+    long long u = 0;
+    int xphase = 0;
+    bool ok = true;
+    for (int k = 0; tk.p >= 0 && ok; k++) {
+      const RtcTask nx = rtc_task(k + 1, ntask, tasks, segs, ops);
+      fill_src(k + 1, nx);
       asm volatile("cp.async.wait_group 0;" ::: "memory");
-    else
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-    __syncthreads();
-    // a stage reads what the previous one wrote; a new task's table slot is
-    // the one the pending block of the previous task still uses
-    if (pend && stage_start) {
-      drain_pending();
-      if (!ok) break;
-      __syncthreads();
-    }
-    if (task_start) {
-      fill(cur.t + 1);
-      __syncthreads();
-    }
-    const RtcTaskInfo& I = info[cur.t & 1];
-    const int buf = (int)(un & 1);
-    if (un >= 2) ok = mbar_wait(stg[buf], ((un - 2) >> 1) & 1);  // the MMAs of unit un - 2 read this buffer
-    convert(cur, buf);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    const int nch = rtc_nchunk(cur.s, I.p, cur.q);
-    const bool last_chunk = cur.c + 1 == nch;
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      const int Kc = min(RTC_KC, ceil8(rtc_rows(cur.s, I.p, cur.q)) - RTC_KC * cur.c);
-      const uint32_t ahi = sA + (uint32_t)(un % RTC_NA) * RTC_ASLOT, alo = ahi + RTC_APART;
-      const uint32_t bhi = sB + (uint32_t)buf * RTC_BSLOT, blo = bhi + RTC_BPART;
-      const uint32_t sbo = (uint32_t)Kc * 32;
-      const uint32_t dacc = tmem + (uint32_t)(2 * (bseq & 1) + cur.c) * 32;
-      for (int j = 0; j < Kc / 8; j++) {
-        const uint64_t dah = umma_desc(ahi + j * 256, 128, sbo), dal = umma_desc(alo + j * 256, 128, sbo);
-        const uint64_t dbh = umma_desc(bhi + j * 256, 128, sbo), dbl = umma_desc(blo + j * 256, 128, sbo);
-        mma_tf32(dacc, dal, dbh, idesc, j ? 1u : 0u);
-        mma_tf32(dacc, dah, dbl, idesc, 1u);
-        mma_tf32(dacc, dah, dbh, idesc, 1u);
+      bar_named(1, RTC_CONV);  // this task's X rows and the next task's table in place
+      for (int s = 0; s < 3 && ok; s++) {
+        if (s > 0) {
+          // the previous stage's drains are all in X
+          bool stop = false;
+          if (ct == 0) stop = !rtc_wait(bar(B->xready), xphase & 1, abort_);
+          xphase++;
+          if (bar_any(1, RTC_CONV, stop)) ok = false;
+        }
+        for (int q = 0; q <= tk.p && ok; q++) {
+          const int bb = rtc_rows(s, tk.p, q), nch = rtc_nchunk(s, tk.p, q);
+          for (int c = 0; c < nch; c++, u++) {
+            const int buf = (int)(u % RTC_NB);
+            bool stop = false;
+            if (ct == 0) stop = (u >= RTC_NB && !rtc_wait(bar(B->bempty[buf]), ((u / RTC_NB) - 1) & 1, abort_)) || *abort_;
+            if (bar_any(1, RTC_CONV, stop)) {
+              ok = false;
+              break;
+            }
+            const int Kc = min(RTC_KC, ceil8(bb) - RTC_KC * c);
+            // thread -> (column, K quad); two passes of 128 cover 32 columns x 8 quads
+            for (int w = ct; w < RTC_NC * 8; w += RTC_CONV) {
+              const int col = w & 31, kq = w >> 5, k0 = 4 * kq, kk = RTC_KC * c + k0;
+              if (k0 >= Kc) continue;
+              const float* xc = X + (size_t)col * XS;
+              float v[4];
+              if (s != 1) {
+                const float4 x4 = *reinterpret_cast<const float4*>(xc + xpad(q) + kk);
+                v[0] = x4.x; v[1] = x4.y; v[2] = x4.z; v[3] = x4.w;
+                for (int e = 0; e < 4; e++)
+                  if (kk + e >= bb) v[e] = 0.0f;
+              } else {
+                // order q: K index k -> degree q + k / 2, part k & 1
+                const int n = q + (kk >> 1);
+                float2 a2 = make_float2(0.f, 0.f), b2 = make_float2(0.f, 0.f);
+                if (kk < bb) a2 = *reinterpret_cast<const float2*>(xc + xpad(n) + 2 * q);
+                if (kk + 2 < bb) b2 = *reinterpret_cast<const float2*>(xc + xpad(n + 1) + 2 * q);
+                v[0] = a2.x; v[1] = a2.y; v[2] = b2.x; v[3] = b2.y;
+              }
+              float4 hi, lo;
+              hi.x = tf32_head(v[0]); lo.x = v[0] - hi.x;
+              hi.y = tf32_head(v[1]); lo.y = v[1] - hi.y;
+              hi.z = tf32_head(v[2]); lo.z = v[2] - hi.z;
+              hi.w = tf32_head(v[3]); lo.w = v[3] - hi.w;
+              unsigned char* b = bstage + buf * RTC_BSLOT + (col & 7) * 16 + kq * 128 + (col >> 3) * Kc * 32;
+              *reinterpret_cast<float4*>(b) = hi;
+              *reinterpret_cast<float4*>(b + RTC_BPART) = lo;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(bar(B->bfull[buf]));
+          }
+          // the last factor has read the rows of degree q: the next task's
+          // source rows of that degree (after the last block, its higher ones)
+          if (s == 2 && ok && nx.p >= 0) {
+            bar_named(1, RTC_CONV);
+            if (q <= nx.p) load_x(k + 1, q, q);
+            if (q == tk.p) load_x(k + 1, tk.p + 1, nx.p);
+          }
+        }
       }
-      mma_commit(stg[buf]);
-      if (last_chunk) mma_commit(blk[bseq & 1]);
+      tk = nx;
     }
-    // the previous block drains while this one multiplies
-    if (pend) {
-      drain_pending();
-      if (!ok) break;
-    }
-    if (last_chunk) {
-      pend = true;
-      pts = cur.t & 1;
-      pss = cur.s;
-      pq = cur.q;
-      pseq = bseq;
-      bseq++;
-    }
-    // ring slot of unit un + 2 held the operator of unit un - 1
-    if (un >= 1) ok = mbar_wait(stg[(un - 1) & 1], ((un - 1) >> 1) & 1);
-    if (pf2.valid) load_a(pf2, (int)((un + 2) % RTC_NA));
-    // the last factor has read the rows of degree q: the next task's source
-    // rows of that degree (and, after the last block, of its higher degrees)
-    if (cur.s == 2 && last_chunk) {
-      const RtcTaskInfo& N = info[(cur.t + 1) & 1];
-      if (N.valid) {
-        if (cur.q <= N.p) load_x(N, cur.q, cur.q);
-        if (cur.q == I.p) load_x(N, I.p + 1, N.p);
+    asm volatile("cp.async.wait_all;" ::: "memory");
+  } else if (warp < 8) {
+    // ---- draining warps: TMEM lanes 32 w4 .. 32 w4 + 15 hold rows 16 w4 ..
+    // 16 w4 + 15 of a block (the M = 64 layout)
+    const int dt = tid - 128, w4 = warp - 4;
+    long long b = 0;
+    bool ok = true;
+    RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
+    for (int k = 0; tk.p >= 0 && ok; k++) {
+      if (dt < RTC_NC) {
+        long long db = -1;
+        float al = 0.0f;
+        const int col = tk.col0 + dt;
+        if (col < tk.ncols) {
+          const TransPair pr = pairs[tk.pair0 + col / C];
+          db = ((long long)pr.dst * C + col % C) * D;
+          al = (float)pr.alpha;
+        }
+        T->dbase[k & 1][dt] = db;
+        T->alpha[k & 1][dt] = al;
       }
+      bar_named(2, RTC_DRAIN);
+      for (int s = 0; s < 3 && ok; s++) {
+        for (int q = 0; q <= tk.p; q++, b++) {
+          const int slot = (int)(b % RTC_NACC);
+          bool stop = false;
+          if (dt == 0) stop = !rtc_wait(bar(B->cfull[slot]), (b / RTC_NACC) & 1, abort_);
+          if (bar_any(2, RTC_DRAIN, stop)) {
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const int bb = rtc_rows(s, tk.p, q);
+          float v[32];
+          if (16 * w4 < bb) {
+            const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)slot * 64;
+            tmem_ld16(ta, v);
+            tmem_ld16(ta + 16, v + 16);
+            if (rtc_nchunk(s, tk.p, q) > 1) {
+              float w[16];
+              tmem_ld16(ta + 32, w);
+#pragma unroll
+              for (int j = 0; j < 16; j++) v[j] += w[j];
+              tmem_ld16(ta + 48, w);
+#pragma unroll
+              for (int j = 0; j < 16; j++) v[16 + j] += w[j];
+            }
+          }
+          asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+          mbar_arrive(bar(B->cempty[slot]));
+          const int i = 16 * w4 + lane;
+          if (16 * w4 < bb && lane < 16 && i < bb) {
+            if (s == 2) {
+              const int row = q * (q + 1) + i;
+#pragma unroll
+              for (int j = 0; j < 32; j++) {
+                const long long db = T->dbase[k & 1][j];
+                if (db >= 0) atomicAdd(dst + db + row, T->alpha[k & 1][j] * v[j]);
+              }
+            } else {
+              const int xrow = s == 0 ? xpad(q) + i : xpad(q + (i >> 1)) + 2 * q + (i & 1);
+#pragma unroll
+              for (int j = 0; j < 32; j++) X[(size_t)j * XS + xrow] = v[j];
+            }
+          }
+        }
+        if (s < 2 && ok) mbar_arrive(bar(B->xready));  // this stage's rows are in X
+      }
+      tk = rtc_task(k + 1, ntask, tasks, segs, ops);
     }
-    asm volatile("cp.async.commit_group;" ::: "memory");
-    ok = __syncthreads_and(ok);
-    if (!ok) break;
-    un++;
-    cur = pf1;
-    pf1 = pf2;
-    if (pf2.valid) pf2 = next_unit(pf2);
+  } else if (warp == 8) {
+    // ---- MMA issuer
+    if (lane == 0) {
+      const uint32_t idesc = tc_idesc_mn(RTC_M, RTC_NC);
+      long long u = 0, b = 0;
+      bool ok = true;
+      RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
+      for (int k = 0; tk.p >= 0 && ok; k++) {
+        for (int s = 0; s < 3 && ok; s++)
+          for (int q = 0; q <= tk.p && ok; q++, b++) {
+            const int slot = (int)(b % RTC_NACC);
+            if (b >= RTC_NACC) ok = rtc_wait(bar(B->cempty[slot]), ((b / RTC_NACC) - 1) & 1, abort_);
+            const int Mr = ceil8(rtc_rows(s, tk.p, q)), nch = rtc_nchunk(s, tk.p, q);
+            for (int c = 0; c < nch && ok; c++, u++) {
+              const int a = (int)(u % RTC_NA), buf = (int)(u % RTC_NB);
+              ok = rtc_wait(bar(B->afull[a]), (u / RTC_NA) & 1, abort_) &&
+                   rtc_wait(bar(B->bfull[buf]), (u / RTC_NB) & 1, abort_);
+              if (!ok) break;
+              asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+              const int Kc = min(RTC_KC, Mr - RTC_KC * c);
+              const uint32_t ahi = sA + (uint32_t)a * RTC_ASLOT, alo = ahi + RTC_APART;
+              const uint32_t bhi = sB + (uint32_t)buf * RTC_BSLOT, blo = bhi + RTC_BPART;
+              const uint32_t sbo = (uint32_t)Kc * 32;
+              const uint32_t dacc = tmem + (uint32_t)slot * 64 + (uint32_t)c * 32;
+              for (int j = 0; j < Kc / 8; j++) {
+                const uint64_t dah = umma_desc(ahi + j * 256, 128, sbo), dal = umma_desc(alo + j * 256, 128, sbo);
+                const uint64_t dbh = umma_desc(bhi + j * 256, 128, sbo), dbl = umma_desc(blo + j * 256, 128, sbo);
+                mma_tf32(dacc, dal, dbh, idesc, j ? 1u : 0u);
+                mma_tf32(dacc, dah, dbl, idesc, 1u);
+                mma_tf32(dacc, dah, dbh, idesc, 1u);
+              }
+              mma_commit(bar(B->aempty[a]));
+              mma_commit(bar(B->bempty[buf]));
+            }
+            if (ok) mma_commit(bar(B->cfull[slot]));
+          }
+        tk = rtc_task(k + 1, ntask, tasks, segs, ops);
+      }
+      // every MMA issued has completed before the TMEM and shared memory go
+      mma_commit(bar(B->done));
+      mbar_wait(bar(B->done), 0);
+    }
+  } else {
+    // ---- operator copies: one bulk copy per part of each unit's chunk
+    if (lane == 0) {
+      long long u = 0;
+      bool ok = true;
+      RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
+      for (int k = 0; tk.p >= 0 && ok; k++) {
+        const RotTcOp op = ops[tk.group];
+        for (int s = 0; s < 3 && ok; s++)
+          for (int q = 0; q <= tk.p && ok; q++) {
+            const int Mr = ceil8(rtc_rows(s, tk.p, q)), nch = rtc_nchunk(s, tk.p, q);
+            for (int c = 0; c < nch; c++, u++) {
+              const int a = (int)(u % RTC_NA);
+              if (u >= RTC_NA) ok = rtc_wait(bar(B->aempty[a]), ((u / RTC_NA) - 1) & 1, abort_);
+              if (!ok) break;
+              const int Kc = min(RTC_KC, Mr - RTC_KC * c);
+              const uint32_t bytes = (uint32_t)Mr * Kc * 4;
+              const float* g = tiles + rtc_tile_off(op, s, q, c);
+              mbar_expect_tx(bar(B->afull[a]), 2 * bytes);
+              bulk_g2s(sA + (uint32_t)a * RTC_ASLOT, g, bytes, bar(B->afull[a]));
+              bulk_g2s(sA + (uint32_t)a * RTC_ASLOT + RTC_APART, g + (size_t)Mr * Kc, bytes, bar(B->afull[a]));
+            }
+          }
+        tk = rtc_task(k + 1, ntask, tasks, segs, ops);
+      }
+      // copies still in flight land before the shared memory goes
+      for (long long v = u > RTC_NA ? u - RTC_NA : 0; v < u; v++)
+        mbar_wait(bar(B->afull[v % RTC_NA]), (v / RTC_NA) & 1);
+    }
   }
-  if (ok && pend) drain_pending();
-  if (!ok) {
-    if (tid == 0) atomicExch(err, 1);
-    // bounded waits for the MMAs in flight before their TMEM and shared memory go
-    for (long long v = un >= 2 ? un - 2 : 0; v <= un; v++) mbar_wait(stg[v & 1], (v >> 1) & 1);
-  }
-  asm volatile("cp.async.wait_all;" ::: "memory");
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncwarp();
   __syncthreads();
-  if (warp == 0)
+  if (tid == 0 && T->abort_) atomicExch(err, 1);
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (warp == 8)
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(RTC_TMEM_COLS)
                  : "memory");
 }
