@@ -45,12 +45,11 @@ namespace efmm {
 namespace {
 
 constexpr int RTC_NC = RTC_COLS, RTC_M = 64, RTC_KC = 32;
-constexpr int RTC_APART = RTC_M * RTC_KC * 4;   // one part (head or tail) of an operator chunk: 8 KB
-constexpr int RTC_ASLOT = 2 * RTC_APART;        // 16 KB
-constexpr int RTC_BPART = RTC_NC * RTC_KC * 4;  // 4 KB
-constexpr int RTC_BSLOT = 2 * RTC_BPART;        // 8 KB
-constexpr int RTC_NA = 3;                       // operator chunks in flight
-constexpr int RTC_NB = 4;                       // staged X chunks in flight
+constexpr int RTC_ARING = 48 * 1024;            // operator chunks in flight, each in its own size
+constexpr int RTC_NA = 16;                       // at most this many of them
+constexpr int RTC_BPART = RTC_NC * RTC_KC * 4;   // 4 KB
+constexpr int RTC_BSLOT = 2 * RTC_BPART;         // 8 KB
+constexpr int RTC_NB = 4;                        // staged X chunks in flight
 constexpr int RTC_NACC = 4;                     // blocks in flight in TMEM (2 K chunks x 32 columns each)
 constexpr int RTC_TMEM_COLS = 256;
 // roles: warps 0-3 stage X (and load the sources), warps 4-7 drain TMEM
@@ -87,16 +86,22 @@ struct RtcBars {
   uint64_t xready, done;
 };
 // per-role tables (by task parity): source offsets of the staging warps,
-// destination offsets and pair factors of the draining warps
+// destination offsets and pair factors of the draining warps; the ring
+// offset of each operator chunk in flight
 struct RtcTables {
   long long sbase[2][RTC_NC], dbase[2][RTC_NC];
   float alpha[2][RTC_NC];
+  uint32_t aoff[RTC_NA], alen[RTC_NA];
   uint32_t tmem;
   int abort_;
 };
 
+// shared memory: the operator ring (the MMAs of a chunk read 64 operator
+// rows from its start; rows past the chunk's own land in the staging
+// buffers that follow: garbage in output rows nobody reads), the staging
+// buffers, X, barriers, tables
 constexpr size_t rtc_smem_bytes(int xs) {
-  return 1024 + (size_t)RTC_NA * RTC_ASLOT + (size_t)RTC_NB * RTC_BSLOT + (size_t)RTC_NC * xs * 4 + sizeof(RtcBars) +
+  return 1024 + (size_t)RTC_ARING + (size_t)RTC_NB * RTC_BSLOT + (size_t)RTC_NC * xs * 4 + sizeof(RtcBars) +
          sizeof(RtcTables);
 }
 
@@ -193,10 +198,10 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
   extern __shared__ __align__(1024) unsigned char rtc_raw[];
   const uint32_t raw = smem_u32(rtc_raw);
   unsigned char* sm = rtc_raw + ((1024 - (raw & 1023)) & 1023);
-  const uint32_t sA = smem_u32(sm), sB = sA + RTC_NA * RTC_ASLOT;
-  unsigned char* bstage = sm + RTC_NA * RTC_ASLOT;
-  float* X = reinterpret_cast<float*>(sm + RTC_NA * RTC_ASLOT + RTC_NB * RTC_BSLOT);
-  RtcBars* B = reinterpret_cast<RtcBars*>(sm + RTC_NA * RTC_ASLOT + RTC_NB * RTC_BSLOT + (size_t)RTC_NC * XS * 4);
+  const uint32_t sA = smem_u32(sm), sB = sA + RTC_ARING;
+  unsigned char* bstage = sm + RTC_ARING;
+  float* X = reinterpret_cast<float*>(sm + RTC_ARING + RTC_NB * RTC_BSLOT);
+  RtcBars* B = reinterpret_cast<RtcBars*>(sm + RTC_ARING + RTC_NB * RTC_BSLOT + (size_t)RTC_NC * XS * 4);
   RtcTables* T = reinterpret_cast<RtcTables*>(B + 1);
   volatile int* abort_ = &T->abort_;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -426,7 +431,7 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
               if (!ok) break;
               asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
               const int Kc = min(RTC_KC, Mr - RTC_KC * c);
-              const uint32_t ahi = sA + (uint32_t)a * RTC_ASLOT, alo = ahi + RTC_APART;
+              const uint32_t ahi = sA + T->aoff[a], alo = ahi + (uint32_t)Mr * Kc * 4;
               const uint32_t bhi = sB + (uint32_t)buf * RTC_BSLOT, blo = bhi + RTC_BPART;
               const uint32_t sbo = (uint32_t)Kc * 32;
               const uint32_t dacc = tmem + (uint32_t)slot * 64 + (uint32_t)c * 32;
@@ -449,9 +454,13 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       mbar_wait(bar(B->done), 0);
     }
   } else {
-    // ---- operator copies: one bulk copy per part of each unit's chunk
+    // ---- operator copies: one bulk copy per part of each unit's chunk, into
+    // a ring of bytes (each chunk contiguous, wrapping to the start when it
+    // does not fit before the end); a chunk's space is taken back once the
+    // MMAs of the oldest chunks in flight are done
     if (lane == 0) {
-      long long u = 0;
+      long long u = 0, oldest = 0;
+      uint32_t head = 0;
       bool ok = true;
       RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
       for (int k = 0; tk.p >= 0 && ok; k++) {
@@ -460,15 +469,35 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
           for (int q = 0; q <= tk.p && ok; q++) {
             const int Mr = ceil8(rtc_rows(s, tk.p, q)), nch = rtc_nchunk(s, tk.p, q);
             for (int c = 0; c < nch; c++, u++) {
-              const int a = (int)(u % RTC_NA);
-              if (u >= RTC_NA) ok = rtc_wait(bar(B->aempty[a]), ((u / RTC_NA) - 1) & 1, abort_);
-              if (!ok) break;
               const int Kc = min(RTC_KC, Mr - RTC_KC * c);
-              const uint32_t bytes = (uint32_t)Mr * Kc * 4;
+              const uint32_t bytes = (uint32_t)Mr * Kc * 4, len = 2 * bytes;
+              const uint32_t pos = head + len <= (uint32_t)RTC_ARING ? head : 0;
+              // [pos, pos + len) must hold no chunk in flight; at most RTC_NA in flight
+              while (oldest < u) {
+                const int o = (int)(oldest % RTC_NA);
+                const uint32_t a0 = T->aoff[o], a1 = a0 + T->alen[o];
+                // the chunks in flight lie in the circular range [a0, head)
+                const bool wrapped = a0 >= head;  // the range runs past the end to the start
+                bool clear;
+                if (!wrapped)
+                  clear = pos >= head || pos + len <= a0;
+                else
+                  clear = pos >= head && pos + len <= a0;
+                (void)a1;
+                if (clear && u - oldest < RTC_NA) break;
+                ok = rtc_wait(bar(B->aempty[o]), (oldest / RTC_NA) & 1, abort_);
+                if (!ok) break;
+                oldest++;
+              }
+              if (!ok) break;
+              const int a = (int)(u % RTC_NA);
+              T->aoff[a] = pos;
+              T->alen[a] = len;
+              head = pos + len;
               const float* g = tiles + rtc_tile_off(op, s, q, c);
-              mbar_expect_tx(bar(B->afull[a]), 2 * bytes);
-              bulk_g2s(sA + (uint32_t)a * RTC_ASLOT, g, bytes, bar(B->afull[a]));
-              bulk_g2s(sA + (uint32_t)a * RTC_ASLOT + RTC_APART, g + (size_t)Mr * Kc, bytes, bar(B->afull[a]));
+              mbar_expect_tx(bar(B->afull[a]), len);
+              bulk_g2s(sA + pos, g, bytes, bar(B->afull[a]));
+              bulk_g2s(sA + pos + bytes, g + (size_t)Mr * Kc, bytes, bar(B->afull[a]));
             }
           }
         tk = rtc_task(k + 1, ntask, tasks, segs, ops);
