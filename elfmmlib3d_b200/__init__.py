@@ -54,12 +54,14 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "elhfmm3dtria_total_", "efmm_mindlin_image_kernel",
            "efmm_pair_eval_host", "elhfmm3dtria_batch_host", "efmm_tri_read", "efmm_tri_write",
            "efmm_tri_refine", "efmm_tri_build", "efmm_rot_tc_selfcheck", "efmm_rot_tc_selfcheck_device",
+           "efmm_rot_tc_bench",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
            "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
            "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host",
            "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_", "efmm_plan_set_forest",
            "efmm_forest_create", "efmm_forest_destroy", "efmm_forest_set_geometry", "efmm_forest_evaluate",
-           "efmm_forest_plan", "efmm_forest_layout", "elhfmm3dtria_many_host"]
+           "efmm_forest_plan", "efmm_forest_layout", "elhfmm3dtria_many_host", "efmm_plan_set_leaf",
+           "efmm_forest_set_leaf"]
 
 
 class ElfmmError(RuntimeError):
@@ -146,6 +148,10 @@ def load():
     L.efmm_forest_evaluate.restype = ctypes.c_int
     L.efmm_forest_evaluate.argtypes = [_vp, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp, _vp, ctypes.c_int,
                                        ctypes.c_int]
+    L.efmm_plan_set_leaf.restype = ctypes.c_int
+    L.efmm_plan_set_leaf.argtypes = [_vp, ctypes.c_int]
+    L.efmm_forest_set_leaf.restype = ctypes.c_int
+    L.efmm_forest_set_leaf.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
     L.efmm_forest_plan.restype = _vp
     L.efmm_forest_plan.argtypes = [_vp, ctypes.c_int]
     L.efmm_forest_layout.restype = ctypes.c_int
@@ -885,6 +891,11 @@ class Forest:
         if not self._h:
             raise ElfmmError(1024, f"cannot create forest on device {device}")
         self.n = 0
+
+    def set_leaf(self, nbox_free=0, nbox_image=0):
+        """Leaf capacities of the two plans for the next set_geometry (<= 0:
+        the iprec table)."""
+        self._L.efmm_forest_set_leaf(self._h, int(nbox_free), int(nbox_image))
 
     def set_geometry(self, counts, tri, nrm, cen, iprec=2, iter=False):
         c = np.ascontiguousarray(counts, dtype=np.int32)

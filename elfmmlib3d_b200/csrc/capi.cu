@@ -88,6 +88,12 @@ extern "C" int efmm_plan_evaluate_direct_subset(efmm_plan* p, double rlam, doubl
   EFMM_GUARD(return p->plan->evaluate_direct(rlam, rmu, ssl, sdl, u_src, e_src, nullptr, nullptr, nsub);)
 }
 
+extern "C" int efmm_plan_set_leaf(efmm_plan* p, int nbox) {
+  if (!p) return IER_BADARG;
+  p->plan->set_leaf(nbox);
+  return IER_OK;
+}
+
 extern "C" int efmm_plan_set_forest(efmm_plan* p, const double* forest) {
   if (!p) return IER_BADARG;
   if (forest && (!(forest[3] > 0.0) || forest[4] < 1.0 || forest[4] > 15.0 || forest[4] != (int)forest[4]))

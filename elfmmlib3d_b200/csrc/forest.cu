@@ -179,6 +179,13 @@ extern "C" void efmm_forest_destroy(efmm_forest* F) {
   delete F;
 }
 
+extern "C" int efmm_forest_set_leaf(efmm_forest* F, int nbox_free, int nbox_image) {
+  if (!F) return IER_BADARG;
+  efmm_plan_set_leaf(F->f, nbox_free);
+  efmm_plan_set_leaf(F->img, nbox_image);
+  return IER_OK;
+}
+
 extern "C" efmm_plan* efmm_forest_plan(efmm_forest* F, int which) {
   if (!F) return nullptr;
   return which == 0 ? F->f : (which == 1 ? F->img : nullptr);

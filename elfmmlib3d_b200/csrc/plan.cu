@@ -333,7 +333,7 @@ int Plan::set_geometry(int n, const double* d_tri, const double* d_nrm, const do
   nt_ = nt;
   iprec_ = iprec;
   eps_ = iprec_eps(iprec);
-  nbox_ = iprec_nbox(iprec, n, nt, iter);
+  nbox_ = leaf_override_ > 0 ? leaf_override_ : iprec_nbox(iprec, n, nt, iter);
   p_ = eps_ > 0 ? order_for_eps(eps_, 1.5) : 0;
   eps_mixed_ = mixed_floor_ > 0 ? std::max(eps_, mixed_floor_) : eps_;
   p_mixed_ = eps_mixed_ > 0 ? std::min(p_, order_for_eps(eps_mixed_, 1.5)) : p_;

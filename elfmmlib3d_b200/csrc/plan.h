@@ -146,6 +146,9 @@ class Plan {
   // A forest of independent problems for the following set_geometry calls:
   // f5 = {root centre x, y, z, root side, level} as build_tree's forest (the
   // Mindlin root needs centre z = 0); null: one problem.
+  // Leaf capacity of the following set_geometry calls (boxes split while
+  // they hold more sources or targets); <= 0: the iprec table.
+  void set_leaf(int nbox) { leaf_override_ = nbox; }
   void set_forest(const double* f5) {
     forest_on_ = f5 != nullptr;
     for (int i = 0; i < 5; i++) forest_[i] = f5 ? f5[i] : 0.0;
@@ -238,6 +241,7 @@ class Plan {
   void build_chunks(int do_src, int do_tgt);
   bool mindlin_ = false, img_sched_ = false;
   bool forest_on_ = false;
+  int leaf_override_ = 0;
   double forest_[5] = {0, 0, 0, 0, 0};
   TransSched m2lv_img_, m2lu_, l2l_img_, l2l_img_u_, m2m_u_;
   template <class T>

@@ -50,8 +50,11 @@ constexpr int RTC_NA = 16;                       // at most this many of them
 constexpr int RTC_BPART = RTC_NC * RTC_KC * 4;   // 4 KB
 constexpr int RTC_BSLOT = 2 * RTC_BPART;         // 8 KB
 constexpr int RTC_NB = 4;                        // staged X chunks in flight
-constexpr int RTC_NACC = 4;                     // blocks in flight in TMEM (2 K chunks x 32 columns each)
-constexpr int RTC_TMEM_COLS = 256;
+// TMEM: per block 2 K chunks x `split` accumulators (the chunk's K steps
+// spread round-robin over them, so that consecutive MMAs are independent) x
+// 32 columns; 512 / (64 split) blocks in flight
+constexpr int RTC_NACC_MAX = 8;
+constexpr int RTC_TMEM_COLS = 512;
 // roles: warps 0-3 stage X (and load the sources), warps 4-7 drain TMEM
 // (warp 4 + i reads TMEM lanes 32 i .. 32 i + 31), warp 8 issues the MMAs,
 // warp 9 copies the operator chunks
@@ -82,7 +85,7 @@ __host__ __device__ inline long long rtc_tile_off(const RotTcOp& op, int s, int 
 // buffer, accumulator full / empty per TMEM block, X ready (the drains of a
 // stage done), teardown
 struct RtcBars {
-  uint64_t afull[RTC_NA], aempty[RTC_NA], bfull[RTC_NB], bempty[RTC_NB], cfull[RTC_NACC], cempty[RTC_NACC];
+  uint64_t afull[RTC_NA], aempty[RTC_NA], bfull[RTC_NB], bempty[RTC_NB], cfull[RTC_NACC_MAX], cempty[RTC_NACC_MAX];
   uint64_t xready, done;
 };
 // per-role tables (by task parity): source offsets of the staging warps,
@@ -189,13 +192,15 @@ size_t rot_tc_smem(int pmax) { return rtc_smem_bytes(rtc_xs(pmax)); }
 
 // The units of a task, in the order every role walks them: stages 0, 1, 2;
 // blocks 0..p; K chunks.  Units index the operator ring (u % RTC_NA) and the
-// staging buffers (u % RTC_NB), blocks the TMEM blocks (b % RTC_NACC), each
+// staging buffers (u % RTC_NB), blocks the TMEM blocks (b % nacc), each
 // role counting its own.
 __global__ void __launch_bounds__(RTC_THREADS, 1)
 k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restrict__ segs,
          const TransPair* __restrict__ pairs, const RotTcOp* __restrict__ ops, const float* __restrict__ tiles, int D,
-         int C, int XS, const float* __restrict__ src, float* __restrict__ dst, int* __restrict__ err) {
+         int C, int XS, int split, const float* __restrict__ src, float* __restrict__ dst, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char rtc_raw[];
+  const int nacc = RTC_NACC_MAX / split;            // blocks in flight in TMEM
+  const uint32_t bcols = (uint32_t)(64 * split);    // TMEM columns per block
   const uint32_t raw = smem_u32(rtc_raw);
   unsigned char* sm = rtc_raw + ((1024 - (raw & 1023)) & 1023);
   const uint32_t sA = smem_u32(sm), sB = sA + RTC_ARING;
@@ -216,7 +221,7 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       mbar_init(bar(B->bfull[i]), RTC_CONV);
       mbar_init(bar(B->bempty[i]), 1);
     }
-    for (int i = 0; i < RTC_NACC; i++) {
+    for (int i = 0; i < RTC_NACC_MAX; i++) {
       mbar_init(bar(B->cfull[i]), 1);
       mbar_init(bar(B->cempty[i]), RTC_DRAIN);
     }
@@ -365,9 +370,9 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       bar_named(2, RTC_DRAIN);
       for (int s = 0; s < 3 && ok; s++) {
         for (int q = 0; q <= tk.p; q++, b++) {
-          const int slot = (int)(b % RTC_NACC);
+          const int slot = (int)(b % nacc);
           bool stop = false;
-          if (dt == 0) stop = !rtc_wait(bar(B->cfull[slot]), (b / RTC_NACC) & 1, abort_);
+          if (dt == 0) stop = !rtc_wait(bar(B->cfull[slot]), (b / nacc) & 1, abort_);
           if (bar_any(2, RTC_DRAIN, stop)) {
             ok = false;
             break;
@@ -376,17 +381,24 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
           const int bb = rtc_rows(s, tk.p, q);
           float v[32];
           if (16 * w4 < bb) {
-            const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)slot * 64;
-            tmem_ld16(ta, v);
-            tmem_ld16(ta + 16, v + 16);
-            if (rtc_nchunk(s, tk.p, q) > 1) {
-              float w[16];
-              tmem_ld16(ta + 32, w);
+            // the sum of the block's accumulators: chunk c, accumulator r
+            // (r < its K steps) at columns (c split + r) x 32
+            const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)slot * bcols;
+            const int Mr = ceil8(bb), nch = rtc_nchunk(s, tk.p, q);
 #pragma unroll
-              for (int j = 0; j < 16; j++) v[j] += w[j];
-              tmem_ld16(ta + 48, w);
+            for (int j = 0; j < 32; j++) v[j] = 0.0f;
+            for (int c = 0; c < nch; c++) {
+              const int J = min(RTC_KC, Mr - RTC_KC * c) / 8;
+              for (int r = 0; r < split && r < J; r++) {
+                float w[16];
+                const uint32_t ca = ta + (uint32_t)(c * split + r) * 32;
+                tmem_ld16(ca, w);
 #pragma unroll
-              for (int j = 0; j < 16; j++) v[16 + j] += w[j];
+                for (int j = 0; j < 16; j++) v[j] += w[j];
+                tmem_ld16(ca + 16, w);
+#pragma unroll
+                for (int j = 0; j < 16; j++) v[16 + j] += w[j];
+              }
             }
           }
           asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -421,8 +433,8 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       for (int k = 0; tk.p >= 0 && ok; k++) {
         for (int s = 0; s < 3 && ok; s++)
           for (int q = 0; q <= tk.p && ok; q++, b++) {
-            const int slot = (int)(b % RTC_NACC);
-            if (b >= RTC_NACC) ok = rtc_wait(bar(B->cempty[slot]), ((b / RTC_NACC) - 1) & 1, abort_);
+            const int slot = (int)(b % nacc);
+            if (b >= nacc) ok = rtc_wait(bar(B->cempty[slot]), ((b / nacc) - 1) & 1, abort_);
             const int Mr = ceil8(rtc_rows(s, tk.p, q)), nch = rtc_nchunk(s, tk.p, q);
             for (int c = 0; c < nch && ok; c++, u++) {
               const int a = (int)(u % RTC_NA), buf = (int)(u % RTC_NB);
@@ -434,14 +446,16 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
               const uint32_t ahi = sA + T->aoff[a], alo = ahi + (uint32_t)Mr * Kc * 4;
               const uint32_t bhi = sB + (uint32_t)buf * RTC_BSLOT, blo = bhi + RTC_BPART;
               const uint32_t sbo = (uint32_t)Kc * 32;
-              const uint32_t dacc = tmem + (uint32_t)slot * 64 + (uint32_t)c * 32;
-              for (int j = 0; j < Kc / 8; j++) {
-                const uint64_t dah = umma_desc(ahi + j * 256, 128, sbo), dal = umma_desc(alo + j * 256, 128, sbo);
-                const uint64_t dbh = umma_desc(bhi + j * 256, 128, sbo), dbl = umma_desc(blo + j * 256, 128, sbo);
-                mma_tf32(dacc, dal, dbh, idesc, j ? 1u : 0u);
-                mma_tf32(dacc, dah, dbl, idesc, 1u);
-                mma_tf32(dacc, dah, dbh, idesc, 1u);
-              }
+              const uint32_t dacc = tmem + (uint32_t)slot * bcols + (uint32_t)(c * split) * 32;
+              const int J = Kc / 8;
+              // term t of K step j into accumulator j % split: consecutive
+              // MMAs go to different accumulators
+              for (int t = 0; t < 3; t++)
+                for (int j = 0; j < J; j++) {
+                  const uint32_t aa = (t == 0 ? alo : ahi) + j * 256, bb2 = (t == 1 ? blo : bhi) + j * 256;
+                  mma_tf32(dacc + (uint32_t)(j % split) * 32, umma_desc(aa, 128, sbo), umma_desc(bb2, 128, sbo), idesc,
+                           (t == 0 && j < split) ? 0u : 1u);
+                }
               mma_commit(bar(B->aempty[a]));
               mma_commit(bar(B->bempty[buf]));
             }
@@ -516,6 +530,14 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
                  : "memory");
 }
 
+// accumulators per K chunk (1, 2 or 4): rot_tc_split
+static int g_rtc_split = 2;
+int rot_tc_split(int split) {
+  const int old = g_rtc_split;
+  if (split == 1 || split == 2 || split == 4) g_rtc_split = split;
+  return old;
+}
+
 void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const RotTcSeg* segs, const TransPair* pairs,
                    const RotTcOp* ops, const float* tiles, int D, int C, int pmax, const float* src, float* dst,
                    int* err) {
@@ -530,8 +552,8 @@ void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const Rot
   const int xs = rtc_xs(pmax);
   const size_t smem = rtc_smem_bytes(xs);
   EFMM_CUDA_TRY(smem_raise(k_rot_tc, (int)smem));
-  k_rot_tc<<<std::min(ntask, nsm), RTC_THREADS, smem, st>>>(ntask, tasks, segs, pairs, ops, tiles, D, C, xs, src, dst,
-                                                            err);
+  k_rot_tc<<<std::min(ntask, nsm), RTC_THREADS, smem, st>>>(ntask, tasks, segs, pairs, ops, tiles, D, C, xs,
+                                                            g_rtc_split, src, dst, err);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -734,15 +756,16 @@ extern "C" int efmm_rot_tc_selfcheck(int p, unsigned seed, double* rel) {
   return 0;
 }
 
-// Device check of the kernel: one M2L, one M2M and one L2L group of order p,
-// npair box pairs each with C columns per box (random normalised source
-// expansions, pair factors alpha, a destination box per group), in one
-// launch, against the factored product of the same FP32 operators in FP64
-// on the host.  Returns 0 and the relative l2 error of the destination
-// expansions in *rel (*timeout != 0 if a bounded wait ran out).
-extern "C" int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double* rel, int* timeout) {
+// The kernel on one M2L, one M2M and one L2L group of order p, npair box
+// pairs each with C columns per box (random normalised source expansions,
+// pair factors alpha, a destination box per group), in one launch; reps > 1
+// launches it reps times more and returns the mean ms of those in *ms.  With
+// rel: the relative l2 error of the destination expansions of the first
+// launch against the factored product of the same FP32 operators in FP64 on
+// the host.  *timeout != 0 if a bounded wait ran out.
+static int rtc_device_run(int p, int C, int npair, unsigned seed, int reps, double* rel, int* timeout, double* ms) {
   using namespace efmm;
-  if (p < 1 || p > 31 || C < 1 || npair < 1 || C * npair > (1 << 20) || !rel || !timeout) return 16;
+  if (p < 1 || p > 31 || C < 1 || npair < 1 || C * npair > (1 << 20) || !timeout) return 16;
   std::vector<RotOp> rops;
   std::vector<float> poolf;
   rtc_test_ops(p, rops, poolf);
@@ -803,9 +826,34 @@ extern "C" int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned se
     return 256;
   }
   cudaMemcpy(hdst.data(), ddst, hdst.size() * 4, cudaMemcpyDeviceToHost);
+  if (reps > 1 && ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    try {
+      for (int r = 0; r < reps; r++)
+        launch_rot_tc(0, (int)tasks.size(), dtask, dseg, dp, dops, dtiles, D, C, p, dsrc, ddst, derr);
+    } catch (const CudaError&) {
+      release();
+      return 256;
+    }
+    cudaEventRecord(e1, 0);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      release();
+      return 256;
+    }
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
   int herr = 0;
   cudaMemcpy(&herr, derr, 4, cudaMemcpyDeviceToHost);
   release();
+  *timeout = herr;
+  if (!rel) return 0;
   // host reference: dst(box) = sum over pairs alpha Bk Z Fw src(box), FP64
   double num = 0, den = 0;
   for (int g = 0; g < 3; g++)
@@ -822,6 +870,23 @@ extern "C" int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned se
       }
     }
   *rel = std::sqrt(num / std::max(den, 1e-300));
-  *timeout = herr;
   return 0;
+}
+
+// Device check of the kernel (rtc_device_run, one launch): returns 0 and
+// the relative l2 error of the destination expansions in *rel.
+extern "C" int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double* rel, int* timeout) {
+  if (!rel) return 16;
+  return rtc_device_run(p, C, npair, seed, 1, rel, timeout, nullptr);
+}
+
+// Timing of the kernel on the same inputs: mean ms of reps launches with
+// `split` accumulators per K chunk (1, 2 or 4; the library's setting is
+// restored afterwards).
+extern "C" int efmm_rot_tc_bench(int p, int C, int npair, int reps, int split, double* ms, int* timeout) {
+  if (reps < 1 || !ms || (split != 1 && split != 2 && split != 4)) return 16;
+  const int old = efmm::rot_tc_split(split);
+  const int ier = rtc_device_run(p, C, npair, 1, reps + 1, nullptr, timeout, ms);
+  efmm::rot_tc_split(old);
+  return ier;
 }

@@ -243,6 +243,12 @@ int efmm_plan_set_geometry(efmm_plan *plan, int n, const double *tri, const doub
                            const double *src, int nt, const double *tgt, int iprec, int iter,
                            int mindlin);
 
+/* Leaf capacity of the plan's following set_geometry calls (boxes split
+ * while they hold more than nbox sources or targets); nbox <= 0 restores the
+ * iprec table (src/elfmm3dtria.f:702-722).  Another capacity gives another
+ * tree (not the reference's) with the same accuracy contract. */
+int efmm_plan_set_leaf(efmm_plan *plan, int nbox);
+
 /* A forest of independent problems for the plan's following set_geometry
  * calls (no counterpart in the reference): forest = {root centre x, y, z,
  * root side, level L} -- the tree's root is this cube instead of the
@@ -525,13 +531,16 @@ int efmm_tune_dump(char *buf, int len);
 
 /* Checks of the FP32 factored translations on the tensor cores (no
  * counterpart in the reference): one M2L, one M2M and one L2L group of order
- * p (1..31).  _selfcheck emulates the three stages on the host (tiles, their
- * layout, the row maps between the stages, the 3-term split); _device runs
- * them on the GPU for npair box pairs of C columns each.  Both return 0 and
- * the relative l2 difference from the FP64 product of the same FP32
- * operators in *rel (_device: *timeout != 0 if a bounded wait ran out). */
+ * p (1..31).  _selfcheck emulates the kernel's arithmetic on the host (tiles,
+ * their layout, the padded rows, the row maps of the three factors, the
+ * 3-term split); _device runs the kernel on the GPU for npair box pairs of C
+ * columns each.  Both return 0 and the relative l2 difference from the FP64
+ * product of the same FP32 operators in *rel (_device: *timeout != 0 if a
+ * bounded wait ran out).  _bench times reps launches on the same inputs with
+ * `split` (1, 2, 4) accumulators per K chunk: mean ms in *ms. */
 int efmm_rot_tc_selfcheck(int p, unsigned seed, double *rel);
 int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double *rel, int *timeout);
+int efmm_rot_tc_bench(int p, int C, int npair, int reps, int split, double *ms, int *timeout);
 
 /* ---- many independent half-space problems in one pass -----------------
  * (no counterpart in the reference, whose drivers evaluate one fault per
@@ -562,6 +571,10 @@ int efmm_forest_set_geometry(efmm_forest *forest, int nprob, const int *counts, 
  * near fields (geometry set with iter != 0).  Blocks. */
 int efmm_forest_evaluate(efmm_forest *forest, double rlam, double rmu, const double *ssl, const double *sdl,
                          double *u, double *e, int precision, int mode);
+
+/* Leaf capacities of the forest's free-space and image plans for the next
+ * efmm_forest_set_geometry (<= 0: the iprec table). */
+int efmm_forest_set_leaf(efmm_forest *forest, int nbox_free, int nbox_image);
 
 /* The forest's plans: which 0 the free-space (direct arrival) plan, 1 the
  * image plan (for efmm_plan_info, efmm_plan_tree_export, timings). */
