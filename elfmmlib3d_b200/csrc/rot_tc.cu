@@ -258,19 +258,16 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
     };
     // source rows of degrees n0..n1 into X (pairs of floats: source rows
     // n(n+1) + 2j, X rows xpad(n) + 2j)
+    // (warp w: columns 8 w .. 8 w + 7, lanes along a degree's pairs)
     auto load_x = [&](int k, int n0, int n1) {
-      if (n1 < n0) return;
-      const int g0 = n0 * (n0 + 1) / 2, np = (n1 + 1) * (n1 + 2) / 2 - g0;
-      for (int idx = ct; idx < RTC_NC * np; idx += RTC_CONV) {
-        const int col = idx / np, g = g0 + idx % np;
-        const long long sb = T->sbase[k & 1][col];
-        if (sb < 0) continue;
-        int n = (int)((sqrtf(8.0f * g + 1.0f) - 1.0f) * 0.5f);
-        while (n * (n + 1) / 2 > g) n--;
-        while ((n + 1) * (n + 2) / 2 <= g) n++;
-        const int j = g - n * (n + 1) / 2;
-        cp_async8(smem_u32(X + (size_t)col * XS + xpad(n) + 2 * j), src + sb + 2 * g);
-      }
+      for (int n = n0; n <= n1; n++)
+        for (int cc = 0; cc < RTC_NC / 4; cc++) {
+          const int col = 8 * warp + cc;
+          const long long sb = T->sbase[k & 1][col];
+          if (sb < 0) continue;
+          for (int j = lane; j <= n; j += 32)
+            cp_async8(smem_u32(X + (size_t)col * XS + xpad(n) + 2 * j), src + sb + n * (n + 1) + 2 * j);
+        }
       asm volatile("cp.async.commit_group;" ::: "memory");
     };
     RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
@@ -352,6 +349,7 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
     // 16 w4 + 15 of a block (the M = 64 layout)
     const int dt = tid - 128, w4 = warp - 4;
     long long b = 0;
+    int bslot = 0, bwrap = 0;  // b = bwrap nacc + bslot
     bool ok = true;
     RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
     for (int k = 0; tk.p >= 0 && ok; k++) {
@@ -370,9 +368,14 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       bar_named(2, RTC_DRAIN);
       for (int s = 0; s < 3 && ok; s++) {
         for (int q = 0; q <= tk.p; q++, b++) {
-          const int slot = (int)(b % nacc);
+          const int slot = bslot;
+          const int par = bwrap & 1;
+          if (++bslot == nacc) {
+            bslot = 0;
+            bwrap++;
+          }
           bool stop = false;
-          if (dt == 0) stop = !rtc_wait(bar(B->cfull[slot]), (b / nacc) & 1, abort_);
+          if (dt == 0) stop = !rtc_wait(bar(B->cfull[slot]), par, abort_);
           if (bar_any(2, RTC_DRAIN, stop)) {
             ok = false;
             break;
@@ -428,13 +431,18 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
     if (lane == 0) {
       const uint32_t idesc = tc_idesc_mn(RTC_M, RTC_NC);
       long long u = 0, b = 0;
+      int bslot = 0, bwrap = 0;  // b = bwrap nacc + bslot
       bool ok = true;
       RtcTask tk = rtc_task(0, ntask, tasks, segs, ops);
       for (int k = 0; tk.p >= 0 && ok; k++) {
         for (int s = 0; s < 3 && ok; s++)
           for (int q = 0; q <= tk.p && ok; q++, b++) {
-            const int slot = (int)(b % nacc);
-            if (b >= nacc) ok = rtc_wait(bar(B->cempty[slot]), ((b / nacc) - 1) & 1, abort_);
+            const int slot = bslot;
+            if (bwrap > 0) ok = rtc_wait(bar(B->cempty[slot]), (bwrap - 1) & 1, abort_);
+            if (++bslot == nacc) {
+              bslot = 0;
+              bwrap++;
+            }
             const int Mr = ceil8(rtc_rows(s, tk.p, q)), nch = rtc_nchunk(s, tk.p, q);
             for (int c = 0; c < nch && ok; c++, u++) {
               const int a = (int)(u % RTC_NA), buf = (int)(u % RTC_NB);

@@ -27,10 +27,13 @@ __host__ __device__ constexpr uint32_t tc_idesc_mn(int M, int N) {
          ((uint32_t)(M >> 4) << 24);
 }
 
+// TF32 value nearest to x, ties away from zero (what cvt.rna.tf32.f32
+// gives), in integer operations: the conversion instruction issues on the XU
+// pipe, which splitting every staged operand element would saturate.
+// Infinities and NaNs pass unchanged.
 __device__ __forceinline__ float tf32_head(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
+  const uint32_t u = __float_as_uint(x);
+  return (u & 0x7f800000u) == 0x7f800000u ? x : __uint_as_float((u + 0x1000u) & ~0x1FFFu);
 }
 
 __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
