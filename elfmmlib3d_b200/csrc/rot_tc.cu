@@ -9,27 +9,29 @@
 // persistent CTA takes 32 columns of one group at a time (a task) and keeps
 // them in shared memory, X[column][row] in FP32 (degree-major rows, each
 // degree padded to a multiple of 4), through all three factors.  Each K
-// chunk (32 input rows) of each block of each factor is one product on the
-// tensor cores,
+// chunk (32 input rows) of each block of each factor (a unit) is one product
+// on the tensor cores,
 //     D[i][col] = sum_k OP[i][k] X[col][k]   (M = 64 operator rows,
 //                                             N = 32 columns, K = 8 per MMA),
 // kind::tf32 with the 3-term split of both operands (x = hi + lo, hi = x
-// rounded to TF32; hi hi + hi lo + lo hi: FP32 accuracy).  The operator
-// chunks are split on the host and stored in the canonical no-swizzle
-// K-major layout, so the CTA copies them with cp.async (a ring of three,
-// two chunks ahead); the X rows are gathered and split while staged (the
-// shift along z reads the rows (n, m), n >= m, of order m, which lie apart in
-// the degree-major layout).  Accumulators live in TMEM, one per K chunk (the
-// tensor cores truncate their sums: chunks are summed in FP32 registers),
-// two blocks deep, so that a block drains while the next one multiplies.
-// The first two factors write their results back into X in place (a block
-// reads and writes the same rows); the third adds alpha x the result into
-// the destination expansions with coalesced atomic adds.  While a CTA
-// applies the third factor, the next task's source columns are copied into
-// the rows of X that the third factor has finished reading, so a task's
-// input is resident when it starts.  Every wait is bounded: one that runs
-// out sets *err, the CTA waits (bounded) for its MMAs in flight, frees its
-// TMEM and returns.
+// rounded to TF32; hi hi + hi lo + lo hi: FP32 accuracy), one FP32
+// accumulator in TMEM per K chunk (the tensor cores truncate their sums:
+// chunks are summed in FP32 registers).
+//
+// Warps have roles and meet only at mbarriers, so that several units are in
+// flight: one thread copies each unit's operator chunk (split on the host,
+// canonical no-swizzle K-major layout) with an untiled bulk copy into a byte
+// ring; four warps gather the unit's X rows (the shift along z reads the
+// rows (n, m), n >= m, of order m, which lie apart in the degree-major
+// layout), split them and stage them; one thread issues the MMAs; four warps
+// drain each block's accumulators from TMEM (8 blocks deep), back into X in
+// place for the first two factors (a block reads and writes the same rows),
+// and as alpha x the result with coalesced atomic adds into the destination
+// expansions for the third.  While the third factor runs, the staging warps
+// copy the next task's source columns into the rows of X it has finished
+// reading.  Every wait is bounded: one that runs out makes every role stop,
+// sets *err, and the CTA waits (bounded) for its copies and MMAs in flight
+// before its TMEM and shared memory go.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -50,10 +52,8 @@ constexpr int RTC_NA = 16;                       // at most this many of them
 constexpr int RTC_BPART = RTC_NC * RTC_KC * 4;   // 4 KB
 constexpr int RTC_BSLOT = 2 * RTC_BPART;         // 8 KB
 constexpr int RTC_NB = 4;                        // staged X chunks in flight
-// TMEM: per block 2 K chunks x `split` accumulators (the chunk's K steps
-// spread round-robin over them, so that consecutive MMAs are independent) x
-// 32 columns; 512 / (64 split) blocks in flight
-constexpr int RTC_NACC_MAX = 8;
+// TMEM: per block 2 K chunks x 32 columns; 8 blocks in flight
+constexpr int RTC_NACC = 8;
 constexpr int RTC_TMEM_COLS = 512;
 // roles: warps 0-3 stage X (and load the sources), warps 4-7 drain TMEM
 // (warp 4 + i reads TMEM lanes 32 i .. 32 i + 31), warp 8 issues the MMAs,
@@ -85,7 +85,7 @@ __host__ __device__ inline long long rtc_tile_off(const RotTcOp& op, int s, int 
 // buffer, accumulator full / empty per TMEM block, X ready (the drains of a
 // stage done), teardown
 struct RtcBars {
-  uint64_t afull[RTC_NA], aempty[RTC_NA], bfull[RTC_NB], bempty[RTC_NB], cfull[RTC_NACC_MAX], cempty[RTC_NACC_MAX];
+  uint64_t afull[RTC_NA], aempty[RTC_NA], bfull[RTC_NB], bempty[RTC_NB], cfull[RTC_NACC], cempty[RTC_NACC];
   uint64_t xready, done;
 };
 // per-role tables (by task parity): source offsets of the staging warps,
@@ -108,18 +108,16 @@ constexpr size_t rtc_smem_bytes(int xs) {
          sizeof(RtcTables);
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t addr, float* v) {
-  uint32_t r[16];
+// 16 columns of TMEM (this warp's 32 lanes) into r; complete after tmem_wait()
+__device__ __forceinline__ void tmem_ld16(uint32_t addr, uint32_t* r) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
       "%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
         "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(addr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int j = 0; j < 16; j++) v[j] = __uint_as_float(r[j]);
 }
+__device__ __forceinline__ void tmem_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
 __device__ __forceinline__ void cp_async8(uint32_t dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src) : "memory");
@@ -197,10 +195,9 @@ size_t rot_tc_smem(int pmax) { return rtc_smem_bytes(rtc_xs(pmax)); }
 __global__ void __launch_bounds__(RTC_THREADS, 1)
 k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restrict__ segs,
          const TransPair* __restrict__ pairs, const RotTcOp* __restrict__ ops, const float* __restrict__ tiles, int D,
-         int C, int XS, int split, const float* __restrict__ src, float* __restrict__ dst, int* __restrict__ err) {
+         int C, int XS, const float* __restrict__ src, float* __restrict__ dst, int* __restrict__ err) {
   extern __shared__ __align__(1024) unsigned char rtc_raw[];
-  const int nacc = RTC_NACC_MAX / split;            // blocks in flight in TMEM
-  const uint32_t bcols = (uint32_t)(64 * split);    // TMEM columns per block
+  constexpr int nacc = RTC_NACC;  // blocks in flight in TMEM, 64 columns each
   const uint32_t raw = smem_u32(rtc_raw);
   unsigned char* sm = rtc_raw + ((1024 - (raw & 1023)) & 1023);
   const uint32_t sA = smem_u32(sm), sB = sA + RTC_ARING;
@@ -221,7 +218,7 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
       mbar_init(bar(B->bfull[i]), RTC_CONV);
       mbar_init(bar(B->bempty[i]), 1);
     }
-    for (int i = 0; i < RTC_NACC_MAX; i++) {
+    for (int i = 0; i < RTC_NACC; i++) {
       mbar_init(bar(B->cfull[i]), 1);
       mbar_init(bar(B->cempty[i]), RTC_DRAIN);
     }
@@ -384,23 +381,27 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
           const int bb = rtc_rows(s, tk.p, q);
           float v[32];
           if (16 * w4 < bb) {
-            // the sum of the block's accumulators: chunk c, accumulator r
-            // (r < its K steps) at columns (c split + r) x 32
-            const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)slot * bcols;
-            const int Mr = ceil8(bb), nch = rtc_nchunk(s, tk.p, q);
+            // chunk 0 at columns 0..31 of the block, chunk 1 at 32..63: all
+            // loads issued, then one wait
+            const uint32_t ta = tmem + ((uint32_t)(32 * w4) << 16) + (uint32_t)slot * 64;
+            uint32_t r0[16], r1[16], r2[16], r3[16];
+            tmem_ld16(ta, r0);
+            tmem_ld16(ta + 16, r1);
+            if (rtc_nchunk(s, tk.p, q) > 1) {
+              tmem_ld16(ta + 32, r2);
+              tmem_ld16(ta + 48, r3);
+              tmem_wait();
 #pragma unroll
-            for (int j = 0; j < 32; j++) v[j] = 0.0f;
-            for (int c = 0; c < nch; c++) {
-              const int J = min(RTC_KC, Mr - RTC_KC * c) / 8;
-              for (int r = 0; r < split && r < J; r++) {
-                float w[16];
-                const uint32_t ca = ta + (uint32_t)(c * split + r) * 32;
-                tmem_ld16(ca, w);
+              for (int j = 0; j < 16; j++) {
+                v[j] = __uint_as_float(r0[j]) + __uint_as_float(r2[j]);
+                v[16 + j] = __uint_as_float(r1[j]) + __uint_as_float(r3[j]);
+              }
+            } else {
+              tmem_wait();
 #pragma unroll
-                for (int j = 0; j < 16; j++) v[j] += w[j];
-                tmem_ld16(ca + 16, w);
-#pragma unroll
-                for (int j = 0; j < 16; j++) v[16 + j] += w[j];
+              for (int j = 0; j < 16; j++) {
+                v[j] = __uint_as_float(r0[j]);
+                v[16 + j] = __uint_as_float(r1[j]);
               }
             }
           }
@@ -454,16 +455,21 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
               const uint32_t ahi = sA + T->aoff[a], alo = ahi + (uint32_t)Mr * Kc * 4;
               const uint32_t bhi = sB + (uint32_t)buf * RTC_BSLOT, blo = bhi + RTC_BPART;
               const uint32_t sbo = (uint32_t)Kc * 32;
-              const uint32_t dacc = tmem + (uint32_t)slot * bcols + (uint32_t)(c * split) * 32;
+              const uint32_t dacc = tmem + (uint32_t)slot * 64 + (uint32_t)c * 32;
+              // descriptors of K step j: the step-0 ones + 256 bytes per step
+              // in the 16-byte address field
+              const uint64_t dah = umma_desc(ahi, 128, sbo), dal = umma_desc(alo, 128, sbo);
+              const uint64_t dbh = umma_desc(bhi, 128, sbo), dbl = umma_desc(blo, 128, sbo);
               const int J = Kc / 8;
-              // term t of K step j into accumulator j % split: consecutive
-              // MMAs go to different accumulators
-              for (int t = 0; t < 3; t++)
-                for (int j = 0; j < J; j++) {
-                  const uint32_t aa = (t == 0 ? alo : ahi) + j * 256, bb2 = (t == 1 ? blo : bhi) + j * 256;
-                  mma_tf32(dacc + (uint32_t)(j % split) * 32, umma_desc(aa, 128, sbo), umma_desc(bb2, 128, sbo), idesc,
-                           (t == 0 && j < split) ? 0u : 1u);
+#pragma unroll
+              for (int j = 0; j < RTC_KC / 8; j++) {
+                if (j < J) {
+                  const uint64_t o = (uint64_t)(16 * j);
+                  mma_tf32(dacc, dal + o, dbh + o, idesc, j ? 1u : 0u);
+                  mma_tf32(dacc, dah + o, dbl + o, idesc, 1u);
+                  mma_tf32(dacc, dah + o, dbh + o, idesc, 1u);
                 }
+              }
               mma_commit(bar(B->aempty[a]));
               mma_commit(bar(B->bempty[buf]));
             }
@@ -538,14 +544,6 @@ k_rot_tc(int ntask, const RotTcTask* __restrict__ tasks, const RotTcSeg* __restr
                  : "memory");
 }
 
-// accumulators per K chunk (1, 2 or 4): rot_tc_split
-static int g_rtc_split = 2;
-int rot_tc_split(int split) {
-  const int old = g_rtc_split;
-  if (split == 1 || split == 2 || split == 4) g_rtc_split = split;
-  return old;
-}
-
 void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const RotTcSeg* segs, const TransPair* pairs,
                    const RotTcOp* ops, const float* tiles, int D, int C, int pmax, const float* src, float* dst,
                    int* err) {
@@ -560,8 +558,8 @@ void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const Rot
   const int xs = rtc_xs(pmax);
   const size_t smem = rtc_smem_bytes(xs);
   EFMM_CUDA_TRY(smem_raise(k_rot_tc, (int)smem));
-  k_rot_tc<<<std::min(ntask, nsm), RTC_THREADS, smem, st>>>(ntask, tasks, segs, pairs, ops, tiles, D, C, xs,
-                                                            g_rtc_split, src, dst, err);
+  k_rot_tc<<<std::min(ntask, nsm), RTC_THREADS, smem, st>>>(ntask, tasks, segs, pairs, ops, tiles, D, C, xs, src, dst,
+                                                            err);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -888,13 +886,8 @@ extern "C" int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned se
   return rtc_device_run(p, C, npair, seed, 1, rel, timeout, nullptr);
 }
 
-// Timing of the kernel on the same inputs: mean ms of reps launches with
-// `split` accumulators per K chunk (1, 2 or 4; the library's setting is
-// restored afterwards).
-extern "C" int efmm_rot_tc_bench(int p, int C, int npair, int reps, int split, double* ms, int* timeout) {
-  if (reps < 1 || !ms || (split != 1 && split != 2 && split != 4)) return 16;
-  const int old = efmm::rot_tc_split(split);
-  const int ier = rtc_device_run(p, C, npair, 1, reps + 1, nullptr, timeout, ms);
-  efmm::rot_tc_split(old);
-  return ier;
+// Timing of the kernel on the same inputs: mean ms of reps launches.
+extern "C" int efmm_rot_tc_bench(int p, int C, int npair, int reps, double* ms, int* timeout) {
+  if (reps < 1 || !ms) return 16;
+  return rtc_device_run(p, C, npair, 1, reps + 1, nullptr, timeout, ms);
 }

@@ -87,9 +87,6 @@ size_t rot_tc_smem(int pmax);
 // (groups of order > 31 get no tiles: their blocks exceed 64 rows).
 void build_rot_tc_tiles(const std::vector<RotOp>& ops, const std::vector<float>& pool_rowmajor,
                         std::vector<RotTcOp>& tops, std::vector<float>& tiles);
-// Accumulators per K chunk of the tensor-core translations (1, 2 or 4; the
-// chunk's K steps round-robin over them); returns the previous setting.
-int rot_tc_split(int split);
 // The three factors of ntask tasks (groups of order <= pmax <= 31): alpha x
 // Bk Z Fw of each column of src is ADDED into its destination column of dst.
 void launch_rot_tc(cudaStream_t st, int ntask, const RotTcTask* tasks, const RotTcSeg* segs, const TransPair* pairs,

@@ -536,11 +536,11 @@ int efmm_tune_dump(char *buf, int len);
  * 3-term split); _device runs the kernel on the GPU for npair box pairs of C
  * columns each.  Both return 0 and the relative l2 difference from the FP64
  * product of the same FP32 operators in *rel (_device: *timeout != 0 if a
- * bounded wait ran out).  _bench times reps launches on the same inputs with
- * `split` (1, 2, 4) accumulators per K chunk: mean ms in *ms. */
+ * bounded wait ran out).  _bench times reps launches on the same inputs:
+ * mean ms in *ms. */
 int efmm_rot_tc_selfcheck(int p, unsigned seed, double *rel);
 int efmm_rot_tc_selfcheck_device(int p, int C, int npair, unsigned seed, double *rel, int *timeout);
-int efmm_rot_tc_bench(int p, int C, int npair, int reps, int split, double *ms, int *timeout);
+int efmm_rot_tc_bench(int p, int C, int npair, int reps, double *ms, int *timeout);
 
 /* ---- many independent half-space problems in one pass -----------------
  * (no counterpart in the reference, whose drivers evaluate one fault per
