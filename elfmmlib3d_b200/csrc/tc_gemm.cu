@@ -161,20 +161,22 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
   for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
   auto drain = [&](int u) {  // add the accumulator of tile u into acc
     const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
+    // every load issued, then one wait
+    uint32_t r[NHALF];
 #pragma unroll
     for (int c16 = 0; c16 < NHALF / 16; c16++) {
       const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
-      uint32_t r[16];
+      uint32_t* q = r + 16 * c16;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
           "%14, %15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+            "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
           : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += (TC)__uint_as_float(r[j]);
     }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < NHALF; j++) acc[j] += (TC)__uint_as_float(r[j]);
   };
   bool ok = true;
   if (nkt > 0) load(0);
@@ -191,15 +193,16 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
       const uint32_t ahi = base, alo = base + TC_TILE_BYTES, bhi = base + 2 * TC_TILE_BYTES,
                      blo = bhi + TC_BTILE;
       const uint32_t dacc = tmem + (uint32_t)s * BN;
+      // K step i: the step-0 descriptors + 2 i TC_LBO bytes in the 16-byte
+      // address field (descriptor arithmetic kept off the issuing thread's path)
+      const uint64_t dah = umma_desc(ahi, TC_LBO, TC_SBO), dal = umma_desc(alo, TC_LBO, TC_SBO);
+      const uint64_t dbh = umma_desc(bhi, TC_LBO, TC_SBO), dbl = umma_desc(blo, TC_LBO, TC_SBO);
 #pragma unroll
       for (int i = 0; i < TC_BK / 8; i++) {
-        const uint64_t dah = umma_desc(ahi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dal = umma_desc(alo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dbh = umma_desc(bhi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dbl = umma_desc(blo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        mma_tf32(dacc, dal, dbh, IDESC, i > 0 ? 1u : 0u);
-        mma_tf32(dacc, dah, dbl, IDESC, 1u);
-        mma_tf32(dacc, dah, dbh, IDESC, 1u);
+        const uint64_t o = (uint64_t)((2 * i * TC_LBO) >> 4);
+        mma_tf32(dacc, dal + o, dbh + o, IDESC, i > 0 ? 1u : 0u);
+        mma_tf32(dacc, dah + o, dbl + o, IDESC, 1u);
+        mma_tf32(dacc, dah + o, dbh + o, IDESC, 1u);
       }
       mma_commit(smem_u32(&bars[s]));
     }
@@ -391,20 +394,22 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
   for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
   auto drain = [&](int u) {
     const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
+    // every load issued, then one wait
+    uint32_t r[NHALF];
 #pragma unroll
     for (int c16 = 0; c16 < NHALF / 16; c16++) {
       const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
-      uint32_t r[16];
+      uint32_t* q = r + 16 * c16;
       asm volatile(
           "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
           "%14, %15}, [%16];"
-          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-            "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+          : "=r"(q[0]), "=r"(q[1]), "=r"(q[2]), "=r"(q[3]), "=r"(q[4]), "=r"(q[5]), "=r"(q[6]), "=r"(q[7]),
+            "=r"(q[8]), "=r"(q[9]), "=r"(q[10]), "=r"(q[11]), "=r"(q[12]), "=r"(q[13]), "=r"(q[14]), "=r"(q[15])
           : "r"(addr));
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-      for (int j = 0; j < 16; j++) acc[16 * c16 + j] += (TC)__uint_as_float(r[j]);
     }
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < NHALF; j++) acc[j] += (TC)__uint_as_float(r[j]);
   };
   // the first RING - 1 tiles in flight (one commit group per tile, empty past the end)
 #pragma unroll
@@ -429,15 +434,16 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
       const uint32_t base = smem_u32(sm + s * TC_STAGE_BYTES);
       const uint32_t ahi = base, alo = base + TC_TILE_BYTES, bhi = base + 2 * TC_TILE_BYTES, blo = bhi + TC_BTILE;
       const uint32_t dacc = tmem + (uint32_t)s * BN;
+      // K step i: the step-0 descriptors + 2 i TC_LBO bytes in the 16-byte
+      // address field (descriptor arithmetic kept off the issuing thread's path)
+      const uint64_t dah = umma_desc(ahi, TC_LBO, TC_SBO), dal = umma_desc(alo, TC_LBO, TC_SBO);
+      const uint64_t dbh = umma_desc(bhi, TC_LBO, TC_SBO), dbl = umma_desc(blo, TC_LBO, TC_SBO);
 #pragma unroll
       for (int i = 0; i < TC_BK / 8; i++) {
-        const uint64_t dah = umma_desc(ahi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dal = umma_desc(alo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dbh = umma_desc(bhi + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        const uint64_t dbl = umma_desc(blo + 2 * i * TC_LBO, TC_LBO, TC_SBO);
-        mma_tf32(dacc, dal, dbh, IDESC, i > 0 ? 1u : 0u);
-        mma_tf32(dacc, dah, dbl, IDESC, 1u);
-        mma_tf32(dacc, dah, dbh, IDESC, 1u);
+        const uint64_t o = (uint64_t)((2 * i * TC_LBO) >> 4);
+        mma_tf32(dacc, dal + o, dbh + o, IDESC, i > 0 ? 1u : 0u);
+        mma_tf32(dacc, dah + o, dbl + o, IDESC, 1u);
+        mma_tf32(dacc, dah + o, dbh + o, IDESC, 1u);
       }
       mma_commit(smem_u32(&bars[s]));
     }
