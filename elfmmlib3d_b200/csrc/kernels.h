@@ -41,8 +41,8 @@ void launch_near_batch(cudaStream_t st, const NearArgs& a, int nchunk, const int
 // of NJ x ntri rounded up to 4), the product tasks (per leaf and 128-row
 // tile: C at coff, ldc = KB x points, FP64 sums), the results ADDED to the
 // outputs, and the self pairs added in FP64 from the FP64 store at base.
-void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K, int KB,
-                          const double* store, float* out);
+void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const long long* fbase,
+                          const int* ntri, int K, int KB, const double* store, float* out);
 void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0, const double* g1,
                     const long long* soff, const int* ntri, float* S, int ntask, const GemmTask* tasks,
                     const float* A, const long long* coff, double* C, int nsrc, int ntgt, const long long* base,

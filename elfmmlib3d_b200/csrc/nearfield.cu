@@ -542,23 +542,30 @@ __device__ __forceinline__ int near_self_pos(const NearArgs& a, int i, int leaf)
 }
 
 // FP64 store [point][near triangle][K] -> FP32 [NJ t + j][KB e + c], per leaf
-// (self pairs zero).
+// at fbase[i] with rows of ceil4(KB x points) floats (padding zero; self
+// pairs zero).
 __global__ void __launch_bounds__(256)
-k_near_store_tc(const NearArgs a, const long long* __restrict__ base, const int* __restrict__ ntri, int K, int KB,
-                const double* __restrict__ store, float* __restrict__ out) {
+k_near_store_tc(const NearArgs a, const long long* __restrict__ base, const long long* __restrict__ fbase,
+                const int* __restrict__ ntri, int K, int KB, const double* __restrict__ store,
+                float* __restrict__ out) {
   const int i = blockIdx.x, leaf = a.leaves[i];
   const int sn = a.do_src ? a.box_src_count[leaf] : 0;
   const int nep = sn + (a.do_tgt ? a.box_tgt_count[leaf] : 0);
-  const long long nt = ntri[i], M = (long long)KB * nep, NJ = K / KB, tot = nep * nt * K;
+  const long long nt = ntri[i], M = (long long)KB * nep, Mp = (M + 3) & ~3LL, NJ = K / KB, tot = nep * nt * K;
   const int self = near_self_pos(a, i, leaf);
   const double* src = store + base[i];
-  float* dst = out + base[i];
+  float* dst = out + fbase[i];
   for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < tot; q += (long long)gridDim.y * blockDim.x) {
     const long long e = q / (nt * K), rem = q % (nt * K), t = rem / K, jc = rem % K;
     const long long j = jc / KB, c = jc % KB;
     const bool is_self = e < sn && self >= 0 && t == self + e;
-    dst[(t * NJ + j) * M + e * KB + c] = is_self ? 0.0f : (float)src[q];
+    dst[(t * NJ + j) * Mp + e * KB + c] = is_self ? 0.0f : (float)src[q];
   }
+  // the padding of each row
+  const long long pad = Mp - M, rows = nt * NJ;
+  for (long long q = blockIdx.y * (long long)blockDim.x + threadIdx.x; q < rows * pad;
+       q += (long long)gridDim.y * blockDim.x)
+    dst[(q / pad) * Mp + M + q % pad] = 0.0f;
 }
 
 // The self pairs of the mixed replay in FP64: per source point of the leaf
@@ -636,10 +643,10 @@ k_near_scatter_tc(const NearArgs a, int R, int KB, const long long* __restrict__
   }
 }
 
-void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const int* ntri, int K, int KB,
-                          const double* store, float* out) {
+void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* base, const long long* fbase,
+                          const int* ntri, int K, int KB, const double* store, float* out) {
   if (a.nleaf <= 0) return;
-  k_near_store_tc<<<dim3(a.nleaf, 64), 256, 0, st>>>(a, base, ntri, K, KB, store, out);
+  k_near_store_tc<<<dim3(a.nleaf, 64), 256, 0, st>>>(a, base, fbase, ntri, K, KB, store, out);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }

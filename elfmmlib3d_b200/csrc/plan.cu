@@ -859,16 +859,26 @@ bool Plan::near_tc_ready(const NearArgs& na) {
   if (!tc_enabled() || !store_valid_ || store_K_ <= 0) return false;
   if (store_tc_gen_ == store_gen_) return true;
   if (capturing_) return false;
-  const size_t tot = store_.size();
+  const int KB0 = 3 + 6 * ((store_flags_ >> 4) & 1), NJ0 = store_K_ / KB0;
+  const int dsrc = (store_flags_ >> 2) & 1, dtgt = (store_flags_ >> 3) & 1;
+  fbase_h_.resize(near_ntri_h_.size());
+  long long tot = 0;
+  for (size_t i = 0; i < near_ntri_h_.size(); i++) {
+    const long long M = (long long)KB0 * ((dsrc ? near_sc_h_[i] : 0) + (dtgt ? near_tc_h_[i] : 0));
+    fbase_h_[i] = tot;
+    tot += ((M + 3) & ~3LL) * NJ0 * near_ntri_h_[i];
+  }
   size_t freeb = 0, totb = 0;
   EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
   if ((double)tot * 4.0 > 0.8 * (double)freeb + 4.0 * (double)store_f_.cap) return false;
-  store_f_.resize(tot);
+  h2d(fbase_, fbase_h_, st_);
+  store_f_.resize((size_t)tot);
   NearArgs sa = na;
   sa.do_src = (store_flags_ >> 2) & 1;
   sa.do_tgt = (store_flags_ >> 3) & 1;
   const int KB = 3 + 6 * ((store_flags_ >> 4) & 1);
-  launch_near_store_tc(st_, sa, near_base_.get(), near_ntri_.get(), store_K_, KB, store_.get(), store_f_.get());
+  launch_near_store_tc(st_, sa, near_base_.get(), fbase_.get(), near_ntri_.get(), store_K_, KB, store_.get(),
+                       store_f_.get());
   store_tc_gen_ = store_gen_;
   return true;
 }
@@ -893,7 +903,8 @@ void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1
       co.push_back(ctot);
       for (int c0 = 0; c0 < R; c0 += 128)
         for (long long r0 = 0; r0 < M; r0 += 128)
-          tasks.push_back({near_base_h_[i], stot, ctot, (int)M, R, (int)K, (int)M, (int)Kp, (int)M, (int)r0, c0});
+          tasks.push_back({fbase_h_[i], stot, ctot, (int)M, R, (int)K, (int)((M + 3) & ~3LL), (int)Kp, (int)M,
+                           (int)r0, c0});
       stot += R * Kp;
       ctot += R * M;
     }

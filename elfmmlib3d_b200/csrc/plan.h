@@ -318,6 +318,10 @@ class Plan {
   // the tensor cores (built from store generation store_tc_gen_), the
   // per-leaf product tasks and the density / product scratch
   DevBuf<float> store_f_, ntc_scratch_;
+  // the FP32 copy's per-leaf offsets (16-byte aligned, rows padded to a
+  // multiple of 4 floats, so that its tiles copy with 16-byte cp.async)
+  std::vector<long long> fbase_h_;
+  DevBuf<long long> fbase_;
   DevBuf<double> ntc_cbuf_;
   DevBuf<long long> ntc_soff_, ntc_coff_;
   DevBuf<GemmTask> ntc_tasks_;
