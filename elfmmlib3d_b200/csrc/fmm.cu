@@ -2234,12 +2234,14 @@ bool launch_l2t_img(cudaStream_t st, int nleaf, const L2TArgs& a, int R, long lo
 template <class T>
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* goff, const long long* soff, int max_pts, T* Gbuf, T* Sbuf,
-                         int ntask, const GemmTask* tasks, const T* local, bool image) {
+                         int ntask, const GemmTask* tasks, const T* local, bool image, bool do_g) {
   if (nwleaf <= 0) return;
   const int nc = ncoef(a.p);
   const int smem = (int)(sizeof(cplx) * 8 * nc);
-  EFMM_CUDA_TRY(smem_raise(k_l2t_features<T>, (int)(smem)));
-  k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
+  if (do_g) {
+    EFMM_CUDA_TRY(smem_raise(k_l2t_features<T>, (int)(smem)));
+    k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
+  }
   gemm_product<T>(st, ntask, tasks, Gbuf, local, Sbuf);
   if (image)
     k_l2t_finish_img<T><<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, Sbuf);
@@ -2250,10 +2252,10 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
 }
 template void launch_l2t_twostage<double>(cudaStream_t, const L2TArgs&, int, int, const int*, const long long*,
                                           const long long*, int, double*, double*, int, const GemmTask*,
-                                          const double*, bool);
+                                          const double*, bool, bool);
 template void launch_l2t_twostage<float>(cudaStream_t, const L2TArgs&, int, int, const int*, const long long*,
                                          const long long*, int, float*, float*, int, const GemmTask*,
-                                         const float*, bool);
+                                         const float*, bool, bool);
 
 // Stage 1 of the factored P2M for one wave of leaves: unit-density
 // multipoles H (nk = 4 or 7 kinds, per leaf at hoff: [kind][ns tn][D]) and
@@ -2263,12 +2265,18 @@ template void launch_l2t_twostage<float>(cudaStream_t, const L2TArgs&, int, int,
 // shared memory.
 template <class T>
 bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
-                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S) {
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h) {
   const int nc = ncoef(a.p);
   const bool fp32 = sizeof(T) == 4;
   const size_t smem = p2m_unit_smem(a.p, fp32);
   if (smem > 227 * 1024 || (fp32 && !a.wnorm)) return false;
   if (nwleaf <= 0) return true;
+  if (!do_h) {
+    k_p2m_sigma<T><<<dim3(nwleaf, 8), 256, 0, st>>>(a, R, wleaves, soff, sbase, ns, S);
+    count_launch();
+    EFMM_CUDA_TRY(cudaGetLastError());
+    return true;
+  }
   const dim3 grid(nwleaf, (maxtn + UNIT_TB - 1) / UNIT_TB);
   // the fewest threads (whole warp quadruples) that cover the coefficients in ceil(nc / NT) rounds
   const int NT = fp32 ? UNITF_THREADS : unit_threads<T>();
@@ -2306,9 +2314,9 @@ size_t p2m_unit_smem(int p, bool fp32) {
          (18 + 12 * 4) * sizeof(double);
 }
 template bool launch_p2m_unit<double>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
-                                      const long long*, const long long*, int, int, double*, double*);
+                                      const long long*, const long long*, int, int, double*, double*, bool);
 template bool launch_p2m_unit<float>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
-                                     const long long*, const long long*, int, int, float*, float*);
+                                     const long long*, const long long*, int, int, float*, float*, bool);
 
 // The batched product of the two-stage P2M: FP32 on the tensor cores
 // (tc_gemm.cu) unless ELFMM3D_TC=0, FP64 (and FP32 when disabled) on the

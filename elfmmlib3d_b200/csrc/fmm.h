@@ -112,10 +112,12 @@ bool launch_l2t_gemm(cudaStream_t st, int nchunk, const int* chunk_leaf, const i
 // and their recombination (k_l2t_finish_img).
 // T = float: normalised-basis functionals (L2TArgs.wnorm) and FP32
 // normalised local expansions, the product on the tensor cores.
+// do_g = false: the functionals at goff are already there (resident from an
+// earlier pass over the same geometry) and are not recomputed.
 template <class T>
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* goff, const long long* soff, int max_pts, T* Gbuf, T* Sbuf,
-                         int ntask, const GemmTask* tasks, const T* local, bool image = false);
+                         int ntask, const GemmTask* tasks, const T* local, bool image = false, bool do_g = true);
 // Two-stage P2M of the half-space image columns (7R per box, tasks cut by
 // the caller): node features with second-derivative rows (9 x 12 x
 // triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12
@@ -128,10 +130,11 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
 // (per leaf at soff, R rows of ns x triangles rounded up to a multiple of 4).
 // Stage 2 is gemm_product with K = ns x triangles, N = R.  False (nothing
 // launched) when the order is too high for its shared memory
-// (p2m_unit_smem(p, T is float) > 227 KB).
+// (p2m_unit_smem(p, T is float) > 227 KB).  do_h = false: H is already
+// there (resident from an earlier pass) and only S is formed.
 template <class T>
 bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
-                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S);
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h = true);
 size_t p2m_unit_smem(int p, bool fp32);
 // Direct P2M of the image columns (one CTA per leaf and right-hand side):
 // columns kind * R + r of 6R per box (kinds 0..5) and the U column at

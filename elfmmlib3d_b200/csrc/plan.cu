@@ -1159,6 +1159,9 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
   if (points_) return IER_BADARG;  // particles: the single-right-hand-side FP64 form only
   switch_precision(precision == 1);
   MixedOrders orders(this, precision == 1);
+  // the mixed form's geometry-only features stay resident for passes that
+  // repeat on the same geometry (store / replay, graph replays)
+  resident_ = precision == 1 && (mode != 0 || graph_pass_);
   const int n = n_, nt = nt_;
   if (mode) {
     const int dosl = d_ssl != nullptr, dodl = d_sdl != nullptr;
@@ -1209,6 +1212,15 @@ int Plan::evaluate_batch(double rlam, double rmu, int R, const double* d_ssl, co
 // scratch budget (at most 8 GB or a quarter of the free memory).  The waves
 // (leaves, offsets, product tasks) are built and uploaded once per column
 // count and element type; later passes (and graph captures) only launch.
+// Whether features of elems elements of esz bytes may stay resident: at
+// most a third of the free memory (what the scratch already holds counts as
+// free).
+bool Plan::resident_fits(long long elems, size_t esz, size_t cap_bytes) {
+  size_t freeb = 0, totb = 0;
+  EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+  return (double)elems * (double)esz <= ((double)freeb + (double)cap_bytes) / 3.0;
+}
+
 template <class T>
 void Plan::p2m_twostage(const P2MArgs& pa, int R, T* mpole) {
   const int D = 2 * ncoef(p_), C = 4 * R;
@@ -1289,13 +1301,24 @@ bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
   // density components carried: single layer 0..2, double layer 3..5
   const int sbase = pa.dosl ? 0 : 3, ns = (pa.dosl && pa.dodl) ? 6 : 3;
   WaveSet& W = p2m_waves_;
-  const long long key = ((long long)p_ << 40) | ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) | (sizeof(T) << 2) | (image ? 3 : 1);
+  const long long key = ((long long)p_ << 40) | ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) |
+                        (sizeof(T) << 2) | (image ? 3 : 1) | ((long long)resident_ << 62);
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    const size_t budget =
-        std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double)) / sizeof(T);
+    size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + p2m_scratch_.cap * sizeof(double)) / sizeof(T);
+    bool res = false;
+    if (resident_) {
+      long long all = 0;
+      for (size_t j = 0; j < p2m_h_.size(); j++) {
+        const long long K = (long long)ns * p2m_sc_h_[j];
+        all += nk * K * D + R * ((K + 3) & ~3LL);
+      }
+      res = resident_fits(all, sizeof(T), p2m_scratch_.cap * sizeof(double));
+      if (res) budget = (size_t)all;
+    }
     W.clear();
+    W.resident = res;
     std::vector<int> wl;
     std::vector<long long> ho, so;
     std::vector<GemmTask> tasks;
@@ -1347,12 +1370,14 @@ bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
   p2m_scratch_.resize((maxu * sizeof(T) + sizeof(double) - 1) / sizeof(double));
   T* scratch = reinterpret_cast<T*>(p2m_scratch_.get());
   const int bn = R <= 64 ? 64 : 128;
+  const bool do_h = !(W.resident && W.feat_valid);
   for (const auto& w : W.w) {
     if (!launch_p2m_unit<T>(st_, pa, R, nk, w.nwl, w.maxn, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
-                            W.off2.get() + w.wl0, sbase, ns, scratch, scratch))
+                            W.off2.get() + w.wl0, sbase, ns, scratch, scratch, do_h))
       return false;
     product_timed<T>(w.ntask, W.htasks, w.t0, W.tasks.get() + w.t0, scratch, scratch, mpole, bn);
   }
+  W.feat_valid = W.resident;
   return true;
 }
 template bool Plan::p2m_factored<double>(const P2MArgs&, int, double*, bool);
@@ -1368,12 +1393,25 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
   WaveSet& W = l2t_waves_;
-  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1 |
+                        ((long long)resident_ << 62);
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    bool res = false;
+    if (resident_) {
+      long long all = 0;
+      for (size_t j = 0; j < l2t_h_.size(); j++) {
+        const int P = (do_src ? l2t_sc_h_[j] : 0) + (do_tgt ? l2t_tc_h_[j] : 0);
+        const long long LD = 9 * P + ((9 * P) & 1);
+        all += (long long)D * LD + (long long)C * LD;
+      }
+      res = resident_fits(all, esz, l2t_scratch_.cap * sizeof(double));
+      if (res) budget = (size_t)all;
+    }
     W.clear();
+    W.resident = res;
     std::vector<int> wl;
     std::vector<long long> go, so;
     std::vector<GemmTask> tasks;
@@ -1414,18 +1452,20 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
   size_t maxu = 1;
   for (const auto& w : W.w) maxu = std::max(maxu, (size_t)w.used);
   l2t_scratch_.resize((maxu * esz + sizeof(double) - 1) / sizeof(double));
+  const bool do_g = !(W.resident && W.feat_valid);
   for (const auto& w : W.w) {
     if (mixed) {
       float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
       launch_l2t_twostage<float>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
                                  W.off2.get() + w.wl0, w.maxn, sc, sc, w.ntask, W.tasks.get() + w.t0,
-                                 local_f_.get());
+                                 local_f_.get(), false, do_g);
     } else {
       launch_l2t_twostage<double>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
                                   W.off2.get() + w.wl0, w.maxn, l2t_scratch_.get(), l2t_scratch_.get(), w.ntask,
-                                  W.tasks.get() + w.t0, local_.get());
+                                  W.tasks.get() + w.t0, local_.get(), false, do_g);
     }
   }
+  W.feat_valid = W.resident;
 }
 
 int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
@@ -1764,6 +1804,10 @@ int Plan::evaluate_batch_graph(double rlam, double rmu, int R, const double* d_s
                                    (double)(uintptr_t)d_u_src, (double)(uintptr_t)d_e_src,
                                    (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision,
                                    (double)mode};
+  struct Flag {
+    bool& f;
+    ~Flag() { f = false; }
+  } flag{graph_pass_ = true};
   return run_graph(key, [&]() {
     return evaluate_batch(rlam, rmu, R, d_ssl, d_sdl, d_u_src, d_e_src, d_u_tgt, d_e_tgt, precision, mode);
   });
@@ -1774,6 +1818,10 @@ int Plan::evaluate_image_graph(double rlam, double rmu, int R, const double* d_s
   if (R < 1 || R > 64) return IER_BADARG;  // one pass per call, as above
   const std::vector<double> key = {2.0, rlam, rmu, (double)R, (double)(uintptr_t)d_ssl, (double)(uintptr_t)d_sdl,
                                    (double)(uintptr_t)d_u_tgt, (double)(uintptr_t)d_e_tgt, (double)precision};
+  struct Flag {
+    bool& f;
+    ~Flag() { f = false; }
+  } flag{graph_pass_ = true};
   return run_graph(key, [&]() {
     return evaluate_image(rlam, rmu, R, d_ssl, d_sdl, d_u_tgt, d_e_tgt, precision, 2);
   });
@@ -2086,12 +2134,24 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
   la.wnorm = mixed ? ops_->wnorm.get() : nullptr;
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
   WaveSet& W = l2t_waves_;
-  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | 3;
+  const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | 3 | ((long long)resident_ << 62);
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    const size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    size_t budget = std::min<size_t>((size_t)8 << 30, freeb / 4 + l2t_scratch_.cap * sizeof(double)) / esz;
+    bool res = false;
+    if (resident_) {
+      long long all = 0;
+      for (size_t j = 0; j < l2t_h_.size(); j++) {
+        const int P = l2t_tc_h_[j];
+        const long long LD = 9 * P + ((9 * P) & 1);
+        all += (long long)D * LD + (long long)C * LD;
+      }
+      res = resident_fits(all, esz, l2t_scratch_.cap * sizeof(double));
+      if (res) budget = (size_t)all;
+    }
     W.clear();
+    W.resident = res;
     std::vector<int> wl;
     std::vector<long long> go, so;
     std::vector<GemmTask> tasks;
@@ -2136,17 +2196,20 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
   size_t maxu = 1;
   for (const auto& w : W.w) maxu = std::max(maxu, (size_t)w.used);
   l2t_scratch_.resize((maxu * esz + sizeof(double) - 1) / sizeof(double));
+  const bool do_g = !(W.resident && W.feat_valid);
   for (const auto& w : W.w) {
     if (mixed) {
       float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
       launch_l2t_twostage<float>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
-                                 W.off2.get() + w.wl0, w.maxn, sc, sc, w.ntask, W.tasks.get() + w.t0, local_f, true);
+                                 W.off2.get() + w.wl0, w.maxn, sc, sc, w.ntask, W.tasks.get() + w.t0, local_f, true,
+                                 do_g);
     } else {
       launch_l2t_twostage<double>(st_, la, R, w.nwl, W.leaves.get() + w.wl0, W.off1.get() + w.wl0,
                                   W.off2.get() + w.wl0, w.maxn, l2t_scratch_.get(), l2t_scratch_.get(), w.ntask,
-                                  W.tasks.get() + w.t0, local, true);
+                                  W.tasks.get() + w.t0, local, true, do_g);
     }
   }
+  W.feat_valid = W.resident;
 }
 
 int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, const double* d_sdl,
@@ -2155,6 +2218,7 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
   if (!mindlin_ || rmu <= 0 || rlam + 2 * rmu <= 0) return IER_BADARG;
   if (points_ && (precision != 0 || 7 * R >= 32)) return IER_BADARG;  // particles: FP64, at most 4 right-hand sides
   switch_precision(precision == 1);
+  resident_ = precision == 1 && (mode != 0 || graph_pass_);
   const int nt = nt_;
   if (nt == 0 || !(d_u_tgt || d_e_tgt)) return IER_OK;
   if (!(d_ssl || d_sdl)) {

@@ -122,6 +122,9 @@ struct WaveSet {
     long long used, nodes;
   };
   long long key = -1;
+  // resident: one wave whose geometry-only features (unit multipoles, L2T
+  // functionals) stay in the scratch between passes; feat_valid: computed
+  bool resident = false, feat_valid = false;
   std::vector<Wave> w;
   std::vector<GemmTask> htasks;
   DevBuf<int> leaves;
@@ -129,6 +132,7 @@ struct WaveSet {
   DevBuf<GemmTask> tasks;
   void clear() {
     key = -1;
+    resident = feat_valid = false;
     w.clear();
     htasks.clear();
   }
@@ -241,6 +245,10 @@ class Plan {
   void build_chunks(int do_src, int do_tgt);
   bool mindlin_ = false, img_sched_ = false;
   bool forest_on_ = false;
+  // keep the geometry-only features of the two-stage P2M / L2T between
+  // passes when they fit (store / replay and graph passes)
+  bool resident_ = false, graph_pass_ = false;
+  bool resident_fits(long long elems, size_t esz, size_t cap_bytes);
   int leaf_override_ = 0;
   double forest_[5] = {0, 0, 0, 0, 0};
   TransSched m2lv_img_, m2lu_, l2l_img_, l2l_img_u_, m2m_u_;
