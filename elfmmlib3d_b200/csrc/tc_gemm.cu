@@ -259,12 +259,17 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
 // elements one by one (zero-filled past the matrix).  Bounded waits and the
 // per-K-tile FP32 drain as in k_gemm_tc.
 template <int BN>
-__host__ __device__ constexpr int tc_ring_depth() { return BN == 64 ? 4 : 3; }
+__host__ __device__ constexpr int tc_ring_depth() { return 3; }
+// split stages (and TMEM accumulators): the drain of a K tile trails its MMAs
+// by tc_ring_stages - 1 tiles, so that the tensor cores' completion latency
+// of that many tiles is hidden
+template <int BN>
+__host__ __device__ constexpr int tc_ring_stages() { return BN == 64 ? 3 : 2; }
 template <int BN>
 __host__ __device__ constexpr int tc_raw_bytes() { return TC_BM * TC_BK * 4 + BN * TC_BK * 4; }
 template <int BN>
 __host__ __device__ constexpr int tc_ring_smem() {
-  return 2 * tc_stage_bytes<BN>() + tc_ring_depth<BN>() * tc_raw_bytes<BN>() + 1024 + 64;
+  return tc_ring_stages<BN>() * tc_stage_bytes<BN>() + tc_ring_depth<BN>() * tc_raw_bytes<BN>() + 1024 + 64;
 }
 
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, int srcbytes) {
@@ -280,6 +285,8 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
                TC* __restrict__ Cm, int* __restrict__ err) {
   constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
   constexpr int RING = tc_ring_depth<BN>(), RAW = tc_raw_bytes<BN>(), RAW_A = TC_BM * TC_BK * 4;
+  constexpr int NST = tc_ring_stages<BN>(), LAG = NST - 1;
+  constexpr uint32_t TMEM_COLS = NST * BN <= 256 ? 256 : 512;
   constexpr int RG = BN / 8, NB = BN / 32, NHALF = BN / 2;
   constexpr int NCA = TC_BM * TC_BK / 4 / TC_THREADS;  // A chunks of 16 bytes per thread and tile (4)
   constexpr int NCB = BN * TC_BK / 4 / TC_THREADS;     // B chunks per thread and tile (2 or 4)
@@ -287,21 +294,20 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
   extern __shared__ __align__(1024) unsigned char tc_ring_raw[];
   const uint32_t raw = smem_u32(tc_ring_raw);
   unsigned char* sm = tc_ring_raw + ((1024 - (raw & 1023)) & 1023);
-  unsigned char* ring = sm + 2 * TC_STAGE_BYTES;
+  unsigned char* ring = sm + NST * TC_STAGE_BYTES;
   uint64_t* bars = reinterpret_cast<uint64_t*>(ring + RING * RAW);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ring + RING * RAW + 16);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(ring + RING * RAW + 32);
   const GemmTask t = tasks[blockIdx.x];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                 "r"(2 * BN)
+                 "r"(TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 0) {
-    mbar_init(smem_u32(&bars[0]), 1);
-    mbar_init(smem_u32(&bars[1]), 1);
+    for (int i = 0; i < NST; i++) mbar_init(smem_u32(&bars[i]), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -393,7 +399,7 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
 #pragma unroll
   for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
   auto drain = [&](int u) {
-    const uint32_t col0 = (uint32_t)(u & 1) * BN + NHALF * half;
+    const uint32_t col0 = (uint32_t)(u % NST) * BN + NHALF * half;
     // every load issued, then one wait
     uint32_t r[NHALF];
 #pragma unroll
@@ -420,12 +426,12 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
   bool ok = true;
   int issued = -1;  // last tile whose MMAs were issued
   for (int kt = 0; kt < nkt; kt++) {
-    const int s = kt & 1;
+    const int s = kt % NST;
     asm volatile("cp.async.wait_group %0;" ::"n"(RING - 2) : "memory");
     __syncthreads();  // tile kt landed for every thread; slot of tile kt - 1 converted
     issue(kt + RING - 1);
     asm volatile("cp.async.commit_group;" ::: "memory");
-    convert(kt, s);  // stage s is free: tile kt - 2 finished before tile kt - 1 was drained
+    convert(kt, s);  // stage s is free: tile kt - NST finished before tile kt - 1 - LAG was drained
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -448,9 +454,9 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
       mma_commit(smem_u32(&bars[s]));
     }
     issued = kt;
-    if (kt >= 1) {
-      const int u = kt - 1;
-      ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+    if (kt >= LAG) {
+      const int u = kt - LAG;
+      ok = mbar_wait(smem_u32(&bars[u % NST]), (u / NST) & 1);
       ok = __syncthreads_and(ok);
       if (!ok) break;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -459,18 +465,20 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");  // no copy outlives the CTA
-  if (ok && nkt > 0) {
-    const int u = nkt - 1;
-    ok = mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+  // the last LAG tiles
+  for (int u = nkt > LAG ? nkt - LAG : 0; ok && u < nkt; u++) {
+    ok = mbar_wait(smem_u32(&bars[u % NST]), (u / NST) & 1);
     ok = __syncthreads_and(ok);
     if (ok) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       drain(u);
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
   }
   if (!ok) {
     if (tid == 0) atomicExch(err, 1);
-    for (int u = (issued >= 1 ? issued - 1 : 0); u <= issued; u++) mbar_wait(smem_u32(&bars[u & 1]), (u >> 1) & 1);
+    for (int u = (issued >= LAG ? issued - LAG : 0); u <= issued; u++)
+      mbar_wait(smem_u32(&bars[u % NST]), (u / NST) & 1);
   } else {
     const int row = t.row0 + 32 * quarter + lane;
     if (row < t.M) {
@@ -485,7 +493,7 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * BN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS) : "memory");
 }
 
 namespace {
