@@ -260,6 +260,7 @@ k_gemm_tc(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const
 // per-K-tile FP32 drain as in k_gemm_tc.
 template <int BN>
 __host__ __device__ constexpr int tc_ring_depth() { return 3; }
+constexpr int TC_RING_THREADS = 512;  // 16 warps: 4 TMEM lane quarters x 4 column parts
 // split stages (and TMEM accumulators): the drain of a K tile trails its MMAs
 // by tc_ring_stages - 1 tiles, so that the tensor cores' completion latency
 // of that many tiles is hidden
@@ -280,16 +281,17 @@ __device__ __forceinline__ void cp_async4(uint32_t dst, const void* src, int src
 }
 
 template <int BN, class TC>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TC_RING_THREADS, 1)
 k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, const float* __restrict__ B,
                TC* __restrict__ Cm, int* __restrict__ err) {
   constexpr int TC_STAGE_BYTES = tc_stage_bytes<BN>(), TC_BTILE = BN * TC_BK * 4;
   constexpr int RING = tc_ring_depth<BN>(), RAW = tc_raw_bytes<BN>(), RAW_A = TC_BM * TC_BK * 4;
   constexpr int NST = tc_ring_stages<BN>(), LAG = NST - 1;
   constexpr uint32_t TMEM_COLS = NST * BN <= 256 ? 256 : 512;
-  constexpr int RG = BN / 8, NB = BN / 32, NHALF = BN / 2;
-  constexpr int NCA = TC_BM * TC_BK / 4 / TC_THREADS;  // A chunks of 16 bytes per thread and tile (4)
-  constexpr int NCB = BN * TC_BK / 4 / TC_THREADS;     // B chunks per thread and tile (2 or 4)
+  constexpr int RT = TC_RING_THREADS, NW = RT / 32;
+  constexpr int RG = BN / 8, NBW = BN / 4 / NW, NPART = BN / 4;
+  constexpr int NCA = TC_BM * TC_BK / 4 / RT;  // A chunks of 16 bytes per thread and tile (2)
+  constexpr int NCB = BN * TC_BK / 4 / RT;     // B chunks per thread and tile (1 or 2)
   constexpr uint32_t IDESC = tc_idesc_mn(TC_BM, BN);
   extern __shared__ __align__(1024) unsigned char tc_ring_raw[];
   const uint32_t raw = smem_u32(tc_ring_raw);
@@ -327,7 +329,7 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     const int k0 = kt * TC_BK;
 #pragma unroll
     for (int it = 0; it < NCA; it++) {
-      const int c = tid + TC_THREADS * it, k = c >> 5, mc = c & 31;
+      const int c = tid + RT * it, k = c >> 5, mc = c & 31;
       const int gk = k0 + k, gm = t.row0 + 4 * mc;
       const uint32_t d = slot + (uint32_t)(k * TC_BM + 4 * mc) * 4;
       const float* g = Ab + (size_t)gk * t.lda + gm;
@@ -343,7 +345,7 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     }
 #pragma unroll
     for (int it = 0; it < NCB; it++) {
-      const int c = tid + TC_THREADS * it, n = c >> 3, kc = c & 7;
+      const int c = tid + RT * it, n = c >> 3, kc = c & 7;
       const int gn = t.col0 + n, gk = k0 + 4 * kc;
       const uint32_t d = slot + RAW_A + (uint32_t)(n * 128 + ((kc ^ (n & 7)) * 16));
       const float* g = Bb + (size_t)gn * t.ldb + gk;
@@ -364,8 +366,8 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     const float* ra = reinterpret_cast<const float*>(slot);
     unsigned char* st = sm + s * TC_STAGE_BYTES;
 #pragma unroll
-    for (int it = 0; it < 4; it++) {
-      const int b = it * 8 + warp;
+    for (int it = 0; it < 32 / NW; it++) {
+      const int b = it * NW + warp;
       const int m = 32 * (b & 3) + lane, ca = b >> 2;
       float v[4];
 #pragma unroll
@@ -380,8 +382,8 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
       *reinterpret_cast<float4*>(st + TC_TILE_BYTES + offa) = lo;
     }
 #pragma unroll
-    for (int it = 0; it < NB; it++) {
-      const int b = it * 8 + warp;
+    for (int it = 0; it < NBW; it++) {
+      const int b = it * NW + warp;
       const int n = 8 * (b % RG) + (lane & 7), kc = 4 * (b / RG) + (lane >> 3);
       const float4 v = *reinterpret_cast<const float4*>(slot + RAW_A + n * 128 + ((kc ^ (n & 7)) * 16));
       const uint32_t offb = (n & 7) * 16 + kc * TC_LBO + (n >> 3) * TC_SBO;
@@ -394,16 +396,18 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
       *reinterpret_cast<float4*>(st + 2 * TC_TILE_BYTES + TC_BTILE + offb) = lo;
     }
   };
-  const int quarter = warp & 3, half = warp >> 2;
-  TC acc[NHALF];
+  // drain: warp w reads TMEM lanes 32 (w % 4) .. + 31 (rows), columns
+  // NPART (w / 4) .. + NPART - 1
+  const int quarter = warp & 3, part = warp >> 2;
+  TC acc[NPART];
 #pragma unroll
-  for (int j = 0; j < NHALF; j++) acc[j] = (TC)0;
+  for (int j = 0; j < NPART; j++) acc[j] = (TC)0;
   auto drain = [&](int u) {
-    const uint32_t col0 = (uint32_t)(u % NST) * BN + NHALF * half;
+    const uint32_t col0 = (uint32_t)(u % NST) * BN + NPART * part;
     // every load issued, then one wait
-    uint32_t r[NHALF];
+    uint32_t r[NPART];
 #pragma unroll
-    for (int c16 = 0; c16 < NHALF / 16; c16++) {
+    for (int c16 = 0; c16 < NPART / 16; c16++) {
       const uint32_t addr = tmem + ((uint32_t)(32 * quarter) << 16) + col0 + 16 * c16;
       uint32_t* q = r + 16 * c16;
       asm volatile(
@@ -415,7 +419,7 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     }
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int j = 0; j < NHALF; j++) acc[j] += (TC)__uint_as_float(r[j]);
+    for (int j = 0; j < NPART; j++) acc[j] += (TC)__uint_as_float(r[j]);
   };
   // the first RING - 1 tiles in flight (one commit group per tile, empty past the end)
 #pragma unroll
@@ -484,8 +488,8 @@ k_gemm_tc_ring(const GemmTask* __restrict__ tasks, const float* __restrict__ A, 
     if (row < t.M) {
       TC* Cp = Cm + t.c_off + row;
 #pragma unroll
-      for (int j = 0; j < NHALF; j++) {
-        const int col = t.col0 + NHALF * half + j;
+      for (int j = 0; j < NPART; j++) {
+        const int col = t.col0 + NPART * part + j;
         if (col < t.N) Cp[(size_t)col * t.ldc] = acc[j];
       }
     }
@@ -549,10 +553,10 @@ static void launch_gemm_tc_t(cudaStream_t st, int ntask, const GemmTask* tasks, 
   if (tc_ring_variant()) {
     if (bn == 64) {
       EFMM_CUDA_TRY(smem_raise(k_gemm_tc_ring<64, TC>, (int)(tc_ring_smem<64>())));
-      k_gemm_tc_ring<64, TC><<<ntask, TC_THREADS, tc_ring_smem<64>(), st>>>(tasks, A, B, C, err);
+      k_gemm_tc_ring<64, TC><<<ntask, TC_RING_THREADS, tc_ring_smem<64>(), st>>>(tasks, A, B, C, err);
     } else {
       EFMM_CUDA_TRY(smem_raise(k_gemm_tc_ring<128, TC>, (int)(tc_ring_smem<128>())));
-      k_gemm_tc_ring<128, TC><<<ntask, TC_THREADS, tc_ring_smem<128>(), st>>>(tasks, A, B, C, err);
+      k_gemm_tc_ring<128, TC><<<ntask, TC_RING_THREADS, tc_ring_smem<128>(), st>>>(tasks, A, B, C, err);
     }
     count_launch();
     EFMM_CUDA_TRY(cudaGetLastError());
