@@ -364,9 +364,9 @@ def make_uneven_problems(w, world=1, rank=None):
 
 # FP64 operations per near-field (point, triangle) pair of the analytic
 # kernel: ncu thread-instruction counts of k_near_leaf on the sphere-5120 case,
-# (dadd + dmul + 2 dfma) / pairs = (0.984e9 + 1.749e9 + 2 * 3.029e9) / 3.194e6
+# (dadd + dmul + 2 dfma) / pairs = (0.999e9 + 1.749e9 + 2 * 3.029e9) / 3.193e6
 # (profiles/near_leaf_sphere5120.md)
-NEAR_FLOPS_PER_PAIR = 2752.0
+NEAR_FLOPS_PER_PAIR = 2758.0
 
 
 def run_ours(args, rank, world, local_rank):
