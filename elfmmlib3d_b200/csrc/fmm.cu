@@ -19,6 +19,23 @@
 
 namespace efmm {
 
+// Origin o of the Lame decomposition for the points of box: the linear
+// pass carries the charge (y - o).sigma and the recombination reads
+// u_a = (2 - c1) phi_a - c1 (x - o)_j d_a phi_j + d_a Phi_4, which gives the
+// same field for every o shared by a source and a target.  In a forest of
+// problems (flev >= 0) o is the centre (x, y) of the box's column of level
+// flev, so that the FP32 forms see coordinates of the problem's own size
+// rather than of its offset in the forest; else o = 0.  o_z is always 0
+// (the half-space image formulas read the absolute depth).
+__device__ __forceinline__ void lame_origin(const int* ijk, const int* level, int box, const double* c0, double size,
+                                            int flev, double o[3]) {
+  o[0] = o[1] = o[2] = 0.0;
+  const int sh = level[box] - flev;
+  if (flev < 0 || sh < 0) return;
+  const double w = size / (double)(1 << flev);
+  for (int d = 0; d < 2; d++) o[d] = c0[d] - 0.5 * size + (((ijk[3 * box + d] - 1) >> sh) + 0.5) * w;
+}
+
 // -------------------------------------------------------------- operators
 // Build one real operator matrix per CTA.  kind 0: M2L (offset vector in box
 // units), kind 1: M2M (child centre - parent centre, parent units), kind 2:
@@ -67,6 +84,8 @@ k_p2m(const P2MArgs a) {
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
   int t0 = a.sstart[box], tn = a.scount[box];
   int nnode = a.points ? tn : 12 * tn;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   const int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
   double acc[CMAX][4][2];
 #pragma unroll
@@ -131,10 +150,12 @@ k_p2m(const P2MArgs a) {
           for (int d = 0; d < 3; d++) o[4 + 3 * j + d] = w * 0.5 * (nn[d] * dl[j] + dl[d] * nn[j]);
         }
         // pass 3: charge (s_sl.y) c1/(2mu) + (s_dl.n) c2, dipole c1 [n (s_dl.y) + s_dl (n.y)]/2
-        double sly = sl[0] * y[0] + sl[1] * y[1] + sl[2] * y[2];
-        double dly = dl[0] * y[0] + dl[1] * y[1] + dl[2] * y[2];
+        // (y relative to the origin of lame_origin)
+        const double yo[3] = {y[0] - org[0], y[1] - org[1], y[2] - org[2]};
+        double sly = sl[0] * yo[0] + sl[1] * yo[1] + sl[2] * yo[2];
+        double dly = dl[0] * yo[0] + dl[1] * yo[1] + dl[2] * yo[2];
         double dln = dl[0] * nn[0] + dl[1] * nn[1] + dl[2] * nn[2];
-        double ny = nn[0] * y[0] + nn[1] * y[1] + nn[2] * y[2];
+        double ny = nn[0] * yo[0] + nn[1] * yo[1] + nn[2] * yo[2];
         o[3] = w * (sly * c1 * inv2mu + dln * c2);
         for (int d = 0; d < 3; d++) o[13 + d] = w * 0.5 * c1 * (nn[d] * dly + dl[d] * ny);
       }
@@ -217,6 +238,8 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
   const int t0 = a.sstart[box], tn = a.scount[box];
   const int nnode = 12 * tn;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   Quad12 Q;
   quad12(Q);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -269,8 +292,8 @@ k_p2m_gemm(const P2MArgs a, int R, T* __restrict__ mpole) {
           const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
                                 e1[0] * e2[1] - e1[1] * e2[0]};
           const double area = 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
-          double* o = nd + 8 * warp;
-          o[0] = y[0]; o[1] = y[1]; o[2] = y[2];
+          double* o = nd + 8 * warp;  // position relative to the origin of lame_origin
+          o[0] = y[0] - org[0]; o[1] = y[1] - org[1]; o[2] = y[2] - org[2];
           const double* nn = a.nrm + 3 * (size_t)it;
           o[3] = nn[0]; o[4] = nn[1]; o[5] = nn[2];
           o[6] = Q.w[iq] * area;
@@ -411,14 +434,17 @@ k_p2m_features(const P2MArgs a, const int* __restrict__ wleaves, const long long
   const double z[3] = {(y[0] - c[0]) * is, (y[1] - c[1]) * is, (y[2] - c[2]) * is};
   const double r2 = z[0] * z[0] + z[1] * z[1] + z[2] * z[2];
   if (lane == 0) {
-    // node record for the weights: position, normal, weight x area, triangle
+    // node record for the weights: position (relative to the origin of
+    // lame_origin), normal, weight x area, triangle
     const double e1[3] = {Tr[3] - Tr[0], Tr[4] - Tr[1], Tr[5] - Tr[2]};
     const double e2[3] = {Tr[6] - Tr[0], Tr[7] - Tr[1], Tr[8] - Tr[2]};
     const double cr[3] = {e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2],
                           e1[0] * e2[1] - e1[1] * e2[0]};
     double* o = nrec + 8 * (noff[blockIdx.x] + node);
     const double* nn = a.nrm + 3 * (size_t)it;
-    o[0] = y[0]; o[1] = y[1]; o[2] = y[2];
+    double org[3];
+    lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
+    o[0] = y[0] - org[0]; o[1] = y[1] - org[1]; o[2] = y[2] - org[2];
     o[3] = nn[0]; o[4] = nn[1]; o[5] = nn[2];
     o[6] = Q.w[iq] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
     o[7] = (double)it;
@@ -719,6 +745,8 @@ k_p2m_unit(const P2MArgs a, const int* __restrict__ wleaves, const long long* __
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, q2 = is * is;
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   for (int i = tid; i < 12 * NY; i += NTr) Ys[i] = {0.0, 0.0};
   for (int i = tid; i < nc; i += NTr) {
     int n = 0;
@@ -765,7 +793,8 @@ k_p2m_unit(const P2MArgs a, const int* __restrict__ wleaves, const long long* __
                               e1[0] * e2[1] - e1[1] * e2[0]};
         const double w = Q.w[j] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
         T* gq = geo + 4 * j;
-        gq[0] = (T)w; gq[1] = (T)(w * y[0]); gq[2] = (T)(w * y[1]); gq[3] = (T)(w * y[2]);
+        gq[0] = (T)w; gq[1] = (T)(w * (y[0] - org[0])); gq[2] = (T)(w * (y[1] - org[1]));
+        gq[3] = (T)(w * (y[2] - org[2]));
       }
       cplx pw = {1.0, 0.0}, b = {-0.5 * z[0], -0.5 * z[1]};
       for (int e = m; e; e >>= 1) {
@@ -928,6 +957,8 @@ k_p2m_unit_f(const P2MArgs a, const int* __restrict__ wleaves, const long long* 
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, q2 = is * is;
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   for (int i = tid; i < 2 * 12 * NY; i += NTr) Yb[i] = make_float2(0.f, 0.f);
   for (int i = tid; i < nc; i += NTr) {
     int n = 0;
@@ -972,7 +1003,8 @@ k_p2m_unit_f(const P2MArgs a, const int* __restrict__ wleaves, const long long* 
                               e1[0] * e2[1] - e1[1] * e2[0]};
         const double w = Q.w[j] * 0.5 * sqrt(cr[0] * cr[0] + cr[1] * cr[1] + cr[2] * cr[2]);
         float* gq = geo + (b * 12 + j) * 4;
-        gq[0] = (float)w; gq[1] = (float)(w * y[0]); gq[2] = (float)(w * y[1]); gq[3] = (float)(w * y[2]);
+        gq[0] = (float)w; gq[1] = (float)(w * (y[0] - org[0])); gq[2] = (float)(w * (y[1] - org[1]));
+        gq[3] = (float)(w * (y[2] - org[2]));
       }
       cplx pw = {1.0, 0.0}, bb = {-0.5 * z[0], -0.5 * z[1]};
       for (int e = m; e; e >>= 1) {
@@ -1144,6 +1176,8 @@ k_p2m_img(const P2MArgs a, int R, long long ubase, T* __restrict__ mpole) {
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s;
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   const int t0 = a.sstart[box], tn = a.scount[box];
   const int nnode = a.points ? tn : 12 * tn;
   constexpr int CMAX = 6;  // coefficients per thread (ncoef(p) <= 1536)
@@ -1202,7 +1236,8 @@ k_p2m_img(const P2MArgs a, int R, long long ubase, T* __restrict__ mpole) {
         if (a.dodl) { dl[0] = a.sdl[off]; dl[1] = a.sdl[off + ds]; dl[2] = a.sdl[off + 2 * ds]; }
         const double nv[3] = {nn[0], nn[1], nn[2]};
         double wv[9];
-        img_node_weights(lane, sl, dl, nv, y, a, wv);
+        const double yo[3] = {y[0] - org[0], y[1] - org[1], y[2] - org[2]};
+        img_node_weights(lane, sl, dl, nv, yo, a, wv);
         for (int k = 0; k < 9; k++) qd[(warp * 7 + lane) * 9 + k] = w * wv[k];
       }
     }
@@ -1564,6 +1599,8 @@ k_l2t(const L2TArgs a) {
   double s = a.size / (double)(1ull << lev);
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   __syncthreads();
   int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   cplx* Y = Yall + (size_t)warp * nc;
@@ -1662,7 +1699,7 @@ k_l2t(const L2TArgs a) {
       double u[3];
       for (int i = 0; i < 3; i++) {
         u[i] = (2.0 - c1) * pot[i] + g[3][i];
-        for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+        for (int j = 0; j < 3; j++) u[i] -= c1 * (x[j] - org[j]) * g[j][i];
       }
       const size_t np = is_src ? a.nsrc : a.ntgt;
       double* U = (is_src ? a.u_src : a.u_tgt) + 3 * np * blockIdx.y;
@@ -1677,7 +1714,7 @@ k_l2t(const L2TArgs a) {
         for (int aa = 0; aa < 3; aa++)
           for (int bb = 0; bb < 3; bb++) {
             double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
-            for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+            for (int j = 0; j < 3; j++) v -= c1 * (x[j] - org[j]) * H[j][aa][bb];
             G[aa][bb] = v;
           }
         double* ee = E + 6 * (size_t)pidx;
@@ -1727,6 +1764,8 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
   const int s0 = a.sstart[box], t0 = a.tstart[box];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1858,7 +1897,7 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
     double u[3];
     for (int i = 0; i < 3; i++) {
       u[i] = (2.0 - c1) * pot[i] + g[3][i];
-      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+      for (int j = 0; j < 3; j++) u[i] -= c1 * (x[j] - org[j]) * g[j][i];
     }
     double* U = (is_src ? a.u_src : a.u_tgt) + 3 * (np * r + pidx);
     U[0] += u[0];
@@ -1869,7 +1908,7 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
       for (int aa = 0; aa < 3; aa++)
         for (int bb = 0; bb < 3; bb++) {
           double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
-          for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+          for (int j = 0; j < 3; j++) v -= c1 * (x[j] - org[j]) * H[j][aa][bb];
           G[aa][bb] = v;
         }
       double* E = (is_src ? a.e_src : a.e_tgt) + 6 * (np * r + pidx);
@@ -1974,6 +2013,8 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
   const int lev = a.level[box];
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   const double c1 = a.c1;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   for (int q = threadIdx.x; q < P * R; q += blockDim.x) {
     const int e = q % P, r = q / P;
     const bool is_src = e < sn;
@@ -1999,7 +2040,7 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
     double u[3];
     for (int i = 0; i < 3; i++) {
       u[i] = (2.0 - c1) * pot[i] + g[3][i];
-      for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+      for (int j = 0; j < 3; j++) u[i] -= c1 * (x[j] - org[j]) * g[j][i];
     }
     double* U = (is_src ? a.u_src : a.u_tgt) + 3 * (np * r + pidx);
     U[0] += u[0];
@@ -2011,7 +2052,7 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
       for (int aa = 0; aa < 3; aa++)
         for (int bb = 0; bb < 3; bb++) {
           double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
-          for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+          for (int j = 0; j < 3; j++) v -= c1 * (x[j] - org[j]) * H[j][aa][bb];
           Gm[aa][bb] = v;
         }
       double* E = (is_src ? a.e_src : a.e_tgt) + 6 * (np * r + pidx);
@@ -2027,17 +2068,18 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
 
 // Image displacement and strain at the original target from the value,
 // gradient and Hessian of the 7 columns at the reflected target x (columns:
-// 0..3 anti-image passes, 4 Phi_a, 5 Phi_c, 6 W); ADDED to U (3) and, if
-// E is set, E (6).
-__device__ __forceinline__ void img_recombine(const double x[3], const double pot[7], const double g[7][3],
-                                              const double H[7][3][3], double c1, double al, double imu, double sc,
+// 0..3 anti-image passes, 4 Phi_a, 5 Phi_c, 6 W; org the origin of
+// lame_origin); ADDED to U (3) and, if E is set, E (6).
+__device__ __forceinline__ void img_recombine(const double x[3], const double org[3], const double pot[7],
+                                              const double g[7][3], const double H[7][3][3], double c1, double al,
+                                              double imu, double sc,
                                               double* U, double* E) {
   const double x3 = -x[2];
   const double Pv[3] = {g[4][0], g[4][1], -g[4][2] - (2.0 - al) * pot[5]};
   double u[3], Gm[3][3];
   for (int i = 0; i < 3; i++) {
     u[i] = (2.0 - c1) * pot[i] + g[3][i];
-    for (int j = 0; j < 3; j++) u[i] -= c1 * x[j] * g[j][i];
+    for (int j = 0; j < 3; j++) u[i] -= c1 * (x[j] - org[j]) * g[j][i];
     u[i] += sc * imu * g[6][i] + x3 * imu * Pv[i];
   }
   U[0] += u[0];
@@ -2047,7 +2089,7 @@ __device__ __forceinline__ void img_recombine(const double x[3], const double po
   for (int aa = 0; aa < 3; aa++)
     for (int bb = 0; bb < 3; bb++) {
       double v = (2.0 - c1) * g[aa][bb] - c1 * g[bb][aa] + H[3][aa][bb];
-      for (int j = 0; j < 3; j++) v -= c1 * x[j] * H[j][aa][bb];
+      for (int j = 0; j < 3; j++) v -= c1 * (x[j] - org[j]) * H[j][aa][bb];
       v += sc * imu * H[6][aa][bb];
       const double dP = aa < 2 ? H[4][aa][bb] : -H[4][2][bb] - (2.0 - al) * g[5][bb];
       v += imu * ((bb == 2 ? -Pv[aa] : 0.0) + x3 * dP);
@@ -2085,6 +2127,8 @@ k_l2t_img(const L2TArgs a, int R, long long ubase) {
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   double c[3];
   for (int d = 0; d < 3; d++) c[d] = a.c0[d] - a.size / 2 + (a.ijk[3 * box + d] - 1) * s + s / 2;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
   cplx* Y = Yall + (size_t)warp * nc;
@@ -2172,7 +2216,7 @@ k_l2t_img(const L2TArgs a, int R, long long ubase) {
         H[q][0][2] = H[q][2][0] = S[q][5] * is2;
         H[q][1][2] = H[q][2][1] = S[q][6] * is2;
       }
-      img_recombine(x, pot, g, H, a.c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
+      img_recombine(x, org, pot, g, H, a.c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
                     a.dostrain_tgt ? a.e_tgt + 6 * (a.ntgt * r + pidx) : nullptr);
     }
   }
@@ -2194,6 +2238,8 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
   const int lev = a.level[box];
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   const double c1 = a.c1, al = a.alpha, imu = 1.0 / a.mu, sc = (1.0 - al) / al;
+  double org[3];
+  lame_origin(a.ijk, a.level, box, a.c0, a.size, a.flev, org);
   for (int q = threadIdx.x; q < P * R; q += blockDim.x) {
     const int e = q % P, r = q / P;
     const int pidx = a.tstart[box] + e;
@@ -2215,7 +2261,7 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
       H[cidx7][0][2] = H[cidx7][2][0] = hxz * is2;
       H[cidx7][1][2] = H[cidx7][2][1] = hyz * is2;
     }
-    img_recombine(x, pot, g, H, c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
+    img_recombine(x, org, pot, g, H, c1, al, imu, sc, a.u_tgt + 3 * (a.ntgt * r + pidx),
                   a.dostrain_tgt ? a.e_tgt + 6 * (a.ntgt * r + pidx) : nullptr);
   }
 }

@@ -52,6 +52,9 @@ struct P2MArgs {
   // 1, nrm = the dipole orientations (src/elfmm3dpart.f:319-420)
   int points = 0;
   const double* pts = nullptr;
+  // level of the forest's problem columns (-1: one problem); sets the origin
+  // of the linear pass (lame_origin)
+  int flev = -1;
 };
 
 struct L2TArgs {
@@ -69,6 +72,7 @@ struct L2TArgs {
   long long nsrc = 0, ntgt = 0;
   double alpha = 0, mu = 0;  // half-space image recombination
   const double* wnorm = nullptr;  // two-stage L2T in FP32: functionals x wnorm[row]
+  int flev = -1;  // as P2MArgs::flev
 };
 
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);

@@ -968,6 +968,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
     for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
     pa.size = tr_.size;
+    pa.flev = tr_.flev;
     pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
     pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
     pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
@@ -989,6 +990,7 @@ int Plan::evaluate(double rlam, double rmu, const double* d_ssl, const double* d
     la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
     for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
     la.size = tr_.size;
+    la.flev = tr_.flev;
     la.local = local_.get();
     la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
     la.p = p_; la.do_src = do_src; la.do_tgt = do_tgt;
@@ -1522,6 +1524,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
     for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
     pa.size = tr_.size;
+    pa.flev = tr_.flev;
     pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
     pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
     pa.c1 = c1; pa.c2 = c2; pa.inv2mu = 0.5 / rmu;
@@ -1559,6 +1562,7 @@ int Plan::batch_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
     for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
     la.size = tr_.size;
+    la.flev = tr_.flev;
     la.local = local_.get();
     la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
     la.p = p_; la.do_src = do_src; la.do_tgt = do_tgt;
@@ -2305,6 +2309,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     pa.sstart = tr_.sstart.get(); pa.scount = tr_.scount.get();
     for (int c = 0; c < 3; c++) pa.c0[c] = tr_.c0[c];
     pa.size = tr_.size;
+    pa.flev = tr_.flev;
     pa.tri = tri_s_.get(); pa.nrm = nrm_s_.get(); pa.ssl = ssl_s_.get(); pa.sdl = sdl_s_.get();
     pa.dosl = dosl; pa.dodl = dodl; pa.p = p_;
     // anti-image: Kelvin kernel with c1 = 2 - alpha, double-layer charge constant (2 lam + 3 mu)/(lam + 2 mu)
@@ -2364,6 +2369,7 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
     la.tstart = tr_.tstart.get(); la.tcount = tr_.tcount.get();
     for (int c = 0; c < 3; c++) la.c0[c] = tr_.c0[c];
     la.size = tr_.size;
+    la.flev = tr_.flev;
     la.local = mixed ? nullptr : img_lc_.get();
     la.src_pts = src_s_.get(); la.tgt_pts = tgt_s_.get();
     la.p = p_; la.do_src = 0; la.do_tgt = 1;
