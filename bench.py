@@ -1538,7 +1538,7 @@ def run_uneven(args, rank, world, local_rank):
         "config": {"workload": args.workload, "problems": len(probs), "triangles_total": int(sizes.sum()),
                    "triangles_min_median_max": [int(sizes.min()), int(np.median(sizes)), int(sizes.max())],
                    "evals_per_step": evals, "iprec": w["iprec"], "engine": engine,
-                   "leaf_capacity": {"free": args.free_leaf or "iprec table", "image": args.image_leaf or "iprec table"},
+                   "leaf_capacity": {"free": args.free_leaf or "iprec table", "image": args.image_leaf or "half the iprec table"},
                    "workers": workers if engine == "plans" else None,
                    "step": forest_step if engine == "forest" else plans_step,
                    "l2": "inputs (geometry > 300 MB) larger than L2",
@@ -1583,7 +1583,7 @@ def main():
     ap.add_argument("--free-leaf", type=int, default=0,
                     help="uneven forest: leaf capacity of the free-space plan (0: the iprec table)")
     ap.add_argument("--image-leaf", type=int, default=0,
-                    help="uneven forest: leaf capacity of the image plan (0: the iprec table)")
+                    help="uneven forest: leaf capacity of the image plan (0: half the iprec table)")
     ap.add_argument("--uneven-workers", type=int, default=0,
                     help="uneven batch: host worker threads (default: the host threads, 4 to 16)")
     ap.add_argument("--no-graph", action="store_true",

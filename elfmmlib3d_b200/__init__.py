@@ -57,6 +57,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_rot_tc_bench",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
            "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
+           "efmm_near_variant", "efmm_near_bulk_selfcheck",
            "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host",
            "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_", "efmm_plan_set_forest",
            "efmm_forest_create", "efmm_forest_destroy", "efmm_forest_set_geometry", "efmm_forest_evaluate",
@@ -894,7 +895,8 @@ class Forest:
 
     def set_leaf(self, nbox_free=0, nbox_image=0):
         """Leaf capacities of the two plans for the next set_geometry (<= 0:
-        the iprec table)."""
+        the default: the iprec table for the free-space plan, half of it for
+        the image plan)."""
         self._L.efmm_forest_set_leaf(self._h, int(nbox_free), int(nbox_image))
 
     def set_geometry(self, counts, tri, nrm, cen, iprec=2, iter=False):

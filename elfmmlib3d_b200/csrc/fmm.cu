@@ -1969,7 +1969,7 @@ k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long
   }
   __syncwarp();
   T* out = G + goff[blockIdx.x] + 9 * (size_t)e;
-  const size_t lda = 9 * (size_t)P + ((9 * P) & 1);  // even: 16-byte rows for the product's vector loads
+  const size_t lda = (size_t)l2t_ld(P);
   for (int row = lane; row < D; row += 32) {
     const int cc = row >> 1, part = row & 1;
     int N = 0;
@@ -2009,7 +2009,7 @@ __global__ void k_l2t_finish(const L2TArgs a, int R, const int* __restrict__ wle
   const int box = a.leaves[wleaves[blockIdx.x]];
   const int sn = a.do_src ? a.scount[box] : 0, tn = a.do_tgt ? a.tcount[box] : 0;
   const int P = sn + tn;
-  const size_t ldc = 9 * (size_t)P + ((9 * P) & 1);
+  const size_t ldc = (size_t)l2t_ld(P);
   const int lev = a.level[box];
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   const double c1 = a.c1;
@@ -2234,7 +2234,7 @@ __global__ void k_l2t_finish_img(const L2TArgs a, int R, const int* __restrict__
                                  const long long* __restrict__ soff, const TS* __restrict__ S) {
   const int box = a.leaves[wleaves[blockIdx.x]];
   const int P = a.tcount[box];
-  const size_t ldc = 9 * (size_t)P + ((9 * P) & 1);
+  const size_t ldc = (size_t)l2t_ld(P);
   const int lev = a.level[box];
   const double s = a.size / (double)(1ull << lev), is = 1.0 / s, is2 = is * is;
   const double c1 = a.c1, al = a.alpha, imu = 1.0 / a.mu, sc = (1.0 - al) / al;

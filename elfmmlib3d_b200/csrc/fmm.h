@@ -75,6 +75,11 @@ struct L2TArgs {
   int flev = -1;  // as P2MArgs::flev
 };
 
+// Leading dimension of the L2T functionals and sums of a leaf of P points:
+// 9 P rounded up to a multiple of 4, so that every row starts on 16 bytes
+// (the products' 16-byte copies in FP32 and FP64).
+__host__ __device__ inline long long l2t_ld(int P) { return (9LL * P + 3) & ~3LL; }
+
 void launch_build_ops(cudaStream_t st, int nop, const OpDesc* ops, double* mats, int maxp);
 void launch_p2m(cudaStream_t st, int nleaf, const P2MArgs& a, int nrhs = 1);
 // P2M of R right-hand sides as a product (columns 4R per box); writes mpole

@@ -47,6 +47,27 @@ void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, c
                     const long long* soff, const int* ntri, float* S, int ntask, const GemmTask* tasks,
                     const float* A, const long long* coff, double* C, int nsrc, int ntgt, const long long* base,
                     const double* store);
+// The mixed replay from the pre-split store (near_bulk.cu): per leaf the
+// FP64 store as tiles of 128 rows x 32 k, TF32 head then tail (8192 floats a
+// tile, row tile mt and K tile kt at tbase[i] + (mt nkt + kt) 8192, nkt =
+// ceil(NJ ntri / 32)), written once; per call the densities as tiles of 64
+// columns x 32 k (4096 floats, column tile ct at sbase[i] + (ct nkt + kt)
+// 4096; positions past R or K must hold zeros), the bulk-copy product
+// (tasks per leaf, row tile and column tile; C at coff, ldc = KB x points,
+// FP64 sums), the results ADDED to the outputs, the self pairs in FP64.
+struct NearTcTask {
+  long long a_off, b_off, c_off;  // floats, floats, doubles
+  int M, N, nkt, row0, col0, ldc;
+};
+int near_split_variant();  // 1: the pre-split store (default), 0: the FP32 copy
+void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long* base, const long long* tbase,
+                             const int* ntri, int K, int KB, const double* store, float* out);
+void launch_near_tc_bulk(cudaStream_t st, int ntask, const NearTcTask* tasks, const float* A, const float* B,
+                         double* C, int* err);
+void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
+                       const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
+                       const NearTcTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
+                       const long long* base, const double* store, int* err);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
                        int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,

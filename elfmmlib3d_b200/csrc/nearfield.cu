@@ -10,6 +10,7 @@
 // accumulators that are written once at the end.
 #include "common.cuh"
 #include "kernels.h"
+#include "tc_common.cuh"
 
 namespace efmm {
 
@@ -568,6 +569,73 @@ k_near_store_tc(const NearArgs a, const long long* __restrict__ base, const long
     dst[(q / pad) * Mp + M + q % pad] = 0.0f;
 }
 
+// FP64 store [point][near triangle][K] -> tiles of the pre-split store: per
+// leaf at tbase[i], tile (mt, kt) at (mt nkt + kt) 8192 floats holding rows
+// 128 mt.. (KB e + c) and k 32 kt.. (NJ t + j) of A, the TF32 head of each
+// element then its tail, in the canonical K-major layout (element (row, k)
+// at (k % 4) + 4 (row % 8) + 32 (k / 4) + 256 (row / 8)); zero past M and K
+// and at the self pairs (applied in FP64).  CTAs (leaf, blockIdx.y) over the
+// leaf's tiles; the stores are coalesced, the loads gather from runs of the
+// pair blocks.
+__global__ void __launch_bounds__(256)
+k_near_split_store(const NearArgs a, const long long* __restrict__ base, const long long* __restrict__ tbase,
+                   const int* __restrict__ ntri, int K, int KB, const double* __restrict__ store,
+                   float* __restrict__ out) {
+  const int i = blockIdx.x, leaf = a.leaves[i];
+  const int sn = a.do_src ? a.box_src_count[leaf] : 0;
+  const int nep = sn + (a.do_tgt ? a.box_tgt_count[leaf] : 0);
+  const long long nt = ntri[i], NJ = K / KB, M = (long long)KB * nep, KK = NJ * nt;
+  const long long nmt = (M + 127) / 128, nkt = (KK + 31) / 32;
+  const int self = near_self_pos(a, i, leaf);
+  const double* src = store + base[i];
+  float* dst = out + tbase[i];
+  for (long long tile = blockIdx.y; tile < nmt * nkt; tile += gridDim.y) {
+    const long long mt = tile / nkt, kt = tile % nkt;
+    float* o = dst + tile * 8192;
+    for (int q = threadIdx.x; q < 4096; q += blockDim.x) {
+      const int k = (q & 3) | (((q >> 5) & 7) << 2), m = ((q >> 2) & 7) | ((q >> 8) << 3);
+      const long long row = 128 * mt + m, kk = 32 * kt + k;
+      float v = 0.0f;
+      if (row < M && kk < KK) {
+        const long long e = row / KB, c = row % KB, t = kk / NJ, j = kk % NJ;
+        if (!(e < sn && self >= 0 && t == self + e)) v = (float)src[(e * nt + t) * K + j * KB + c];
+      }
+      const float h = tf32_head(v);
+      o[q] = h;
+      o[4096 + q] = v - h;
+    }
+  }
+}
+
+// Near densities of each leaf as pre-split tiles of 64 columns (right-hand
+// sides) x 32 k (k = NJ t + j), TF32 head then tail, canonical layout: per
+// leaf at sbase[i], tile (ct, kt) at (ct nkt + kt) 4096 floats.  Only the
+// positions with r < R and k < K are written (the rest keep their zeros).
+__global__ void __launch_bounds__(256)
+k_near_sigma_split(const NearArgs a, int R, int NJ, const double* __restrict__ g0, const double* __restrict__ g1,
+                   const long long* __restrict__ sbase, const int* __restrict__ ntri, float* __restrict__ S) {
+  const int i = blockIdx.x;
+  const long long nkt = ((long long)NJ * ntri[i] + 31) / 32;
+  float* o = S + sbase[i];
+  int pos = 0;
+  for (int b = a.nb_start[i]; b < a.nb_start[i + 1]; b++) {
+    const int sb = a.nb_items[b];
+    const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
+    for (int q = threadIdx.x; q < trn * NJ * R; q += blockDim.x) {
+      const int r = q / (trn * NJ), k = q % (trn * NJ), t = k / NJ, j = k % NJ;
+      const double* sg = j >= 3 ? g1 : g0;
+      const float v = (float)sg[((size_t)(tr0 + t) * 3 + (j % 3)) * R + r];
+      const int kk = pos * NJ + k, kl = kk & 31, n = r & 63;
+      float* tile = o + ((long long)(r >> 6) * nkt + (kk >> 5)) * 4096;
+      const int idx = (kl & 3) + 4 * (n & 7) + 32 * (kl >> 2) + 256 * (n >> 3);
+      const float h = tf32_head(v);
+      tile[idx] = h;
+      tile[2048 + idx] = v - h;
+    }
+    pos += trn;
+  }
+}
+
 // The self pairs of the mixed replay in FP64: per source point of the leaf
 // (thread) and right-hand side (blockIdx.y), the FP64 stored block times the
 // FP64 densities of the point's own triangle, ADDED to the outputs.
@@ -648,6 +716,31 @@ void launch_near_store_tc(cudaStream_t st, const NearArgs& a, const long long* b
   if (a.nleaf <= 0) return;
   k_near_store_tc<<<dim3(a.nleaf, 64), 256, 0, st>>>(a, base, fbase, ntri, K, KB, store, out);
   count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long* base, const long long* tbase,
+                             const int* ntri, int K, int KB, const double* store, float* out) {
+  if (a.nleaf <= 0) return;
+  k_near_split_store<<<dim3(a.nleaf, 32), 256, 0, st>>>(a, base, tbase, ntri, K, KB, store, out);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
+void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
+                       const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
+                       const NearTcTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
+                       const long long* base, const double* store, int* err) {
+  if (a.nleaf <= 0 || R <= 0) return;
+  k_near_sigma_split<<<a.nleaf, 256, 0, st>>>(a, R, NJ, g0, g1, sbase, ntri, S);
+  count_launch();
+  launch_near_tc_bulk(st, ntask, tasks, A, S, C, err);
+  k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
+  count_launch();
+  if (a.do_src) {
+    k_near_self64<<<dim3(a.nleaf, R), 128, 0, st>>>(a, R, NJ * KB, KB, g0, g1, base, ntri, store, nsrc);
+    count_launch();
+  }
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 

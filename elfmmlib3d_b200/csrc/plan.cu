@@ -770,6 +770,7 @@ void Plan::switch_precision(bool mixed) {
   graph_reset();
   if (!mixed) {
     store_f_.release();
+    store_s_.release();
     store_tc_gen_ = -1;
     mpole_f_.release();
     local_f_.release();
@@ -857,10 +858,45 @@ int Plan::store_alloc(int flags, double rlam, double rmu) {
 // the caller then replays the FP64 store).
 bool Plan::near_tc_ready(const NearArgs& na) {
   if (!tc_enabled() || !store_valid_ || store_K_ <= 0) return false;
-  if (store_tc_gen_ == store_gen_) return true;
+  const bool split_on = near_split_variant() != 0;
+  if (store_tc_gen_ == store_gen_ && (near_req_ == (int)split_on || capturing_)) return true;
   if (capturing_) return false;
+  near_req_ = split_on ? 1 : 0;
   const int KB0 = 3 + 6 * ((store_flags_ >> 4) & 1), NJ0 = store_K_ / KB0;
   const int dsrc = (store_flags_ >> 2) & 1, dtgt = (store_flags_ >> 3) & 1;
+  NearArgs sa = na;
+  sa.do_src = dsrc;
+  sa.do_tgt = dtgt;
+  ntc_key_ = -1;
+  // the pre-split store where it fits (else, or with efmm_near_variant(0),
+  // the FP32 copy)
+  if (split_on) {
+    const size_t nl = near_ntri_h_.size();
+    tbase_h_.resize(nl);
+    nkt_h_.resize(nl);
+    long long tot = 0;
+    for (size_t i = 0; i < nl; i++) {
+      const long long M = (long long)KB0 * ((dsrc ? near_sc_h_[i] : 0) + (dtgt ? near_tc_h_[i] : 0));
+      const long long KK = (long long)NJ0 * near_ntri_h_[i];
+      tbase_h_[i] = tot;
+      nkt_h_[i] = (int)((KK + 31) / 32);
+      tot += ((M + 127) / 128) * nkt_h_[i] * 8192;
+    }
+    size_t freeb = 0, totb = 0;
+    EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
+    if ((double)tot * 4.0 <= 0.8 * (double)freeb + 4.0 * (double)(store_s_.cap + store_f_.cap)) {
+      store_f_.release();
+      h2d(tbase_, tbase_h_, st_);
+      store_s_.resize((size_t)tot);
+      launch_near_split_store(st_, sa, near_base_.get(), tbase_.get(), near_ntri_.get(), store_K_, KB0,
+                              store_.get(), store_s_.get());
+      near_split_ = true;
+      store_tc_gen_ = store_gen_;
+      return true;
+    }
+  }
+  near_split_ = false;
+  store_s_.release();
   fbase_h_.resize(near_ntri_h_.size());
   long long tot = 0;
   for (size_t i = 0; i < near_ntri_h_.size(); i++) {
@@ -873,11 +909,7 @@ bool Plan::near_tc_ready(const NearArgs& na) {
   if ((double)tot * 4.0 > 0.8 * (double)freeb + 4.0 * (double)store_f_.cap) return false;
   h2d(fbase_, fbase_h_, st_);
   store_f_.resize((size_t)tot);
-  NearArgs sa = na;
-  sa.do_src = (store_flags_ >> 2) & 1;
-  sa.do_tgt = (store_flags_ >> 3) & 1;
-  const int KB = 3 + 6 * ((store_flags_ >> 4) & 1);
-  launch_near_store_tc(st_, sa, near_base_.get(), fbase_.get(), near_ntri_.get(), store_K_, KB, store_.get(),
+  launch_near_store_tc(st_, sa, near_base_.get(), fbase_.get(), near_ntri_.get(), store_K_, KB0, store_.get(),
                        store_f_.get());
   store_tc_gen_ = store_gen_;
   return true;
@@ -891,6 +923,45 @@ bool Plan::near_tc_ready(const NearArgs& na) {
 void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt) {
   const int KB = 3 + 6 * ((store_flags_ >> 4) & 1), NJ = store_K_ / KB;
   const int do_src = (store_flags_ >> 2) & 1, do_tgt = (store_flags_ >> 3) & 1;
+  if (near_split_) {
+    // tasks per (leaf, 64-column tile, 128-row tile); the split densities of
+    // a leaf at so (ceil(R / 64) x nkt tiles of 4096 floats, zero outside
+    // the densities: cleared whenever the layout is made)
+    const long long key = ((long long)R << 8) | store_flags_ | (1LL << 40);
+    if (ntc_key_ != key) {
+      std::vector<long long> so, co;
+      std::vector<NearTcTask> tasks;
+      long long stot = 0, ctot = 0;
+      const int nct = (R + 63) / 64;
+      for (size_t i = 0; i < near_ntri_h_.size(); i++) {
+        const long long nep = (do_src ? near_sc_h_[i] : 0) + (do_tgt ? near_tc_h_[i] : 0);
+        const long long M = KB * nep, nkt = nkt_h_[i];
+        so.push_back(stot);
+        co.push_back(ctot);
+        for (int ct = 0; ct < nct; ct++)
+          for (long long mt = 0; mt * 128 < M; mt++)
+            tasks.push_back({tbase_h_[i] + mt * nkt * 8192, stot + ct * nkt * 4096, ctot, (int)M, R, (int)nkt,
+                             (int)(128 * mt), 64 * ct, (int)M});
+        stot += nct * nkt * 4096;
+        ctot += R * M;
+      }
+      h2d(ntc_soff_, so, st_);
+      h2d(ntc_coff_, co, st_);
+      h2d(nsp_tasks_, tasks, st_);
+      ntc_scratch_.resize((size_t)stot);
+      ntc_scratch_.zero(st_);
+      EFMM_CUDA_TRY(cudaStreamSynchronize(st_));  // the host vectors go away
+      ntc_ntask_ = (int)tasks.size();
+      ntc_stot_ = stot;
+      ntc_ctot_ = ctot;
+      ntc_key_ = key;
+    }
+    ntc_cbuf_.resize((size_t)ntc_ctot_);
+    launch_near_split(st_, na, R, NJ, KB, g0, g1, ntc_soff_.get(), near_ntri_.get(), ntc_scratch_.get(), ntc_ntask_,
+                      nsp_tasks_.get(), store_s_.get(), ntc_coff_.get(), ntc_cbuf_.get(), n, nt, near_base_.get(),
+                      store_.get(), tc_err_ptr());
+    return;
+  }
   const long long key = ((long long)R << 8) | store_flags_;
   if (ntc_key_ != key) {
     std::vector<long long> so, co;
@@ -1406,7 +1477,7 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
       long long all = 0;
       for (size_t j = 0; j < l2t_h_.size(); j++) {
         const int P = (do_src ? l2t_sc_h_[j] : 0) + (do_tgt ? l2t_tc_h_[j] : 0);
-        const long long LD = 9 * P + ((9 * P) & 1);
+        const long long LD = l2t_ld(P);
         all += (long long)D * LD + (long long)C * LD;
       }
       res = resident_fits(all, esz, l2t_scratch_.cap * sizeof(double));
@@ -1428,7 +1499,7 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
           i++;
           continue;
         }
-        const int LD = 9 * P + ((9 * P) & 1);  // even leading dimension (16-byte vector loads)
+        const int LD = (int)l2t_ld(P);
         const long long need = (long long)D * LD + (long long)C * LD;
         if (w.nwl > 0 && used + need > (long long)budget) break;
         wl.push_back((int)i);
@@ -2148,7 +2219,7 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
       long long all = 0;
       for (size_t j = 0; j < l2t_h_.size(); j++) {
         const int P = l2t_tc_h_[j];
-        const long long LD = 9 * P + ((9 * P) & 1);
+        const long long LD = l2t_ld(P);
         all += (long long)D * LD + (long long)C * LD;
       }
       res = resident_fits(all, esz, l2t_scratch_.cap * sizeof(double));
@@ -2170,7 +2241,7 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
           i++;
           continue;
         }
-        const int LD = 9 * P + ((9 * P) & 1);
+        const int LD = (int)l2t_ld(P);
         const long long need = (long long)D * LD + (long long)C * LD;
         if (w.nwl > 0 && used + need > (long long)budget) break;
         wl.push_back((int)i);

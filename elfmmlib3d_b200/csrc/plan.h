@@ -335,6 +335,16 @@ class Plan {
   DevBuf<GemmTask> ntc_tasks_;
   long long store_gen_ = 0, store_tc_gen_ = -1, ntc_key_ = -1, ntc_stot_ = 0, ntc_ctot_ = 0;
   int ntc_ntask_ = 0;
+  // the pre-split store (tiles of 128 rows x 32 k, TF32 head then tail; the
+  // bulk-copy product of near_bulk.cu), used instead of store_f_ when it
+  // fits: per-leaf tile bases and K tiles, the product tasks
+  bool near_split_ = false;
+  int near_req_ = -1;  // near_split_variant() when the copy was made
+  DevBuf<float> store_s_;
+  std::vector<long long> tbase_h_;
+  std::vector<int> nkt_h_;
+  DevBuf<long long> tbase_;
+  DevBuf<NearTcTask> nsp_tasks_;
   bool near_tc_ready(const NearArgs& na);
   void near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt);
   DevBuf<double> store_;

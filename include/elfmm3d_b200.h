@@ -513,6 +513,21 @@ int efmm_gcr_dense_host(int n, int nrhs, const double *A, const double *B, doubl
  * counterpart in the reference. */
 int efmm_tc_variant(int ring);
 
+/* Form of the mixed replay of a stored near field for this process: 1
+ * (default) the store split once into TF32 head / tail tiles streamed by
+ * bulk copies into the tensor cores (8 bytes per stored element), 0 the FP32
+ * copy split in shared memory on every replay (4 bytes per element; also
+ * used when the split store does not fit).  Returns the previous form.
+ * Replaces nothing in the reference (an implementation choice). */
+int efmm_near_variant(int split);
+
+/* Self-check of the bulk-copy product of the split store on random operands
+ * (A K x M, B N x K in [-1, 1), M <= 4096, N <= 1024): relative l2 error
+ * against an FP64 host product in *rel, the kernel's error flag (a wait that
+ * ran out) in *timeout.  Returns 0, 16 (bad sizes) or 256 (device error).
+ * Test entry; no counterpart in the reference. */
+int efmm_near_bulk_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
+
 /* The autotuner (no counterpart in the reference, whose tuning is the fixed
  * iprec tables, src/elfmm3dtria.f:702-722): per key (knob, expansion order,
  * leaf capacity, expansion columns per box, precision, plan kind) the first
@@ -573,7 +588,9 @@ int efmm_forest_evaluate(efmm_forest *forest, double rlam, double rmu, const dou
                          double *u, double *e, int precision, int mode);
 
 /* Leaf capacities of the forest's free-space and image plans for the next
- * efmm_forest_set_geometry (<= 0: the iprec table). */
+ * efmm_forest_set_geometry (<= 0: the default, the plans' iprec table for
+ * the free-space plan and half of it for the image plan, whose refined
+ * image near field costs more per pair than its far field). */
 int efmm_forest_set_leaf(efmm_forest *forest, int nbox_free, int nbox_image);
 
 /* The forest's plans: which 0 the free-space (direct arrival) plan, 1 the

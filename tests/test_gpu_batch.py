@@ -294,3 +294,4 @@ def test_mixed_form_orders_floor(gpu):
     # the FP64 form keeps the iprec orders whatever the mixed floor
     assert rel(_batch(P, d, R, ssl, sdl, n, m)[0], ref[0]) < SAME
     P.close()
+

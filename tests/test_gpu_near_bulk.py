@@ -1,0 +1,93 @@
+"""The mixed replay of a stored near field from the pre-split store: TF32
+head / tail tiles of the store and of the densities streamed by bulk copies
+into the tensor cores (k_near_tc_bulk).  The product alone against an FP64
+host product (full tiles, ragged M, N, K, an empty K), and the replay of a
+plan against the replay from the FP32 copy (efmm_near_variant(0), the same
+splits and K-tile sums) and against the FP64 replay."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import rel
+from elfmmlib3d_b200 import geometry as G
+
+pytestmark = pytest.mark.gpu
+
+
+def _check(gpu, M, N, K, seed):
+    f = gpu.load().efmm_near_bulk_selfcheck
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_double),
+                  ctypes.POINTER(ctypes.c_int)]
+    r, to = ctypes.c_double(), ctypes.c_int()
+    ier = f(M, N, K, seed, ctypes.byref(r), ctypes.byref(to))
+    return ier, r.value, to.value
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 64, 32), (256, 64, 640), (300, 37, 1000), (1700, 64, 6000),
+                                   (9, 130, 45), (5, 7, 3)])
+def test_bulk_product_fp32_accuracy(gpu, M, N, K):
+    ier, r, to = _check(gpu, M, N, K, 5)
+    print(f"bulk product {M}x{N}x{K}: rel {r:.2e}")
+    assert ier == 0 and to == 0
+    # FP32 products of K terms in [-1, 1), K-tile sums in FP64: ~1e-7
+    assert r < 2e-6
+
+
+def test_bulk_product_empty_k(gpu):
+    ier, r, to = _check(gpu, 200, 64, 0, 1)
+    assert ier == 0 and to == 0 and r == 0.0
+
+
+def test_bulk_product_rejects_bad_sizes(gpu):
+    assert _check(gpu, 0, 64, 32, 1)[0] == 16
+    assert _check(gpu, 128, 2000, 32, 1)[0] == 16
+
+
+def _batch_mode(P, d, R, ssl, sdl, n, m, mode, precision=0, strain=True):
+    import torch
+    u = torch.zeros((R, n, 3), dtype=torch.float64, device="cuda")
+    e = torch.zeros((R, n, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    ut = torch.zeros((R, m, 3), dtype=torch.float64, device="cuda")
+    et = torch.zeros((R, m, 3, 3), dtype=torch.float64, device="cuda") if strain else None
+    P.evaluate_batch(1.3, 0.7, R, d(ssl) if ssl is not None else None, d(sdl) if sdl is not None else None,
+                     u, e, ut, et, mode=mode, precision=precision)
+    return [u.cpu().numpy(), e.cpu().numpy() if strain else None, ut.cpu().numpy(),
+            et.cpu().numpy() if strain else None]
+
+
+@pytest.mark.parametrize("R,strain,layers", [(64, True, 2), (70, True, 2), (5, False, 1)])
+def test_split_replay_matches_fp32_copy_and_fp64(gpu, R, strain, layers):
+    # R = 70 runs as two passes; R = 5 leaves 59 columns of the density tile
+    # empty; one layer without strain rows is the smallest stored block
+    import torch
+    var = gpu.load().efmm_near_variant
+    var.restype = ctypes.c_int
+    tri, nrm, cen = G.sphere_triangles(3)
+    tg = G.box_targets(90, 47)
+    d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device="cuda")
+    P = gpu.Plan(0)
+    P.set_geometry(d(tri), d(nrm), d(cen), d(tg), iprec=2, iter=True)
+    n, m = len(cen), len(tg)
+    rng = np.random.default_rng(300 + R)
+    ssl = rng.normal(size=(R, n, 3))
+    sdl = rng.normal(size=(R, n, 3)) if layers == 2 else None
+    _batch_mode(P, d, R, ssl, sdl, n, m, 1, strain=strain)
+    s2 = rng.normal(size=(R, n, 3))
+    d2 = rng.normal(size=(R, n, 3)) if layers == 2 else None
+    ref = _batch_mode(P, d, R, s2, d2, n, m, 2, strain=strain)
+    old = var(1)
+    try:
+        a = _batch_mode(P, d, R, s2, d2, n, m, 2, strain=strain, precision=1)
+        var(0)
+        b = _batch_mode(P, d, R, s2, d2, n, m, 2, strain=strain, precision=1)
+    finally:
+        var(old)
+    for i in ([0, 1, 2, 3] if strain else [0, 2]):
+        eab, ea = rel(a[i], b[i]), rel(a[i], ref[i])
+        print(f"output {i}: split vs FP32 copy {eab:.2e}, split vs FP64 {ea:.2e}")
+        # the two forms differ only through the far field's FP32 atomics
+        assert eab < 3e-7
+        assert 1e-13 < ea < (0.5e-6 if i in (0, 2) else 0.5e-5)
+    P.close()
