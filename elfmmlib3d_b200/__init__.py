@@ -57,7 +57,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "efmm_rot_tc_bench",
            "efmm_hs_capped", "efmm_plan_solve", "efmm_gcr_dense_host",
            "efmm_tune_pick", "efmm_tune_report", "efmm_tune_reset", "efmm_tune_dump", "efmm_tc_variant",
-           "efmm_near_variant", "efmm_near_bulk_selfcheck",
+           "efmm_split_variant", "efmm_tc_bulk_selfcheck",
            "elfmm3dparttarg_", "elfmm3dpart_", "el3dpartdirecttarg_", "efmm_part_pair_host",
            "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_", "efmm_plan_set_forest",
            "efmm_forest_create", "efmm_forest_destroy", "efmm_forest_set_geometry", "efmm_forest_evaluate",

@@ -16,6 +16,8 @@
 //        with the Lame recombination fused in, writing displacement and strain.
 #include "common.cuh"
 #include "fmm.h"
+#include "kernels.h"
+#include "tc_common.cuh"
 
 namespace efmm {
 
@@ -939,7 +941,7 @@ __host__ __device__ inline size_t unitf_smem(int p) {
 template <int NK>
 __global__ void __launch_bounds__(UNITF_THREADS, 1)
 k_p2m_unit_f(const P2MArgs a, const int* __restrict__ wleaves, const long long* __restrict__ hoff, int sbase,
-             int ns, float* __restrict__ H) {
+             int ns, float* __restrict__ H, int split) {
   constexpr int NF = NK == 7 ? 9 : 4;
   extern __shared__ __align__(16) unsigned char pf_smem2[];
   const int p = a.p, nc = ncoef(p), D = 2 * nc, NY = unit_ylen(p);
@@ -1120,6 +1122,20 @@ k_p2m_unit_f(const P2MArgs a, const int* __restrict__ wleaves, const long long* 
       auto put = [&](int q, int sidx, float vr, float vi) {
         const int sl = sidx - sbase;
         if (sl < 0 || sl >= ns) return;
+        if (split) {
+          // split tiles: kind q's (row, k = ns tl + sl) in tile (row / 128, k / 32)
+          const int k = ns * tl + sl, kl = k & 31, nmt = (D + 127) / 128, snkt = (ns * tn + 31) / 32;
+#pragma unroll
+          for (int h = 0; h < 2; h++) {
+            const int row = 2 * cc + h;
+            float* tile = Hb + ((long long)(q * nmt + (row >> 7)) * snkt + (k >> 5)) * 8192;
+            const int idx = (kl & 3) + 4 * (row & 7) + 32 * (kl >> 2) + 256 * ((row & 127) >> 3);
+            const float v = h ? vi : vr, hd = tf32_head(v);
+            tile[idx] = hd;
+            tile[4096 + idx] = v - hd;
+          }
+          return;
+        }
         float* oo = o + q * kstride + (size_t)sl * D;
         oo[0] = vr;
         oo[1] = vi;
@@ -1156,6 +1172,48 @@ k_p2m_sigma(const P2MArgs a, int R, const int* __restrict__ wleaves, const long 
       }
     }
     out[q] = (T)v;
+  }
+}
+
+// The densities of each leaf of the wave as split B tiles of 64 columns
+// (right-hand sides) x 32 k (k = ns t + j: density component sbase + j of the
+// leaf's triangle t), 4096 floats a tile (TF32 head then tail, canonical
+// layout; column tile ct, K tile kt at soff[i] + (ct nkt + kt) 4096);
+// positions past R or K written as zeros.  A tile is read k-fastest into
+// shared memory (rows of 36 floats) and written in tile order.
+__global__ void __launch_bounds__(256)
+k_p2m_sigma_split(const P2MArgs a, int R, const int* __restrict__ wleaves, const long long* __restrict__ soff,
+                  int sbase, int ns, float* __restrict__ S) {
+  __shared__ float sv[64][36];
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int t0 = a.sstart[box], tn = a.scount[box];
+  const int K = ns * tn, nkt = (K + 31) / 32, nct = (R + 63) / 64;
+  float* o = S + soff[blockIdx.x];
+  for (int tile = blockIdx.y; tile < nct * nkt; tile += gridDim.y) {
+    const int ct = tile / nkt, kt = tile % nkt;
+    __syncthreads();  // the previous tile's reads of sv are done
+    for (int q = threadIdx.x; q < 2048; q += blockDim.x) {
+      const int k = q & 31, n = q >> 5, r = 64 * ct + n, kk = 32 * kt + k;
+      float v = 0.0f;
+      if (r < R && kk < K) {
+        const int tl = kk / ns, sc = sbase + kk % ns;
+        const long long off = r * a.rstride + (long long)(t0 + tl) * a.tstride + (sc % 3) * a.dstride;
+        if (sc < 3) {
+          if (a.dosl) v = (float)a.ssl[off];
+        } else if (a.dodl) {
+          v = (float)a.sdl[off];
+        }
+      }
+      sv[n][k] = v;
+    }
+    __syncthreads();
+    float* t = o + (long long)tile * 4096;
+    for (int q = threadIdx.x; q < 2048; q += blockDim.x) {
+      const int k = (q & 3) | (((q >> 5) & 7) << 2), n = ((q >> 2) & 7) | ((q >> 8) << 3);
+      const float v = sv[n][k], h = tf32_head(v);
+      t[q] = h;
+      t[2048 + q] = v - h;
+    }
   }
 }
 
@@ -1929,10 +1987,14 @@ k_l2t_gemm(const L2TArgs a, const int* __restrict__ chunk_leaf, const int* __res
 // (k_gemm_tn); stage 3 applies the Lame recombination per (point, rhs).
 // T = float: the functionals of the normalised basis (x wnorm), multiplied
 // with the FP32 normalised local expansions on the tensor cores.
+// snkt > 0 (T = float): G written as split tiles instead (rows 9 point + v
+// in tiles of 128, coefficients in K tiles of 32, snkt of them; tile
+// (mt, kt) at goff + (mt snkt + kt) 8192 floats, TF32 head then tail in the
+// tensor cores' canonical layout; the product is k_tc_bulk).
 template <class T>
 __global__ void __launch_bounds__(256)
 k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long* __restrict__ goff,
-               T* __restrict__ G) {
+               T* __restrict__ G, int snkt) {
   extern __shared__ __align__(16) unsigned char lf_smem[];
   const int p = a.p, nc = ncoef(p), D = 2 * nc;
   const int box = a.leaves[wleaves[blockIdx.x]];
@@ -1998,7 +2060,64 @@ k_l2t_features(const L2TArgs a, const int* __restrict__ wleaves, const long long
           g = part == 0 ? -yid - sM * yim : yrd - sM * yrm;
         g *= t.sg;
       }
-      out[(size_t)row * lda + v] = (T)(a.wnorm ? g * a.wnorm[row] : g);
+      const T val = (T)(a.wnorm ? g * a.wnorm[row] : g);
+      if constexpr (sizeof(T) == 4) {
+        if (snkt > 0) {
+          const int m = 9 * e + v, kl = row & 31;
+          float* tile = G + goff[blockIdx.x] + ((long long)(m >> 7) * snkt + (row >> 5)) * 8192;
+          const int idx = (kl & 3) + 4 * (m & 7) + 32 * (kl >> 2) + 256 * ((m & 127) >> 3);
+          const float h = tf32_head(val);
+          tile[idx] = h;
+          tile[4096 + idx] = val - h;
+          continue;
+        }
+      }
+      out[(size_t)row * lda + v] = val;
+    }
+  }
+}
+
+// The local expansions of each leaf of the wave as split B tiles of 128
+// columns x 32 coefficients (8192 floats, TF32 head then tail, canonical
+// layout; column tile ct, K tile kt at boff[i] + (ct nkt + kt) 8192): the C
+// columns of the box (free space, C = 4R: local[(box C + col) D + k]; image,
+// C = 7R: the 6R columns at local[(box 6R + col) D + k], then the R columns
+// of U after all nb boxes' 6R columns).  CTAs (leaf, blockIdx.y) over the
+// leaf's tiles: a tile is read column by column (128-byte runs) into shared
+// memory (rows of 36 floats: neither phase has bank conflicts) and written
+// in tile order, both coalesced; positions past C or D are written as zeros.
+__global__ void __launch_bounds__(256)
+k_l2t_local_split(const L2TArgs a, int R, int image, long long nb, const int* __restrict__ wleaves,
+                  const long long* __restrict__ boff, const float* __restrict__ local, float* __restrict__ Bs) {
+  __shared__ float sv[128][36];
+  const int box = a.leaves[wleaves[blockIdx.x]];
+  const int D = 2 * ncoef(a.p), nkt = (D + 31) / 32, C = image ? 7 * R : 4 * R, nct = (C + 127) / 128;
+  float* o = Bs + boff[blockIdx.x];
+  for (int tile = blockIdx.y; tile < nct * nkt; tile += gridDim.y) {
+    const int ct = tile / nkt, kt = tile % nkt;
+    __syncthreads();  // the previous tile's reads of sv are done
+    for (int q = threadIdx.x; q < 4096; q += blockDim.x) {
+      const int n = q >> 5, k = q & 31, col = 128 * ct + n, kk = 32 * kt + k;
+      float v = 0.0f;
+      if (col < C && kk < D) {
+        const float* src;
+        if (!image)
+          src = local + ((long long)box * C + col) * D;
+        else if (col < 6 * R)
+          src = local + ((long long)box * 6 * R + col) * D;
+        else
+          src = local + nb * 6 * R * D + ((long long)box * R + (col - 6 * R)) * D;
+        v = src[kk];
+      }
+      sv[n][k] = v;
+    }
+    __syncthreads();
+    float* t = o + (long long)tile * 8192;
+    for (int q = threadIdx.x; q < 4096; q += blockDim.x) {
+      const int k = (q & 3) | (((q >> 5) & 7) << 2), n = ((q >> 2) & 7) | ((q >> 8) << 3);
+      const float v = sv[n][k], h = tf32_head(v);
+      t[q] = h;
+      t[4096 + q] = v - h;
     }
   }
 }
@@ -2286,7 +2405,8 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
   const int smem = (int)(sizeof(cplx) * 8 * nc);
   if (do_g) {
     EFMM_CUDA_TRY(smem_raise(k_l2t_features<T>, (int)(smem)));
-    k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf); count_launch();
+    k_l2t_features<T><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, Gbuf, 0);
+    count_launch();
   }
   gemm_product<T>(st, ntask, tasks, Gbuf, local, Sbuf);
   if (image)
@@ -2296,6 +2416,28 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
+void launch_l2t_bulk(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves, const long long* goff,
+                     const long long* soff, const long long* boff, int max_pts, float* scratch, int ntask,
+                     const BulkTask* tasks, const float* local, long long nb, bool image, bool do_g, int* err) {
+  if (nwleaf <= 0) return;
+  const int nc = ncoef(a.p), nkt = (2 * nc + 31) / 32;
+  const int smem = (int)(sizeof(cplx) * 8 * nc);
+  if (do_g) {
+    EFMM_CUDA_TRY(smem_raise(k_l2t_features<float>, (int)(smem)));
+    k_l2t_features<float><<<dim3(nwleaf, (max_pts + 7) / 8), 256, smem, st>>>(a, wleaves, goff, scratch, nkt);
+    count_launch();
+  }
+  k_l2t_local_split<<<dim3(nwleaf, 16), 256, 0, st>>>(a, R, image ? 1 : 0, nb, wleaves, boff, local, scratch);
+  count_launch();
+  launch_tc_bulk<float>(st, ntask, tasks, scratch, scratch, scratch, err, 128);
+  if (image)
+    k_l2t_finish_img<float><<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, scratch);
+  else
+    k_l2t_finish<float><<<nwleaf, 256, 0, st>>>(a, R, wleaves, soff, scratch);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
 template void launch_l2t_twostage<double>(cudaStream_t, const L2TArgs&, int, int, const int*, const long long*,
                                           const long long*, int, double*, double*, int, const GemmTask*,
                                           const double*, bool, bool);
@@ -2311,14 +2453,24 @@ template void launch_l2t_twostage<float>(cudaStream_t, const L2TArgs&, int, int,
 // shared memory.
 template <class T>
 bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
-                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h) {
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h,
+                     bool split) {
   const int nc = ncoef(a.p);
   const bool fp32 = sizeof(T) == 4;
   const size_t smem = p2m_unit_smem(a.p, fp32);
   if (smem > 227 * 1024 || (fp32 && !a.wnorm)) return false;
   if (nwleaf <= 0) return true;
-  if (!do_h) {
+  auto sigma = [&]() {
+    if constexpr (sizeof(T) == 4) {
+      if (split) {
+        k_p2m_sigma_split<<<dim3(nwleaf, 8), 256, 0, st>>>(a, R, wleaves, soff, sbase, ns, S);
+        return;
+      }
+    }
     k_p2m_sigma<T><<<dim3(nwleaf, 8), 256, 0, st>>>(a, R, wleaves, soff, sbase, ns, S);
+  };
+  if (!do_h) {
+    sigma();
     count_launch();
     EFMM_CUDA_TRY(cudaGetLastError());
     return true;
@@ -2332,10 +2484,10 @@ bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwlea
     float* Hf = reinterpret_cast<float*>(H);
     if (nk == 7) {
       EFMM_CUDA_TRY(smem_raise(k_p2m_unit_f<7>, (int)smem));
-      k_p2m_unit_f<7><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
+      k_p2m_unit_f<7><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf, split ? 1 : 0);
     } else {
       EFMM_CUDA_TRY(smem_raise(k_p2m_unit_f<4>, (int)smem));
-      k_p2m_unit_f<4><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf);
+      k_p2m_unit_f<4><<<grid, nthr, smem, st>>>(a, wleaves, hoff, sbase, ns, Hf, split ? 1 : 0);
     }
   } else {
     constexpr int NTD = unit_threads<T>();
@@ -2348,7 +2500,7 @@ bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwlea
     }
   }
   count_launch();
-  k_p2m_sigma<T><<<dim3(nwleaf, 8), 256, 0, st>>>(a, R, wleaves, soff, sbase, ns, S);
+  sigma();
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
   return true;
@@ -2360,9 +2512,9 @@ size_t p2m_unit_smem(int p, bool fp32) {
          (18 + 12 * 4) * sizeof(double);
 }
 template bool launch_p2m_unit<double>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
-                                      const long long*, const long long*, int, int, double*, double*, bool);
+                                      const long long*, const long long*, int, int, double*, double*, bool, bool);
 template bool launch_p2m_unit<float>(cudaStream_t, const P2MArgs&, int, int, int, int, const int*,
-                                     const long long*, const long long*, int, int, float*, float*, bool);
+                                     const long long*, const long long*, int, int, float*, float*, bool, bool);
 
 // The batched product of the two-stage P2M: FP32 on the tensor cores
 // (tc_gemm.cu) unless ELFMM3D_TC=0, FP64 (and FP32 when disabled) on the

@@ -127,6 +127,16 @@ template <class T>
 void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves,
                          const long long* goff, const long long* soff, int max_pts, T* Gbuf, T* Sbuf,
                          int ntask, const GemmTask* tasks, const T* local, bool image = false, bool do_g = true);
+// The two-stage L2T from split operands (mixed form, functionals resident):
+// functionals as split A tiles (per leaf at goff, written when do_g), the
+// wave's local expansions (FP32 normalised, free-space or image column
+// layout, nb boxes) as split B tiles at boff, the bulk-copy product
+// (k_tc_bulk, 128-column tiles) into S at soff (columns of l2t_ld(P)), then
+// the Lame recombination.
+struct BulkTask;
+void launch_l2t_bulk(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, const int* wleaves, const long long* goff,
+                     const long long* soff, const long long* boff, int max_pts, float* scratch, int ntask,
+                     const BulkTask* tasks, const float* local, long long nb, bool image, bool do_g, int* err);
 // Two-stage P2M of the half-space image columns (7R per box, tasks cut by
 // the caller): node features with second-derivative rows (9 x 12 x
 // triangles rows of D per leaf at foff), node weights (7R columns of 9 x 12
@@ -140,10 +150,15 @@ void launch_l2t_twostage(cudaStream_t st, const L2TArgs& a, int R, int nwleaf, c
 // Stage 2 is gemm_product with K = ns x triangles, N = R.  False (nothing
 // launched) when the order is too high for its shared memory
 // (p2m_unit_smem(p, T is float) > 227 KB).  do_h = false: H is already
-// there (resident from an earlier pass) and only S is formed.
+// there (resident from an earlier pass) and only S is formed.  split (T =
+// float): H and S as split tiles for k_tc_bulk instead: per leaf and kind q,
+// H's tile (row tile mt of ceil(D / 128), K tile kt of nkt = ceil(ns tn /
+// 32)) at hoff + ((q ceil(D / 128) + mt) nkt + kt) 8192, S's tiles of 64
+// right-hand sides at soff + (ct nkt + kt) 4096 (k_p2m_sigma_split).
 template <class T>
 bool launch_p2m_unit(cudaStream_t st, const P2MArgs& a, int R, int nk, int nwleaf, int maxtn, const int* wleaves,
-                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h = true);
+                     const long long* hoff, const long long* soff, int sbase, int ns, T* H, T* S, bool do_h = true,
+                     bool split = false);
 size_t p2m_unit_smem(int p, bool fp32);
 // Direct P2M of the image columns (one CTA per leaf and right-hand side):
 // columns kind * R + r of 6R per box (kinds 0..5) and the U column at

@@ -47,26 +47,33 @@ void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, c
                     const long long* soff, const int* ntri, float* S, int ntask, const GemmTask* tasks,
                     const float* A, const long long* coff, double* C, int nsrc, int ntgt, const long long* base,
                     const double* store);
-// The mixed replay from the pre-split store (near_bulk.cu): per leaf the
-// FP64 store as tiles of 128 rows x 32 k, TF32 head then tail (8192 floats a
-// tile, row tile mt and K tile kt at tbase[i] + (mt nkt + kt) 8192, nkt =
-// ceil(NJ ntri / 32)), written once; per call the densities as tiles of 64
-// columns x 32 k (4096 floats, column tile ct at sbase[i] + (ct nkt + kt)
-// 4096; positions past R or K must hold zeros), the bulk-copy product
-// (tasks per leaf, row tile and column tile; C at coff, ldc = KB x points,
-// FP64 sums), the results ADDED to the outputs, the self pairs in FP64.
-struct NearTcTask {
-  long long a_off, b_off, c_off;  // floats, floats, doubles
+// Products from pre-split operands (tc_bulk.cu): A as tiles of 128 rows x
+// 32 k (8192 floats: TF32 head then tail, canonical K-major layout; tile kt
+// of a task at a_off + 8192 kt), B as tiles of BN columns x 32 k (64 BN
+// floats; tile kt at b_off + 64 BN kt), zeros past the matrices;
+// C[c_off + col ldc + row] = sum_k A[k][row] B[col][k] stored for row < M,
+// col < N of the task's tile (rows row0.., columns col0..), K-tile sums in
+// TC (float or double).
+struct BulkTask {
+  long long a_off, b_off, c_off;  // floats, floats, elements of C
   int M, N, nkt, row0, col0, ldc;
 };
-int near_split_variant();  // 1: the pre-split store (default), 0: the FP32 copy
+template <class TC>
+void launch_tc_bulk(cudaStream_t st, int ntask, const BulkTask* tasks, const float* A, const float* B, TC* C,
+                    int* err, int bn);
+int split_variant();  // 1: pre-split operands where they fit (default), 0: FP32 operands
+// The mixed replay of the stored near field from its split: the FP64 store
+// as A tiles per leaf (row tile mt, K tile kt at tbase[i] + (mt nkt + kt)
+// 8192, nkt = ceil(NJ ntri / 32)), written once; per call the densities as
+// B tiles of 64 columns (column tile ct at sbase[i] + (ct nkt + kt) 4096;
+// positions past R or K must hold zeros), the product (tasks per leaf, row
+// tile and column tile; C at coff, ldc = KB x points, FP64 sums), the
+// results ADDED to the outputs, the self pairs in FP64.
 void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long* base, const long long* tbase,
                              const int* ntri, int K, int KB, const double* store, float* out);
-void launch_near_tc_bulk(cudaStream_t st, int ntask, const NearTcTask* tasks, const float* A, const float* B,
-                         double* C, int* err);
 void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
                        const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
-                       const NearTcTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
+                       const BulkTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
                        const long long* base, const double* store, int* err);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,

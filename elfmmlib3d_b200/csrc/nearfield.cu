@@ -608,31 +608,58 @@ k_near_split_store(const NearArgs a, const long long* __restrict__ base, const l
 }
 
 // Near densities of each leaf as pre-split tiles of 64 columns (right-hand
-// sides) x 32 k (k = NJ t + j), TF32 head then tail, canonical layout: per
-// leaf at sbase[i], tile (ct, kt) at (ct nkt + kt) 4096 floats.  Only the
-// positions with r < R and k < K are written (the rest keep their zeros).
+// sides) x 32 k (k = NJ t + j over the leaf's near triangles t, components
+// j), TF32 head then tail, canonical layout: per leaf at sbase[i], tile (ct,
+// kt) at (ct nkt + kt) 4096 floats; positions past R or K written as zeros.
+// CTAs (leaf, blockIdx.y) over the leaf's tiles: the triangle of each k is
+// found by walking the leaf's near boxes, the densities are read 64
+// right-hand sides at a time (coalesced) into shared memory (rows of 72
+// floats: neither phase has bank conflicts) and written in tile order.
 __global__ void __launch_bounds__(256)
 k_near_sigma_split(const NearArgs a, int R, int NJ, const double* __restrict__ g0, const double* __restrict__ g1,
                    const long long* __restrict__ sbase, const int* __restrict__ ntri, float* __restrict__ S) {
+  __shared__ float sv[32][72];
+  __shared__ int tri_k[32];
   const int i = blockIdx.x;
-  const long long nkt = ((long long)NJ * ntri[i] + 31) / 32;
+  const int K = NJ * ntri[i], nkt = (K + 31) / 32, nct = (R + 63) / 64;
   float* o = S + sbase[i];
-  int pos = 0;
-  for (int b = a.nb_start[i]; b < a.nb_start[i + 1]; b++) {
-    const int sb = a.nb_items[b];
-    const int tr0 = a.box_src_start[sb], trn = a.box_src_count[sb];
-    for (int q = threadIdx.x; q < trn * NJ * R; q += blockDim.x) {
-      const int r = q / (trn * NJ), k = q % (trn * NJ), t = k / NJ, j = k % NJ;
-      const double* sg = j >= 3 ? g1 : g0;
-      const float v = (float)sg[((size_t)(tr0 + t) * 3 + (j % 3)) * R + r];
-      const int kk = pos * NJ + k, kl = kk & 31, n = r & 63;
-      float* tile = o + ((long long)(r >> 6) * nkt + (kk >> 5)) * 4096;
-      const int idx = (kl & 3) + 4 * (n & 7) + 32 * (kl >> 2) + 256 * (n >> 3);
-      const float h = tf32_head(v);
-      tile[idx] = h;
-      tile[2048 + idx] = v - h;
+  for (int tile = blockIdx.y; tile < nct * nkt; tile += gridDim.y) {
+    const int ct = tile / nkt, kt = tile % nkt;
+    __syncthreads();  // the previous tile's reads of sv and tri_k are done
+    if (threadIdx.x < 32) {
+      const int kk = 32 * kt + threadIdx.x;
+      int tri = -1;
+      if (kk < K) {
+        int u = kk / NJ;
+        for (int b = a.nb_start[i]; b < a.nb_start[i + 1]; b++) {
+          const int sb = a.nb_items[b], cnt = a.box_src_count[sb];
+          if (u < cnt) {
+            tri = a.box_src_start[sb] + u;
+            break;
+          }
+          u -= cnt;
+        }
+      }
+      tri_k[threadIdx.x] = tri;
     }
-    pos += trn;
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2048; q += blockDim.x) {
+      const int n = q & 63, k = q >> 6, r = 64 * ct + n, tri = tri_k[k];
+      float v = 0.0f;
+      if (tri >= 0 && r < R) {
+        const int j = (32 * kt + k) % NJ;
+        v = (float)(j >= 3 ? g1 : g0)[((size_t)tri * 3 + (j % 3)) * R + r];
+      }
+      sv[k][n] = v;
+    }
+    __syncthreads();
+    float* t = o + (long long)tile * 4096;
+    for (int q = threadIdx.x; q < 2048; q += blockDim.x) {
+      const int k = (q & 3) | (((q >> 5) & 7) << 2), n = ((q >> 2) & 7) | ((q >> 8) << 3);
+      const float v = sv[k][n], h = tf32_head(v);
+      t[q] = h;
+      t[2048 + q] = v - h;
+    }
   }
 }
 
@@ -729,12 +756,12 @@ void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long
 
 void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
                        const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
-                       const NearTcTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
+                       const BulkTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
                        const long long* base, const double* store, int* err) {
   if (a.nleaf <= 0 || R <= 0) return;
-  k_near_sigma_split<<<a.nleaf, 256, 0, st>>>(a, R, NJ, g0, g1, sbase, ntri, S);
+  k_near_sigma_split<<<dim3(a.nleaf, 8), 256, 0, st>>>(a, R, NJ, g0, g1, sbase, ntri, S);
   count_launch();
-  launch_near_tc_bulk(st, ntask, tasks, A, S, C, err);
+  launch_tc_bulk<double>(st, ntask, tasks, A, S, C, err, 64);
   k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
   count_launch();
   if (a.do_src) {

@@ -858,7 +858,7 @@ int Plan::store_alloc(int flags, double rlam, double rmu) {
 // the caller then replays the FP64 store).
 bool Plan::near_tc_ready(const NearArgs& na) {
   if (!tc_enabled() || !store_valid_ || store_K_ <= 0) return false;
-  const bool split_on = near_split_variant() != 0;
+  const bool split_on = split_variant() != 0;
   if (store_tc_gen_ == store_gen_ && (near_req_ == (int)split_on || capturing_)) return true;
   if (capturing_) return false;
   near_req_ = split_on ? 1 : 0;
@@ -868,7 +868,7 @@ bool Plan::near_tc_ready(const NearArgs& na) {
   sa.do_src = dsrc;
   sa.do_tgt = dtgt;
   ntc_key_ = -1;
-  // the pre-split store where it fits (else, or with efmm_near_variant(0),
+  // the pre-split store where it fits (else, or with efmm_split_variant(0),
   // the FP32 copy)
   if (split_on) {
     const size_t nl = near_ntri_h_.size();
@@ -930,7 +930,7 @@ void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1
     const long long key = ((long long)R << 8) | store_flags_ | (1LL << 40);
     if (ntc_key_ != key) {
       std::vector<long long> so, co;
-      std::vector<NearTcTask> tasks;
+      std::vector<BulkTask> tasks;
       long long stot = 0, ctot = 0;
       const int nct = (R + 63) / 64;
       for (size_t i = 0; i < near_ntri_h_.size(); i++) {
@@ -1366,6 +1366,97 @@ template void Plan::p2m_twostage<float>(const P2MArgs&, int, float*);
 // (64-column tensor-core tiles when R <= 64).  Column layouts: the
 // free-space plan writes columns 4 r + kind of 4R per box; the image plan
 // columns kind R + r of 6R (kinds 0..5) and the U column at nb 6R D + box R D.
+//
+// The resident FP32 form from split operands: one wave of all leaves, per
+// leaf the unit multipoles as split tiles (nk kinds x ceil(D / 128) row
+// tiles x nkt = ceil(ns tn / 32) K tiles of 8192 floats, off1) and the
+// densities as split tiles (ceil(R / 64) x nkt tiles of 4096 floats, off2);
+// tasks per (leaf, kind, column tile, row tile) into the same expansion
+// columns as the FP32 products.  The scratch is cleared when the layout is
+// made (the tiles' padding stays zero).  False when it does not fit.
+bool Plan::p2m_split_layout(WaveSet& W, int D, int R, int nk, int ns, bool image, long long key) {
+  const long long nb = tr_.nboxes, nmt = (D + 127) / 128, nct = (R + 63) / 64;
+  long long all = 0;
+  for (size_t j = 0; j < p2m_h_.size(); j++) {
+    const long long nkt = ((long long)ns * p2m_sc_h_[j] + 31) / 32;
+    all += nk * nmt * nkt * 8192 + nct * nkt * 4096;
+  }
+  if (!resident_fits(all, sizeof(float), p2m_scratch_.cap * sizeof(double))) return false;
+  W.clear();
+  W.resident = true;
+  W.split = true;
+  std::vector<int> wl;
+  std::vector<long long> ho, so;
+  std::vector<BulkTask> tasks;
+  WaveSet::Wave w{0, 0, 0, 0, 0, 0, 0};
+  long long used = 0;
+  double flops = 0;
+  for (size_t i = 0; i < p2m_h_.size(); i++) {
+    const int tn = p2m_sc_h_[i];
+    const long long K = (long long)ns * tn, nkt = (K + 31) / 32;
+    wl.push_back((int)i);
+    ho.push_back(used);
+    so.push_back(used + nk * nmt * nkt * 8192);
+    const long long box = p2m_h_[i];
+    for (int q = 0; q < nk; q++) {
+      long long coff;
+      int ldc;
+      if (!image) {
+        coff = box * 4 * R * D + (long long)q * D;
+        ldc = 4 * D;
+      } else if (q < 6) {
+        coff = box * 6 * R * D + (long long)q * R * D;
+        ldc = D;
+      } else {
+        coff = nb * 6 * R * D + box * R * D;
+        ldc = D;
+      }
+      for (long long ct = 0; ct < nct; ct++)
+        for (long long mt = 0; mt < nmt; mt++) {
+          tasks.push_back({ho.back() + (q * nmt + mt) * nkt * 8192, so.back() + ct * nkt * 4096, coff, D, R, (int)nkt,
+                           (int)(128 * mt), (int)(64 * ct), ldc});
+          flops += 2.0 * std::min<long long>(128, D - 128 * mt) * std::min<long long>(64, R - 64 * ct) * (double)K;
+        }
+    }
+    used += nk * nmt * nkt * 8192 + nct * nkt * 4096;
+    w.maxn = std::max(w.maxn, tn);
+    w.nwl++;
+  }
+  w.ntask = (int)tasks.size();
+  w.used = used;
+  if (w.nwl > 0) W.w.push_back(w);
+  W.upload(wl, ho, so, {}, {}, st_);
+  h2d(W.btasks, tasks, st_);
+  W.bulk_flops = flops;
+  p2m_scratch_.resize((std::max<long long>(used, 1) * sizeof(float) + sizeof(double) - 1) / sizeof(double));
+  p2m_scratch_.zero(st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));  // the host vectors go away
+  W.key = key;
+  return true;
+}
+
+// k_tc_bulk (FP32 sums) timed with the tensor-core products (product_ms,
+// product_flops: the useful flops of the tasks, flops)
+void Plan::bulk_timed(int ntask, double flops, const BulkTask* dtasks, const float* A, const float* B, float* C,
+                      int bn) {
+  if (capturing_) {
+    launch_tc_bulk<float>(st_, ntask, dtasks, A, B, C, tc_err_ptr(), bn);
+    return;
+  }
+  if (npev_ + 2 > (int)pev_.size()) {
+    cudaEvent_t a, b;
+    EFMM_CUDA_TRY(cudaEventCreate(&a));
+    EFMM_CUDA_TRY(cudaEventCreate(&b));
+    pev_.push_back(a);
+    pev_.push_back(b);
+  }
+  EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_], st_));
+  launch_tc_bulk<float>(st_, ntask, dtasks, A, B, C, tc_err_ptr(), bn);
+  EFMM_CUDA_TRY(cudaEventRecord(pev_[npev_ + 1], st_));
+  npev_ += 2;
+  product_flops_ += flops;
+}
+
 template <class T>
 bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
   const int D = 2 * ncoef(p_), nk = image ? 7 : 4;
@@ -1376,6 +1467,26 @@ bool Plan::p2m_factored(const P2MArgs& pa, int R, T* mpole, bool image) {
   WaveSet& W = p2m_waves_;
   const long long key = ((long long)p_ << 40) | ((long long)R << 12) | ((long long)ns << 8) | (sbase << 5) |
                         (sizeof(T) << 2) | (image ? 3 : 1) | ((long long)resident_ << 62);
+  // FP32 and resident: the unit multipoles and densities as split tiles and
+  // the bulk-copy product, where they fit
+  if constexpr (sizeof(T) == 4) {
+    if (resident_ && tc_enabled() && split_variant()) {
+      const long long skey = key | (1LL << 61);
+      if (W.key != skey && !p2m_split_layout(W, D, R, nk, ns, image, skey)) goto dense;
+      const bool do_h = !W.feat_valid;
+      for (const auto& w : W.w) {
+        if (!launch_p2m_unit<T>(st_, pa, R, nk, w.nwl, w.maxn, W.leaves.get(), W.off1.get(), W.off2.get(), sbase,
+                                ns, reinterpret_cast<T*>(p2m_scratch_.get()), reinterpret_cast<T*>(p2m_scratch_.get()),
+                                do_h, true))
+          return false;
+        float* sc = reinterpret_cast<float*>(p2m_scratch_.get());
+        bulk_timed(w.ntask, W.bulk_flops, W.btasks.get(), sc, sc, reinterpret_cast<float*>(mpole), 64);
+      }
+      W.feat_valid = true;
+      return true;
+    }
+  }
+dense:
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -1460,6 +1571,64 @@ template bool Plan::p2m_factored<float>(const P2MArgs&, int, float*, bool);
 // scratch budget (at most 8 GB or a quarter of the free memory).
 // mixed: FP32 normalised locals (local_f_) against normalised functionals,
 // the product on the tensor cores
+// One resident wave of all L2T leaves from split operands: per leaf (P
+// points) the functionals as split tiles (nmt = ceil(9P / 128) row tiles x
+// nkt = ceil(D / 32) K tiles of 8192 floats, off1), the products S (C
+// columns of l2t_ld(P), off2) and the local expansions as split tiles (nct
+// = ceil(C / 128) column tiles x nkt, off3); tasks per (leaf, column tile,
+// row tile).  The scratch is cleared when the layout is made (the tiles'
+// padding stays zero).
+bool Plan::l2t_split_layout(WaveSet& W, int D, int C, const std::vector<int>& Pl, long long key) {
+  const long long nkt = (D + 31) / 32, nct = (C + 127) / 128;
+  long long all = 0;
+  for (int P : Pl)
+    if (P > 0) all += ((9LL * P + 127) / 128) * nkt * 8192 + nct * nkt * 8192 + (long long)C * l2t_ld(P);
+  if (!resident_fits(all, sizeof(float), l2t_scratch_.cap * sizeof(double))) return false;
+  W.clear();
+  W.resident = true;
+  W.split = true;
+  std::vector<int> wl;
+  std::vector<long long> go, so, bo;
+  std::vector<BulkTask> tasks;
+  WaveSet::Wave w{0, 0, 0, 0, 0, 0, 0};
+  long long used = 0;
+  for (size_t i = 0; i < Pl.size(); i++) {
+    const int P = Pl[i];
+    if (P == 0) continue;
+    const long long nmt = (9LL * P + 127) / 128, LD = l2t_ld(P);
+    wl.push_back((int)i);
+    go.push_back(used);
+    so.push_back(used + nmt * nkt * 8192);
+    bo.push_back(used + nmt * nkt * 8192 + C * LD);
+    for (long long ct = 0; ct < nct; ct++)
+      for (long long mt = 0; mt < nmt; mt++)
+        tasks.push_back({go.back() + mt * nkt * 8192, bo.back() + ct * nkt * 8192, so.back(), 9 * P, C, (int)nkt,
+                         (int)(128 * mt), (int)(128 * ct), (int)LD});
+    used += nmt * nkt * 8192 + C * LD + nct * nkt * 8192;
+    w.maxn = std::max(w.maxn, P);
+    w.nwl++;
+  }
+  w.ntask = (int)tasks.size();
+  w.used = used;
+  if (w.nwl > 0) W.w.push_back(w);
+  W.upload(wl, go, so, bo, {}, st_);
+  h2d(W.btasks, tasks, st_);
+  l2t_scratch_.resize((std::max<long long>(used, 1) * sizeof(float) + sizeof(double) - 1) / sizeof(double));
+  l2t_scratch_.zero(st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));  // the host vectors go away
+  W.key = key;
+  return true;
+}
+
+void Plan::l2t_split_run(const L2TArgs& la, int R, const float* local, bool image) {
+  WaveSet& W = l2t_waves_;
+  float* sc = reinterpret_cast<float*>(l2t_scratch_.get());
+  for (const auto& w : W.w)
+    launch_l2t_bulk(st_, la, R, w.nwl, W.leaves.get(), W.off1.get(), W.off2.get(), W.off3.get(), w.maxn, sc, w.ntask,
+                    W.btasks.get(), local, (long long)tr_.nboxes, image, !W.feat_valid, tc_err_ptr());
+  W.feat_valid = true;
+}
+
 void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool mixed) {
   const int D = 2 * ncoef(p_), C = 4 * R;
   L2TArgs la = la0;
@@ -1468,6 +1637,20 @@ void Plan::l2t_twostage(const L2TArgs& la0, int R, int do_src, int do_tgt, bool 
   WaveSet& W = l2t_waves_;
   const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | (do_src << 3) | (do_tgt << 2) | 1 |
                         ((long long)resident_ << 62);
+  // mixed and resident: split operands streamed by bulk copies, where they fit
+  if (mixed && resident_ && tc_enabled() && split_variant()) {
+    const long long skey = key | (1LL << 61);
+    bool ok = W.key == skey;
+    if (!ok) {
+      std::vector<int> Pl(l2t_h_.size());
+      for (size_t j = 0; j < Pl.size(); j++) Pl[j] = (do_src ? l2t_sc_h_[j] : 0) + (do_tgt ? l2t_tc_h_[j] : 0);
+      ok = l2t_split_layout(W, D, C, Pl, skey);
+    }
+    if (ok) {
+      l2t_split_run(la, R, local_f_.get(), false);
+      return;
+    }
+  }
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -2210,6 +2393,19 @@ void Plan::l2t_img_twostage(const L2TArgs& la0, int R, const double* local, cons
   const size_t esz = mixed ? sizeof(float) : sizeof(double);
   WaveSet& W = l2t_waves_;
   const long long key = ((long long)p_ << 40) | ((long long)R << 8) | (esz << 4) | 3 | ((long long)resident_ << 62);
+  if (mixed && resident_ && tc_enabled() && split_variant()) {
+    const long long skey = key | (1LL << 61);
+    bool ok = W.key == skey;
+    if (!ok) {
+      std::vector<int> Pl(l2t_h_.size());
+      for (size_t j = 0; j < Pl.size(); j++) Pl[j] = l2t_tc_h_[j];
+      ok = l2t_split_layout(W, D, C, Pl, skey);
+    }
+    if (ok) {
+      l2t_split_run(la, R, local_f, true);
+      return;
+    }
+  }
   if (W.key != key) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
@@ -2326,8 +2522,11 @@ int Plan::evaluate_image(double rlam, double rmu, int R, const double* d_ssl, co
   } else if (far_) {
     size_t freeb = 0, totb = 0;
     EFMM_CUDA_TRY(cudaMemGetInfo(&freeb, &totb));
-    const double have = 0.5 * (double)freeb + 8.0 * (double)(img_mp_.cap + img_lc_.cap);
-    while (Rc > 1 && 3.0 * 8.0 * nb * 7 * Rc * D > have) Rc /= 2;
+    // the pass's two expansion arrays (FP32 in the mixed form), with room to spare
+    const double esz = precision == 1 ? 4.0 : 8.0;
+    const double have = 0.5 * (double)freeb + (precision == 1 ? 4.0 * (double)(img_mp_f_.cap + img_lc_f_.cap)
+                                                              : 8.0 * (double)(img_mp_.cap + img_lc_.cap));
+    while (Rc > 1 && 3.0 * esz * nb * 7 * Rc * D > have) Rc /= 2;
   }
   rc_last_ = Rc;
   float tot = 0;

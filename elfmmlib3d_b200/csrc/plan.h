@@ -125,6 +125,11 @@ struct WaveSet {
   // resident: one wave whose geometry-only features (unit multipoles, L2T
   // functionals) stay in the scratch between passes; feat_valid: computed
   bool resident = false, feat_valid = false;
+  // split: the resident wave keeps its geometry-only operand as split tiles
+  // and runs k_tc_bulk (btasks; off3 the other operand's split tiles)
+  bool split = false;
+  DevBuf<BulkTask> btasks;
+  double bulk_flops = 0;  // useful flops of btasks
   std::vector<Wave> w;
   std::vector<GemmTask> htasks;
   DevBuf<int> leaves;
@@ -132,7 +137,7 @@ struct WaveSet {
   DevBuf<GemmTask> tasks;
   void clear() {
     key = -1;
-    resident = feat_valid = false;
+    resident = feat_valid = split = false;
     w.clear();
     htasks.clear();
   }
@@ -249,6 +254,13 @@ class Plan {
   // passes when they fit (store / replay and graph passes)
   bool resident_ = false, graph_pass_ = false;
   bool resident_fits(long long elems, size_t esz, size_t cap_bytes);
+  // the resident L2T wave from split operands (mixed form): layout of the
+  // per-leaf split functionals, split local expansions and products for P
+  // points per leaf and C columns; false when it does not fit
+  bool l2t_split_layout(WaveSet& W, int D, int C, const std::vector<int>& P, long long key);
+  void l2t_split_run(const L2TArgs& la, int R, const float* local, bool image);
+  bool p2m_split_layout(WaveSet& W, int D, int R, int nk, int ns, bool image, long long key);
+  void bulk_timed(int ntask, double flops, const BulkTask* dtasks, const float* A, const float* B, float* C, int bn);
   int leaf_override_ = 0;
   double forest_[5] = {0, 0, 0, 0, 0};
   TransSched m2lv_img_, m2lu_, l2l_img_, l2l_img_u_, m2m_u_;
@@ -336,15 +348,15 @@ class Plan {
   long long store_gen_ = 0, store_tc_gen_ = -1, ntc_key_ = -1, ntc_stot_ = 0, ntc_ctot_ = 0;
   int ntc_ntask_ = 0;
   // the pre-split store (tiles of 128 rows x 32 k, TF32 head then tail; the
-  // bulk-copy product of near_bulk.cu), used instead of store_f_ when it
+  // bulk-copy product of tc_bulk.cu), used instead of store_f_ when it
   // fits: per-leaf tile bases and K tiles, the product tasks
   bool near_split_ = false;
-  int near_req_ = -1;  // near_split_variant() when the copy was made
+  int near_req_ = -1;  // split_variant() when the copy was made
   DevBuf<float> store_s_;
   std::vector<long long> tbase_h_;
   std::vector<int> nkt_h_;
   DevBuf<long long> tbase_;
-  DevBuf<NearTcTask> nsp_tasks_;
+  DevBuf<BulkTask> nsp_tasks_;
   bool near_tc_ready(const NearArgs& na);
   void near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt);
   DevBuf<double> store_;

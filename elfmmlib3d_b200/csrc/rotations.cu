@@ -404,6 +404,17 @@ __device__ __forceinline__ void coef_nm(int cc, int& n, int& m) {
 
 constexpr int ROT_THREADS = 512;
 
+// a0 += wx x, a1 += wy x over G columns (paired FP32 FMAs measured slower
+// here than in k_translate_rot_w: this kernel is not issue-bound)
+template <class T, int G>
+__device__ __forceinline__ void fma_rows(T* a0, T* a1, T wx, T wy, const T* x) {
+#pragma unroll
+  for (int g = 0; g < G; g++) {
+    a0[g] += wx * x[g];
+    a1[g] += wy * x[g];
+  }
+}
+
 template <class T, int NCT>
 __global__ void __launch_bounds__(ROT_THREADS)
 k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
@@ -465,22 +476,14 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
         for (int u = 0; u < 2 * UNR; u++) {
           T xv[G];
           V::ld(in + (size_t)(r0 + k + u) * NCT + cg * G, xv);
-#pragma unroll
-          for (int g = 0; g < G; g++) {
-            a0[g] += w[u].x * xv[g];
-            a1[g] += w[u].y * xv[g];
-          }
+          fma_rows<T, G>(a0, a1, w[u].x, w[u].y, xv);
         }
       }
       for (; k < bb; k++) {
         const V2 w = *reinterpret_cast<const V2*>(o + (size_t)k * bb);
         T xv[G];
         V::ld(in + (size_t)(r0 + k) * NCT + cg * G, xv);
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-          a0[g] += w.x * xv[g];
-          a1[g] += w.y * xv[g];
-        }
+        fma_rows<T, G>(a0, a1, w.x, w.y, xv);
       }
       V::st(out + (size_t)(2 * cc) * NCT + cg * G, a0);
       V::st(out + (size_t)(2 * cc + 1) * NCT + cg * G, a1);
@@ -519,11 +522,8 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
         T xr[G], xi[G];
         V::ld(Y + (size_t)rk * NCT + cg * G, xr);
         V::ld(Y + (size_t)(rk + 1) * NCT + cg * G, xi);
-#pragma unroll
-        for (int g = 0; g < G; g++) {
-          a0[g] += wr[u].x * xr[g] + wi[u].x * xi[g];
-          a1[g] += wr[u].y * xr[g] + wi[u].y * xi[g];
-        }
+        fma_rows<T, G>(a0, a1, wr[u].x, wr[u].y, xr);
+        fma_rows<T, G>(a0, a1, wi[u].x, wi[u].y, xi);
       }
     }
     for (; k <= p; k++) {
@@ -534,11 +534,8 @@ k_translate_rot(const TransTask* __restrict__ tasks, const TransPair* __restrict
       T xr[G], xi[G];
       V::ld(Y + (size_t)rk * NCT + cg * G, xr);
       V::ld(Y + (size_t)(rk + 1) * NCT + cg * G, xi);
-#pragma unroll
-      for (int g = 0; g < G; g++) {
-        a0[g] += wr.x * xr[g] + wi.x * xi[g];
-        a1[g] += wr.y * xr[g] + wi.y * xi[g];
-      }
+      fma_rows<T, G>(a0, a1, wr.x, wr.y, xr);
+      fma_rows<T, G>(a0, a1, wi.x, wi.y, xi);
     }
     const int cc = n * (n + 1) / 2 + m;
     V::st(X + (size_t)(2 * cc) * NCT + cg * G, a0);
@@ -632,13 +629,16 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
     *reinterpret_cast<float4*>(X + (size_t)r * NCT + cg * G) = make_float4(v[0], v[1], v[2], v[3]);
   }
   __syncthreads();
-  auto put_rows = [&](int ra, int rb, const float* a0, const float* a1) {
+  // accumulators: column pairs (2c, 2c + 1) packed in a float2, updated by
+  // the paired FP32 FMA (__ffma2_rn: two correctly rounded FMAs in one
+  // instruction, half the issue slots of the products)
+  auto put_rows = [&](int ra, int rb, const float2* a0, const float2* a1) {
 #pragma unroll
     for (int q = 0; q < NCT / 4; q++) {
       *reinterpret_cast<float4*>(X + (size_t)ra * NCT + 4 * q) =
-          make_float4(a0[4 * q], a0[4 * q + 1], a0[4 * q + 2], a0[4 * q + 3]);
+          make_float4(a0[2 * q].x, a0[2 * q].y, a0[2 * q + 1].x, a0[2 * q + 1].y);
       *reinterpret_cast<float4*>(X + (size_t)rb * NCT + 4 * q) =
-          make_float4(a1[4 * q], a1[4 * q + 1], a1[4 * q + 2], a1[4 * q + 3]);
+          make_float4(a1[2 * q].x, a1[2 * q].y, a1[2 * q + 1].x, a1[2 * q + 1].y);
     }
   };
   // the warp's operator columns, ROTW_CH at a time, copied asynchronously
@@ -660,7 +660,7 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
   // one block product: rows 2 lane, 2 lane + 1 of the block (if < nrow),
   // columns kk < ncol of the operator (ld = nrow); the operator column pairs
   // of input row k are (2k, 2k + 1) for the shift (pair = true), else k
-  auto block = [&](const float* blk, int nrow, int ncol, bool pair, auto xrow, float* a0, float* a1) {
+  auto block = [&](const float* blk, int nrow, int ncol, bool pair, auto xrow, float2* a0, float2* a1) {
     const bool act = 2 * lane < nrow;
     const int nch = (ncol + ROTW_CH - 1) / ROTW_CH;
     fetch(blk, nrow, ncol, 0);
@@ -676,12 +676,16 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
       if (!pair) {
         for (int u = 0; u < cend; u++) {
           const float2 w = act ? *reinterpret_cast<const float2*>(wb + u * nrow) : make_float2(0.f, 0.f);
+          const float2 wx = make_float2(w.x, w.x), wy = make_float2(w.y, w.y);
           const float4* xr = reinterpret_cast<const float4*>(X + (size_t)xrow(ch * ROTW_CH + u) * NCT);
 #pragma unroll
           for (int q = 0; q < NCT / 4; q++) {
             const float4 x = xr[q];
-            a0[4 * q] += w.x * x.x; a0[4 * q + 1] += w.x * x.y; a0[4 * q + 2] += w.x * x.z; a0[4 * q + 3] += w.x * x.w;
-            a1[4 * q] += w.y * x.x; a1[4 * q + 1] += w.y * x.y; a1[4 * q + 2] += w.y * x.z; a1[4 * q + 3] += w.y * x.w;
+            const float2 xl = make_float2(x.x, x.y), xh = make_float2(x.z, x.w);
+            a0[2 * q] = __ffma2_rn(wx, xl, a0[2 * q]);
+            a0[2 * q + 1] = __ffma2_rn(wx, xh, a0[2 * q + 1]);
+            a1[2 * q] = __ffma2_rn(wy, xl, a1[2 * q]);
+            a1[2 * q + 1] = __ffma2_rn(wy, xh, a1[2 * q + 1]);
           }
         }
       } else {
@@ -691,13 +695,17 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
           const int rk = xrow((ch * ROTW_CH + u) >> 1);
           const float4* xre = reinterpret_cast<const float4*>(X + (size_t)rk * NCT);
           const float4* xim = reinterpret_cast<const float4*>(X + (size_t)(rk + 1) * NCT);
+          const float2 wrx = make_float2(wr.x, wr.x), wry = make_float2(wr.y, wr.y);
+          const float2 wix = make_float2(wi.x, wi.x), wiy = make_float2(wi.y, wi.y);
 #pragma unroll
           for (int q = 0; q < NCT / 4; q++) {
             const float4 xr = xre[q], xi = xim[q];
-            a0[4 * q] += wr.x * xr.x + wi.x * xi.x; a0[4 * q + 1] += wr.x * xr.y + wi.x * xi.y;
-            a0[4 * q + 2] += wr.x * xr.z + wi.x * xi.z; a0[4 * q + 3] += wr.x * xr.w + wi.x * xi.w;
-            a1[4 * q] += wr.y * xr.x + wi.y * xi.x; a1[4 * q + 1] += wr.y * xr.y + wi.y * xi.y;
-            a1[4 * q + 2] += wr.y * xr.z + wi.y * xi.z; a1[4 * q + 3] += wr.y * xr.w + wi.y * xi.w;
+            const float2 rl = make_float2(xr.x, xr.y), rh = make_float2(xr.z, xr.w);
+            const float2 il = make_float2(xi.x, xi.y), ih = make_float2(xi.z, xi.w);
+            a0[2 * q] = __ffma2_rn(wix, il, __ffma2_rn(wrx, rl, a0[2 * q]));
+            a0[2 * q + 1] = __ffma2_rn(wix, ih, __ffma2_rn(wrx, rh, a0[2 * q + 1]));
+            a1[2 * q] = __ffma2_rn(wiy, il, __ffma2_rn(wry, rl, a1[2 * q]));
+            a1[2 * q + 1] = __ffma2_rn(wiy, ih, __ffma2_rn(wry, rh, a1[2 * q + 1]));
           }
         }
       }
@@ -708,9 +716,9 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
     for (int n = 0; n <= p; n++) {
       if (owner[n] != warp) continue;
       const int bb = 2 * n + 2, r0 = n * (n + 1);
-      float a0[NCT], a1[NCT];
+      float2 a0[NCT / 2], a1[NCT / 2];
 #pragma unroll
-      for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
+      for (int c = 0; c < NCT / 2; c++) a0[c] = a1[c] = make_float2(0.0f, 0.0f);
       block(pool + base + rot_block_off(n), bb, bb, false, [&](int k) { return r0 + k; }, a0, a1);
       if (2 * lane < bb) put_rows(r0 + 2 * lane, r0 + 2 * lane + 1, a0, a1);
       __syncwarp();
@@ -722,9 +730,9 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
   for (int m = 0; m <= p; m++) {
     if (owner[p - m] != warp) continue;
     const int bz = 2 * (p - m + 1);
-    float a0[NCT], a1[NCT];
+    float2 a0[NCT / 2], a1[NCT / 2];
 #pragma unroll
-    for (int c = 0; c < NCT; c++) a0[c] = a1[c] = 0.0f;
+    for (int c = 0; c < NCT / 2; c++) a0[c] = a1[c] = make_float2(0.0f, 0.0f);
     block(pool + op.z + z_block_off(p, m), bz, bz, true,
           [&](int kq) { const int k = m + kq; return 2 * (k * (k + 1) / 2 + m); }, a0, a1);
     if (2 * lane < bz) {

@@ -513,20 +513,23 @@ int efmm_gcr_dense_host(int n, int nrhs, const double *A, const double *B, doubl
  * counterpart in the reference. */
 int efmm_tc_variant(int ring);
 
-/* Form of the mixed replay of a stored near field for this process: 1
- * (default) the store split once into TF32 head / tail tiles streamed by
- * bulk copies into the tensor cores (8 bytes per stored element), 0 the FP32
- * copy split in shared memory on every replay (4 bytes per element; also
- * used when the split store does not fit).  Returns the previous form.
- * Replaces nothing in the reference (an implementation choice). */
-int efmm_near_variant(int split);
+/* Form of the mixed-precision products whose one operand depends on the
+ * geometry only (the stored near field's replay, the resident L2T
+ * functionals) for this process: 1 (default) that operand split once into
+ * TF32 head / tail tiles, the other split per call, both streamed by bulk
+ * copies into the tensor cores (8 bytes per element; used where it fits), 0
+ * FP32 operands split in shared memory on every call (also
+ * ELFMM3D_SPLIT=0).  Returns the previous form.  No counterpart in the
+ * reference. */
+int efmm_split_variant(int split);
 
-/* Self-check of the bulk-copy product of the split store on random operands
- * (A K x M, B N x K in [-1, 1), M <= 4096, N <= 1024): relative l2 error
- * against an FP64 host product in *rel, the kernel's error flag (a wait that
- * ran out) in *timeout.  Returns 0, 16 (bad sizes) or 256 (device error).
- * Test entry; no counterpart in the reference. */
-int efmm_near_bulk_selfcheck(int M, int N, int K, unsigned seed, double *rel, int *timeout);
+/* Self-check of the bulk-copy product of split operands on random A (K x M)
+ * and B (N x K) in [-1, 1) (M <= 8192, N <= 1024, bn 64 or 128 columns per
+ * tile, fp64 != 0: FP64 K-tile sums): relative l2 error against an FP64 host
+ * product in *rel, the kernel's error flag (a wait that ran out) in
+ * *timeout.  Returns 0, 16 (bad sizes) or 256 (device error).  Test entry;
+ * no counterpart in the reference. */
+int efmm_tc_bulk_selfcheck(int M, int N, int K, int bn, int fp64, unsigned seed, double *rel, int *timeout);
 
 /* The autotuner (no counterpart in the reference, whose tuning is the fixed
  * iprec tables, src/elfmm3dtria.f:702-722): per key (knob, expansion order,

@@ -1,9 +1,10 @@
-"""The mixed replay of a stored near field from the pre-split store: TF32
-head / tail tiles of the store and of the densities streamed by bulk copies
-into the tensor cores (k_near_tc_bulk).  The product alone against an FP64
-host product (full tiles, ragged M, N, K, an empty K), and the replay of a
-plan against the replay from the FP32 copy (efmm_near_variant(0), the same
-splits and K-tile sums) and against the FP64 replay."""
+"""Products from pre-split operands: TF32 head / tail tiles streamed by bulk
+copies into the tensor cores (k_tc_bulk, tc_bulk.cu).  The product alone
+against an FP64 host product (64- and 128-column tiles, FP32 and FP64 K-tile
+sums, full tiles, ragged M, N, K, an empty K); the mixed replay of a stored
+near field from its split against the replay from the FP32 copy
+(efmm_split_variant(0), the same splits and K-tile sums) and against the FP64
+replay."""
 import ctypes
 
 import numpy as np
@@ -15,34 +16,37 @@ from elfmmlib3d_b200 import geometry as G
 pytestmark = pytest.mark.gpu
 
 
-def _check(gpu, M, N, K, seed):
-    f = gpu.load().efmm_near_bulk_selfcheck
+def _check(gpu, M, N, K, seed, bn=64, fp64=1):
+    f = gpu.load().efmm_tc_bulk_selfcheck
     f.restype = ctypes.c_int
-    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint, ctypes.POINTER(ctypes.c_double),
-                  ctypes.POINTER(ctypes.c_int)]
+    f.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint,
+                  ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     r, to = ctypes.c_double(), ctypes.c_int()
-    ier = f(M, N, K, seed, ctypes.byref(r), ctypes.byref(to))
+    ier = f(M, N, K, bn, fp64, seed, ctypes.byref(r), ctypes.byref(to))
     return ier, r.value, to.value
 
 
+@pytest.mark.parametrize("bn,fp64", [(64, 1), (64, 0), (128, 0), (128, 1)])
 @pytest.mark.parametrize("M,N,K", [(128, 64, 32), (256, 64, 640), (300, 37, 1000), (1700, 64, 6000),
-                                   (9, 130, 45), (5, 7, 3)])
-def test_bulk_product_fp32_accuracy(gpu, M, N, K):
-    ier, r, to = _check(gpu, M, N, K, 5)
-    print(f"bulk product {M}x{N}x{K}: rel {r:.2e}")
+                                   (9, 130, 45), (5, 7, 3), (4320, 256, 992)])
+def test_bulk_product_fp32_accuracy(gpu, M, N, K, bn, fp64):
+    ier, r, to = _check(gpu, M, N, K, 5, bn, fp64)
+    print(f"bulk product {M}x{N}x{K} (bn {bn}, fp64 sums {fp64}): rel {r:.2e}")
     assert ier == 0 and to == 0
     # FP32 products of K terms in [-1, 1), K-tile sums in FP64: ~1e-7
     assert r < 2e-6
 
 
-def test_bulk_product_empty_k(gpu):
-    ier, r, to = _check(gpu, 200, 64, 0, 1)
+@pytest.mark.parametrize("bn", [64, 128])
+def test_bulk_product_empty_k(gpu, bn):
+    ier, r, to = _check(gpu, 200, 64, 0, 1, bn)
     assert ier == 0 and to == 0 and r == 0.0
 
 
 def test_bulk_product_rejects_bad_sizes(gpu):
     assert _check(gpu, 0, 64, 32, 1)[0] == 16
     assert _check(gpu, 128, 2000, 32, 1)[0] == 16
+    assert _check(gpu, 128, 64, 32, 1, bn=96)[0] == 16
 
 
 def _batch_mode(P, d, R, ssl, sdl, n, m, mode, precision=0, strain=True):
@@ -62,7 +66,7 @@ def test_split_replay_matches_fp32_copy_and_fp64(gpu, R, strain, layers):
     # R = 70 runs as two passes; R = 5 leaves 59 columns of the density tile
     # empty; one layer without strain rows is the smallest stored block
     import torch
-    var = gpu.load().efmm_near_variant
+    var = gpu.load().efmm_split_variant
     var.restype = ctypes.c_int
     tri, nrm, cen = G.sphere_triangles(3)
     tg = G.box_targets(90, 47)
