@@ -830,7 +830,7 @@ def run_hsbatch(args, rank, world, local_rank):
     pe0.record()
     for _ in range(args.steps):
         step()
-        stages.append((F.timings(), I.timings(), F.product_stats(), I.product_stats()))
+        stages.append((F.timings(), I.timings(), F.product_stats(), I.product_stats(), F.near_stats()))
     pe1.record()
     pe1.synchronize()
     nograph_ms = pe0.elapsed_time(pe1) / args.steps
@@ -980,12 +980,32 @@ def run_hsbatch(args, rank, world, local_rank):
         peak_source += f" (its bf16_tflops is {bf16})"
     except (OSError, ValueError, TypeError):
         pass
-    roof_tc = {"kernel": "k_gemm_tc (P2M products, tcgen05.mma kind::tf32, free-space and image plans)",
+    roof_tc = {"kernel": "k_tc_bulk<64, float> (P2M products: split unit multipoles x split densities streamed "
+                         "by bulk copies, tcgen05.mma kind::tf32, free-space and image plans)",
                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                "frac": (achieved / peak) if peak else None, "traffic": None, "peak_source": peak_source,
                "useful_fp32_tflops": useful,
                "algorithmic": f"{prod_flops:.4g} useful FP32 flop per step (unit multipoles x densities) in "
                               f"{prod_ms:.1f} ms of product launches; 3 TF32 MMAs per FP32 product"}
+    # the stored free-space near field's product (k_tc_bulk<64, double>):
+    # the split store (TF32 head + tail per element), the split densities and
+    # the FP64 products it writes, against the measured HBM copy rate
+    nms = float(np.mean([s_[4][0] for s_ in stages]))
+    nbytes = float(np.mean([s_[4][1] for s_ in stages]))
+    roof_near = None
+    if nms > 0 and nbytes > 0:
+        try:
+            hbm = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))).get("hbm_gbs")
+        except (OSError, ValueError):
+            hbm = None
+        nach = nbytes / (nms * 1e-3) / 1e9
+        roof_near = {"kernel": "k_tc_bulk<64, double> (replay of the stored free-space near field from its split: "
+                               "pre-split tiles streamed by bulk copies into the tensor cores, FP64 K-tile sums)",
+                     "bound": "hbm", "achieved": nach, "peak": hbm, "unit": "GB/s",
+                     "frac": nach / hbm if hbm else None, "traffic": None,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs" if hbm else "MEASURED_PEAKS.json absent",
+                     "algorithmic": f"{nbytes:.4g} bytes per replay (split store 8 bytes per stored element, split "
+                                    f"densities, FP64 products) in {nms:.2f} ms (CUDA events around the launch)"}
     # the dominant kernels of the step (ncu launch shares): the factored
     # translations (k_translate_rot_w / k_translate_rot, FP32 FMA pipe),
     # flops counted per pair and column as they run, time = the M2M + M2L +
@@ -1062,6 +1082,7 @@ def run_hsbatch(args, rank, world, local_rank):
         "gpu_launches": launches,
         "roofline": roof,
         "roofline_tc": roof_tc,
+        "roofline_near": roof_near,
         "cpu_baseline": cpu,
         "clocks": clk.summary(),
     }

@@ -44,7 +44,7 @@ _vp = ctypes.c_void_p
 # symbols the library must export (checked by the CPU test suite)
 EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_device_count",
            "efmm_plan_create", "efmm_plan_destroy", "efmm_plan_set_geometry",
-           "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings", "efmm_plan_product_stats",
+           "efmm_plan_evaluate", "efmm_plan_evaluate_direct", "efmm_plan_timings", "efmm_plan_product_stats", "efmm_plan_near_stats",
            "efmm_plan_info", "efmm_plan_tree_export", "efmm_kernel_launches", "efmm_plan_record",
            "efmm_plan_elapsed", "efmm_direct_noalloc", "elfmm3dtriatargiter_", "elfmm3dtriaiter_",
            "efmm_iter_release", "efmm_iter_stored_bytes", "efmm_plan_setup_timings",
@@ -757,6 +757,13 @@ class Plan:
         """(device ms, useful flops) of the P2M product stage of the last batch."""
         a = (ctypes.c_double * 2)()
         self._L.efmm_plan_product_stats(self._h, a)
+        return float(a[0]), float(a[1])
+
+    def near_stats(self):
+        """(device ms, bytes) of the tensor-core product of the last mixed
+        replay of the stored near field from its split (zeros otherwise)."""
+        a = (ctypes.c_double * 2)()
+        self._L.efmm_plan_near_stats(self._h, a)
         return float(a[0]), float(a[1])
 
     def evaluate_direct_subset(self, rlam, rmu, nsub, ssl=None, sdl=None, u=None, e=None):

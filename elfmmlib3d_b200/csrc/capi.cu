@@ -195,6 +195,8 @@ extern "C" void efmm_plan_product_stats(const efmm_plan* p, double* out2) {
   out2[1] = p->plan->product_flops();
 }
 
+extern "C" void efmm_plan_near_stats(const efmm_plan* p, double* out2) { p->plan->near_stats(out2); }
+
 extern "C" void efmm_plan_setup_timings(const efmm_plan* p, float* ms) {
   const Timings& t = p->plan->timings;
   ms[0] = t.geo_tree; ms[1] = t.geo_lists; ms[2] = t.geo_work; ms[3] = t.geo_ops;

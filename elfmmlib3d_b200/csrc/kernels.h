@@ -68,13 +68,14 @@ int split_variant();  // 1: pre-split operands where they fit (default), 0: FP32
 // B tiles of 64 columns (column tile ct at sbase[i] + (ct nkt + kt) 4096;
 // positions past R or K must hold zeros), the product (tasks per leaf, row
 // tile and column tile; C at coff, ldc = KB x points, FP64 sums), the
-// results ADDED to the outputs, the self pairs in FP64.
+// results ADDED to the outputs, the self pairs in FP64; ev (two events, or
+// null) recorded around the product.
 void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long* base, const long long* tbase,
                              const int* ntri, int K, int KB, const double* store, float* out);
 void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
                        const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
                        const BulkTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
-                       const long long* base, const double* store, int* err);
+                       const long long* base, const double* store, int* err, cudaEvent_t* ev = nullptr);
 void launch_direct_all(cudaStream_t st, int ntri, const TriRec* trir, int nsrc, const double* src_pts,
                        int ntgt, const double* tgt_pts, int dosl, int dodl, int dostrain_src,
                        int dostrain_tgt, double rlam, double rmu, double* u_src, double* e_src,

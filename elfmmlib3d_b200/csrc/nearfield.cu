@@ -757,11 +757,13 @@ void launch_near_split_store(cudaStream_t st, const NearArgs& a, const long long
 void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
                        const double* g1, const long long* sbase, const int* ntri, float* S, int ntask,
                        const BulkTask* tasks, const float* A, const long long* coff, double* C, int nsrc, int ntgt,
-                       const long long* base, const double* store, int* err) {
+                       const long long* base, const double* store, int* err, cudaEvent_t* ev) {
   if (a.nleaf <= 0 || R <= 0) return;
   k_near_sigma_split<<<dim3(a.nleaf, 8), 256, 0, st>>>(a, R, NJ, g0, g1, sbase, ntri, S);
   count_launch();
+  if (ev) EFMM_CUDA_TRY(cudaEventRecord(ev[0], st));
   launch_tc_bulk<double>(st, ntask, tasks, A, S, C, err, 64);
+  if (ev) EFMM_CUDA_TRY(cudaEventRecord(ev[1], st));
   k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
   count_launch();
   if (a.do_src) {

@@ -276,6 +276,8 @@ Plan::~Plan() {
   graph_reset();
   for (int i = 0; i < 10; i++) cudaEventDestroy(ev_[i]);
   for (cudaEvent_t e : pev_) cudaEventDestroy(e);
+  for (cudaEvent_t e : nev_)
+    if (e) cudaEventDestroy(e);
 }
 
 void Plan::product_begin() { npev_ = 0; }
@@ -316,6 +318,16 @@ void Plan::product_timed(int ntask, const std::vector<GemmTask>& tasks, long lon
 }
 
 // after the pass's final synchronisation
+// the near-field product of the last replay from the split store (events
+// recorded outside graph capture): out[0] ms, out[1] the bytes its operands
+// and results take (split store, split densities, FP64 products)
+void Plan::near_stats(double* out) const {
+  float ms = 0;
+  if (near_timed_ && nev_[0] && cudaEventQuery(nev_[1]) == cudaSuccess) cudaEventElapsedTime(&ms, nev_[0], nev_[1]);
+  out[0] = near_timed_ ? ms : 0.0;
+  out[1] = near_timed_ ? near_bytes_ : 0.0;
+}
+
 void Plan::product_collect() {
   for (int i = 0; i + 1 < npev_; i += 2) {
     float ms = 0;
@@ -957,9 +969,14 @@ void Plan::near_tc(const NearArgs& na, int R, const double* g0, const double* g1
       ntc_key_ = key;
     }
     ntc_cbuf_.resize((size_t)ntc_ctot_);
+    near_timed_ = !capturing_;
+    if (near_timed_)
+      for (cudaEvent_t& e : nev_)
+        if (!e) EFMM_CUDA_TRY(cudaEventCreate(&e));
+    near_bytes_ = 4.0 * (double)store_s_.size() + 4.0 * (double)ntc_stot_ + 8.0 * (double)ntc_ctot_;
     launch_near_split(st_, na, R, NJ, KB, g0, g1, ntc_soff_.get(), near_ntri_.get(), ntc_scratch_.get(), ntc_ntask_,
                       nsp_tasks_.get(), store_s_.get(), ntc_coff_.get(), ntc_cbuf_.get(), n, nt, near_base_.get(),
-                      store_.get(), tc_err_ptr());
+                      store_.get(), tc_err_ptr(), near_timed_ ? nev_ : nullptr);
     return;
   }
   const long long key = ((long long)R << 8) | store_flags_;

@@ -234,6 +234,7 @@ class Plan {
   // P2M product stage of the last evaluate_batch / evaluate_image: device ms
   // (CUDA events around each product launch) and useful flops
   double product_ms() const { return product_ms_; }
+  void near_stats(double* out) const;
   double product_flops() const { return product_flops_; }
   bool far_enabled() const { return far_; }
 
@@ -357,6 +358,10 @@ class Plan {
   std::vector<int> nkt_h_;
   DevBuf<long long> tbase_;
   DevBuf<BulkTask> nsp_tasks_;
+  // events around the split near-field product (outside graph capture)
+  cudaEvent_t nev_[2] = {nullptr, nullptr};
+  bool near_timed_ = false;
+  double near_bytes_ = 0;
   bool near_tc_ready(const NearArgs& na);
   void near_tc(const NearArgs& na, int R, const double* g0, const double* g1, int n, int nt);
   DevBuf<double> store_;

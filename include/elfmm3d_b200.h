@@ -466,6 +466,13 @@ void efmm_plan_timings(const efmm_plan *plan, float *ms8);
  * around each product launch), out2[1] its useful FP32 flops. */
 void efmm_plan_product_stats(const efmm_plan *plan, double *out2);
 
+/* The tensor-core product of the last mixed replay of the stored near field
+ * from its split (outside CUDA-graph capture): out2[0] device ms (CUDA
+ * events around the launch), out2[1] the bytes of its operands and results
+ * (split store, split densities, FP64 products); zeros when the last mixed
+ * replay did not use the split.  No counterpart in the reference. */
+void efmm_plan_near_stats(const efmm_plan *plan, double *out2);
+
 /* Host wall-clock ms of the last set_geometry: tree, lists, work lists
  * (with the tree-order gathers), translation operators. */
 void efmm_plan_setup_timings(const efmm_plan *plan, float *ms4);
