@@ -811,9 +811,9 @@ def run_hsbatch(args, rank, world, local_rank):
         F.evaluate_batch(1.0, 1.0, R, None, dsdl, uf, ef, precision=precision, mode=mode, graph=graph)
         I.evaluate_image(1.0, 1.0, R, None, dsdl, ui, ei, precision=precision, mode=mode, graph=graph)
 
-    # mixed form's truncation floor (the library default): orders for
-    # max(eps(iprec), 5e-8), no truncation finer than the FP32 rounding
-    mixed_floor = 5e-8
+    # mixed form's truncation floor: orders for max(eps(iprec), floor), by
+    # default the library's 5e-8 (the FP32 rounding of the result)
+    mixed_floor = args.mixed_floor
     p_mixed = F.set_mixed_floor(mixed_floor)
     I.set_mixed_floor(mixed_floor)
     t0 = time.perf_counter()
@@ -876,6 +876,22 @@ def run_hsbatch(args, rank, world, local_rank):
     pe1.synchronize()
     mixed_iprec_ms = pe0.elapsed_time(pe1) / args.steps
     u_mi, e_mi = (uf + ui).clone(), (ef + ei).clone()
+    # and at a coarser floor (5e-7: orders 26 at iprec 3), to show the
+    # order / time trade-off; plain passes timed with events
+    coarse_floor = 5e-7
+    p_coarse = F.set_mixed_floor(coarse_floor)
+    I.set_mixed_floor(coarse_floor)
+    for _ in range(2):
+        step()
+    torch.cuda.synchronize()
+    pe0, pe1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    pe0.record()
+    for _ in range(args.steps):
+        step()
+    pe1.record()
+    pe1.synchronize()
+    mixed_coarse_ms = pe0.elapsed_time(pe1) / args.steps
+    u_mc, e_mc = (uf + ui).clone(), (ef + ei).clone()
     F.set_mixed_floor(mixed_floor)
     I.set_mixed_floor(mixed_floor)
 
@@ -910,7 +926,7 @@ def run_hsbatch(args, rank, world, local_rank):
     ed = torch.zeros((ns, 3, 3), dtype=torch.float64, device=dev)
     rel = lambda a, b: float(torch.linalg.norm(a - b) / torch.linalg.norm(b))
     errs = {"plain_fp64": [0.0, 0.0], "batched_fp64": [0.0, 0.0], "mixed_batched": [0.0, 0.0],
-            "mixed_batched_iprec_orders": [0.0, 0.0]}
+            "mixed_batched_iprec_orders": [0.0, 0.0], "mixed_batched_floor_5e-7": [0.0, 0.0]}
     for r in (0, R - 1):
         F.evaluate_direct_subset(1.0, 1.0, ns, None, dsdl[r], ud, ed)
         ier, uid, eid = E.hs_image_direct(1.0, 1.0, tri, nrm, None, sdl[r], cen[:ns])
@@ -919,7 +935,8 @@ def run_hsbatch(args, rank, world, local_rank):
         edt = ed + torch.from_numpy(eid).to(dev)
         for key, (uu, ee) in (("plain_fp64", (u1, e1)), ("batched_fp64", (u64, e64)),
                               ("mixed_batched", (u_mixed, e_mixed)),
-                              ("mixed_batched_iprec_orders", (u_mi, e_mi))):
+                              ("mixed_batched_iprec_orders", (u_mi, e_mi)),
+                              ("mixed_batched_floor_5e-7", (u_mc, e_mc))):
             errs[key][0] = max(errs[key][0], rel(uu[r, :ns], udt))
             errs[key][1] = max(errs[key][1], rel(ee[r, :ns], edt))
     trf = F.translation_flops(R, 1)
@@ -1056,11 +1073,14 @@ def run_hsbatch(args, rank, world, local_rank):
                              "plain_fp64": plain_value, "mixed_over_plain": value / world / plain_value,
                              "plain_fp64_ms": plain_ms, "batched_fp64_ms": b64_ms,
                              "mixed_batched_iprec_orders": evals / (mixed_iprec_ms * 1e-3),
-                             "mixed_iprec_orders_ms": mixed_iprec_ms},
+                             "mixed_iprec_orders_ms": mixed_iprec_ms,
+                             "mixed_batched_floor_5e-7": evals / (mixed_coarse_ms * 1e-3),
+                             "mixed_floor_5e-7_ms": mixed_coarse_ms, "mixed_floor_5e-7_order": p_coarse},
                    "orders": {"iprec": fi["p"], "mixed": p_mixed, "mixed_floor": mixed_floor,
                               "rule": "mixed form: expansions and translations truncated at max(eps(iprec), "
-                                      "floor), no finer than its FP32 rounding; plain and batched FP64 forms "
-                                      "at eps(iprec)"},
+                                      "floor), by default the library's floor 5e-8 (the FP32 rounding of the "
+                                      "result); plain and batched FP64 forms at eps(iprec); the forms at the "
+                                      "iprec orders and at the floor 5e-7 are timed beside it (plain passes)"},
                    "rel_err_vs_direct": {k: {"u": v[0], "strain": v[1]} for k, v in errs.items()},
                    "rel_err_sample": f"{ns} centroids, right-hand sides 0 and {R - 1}",
                    "rel_err_vs_oracle": oerr,
@@ -1470,6 +1490,7 @@ def run_uneven(args, rank, world, local_rank):
     F = E.Forest(local_rank) if engine == "forest" else None
     if F is not None:
         F.set_leaf(args.free_leaf, args.image_leaf)
+        F.set_mixed_floor(args.mixed_floor)
 
     split = {}
 
@@ -1521,6 +1542,7 @@ def run_uneven(args, rank, world, local_rank):
     # e2e: host arrays through the C ABI, host wall clock
     e2e_t = []
     if engine == "forest":
+        E.set_many_host_mixed_floor(args.mixed_floor)
         for _ in range(args.steps):
             t0 = time.perf_counter()
             ier, uu, ee = E.hs_many_host(w["iprec"], 1.0, 1.0, counts, h_tri, h_nrm, h_cen, None, h_sdl, precision=1)
@@ -1607,6 +1629,9 @@ def main():
                     help="uneven forest: leaf capacity of the image plan (0: half the iprec table)")
     ap.add_argument("--uneven-workers", type=int, default=0,
                     help="uneven batch: host worker threads (default: the host threads, 4 to 16)")
+    ap.add_argument("--mixed-floor", type=float, default=5e-8,
+                    help="half-space workloads: tolerance floor of the mixed form's expansion orders (default: "
+                         "the library's, 5e-8, the FP32 rounding of the result)")
     ap.add_argument("--no-graph", action="store_true",
                     help="half-space batch: time plain passes instead of CUDA-graph replays (profiling)")
     args = ap.parse_args()

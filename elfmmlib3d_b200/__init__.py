@@ -62,7 +62,7 @@ EXPORTS = ["elfmm3dtria_", "elfmm3dtriatarg_", "el3dtriadirecttarg_", "efmm_devi
            "elhfmm3dparttarg_", "elhfmm3dpart_", "elh3dpartdirecttarg_", "efmm_plan_set_forest",
            "efmm_forest_create", "efmm_forest_destroy", "efmm_forest_set_geometry", "efmm_forest_evaluate",
            "efmm_forest_plan", "efmm_forest_layout", "elhfmm3dtria_many_host", "efmm_plan_set_leaf",
-           "efmm_forest_set_leaf"]
+           "efmm_forest_set_leaf", "efmm_forest_set_mixed_floor", "efmm_many_host_set_mixed_floor"]
 
 
 class ElfmmError(RuntimeError):
@@ -153,6 +153,10 @@ def load():
     L.efmm_plan_set_leaf.argtypes = [_vp, ctypes.c_int]
     L.efmm_forest_set_leaf.restype = ctypes.c_int
     L.efmm_forest_set_leaf.argtypes = [_vp, ctypes.c_int, ctypes.c_int]
+    L.efmm_forest_set_mixed_floor.restype = ctypes.c_int
+    L.efmm_forest_set_mixed_floor.argtypes = [_vp, ctypes.c_double]
+    L.efmm_many_host_set_mixed_floor.restype = ctypes.c_int
+    L.efmm_many_host_set_mixed_floor.argtypes = [ctypes.c_double]
     L.efmm_forest_plan.restype = _vp
     L.efmm_forest_plan.argtypes = [_vp, ctypes.c_int]
     L.efmm_forest_layout.restype = ctypes.c_int
@@ -900,6 +904,13 @@ class Forest:
             raise ElfmmError(1024, f"cannot create forest on device {device}")
         self.n = 0
 
+    def set_mixed_floor(self, eps):
+        """Tolerance floor of both plans' mixed-form orders (<= 0: the iprec
+        orders)."""
+        ier = self._L.efmm_forest_set_mixed_floor(self._h, float(eps))
+        if ier:
+            raise ElfmmError(ier, "forest set_mixed_floor")
+
     def set_leaf(self, nbox_free=0, nbox_image=0):
         """Leaf capacities of the two plans for the next set_geometry (<= 0:
         the default: the iprec table for the free-space plan, half of it for
@@ -936,6 +947,12 @@ class Forest:
             self.close()
         except Exception:
             pass
+
+
+def set_many_host_mixed_floor(eps):
+    """Tolerance floor of the mixed-form orders of the forest behind
+    hs_many_host (efmm_many_host_set_mixed_floor; <= 0: the iprec orders)."""
+    load().efmm_many_host_set_mixed_floor(float(eps))
 
 
 def hs_many_host(iprec, rlam, rmu, counts, triangle, trinorm, centroids, sigma_sl=None, sigma_dl=None,

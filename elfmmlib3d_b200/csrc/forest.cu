@@ -31,6 +31,7 @@ struct efmm_forest {
   efmm_plan* img = nullptr;  // image part: targets = reflected centroids, Mindlin root
   int nprob = 0, n = 0;
   int leaf_free = 0, leaf_img = 0;  // efmm_forest_set_leaf (0: default)
+  double floor = -1;                 // efmm_forest_set_mixed_floor (< 0: the plans' default)
   DevBuf<long long> off;
   DevBuf<double> bb, tri, cen, refl, uf, ui, ei;
   DevBuf<int> flag;
@@ -119,6 +120,7 @@ int guard(efmm_forest* F, const std::function<int()>& body) {
 
 std::mutex g_forest_mu;
 efmm_forest* g_forest = nullptr;
+double g_forest_floor = -1;  // efmm_many_host_set_mixed_floor
 
 }  // namespace
 
@@ -184,6 +186,16 @@ extern "C" int efmm_forest_set_leaf(efmm_forest* F, int nbox_free, int nbox_imag
   if (!F) return IER_BADARG;
   F->leaf_free = std::max(nbox_free, 0);
   F->leaf_img = std::max(nbox_image, 0);
+  return IER_OK;
+}
+
+extern "C" int efmm_forest_set_mixed_floor(efmm_forest* F, double eps) {
+  if (!F) return IER_BADARG;
+  F->floor = eps;
+  for (efmm_plan* p : {F->f, F->img}) {
+    const int ier = efmm_plan_set_mixed_floor(p, eps, nullptr);
+    if (ier) return ier;
+  }
   return IER_OK;
 }
 
@@ -305,6 +317,10 @@ extern "C" int elhfmm3dtria_many_host(int iprec, double rlam, double rmu, int np
     if (!g_forest) return IER_NODEVICE;
   }
   efmm_forest* F = g_forest;
+  if (g_forest_floor >= 0 && F->floor != g_forest_floor) {
+    const int ier = efmm_forest_set_mixed_floor(F, g_forest_floor);
+    if (ier) return ier;
+  }
   return guard(F, [&]() -> int {
     cudaStream_t st = F->f->stream;
     DevBuf<double> dt, dn, dc, ds, dd, du, de;
@@ -330,4 +346,10 @@ extern "C" int elhfmm3dtria_many_host(int iprec, double rlam, double rmu, int np
     EFMM_CUDA_TRY(cudaStreamSynchronize(st));
     return IER_OK;
   });
+}
+
+extern "C" int efmm_many_host_set_mixed_floor(double eps) {
+  std::lock_guard<std::mutex> lk(g_forest_mu);
+  g_forest_floor = eps > 0 ? eps : 0.0;
+  return IER_OK;
 }

@@ -603,6 +603,14 @@ int efmm_forest_evaluate(efmm_forest *forest, double rlam, double rmu, const dou
  * image near field costs more per pair than its far field). */
 int efmm_forest_set_leaf(efmm_forest *forest, int nbox_free, int nbox_image);
 
+/* Tolerance floor of both plans' mixed-form orders (efmm_plan_set_mixed_floor;
+ * eps <= 0 keeps the iprec orders).  No counterpart in the reference. */
+int efmm_forest_set_mixed_floor(efmm_forest *forest, double eps);
+
+/* The same for the forest behind elhfmm3dtria_many_host (its later calls).
+ * No counterpart in the reference. */
+int efmm_many_host_set_mixed_floor(double eps);
+
 /* The forest's plans: which 0 the free-space (direct arrival) plan, 1 the
  * image plan (for efmm_plan_info, efmm_plan_tree_export, timings). */
 efmm_plan *efmm_forest_plan(efmm_forest *forest, int which);

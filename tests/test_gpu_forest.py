@@ -25,7 +25,7 @@ def _problems(k, seed, nmin=300, nmax=3000):
     return out
 
 
-def _forest(gpu, probs, iprec, precision):
+def _forest(gpu, probs, iprec, precision, floor=None):
     import torch
     dev = torch.device("cuda", 0)
     d = lambda a: torch.tensor(np.ascontiguousarray(a), dtype=torch.float64, device=dev)
@@ -36,6 +36,8 @@ def _forest(gpu, probs, iprec, precision):
     u = torch.zeros((n, 3), dtype=torch.float64, device=dev)
     e = torch.zeros((n, 3, 3), dtype=torch.float64, device=dev)
     F = gpu.Forest(0)
+    if floor is not None:
+        F.set_mixed_floor(floor)
     F.set_geometry(counts, d(cat(0, 9)), d(cat(1, 3)), d(cat(2, 3)), iprec=iprec)
     F.evaluate(1.3, 0.7, d(ssl), d(cat(4, 3)), u, e, precision=precision)
     off = np.concatenate([[0], np.cumsum(counts)])
@@ -61,15 +63,22 @@ def test_forest_matches_single_problem_plans(gpu, precision):
 
 
 def test_forest_matches_direct_sums(gpu):
+    # the mixed form at the library's order floor (5e-8) within 1e-6; a
+    # floor of 5e-7 (efmm_forest_set_mixed_floor) lowers the orders of both
+    # plans: a larger truncation error, measured 2.1e-6 on these problems
+    # against 4.9e-7 (small leaves: the far field carries much of the field)
     import torch
     from elfmmlib3d_b200.batch import _check
     probs = _problems(5, 12)
-    F, res = _forest(gpu, probs, 3, 1)
-    F.close()
-    errs = [_check(p, u, e, 150, 1.3, 0.7, torch.device("cuda", 0)) for p, (u, e) in zip(probs, res)]
-    worst = max(max(x) for x in errs)
-    print(f"forest (mixed) vs FP64 direct sums: {worst:.2e}")
-    assert worst < 1e-6
+    worst = {}
+    for floor in (None, 5e-7):
+        F, res = _forest(gpu, probs, 3, 1, floor)
+        F.close()
+        errs = [_check(p, u, e, 150, 1.3, 0.7, torch.device("cuda", 0)) for p, (u, e) in zip(probs, res)]
+        worst[floor] = max(max(x) for x in errs)
+        print(f"forest (mixed, floor {floor}) vs FP64 direct sums: {worst[floor]:.2e}")
+    assert worst[None] < 1e-6
+    assert worst[None] < worst[5e-7] < 1e-5
 
 
 def test_forest_lists_stay_in_their_column(gpu):
