@@ -712,6 +712,42 @@ void Plan::ensure_factored(bool tc) {
   P->rot_ready = true;
 }
 
+// parity-split FP32 operators (rotations.cu build_split_ops), once per pool
+void Plan::ensure_split() {
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  OpPool* P = ops_;
+  if (P->rots_ready) return;
+  std::vector<int> kinds, orders;
+  std::vector<double> offs;
+  for (const OpDesc& d : P->descs) {
+    kinds.push_back(d.kind);
+    orders.push_back(d.p);
+    offs.insert(offs.end(), {d.d[0], d.d[1], d.d[2]});
+  }
+  std::vector<double> w(2 * (size_t)ncoef(p_));
+  for (int n = 0; n <= p_; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] =
+          std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<RotSOp> sops;
+  std::vector<float> spool;
+  build_split_ops(kinds, orders, offs, w, sops, spool);
+  h2d(P->rots_ops, sops, st_);
+  h2d(P->rots_f, spool, st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  P->rots_ready = true;
+}
+
+// The FP32 translations of orders <= 31 run in the parity-split form unless
+// ELFMM3D_ROT_SPLIT=0 (then the full-block kernels of rotations.cu).
+bool Plan::split_rot() const {
+  static const bool on = [] {
+    const char* e = getenv("ELFMM3D_ROT_SPLIT");
+    return !(e && e[0] == '0');
+  }();
+  return on && factored_ && p_ <= 31;
+}
+
 // The tensor-core form serves the FP32 translations of pools of order <= 31
 // (blocks of at most 64 rows); ELFMM3D_ROT_TC=0 keeps them on the CUDA cores.
 bool Plan::rot_tc_usable() const {
@@ -824,9 +860,18 @@ void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T
       pool = reinterpret_cast<const T*>(ops_->rot_d.get());
     else
       pool = reinterpret_cast<const T*>(ops_->rot_f.get());
-    for (size_t i = 0; i < S.lev_rtasks.size(); i++)
+    const bool split = sizeof(T) == 4 && split_rot();
+    if (split) ensure_split();
+    for (size_t i = 0; i < S.lev_rtasks.size(); i++) {
+      if (split && rot_split_ok(S.lev_rdim[i])) {
+        launch_translate_rot_split(st_, S.lev_rtasks[i].second, S.rtasks.get() + S.lev_rtasks[i].first,
+                                   S.pairs.get(), ops_->rots_ops.get(), ops_->rots_f.get(), D, C, S.lev_rdim[i],
+                                   reinterpret_cast<const float*>(src), reinterpret_cast<float*>(dst));
+        continue;
+      }
       launch_translate_rot<T>(st_, S.lev_rtasks[i].second, S.rtasks.get() + S.lev_rtasks[i].first, S.pairs.get(),
                               ops_->rot_ops.get(), pool, D, C, S.lev_rdim[i], src, dst);
+    }
     return;
   }
   cut_tasks(S, C);
@@ -1213,10 +1258,18 @@ void Plan::translation_flops(int R, bool mixed, double* f) {
   ensure_ops();
   const double D = 2.0 * ncoef(p_);
   const bool fact = factored_ && 2.0 * D * rot_cols_per_cta((int)D, 4) * 4 <= 227.0 * 1024;
+  // the parity-split form (FP32): per column two Ry of sum_n (n+1)^2 + n^2,
+  // the shift's re and im blocks (none of order 0 im), two Rz of 4 per
+  // coefficient of order m > 0 (1 for m = 0) multiply-adds
+  const bool split = mixed && split_rot();
+  auto s2 = [](double x) { return x * (x + 1) * (2 * x + 1) / 6.0; };
   auto add = [&](const TransSched& S, int k, double cols) {
     for (const TransSeg& g : S.segs) {
-      if (fact) {
-        const double q = ops_->descs[g.group].p + 1;
+      const double q = ops_->descs[g.group].p + 1;
+      if (fact && split && q <= 32) {
+        const double ma = 2.0 * (s2(q) + s2(q - 1)) + 2.0 * s2(q) - q * q + 2.0 * (4.0 * (q * (q + 1) / 2 - q) + q);
+        f[k] += 2.0 * ma * g.npair * cols;
+      } else if (fact) {
         f[k] += 2.0 * 3.0 * (4.0 * q * (q + 1) * (2 * q + 1) / 6.0) * g.npair * cols;
       } else {
         const double dim = ops_->dims[g.group];

@@ -41,6 +41,11 @@ struct OpPool {
   bool rot_tc_ready = false;
   DevBuf<RotTcOp> rot_tc_ops;
   DevBuf<float> rot_tc_tiles;
+  // the FP32 factored operators in the parity-split form (rotations as Rz
+  // then Ry, re / im blocks); made on the first FP32 pass that uses them
+  bool rots_ready = false;
+  DevBuf<RotSOp> rots_ops;
+  DevBuf<float> rots_f;
   DevBuf<long long> off;
   DevBuf<int> dim;
   int m2l_group[343];
@@ -373,6 +378,9 @@ class Plan {
   void cut_tasks(TransSched& S, int C, const std::vector<int>* dims = nullptr);
   void cut_rot_tasks(TransSched& S, int C, int W);
   void ensure_factored(bool tc = false);
+  void ensure_split();
+  // whether the FP32 translations run in the parity-split form
+  bool split_rot() const;
   // the FP32 translations of a schedule on the tensor cores (rot_tc.cu)
   bool rot_tc_usable() const;
   void cut_tc_tasks(TransSched& S, int C, bool one_launch);

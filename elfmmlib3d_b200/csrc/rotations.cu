@@ -13,6 +13,7 @@
 #include <cmath>
 #include <random>
 #include <thread>
+#include <type_traits>
 #include <cstdlib>
 #include <cstring>
 #include "common.cuh"
@@ -362,6 +363,259 @@ double check_factored_ops(const std::vector<int>& kinds, const std::vector<int>&
     worst = std::max(worst, std::sqrt(num / std::max(den, 1e-300)));
   }
   return worst;
+}
+
+// ------------------------------------------------------- parity-split form
+// The frame change of a translation is taken as Q = Ry(-theta) Rz(-phi)
+// (theta, phi the polar angles of the offset), so the coefficient map is
+// M(Q) = M(Ry) M(Rz).  M(Rz) mixes only the (re, im) pair of each (n, m): a
+// 2 x 2 matrix per order m, the same for every degree.  A rotation about y
+// commutes with the reflection y -> -y, so M(Ry) never mixes the re (cos m
+// phi) and im (sin m phi) parts: per degree n an (n+1) x (n+1) re block and
+// an n x n im block.  The shift along z commutes with both, so it is an
+// re block and an im block per order m as well.  Per pair and column this is
+// about 2 p^3 multiply-adds against the 4 p^3 of the full (2n+2)^2 and
+// (2(p-m+1))^2 blocks.
+
+namespace {
+
+// The parity-split factors of one group, factorial basis, double.
+// Block b of r rows is stored row-major as re[r*r], then im[r*r] (im row and
+// column 0 zero in the rotations: m = 0 has no sin part; the shift's im block
+// of order 0 zero).
+struct SplitHost {
+  int p = 0;
+  std::vector<double> rz[2];  // [fw, bk]: 4 per order m (re<-re, re<-im, im<-re, im<-im)
+  std::vector<std::vector<double>> ry[2];  // [fw, bk][n]: 2 (n+1)^2
+  std::vector<std::vector<double>> z;      // [m]: 2 (p-m+1)^2
+  double cross = 0;  // largest coupling dropped by the split (relative)
+};
+
+void rot_y(double a, double Q[9]) {  // frame change x' = Ry(a) x
+  const double c = std::cos(a), s = std::sin(a);
+  const double q[9] = {c, 0, s, 0, 1, 0, -s, 0, c};
+  for (int i = 0; i < 9; i++) Q[i] = q[i];
+}
+void rot_z(double a, double Q[9]) {  // frame change x' = Rz(a) x
+  const double c = std::cos(a), s = std::sin(a);
+  const double q[9] = {c, -s, 0, s, c, 0, 0, 0, 1};
+  for (int i = 0; i < 9; i++) Q[i] = q[i];
+}
+
+// degree blocks of a fitted rotation (slot order 2m + part) -> re / im
+// blocks; the largest cross term relative to the block's largest entry
+double split_rotation(const std::vector<double>& full, int p, std::vector<std::vector<double>>& out) {
+  double cross = 0;
+  out.assign(p + 1, {});
+  for (int n = 0; n <= p; n++) {
+    const int bb = 2 * n + 2, r = n + 1;
+    const double* B = &full[rot_block_off(n)];
+    std::vector<double>& o = out[n];
+    o.assign(2 * (size_t)r * r, 0.0);
+    double big = 0, cr = 0;
+    for (int i = 0; i < r; i++)
+      for (int k = 0; k < r; k++) {
+        o[(size_t)i * r + k] = B[(size_t)(2 * i) * bb + 2 * k];
+        if (i > 0 && k > 0) o[(size_t)r * r + (size_t)i * r + k] = B[(size_t)(2 * i + 1) * bb + 2 * k + 1];
+        big = std::max(big, std::fabs(B[(size_t)(2 * i) * bb + 2 * k]));
+        cr = std::max({cr, std::fabs(B[(size_t)(2 * i) * bb + 2 * k + 1]), std::fabs(B[(size_t)(2 * i + 1) * bb + 2 * k])});
+      }
+    cross = std::max(cross, cr / std::max(big, 1e-300));
+  }
+  return cross;
+}
+
+// the 2 x 2 per order of a fitted rotation about z (taken from degree p; the
+// other degrees and every off-order entry checked)
+double split_rz(const std::vector<double>& full, int p, std::vector<double>& out) {
+  out.assign(4 * (size_t)(p + 1), 0.0);
+  double dev = 0;
+  for (int n = 0; n <= p; n++) {
+    const int bb = 2 * n + 2;
+    const double* B = &full[rot_block_off(n)];
+    for (int i = 0; i < bb; i++)
+      for (int k = 0; k < bb; k++) {
+        const double v = B[(size_t)i * bb + k];
+        if ((i >> 1) != (k >> 1)) {
+          dev = std::max(dev, std::fabs(v));
+          continue;
+        }
+        const int m = i >> 1, q = 2 * (i & 1) + (k & 1);
+        if (m == 0 && (i == 1 || k == 1)) continue;  // inactive slot
+        if (n == p)
+          out[4 * m + q] = v;
+      }
+  }
+  for (int n = 0; n < p; n++) {
+    const int bb = 2 * n + 2;
+    const double* B = &full[rot_block_off(n)];
+    for (int m = 0; m <= n; m++)
+      for (int q = 0; q < 4; q++) {
+        if (m == 0 && q != 0) continue;
+        const int i = 2 * m + (q >> 1), k = 2 * m + (q & 1);
+        dev = std::max(dev, std::fabs(B[(size_t)i * bb + k] - out[4 * m + q]));
+      }
+  }
+  return dev;
+}
+
+void build_split_host(int kind, int p, const double d[3], const Fitter& F, SplitHost& S) {
+  S.p = p;
+  const double rho = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+  const double th = std::acos(std::max(-1.0, std::min(1.0, d[2] / rho)));
+  const double ph = (d[0] == 0.0 && d[1] == 0.0) ? 0.0 : std::atan2(d[1], d[0]);
+  double Qz[9], Qy[9], Qzt[9], Qyt[9];
+  rot_z(-ph, Qz);
+  rot_y(-th, Qy);
+  rot_z(ph, Qzt);
+  rot_y(th, Qyt);
+  const int bin = kind == 2 ? 1 : 0, bout = kind == 1 ? 0 : 1;
+  std::vector<double> full(rot_size(p));
+  double cross = 0;
+  F.rotation(bin, p, Qz, full.data());
+  cross = std::max(cross, split_rz(full, p, S.rz[0]));
+  F.rotation(bin, p, Qy, full.data());
+  cross = std::max(cross, split_rotation(full, p, S.ry[0]));
+  F.rotation(bout, p, Qyt, full.data());
+  cross = std::max(cross, split_rotation(full, p, S.ry[1]));
+  F.rotation(bout, p, Qzt, full.data());
+  cross = std::max(cross, split_rz(full, p, S.rz[1]));
+  std::vector<double> zf(z_size(p));
+  zshift(kind, p, rho, zf.data());
+  S.z.assign(p + 1, {});
+  for (int m = 0; m <= p; m++) {
+    const int r = p - m + 1, bz = 2 * r;
+    const double* B = &zf[z_block_off(p, m)];
+    std::vector<double>& o = S.z[m];
+    o.assign(2 * (size_t)r * r, 0.0);
+    double big = 0, cr = 0;
+    for (int i = 0; i < r; i++)
+      for (int k = 0; k < r; k++) {
+        o[(size_t)i * r + k] = B[(size_t)(2 * i) * bz + 2 * k];
+        if (m > 0) o[(size_t)r * r + (size_t)i * r + k] = B[(size_t)(2 * i + 1) * bz + 2 * k + 1];
+        big = std::max(big, std::fabs(B[(size_t)(2 * i) * bz + 2 * k]));
+        cr = std::max({cr, std::fabs(B[(size_t)(2 * i) * bz + 2 * k + 1]), std::fabs(B[(size_t)(2 * i + 1) * bz + 2 * k])});
+      }
+    cross = std::max(cross, cr / std::max(big, 1e-300));
+  }
+  S.cross = cross;
+}
+
+// y = Bk Z Fw v of the split factors (v, y: 2 ncoef(p) in storage order)
+void apply_split_host(const SplitHost& S, const std::vector<double>& v, std::vector<double>& y) {
+  const int p = S.p, dim = 2 * ncoef(p);
+  std::vector<double> a(v), b(dim, 0.0);
+  auto rz = [&](const std::vector<double>& R, std::vector<double>& x) {
+    for (int n = 0; n <= p; n++)
+      for (int m = 0; m <= n; m++) {
+        const int c = 2 * cidx(n, m);
+        const double re = x[c], im = x[c + 1];
+        x[c] = R[4 * m] * re + R[4 * m + 1] * im;
+        x[c + 1] = R[4 * m + 2] * re + R[4 * m + 3] * im;
+      }
+  };
+  auto ry = [&](const std::vector<std::vector<double>>& Bl, std::vector<double>& x) {
+    std::vector<double> t(x);
+    for (int n = 0; n <= p; n++) {
+      const int r = n + 1;
+      for (int i = 0; i < r; i++) {
+        double sr = 0, si = 0;
+        for (int k = 0; k < r; k++) {
+          sr += Bl[n][(size_t)i * r + k] * t[2 * cidx(n, k)];
+          si += Bl[n][(size_t)r * r + (size_t)i * r + k] * t[2 * cidx(n, k) + 1];
+        }
+        x[2 * cidx(n, i)] = sr;
+        x[2 * cidx(n, i) + 1] = si;
+      }
+    }
+  };
+  rz(S.rz[0], a);
+  ry(S.ry[0], a);
+  for (int m = 0; m <= p; m++) {
+    const int r = p - m + 1;
+    for (int i = 0; i < r; i++) {
+      double sr = 0, si = 0;
+      for (int k = 0; k < r; k++) {
+        sr += S.z[m][(size_t)i * r + k] * a[2 * cidx(m + k, m)];
+        si += S.z[m][(size_t)r * r + (size_t)i * r + k] * a[2 * cidx(m + k, m) + 1];
+      }
+      b[2 * cidx(m + i, m)] = sr;
+      b[2 * cidx(m + i, m) + 1] = si;
+    }
+  }
+  ry(S.ry[1], b);
+  rz(S.rz[1], b);
+  y = b;
+}
+
+}  // namespace
+
+// floats of the split blocks of r = 1..R rows (4 r ceil(r/2) each)
+EFMM_HD constexpr long long rots_blocks(int R) {
+  long long s = 0;
+  for (int r = 1; r <= R; r++) s += 4LL * r * ((r + 1) / 2);
+  return s;
+}
+long long rots_group_size(int p) { return 8LL * (p + 1) + 3 * rots_blocks(p + 1); }
+
+void build_split_ops(const std::vector<int>& kinds, const std::vector<int>& orders,
+                     const std::vector<double>& offsets, const std::vector<double>& w,
+                     std::vector<RotSOp>& ops, std::vector<float>& pool) {
+  const int ng = (int)kinds.size();
+  int pmax = 0;
+  for (int q : orders) pmax = std::max(pmax, q);
+  Fitter F;
+  F.init(pmax);
+  ops.resize(ng);
+  long long off = 0;
+  for (int g = 0; g < ng; g++) {
+    ops[g].p = orders[g];
+    ops[g].pad = 0;
+    ops[g].base = off;
+    off += rots_group_size(orders[g]);
+  }
+  pool.assign((size_t)off, 0.0f);
+  parallel_for(ng, [&](int g) {
+    const int kind = kinds[g], p = orders[g];
+    SplitHost S;
+    build_split_host(kind, p, &offsets[3 * g], F, S);
+    // normalised basis: multipole rows x w, local rows / w (columns inverse)
+    auto rs = [&](bool local, int n, int m) {
+      const double v = w[2 * cidx(n, m)];
+      return local ? 1.0 / v : v;
+    };
+    const bool fw_local = kind == 2, z_in_local = kind == 2, z_out_local = kind != 1, bk_local = kind != 1;
+    float* o = &pool[ops[g].base];
+    for (int s = 0; s < 2; s++) {
+      float* rz = s == 0 ? o : o + 4 * (p + 1) + 3 * rots_blocks(p + 1);
+      for (int q = 0; q < 4 * (p + 1); q++) rz[q] = (float)S.rz[s][q];
+    }
+    // a block of r rows: column k holds ceil(r/2) float4 (re[2j][k],
+    // re[2j+1][k], im[2j][k], im[2j+1][k])
+    auto pack = [&](float* dst, const std::vector<double>& B, int r, auto scale) {
+      const int h = (r + 1) / 2;
+      for (int k = 0; k < r; k++)
+        for (int j = 0; j < h; j++)
+          for (int e = 0; e < 4; e++) {
+            const int i = 2 * j + (e & 1), part = e >> 1;
+            double v = 0;
+            if (i < r) v = B[(size_t)part * r * r + (size_t)i * r + k] * scale(i, k);
+            dst[((size_t)k * h + j) * 4 + e] = (float)v;
+          }
+    };
+    float* ryf = o + 4 * (p + 1);
+    float* zb = ryf + rots_blocks(p + 1);
+    float* ryb = zb + rots_blocks(p + 1);
+    for (int n = 0; n <= p; n++) {
+      pack(ryf + rots_blocks(n), S.ry[0][n], n + 1,
+           [&](int i, int k) { return rs(fw_local, n, i) / rs(fw_local, n, k); });
+      pack(ryb + rots_blocks(n), S.ry[1][n], n + 1,
+           [&](int i, int k) { return rs(bk_local, n, i) / rs(bk_local, n, k); });
+    }
+    for (int m = 0; m <= p; m++)
+      pack(zb + rots_blocks(p + 1) - rots_blocks(p + 1 - m), S.z[m], p - m + 1,
+           [&](int i, int k) { return rs(z_out_local, m + i, m) / rs(z_in_local, m + k, m); });
+  });
 }
 
 // ------------------------------------------------------------------ kernel
@@ -754,6 +1008,214 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
   }
 }
 
+// FP32 translations in the parity-split form (build_split_ops): five factors
+// per column, Rz forward (applied while the sources are staged), the re / im
+// blocks of Ry forward, of the shift along z and of Ry back (one warp per
+// block, in place in X[row][16]), Rz back (applied to the last blocks'
+// results in registers).  In a block of r rows, lane (rp, ch) owns output
+// rows 2 rp, 2 rp + 1 of both parts for NCT / CG columns; per input row k it
+// reads one float4 of operator (re and im of its two rows) and the re and im
+// input rows of its columns as broadcasts: CG = 2 (16 row pairs x 8
+// columns) for r > 16, CG = 4 (8 row pairs x 4 columns) below.  Operator
+// columns are copied per warp by cp.async into two chunk buffers, one chunk
+// ahead.  For orders p <= 31; two CTAs of 12 warps per SM up to p = 30.
+constexpr int RS_THREADS = 384, RS_NCT = 16, RS_NW = RS_THREADS / 32, RS_CH = 8, RS_PMAX = 31;
+struct RsBlocks {
+  int s[RS_PMAX + 3];
+};
+constexpr RsBlocks make_rs_blocks() {
+  RsBlocks b{};
+  for (int R = 0; R <= RS_PMAX + 2; R++) b.s[R] = (int)rots_blocks(R);
+  return b;
+}
+__constant__ RsBlocks c_rs_blocks = make_rs_blocks();
+__host__ __device__ inline size_t rs_cbase_off(int dim) { return sizeof(float) * (size_t)dim * RS_NCT; }
+__host__ __device__ inline size_t rs_wbuf_off(int dim) { return rs_cbase_off(dim) + 8 * RS_NCT; }
+// per warp two chunk buffers of RS_CH operator columns of <= 16 float4
+__host__ __device__ inline size_t rs_smem(int dim) {
+  return rs_wbuf_off(dim) + (size_t)RS_NW * 2 * RS_CH * 16 * sizeof(float4);
+}
+
+__global__ void __launch_bounds__(RS_THREADS, 2)
+k_translate_rot_s(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
+                  const RotSOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
+                  const float* __restrict__ src, float* __restrict__ dst) {
+  constexpr int NCT = RS_NCT;
+  extern __shared__ __align__(16) unsigned char rs_smem_[];
+  const TransTask t = tasks[blockIdx.x];
+  const RotSOp op = ops[t.group];
+  const int p = op.p, nc = (p + 1) * (p + 2) / 2, dim = 2 * nc;
+  const int nblk = c_rs_blocks.s[p + 1];
+  const float* g0 = pool + op.base;
+  const float4* rzf = reinterpret_cast<const float4*>(g0);
+  const float* ryf = g0 + 4 * (p + 1);
+  const float* zb = ryf + nblk;
+  const float* ryb = zb + nblk;
+  const float4* rzb = reinterpret_cast<const float4*>(ryb + nblk);
+  float* X = reinterpret_cast<float*>(rs_smem_);                                   // [dim][NCT]
+  long long* cbase = reinterpret_cast<long long*>(rs_smem_ + rs_cbase_off(dim));  // [NCT]: source columns
+  const unsigned char* owner = c_rotw_owners.o[p];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid < NCT) {
+    const int col = t.col0 + tid;
+    long long b = -1;
+    if (col < t.ncols) {
+      const TransPair pr = pairs[t.pair0 + col / C];
+      b = ((long long)pr.src * C + col % C) * D;
+    }
+    cbase[tid] = b;
+  }
+  __syncthreads();
+  // stage the sources with Rz forward: thread (coefficient, 4 columns)
+  for (int q = tid; q < nc * 4; q += RS_THREADS) {
+    const int c = q % nc, cg = q / nc;
+    int n, m;
+    coef_nm(c, n, m);
+    const float4 R = __ldg(rzf + m);
+    float re[4], im[4];
+#pragma unroll
+    for (int g = 0; g < 4; g++) {
+      const long long b = cbase[cg * 4 + g];
+      const float2 v = b >= 0 ? __ldg(reinterpret_cast<const float2*>(src + b + 2 * c)) : make_float2(0.f, 0.f);
+      re[g] = R.x * v.x + R.y * v.y;
+      im[g] = R.z * v.x + R.w * v.y;
+    }
+    *reinterpret_cast<float4*>(X + (size_t)(2 * c) * NCT + cg * 4) = make_float4(re[0], re[1], re[2], re[3]);
+    *reinterpret_cast<float4*>(X + (size_t)(2 * c + 1) * NCT + cg * 4) = make_float4(im[0], im[1], im[2], im[3]);
+  }
+  __syncthreads();
+  float4* wbuf = reinterpret_cast<float4*>(rs_smem_ + rs_wbuf_off(dim)) + (size_t)warp * 2 * RS_CH * 16;
+  // operator columns [chunk RS_CH, +RS_CH) of a block (h float4 per column)
+  auto fetch = [&](const float* blk, int h, int ncol, int chunk) {
+    const int c0 = chunk * RS_CH, nbytes = 16 * h * min(RS_CH, ncol - c0);
+    const char* g = reinterpret_cast<const char*>(blk + (size_t)c0 * 4 * h);
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(wbuf + (chunk & 1) * RS_CH * 16));
+    for (int b = 16 * lane; b < nbytes; b += 16 * 32)
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + b), "l"(g + b) : "memory");
+    asm volatile("cp.async.commit_group;" ::: "memory");
+  };
+  // one block of r rows; xrow(k): X row of the re part of row k (im: + 1);
+  // the results go back to the same rows, through rz (4 per order, indexed
+  // by the row) when given
+  auto block = [&](auto cgtag, const float* blk, int r, auto xrow, const float4* rz) {
+    constexpr int CG = decltype(cgtag)::value, RP = 32 / CG, COLS = NCT / CG, NV = COLS / 2;
+    const int h = (r + 1) / 2, rp = lane % RP, ch = lane / RP;
+    const bool act = rp < h;
+    float2 aR0[NV], aR1[NV], aI0[NV], aI1[NV];
+#pragma unroll
+    for (int v = 0; v < NV; v++) aR0[v] = aR1[v] = aI0[v] = aI1[v] = make_float2(0.f, 0.f);
+    const int nch = (r + RS_CH - 1) / RS_CH;
+    fetch(blk, h, r, 0);
+    for (int chk = 0; chk < nch; chk++) {
+      if (chk + 1 < nch)
+        fetch(blk, h, r, chk + 1);
+      else
+        asm volatile("cp.async.commit_group;" ::: "memory");
+      asm volatile("cp.async.wait_group 1;" ::: "memory");
+      __syncwarp();
+      const float4* wb = wbuf + (chk & 1) * RS_CH * 16;
+      const int cend = min(RS_CH, r - chk * RS_CH);
+      for (int u = 0; u < cend; u++) {
+        const float4 o = act ? wb[u * h + rp] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float* xre = X + (size_t)xrow(chk * RS_CH + u) * NCT + ch * COLS;
+        float xr[COLS], xi[COLS];
+#pragma unroll
+        for (int v = 0; v < COLS / 4; v++) {
+          const float4 a = reinterpret_cast<const float4*>(xre)[v];
+          const float4 b = reinterpret_cast<const float4*>(xre + NCT)[v];
+          xr[4 * v] = a.x; xr[4 * v + 1] = a.y; xr[4 * v + 2] = a.z; xr[4 * v + 3] = a.w;
+          xi[4 * v] = b.x; xi[4 * v + 1] = b.y; xi[4 * v + 2] = b.z; xi[4 * v + 3] = b.w;
+        }
+        const float2 w0 = make_float2(o.x, o.x), w1 = make_float2(o.y, o.y);
+        const float2 w2 = make_float2(o.z, o.z), w3 = make_float2(o.w, o.w);
+#pragma unroll
+        for (int v = 0; v < NV; v++) {
+          const float2 x2 = make_float2(xr[2 * v], xr[2 * v + 1]), y2 = make_float2(xi[2 * v], xi[2 * v + 1]);
+          aR0[v] = __ffma2_rn(w0, x2, aR0[v]);
+          aR1[v] = __ffma2_rn(w1, x2, aR1[v]);
+          aI0[v] = __ffma2_rn(w2, y2, aI0[v]);
+          aI1[v] = __ffma2_rn(w3, y2, aI1[v]);
+        }
+      }
+      __syncwarp();  // buffer (chk & 1) is refilled by the fetch of chunk chk + 2
+    }
+    auto put = [&](int i, const float2* aR, const float2* aI) {
+      float* xo = X + (size_t)xrow(i) * NCT + ch * COLS;
+      float ore[COLS], oim[COLS];
+#pragma unroll
+      for (int v = 0; v < NV; v++) {
+        ore[2 * v] = aR[v].x; ore[2 * v + 1] = aR[v].y;
+        oim[2 * v] = aI[v].x; oim[2 * v + 1] = aI[v].y;
+      }
+      if (rz) {
+        const float4 R = __ldg(rz + i);
+#pragma unroll
+        for (int e = 0; e < COLS; e++) {
+          const float a = ore[e], b = oim[e];
+          ore[e] = R.x * a + R.y * b;
+          oim[e] = R.z * a + R.w * b;
+        }
+      }
+#pragma unroll
+      for (int v = 0; v < COLS / 4; v++) {
+        reinterpret_cast<float4*>(xo)[v] = make_float4(ore[4 * v], ore[4 * v + 1], ore[4 * v + 2], ore[4 * v + 3]);
+        reinterpret_cast<float4*>(xo + NCT)[v] = make_float4(oim[4 * v], oim[4 * v + 1], oim[4 * v + 2], oim[4 * v + 3]);
+      }
+    };
+    if (act) {
+      put(2 * rp, aR0, aI0);
+      if (2 * rp + 1 < r) put(2 * rp + 1, aR1, aI1);
+    }
+    __syncwarp();
+  };
+  auto run_block = [&](const float* blk, int r, auto xrow, const float4* rz) {
+    if (r > 16)
+      block(std::integral_constant<int, 2>{}, blk, r, xrow, rz);
+    else
+      block(std::integral_constant<int, 4>{}, blk, r, xrow, rz);
+  };
+  auto rotate = [&](const float* base, const float4* rz) {
+    for (int n = 0; n <= p; n++) {
+      if (owner[n] != warp) continue;
+      const int r0 = n * (n + 1);
+      run_block(base + c_rs_blocks.s[n], n + 1, [&](int k) { return r0 + 2 * k; }, rz);
+    }
+  };
+  rotate(ryf, nullptr);
+  __syncthreads();
+  // shift along z: order block m (rows (n, m), n = m..p), owned like degree block p - m
+  for (int m = 0; m <= p; m++) {
+    if (owner[p - m] != warp) continue;
+    run_block(zb + nblk - c_rs_blocks.s[p + 1 - m], p - m + 1,
+              [&](int k) { const int n = m + k; return n * (n + 1) + 2 * m; }, nullptr);
+  }
+  __syncthreads();
+  rotate(ryb, rzb);
+  __syncthreads();
+  for (int j = 0; j < NCT; j++) {
+    const int col = t.col0 + j;
+    if (col >= t.ncols) break;
+    const TransPair pr = pairs[t.pair0 + col / C];
+    float* dp = dst + ((size_t)pr.dst * C + col % C) * D;
+    const float al = (float)pr.alpha;
+    for (int r = tid; r < dim; r += RS_THREADS) atomicAdd(dp + r, al * X[(size_t)r * NCT + j]);
+  }
+}
+
+bool rot_split_ok(int maxdim) { return maxdim <= (RS_PMAX + 1) * (RS_PMAX + 2); }
+
+void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
+                                const RotSOp* ops, const float* pool, int D, int C, int maxdim, const float* src,
+                                float* dst) {
+  if (ntask <= 0) return;
+  if (!rot_split_ok(maxdim)) throw CudaError{(int)cudaErrorInvalidValue};
+  const size_t smem = rs_smem(maxdim);
+  EFMM_CUDA_TRY(smem_raise(k_translate_rot_s, (int)smem));
+  k_translate_rot_s<<<ntask, RS_THREADS, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
 // The warp-block kernel for launches of orders pmin..31 (smaller orders
 // have fewer blocks than warps: the coefficient-tile kernel serves them).
 bool rot_warp_blocks_ok(int maxdim) {
@@ -832,4 +1294,280 @@ extern "C" int efmm_factored_selfcheck(int p, double eps, int stride, double* wo
   build_factored_ops(p, kinds, orders, offs, ops, pool);
   *worst = check_factored_ops(kinds, orders, offs, ops, pool, stride);
   return (int)kinds.size();
+}
+
+namespace efmm {
+namespace {
+// The packed FP32 pool of one group applied on the host exactly as the
+// device kernel reads it (normalised basis): layout check without a device.
+void apply_split_packed(const float* g, int p, const std::vector<double>& v, std::vector<double>& y) {
+  const int nc = ncoef(p), dim = 2 * nc;
+  const long long nb = rots_blocks(p + 1);
+  const float* rzf = g;
+  const float* ryf = g + 4 * (p + 1);
+  const float* zb = ryf + nb;
+  const float* ryb = zb + nb;
+  const float* rzb = ryb + nb;
+  std::vector<double> x(v);
+  auto rz = [&](const float* R) {
+    for (int n = 0; n <= p; n++)
+      for (int m = 0; m <= n; m++) {
+        const int c = 2 * cidx(n, m);
+        const double re = x[c], im = x[c + 1];
+        x[c] = R[4 * m] * re + R[4 * m + 1] * im;
+        x[c + 1] = R[4 * m + 2] * re + R[4 * m + 3] * im;
+      }
+  };
+  auto blk = [&](const float* B, int r, auto row) {
+    const int h = (r + 1) / 2;
+    std::vector<double> o(2 * r, 0.0);
+    for (int k = 0; k < r; k++)
+      for (int i = 0; i < r; i++) {
+        const float* q = B + ((size_t)k * h + i / 2) * 4;
+        o[2 * i] += q[i & 1] * x[row(k)];
+        o[2 * i + 1] += q[2 + (i & 1)] * x[row(k) + 1];
+      }
+    for (int i = 0; i < r; i++) {
+      x[row(i)] = o[2 * i];
+      x[row(i) + 1] = o[2 * i + 1];
+    }
+  };
+  rz(rzf);
+  for (int n = 0; n <= p; n++) blk(ryf + rots_blocks(n), n + 1, [&](int k) { return n * (n + 1) + 2 * k; });
+  for (int m = 0; m <= p; m++)
+    blk(zb + nb - rots_blocks(p + 1 - m), p - m + 1, [&](int k) { return (m + k) * (m + k + 1) + 2 * m; });
+  for (int n = 0; n <= p; n++) blk(ryb + rots_blocks(n), n + 1, [&](int k) { return n * (n + 1) + 2 * k; });
+  rz(rzb);
+  y.assign(x.begin(), x.begin() + dim);
+}
+}  // namespace
+}  // namespace efmm
+
+// CPU self-check of the parity-split factors (no device needed), over the
+// same groups as efmm_factored_selfcheck: worst[0] the split factors in
+// double against the dense operators, worst[1] the packed FP32 device pool
+// applied as the kernel reads it, worst[2] the largest coupling the split
+// drops (re <-> im terms of Ry and the shift, off-order terms of Rz).
+extern "C" int efmm_split_selfcheck(int p, double eps, int stride, double* worst) {
+  using namespace efmm;
+  std::vector<int> kinds, orders;
+  std::vector<double> offs;
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = -3; k <= 3; k++) {
+        if (std::max(std::abs(i), std::max(std::abs(j), std::abs(k))) < 2) continue;
+        kinds.push_back(0);
+        orders.push_back(std::min(p, eps > 0 ? m2l_order(eps, i, j, k) : p));
+        offs.insert(offs.end(), {(double)i, (double)j, (double)k});
+      }
+  for (int kind = 1; kind <= 2; kind++)
+    for (int dg = 0; dg < 8; dg++) {
+      kinds.push_back(kind);
+      orders.push_back(p);
+      offs.insert(offs.end(), {(dg & 1) ? 0.25 : -0.25, ((dg >> 1) & 1) ? 0.25 : -0.25,
+                               ((dg >> 2) & 1) ? 0.25 : -0.25});
+    }
+  std::vector<double> w(2 * (size_t)ncoef(p));
+  for (int n = 0; n <= p; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] = std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<RotSOp> sops;
+  std::vector<float> spool;
+  build_split_ops(kinds, orders, offs, w, sops, spool);
+  Fitter F;
+  F.init(p);
+  worst[0] = worst[1] = worst[2] = 0;
+  std::mt19937_64 rng(11);
+  std::normal_distribution<double> N01;
+  for (int g = 0; g < (int)kinds.size(); g += std::max(stride, 1)) {
+    const int kind = kinds[g], pg = orders[g], nc = ncoef(pg), dim = 2 * nc;
+    const double* d = &offs[3 * g];
+    SplitHost S;
+    build_split_host(kind, pg, d, F, S);
+    worst[2] = std::max(worst[2], S.cross);
+    std::vector<cplx> tab(ncoef(2 * pg + 1));
+    if (kind == 0)
+      irregular_harmonics(2 * pg, d[0], d[1], d[2], tab.data());
+    else
+      regular_harmonics(pg, d[0], d[1], d[2], tab.data());
+    const bool in_local = kind == 2, out_local = kind != 1;
+    std::vector<double> v(dim), a(dim, 0.0), vn(dim), y, yn;
+    for (int q = 0; q < dim; q++) v[q] = N01(rng) * (in_local ? w[q] : 1.0 / w[q]);
+    for (int n = 0; n <= pg; n++) v[2 * cidx(n, 0) + 1] = 0.0;
+    for (int r = 0; r < nc; r++)
+      for (int c = 0; c < nc; c++) {
+        double rr, ri, ir, ii;
+        op_entry(kind, tab.data(), r, c, &rr, &ri, &ir, &ii);
+        a[2 * r] += rr * v[2 * c] + ri * v[2 * c + 1];
+        a[2 * r + 1] += ir * v[2 * c] + ii * v[2 * c + 1];
+      }
+    apply_split_host(S, v, y);
+    for (int q = 0; q < dim; q++) vn[q] = v[q] * (in_local ? 1.0 / w[q] : w[q]);
+    apply_split_packed(&spool[sops[g].base], pg, vn, yn);
+    double num0 = 0, num1 = 0, den = 0;
+    for (int n = 0; n <= pg; n++)
+      for (int m = 0; m <= n; m++)
+        for (int part = 0; part < 2; part++) {
+          if (m == 0 && part == 1) continue;
+          const int q = 2 * cidx(n, m) + part;
+          const double sc = out_local ? 1.0 / w[q] : w[q];
+          const double y1 = yn[q] / sc;
+          num0 += (a[q] - y[q]) * (a[q] - y[q]) * sc * sc;
+          num1 += (a[q] - y1) * (a[q] - y1) * sc * sc;
+          den += a[q] * a[q] * sc * sc;
+        }
+    worst[0] = std::max(worst[0], std::sqrt(num0 / std::max(den, 1e-300)));
+    worst[1] = std::max(worst[1], std::sqrt(num1 / std::max(den, 1e-300)));
+  }
+  return (int)kinds.size();
+}
+
+// Device run of the FP32 translation kernels on four groups of order p (an
+// M2L offset, one along -z, an M2M and an L2L shift), npair box pairs each
+// with C columns per box (random normalised sources, pair factors alpha, one
+// destination box per group), in one launch.  engine 0: the parity-split
+// kernel (k_translate_rot_s); 1: the full-block kernels (k_translate_rot_w /
+// k_translate_rot, as launch_translate_rot<float> picks them).  reps > 0
+// then times reps more launches (mean ms in *ms).  With rel: the relative l2
+// error of the destinations of the first launch against the split factors
+// of the same FP32 pool applied in FP64 on the host.
+static int rot_split_device_run(int p, int C, int npair, unsigned seed, int engine, int reps, double* rel,
+                                double* ms) {
+  using namespace efmm;
+  if (p < 1 || p > 31 || C < 1 || npair < 1 || (long long)C * npair > (1 << 20) || engine < 0 || engine > 1)
+    return 16;
+  const int NG = 4;
+  std::vector<int> kinds = {0, 0, 1, 2}, orders(NG, p);
+  std::vector<double> offs = {2, -1, 3, 0, 0, -2, 0.25, 0.25, -0.25, -0.25, 0.25, 0.25};
+  std::vector<double> w(2 * (size_t)ncoef(p));
+  for (int n = 0; n <= p; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] = std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<RotSOp> sops;
+  std::vector<float> spool;
+  build_split_ops(kinds, orders, offs, w, sops, spool);
+  std::vector<RotOp> rops;
+  std::vector<double> pool;
+  std::vector<float> poolf;
+  if (engine == 1) {
+    build_factored_ops(p, kinds, orders, offs, rops, pool);
+    normalise_factored_ops(kinds, rops, pool, w, poolf);
+    std::vector<double> tmp(poolf.begin(), poolf.end());
+    column_major_factored(rops, tmp);
+    for (size_t i = 0; i < tmp.size(); i++) poolf[i] = (float)tmp[i];
+  }
+  const int D = 2 * ncoef(p), dim = D;
+  const int nsrc = NG * npair, nbox = nsrc + NG;
+  std::mt19937_64 rng(seed);
+  std::uniform_real_distribution<float> U(-1.f, 1.f);
+  std::vector<float> hsrc((size_t)nbox * C * D, 0.f), hdst((size_t)nbox * C * D, 0.f);
+  for (int b = 0; b < nsrc; b++)
+    for (int c = 0; c < C; c++)
+      for (int q = 0; q < D; q++) {
+        const bool m0im = (q & 1) && q / 2 == cidx((int)((std::sqrt(8.0 * (q / 2) + 1) - 1) / 2), 0);
+        hsrc[((size_t)b * C + c) * D + q] = m0im ? 0.f : U(rng);
+      }
+  std::vector<TransPair> hp;
+  std::vector<TransTask> tasks;
+  for (int g = 0; g < NG; g++) {
+    for (int k = 0; k < npair; k++) hp.push_back({g * npair + k, nsrc + g, 0.5 + 0.25 * k});
+    const int ncols = npair * C;
+    for (int c0 = 0; c0 < ncols; c0 += RS_NCT) tasks.push_back({g, 0, g * npair, ncols, c0});
+  }
+  float *dsrc = nullptr, *ddst = nullptr, *dpool = nullptr;
+  TransPair* dp = nullptr;
+  TransTask* dtask = nullptr;
+  RotSOp* dsops = nullptr;
+  RotOp* drops = nullptr;
+  auto release = [&]() {
+    cudaFree(dsrc); cudaFree(ddst); cudaFree(dpool); cudaFree(dp); cudaFree(dtask); cudaFree(dsops); cudaFree(drops);
+  };
+  const size_t pbytes = 4 * (engine == 0 ? spool.size() : poolf.size());
+  if (cudaMalloc(&dsrc, hsrc.size() * 4) || cudaMalloc(&ddst, hdst.size() * 4) || cudaMalloc(&dpool, pbytes) ||
+      cudaMalloc(&dp, hp.size() * sizeof(TransPair)) || cudaMalloc(&dtask, tasks.size() * sizeof(TransTask)) ||
+      cudaMalloc(&dsops, sops.size() * sizeof(RotSOp)) || cudaMalloc(&drops, NG * sizeof(RotOp))) {
+    release();
+    return 256;
+  }
+  cudaMemcpy(dsrc, hsrc.data(), hsrc.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(ddst, hdst.data(), hdst.size() * 4, cudaMemcpyHostToDevice);
+  cudaMemcpy(dpool, engine == 0 ? spool.data() : poolf.data(), pbytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(dp, hp.data(), hp.size() * sizeof(TransPair), cudaMemcpyHostToDevice);
+  cudaMemcpy(dtask, tasks.data(), tasks.size() * sizeof(TransTask), cudaMemcpyHostToDevice);
+  cudaMemcpy(dsops, sops.data(), sops.size() * sizeof(RotSOp), cudaMemcpyHostToDevice);
+  if (engine == 1) cudaMemcpy(drops, rops.data(), NG * sizeof(RotOp), cudaMemcpyHostToDevice);
+  auto launch = [&]() {
+    if (engine == 0)
+      launch_translate_rot_split(0, (int)tasks.size(), dtask, dp, dsops, dpool, D, C, dim, dsrc, ddst);
+    else
+      launch_translate_rot<float>(0, (int)tasks.size(), dtask, dp, drops, dpool, D, C, dim, dsrc, ddst);
+  };
+  try {
+    launch();
+  } catch (const CudaError&) {
+    release();
+    return 256;
+  }
+  if (cudaDeviceSynchronize() != cudaSuccess) {
+    release();
+    return 256;
+  }
+  cudaMemcpy(hdst.data(), ddst, hdst.size() * 4, cudaMemcpyDeviceToHost);
+  if (reps > 0 && ms) {
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, 0);
+    try {
+      for (int r = 0; r < reps; r++) launch();
+    } catch (const CudaError&) {
+      release();
+      return 256;
+    }
+    cudaEventRecord(e1, 0);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      release();
+      return 256;
+    }
+    float t = 0.f;
+    cudaEventElapsedTime(&t, e0, e1);
+    *ms = t / reps;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+  }
+  release();
+  if (!rel) return 0;
+  double num = 0, den = 0;
+  for (int g = 0; g < NG; g++)
+    for (int c = 0; c < C; c++) {
+      std::vector<double> ref(dim, 0.0), v(dim), y;
+      for (int k = 0; k < npair; k++) {
+        const float* s = &hsrc[((size_t)(g * npair + k) * C + c) * D];
+        for (int q = 0; q < dim; q++) v[q] = s[q];
+        apply_split_packed(&spool[sops[g].base], p, v, y);
+        for (int q = 0; q < dim; q++) ref[q] += (0.5 + 0.25 * k) * y[q];
+      }
+      const float* got = &hdst[((size_t)(nsrc + g) * C + c) * D];
+      for (int n = 0; n <= p; n++)
+        for (int m = 0; m <= n; m++)
+          for (int part = 0; part < 2; part++) {
+            if (m == 0 && part == 1) continue;
+            const int q = 2 * cidx(n, m) + part;
+            num += (got[q] - ref[q]) * (got[q] - ref[q]);
+            den += ref[q] * ref[q];
+          }
+    }
+  *rel = std::sqrt(num / std::max(den, 1e-300));
+  return 0;
+}
+
+extern "C" int efmm_rot_split_selfcheck_device(int p, int C, int npair, unsigned seed, int engine, double* rel) {
+  if (!rel) return 16;
+  return rot_split_device_run(p, C, npair, seed, engine, 0, rel, nullptr);
+}
+
+// Mean ms of reps launches of the kernel of `engine` on the same inputs.
+extern "C" int efmm_rot_split_bench(int p, int C, int npair, int engine, int reps, double* ms) {
+  if (reps < 1 || !ms) return 16;
+  return rot_split_device_run(p, C, npair, 1, engine, reps, nullptr, ms);
 }

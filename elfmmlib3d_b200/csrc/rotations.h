@@ -48,6 +48,26 @@ double check_factored_ops(const std::vector<int>& kinds, const std::vector<int>&
                           const std::vector<double>& offsets, const std::vector<RotOp>& ops,
                           const std::vector<double>& pool, int stride);
 
+// Parity-split factored form (FP32 device pool, normalised basis): the frame
+// change as Ry(-theta) Rz(-phi); Rz a 2 x 2 per order m, Ry and the shift
+// along z re / im blocks per degree / order.  Per group at `base` (floats):
+// Rz forward [4 (p+1)], Ry forward blocks n = 0..p, shift blocks m = 0..p,
+// Ry back blocks n = 0..p, Rz back [4 (p+1)]; a block of r rows holds, per
+// input row k, ceil(r/2) float4 (re[2j][k], re[2j+1][k], im[2j][k],
+// im[2j+1][k]).
+struct RotSOp {
+  int p, pad;
+  long long base;
+};
+long long rots_group_size(int p);
+// The split pool of every group; w: normalisation per real row at the
+// largest order (2 ncoef(pmax)).
+void build_split_ops(const std::vector<int>& kinds, const std::vector<int>& orders,
+                     const std::vector<double>& offsets, const std::vector<double>& w,
+                     std::vector<RotSOp>& ops, std::vector<float>& pool);
+// Whether the split kernel serves a launch whose largest operator size is maxdim.
+bool rot_split_ok(int maxdim);
+
 struct TransTask;
 struct TransPair;
 
@@ -56,6 +76,11 @@ struct TransPair;
 template <class T>
 void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                           const RotOp* ops, const T* pool, int D, int C, int maxdim, const T* src, T* dst);
+
+// The same translations from the split pool (FP32, orders <= 31).
+void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
+                                const RotSOp* ops, const float* pool, int D, int C, int maxdim, const float* src,
+                                float* dst);
 
 // Columns per CTA of the factored kernel for a given largest operator size.
 int rot_cols_per_cta(int maxdim, int elem_bytes);

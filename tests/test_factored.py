@@ -31,3 +31,19 @@ def test_u_kernel_m2l_selfcheck(lib):
         e20 = f(20, *X, 20, 3)
         assert 0 <= e20 < 1e-6 and e20 < e8, (X, e8, e20)
     assert f(0, 2.0, 0, 0, 5, 1) == -1.0
+
+
+@pytest.mark.parametrize("p,eps,stride", [(6, 0.5e-2, 1), (14, 0.5e-3, 1), (26, 0.5e-6, 9), (30, 5e-8, 13), (31, 5e-8, 29)])
+def test_parity_split_equals_dense(lib, p, eps, stride):
+    """The translations as Rz, the re / im blocks of Ry, the shift's re / im
+    blocks, Ry back and Rz back: in double against the dense operators, and
+    the packed FP32 pool of the device kernel applied on the host as the
+    kernel reads it (FP32 operator rounding only)."""
+    L = lib.load()
+    f = L.efmm_split_selfcheck
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    worst = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    assert f(p, eps, stride, worst) == 316 + 16
+    assert worst[0] < 1e-12
+    assert worst[1] < 1e-6
