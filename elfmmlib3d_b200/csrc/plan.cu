@@ -850,8 +850,11 @@ void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T
     }
   }
   // factored form when its column tiles fit in shared memory
-  const int W = rot_cols_per_cta(D, (int)sizeof(T));
-  const size_t smem = sizeof(T) * 2 * (size_t)D * W;
+  // (the split kernel's tiles have rot_split_cols() columns; the split
+  // serves every launch when it is on: p <= 31 bounds every group's order)
+  const bool split = sizeof(T) == 4 && split_rot();
+  const int W = split ? rot_split_cols() : rot_cols_per_cta(D, (int)sizeof(T));
+  const size_t smem = sizeof(T) * 2 * (size_t)D * rot_cols_per_cta(D, (int)sizeof(T));
   if (factored_ && smem <= 227 * 1024) {
     ensure_factored();
     cut_rot_tasks(S, C, W);
@@ -860,7 +863,6 @@ void Plan::run_translations(TransSched& S, int C, const T* mats, const T* src, T
       pool = reinterpret_cast<const T*>(ops_->rot_d.get());
     else
       pool = reinterpret_cast<const T*>(ops_->rot_f.get());
-    const bool split = sizeof(T) == 4 && split_rot();
     if (split) ensure_split();
     for (size_t i = 0; i < S.lev_rtasks.size(); i++) {
       if (split && rot_split_ok(S.lev_rdim[i])) {

@@ -550,10 +550,11 @@ void apply_split_host(const SplitHost& S, const std::vector<double>& v, std::vec
 
 }  // namespace
 
-// floats of the split blocks of r = 1..R rows (4 r ceil(r/2) each)
+// floats of the split blocks of r = 1..R rows: r operator columns and one
+// zero column, ceil(r/2) float4 each
 EFMM_HD constexpr long long rots_blocks(int R) {
   long long s = 0;
-  for (int r = 1; r <= R; r++) s += 4LL * r * ((r + 1) / 2);
+  for (int r = 1; r <= R; r++) s += 4LL * (r + 1) * ((r + 1) / 2);
   return s;
 }
 long long rots_group_size(int p) { return 8LL * (p + 1) + 3 * rots_blocks(p + 1); }
@@ -591,13 +592,13 @@ void build_split_ops(const std::vector<int>& kinds, const std::vector<int>& orde
       for (int q = 0; q < 4 * (p + 1); q++) rz[q] = (float)S.rz[s][q];
     }
     // a block of r rows: column k holds ceil(r/2) float4 (re[2j][k],
-    // re[2j+1][k], im[2j][k], im[2j+1][k])
+    // im[2j][k], re[2j+1][k], im[2j+1][k]); column r stays zero
     auto pack = [&](float* dst, const std::vector<double>& B, int r, auto scale) {
       const int h = (r + 1) / 2;
       for (int k = 0; k < r; k++)
         for (int j = 0; j < h; j++)
           for (int e = 0; e < 4; e++) {
-            const int i = 2 * j + (e & 1), part = e >> 1;
+            const int i = 2 * j + (e >> 1), part = e & 1;
             double v = 0;
             if (i < r) v = B[(size_t)part * r * r + (size_t)i * r + k] * scale(i, k);
             dst[((size_t)k * h + j) * 4 + e] = (float)v;
@@ -1011,15 +1012,22 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
 // FP32 translations in the parity-split form (build_split_ops): five factors
 // per column, Rz forward (applied while the sources are staged), the re / im
 // blocks of Ry forward, of the shift along z and of Ry back (one warp per
-// block, in place in X[row][16]), Rz back (applied to the last blocks'
-// results in registers).  In a block of r rows, lane (rp, ch) owns output
-// rows 2 rp, 2 rp + 1 of both parts for NCT / CG columns; per input row k it
-// reads one float4 of operator (re and im of its two rows) and the re and im
-// input rows of its columns as broadcasts: CG = 2 (16 row pairs x 8
-// columns) for r > 16, CG = 4 (8 row pairs x 4 columns) below.  Operator
-// columns are copied per warp by cp.async into two chunk buffers, one chunk
-// ahead.  For orders p <= 31; two CTAs of 12 warps per SM up to p = 30.
-constexpr int RS_THREADS = 384, RS_NCT = 16, RS_NW = RS_THREADS / 32, RS_CH = 8, RS_PMAX = 31;
+// block, in place in shared memory), Rz back (applied to the last blocks'
+// results in registers).  Shared layout: per coefficient c one row of the
+// task's 16 columns as (re, im) pairs, rows 36 floats apart (the 4-float pad
+// keeps the staging and the output conflict-free).  In a block of r rows,
+// lane (rp, ch) owns output rows 2 rp, 2 rp + 1 for 16 / CG columns; per
+// input row k it reads one float4 of operator (re, im of row 2 rp; re, im of
+// row 2 rp + 1; 16 lanes read 256 contiguous bytes) and the (re, im) pairs
+// of its columns as shared-memory broadcasts, so that every product is one
+// paired FMA (re and im lanes of the pair) with no register moves: CG = 2
+// (16 row pairs x 8 columns) for r > 16, CG = 4 (8 row pairs x 4 columns)
+// below.  The operator float4 come straight from global memory (L2), PF
+// rows ahead in registers; the product loop runs whole groups of PF rows
+// with no branch inside (the steps past a block's last row read its zero
+// column).  NW warps per CTA, 3 (NW = 8) or 2 (NW = 12) CTAs per SM, 80
+// registers; for orders p <= 31.
+constexpr int RS_PMAX = 31, RS_NCT = 16, RS_XS = 2 * RS_NCT + 4;
 struct RsBlocks {
   int s[RS_PMAX + 3];
 };
@@ -1029,18 +1037,39 @@ constexpr RsBlocks make_rs_blocks() {
   return b;
 }
 __constant__ RsBlocks c_rs_blocks = make_rs_blocks();
-__host__ __device__ inline size_t rs_cbase_off(int dim) { return sizeof(float) * (size_t)dim * RS_NCT; }
-__host__ __device__ inline size_t rs_wbuf_off(int dim) { return rs_cbase_off(dim) + 8 * RS_NCT; }
-// per warp two chunk buffers of RS_CH operator columns of <= 16 float4
-__host__ __device__ inline size_t rs_smem(int dim) {
-  return rs_wbuf_off(dim) + (size_t)RS_NW * 2 * RS_CH * 16 * sizeof(float4);
+// Warp of degree block n at order p (order block p - n of the shift), nw
+// warps: a block of r rows costs r steps rounded up to the prefetch depth
+// (all its rows are spread over the lanes), a step of the 8-column form
+// about twice one of the 4-column form, plus a fixed cost per block; largest
+// first onto the least loaded warp.
+constexpr RotwOwners make_rs_owners(int nw) {
+  RotwOwners o{};
+  for (int p = 0; p <= RS_PMAX; p++) {
+    int load[16] = {};
+    for (int n = p; n >= 0; n--) {
+      int best = 0;
+      for (int w = 1; w < nw; w++)
+        if (load[w] < load[best]) best = w;
+      o.o[p][n] = (unsigned char)best;
+      const int r = n + 1;
+      load[best] += (r + 3) / 4 * 4 * (r > 16 ? 20 : 11) + 60;
+    }
+  }
+  return o;
 }
+__constant__ RotwOwners c_rs_owners8 = make_rs_owners(8);
+__constant__ RotwOwners c_rs_owners12 = make_rs_owners(12);
+__host__ __device__ inline size_t rs_cbase_off(int dim) { return sizeof(float) * (size_t)(dim / 2) * RS_XS; }
+__host__ __device__ inline size_t rs_smem(int dim) { return rs_cbase_off(dim) + 8 * RS_NCT; }
+// float4 f (columns 2f, 2f + 1) of coefficient c in the shared rows
+__device__ __forceinline__ float4* rs_x(float* X, int c, int f) { return reinterpret_cast<float4*>(X + c * RS_XS) + f; }
 
-__global__ void __launch_bounds__(RS_THREADS, 2)
+template <int NW, int PF>
+__global__ void __launch_bounds__(NW * 32, NW == 8 ? 3 : 2)
 k_translate_rot_s(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
                   const RotSOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
                   const float* __restrict__ src, float* __restrict__ dst) {
-  constexpr int NCT = RS_NCT;
+  constexpr int NCT = RS_NCT, XS = RS_XS, NT = NW * 32;
   extern __shared__ __align__(16) unsigned char rs_smem_[];
   const TransTask t = tasks[blockIdx.x];
   const RotSOp op = ops[t.group];
@@ -1052,9 +1081,9 @@ k_translate_rot_s(const TransTask* __restrict__ tasks, const TransPair* __restri
   const float* zb = ryf + nblk;
   const float* ryb = zb + nblk;
   const float4* rzb = reinterpret_cast<const float4*>(ryb + nblk);
-  float* X = reinterpret_cast<float*>(rs_smem_);                                   // [dim][NCT]
+  float* X = reinterpret_cast<float*>(rs_smem_);                                   // [nc][XS]
   long long* cbase = reinterpret_cast<long long*>(rs_smem_ + rs_cbase_off(dim));  // [NCT]: source columns
-  const unsigned char* owner = c_rotw_owners.o[p];
+  const unsigned char* owner = (NW == 8 ? c_rs_owners8 : c_rs_owners12).o[p];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (tid < NCT) {
     const int col = t.col0 + tid;
@@ -1067,151 +1096,153 @@ k_translate_rot_s(const TransTask* __restrict__ tasks, const TransPair* __restri
   }
   __syncthreads();
   // stage the sources with Rz forward: thread (coefficient, 4 columns)
-  for (int q = tid; q < nc * 4; q += RS_THREADS) {
+  for (int q = tid; q < nc * (NCT / 4); q += NT) {
     const int c = q % nc, cg = q / nc;
     int n, m;
     coef_nm(c, n, m);
     const float4 R = __ldg(rzf + m);
-    float re[4], im[4];
+    float2 v[4];
 #pragma unroll
     for (int g = 0; g < 4; g++) {
       const long long b = cbase[cg * 4 + g];
-      const float2 v = b >= 0 ? __ldg(reinterpret_cast<const float2*>(src + b + 2 * c)) : make_float2(0.f, 0.f);
-      re[g] = R.x * v.x + R.y * v.y;
-      im[g] = R.z * v.x + R.w * v.y;
+      const float2 s = b >= 0 ? __ldg(reinterpret_cast<const float2*>(src + b + 2 * c)) : make_float2(0.f, 0.f);
+      v[g] = make_float2(R.x * s.x + R.y * s.y, R.z * s.x + R.w * s.y);
     }
-    *reinterpret_cast<float4*>(X + (size_t)(2 * c) * NCT + cg * 4) = make_float4(re[0], re[1], re[2], re[3]);
-    *reinterpret_cast<float4*>(X + (size_t)(2 * c + 1) * NCT + cg * 4) = make_float4(im[0], im[1], im[2], im[3]);
+    *rs_x(X, c, 2 * cg) = make_float4(v[0].x, v[0].y, v[1].x, v[1].y);
+    *rs_x(X, c, 2 * cg + 1) = make_float4(v[2].x, v[2].y, v[3].x, v[3].y);
   }
   __syncthreads();
-  float4* wbuf = reinterpret_cast<float4*>(rs_smem_ + rs_wbuf_off(dim)) + (size_t)warp * 2 * RS_CH * 16;
-  // operator columns [chunk RS_CH, +RS_CH) of a block (h float4 per column)
-  auto fetch = [&](const float* blk, int h, int ncol, int chunk) {
-    const int c0 = chunk * RS_CH, nbytes = 16 * h * min(RS_CH, ncol - c0);
-    const char* g = reinterpret_cast<const char*>(blk + (size_t)c0 * 4 * h);
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(wbuf + (chunk & 1) * RS_CH * 16));
-    for (int b = 16 * lane; b < nbytes; b += 16 * 32)
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d + b), "l"(g + b) : "memory");
-    asm volatile("cp.async.commit_group;" ::: "memory");
-  };
-  // one block of r rows; xrow(k): X row of the re part of row k (im: + 1);
-  // the results go back to the same rows, through rz (4 per order, indexed
-  // by the row) when given
-  auto block = [&](auto cgtag, const float* blk, int r, auto xrow, const float4* rz) {
-    constexpr int CG = decltype(cgtag)::value, RP = 32 / CG, COLS = NCT / CG, NV = COLS / 2;
+  // one block of r rows (operator columns at blk, h float4 each, then a
+  // zero column); row k of the block is coefficient c(k) = c0 + k (Ry:
+  // dc = 0) or c0 + k (i + 1) + k (k - 1) / 2 (the shift's order block i:
+  // c(k + 1) - c(k) = i + k + 1, dc = 1); the results go back to the same
+  // coefficients, through rz (4 per order, indexed by the row) when given.
+  // Lanes past the block's rows read the last row pair's operator (no
+  // divergence in the product loop) and write nothing.
+  auto block = [&](auto cgtag, const float* blk, int r, int c0, int i, int dc, const float4* rz) {
+    constexpr int CG = decltype(cgtag)::value, RP = 32 / CG, COLS = NCT / CG, NF = COLS / 2;
     const int h = (r + 1) / 2, rp = lane % RP, ch = lane / RP;
     const bool act = rp < h;
-    float2 aR0[NV], aR1[NV], aI0[NV], aI1[NV];
+    const float4* opp = reinterpret_cast<const float4*>(blk) + min(rp, h - 1);
+    float2 a0[COLS], a1[COLS];  // (re, im) of rows 2 rp, 2 rp + 1 per column
 #pragma unroll
-    for (int v = 0; v < NV; v++) aR0[v] = aR1[v] = aI0[v] = aI1[v] = make_float2(0.f, 0.f);
-    const int nch = (r + RS_CH - 1) / RS_CH;
-    fetch(blk, h, r, 0);
-    for (int chk = 0; chk < nch; chk++) {
-      if (chk + 1 < nch)
-        fetch(blk, h, r, chk + 1);
-      else
-        asm volatile("cp.async.commit_group;" ::: "memory");
-      asm volatile("cp.async.wait_group 1;" ::: "memory");
-      __syncwarp();
-      const float4* wb = wbuf + (chk & 1) * RS_CH * 16;
-      const int cend = min(RS_CH, r - chk * RS_CH);
-      for (int u = 0; u < cend; u++) {
-        const float4 o = act ? wb[u * h + rp] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float* xre = X + (size_t)xrow(chk * RS_CH + u) * NCT + ch * COLS;
-        float xr[COLS], xi[COLS];
+    for (int v = 0; v < COLS; v++) a0[v] = a1[v] = make_float2(0.f, 0.f);
+    // shared position of row k: xo (floats from X), advanced by xs per row,
+    // xs growing by dxs (the shift's rows lie further apart as n grows);
+    // the steps past the last row read the zero operator column r and the
+    // last row
+    int xo = c0 * XS + ch * 2 * COLS;
+    int xs = dc ? (i + 1) * XS : XS;
+    const int dxs = dc ? XS : 0;
+    const int xlast = xo + (dc ? (r - 1) * (i + 1) + (r - 1) * (r - 2) / 2 : r - 1) * XS;
+    // operator rows k .. k + PF - 1 in flight
+    float4 oq[PF];
 #pragma unroll
-        for (int v = 0; v < COLS / 4; v++) {
-          const float4 a = reinterpret_cast<const float4*>(xre)[v];
-          const float4 b = reinterpret_cast<const float4*>(xre + NCT)[v];
-          xr[4 * v] = a.x; xr[4 * v + 1] = a.y; xr[4 * v + 2] = a.z; xr[4 * v + 3] = a.w;
-          xi[4 * v] = b.x; xi[4 * v + 1] = b.y; xi[4 * v + 2] = b.z; xi[4 * v + 3] = b.w;
-        }
-        const float2 w0 = make_float2(o.x, o.x), w1 = make_float2(o.y, o.y);
-        const float2 w2 = make_float2(o.z, o.z), w3 = make_float2(o.w, o.w);
+    for (int j = 0; j < PF; j++) oq[j] = __ldg(opp + min(j, r) * h);
+    const int nit = (r + PF - 1) / PF;
+    for (int it = 0, k = PF; it < nit; it++) {
 #pragma unroll
-        for (int v = 0; v < NV; v++) {
-          const float2 x2 = make_float2(xr[2 * v], xr[2 * v + 1]), y2 = make_float2(xi[2 * v], xi[2 * v + 1]);
-          aR0[v] = __ffma2_rn(w0, x2, aR0[v]);
-          aR1[v] = __ffma2_rn(w1, x2, aR1[v]);
-          aI0[v] = __ffma2_rn(w2, y2, aI0[v]);
-          aI1[v] = __ffma2_rn(w3, y2, aI1[v]);
+      for (int j = 0; j < PF; j++, k++) {
+        const float4 o = oq[j];
+        oq[j] = __ldg(opp + min(k, r) * h);
+        const float2 w0 = make_float2(o.x, o.y), w1 = make_float2(o.z, o.w);
+        const float4* xq = reinterpret_cast<const float4*>(X + min(xo, xlast));
+        xo += xs;
+        xs += dxs;
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          const float4 x = xq[f];
+          const float2 xa = make_float2(x.x, x.y), xb = make_float2(x.z, x.w);
+          a0[2 * f] = __ffma2_rn(w0, xa, a0[2 * f]);
+          a0[2 * f + 1] = __ffma2_rn(w0, xb, a0[2 * f + 1]);
+          a1[2 * f] = __ffma2_rn(w1, xa, a1[2 * f]);
+          a1[2 * f + 1] = __ffma2_rn(w1, xb, a1[2 * f + 1]);
         }
       }
-      __syncwarp();  // buffer (chk & 1) is refilled by the fetch of chunk chk + 2
     }
-    auto put = [&](int i, const float2* aR, const float2* aI) {
-      float* xo = X + (size_t)xrow(i) * NCT + ch * COLS;
-      float ore[COLS], oim[COLS];
-#pragma unroll
-      for (int v = 0; v < NV; v++) {
-        ore[2 * v] = aR[v].x; ore[2 * v + 1] = aR[v].y;
-        oim[2 * v] = aI[v].x; oim[2 * v + 1] = aI[v].y;
-      }
+    __syncwarp();  // every lane's reads of the block's rows are done
+    auto put = [&](int k, const float2* a) {
+      const int c = c0 + (dc ? k * (i + 1) + k * (k - 1) / 2 : k);
+      float2 o[COLS];
       if (rz) {
-        const float4 R = __ldg(rz + i);
+        const float4 R = __ldg(rz + k);
 #pragma unroll
-        for (int e = 0; e < COLS; e++) {
-          const float a = ore[e], b = oim[e];
-          ore[e] = R.x * a + R.y * b;
-          oim[e] = R.z * a + R.w * b;
-        }
+        for (int e = 0; e < COLS; e++) o[e] = make_float2(R.x * a[e].x + R.y * a[e].y, R.z * a[e].x + R.w * a[e].y);
+      } else {
+#pragma unroll
+        for (int e = 0; e < COLS; e++) o[e] = a[e];
       }
 #pragma unroll
-      for (int v = 0; v < COLS / 4; v++) {
-        reinterpret_cast<float4*>(xo)[v] = make_float4(ore[4 * v], ore[4 * v + 1], ore[4 * v + 2], ore[4 * v + 3]);
-        reinterpret_cast<float4*>(xo + NCT)[v] = make_float4(oim[4 * v], oim[4 * v + 1], oim[4 * v + 2], oim[4 * v + 3]);
-      }
+      for (int f = 0; f < NF; f++) *rs_x(X, c, ch * NF + f) = make_float4(o[2 * f].x, o[2 * f].y, o[2 * f + 1].x, o[2 * f + 1].y);
     };
     if (act) {
-      put(2 * rp, aR0, aI0);
-      if (2 * rp + 1 < r) put(2 * rp + 1, aR1, aI1);
+      put(2 * rp, a0);
+      if (2 * rp + 1 < r) put(2 * rp + 1, a1);
     }
     __syncwarp();
   };
-  auto run_block = [&](const float* blk, int r, auto xrow, const float4* rz) {
-    if (r > 16)
-      block(std::integral_constant<int, 2>{}, blk, r, xrow, rz);
-    else
-      block(std::integral_constant<int, 4>{}, blk, r, xrow, rz);
-  };
-  auto rotate = [&](const float* base, const float4* rz) {
-    for (int n = 0; n <= p; n++) {
-      if (owner[n] != warp) continue;
-      const int r0 = n * (n + 1);
-      run_block(base + c_rs_blocks.s[n], n + 1, [&](int k) { return r0 + 2 * k; }, rz);
+  // the three factors: degree blocks n of Ry forward, order blocks m of the
+  // shift (owned like degree block p - m), degree blocks of Ry back
+  for (int st = 0; st < 3; st++) {
+    for (int i = 0; i <= p; i++) {
+      if (owner[st == 1 ? p - i : i] != warp) continue;
+      const int r = st == 1 ? p - i + 1 : i + 1;
+      const float* blk = st == 1 ? zb + nblk - c_rs_blocks.s[p + 1 - i] : (st == 0 ? ryf : ryb) + c_rs_blocks.s[i];
+      // first coefficient of the block: (i, i) for the shift's order i, (i, 0) for degree i
+      const int c0 = i * (i + 1) / 2 + (st == 1 ? i : 0);
+      const float4* rz = st == 2 ? rzb : nullptr;
+      if (r > 16)
+        block(std::integral_constant<int, 2>{}, blk, r, c0, i, st == 1, rz);
+      else
+        block(std::integral_constant<int, 4>{}, blk, r, c0, i, st == 1, rz);
     }
-  };
-  rotate(ryf, nullptr);
-  __syncthreads();
-  // shift along z: order block m (rows (n, m), n = m..p), owned like degree block p - m
-  for (int m = 0; m <= p; m++) {
-    if (owner[p - m] != warp) continue;
-    run_block(zb + nblk - c_rs_blocks.s[p + 1 - m], p - m + 1,
-              [&](int k) { const int n = m + k; return n * (n + 1) + 2 * m; }, nullptr);
+    __syncthreads();
   }
-  __syncthreads();
-  rotate(ryb, rzb);
-  __syncthreads();
   for (int j = 0; j < NCT; j++) {
     const int col = t.col0 + j;
     if (col >= t.ncols) break;
     const TransPair pr = pairs[t.pair0 + col / C];
     float* dp = dst + ((size_t)pr.dst * C + col % C) * D;
     const float al = (float)pr.alpha;
-    for (int r = tid; r < dim; r += RS_THREADS) atomicAdd(dp + r, al * X[(size_t)r * NCT + j]);
+    for (int r = tid; r < dim; r += NT) {
+      const float* x = reinterpret_cast<const float*>(rs_x(X, r >> 1, j >> 1));
+      atomicAdd(dp + r, al * x[2 * (j & 1) + (r & 1)]);
+    }
   }
 }
 
 bool rot_split_ok(int maxdim) { return maxdim <= (RS_PMAX + 1) * (RS_PMAX + 2); }
 
+// Columns per CTA of the split kernel.
+int rot_split_cols() { return RS_NCT; }
+
+// Variants of the split kernel: 1 (12 warps, operator rows 2 ahead), 2 (8
+// warps, 3), 3 (8, 2), 4 (8, 4); <= 0 takes ELFMM3D_ROTS_VARIANT, default 3.
 void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                                 const RotSOp* ops, const float* pool, int D, int C, int maxdim, const float* src,
-                                float* dst) {
+                                float* dst, int variant) {
   if (ntask <= 0) return;
   if (!rot_split_ok(maxdim)) throw CudaError{(int)cudaErrorInvalidValue};
+  static const int v_env = [] {
+    const char* e = getenv("ELFMM3D_ROTS_VARIANT");
+    const int v = e ? atoi(e) : 3;
+    return (v >= 1 && v <= 4) ? v : 3;
+  }();
+  const int v = variant > 0 ? variant : v_env;
+  if (v < 1 || v > 4) throw CudaError{(int)cudaErrorInvalidValue};
   const size_t smem = rs_smem(maxdim);
-  EFMM_CUDA_TRY(smem_raise(k_translate_rot_s, (int)smem));
-  k_translate_rot_s<<<ntask, RS_THREADS, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
+  auto go = [&](auto kern, int nw) {
+    EFMM_CUDA_TRY(smem_raise(kern, (int)smem));
+    kern<<<ntask, nw * 32, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
+  };
+  if (v == 1)
+    go(k_translate_rot_s<12, 2>, 12);
+  else if (v == 2)
+    go(k_translate_rot_s<8, 3>, 8);
+  else if (v == 3)
+    go(k_translate_rot_s<8, 2>, 8);
+  else
+    go(k_translate_rot_s<8, 4>, 8);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -1323,9 +1354,9 @@ void apply_split_packed(const float* g, int p, const std::vector<double>& v, std
     std::vector<double> o(2 * r, 0.0);
     for (int k = 0; k < r; k++)
       for (int i = 0; i < r; i++) {
-        const float* q = B + ((size_t)k * h + i / 2) * 4;
-        o[2 * i] += q[i & 1] * x[row(k)];
-        o[2 * i + 1] += q[2 + (i & 1)] * x[row(k) + 1];
+        const float* q = B + ((size_t)k * h + i / 2) * 4 + 2 * (i & 1);
+        o[2 * i] += q[0] * x[row(k)];
+        o[2 * i + 1] += q[1] * x[row(k) + 1];
       }
     for (int i = 0; i < r; i++) {
       x[row(i)] = o[2 * i];
@@ -1426,15 +1457,16 @@ extern "C" int efmm_split_selfcheck(int p, double eps, int stride, double* worst
 // M2L offset, one along -z, an M2M and an L2L shift), npair box pairs each
 // with C columns per box (random normalised sources, pair factors alpha, one
 // destination box per group), in one launch.  engine 0: the parity-split
-// kernel (k_translate_rot_s); 1: the full-block kernels (k_translate_rot_w /
-// k_translate_rot, as launch_translate_rot<float> picks them).  reps > 0
+// kernel (k_translate_rot_s, default variant); 1: the full-block kernels
+// (k_translate_rot_w / k_translate_rot, as launch_translate_rot<float> picks
+// them); 2..5: the split kernel's variants 1..4.  reps > 0
 // then times reps more launches (mean ms in *ms).  With rel: the relative l2
 // error of the destinations of the first launch against the split factors
 // of the same FP32 pool applied in FP64 on the host.
 static int rot_split_device_run(int p, int C, int npair, unsigned seed, int engine, int reps, double* rel,
                                 double* ms) {
   using namespace efmm;
-  if (p < 1 || p > 31 || C < 1 || npair < 1 || (long long)C * npair > (1 << 20) || engine < 0 || engine > 1)
+  if (p < 1 || p > 31 || C < 1 || npair < 1 || (long long)C * npair > (1 << 20) || engine < 0 || engine > 5)
     return 16;
   const int NG = 4;
   std::vector<int> kinds = {0, 0, 1, 2}, orders(NG, p);
@@ -1482,7 +1514,7 @@ static int rot_split_device_run(int p, int C, int npair, unsigned seed, int engi
   auto release = [&]() {
     cudaFree(dsrc); cudaFree(ddst); cudaFree(dpool); cudaFree(dp); cudaFree(dtask); cudaFree(dsops); cudaFree(drops);
   };
-  const size_t pbytes = 4 * (engine == 0 ? spool.size() : poolf.size());
+  const size_t pbytes = 4 * (engine != 1 ? spool.size() : poolf.size());
   if (cudaMalloc(&dsrc, hsrc.size() * 4) || cudaMalloc(&ddst, hdst.size() * 4) || cudaMalloc(&dpool, pbytes) ||
       cudaMalloc(&dp, hp.size() * sizeof(TransPair)) || cudaMalloc(&dtask, tasks.size() * sizeof(TransTask)) ||
       cudaMalloc(&dsops, sops.size() * sizeof(RotSOp)) || cudaMalloc(&drops, NG * sizeof(RotOp))) {
@@ -1491,14 +1523,15 @@ static int rot_split_device_run(int p, int C, int npair, unsigned seed, int engi
   }
   cudaMemcpy(dsrc, hsrc.data(), hsrc.size() * 4, cudaMemcpyHostToDevice);
   cudaMemcpy(ddst, hdst.data(), hdst.size() * 4, cudaMemcpyHostToDevice);
-  cudaMemcpy(dpool, engine == 0 ? spool.data() : poolf.data(), pbytes, cudaMemcpyHostToDevice);
+  cudaMemcpy(dpool, engine != 1 ? spool.data() : poolf.data(), pbytes, cudaMemcpyHostToDevice);
   cudaMemcpy(dp, hp.data(), hp.size() * sizeof(TransPair), cudaMemcpyHostToDevice);
   cudaMemcpy(dtask, tasks.data(), tasks.size() * sizeof(TransTask), cudaMemcpyHostToDevice);
   cudaMemcpy(dsops, sops.data(), sops.size() * sizeof(RotSOp), cudaMemcpyHostToDevice);
   if (engine == 1) cudaMemcpy(drops, rops.data(), NG * sizeof(RotOp), cudaMemcpyHostToDevice);
   auto launch = [&]() {
-    if (engine == 0)
-      launch_translate_rot_split(0, (int)tasks.size(), dtask, dp, dsops, dpool, D, C, dim, dsrc, ddst);
+    if (engine != 1)
+      launch_translate_rot_split(0, (int)tasks.size(), dtask, dp, dsops, dpool, D, C, dim, dsrc, ddst,
+                                 engine == 0 ? 0 : engine - 1);
     else
       launch_translate_rot<float>(0, (int)tasks.size(), dtask, dp, drops, dpool, D, C, dim, dsrc, ddst);
   };

@@ -53,8 +53,8 @@ double check_factored_ops(const std::vector<int>& kinds, const std::vector<int>&
 // along z re / im blocks per degree / order.  Per group at `base` (floats):
 // Rz forward [4 (p+1)], Ry forward blocks n = 0..p, shift blocks m = 0..p,
 // Ry back blocks n = 0..p, Rz back [4 (p+1)]; a block of r rows holds, per
-// input row k, ceil(r/2) float4 (re[2j][k], re[2j+1][k], im[2j][k],
-// im[2j+1][k]).
+// input row k, ceil(r/2) float4 (re[2j][k], im[2j][k], re[2j+1][k],
+// im[2j+1][k]), then one zero column.
 struct RotSOp {
   int p, pad;
   long long base;
@@ -77,10 +77,13 @@ template <class T>
 void launch_translate_rot(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                           const RotOp* ops, const T* pool, int D, int C, int maxdim, const T* src, T* dst);
 
-// The same translations from the split pool (FP32, orders <= 31).
+// The same translations from the split pool (FP32, orders <= 31), tasks cut
+// for rot_split_cols() columns; variant <= 0: the default kernel variant.
 void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                                 const RotSOp* ops, const float* pool, int D, int C, int maxdim, const float* src,
-                                float* dst);
+                                float* dst, int variant = 0);
+// Columns per CTA of the split kernel.
+int rot_split_cols();
 
 // Columns per CTA of the factored kernel for a given largest operator size.
 int rot_cols_per_cta(int maxdim, int elem_bytes);
