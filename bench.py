@@ -590,13 +590,14 @@ def run_single_mixed(args, rank, world, local_rank):
         return None
     achieved = tr_flops / (tr_ms * 1e-3) / 1e12
     peak32 = gemm_peak(torch, dev, torch.float32)
-    roof = {"kernel": "translations (k_translate_rot_w / k_translate_rot<float>: M2M + M2L + L2L)",
+    roof = {"kernel": "translations (k_translate_rot_s, parity-split factored M2M + M2L + L2L, FP32)",
             "bound": "fp32", "achieved": achieved, "peak": peak32, "unit": "TFLOP/s",
             "frac": achieved / peak32 if peak32 else None, "traffic": None,
             "peak_source": "measured cuBLAS SGEMM 8192^3 with TF32 off (best of 5) in this run; the FP32 FMA "
                            "pipe (MEASURED_PEAKS.json has no FP32 entry)",
-            "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
-                           f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages"}
+            "algorithmic": f"{tr_flops:.4g} useful FP32 flop per step (per box pair and column: two Ry of "
+                           f"sum_n (n+1)^2 + n^2, the z shift's re / im blocks, two Rz; per-offset orders) in "
+                           f"{tr_ms:.1f} ms of translation stages"}
     return {
         "metric": SINGLE_MIXED_METRIC,
         "value": value, "unit": "triangle-evals/s", "n_gpus": world, "steps": args.steps,
@@ -730,11 +731,11 @@ def run_batch(args, rank, world, local_rank):
     tr_ms = tim["m2m"] + tim["m2l"] + tim["l2l"]
     achieved = tr_flops / (tr_ms * 1e-3) / 1e12
     peak32 = gemm_peak(torch, dev, torch.float32)
-    roof = {"kernel": "k_translate_rot<float> (M2M+M2L+L2L)", "bound": "fp32", "achieved": achieved,
+    roof = {"kernel": "k_translate_rot_s (parity-split M2M+M2L+L2L, FP32)", "bound": "fp32", "achieved": achieved,
             "peak": peak32, "unit": "TFLOP/s", "frac": achieved / peak32, "traffic": None,
             "peak_source": "measured cuBLAS SGEMM 8192^3 (FP32 pipe, TF32 off) in this run; "
                            "MEASURED_PEAKS.json has no FP32 entry",
-            "algorithmic": f"factored translations (rotation, shift along z, rotation back): "
+            "algorithmic": f"parity-split factored translations (Rz, Ry, shift along z, Ry back, Rz back): "
                            f"{tr_flops:.4g} flop per step over {info['m2l_pairs']} M2L pairs x {C} columns"}
     stage_tf = {k: fl[k] * C / (tim[k] * 1e-3) / 1e12 for k in ("p2m", "m2m", "m2l", "l2l", "l2t") if tim[k] > 0}
     cpu, oerr = None, None
@@ -1024,21 +1025,23 @@ def run_hsbatch(args, rank, world, local_rank):
                      "algorithmic": f"{nbytes:.4g} bytes per replay (split store 8 bytes per stored element, split "
                                     f"densities, FP64 products) in {nms:.2f} ms (CUDA events around the launch)"}
     # the dominant kernels of the step (ncu launch shares): the factored
-    # translations (k_translate_rot_w / k_translate_rot, FP32 FMA pipe),
-    # flops counted per pair and column as they run, time = the M2M + M2L +
-    # L2L stage events of both plans, against the measured SGEMM rate
+    # translations in the parity-split form (k_translate_rot_s, FP32 FMA
+    # pipe), useful flops per pair and column, time = the M2M + M2L + L2L
+    # stage events of both plans, against the measured SGEMM rate
     tr_flops = sum(trf.values()) + sum(tri_.values())
     tr_ms = float(np.mean([sum(s_[0][k] + s_[1][k] for k in ("m2m", "m2l", "l2l")) for s_ in stages]))
     peak32 = gemm_peak(torch, dev, torch.float32)
     tr_ach = tr_flops / (tr_ms * 1e-3) / 1e12
-    roof = {"kernel": "k_translate_rot_w + k_translate_rot (factored M2M / M2L / L2L, FP32, both plans; "
-                      "the largest share of the step's launch time)",
+    roof = {"kernel": "k_translate_rot_s (parity-split factored M2M / M2L / L2L: Rz, the re / im blocks of "
+                      "Ry and of the z shift, Ry back, Rz back; paired FP32 FMAs, both plans; the largest share "
+                      "of the step's launch time)",
             "bound": "fp32", "achieved": tr_ach, "peak": peak32, "unit": "TFLOP/s",
             "frac": tr_ach / peak32 if peak32 else None, "traffic": None,
             "peak_source": "measured cuBLAS SGEMM 8192^3 with TF32 off (best of 5) in this run; the FP32 FMA "
                            "pipe (MEASURED_PEAKS.json has no FP32 entry)",
-            "algorithmic": f"{tr_flops:.4g} FP32 flop per step (two rotations and the z shift per box pair and "
-                           f"column, per-offset orders) in {tr_ms:.1f} ms of translation stages",
+            "algorithmic": f"{tr_flops:.4g} useful FP32 flop per step (per box pair and column: two Ry of "
+                           f"sum_n (n+1)^2 + n^2, the z shift's re / im blocks, two Rz; per-offset orders) in "
+                           f"{tr_ms:.1f} ms of translation stages",
             "flops_by_stage": {"free": trf, "image": tri_}}
     cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
