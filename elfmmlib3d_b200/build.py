@@ -21,7 +21,7 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I" + CSRC, "-I" + INCLUDE]
 
-SOURCES = ["nearfield.cu", "tree.cu", "fmm.cu", "plan.cu", "capi.cu", "noalloc.cu", "rotations.cu", "halfspace.cu", "tc_gemm.cu", "geomio.cu", "rot_tc.cu", "solve.cu", "tune.cu", "particles.cu", "forest.cu", "tc_bulk.cu"]
+SOURCES = ["nearfield.cu", "tree.cu", "fmm.cu", "plan.cu", "capi.cu", "noalloc.cu", "rotations.cu", "halfspace.cu", "tc_gemm.cu", "geomio.cu", "rot_tc.cu", "solve.cu", "tune.cu", "particles.cu", "forest.cu", "tc_bulk.cu", "sort.cu"]
 
 
 def _headers():

@@ -1025,8 +1025,8 @@ k_translate_rot_w(const TransTask* __restrict__ tasks, const TransPair* __restri
 // below.  The operator float4 come straight from global memory (L2), PF
 // rows ahead in registers; the product loop runs whole groups of PF rows
 // with no branch inside (the steps past a block's last row read its zero
-// column).  NW warps per CTA, 3 (NW = 8) or 2 (NW = 12) CTAs per SM, 80
-// registers; for orders p <= 31.
+// column).  NW warps per CTA, registers sized for MINB CTAs per SM; for
+// orders p <= 31.
 constexpr int RS_PMAX = 31, RS_NCT = 16, RS_XS = 2 * RS_NCT + 4;
 struct RsBlocks {
   int s[RS_PMAX + 3];
@@ -1064,8 +1064,8 @@ __host__ __device__ inline size_t rs_smem(int dim) { return rs_cbase_off(dim) + 
 // float4 f (columns 2f, 2f + 1) of coefficient c in the shared rows
 __device__ __forceinline__ float4* rs_x(float* X, int c, int f) { return reinterpret_cast<float4*>(X + c * RS_XS) + f; }
 
-template <int NW, int PF>
-__global__ void __launch_bounds__(NW * 32, NW == 8 ? 3 : 2)
+template <int NW, int PF, int MINB>
+__global__ void __launch_bounds__(NW * 32, MINB)
 k_translate_rot_s(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
                   const RotSOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
                   const float* __restrict__ src, float* __restrict__ dst) {
@@ -1216,8 +1216,9 @@ bool rot_split_ok(int maxdim) { return maxdim <= (RS_PMAX + 1) * (RS_PMAX + 2); 
 // Columns per CTA of the split kernel.
 int rot_split_cols() { return RS_NCT; }
 
-// Variants of the split kernel: 1 (12 warps, operator rows 2 ahead), 2 (8
-// warps, 3), 3 (8, 2), 4 (8, 4); <= 0 takes ELFMM3D_ROTS_VARIANT, default 3.
+// Variants of the split kernel (warps, operator rows ahead, CTAs per SM the
+// registers are sized for): 1 (12, 2, 2), 2 (8, 4, 2), 3 (8, 2, 3), 4 (8, 6,
+// 2), 5 (8, 8, 2); <= 0 takes ELFMM3D_ROTS_VARIANT, default 3.
 void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs,
                                 const RotSOp* ops, const float* pool, int D, int C, int maxdim, const float* src,
                                 float* dst, int variant) {
@@ -1226,23 +1227,25 @@ void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tas
   static const int v_env = [] {
     const char* e = getenv("ELFMM3D_ROTS_VARIANT");
     const int v = e ? atoi(e) : 3;
-    return (v >= 1 && v <= 4) ? v : 3;
+    return (v >= 1 && v <= 5) ? v : 3;
   }();
   const int v = variant > 0 ? variant : v_env;
-  if (v < 1 || v > 4) throw CudaError{(int)cudaErrorInvalidValue};
+  if (v < 1 || v > 5) throw CudaError{(int)cudaErrorInvalidValue};
   const size_t smem = rs_smem(maxdim);
   auto go = [&](auto kern, int nw) {
     EFMM_CUDA_TRY(smem_raise(kern, (int)smem));
     kern<<<ntask, nw * 32, smem, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
   };
   if (v == 1)
-    go(k_translate_rot_s<12, 2>, 12);
+    go(k_translate_rot_s<12, 2, 2>, 12);
   else if (v == 2)
-    go(k_translate_rot_s<8, 3>, 8);
+    go(k_translate_rot_s<8, 4, 2>, 8);
   else if (v == 3)
-    go(k_translate_rot_s<8, 2>, 8);
+    go(k_translate_rot_s<8, 2, 3>, 8);
+  else if (v == 4)
+    go(k_translate_rot_s<8, 6, 2>, 8);
   else
-    go(k_translate_rot_s<8, 4>, 8);
+    go(k_translate_rot_s<8, 8, 2>, 8);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -1459,14 +1462,14 @@ extern "C" int efmm_split_selfcheck(int p, double eps, int stride, double* worst
 // destination box per group), in one launch.  engine 0: the parity-split
 // kernel (k_translate_rot_s, default variant); 1: the full-block kernels
 // (k_translate_rot_w / k_translate_rot, as launch_translate_rot<float> picks
-// them); 2..5: the split kernel's variants 1..4.  reps > 0
+// them); 2..6: the split kernel's variants 1..5.  reps > 0
 // then times reps more launches (mean ms in *ms).  With rel: the relative l2
 // error of the destinations of the first launch against the split factors
 // of the same FP32 pool applied in FP64 on the host.
 static int rot_split_device_run(int p, int C, int npair, unsigned seed, int engine, int reps, double* rel,
                                 double* ms) {
   using namespace efmm;
-  if (p < 1 || p > 31 || C < 1 || npair < 1 || (long long)C * npair > (1 << 20) || engine < 0 || engine > 5)
+  if (p < 1 || p > 31 || C < 1 || npair < 1 || (long long)C * npair > (1 << 20) || engine < 0 || engine > 6)
     return 16;
   const int NG = 4;
   std::vector<int> kinds = {0, 0, 1, 2}, orders(NG, p);

@@ -23,11 +23,11 @@
 // box above level L splits, and boxes of different columns are never
 // colleagues, so every list stays inside one problem and each problem sees
 // the FMM of the subtree below its column.
-#include <cub/cub.cuh>
 #include <vector>
 #include <algorithm>
 #include "common.cuh"
 #include "devbuf.h"
+#include "sort.h"
 #include "tree.h"
 
 namespace efmm {
@@ -307,10 +307,18 @@ static std::vector<T> to_host(const T* d, size_t n, cudaStream_t st) {
 
 static void exclusive_scan(cudaStream_t st, const int* in, int* out, int n, DevBuf<char>& tmp) {
   if (n <= 0) return;
-  size_t bytes = 0;
-  cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, st);
+  const size_t bytes = scan_scratch_bytes(n);
   if (bytes > tmp.size()) tmp.resize(bytes);
-  cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, st);
+  exclusive_scan_dev(st, in, out, n, tmp.get());
+}
+
+// stable sort of (key, value) pairs whose keys are below 2^bits (sort.cu)
+static void sort_pairs(cudaStream_t st, const unsigned long long* kin, unsigned long long* kout, const int* vin,
+                       int* vout, int n, const std::vector<int>& shifts, DevBuf<char>& tmp) {
+  if (n <= 0) return;
+  const size_t bytes = radix_scratch_bytes(n);
+  if (bytes > tmp.size()) tmp.resize(bytes);
+  radix_sort_pairs(st, kin, kout, vin, vout, n, shifts.data(), (int)shifts.size(), tmp.get());
 }
 
 // sort pairs (a, b) of box ids by (a, b) and build CSR over nb boxes
@@ -341,10 +349,13 @@ static void pairs_to_csr(cudaStream_t st, DevBuf<int2>& pairs, int np, int nb, D
   items.resize(np);
   if (np > 0) {
     k_pair_keys<<<(np + 255) / 256, 256, 0, st>>>(np, pairs.get(), k0.get(), v0.get()); count_launch();
-    size_t bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, bytes, k0.get(), k1.get(), v0.get(), items.get(), np, 0, 64, st);
-    if (bytes > tmp.size()) tmp.resize(bytes);
-    cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, k0.get(), k1.get(), v0.get(), items.get(), np, 0, 64, st);
+    // keys (a << 32) | b with a, b < nb: only the low digits of each word vary
+    int nbits = 1;
+    while ((1ll << nbits) < (long long)nb) nbits++;
+    std::vector<int> shifts;
+    for (int b = 0; b < nbits; b += 8) shifts.push_back(b);
+    for (int b = 0; b < nbits; b += 8) shifts.push_back(32 + b);
+    sort_pairs(st, k0.get(), k1.get(), v0.get(), items.get(), np, shifts, tmp);
   }
   DevBuf<int>& cnt = S.cnt;
   cnt.resize(nb + 1);
@@ -514,16 +525,12 @@ int build_tree(cudaStream_t st, int n, const double* d_src, int nt, const double
     int bits = 3;
     while ((1ll << (bits - 3)) <= (long long)std::max(n, nt) && bits < 64) bits++;
     {
-      size_t bytes = 0;
-      cub::DeviceRadixSort::SortPairs(nullptr, bytes, ks.get(), ks2.get(), tr.iz.get(), izs2.get(), n, 0, bits, st);
-      if (bytes > tmp.size()) tmp.resize(bytes);
-      cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, ks.get(), ks2.get(), tr.iz.get(), izs2.get(), n, 0, bits, st);
+      std::vector<int> shifts;
+      for (int b = 0; b < bits; b += 8) shifts.push_back(b);
+      sort_pairs(st, ks.get(), ks2.get(), tr.iz.get(), izs2.get(), n, shifts, tmp);
       tr.iz.swap(izs2);
       if (nt > 0) {
-        bytes = 0;
-        cub::DeviceRadixSort::SortPairs(nullptr, bytes, kt.get(), kt2.get(), tr.izt.get(), izt2.get(), nt, 0, bits, st);
-        if (bytes > tmp.size()) tmp.resize(bytes);
-        cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kt.get(), kt2.get(), tr.izt.get(), izt2.get(), nt, 0, bits, st);
+        sort_pairs(st, kt.get(), kt2.get(), tr.izt.get(), izt2.get(), nt, shifts, tmp);
         tr.izt.swap(izt2);
       }
     }
