@@ -664,33 +664,67 @@ k_near_sigma_split(const NearArgs a, int R, int NJ, const double* __restrict__ g
 }
 
 // The self pairs of the mixed replay in FP64: per source point of the leaf
-// (thread) and right-hand side (blockIdx.y), the FP64 stored block times the
-// FP64 densities of the point's own triangle, ADDED to the outputs.
+// (thread) and group of SELF_RB right-hand sides (blockIdx.y), the FP64
+// stored block (NJ density components x KB outputs, read once into
+// registers) times the FP64 densities of the point's own triangle, ADDED to
+// the outputs.
+constexpr int SELF_RB = 8;
+template <int NJ, int KB>
 __global__ void __launch_bounds__(128)
-k_near_self64(const NearArgs a, int R, int K, int KB, const double* __restrict__ g0, const double* __restrict__ g1,
+k_near_self64(const NearArgs a, int R, const double* __restrict__ g0, const double* __restrict__ g1,
               const long long* __restrict__ base, const int* __restrict__ ntri, const double* __restrict__ store,
               int nsrc) {
-  const int i = blockIdx.x, r = blockIdx.y, leaf = a.leaves[i];
+  constexpr int K = NJ * KB;
+  const int i = blockIdx.x, r0 = blockIdx.y * SELF_RB, leaf = a.leaves[i];
   const int s0 = a.box_src_start[leaf], sn = a.do_src ? a.box_src_count[leaf] : 0;
   const int self = near_self_pos(a, i, leaf);
   if (self < 0) return;
   const long long nt = ntri[i];
-  const int NJ = K / KB;
+  const int rn = min(SELF_RB, R - r0);
   for (int e = threadIdx.x; e < sn; e += blockDim.x) {
     const int pid = s0 + e;
     const double* blk = store + base[i] + ((long long)e * nt + self + e) * K;
-    double out[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int j = 0; j < NJ; j++) {
-      const double sv = (j >= 3 ? g1 : g0)[((size_t)pid * 3 + (j % 3)) * R + r];
-      for (int c = 0; c < KB; c++) out[c] += blk[j * KB + c] * sv;
-    }
-    double* U = a.u_src + 3 * ((size_t)nsrc * r + pid);
-    for (int c = 0; c < 3; c++) U[c] += out[c];
-    if (KB == 9 && a.dostrain_src) {
-      double* E = a.e_src + 6 * ((size_t)nsrc * r + pid);
-      for (int c = 0; c < 6; c++) E[c] += out[3 + c];
+    double bk[K];
+#pragma unroll
+    for (int k = 0; k < K; k++) bk[k] = blk[k];
+    for (int rr = 0; rr < rn; rr++) {
+      const int r = r0 + rr;
+      double out[KB];
+#pragma unroll
+      for (int c = 0; c < KB; c++) out[c] = 0.0;
+#pragma unroll
+      for (int j = 0; j < NJ; j++) {
+        const double sv = (j >= 3 ? g1 : g0)[((size_t)pid * 3 + (j % 3)) * R + r];
+#pragma unroll
+        for (int c = 0; c < KB; c++) out[c] += bk[j * KB + c] * sv;
+      }
+      double* U = a.u_src + 3 * ((size_t)nsrc * r + pid);
+#pragma unroll
+      for (int c = 0; c < 3; c++) U[c] += out[c];
+      if (KB == 9 && a.dostrain_src) {
+        double* E = a.e_src + 6 * ((size_t)nsrc * r + pid);
+#pragma unroll
+        for (int c = 0; c < 6; c++) E[c] += out[3 + c];
+      }
     }
   }
+}
+
+static void launch_near_self64(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, const double* g0,
+                               const double* g1, const long long* base, const int* ntri, const double* store,
+                               int nsrc) {
+  const dim3 grid(a.nleaf, (R + SELF_RB - 1) / SELF_RB);
+  if (NJ == 3 && KB == 3)
+    k_near_self64<3, 3><<<grid, 128, 0, st>>>(a, R, g0, g1, base, ntri, store, nsrc);
+  else if (NJ == 3 && KB == 9)
+    k_near_self64<3, 9><<<grid, 128, 0, st>>>(a, R, g0, g1, base, ntri, store, nsrc);
+  else if (NJ == 6 && KB == 3)
+    k_near_self64<6, 3><<<grid, 128, 0, st>>>(a, R, g0, g1, base, ntri, store, nsrc);
+  else if (NJ == 6 && KB == 9)
+    k_near_self64<6, 9><<<grid, 128, 0, st>>>(a, R, g0, g1, base, ntri, store, nsrc);
+  else
+    throw CudaError{(int)cudaErrorInvalidValue};
+  count_launch();
 }
 
 // Near densities of each leaf as the B operand: S[r][NJ t + j] at soff[leaf]
@@ -767,8 +801,7 @@ void launch_near_split(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB
   k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
   count_launch();
   if (a.do_src) {
-    k_near_self64<<<dim3(a.nleaf, R), 128, 0, st>>>(a, R, NJ * KB, KB, g0, g1, base, ntri, store, nsrc);
-    count_launch();
+    launch_near_self64(st, a, R, NJ, KB, g0, g1, base, ntri, store, nsrc);
   }
   EFMM_CUDA_TRY(cudaGetLastError());
 }
@@ -784,8 +817,7 @@ void launch_near_tc(cudaStream_t st, const NearArgs& a, int R, int NJ, int KB, c
   k_near_scatter_tc<<<dim3(a.nleaf, R), 256, 0, st>>>(a, R, KB, coff, C, nsrc, ntgt);
   count_launch();
   if (a.do_src) {
-    k_near_self64<<<dim3(a.nleaf, R), 128, 0, st>>>(a, R, NJ * KB, KB, g0, g1, base, ntri, store, nsrc);
-    count_launch();
+    launch_near_self64(st, a, R, NJ, KB, g0, g1, base, ntri, store, nsrc);
   }
   EFMM_CUDA_TRY(cudaGetLastError());
 }
