@@ -763,21 +763,42 @@ std::vector<IterSlot*> g_iter;
 long long g_iter_next_id = 1, g_iter_clock = 0;
 
 // 64-bit FNV-1a over the geometry bytes, kept to 53 bits so it is exact in a double
+// A 64-bit hash of the geometry arrays (a repeated call must bring the
+// geometry its store was made for): the words of each array go round-robin
+// into eight independent multiply-xorshift lanes (no serial chain through
+// all the bytes: about a word per cycle), which are folded with the array
+// lengths at the end.
 double geometry_checksum(const double* tri, const double* nrm, const double* src, int n,
                          const double* tgt, int nt) {
-  unsigned long long h = 1469598103934665603ull;
+  constexpr unsigned long long K = 0x9E3779B97F4A7C15ull;
+  unsigned long long h[8];
+  for (int l = 0; l < 8; l++) h[l] = 0x243F6A8885A308D3ull + (unsigned long long)l * K;
   auto mix = [&](const double* a, size_t cnt) {
-    const unsigned char* b = reinterpret_cast<const unsigned char*>(a);
-    for (size_t i = 0; i < cnt * sizeof(double); i++) {
-      h ^= b[i];
-      h *= 1099511628211ull;
+    size_t i = 0;
+    for (; i + 8 <= cnt; i += 8)
+      for (int l = 0; l < 8; l++) {
+        unsigned long long w;
+        std::memcpy(&w, a + i + l, sizeof(w));
+        h[l] = (h[l] ^ w) * K;
+        h[l] ^= h[l] >> 29;
+      }
+    for (; i < cnt; i++) {
+      unsigned long long w;
+      std::memcpy(&w, a + i, sizeof(w));
+      h[0] = (h[0] ^ w) * K;
+      h[0] ^= h[0] >> 29;
     }
   };
   mix(tri, 9 * (size_t)n);
   mix(nrm, 3 * (size_t)n);
   mix(src, 3 * (size_t)n);
   if (nt > 0) mix(tgt, 3 * (size_t)nt);
-  return (double)(h >> 11);
+  unsigned long long x = ((unsigned long long)(unsigned)n << 32) ^ (unsigned)nt;
+  for (int l = 0; l < 8; l++) {
+    x = (x ^ h[l]) * K;
+    x ^= x >> 31;
+  }
+  return (double)(x >> 11);
 }
 
 IterSlot* iter_find(const double* wsave, int lwsave) {
