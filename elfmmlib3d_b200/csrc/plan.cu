@@ -738,6 +738,66 @@ void Plan::ensure_split() {
   P->rots_ready = true;
 }
 
+// parity-split U-kernel M2L operators (rotations.cu build_usplit_ops), once
+// per pool
+void Plan::ensure_usplit() {
+  ensure_uops();
+  std::lock_guard<std::mutex> lk(g_ops_mu);
+  OpPool* P = ops_;
+  if (P->us_ready) return;
+  std::vector<int> orders;
+  std::vector<double> offs;
+  for (const OpDesc& d : P->udescs) {
+    orders.push_back(d.p);
+    offs.insert(offs.end(), {d.d[0], d.d[1], d.d[2]});
+  }
+  std::vector<double> w(2 * (size_t)ncoef(p_));
+  for (int n = 0; n <= p_; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] =
+          std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<USOp> uops;
+  std::vector<float> upool;
+  double cross = 0;
+  build_usplit_ops(orders, offs, w, uops, upool, &cross);
+  h2d(P->us_ops, uops, st_);
+  h2d(P->us_pool, upool, st_);
+  EFMM_CUDA_TRY(cudaStreamSynchronize(st_));
+  P->us_ready = true;
+}
+
+bool Plan::usplit_on() const {
+  static const bool on = [] {
+    const char* e = getenv("ELFMM3D_USPLIT");
+    return !(e && e[0] == '0');
+  }();
+  return on && p_ <= 63;
+}
+
+// The U-kernel M2L (schedule m2lu_) in the parity-split form: per group and
+// part (re, im) 128 x 128 tiles of (coefficient rows, concatenated columns)
+void Plan::run_u_split(int C, const float* src, float* dst) {
+  ensure_usplit();
+  TransSched& S = m2lu_;
+  if (S.uC != C || S.upool != ops_) {
+    std::vector<TransTask> tasks;
+    for (auto& r : S.lev)
+      for (int q = r.first; q < r.first + r.second; q++) {
+        const TransSeg& g = S.segs[q];
+        const int ncols = g.npair * C, nc = ncoef(ops_->udescs[g.group].p);
+        for (int part = 0; part < 2; part++)
+          for (int c0 = 0; c0 < ncols; c0 += 128)
+            for (int r0 = 0; r0 < nc; r0 += 128) tasks.push_back({g.group, (part << 20) | r0, g.pair0, ncols, c0});
+      }
+    h2d(S.utasks, tasks, st_);
+    S.untask = (int)tasks.size();
+    S.uC = C;
+    S.upool = ops_;
+  }
+  launch_translate_us(st_, S.untask, S.utasks.get(), S.pairs.get(), ops_->us_ops.get(), ops_->us_pool.get(),
+                      2 * ncoef(p_), C, src, dst);
+}
+
 // The FP32 translations of orders <= 31 run in the parity-split form unless
 // ELFMM3D_ROT_SPLIT=0 (then the full-block kernels of rotations.cu).
 bool Plan::split_rot() const {
@@ -1290,8 +1350,13 @@ void Plan::translation_flops(int R, bool mixed, double* f) {
   add(m2m_u_, 0, 1.0 * R);
   add(m2lv_img_, 1, 6.0 * R);
   for (const TransSeg& g : m2lu_.segs) {
-    const double dim = ops_->udims[g.group];
-    f[1] += 2.0 * dim * dim * g.npair * R;
+    if (mixed && usplit_on()) {  // re block ncoef^2, im block (ncoef - p - 1)^2, two Rz
+      const double pg = ops_->udescs[g.group].p, nc = (pg + 1) * (pg + 2) / 2, ni = nc - pg - 1;
+      f[1] += (2.0 * (nc * nc + ni * ni) + 16.0 * nc) * g.npair * R;
+    } else {
+      const double dim = ops_->udims[g.group];
+      f[1] += 2.0 * dim * dim * g.npair * R;
+    }
   }
   add(l2l_img_, 2, 6.0 * R);
   add(l2l_img_u_, 2, 1.0 * R);
@@ -2229,6 +2294,7 @@ void Plan::ensure_uops() {
         descs.push_back(d);
       }
   P->umats.resize(off);
+  P->udescs = descs;
   DevBuf<OpDesc> dd;
   dd.resize(descs.size());
   EFMM_CUDA_TRY(cudaMemcpyAsync(dd.get(), descs.data(), descs.size() * sizeof(OpDesc), cudaMemcpyHostToDevice,
@@ -2678,7 +2744,10 @@ int Plan::image_pass(double rlam, double rmu, int R, const double* d_ssl, const 
       run_translations(m2m_u_, Cu, ops_->mats_f.get(), mp + nb * Cv * D, mp + nb * Cv * D);
       rec(3);
       run_translations(m2lv_img_, Cv, ops_->mats_f.get(), mp, lc);
-      run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
+      if (usplit_on())
+        run_u_split(Cu, mp + nb * Cv * D, lc + nb * Cv * D);
+      else
+        run_dense(m2lu_, Cu, ops_->umats_f.get(), mp + nb * Cv * D, lc + nb * Cv * D);
       rec(4);
       run_translations(l2l_img_, Cv, ops_->mats_f.get(), lc, lc);
       run_translations(l2l_img_u_, Cu, ops_->mats_f.get(), lc + nb * Cv * D, lc + nb * Cv * D);

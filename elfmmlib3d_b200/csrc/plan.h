@@ -60,7 +60,12 @@ struct OpPool {
   DevBuf<long long> uoff;
   DevBuf<int> udim, ukinds, m2lug_dev;
   std::vector<int> udims;
+  std::vector<OpDesc> udescs;  // the U groups (offsets, orders)
   int m2lu_group[343];
+  // the U-kernel M2L in the parity-split form (FP32), made on first use
+  bool us_ready = false;
+  DevBuf<USOp> us_ops;
+  DevBuf<float> us_pool;
 };
 
 struct Timings {  // milliseconds of the last evaluate(), CUDA events
@@ -99,6 +104,10 @@ struct TransSched {
     int task0, ntask, pmax;
   };
   std::vector<TcBatch> tcb;
+  // tiles of the parity-split U-kernel M2L (run_u_split), cut for uC
+  int uC = -1, untask = 0;
+  const void* upool = nullptr;
+  DevBuf<TransTask> utasks;
   void clear() {
     segs.clear();
     lev.clear();
@@ -111,6 +120,8 @@ struct TransSched {
     tcC = -1;
     tcpool = nullptr;
     tcb.clear();
+    uC = -1;
+    upool = nullptr;
   }
 };
 
@@ -379,6 +390,11 @@ class Plan {
   void cut_rot_tasks(TransSched& S, int C, int W);
   void ensure_factored(bool tc = false);
   void ensure_split();
+  // the U-kernel M2L in the parity-split form (mixed form; ELFMM3D_USPLIT=0:
+  // the dense FP32 operators)
+  void ensure_usplit();
+  bool usplit_on() const;
+  void run_u_split(int C, const float* src, float* dst);
   // whether the FP32 translations run in the parity-split form
   bool split_rot() const;
   // the FP32 translations of a schedule on the tensor cores (rot_tc.cu)

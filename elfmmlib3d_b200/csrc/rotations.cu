@@ -619,6 +619,127 @@ void build_split_ops(const std::vector<int>& kinds, const std::vector<int>& orde
   });
 }
 
+// ------------------------------ M2L of the half-space kernel U, parity split
+// U is unchanged by rotations about z and by the reflection y -> -y, so its
+// M2L operator for an offset d = (rho cos phi, rho sin phi, dz) is
+//   T(d) = M_out(Rz(phi)) T(d0) M_in(Rz(-phi)),  d0 = (rho, 0, dz),
+// and T(d0) (offset in the xz plane) never mixes the re and im parts: an
+// ncoef x ncoef re block and an im block (row and column of order 0 zero).
+// Groups with the same (rho, dz, order) share their blocks.
+
+namespace {
+// T(d) of the U kernel at order p in the factorial basis (rows and columns
+// 2 ncoef, row-major), from the same J table and entries as the device builder
+void u_dense(int p, const double d[3], std::vector<double>& T) {
+  const int nc = ncoef(p), dim = 2 * nc;
+  std::vector<cplx> J(ncoef(2 * p + 1));
+  u_harmonics(2 * p, d[0], d[1], d[2], J.data());
+  T.assign((size_t)dim * dim, 0.0);
+  for (int r = 0; r < nc; r++)
+    for (int c = 0; c < nc; c++) {
+      double rr, ri, ir, ii;
+      op_entry(0, J.data(), r, c, &rr, &ri, &ir, &ii);
+      T[(size_t)(2 * r) * dim + 2 * c] = rr;
+      T[(size_t)(2 * r) * dim + 2 * c + 1] = ri;
+      T[(size_t)(2 * r + 1) * dim + 2 * c] = ir;
+      T[(size_t)(2 * r + 1) * dim + 2 * c + 1] = ii;
+    }
+}
+}  // namespace
+
+void build_usplit_ops(const std::vector<int>& orders, const std::vector<double>& offsets, const std::vector<double>& w,
+                      std::vector<USOp>& ops, std::vector<float>& pool, double* cross) {
+  const int ng = (int)orders.size();
+  int pmax = 0;
+  for (int q : orders) pmax = std::max(pmax, q);
+  Fitter F;
+  F.init(pmax);
+  // distinct (rho^2, dz, order): the blocks
+  std::vector<long long> key(ng);
+  std::vector<int> bidx(ng);
+  std::vector<long long> bkeys;
+  std::vector<int> bg;  // a group of each block
+  for (int g = 0; g < ng; g++) {
+    const double* d = &offsets[3 * g];
+    const long long r2 = llround(d[0] * d[0] + d[1] * d[1]);
+    key[g] = (r2 * 64 + llround(d[2]) + 32) * 64 + orders[g];
+    int b = -1;
+    for (size_t q = 0; q < bkeys.size(); q++)
+      if (bkeys[q] == key[g]) b = (int)q;
+    if (b < 0) {
+      b = (int)bkeys.size();
+      bkeys.push_back(key[g]);
+      bg.push_back(g);
+    }
+    bidx[g] = b;
+  }
+  const int nbk = (int)bkeys.size();
+  ops.resize(ng);
+  long long off = 0;
+  std::vector<long long> boff(nbk);
+  for (int b = 0; b < nbk; b++) {
+    const int nc = ncoef(orders[bg[b]]), ld = (nc + 3) & ~3;
+    boff[b] = off;
+    off += 2LL * nc * ld;
+  }
+  for (int g = 0; g < ng; g++) {
+    const int nc = ncoef(orders[g]), ld = (nc + 3) & ~3;
+    ops[g].p = orders[g];
+    ops[g].ld = ld;
+    ops[g].re = boff[bidx[g]];
+    ops[g].im = boff[bidx[g]] + (long long)nc * ld;
+    ops[g].rzi = off;
+    off += 4LL * (orders[g] + 1);
+    ops[g].rzo = off;
+    off += 4LL * (orders[g] + 1);
+  }
+  pool.assign((size_t)off, 0.0f);
+  std::vector<double> bcross(nbk, 0.0);
+  parallel_for(nbk, [&](int b) {
+    const int g = bg[b], p = orders[g], nc = ncoef(p), dim = 2 * nc, ld = ops[g].ld;
+    const double* d = &offsets[3 * g];
+    const double d0[3] = {std::sqrt(d[0] * d[0] + d[1] * d[1]), 0.0, d[2]};
+    std::vector<double> T;
+    u_dense(p, d0, T);
+    double big = 0, cr = 0;
+    float* re = &pool[ops[g].re];
+    float* im = &pool[ops[g].im];
+    std::vector<int> mof(nc);
+    for (int n = 0; n <= p; n++)
+      for (int m = 0; m <= n; m++) mof[cidx(n, m)] = m;
+    for (int r = 0; r < nc; r++)
+      for (int c = 0; c < nc; c++) {
+        const double s = 1.0 / (w[2 * r] * w[2 * c]);  // local rows / w, multipole columns x w
+        const double a = T[(size_t)(2 * r) * dim + 2 * c], e = T[(size_t)(2 * r + 1) * dim + 2 * c + 1];
+        re[(size_t)r * ld + c] = (float)(a * s);
+        if (mof[r] > 0 && mof[c] > 0) im[(size_t)r * ld + c] = (float)(e * s);
+        big = std::max(big, std::fabs(a * s));
+        cr = std::max({cr, std::fabs(T[(size_t)(2 * r) * dim + 2 * c + 1] * s),
+                       std::fabs(T[(size_t)(2 * r + 1) * dim + 2 * c] * s)});
+      }
+    bcross[b] = cr / std::max(big, 1e-300);
+  });
+  parallel_for(ng, [&](int g) {
+    const int p = orders[g];
+    const double* d = &offsets[3 * g];
+    const double ph = (d[0] == 0.0 && d[1] == 0.0) ? 0.0 : std::atan2(d[1], d[0]);
+    double Qz[9], Qzt[9];
+    rot_z(-ph, Qz);
+    rot_z(ph, Qzt);
+    std::vector<double> full(rot_size(p)), rz;
+    F.rotation(0, p, Qz, full.data());
+    split_rz(full, p, rz);
+    for (int q = 0; q < 4 * (p + 1); q++) pool[ops[g].rzi + q] = (float)rz[q];
+    F.rotation(1, p, Qzt, full.data());
+    split_rz(full, p, rz);
+    for (int q = 0; q < 4 * (p + 1); q++) pool[ops[g].rzo + q] = (float)rz[q];
+  });
+  if (cross) {
+    *cross = 0;
+    for (double c : bcross) *cross = std::max(*cross, c);
+  }
+}
+
 // ------------------------------------------------------------------ kernel
 // One CTA per tile of NCT columns of one group.  The columns are staged in
 // shared memory (rows x NCT), rotated (X -> Y), shifted (Y -> X), rotated
@@ -1250,6 +1371,150 @@ void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tas
   EFMM_CUDA_TRY(cudaGetLastError());
 }
 
+// M2L of the half-space kernel U in the parity-split form (build_usplit_ops):
+// a task is one 128 x 128 output tile of one part (re or im block) of a
+// group, rows = coefficients, columns = the concatenated columns of the
+// group's pairs (as k_translate).  The B tile loader rotates each source
+// coefficient by Rz in on the way (both its re and im words, one part
+// kept); the epilogue adds the two terms of Rz out of every result into the
+// destination's re and im rows.  256 threads, 8 x 8 outputs per thread, K
+// tiles of 16 double-buffered in shared memory; half the multiply-adds of
+// the dense operator.
+constexpr int US_R = 128, US_C = 128, US_K = 16, US_PMAX = 63;
+struct UsMof {
+  unsigned char m[(US_PMAX + 1) * (US_PMAX + 2) / 2];
+};
+constexpr UsMof make_us_mof() {
+  UsMof t{};
+  for (int n = 0; n <= US_PMAX; n++)
+    for (int m = 0; m <= n; m++) t.m[n * (n + 1) / 2 + m] = (unsigned char)m;
+  return t;
+}
+__constant__ UsMof c_us_mof = make_us_mof();
+
+__global__ void __launch_bounds__(256, 2)
+k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
+               const USOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
+               const float* __restrict__ src, float* __restrict__ dst) {
+  __shared__ __align__(16) float As[2][US_K][US_R];
+  __shared__ __align__(16) float Bs[2][US_K][US_C];
+  const TransTask t = tasks[blockIdx.x];
+  const int part = t.row0 >> 20, r0 = t.row0 & 0xFFFFF;
+  const USOp op = ops[t.group];
+  const int nc = (op.p + 1) * (op.p + 2) / 2, ld = op.ld;
+  const float* A = pool + (part ? op.im : op.re);
+  const float4* rzi = reinterpret_cast<const float4*>(pool + op.rzi);
+  const float4* rzo = reinterpret_cast<const float4*>(pool + op.rzo);
+  const int tid = threadIdx.x;
+  // loader roles: A row (tid >> 1), k half (tid & 1); B column (tid & 127), k half (tid >> 7)
+  const int arow = tid >> 1, akh = (tid & 1) * 8;
+  const bool arow_ok = r0 + arow < nc;
+  const float* Ap = A + (size_t)(arow_ok ? r0 + arow : 0) * ld;
+  const int bcol = tid & 127, bkh = (tid >> 7) * 8;
+  const float* Bp = nullptr;
+  {
+    const int col = t.col0 + bcol;
+    if (col < t.ncols) {
+      const TransPair pr = pairs[t.pair0 + col / C];
+      Bp = src + ((size_t)pr.src * C + (col % C)) * D;
+    }
+  }
+  float ra[8], rb[8];
+  auto load = [&](int k0) {
+    const int ka = k0 + akh, kb = k0 + bkh;
+    if (arow_ok && ka + 8 <= nc) {
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float2 v = *reinterpret_cast<const float2*>(Ap + ka + 2 * i);
+        ra[2 * i] = v.x;
+        ra[2 * i + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 8; i++) ra[i] = (arow_ok && ka + i < nc) ? Ap[ka + i] : 0.0f;
+    }
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int c = kb + i;
+      float v = 0.0f;
+      if (Bp && c < nc) {
+        const float2 x = *reinterpret_cast<const float2*>(Bp + 2 * c);
+        const float4 R = __ldg(rzi + c_us_mof.m[c]);
+        v = part ? R.z * x.x + R.w * x.y : R.x * x.x + R.y * x.y;
+      }
+      rb[i] = v;
+    }
+  };
+  auto store = [&](int buf) {
+#pragma unroll
+    for (int i = 0; i < 8; i++) As[buf][akh + i][arow] = ra[i];
+#pragma unroll
+    for (int i = 0; i < 8; i++) Bs[buf][bkh + i][bcol] = rb[i];
+  };
+  const int tx = tid & 15, ty = tid >> 4;
+  float acc[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; i++)
+#pragma unroll
+    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+  const int nk = (nc + US_K - 1) / US_K;
+  load(0);
+  store(0);
+  __syncthreads();
+  for (int kt = 0; kt < nk; kt++) {
+    const int cur = kt & 1;
+    if (kt + 1 < nk) load((kt + 1) * US_K);
+#pragma unroll
+    for (int kk = 0; kk < US_K; kk++) {
+      float a[8], b[8];
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const float2 v = *reinterpret_cast<const float2*>(&As[cur][kk][ty * 8 + 2 * i]);
+        a[2 * i] = v.x;
+        a[2 * i + 1] = v.y;
+      }
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const float2 v = *reinterpret_cast<const float2*>(&Bs[cur][kk][32 * j + 2 * tx]);
+        b[2 * j] = v.x;
+        b[2 * j + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < 8; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] += a[i] * b[j];
+    }
+    if (kt + 1 < nk) store(cur ^ 1);
+    __syncthreads();
+  }
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int col = t.col0 + 32 * (j >> 1) + 2 * tx + (j & 1);
+    if (col >= t.ncols) continue;
+    const TransPair pr = pairs[t.pair0 + col / C];
+    float* dp = dst + ((size_t)pr.dst * C + (col % C)) * D;
+    const float al = (float)pr.alpha;
+#pragma unroll
+    for (int i = 0; i < 8; i++) {
+      const int r = r0 + ty * 8 + i;
+      if (r < nc) {
+        const float4 R = __ldg(rzo + c_us_mof.m[r]);
+        const float v = al * acc[i][j];
+        atomicAdd(dp + 2 * r, (part ? R.y : R.x) * v);
+        atomicAdd(dp + 2 * r + 1, (part ? R.w : R.z) * v);
+      }
+    }
+  }
+}
+
+void launch_translate_us(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs, const USOp* ops,
+                         const float* pool, int D, int C, const float* src, float* dst) {
+  if (ntask <= 0) return;
+  k_translate_us<<<ntask, 256, 0, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
+  count_launch();
+  EFMM_CUDA_TRY(cudaGetLastError());
+}
+
 // The warp-block kernel for launches of orders pmin..31 (smaller orders
 // have fewer blocks than warps: the coefficient-tile kernel serves them).
 bool rot_warp_blocks_ok(int maxdim) {
@@ -1606,4 +1871,110 @@ extern "C" int efmm_rot_split_selfcheck_device(int p, int C, int npair, unsigned
 extern "C" int efmm_rot_split_bench(int p, int C, int npair, int engine, int reps, double* ms) {
   if (reps < 1 || !ms) return 16;
   return rot_split_device_run(p, C, npair, 1, engine, reps, nullptr, ms);
+}
+
+// CPU self-check of the parity-split U-kernel M2L (no device needed), over
+// every stride-th of the U groups (offsets with max |i|, |j|, |k| in 2..3,
+// dz >= 0) at order p and tolerance eps: worst[0] the split in double (Rz
+// fitted, blocks of T(d0)) against T(d), worst[1] the packed FP32 pool
+// applied as the kernel reads it, worst[2] the re / im coupling dropped.
+extern "C" int efmm_usplit_selfcheck(int p, double eps, int stride, double* worst) {
+  using namespace efmm;
+  if (p < 1 || p > 40 || !worst) return -1;
+  std::vector<int> orders;
+  std::vector<double> offs;
+  for (int i = -3; i <= 3; i++)
+    for (int j = -3; j <= 3; j++)
+      for (int k = 0; k <= 3; k++) {
+        if (std::max(std::abs(i), std::max(std::abs(j), std::abs(k))) < 2) continue;
+        orders.push_back(std::min(p, eps > 0 ? m2l_order(eps, i, j, k) : p));
+        offs.insert(offs.end(), {(double)i, (double)j, (double)k});
+      }
+  std::vector<double> w(2 * (size_t)ncoef(p));
+  for (int n = 0; n <= p; n++)
+    for (int m = 0; m <= n; m++)
+      w[2 * cidx(n, m)] = w[2 * cidx(n, m) + 1] = std::exp(0.5 * (std::lgamma(n + m + 1.0) + std::lgamma(n - m + 1.0)));
+  std::vector<USOp> ops;
+  std::vector<float> pool;
+  build_usplit_ops(orders, offs, w, ops, pool, &worst[2]);
+  Fitter F;
+  F.init(p);
+  worst[0] = worst[1] = 0;
+  std::mt19937_64 rng(13);
+  std::normal_distribution<double> N01;
+  for (int g = 0; g < (int)orders.size(); g += std::max(stride, 1)) {
+    const int pg = orders[g], nc = ncoef(pg), dim = 2 * nc;
+    const double* d = &offs[3 * g];
+    std::vector<double> T, T0;
+    u_dense(pg, d, T);
+    const double d0[3] = {std::sqrt(d[0] * d[0] + d[1] * d[1]), 0.0, d[2]};
+    u_dense(pg, d0, T0);
+    const double ph = (d[0] == 0.0 && d[1] == 0.0) ? 0.0 : std::atan2(d[1], d[0]);
+    double Qz[9], Qzt[9];
+    rot_z(-ph, Qz);
+    rot_z(ph, Qzt);
+    std::vector<double> full(rot_size(pg)), ri, ro;
+    F.rotation(0, pg, Qz, full.data());
+    split_rz(full, pg, ri);
+    F.rotation(1, pg, Qzt, full.data());
+    split_rz(full, pg, ro);
+    std::vector<int> mof(nc);
+    for (int n = 0; n <= pg; n++)
+      for (int m = 0; m <= n; m++) mof[cidx(n, m)] = m;
+    // a random multipole expansion of a real field, O(1) in the normalised basis
+    std::vector<double> v(dim), a(dim, 0.0), x(dim), y(dim, 0.0), xn(dim), yn(dim, 0.0);
+    for (int q = 0; q < dim; q++) v[q] = N01(rng) / w[q];
+    for (int c = 0; c < nc; c++)
+      if (mof[c] == 0) v[2 * c + 1] = 0.0;
+    for (int r = 0; r < dim; r++)
+      for (int c = 0; c < dim; c++) a[r] += T[(size_t)r * dim + c] * v[c];
+    // double: y = Rz_out T0 Rz_in v (re / im blocks of T0 only)
+    for (int c = 0; c < nc; c++) {
+      const double* R = &ri[4 * mof[c]];
+      x[2 * c] = R[0] * v[2 * c] + R[1] * v[2 * c + 1];
+      x[2 * c + 1] = R[2] * v[2 * c] + R[3] * v[2 * c + 1];
+    }
+    std::vector<double> t(dim, 0.0);
+    for (int r = 0; r < nc; r++)
+      for (int c = 0; c < nc; c++) {
+        t[2 * r] += T0[(size_t)(2 * r) * dim + 2 * c] * x[2 * c];
+        t[2 * r + 1] += T0[(size_t)(2 * r + 1) * dim + 2 * c + 1] * x[2 * c + 1];
+      }
+    for (int r = 0; r < nc; r++) {
+      const double* R = &ro[4 * mof[r]];
+      y[2 * r] = R[0] * t[2 * r] + R[1] * t[2 * r + 1];
+      y[2 * r + 1] = R[2] * t[2 * r] + R[3] * t[2 * r + 1];
+    }
+    // the packed FP32 pool as the kernel reads it (normalised basis)
+    const USOp& o = ops[g];
+    for (int c = 0; c < nc; c++) {
+      const float* R = &pool[o.rzi + 4 * mof[c]];
+      const double re = v[2 * c] * w[2 * c], im = v[2 * c + 1] * w[2 * c + 1];
+      xn[2 * c] = R[0] * re + R[1] * im;
+      xn[2 * c + 1] = R[2] * re + R[3] * im;
+    }
+    for (int r = 0; r < nc; r++) {
+      double sr = 0, si = 0;
+      for (int c = 0; c < nc; c++) {
+        sr += pool[o.re + (size_t)r * o.ld + c] * xn[2 * c];
+        si += pool[o.im + (size_t)r * o.ld + c] * xn[2 * c + 1];
+      }
+      const float* R = &pool[o.rzo + 4 * mof[r]];
+      yn[2 * r] = (R[0] * sr + R[1] * si) * w[2 * r];
+      yn[2 * r + 1] = (R[2] * sr + R[3] * si) * w[2 * r + 1];
+    }
+    double num0 = 0, num1 = 0, den = 0;
+    for (int c = 0; c < nc; c++)
+      for (int part = 0; part < 2; part++) {
+        if (mof[c] == 0 && part == 1) continue;
+        const int q = 2 * c + part;
+        const double sc = 1.0 / w[q];  // the normalised local basis
+        num0 += (a[q] - y[q]) * (a[q] - y[q]) * sc * sc;
+        num1 += (a[q] - yn[q]) * (a[q] - yn[q]) * sc * sc;
+        den += a[q] * a[q] * sc * sc;
+      }
+    worst[0] = std::max(worst[0], std::sqrt(num0 / std::max(den, 1e-300)));
+    worst[1] = std::max(worst[1], std::sqrt(num1 / std::max(den, 1e-300)));
+  }
+  return (int)orders.size();
 }

@@ -68,6 +68,21 @@ void build_split_ops(const std::vector<int>& kinds, const std::vector<int>& orde
 // Whether the split kernel serves a launch whose largest operator size is maxdim.
 bool rot_split_ok(int maxdim);
 
+// M2L of the half-space kernel U in the parity-split form (FP32 normalised
+// pool): per group the order, the leading dimension of its blocks (ncoef
+// rounded up to 4), the offsets (floats) of its re and im blocks (row-major,
+// shared by the groups with the same (rho, dz, order)) and of its Rz in /
+// out tables (4 per order m).
+struct USOp {
+  int p, ld;
+  long long re, im, rzi, rzo;
+};
+// orders[g] and offsets d[g] (box units, dz >= 0) of the U groups; w:
+// normalisation per real row; *cross: the largest re / im coupling dropped
+// (relative to the block's largest entry).
+void build_usplit_ops(const std::vector<int>& orders, const std::vector<double>& offsets, const std::vector<double>& w,
+                      std::vector<USOp>& ops, std::vector<float>& pool, double* cross);
+
 struct TransTask;
 struct TransPair;
 
@@ -84,6 +99,12 @@ void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tas
                                 float* dst, int variant = 0);
 // Columns per CTA of the split kernel.
 int rot_split_cols();
+
+// The U-kernel M2L in the parity-split form: tasks (group, row0 = part <<
+// 20 | first coefficient row, pair0, columns, first column) of 128 x 128
+// tiles, orders <= 63; ADDS into dst.
+void launch_translate_us(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs, const USOp* ops,
+                         const float* pool, int D, int C, const float* src, float* dst);
 
 // Columns per CTA of the factored kernel for a given largest operator size.
 int rot_cols_per_cta(int maxdim, int elem_bytes);

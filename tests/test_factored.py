@@ -47,3 +47,20 @@ def test_parity_split_equals_dense(lib, p, eps, stride):
     assert f(p, eps, stride, worst) == 316 + 16
     assert worst[0] < 1e-12
     assert worst[1] < 1e-6
+
+
+@pytest.mark.parametrize("p,eps,stride", [(6, 0.5e-2, 1), (14, 0.5e-3, 3), (30, 5e-8, 17), (39, 5e-10, 41)])
+def test_u_kernel_m2l_parity_split(lib, p, eps, stride):
+    """The half-space U-kernel M2L as Rz out, the re / im blocks of the
+    operator at the offset rotated into the xz plane, Rz in: in double
+    against the dense operator, and the packed FP32 pool as the kernel reads
+    it; the dropped re / im coupling is zero (U is even in y)."""
+    L = lib.load()
+    f = L.efmm_usplit_selfcheck
+    f.restype = ctypes.c_int
+    f.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_double)]
+    worst = (ctypes.c_double * 3)(1.0, 1.0, 1.0)
+    assert f(p, eps, stride, worst) == 178
+    assert worst[0] < 1e-12
+    assert worst[1] < 1e-6
+    assert worst[2] < 1e-12
