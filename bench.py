@@ -1034,14 +1034,14 @@ def run_hsbatch(args, rank, world, local_rank):
     tr_ach = tr_flops / (tr_ms * 1e-3) / 1e12
     roof = {"kernel": "k_translate_rot_s (parity-split factored M2M / M2L / L2L: Rz, the re / im blocks of "
                       "Ry and of the z shift, Ry back, Rz back; paired FP32 FMAs, both plans; the largest share "
-                      "of the step's launch time)",
+                      "of the step's launch time) with the image U-kernel M2L (k_translate_us, parity split)",
             "bound": "fp32", "achieved": tr_ach, "peak": peak32, "unit": "TFLOP/s",
             "frac": tr_ach / peak32 if peak32 else None, "traffic": None,
             "peak_source": "measured cuBLAS SGEMM 8192^3 with TF32 off (best of 5) in this run; the FP32 FMA "
                            "pipe (MEASURED_PEAKS.json has no FP32 entry)",
             "algorithmic": f"{tr_flops:.4g} useful FP32 flop per step (per box pair and column: two Ry of "
-                           f"sum_n (n+1)^2 + n^2, the z shift's re / im blocks, two Rz; per-offset orders) in "
-                           f"{tr_ms:.1f} ms of translation stages",
+                           f"sum_n (n+1)^2 + n^2, the z shift's re / im blocks, two Rz; the U-kernel M2L's re / "
+                           f"im blocks; per-offset orders) in {tr_ms:.1f} ms of translation stages",
             "flops_by_stage": {"free": trf, "image": tri_}}
     cpu, oerr = None, None
     if not args.no_cpu_baseline and world == 1:
