@@ -774,8 +774,8 @@ bool Plan::usplit_on() const {
   return on && p_ <= 63;
 }
 
-// The U-kernel M2L (schedule m2lu_) in the parity-split form: per group and
-// part (re, im) 128 x 128 tiles of (coefficient rows, concatenated columns)
+// The U-kernel M2L (schedule m2lu_) in the parity-split form: per group 64 x
+// 128 tiles of (coefficient rows, concatenated columns), both parts at once
 void Plan::run_u_split(int C, const float* src, float* dst) {
   ensure_usplit();
   TransSched& S = m2lu_;
@@ -785,9 +785,8 @@ void Plan::run_u_split(int C, const float* src, float* dst) {
       for (int q = r.first; q < r.first + r.second; q++) {
         const TransSeg& g = S.segs[q];
         const int ncols = g.npair * C, nc = ncoef(ops_->udescs[g.group].p);
-        for (int part = 0; part < 2; part++)
-          for (int c0 = 0; c0 < ncols; c0 += 128)
-            for (int r0 = 0; r0 < nc; r0 += 128) tasks.push_back({g.group, (part << 20) | r0, g.pair0, ncols, c0});
+        for (int c0 = 0; c0 < ncols; c0 += 128)
+          for (int r0 = 0; r0 < nc; r0 += 64) tasks.push_back({g.group, r0, g.pair0, ncols, c0});
       }
     h2d(S.utasks, tasks, st_);
     S.untask = (int)tasks.size();

@@ -1372,15 +1372,16 @@ void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tas
 }
 
 // M2L of the half-space kernel U in the parity-split form (build_usplit_ops):
-// a task is one 128 x 128 output tile of one part (re or im block) of a
-// group, rows = coefficients, columns = the concatenated columns of the
-// group's pairs (as k_translate).  The B tile loader rotates each source
-// coefficient by Rz in on the way (both its re and im words, one part
-// kept); the epilogue adds the two terms of Rz out of every result into the
-// destination's re and im rows.  256 threads, 8 x 8 outputs per thread, K
-// tiles of 16 double-buffered in shared memory; half the multiply-adds of
-// the dense operator.
-constexpr int US_R = 128, US_C = 128, US_K = 16, US_PMAX = 63;
+// a task is one output tile of 64 coefficient rows x 128 columns of a group
+// (columns: the concatenated columns of the group's pairs, as k_translate),
+// both parts at once: the B tile loader reads each source coefficient's re
+// and im words once and keeps both parts of its Rz in rotation, the CTA
+// accumulates the re block's and the im block's products side by side, and
+// the epilogue rotates each (re, im) result pair by Rz out and adds it into
+// the destination with one atomic per real row.  256 threads, 4 x 8 outputs
+// of each part per thread, K tiles of 16 double-buffered in shared memory;
+// half the multiply-adds of the dense operator.
+constexpr int US_R = 64, US_C = 128, US_K = 16, US_PMAX = 63;
 struct UsMof {
   unsigned char m[(US_PMAX + 1) * (US_PMAX + 2) / 2];
 };
@@ -1391,25 +1392,29 @@ constexpr UsMof make_us_mof() {
   return t;
 }
 __constant__ UsMof c_us_mof = make_us_mof();
+constexpr int US_SMEM = (int)sizeof(float) * 2 * US_K * (2 * US_R + 2 * US_C);
 
 __global__ void __launch_bounds__(256, 2)
 k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict__ pairs,
                const USOp* __restrict__ ops, const float* __restrict__ pool, int D, int C,
                const float* __restrict__ src, float* __restrict__ dst) {
-  __shared__ __align__(16) float As[2][US_K][US_R];
-  __shared__ __align__(16) float Bs[2][US_K][US_C];
+  extern __shared__ __align__(16) float us_smem[];
+  float* Ar = us_smem;                   // [2][US_K][US_R]
+  float* Ai = Ar + 2 * US_K * US_R;      // [2][US_K][US_R]
+  float* Br = Ai + 2 * US_K * US_R;      // [2][US_K][US_C]
+  float* Bi = Br + 2 * US_K * US_C;      // [2][US_K][US_C]
   const TransTask t = tasks[blockIdx.x];
-  const int part = t.row0 >> 20, r0 = t.row0 & 0xFFFFF;
+  const int r0 = t.row0;
   const USOp op = ops[t.group];
   const int nc = (op.p + 1) * (op.p + 2) / 2, ld = op.ld;
-  const float* A = pool + (part ? op.im : op.re);
   const float4* rzi = reinterpret_cast<const float4*>(pool + op.rzi);
   const float4* rzo = reinterpret_cast<const float4*>(pool + op.rzo);
   const int tid = threadIdx.x;
-  // loader roles: A row (tid >> 1), k half (tid & 1); B column (tid & 127), k half (tid >> 7)
-  const int arow = tid >> 1, akh = (tid & 1) * 8;
+  // loader roles: A row (tid >> 2), 4 k (tid & 3); B column (tid & 127), k half (tid >> 7)
+  const int arow = tid >> 2, akq = (tid & 3) * 4;
   const bool arow_ok = r0 + arow < nc;
-  const float* Ap = A + (size_t)(arow_ok ? r0 + arow : 0) * ld;
+  const float* Apr = pool + op.re + (size_t)(arow_ok ? r0 + arow : 0) * ld;
+  const float* Api = pool + op.im + (size_t)(arow_ok ? r0 + arow : 0) * ld;
   const int bcol = tid & 127, bkh = (tid >> 7) * 8;
   const float* Bp = nullptr;
   {
@@ -1419,44 +1424,54 @@ k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict_
       Bp = src + ((size_t)pr.src * C + (col % C)) * D;
     }
   }
-  float ra[8], rb[8];
+  float rar[4], rai[4], rbr[8], rbi[8];
   auto load = [&](int k0) {
-    const int ka = k0 + akh, kb = k0 + bkh;
-    if (arow_ok && ka + 8 <= nc) {
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const float2 v = *reinterpret_cast<const float2*>(Ap + ka + 2 * i);
-        ra[2 * i] = v.x;
-        ra[2 * i + 1] = v.y;
-      }
+    const int ka = k0 + akq, kb = k0 + bkh;
+    if (arow_ok && ka + 4 <= nc) {
+      const float4 u = *reinterpret_cast<const float4*>(Apr + ka);
+      const float4 v = *reinterpret_cast<const float4*>(Api + ka);
+      rar[0] = u.x; rar[1] = u.y; rar[2] = u.z; rar[3] = u.w;
+      rai[0] = v.x; rai[1] = v.y; rai[2] = v.z; rai[3] = v.w;
     } else {
 #pragma unroll
-      for (int i = 0; i < 8; i++) ra[i] = (arow_ok && ka + i < nc) ? Ap[ka + i] : 0.0f;
+      for (int i = 0; i < 4; i++) {
+        const bool ok = arow_ok && ka + i < nc;
+        rar[i] = ok ? Apr[ka + i] : 0.0f;
+        rai[i] = ok ? Api[ka + i] : 0.0f;
+      }
     }
 #pragma unroll
     for (int i = 0; i < 8; i++) {
       const int c = kb + i;
-      float v = 0.0f;
+      float vr = 0.0f, vi = 0.0f;
       if (Bp && c < nc) {
         const float2 x = *reinterpret_cast<const float2*>(Bp + 2 * c);
         const float4 R = __ldg(rzi + c_us_mof.m[c]);
-        v = part ? R.z * x.x + R.w * x.y : R.x * x.x + R.y * x.y;
+        vr = R.x * x.x + R.y * x.y;
+        vi = R.z * x.x + R.w * x.y;
       }
-      rb[i] = v;
+      rbr[i] = vr;
+      rbi[i] = vi;
     }
   };
   auto store = [&](int buf) {
 #pragma unroll
-    for (int i = 0; i < 8; i++) As[buf][akh + i][arow] = ra[i];
+    for (int i = 0; i < 4; i++) {
+      Ar[(buf * US_K + akq + i) * US_R + arow] = rar[i];
+      Ai[(buf * US_K + akq + i) * US_R + arow] = rai[i];
+    }
 #pragma unroll
-    for (int i = 0; i < 8; i++) Bs[buf][bkh + i][bcol] = rb[i];
+    for (int i = 0; i < 8; i++) {
+      Br[(buf * US_K + bkh + i) * US_C + bcol] = rbr[i];
+      Bi[(buf * US_K + bkh + i) * US_C + bcol] = rbi[i];
+    }
   };
   const int tx = tid & 15, ty = tid >> 4;
-  float acc[8][8];
+  float cr[4][8], ci[4][8];
 #pragma unroll
-  for (int i = 0; i < 8; i++)
+  for (int i = 0; i < 4; i++)
 #pragma unroll
-    for (int j = 0; j < 8; j++) acc[i][j] = 0.0f;
+    for (int j = 0; j < 8; j++) cr[i][j] = ci[i][j] = 0.0f;
   const int nk = (nc + US_K - 1) / US_K;
   load(0);
   store(0);
@@ -1466,23 +1481,26 @@ k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict_
     if (kt + 1 < nk) load((kt + 1) * US_K);
 #pragma unroll
     for (int kk = 0; kk < US_K; kk++) {
-      float a[8], b[8];
-#pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const float2 v = *reinterpret_cast<const float2*>(&As[cur][kk][ty * 8 + 2 * i]);
-        a[2 * i] = v.x;
-        a[2 * i + 1] = v.y;
-      }
+      const float4 ar = *reinterpret_cast<const float4*>(&Ar[(cur * US_K + kk) * US_R + ty * 4]);
+      const float4 ai = *reinterpret_cast<const float4*>(&Ai[(cur * US_K + kk) * US_R + ty * 4]);
+      const float a_r[4] = {ar.x, ar.y, ar.z, ar.w}, a_i[4] = {ai.x, ai.y, ai.z, ai.w};
+      float b_r[8], b_i[8];
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        const float2 v = *reinterpret_cast<const float2*>(&Bs[cur][kk][32 * j + 2 * tx]);
-        b[2 * j] = v.x;
-        b[2 * j + 1] = v.y;
+        const float2 u = *reinterpret_cast<const float2*>(&Br[(cur * US_K + kk) * US_C + 32 * j + 2 * tx]);
+        const float2 v = *reinterpret_cast<const float2*>(&Bi[(cur * US_K + kk) * US_C + 32 * j + 2 * tx]);
+        b_r[2 * j] = u.x;
+        b_r[2 * j + 1] = u.y;
+        b_i[2 * j] = v.x;
+        b_i[2 * j + 1] = v.y;
       }
 #pragma unroll
-      for (int i = 0; i < 8; i++)
+      for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] += a[i] * b[j];
+        for (int j = 0; j < 8; j++) {
+          cr[i][j] += a_r[i] * b_r[j];
+          ci[i][j] += a_i[i] * b_i[j];
+        }
     }
     if (kt + 1 < nk) store(cur ^ 1);
     __syncthreads();
@@ -1495,13 +1513,12 @@ k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict_
     float* dp = dst + ((size_t)pr.dst * C + (col % C)) * D;
     const float al = (float)pr.alpha;
 #pragma unroll
-    for (int i = 0; i < 8; i++) {
-      const int r = r0 + ty * 8 + i;
+    for (int i = 0; i < 4; i++) {
+      const int r = r0 + ty * 4 + i;
       if (r < nc) {
         const float4 R = __ldg(rzo + c_us_mof.m[r]);
-        const float v = al * acc[i][j];
-        atomicAdd(dp + 2 * r, (part ? R.y : R.x) * v);
-        atomicAdd(dp + 2 * r + 1, (part ? R.w : R.z) * v);
+        atomicAdd(dp + 2 * r, al * (R.x * cr[i][j] + R.y * ci[i][j]));
+        atomicAdd(dp + 2 * r + 1, al * (R.z * cr[i][j] + R.w * ci[i][j]));
       }
     }
   }
@@ -1510,7 +1527,8 @@ k_translate_us(const TransTask* __restrict__ tasks, const TransPair* __restrict_
 void launch_translate_us(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs, const USOp* ops,
                          const float* pool, int D, int C, const float* src, float* dst) {
   if (ntask <= 0) return;
-  k_translate_us<<<ntask, 256, 0, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
+  EFMM_CUDA_TRY(smem_raise(k_translate_us, US_SMEM));
+  k_translate_us<<<ntask, 256, US_SMEM, st>>>(tasks, pairs, ops, pool, D, C, src, dst);
   count_launch();
   EFMM_CUDA_TRY(cudaGetLastError());
 }

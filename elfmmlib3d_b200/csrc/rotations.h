@@ -100,9 +100,9 @@ void launch_translate_rot_split(cudaStream_t st, int ntask, const TransTask* tas
 // Columns per CTA of the split kernel.
 int rot_split_cols();
 
-// The U-kernel M2L in the parity-split form: tasks (group, row0 = part <<
-// 20 | first coefficient row, pair0, columns, first column) of 128 x 128
-// tiles, orders <= 63; ADDS into dst.
+// The U-kernel M2L in the parity-split form: tasks (group, first coefficient
+// row, pair0, columns, first column) of 64 x 128 tiles (both parts), orders
+// <= 63; ADDS into dst.
 void launch_translate_us(cudaStream_t st, int ntask, const TransTask* tasks, const TransPair* pairs, const USOp* ops,
                          const float* pool, int D, int C, const float* src, float* dst);
 
