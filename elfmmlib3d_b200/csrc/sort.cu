@@ -16,6 +16,9 @@
 // Scan: CTAs of 1024 ints scan in shared memory and write their sums, the
 // sums are scanned the same way (recursively), and a last kernel adds each
 // CTA's offset.
+#include <algorithm>
+#include <numeric>
+#include <random>
 #include <vector>
 #include "common.cuh"
 #include "sort.h"
@@ -230,9 +233,6 @@ void radix_sort_pairs(cudaStream_t st, const unsigned long long* kin, unsigned l
 // sort over the digits of [0, bits), compared with a stable host sort (keys
 // and values); the scan of n small ints against the host prefix sums.
 // Returns 0 and *bad = the number of mismatches (sorted keys, values, scan).
-#include <algorithm>
-#include <numeric>
-#include <random>
 extern "C" int efmm_sort_selfcheck_device(int n, int bits, unsigned seed, long long* bad) {
   using namespace efmm;
   if (n < 0 || n > (1 << 26) || bits < 1 || bits > 64 || !bad) return 16;
